@@ -1,0 +1,207 @@
+/*
+ * monc_gpu.h -- C ABI of the B200 dynamical-core library (libmoncgpu.so).
+ *
+ * The library replaces MONC's per-column dynamical-core components with whole-domain
+ * CUDA kernels that keep every prognostic field resident in GPU memory.  A MONC build
+ * binds these entry points from a Fortran `bind(C)` component module; Python binds them
+ * with ctypes (monc_b200/api.py).  Signatures use plain pointers, sizes and C structs.
+ *
+ * Reference interfaces replaced (paths inside the MONC source tree):
+ *   component descriptor / callbacks    model_core/src/components/monc_component.F90:62-118
+ *   group execution of callbacks        model_core/src/components/timestepper.F90:40-102
+ *   state container                     model_core/src/state.F90:55-141
+ *   prognostic field (z,y,x with halo)  model_core/src/grid/prognostics.F90:13-20
+ *
+ * Every function returns MGPU_OK (0) or a negative MGPU_ERR_* code; the message of the
+ * last failure on a handle is returned by mgpu_last_error().  Nothing traps on the device.
+ */
+#ifndef MONC_GPU_H
+#define MONC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGPU_MAX_NZ   1024
+#define MGPU_MAX_KGD  16
+#define MGPU_MAX_Q    8
+
+/* status codes */
+#define MGPU_OK                 0
+#define MGPU_ERR_ARGUMENT      -1   /* bad size, id or pointer */
+#define MGPU_ERR_CUDA          -2   /* a CUDA runtime call failed */
+#define MGPU_ERR_NOT_CONVERGED -3   /* iterative solver stopped at max_iterations */
+#define MGPU_ERR_TIMEOUT       -4   /* a bounded device-side wait gave up */
+#define MGPU_ERR_UNSUPPORTED   -5   /* option not implemented on this path */
+#define MGPU_ERR_NO_DEVICE     -6   /* no CUDA device visible */
+
+/* precision modes */
+#define MGPU_FP64        0  /* every field and every operation in FP64 (MONC's DEFAULT_PRECISION) */
+#define MGPU_FP32_MIXED  1  /* FP32 fields and stencils; FP64 tridiagonal, solver reductions, profiles */
+
+/* pressure solvers (fftsolver / iterativesolver components) */
+#define MGPU_SOLVER_FFT        0
+#define MGPU_SOLVER_ITERATIVE  1
+
+/* iterative solver types (iterativesolver.F90 solver_type) */
+#define MGPU_ITER_BICGSTAB 0
+#define MGPU_ITER_CG       1
+
+/* host array layouts accepted by upload/download */
+#define MGPU_LAYOUT_XFAST    0  /* C order [nz][ny][nx], interior only (the device layout) */
+#define MGPU_LAYOUT_MONC     1  /* Fortran data(nz, ny+4, nx+4): z fastest, 2-deep x/y halo */
+
+/* field identifiers (state.F90:86-92 names) */
+enum mgpu_field_id {
+  MGPU_U = 0, MGPU_V, MGPU_W, MGPU_TH,
+  MGPU_ZU, MGPU_ZV, MGPU_ZW, MGPU_ZTH,
+  MGPU_P,
+  MGPU_SU, MGPU_SV, MGPU_SW, MGPU_STH,
+  MGPU_VIS, MGPU_DIFF,
+  MGPU_SAVU, MGPU_SAVV, MGPU_SAVW,
+  MGPU_Q0 = 32,   /* q(n)  = MGPU_Q0  + n, n < MGPU_MAX_Q */
+  MGPU_ZQ0 = 48,  /* zq(n) = MGPU_ZQ0 + n */
+  MGPU_SQ0 = 64   /* sq(n) = MGPU_SQ0 + n */
+};
+
+/* component identifiers: the registered names of the MONC components this library replaces */
+enum mgpu_component_id {
+  MGPU_C_CLEARSOURCETERMS = 0,  /* clearsourceterms.F90:25-56 */
+  MGPU_C_STEPPING_DIRECTION,    /* steppingdirection.F90:41-49 */
+  MGPU_C_HALO_SWAPPER,          /* haloswapper.F90:62-71 */
+  MGPU_C_LOWER_BC,              /* lowerbc.F90:194-305 */
+  MGPU_C_SMAGORINSKY,           /* smagorinsky.F90:99-130 */
+  MGPU_C_PW_ADVECTION,          /* pwadvection.F90:258-610 */
+  MGPU_C_TVD_ADVECTION,         /* tvdadvection.F90:528-762 */
+  MGPU_C_DIFFUSION,             /* diffusion.F90:376-545 */
+  MGPU_C_VISCOSITY,             /* viscosity.F90:237-498 */
+  MGPU_C_CORIOLIS,              /* coriolis.F90:206-262 */
+  MGPU_C_BUOYANCY,              /* buoyancy.F90:190-269 */
+  MGPU_C_SET_CONSISTENT_LOWBC,  /* set_consistent_lowbc.F90:41-144 */
+  MGPU_C_SIMPLECLOUD,           /* simplecloud.F90:262-379 */
+  MGPU_C_DIVERR,                /* diverr.F90:44-175 */
+  MGPU_C_PSRCE,                 /* pressuresource.F90:61-238 */
+  MGPU_C_STEPFIELDS,            /* stepfields.F90:231-627 */
+  MGPU_C_FFTSOLVER,             /* fftsolver.F90:129-309 */
+  MGPU_C_ITERATIVESOLVER,       /* iterativesolver.F90:87-602 */
+  MGPU_C_PSTEP,                 /* pstep.F90:310-469 */
+  MGPU_C_SWAP_SMOOTH,           /* swapsmooth.F90:45-289 */
+  MGPU_C_COUNT
+};
+
+/* Model configuration: the option-database keys of MONC's global_config that the
+ * dynamical core reads (names in comments).  mgpu_config_defaults() fills the
+ * global_config defaults. */
+typedef struct mgpu_config {
+  int32_t nx, ny, nz;                 /* x_size, y_size, z_size */
+  int32_t n_kgd;                      /* number of kgd/hgd entries */
+  int32_t kgd[MGPU_MAX_KGD];          /* kgd */
+  double  hgd[MGPU_MAX_KGD];          /* hgd */
+  int32_t nsmth;                      /* nsmth (vertical grid smoothing passes) */
+  int32_t explicit_z;                 /* 1: w-level heights given in z_levels[0..nz-1] */
+  double  dxx, dyy, zztop;            /* dxx, dyy, zztop */
+  double  z_levels[MGPU_MAX_NZ];
+  double  thref0, rhobous;            /* thref0, rhobous */
+  double  surface_pressure, surface_reference_pressure;
+  double  rmlmax;                     /* rmlmax (<=0: 0.23*max(dxx,dyy), simplesetup.F90:234) */
+  double  dtm;                        /* dtm (fixed timestep, s) */
+  int32_t passive_th, passive_q;      /* passive_th, passive_q */
+  int32_t number_q_fields;            /* number_q_fields */
+  int32_t use_viscosity_and_diffusion;
+  int32_t use_surface_boundary_conditions;
+  int32_t type_of_surface_boundary_conditions;  /* 0 = prescribed flux */
+  double  surface_sensible_heat_flux; /* W m-2 */
+  double  surface_latent_heat_flux;   /* W m-2 */
+  int32_t coriolis_enabled;
+  double  fcoriol;
+  double  surface_geostrophic_wind_x, surface_geostrophic_wind_y;
+  double  smag_subb, smag_subc;       /* smag-subb, smag-subc */
+  int32_t simplecloud_enabled;
+  double  max_height_cloud;
+  int32_t solver;                     /* MGPU_SOLVER_* */
+  int32_t solver_type;                /* MGPU_ITER_* */
+  double  tolerance;                  /* tolerance */
+  int32_t max_iterations;             /* max_iterations */
+  int32_t precision;                  /* MGPU_FP64 / MGPU_FP32_MIXED */
+  /* science constants (global_config:355-372) */
+  double  von_karman_constant, z0, z0th, alphah, betam, betah, gammam, gammah;
+  double  pi, cp, rlvap, r, G, convective_limit, ratio_mol_wts, rlargep;
+} mgpu_config;
+
+/* Diagnostic reductions computed on the device after a step. */
+typedef struct mgpu_reductions {
+  double  global_divmax;              /* max |p| from diverr (diverr.F90:84-93) */
+  int32_t solver_iterations;          /* iterations of the last iterative solve */
+  double  solver_residual;            /* relative residual of the last iterative solve */
+  int32_t timestep;                   /* next MONC timestep number (1 = first, forward) */
+} mgpu_reductions;
+
+typedef struct mgpu_handle mgpu_handle;
+
+/* Fill a configuration with MONC's global_config defaults (global_config:100-372). */
+void mgpu_config_defaults(mgpu_config* cfg);
+
+/* Create a device-resident model: builds the vertical grid and reference state
+ * (replaces gridmanager.F90:2008-2075 + simplesetup.F90:60-126 initialisation callbacks)
+ * and allocates every field on the current CUDA device. */
+int mgpu_create(const mgpu_config* cfg, mgpu_handle** out);
+
+/* Release every device allocation (the finalisation callbacks). */
+int mgpu_destroy(mgpu_handle* h);
+
+/* Copy a field between host and device (host pointer to FP64 data).  In MONC layout the
+ * halo is ignored on upload and filled periodically on download. */
+int mgpu_upload_field(mgpu_handle* h, int32_t field_id, const double* host, int32_t layout);
+int mgpu_download_field(mgpu_handle* h, int32_t field_id, double* host, int32_t layout);
+
+/* Read back a 1-D vertical-grid profile (names as in grids.F90:91-159, e.g. "rdz",
+ * "tzc1", "czg", "rneutml_sq", "buoy_co"); n receives the length (nz). */
+int mgpu_get_profile(mgpu_handle* h, const char* name, double* out, int32_t* n);
+
+/* Host-only: build the reference state of a configuration without a device and return one
+ * profile (same names as mgpu_get_profile), for setup checks on machines without a GPU. */
+int mgpu_reference_profile(const mgpu_config* cfg, const char* name, double* out);
+
+/* Run one or more complete MONC timesteps (timestepper.F90:40-54 over the start, subgrid,
+ * dynamics, solver and pressure-terms groups) with the fused kernels. */
+int mgpu_step(mgpu_handle* h, int32_t nsteps);
+
+/* Run a single component's timestep callback over the whole domain (the `entire` group
+ * form of a column callback), for drop-in use and component-level parity tests. */
+int mgpu_component_timestep(mgpu_handle* h, int32_t component_id);
+
+/* Select forward (first-step) or centred stepping for component calls
+ * (steppingdirection.F90:41-49 sets this from the timestep number). */
+int mgpu_set_timestep(mgpu_handle* h, int32_t timestep);
+
+int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out);
+
+/* Horizontal-mean profile of a field (meanprofiles.F90:155-293 style sum / (nx*ny)). */
+int mgpu_mean_profile(mgpu_handle* h, int32_t field_id, double* out);
+
+/* CUDA stream used by the handle (cudaStream_t as void*), for callers that overlap work. */
+void* mgpu_stream(mgpu_handle* h);
+
+/* Number of kernels this handle has launched so far. */
+int64_t mgpu_launch_count(mgpu_handle* h);
+
+/* Horizontal-mean profiles computed on the device in FP64: mean theta (th + thref) and the
+ * mean of w squared per level (the domain-mean theta and w'^2 profiles used to judge runs);
+ * either pointer may be NULL.  Reads back 8*nz bytes per non-NULL pointer. */
+int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2);
+
+/* Per-stage device timing of mgpu_step (CUDA events on the handle's stream).  Stage order:
+ * 0 subgrid, 1 dynamics, 2 pressure source, 3 fft x forward, 4 fft y forward, 5 tridiagonal,
+ * 6 fft y inverse, 7 fft x inverse, 8 pstep + swap_smooth, 9 iterative solve. */
+#define MGPU_NSTAGES 10
+int mgpu_set_profiling(mgpu_handle* h, int32_t on);
+int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches);
+
+const char* mgpu_last_error(mgpu_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MONC_GPU_H */

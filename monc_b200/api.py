@@ -1,0 +1,309 @@
+"""Python binding of libmoncgpu.so and a host-side mirror of MONC's component API.
+
+`Model` owns one device-resident model (mgpu_create ... mgpu_destroy).  `component_descriptor`
+returns, for each dynamical-core component MONC registers (monc_component.F90:62-71), a
+descriptor with the same name and initialisation / timestep / finalisation callbacks, whose
+timestep callback runs the GPU kernel of that component over the whole domain -- the form a
+MONC `entire` group expects.
+
+The CUDA library is required: every entry point raises if libmoncgpu.so cannot be loaded or
+no CUDA device is visible; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import config as cf
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmoncgpu.so")
+
+OK = 0
+ERR_ARGUMENT = -1
+ERR_CUDA = -2
+ERR_NOT_CONVERGED = -3
+ERR_TIMEOUT = -4
+ERR_UNSUPPORTED = -5
+ERR_NO_DEVICE = -6
+
+LAYOUT_XFAST = 0
+LAYOUT_MONC = 1
+
+FIELDS = {
+    "u": 0, "v": 1, "w": 2, "th": 3, "zu": 4, "zv": 5, "zw": 6, "zth": 7, "p": 8,
+    "su": 9, "sv": 10, "sw": 11, "sth": 12, "vis": 13, "diff": 14,
+    "savu": 15, "savv": 16, "savw": 17,
+}
+Q0, ZQ0, SQ0 = 32, 48, 64
+
+STAGES = ["subgrid", "dynamics", "pressure_source", "fft_x_fwd", "fft_y_fwd", "tridiag", "fft_y_inv",
+          "fft_x_inv", "pstep_swap", "iterative"]
+
+# registered MONC component names -> mgpu_component_id
+COMPONENTS = {
+    "clearsourceterms": 0,
+    "stepping_direction": 1,
+    "halo_swapper": 2,
+    "lower_bc": 3,
+    "smagorinsky": 4,
+    "pw_advection": 5,
+    "tvd_advection": 6,
+    "diffusion": 7,
+    "viscosity": 8,
+    "coriolis": 9,
+    "buoyancy": 10,
+    "set_consistent_lowbc": 11,
+    "simplecloud": 12,
+    "diverr": 13,
+    "psrce": 14,
+    "stepfields": 15,
+    "fftsolver": 16,
+    "iterativesolver": 17,
+    "pstep": 18,
+    "swap_smooth": 19,
+}
+
+# MONC's default group layout of these components (global_config:77-92)
+GROUPS = {
+    "start": ["clearsourceterms", "stepping_direction", "halo_swapper"],
+    "subgrid": ["lower_bc", "smagorinsky"],
+    "dynamics": ["pw_advection", "tvd_advection", "diffusion", "viscosity", "coriolis", "buoyancy",
+                 "set_consistent_lowbc", "simplecloud", "diverr", "psrce", "stepfields"],
+    "solver": ["fftsolver", "iterativesolver"],
+    "pressure-terms": ["pstep", "swap_smooth"],
+}
+
+
+class MgpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libmoncgpu error {code}: {msg}")
+        self.code = code
+
+
+class Reductions(C.Structure):
+    _fields_ = [("global_divmax", C.c_double), ("solver_iterations", C.c_int32),
+                ("solver_residual", C.c_double), ("timestep", C.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libmoncgpu.so (building it first if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from .build import build
+        build()
+    L = C.CDLL(LIB_PATH)
+    L.mgpu_config_defaults.argtypes = [C.c_void_p]
+    L.mgpu_config_defaults.restype = None
+    L.mgpu_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.mgpu_create.restype = C.c_int
+    L.mgpu_destroy.argtypes = [C.c_void_p]
+    L.mgpu_destroy.restype = C.c_int
+    for name in ("mgpu_upload_field", "mgpu_download_field"):
+        f = getattr(L, name)
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        f.restype = C.c_int
+    L.mgpu_get_profile.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.POINTER(C.c_int32)]
+    L.mgpu_get_profile.restype = C.c_int
+    L.mgpu_step.argtypes = [C.c_void_p, C.c_int32]
+    L.mgpu_step.restype = C.c_int
+    L.mgpu_component_timestep.argtypes = [C.c_void_p, C.c_int32]
+    L.mgpu_component_timestep.restype = C.c_int
+    L.mgpu_set_timestep.argtypes = [C.c_void_p, C.c_int32]
+    L.mgpu_set_timestep.restype = C.c_int
+    L.mgpu_get_reductions.argtypes = [C.c_void_p, C.c_void_p]
+    L.mgpu_get_reductions.restype = C.c_int
+    L.mgpu_mean_profile.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.mgpu_mean_profile.restype = C.c_int
+    L.mgpu_stream.argtypes = [C.c_void_p]
+    L.mgpu_stream.restype = C.c_void_p
+    L.mgpu_launch_count.argtypes = [C.c_void_p]
+    L.mgpu_launch_count.restype = C.c_int64
+    L.mgpu_diagnostics.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mgpu_diagnostics.restype = C.c_int
+    L.mgpu_set_profiling.argtypes = [C.c_void_p, C.c_int32]
+    L.mgpu_set_profiling.restype = C.c_int
+    L.mgpu_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mgpu_stage_times.restype = C.c_int
+    L.mgpu_reference_profile.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+    L.mgpu_reference_profile.restype = C.c_int
+    L.mgpu_last_error.argtypes = [C.c_void_p]
+    L.mgpu_last_error.restype = C.c_char_p
+    _lib = L
+    return _lib
+
+
+def field_id(name_or_id) -> int:
+    if isinstance(name_or_id, (int, np.integer)):
+        return int(name_or_id)
+    name = str(name_or_id)
+    if name in FIELDS:
+        return FIELDS[name]
+    for prefix, base in (("zq", ZQ0), ("sq", SQ0), ("q", Q0)):
+        if name.startswith(prefix) and name[len(prefix):].isdigit():
+            return base + int(name[len(prefix):])
+    raise KeyError(name)
+
+
+def reference_profile(cfg: cf.MgpuConfig, name: str) -> np.ndarray:
+    """Host-only reference-state profile of a configuration (no device needed)."""
+    out = np.empty(cfg.nz, dtype=np.float64)
+    rc = lib().mgpu_reference_profile(C.byref(cfg), name.encode(), out.ctypes.data)
+    if rc != OK:
+        raise MgpuError(rc, f"reference profile {name}")
+    return out
+
+
+class Model:
+    """A device-resident MONC dynamical core on the current CUDA device."""
+
+    def __init__(self, cfg: cf.MgpuConfig):
+        self.cfg = cfg
+        self.nx, self.ny, self.nz = cfg.nx, cfg.ny, cfg.nz
+        h = C.c_void_p()
+        rc = lib().mgpu_create(C.byref(cfg), C.byref(h))
+        if rc != OK:
+            raise MgpuError(rc, "mgpu_create failed (no CUDA device, bad configuration or out of memory)")
+        self.h = h
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mgpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            msg = lib().mgpu_last_error(self.h)
+            raise MgpuError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    # -- data
+    def upload(self, name, arr: np.ndarray, layout: int = LAYOUT_XFAST):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if layout == LAYOUT_XFAST:
+            a = a.reshape(self.nz, self.ny, self.nx)
+        self._check(lib().mgpu_upload_field(self.h, field_id(name), a.ctypes.data, layout), f"upload {name}")
+
+    def download(self, name, layout: int = LAYOUT_XFAST) -> np.ndarray:
+        if layout == LAYOUT_XFAST:
+            a = np.empty((self.nz, self.ny, self.nx), dtype=np.float64)
+        else:
+            a = np.empty((self.nx + 4, self.ny + 4, self.nz), dtype=np.float64)
+        self._check(lib().mgpu_download_field(self.h, field_id(name), a.ctypes.data, layout), f"download {name}")
+        return a
+
+    def set_state(self, state: dict):
+        for k, v in state.items():
+            self.upload(k, v)
+
+    def profile(self, name: str) -> np.ndarray:
+        out = np.empty(self.nz, dtype=np.float64)
+        n = C.c_int32()
+        self._check(lib().mgpu_get_profile(self.h, name.encode(), out.ctypes.data, C.byref(n)), f"profile {name}")
+        return out
+
+    # -- stepping
+    def step(self, n: int = 1):
+        self._check(lib().mgpu_step(self.h, n), "step")
+
+    def component(self, name: str):
+        self._check(lib().mgpu_component_timestep(self.h, COMPONENTS[name]), f"component {name}")
+
+    def set_timestep(self, ts: int):
+        self._check(lib().mgpu_set_timestep(self.h, ts), "set_timestep")
+
+    def reductions(self) -> Reductions:
+        r = Reductions()
+        self._check(lib().mgpu_get_reductions(self.h, C.byref(r)), "reductions")
+        return r
+
+    def mean_profile(self, name) -> np.ndarray:
+        out = np.empty(self.nz, dtype=np.float64)
+        self._check(lib().mgpu_mean_profile(self.h, field_id(name), out.ctypes.data), "mean_profile")
+        return out
+
+    def diagnostics(self, out_th: np.ndarray | None = None, out_w2: np.ndarray | None = None):
+        """Device-computed horizontal means: theta (incl. thref) and w**2 per level."""
+        th = out_th if out_th is not None else np.empty(self.nz, dtype=np.float64)
+        w2 = out_w2 if out_w2 is not None else np.empty(self.nz, dtype=np.float64)
+        self._check(lib().mgpu_diagnostics(self.h, th.ctypes.data, w2.ctypes.data), "diagnostics")
+        return th, w2
+
+    def set_profiling(self, on: bool):
+        self._check(lib().mgpu_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def stage_times(self) -> dict:
+        ms = np.zeros(10, dtype=np.float64)
+        n = np.zeros(10, dtype=np.int64)
+        self._check(lib().mgpu_stage_times(self.h, ms.ctypes.data, n.ctypes.data), "stage_times")
+        return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(STAGES)}
+
+    @property
+    def stream(self) -> int:
+        return lib().mgpu_stream(self.h) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(lib().mgpu_launch_count(self.h))
+
+
+@dataclass
+class ComponentDescriptor:
+    """Mirror of component_descriptor_type (monc_component.F90:62-71)."""
+
+    name: str
+    version: float
+    initialisation: Optional[Callable] = None
+    timestep: Optional[Callable] = None
+    finalisation: Optional[Callable] = None
+
+
+def component_descriptor(name: str) -> ComponentDescriptor:
+    """The descriptor a MONC registry would receive for a GPU drop-in of `name`.
+
+    The callbacks take the `Model` that stands for `current_state`."""
+    if name not in COMPONENTS:
+        raise KeyError(f"no GPU drop-in for component {name}")
+
+    def timestep(model: Model):
+        model.component(name)
+
+    return ComponentDescriptor(name=name, version=0.1, timestep=timestep)
+
+
+def run_groups(model: Model, groups=("start", "subgrid", "dynamics", "solver", "pressure-terms")):
+    """One MONC timestep through the per-component entry points, in the configured group order
+    (timestepper.F90:40-54).  mgpu_step runs the same sequence with the fused kernels."""
+    solver = "fftsolver" if model.cfg.solver == cf.SOLVER_FFT else "iterativesolver"
+    for g in groups:
+        for name in GROUPS[g]:
+            if name in ("fftsolver", "iterativesolver") and name != solver:
+                continue
+            if name == "simplecloud" and not model.cfg.simplecloud_enabled:
+                continue
+            if name == "coriolis" and not model.cfg.coriolis_enabled:
+                continue
+            model.component(name)
+    ts = model.reductions().timestep
+    model.set_timestep(ts + 1)

@@ -1,0 +1,202 @@
+"""Model configuration for the B200 dynamical core.
+
+`MgpuConfig` mirrors `mgpu_config` in include/monc_gpu.h field for field.  Its defaults are
+MONC's `global_config` values (global_config:100-372) for the keys the dynamical core reads.
+
+`dry_cbl_config`, `moist_sc_config` ... build the synthetic workloads the benchmarks run
+(dry convective boundary layer, moist stratocumulus-like layer, large moist convective layer).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+MAX_NZ = 1024
+MAX_KGD = 16
+MAX_Q = 8
+
+FP64 = 0
+FP32_MIXED = 1
+SOLVER_FFT = 0
+SOLVER_ITERATIVE = 1
+ITER_BICGSTAB = 0
+ITER_CG = 1
+
+
+class MgpuConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("n_kgd", C.c_int32),
+        ("kgd", C.c_int32 * MAX_KGD),
+        ("hgd", C.c_double * MAX_KGD),
+        ("nsmth", C.c_int32),
+        ("explicit_z", C.c_int32),
+        ("dxx", C.c_double), ("dyy", C.c_double), ("zztop", C.c_double),
+        ("z_levels", C.c_double * MAX_NZ),
+        ("thref0", C.c_double), ("rhobous", C.c_double),
+        ("surface_pressure", C.c_double), ("surface_reference_pressure", C.c_double),
+        ("rmlmax", C.c_double),
+        ("dtm", C.c_double),
+        ("passive_th", C.c_int32), ("passive_q", C.c_int32),
+        ("number_q_fields", C.c_int32),
+        ("use_viscosity_and_diffusion", C.c_int32),
+        ("use_surface_boundary_conditions", C.c_int32),
+        ("type_of_surface_boundary_conditions", C.c_int32),
+        ("surface_sensible_heat_flux", C.c_double),
+        ("surface_latent_heat_flux", C.c_double),
+        ("coriolis_enabled", C.c_int32),
+        ("fcoriol", C.c_double),
+        ("surface_geostrophic_wind_x", C.c_double), ("surface_geostrophic_wind_y", C.c_double),
+        ("smag_subb", C.c_double), ("smag_subc", C.c_double),
+        ("simplecloud_enabled", C.c_int32),
+        ("max_height_cloud", C.c_double),
+        ("solver", C.c_int32),
+        ("solver_type", C.c_int32),
+        ("tolerance", C.c_double),
+        ("max_iterations", C.c_int32),
+        ("precision", C.c_int32),
+        ("von_karman_constant", C.c_double), ("z0", C.c_double), ("z0th", C.c_double),
+        ("alphah", C.c_double), ("betam", C.c_double), ("betah", C.c_double),
+        ("gammam", C.c_double), ("gammah", C.c_double),
+        ("pi", C.c_double), ("cp", C.c_double), ("rlvap", C.c_double), ("r", C.c_double),
+        ("G", C.c_double), ("convective_limit", C.c_double), ("ratio_mol_wts", C.c_double),
+        ("rlargep", C.c_double),
+    ]
+
+
+def default_config() -> MgpuConfig:
+    """A config holding MONC's global_config defaults (same values as mgpu_config_defaults)."""
+    c = MgpuConfig()
+    c.nx = c.ny = c.nz = 1
+    c.n_kgd = 1
+    c.kgd[0] = 10
+    c.hgd[0] = 10.0
+    c.nsmth = 40
+    c.explicit_z = 0
+    c.dxx = c.dyy = 1.0
+    c.zztop = 1.0
+    c.thref0 = 288.0
+    c.rhobous = 1.0
+    c.surface_pressure = 100000.0
+    c.surface_reference_pressure = 100000.0
+    c.rmlmax = -1.0
+    c.dtm = 0.001
+    c.passive_th = 1
+    c.passive_q = 1
+    c.number_q_fields = 0
+    c.use_viscosity_and_diffusion = 1
+    c.use_surface_boundary_conditions = 0
+    c.type_of_surface_boundary_conditions = 0
+    c.surface_sensible_heat_flux = 0.0
+    c.surface_latent_heat_flux = 0.0
+    c.coriolis_enabled = 0
+    c.fcoriol = 0.0
+    c.surface_geostrophic_wind_x = 0.0
+    c.surface_geostrophic_wind_y = 0.0
+    c.smag_subb = 40.0
+    c.smag_subc = 16.0
+    c.simplecloud_enabled = 0
+    c.max_height_cloud = 20000.0
+    c.solver = SOLVER_FFT
+    c.solver_type = ITER_BICGSTAB
+    c.tolerance = 1.0e-4
+    c.max_iterations = 500
+    c.precision = FP64
+    c.von_karman_constant = 0.4
+    c.z0 = 2.0e-3
+    c.z0th = 2.0e-4
+    c.alphah = 1.0
+    c.betam = 4.8
+    c.betah = 7.8
+    c.gammam = 19.3
+    c.gammah = 12.0
+    c.pi = 3.14159
+    c.cp = 1005.0
+    c.rlvap = 2.501e6
+    c.r = 287.05
+    c.G = 9.81
+    c.convective_limit = -0.5
+    c.ratio_mol_wts = 1.608
+    c.rlargep = 1.0e37
+    return c
+
+
+def dry_cbl_config(nx: int, ny: int, nz: int, dx: float, dz: float, dtm: float,
+                   ug: float = 0.0, fcoriol: float = 0.0, shf_kms: float = 0.1,
+                   cs: float = 0.23, thref0: float = 300.0, precision: int = FP64,
+                   solver: int = SOLVER_FFT) -> MgpuConfig:
+    """Dry convective boundary layer on a uniform vertical grid (dz, nz levels incl. level 1).
+
+    The surface sensible heat flux is given kinematically (K m/s); MONC takes W m-2 and divides
+    by rho(1)*cp (setfluxlook.F90:84-85), so the W m-2 value passed is shf_kms*rhobous*cp.
+    Cs maps to MONC's rmlmax = Cs*max(dx,dy) (simplesetup.F90:234 uses 0.23 as the default).
+    """
+    c = default_config()
+    c.nx, c.ny, c.nz = nx, ny, nz
+    c.dxx = c.dyy = float(dx)
+    c.zztop = dz * (nz - 1)
+    c.n_kgd = 1
+    c.kgd[0] = nz
+    c.hgd[0] = c.zztop
+    c.nsmth = 40
+    c.thref0 = thref0
+    c.rmlmax = cs * max(dx, dx)
+    c.dtm = dtm
+    c.passive_th = 0
+    c.passive_q = 1
+    c.use_surface_boundary_conditions = 1
+    c.type_of_surface_boundary_conditions = 0
+    c.surface_sensible_heat_flux = shf_kms * c.rhobous * c.cp
+    c.surface_latent_heat_flux = 0.0
+    c.z0 = 0.1
+    c.z0th = 0.1
+    if fcoriol != 0.0:
+        c.coriolis_enabled = 1
+        c.fcoriol = fcoriol
+        c.surface_geostrophic_wind_x = ug
+    c.precision = precision
+    c.solver = solver
+    return c
+
+
+def stretched_levels(nz: int, dz_bottom: float, dz_top: float, ztop: float | None = None):
+    """w-level heights with spacing growing geometrically from dz_bottom to dz_top.
+
+    When ztop is given the geometric ratio is solved so that the top level lands on ztop.
+    """
+    import numpy as np
+
+    n = nz - 1
+    if ztop is None:
+        r = (dz_top / dz_bottom) ** (1.0 / max(n - 1, 1))
+        dzs = dz_bottom * r ** np.arange(n)
+    else:
+        lo, hi = 1.0, 2.0
+        for _ in range(200):
+            mid = 0.5 * (lo + hi)
+            dzs = np.minimum(dz_bottom * mid ** np.arange(n), dz_top)
+            if dzs.sum() > ztop:
+                hi = mid
+            else:
+                lo = mid
+        dzs = np.minimum(dz_bottom * lo ** np.arange(n), dz_top)
+        dzs *= ztop / dzs.sum()
+    z = np.concatenate([[0.0], np.cumsum(dzs)])
+    return z
+
+
+def set_explicit_levels(c: MgpuConfig, z) -> None:
+    c.explicit_z = 1
+    c.nz = len(z)
+    c.zztop = float(z[-1])
+    for k, zk in enumerate(z):
+        c.z_levels[k] = float(zk)
+
+
+def config_dict(c: MgpuConfig) -> dict:
+    out = {}
+    for name, _ in MgpuConfig._fields_:
+        v = getattr(c, name)
+        if hasattr(v, "__len__"):
+            continue
+        out[name] = v
+    return out

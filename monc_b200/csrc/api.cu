@@ -1,0 +1,561 @@
+// C ABI of libmoncgpu.so (include/monc_gpu.h): device-resident model state, host<->device
+// transfers with the MONC <-> x-fastest layout change, the fused timestep driver and the
+// per-component entry points.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "dycore.h"
+
+using namespace mgpu;
+
+struct mgpu_handle {
+  mgpu_config cfg;
+  RefState rs;
+  Scalars sc;
+  int timestep = 1;
+  int device = 0;
+  bool fp32 = false;
+  cudaStream_t stream = nullptr;
+  double* prof_d = nullptr;
+  double* lookup_d = nullptr;
+  DevState<double> d64;
+  DevState<float> d32;
+  std::vector<void*> allocations;
+  bool component_fields = false;
+  FftPlanDev fft;
+  IterSolverDev* iter = nullptr;
+  unsigned long long* divmax_d = nullptr;
+  double global_divmax = 0.0;
+  int solver_iterations = 0;
+  double solver_residual = 0.0;
+  int64_t launches = 0;
+  double* xfer = nullptr;  // device staging buffer (FP64 field) for uploads/downloads
+  double* diag_d = nullptr;  // 2*nz FP64 diagnostics
+  bool profiling = false;
+  cudaEvent_t ev[16] = {};
+  double stage_ms[MGPU_NSTAGES] = {};
+  int64_t stage_n[MGPU_NSTAGES] = {};
+  std::string err;
+};
+
+static int fail(mgpu_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return fail(h, MGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static size_t field_elems(const mgpu_handle* h) { return (size_t)h->cfg.nx * h->cfg.ny * h->cfg.nz; }
+
+template <typename T>
+static int alloc_field(mgpu_handle* h, T** p) {
+  void* ptr = nullptr;
+  cudaError_t e = cudaMalloc(&ptr, field_elems(h) * sizeof(T));
+  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  cudaMemsetAsync(ptr, 0, field_elems(h) * sizeof(T), h->stream);
+  h->allocations.push_back(ptr);
+  *p = reinterpret_cast<T*>(ptr);
+  return MGPU_OK;
+}
+
+template <typename T>
+static int alloc_state(mgpu_handle* h, DevState<T>& d) {
+  std::memset(&d, 0, sizeof(d));
+  T** core[] = {&d.u, &d.v, &d.w, &d.th, &d.zu, &d.zv, &d.zw, &d.zth, &d.p, &d.vis, &d.diff,
+                &d.zu_n, &d.zv_n, &d.zw_n, &d.th_n, &d.zth_n};
+  for (T** pp : core) {
+    int rc = alloc_field<T>(h, pp);
+    if (rc) return rc;
+  }
+  for (int n = 0; n < h->cfg.number_q_fields; ++n) {
+    T** qq[] = {&d.q[n], &d.zq[n], &d.q_n[n], &d.zq_n[n]};
+    for (T** pp : qq) {
+      int rc = alloc_field<T>(h, pp);
+      if (rc) return rc;
+    }
+  }
+  return MGPU_OK;
+}
+
+template <typename T>
+static int alloc_component_fields(mgpu_handle* h, DevState<T>& d) {
+  if (h->component_fields) return MGPU_OK;
+  T** extra[] = {&d.su, &d.sv, &d.sw, &d.sth, &d.savu, &d.savv, &d.savw};
+  for (T** pp : extra) {
+    int rc = alloc_field<T>(h, pp);
+    if (rc) return rc;
+  }
+  for (int n = 0; n < h->cfg.number_q_fields; ++n) {
+    int rc = alloc_field<T>(h, &d.sq[n]);
+    if (rc) return rc;
+  }
+  h->component_fields = true;
+  return MGPU_OK;
+}
+
+static void fill_scalars(mgpu_handle* h) {
+  const mgpu_config& c = h->cfg;
+  const RefState& r = h->rs;
+  Scalars& s = h->sc;
+  std::memset(&s, 0, sizeof(s));
+  s.nx = c.nx; s.ny = c.ny; s.nz = c.nz;
+  s.plane = (long long)c.nx * c.ny;
+  s.cx = r.cx; s.cy = r.cy; s.cx2 = r.cx2; s.cy2 = r.cy2; s.tcx = r.tcx; s.tcy = r.tcy;
+  s.dtm = c.dtm; s.tsmth = 1e-2; s.ugal = 0.0; s.vgal = 0.0;
+  s.fcoriol = c.fcoriol; s.smallp = r.smallp;
+  s.czn = r.czn; s.zn2 = r.zn[2]; s.zlogm = r.zlogm; s.zlogth = r.zlogth; s.vk_on_zlogm = r.vk_on_zlogm;
+  s.vk = c.von_karman_constant; s.z0 = c.z0; s.z0th = c.z0th; s.alphah = c.alphah; s.betam = c.betam;
+  s.betah = c.betah; s.gammah = c.gammah; s.pi = c.pi;
+  s.surface_temperature_flux = r.surface_temperature_flux; s.surface_vapour_flux = r.surface_vapour_flux;
+  s.fbuoy = r.fbuoy;
+  s.max_diff_or_visc = 1.7976931348623157e308;  // huge(0.5_DEFAULT_PRECISION): no surface-exchange limit
+  s.velmin = r.velmin; s.aloginv = r.aloginv; s.cneut = r.cneut; s.cfc = r.cfc;
+  s.convective_limit = c.convective_limit;
+  s.subb = c.smag_subb; s.subc = c.smag_subc; s.subg = 1.2; s.subh = 0.0;
+  s.suba = 1.0 / 0.7; s.ric = 0.25; s.ricinv = 1.0 / 0.25;
+  s.eps = 0.01; s.repsh = 0.5 / 0.01;
+  s.thcona = c.ratio_mol_wts * c.thref0; s.thconb = s.thcona - c.thref0; s.thconap1 = s.thcona;
+  s.rlvap_over_cp = r.rlvap_over_cp; s.G = c.G;
+  s.cq0 = r.cq.empty() ? 0.0 : r.cq[0];
+  s.lookup_entries = r.lookup_entries;
+  s.forward = 1;
+  s.passive_th = c.passive_th; s.passive_q = c.passive_q; s.nq = c.number_q_fields;
+  s.iqv = 0; s.iql = c.number_q_fields > 1 ? 1 : 0;
+  s.coriolis = c.coriolis_enabled; s.surface_bcs = c.use_surface_boundary_conditions;
+  s.use_vd = c.use_viscosity_and_diffusion;
+  s.prof = h->prof_d;
+  s.lookup = h->lookup_d;
+}
+
+static const std::vector<double>* prof_vec(const RefState& r, int id) {
+  switch (id) {
+    case P_RDZ: return &r.rdz; case P_RDZN: return &r.rdzn; case P_DZN: return &r.dzn; case P_RHO: return &r.rho;
+    case P_RHON: return &r.rhon; case P_DTHREF: return &r.dthref; case P_CZB: return &r.czb; case P_CZA: return &r.cza;
+    case P_CZG: return &r.czg; case P_CZH: return &r.czh; case P_TZC1: return &r.tzc1; case P_TZC2: return &r.tzc2;
+    case P_TZD1: return &r.tzd1; case P_TZD2: return &r.tzd2; case P_RNEUTML_SQ: return &r.rneutml_sq;
+    case P_BUOY_CO: return &r.buoy_co; case P_THREF: return &r.thref; case P_PREFRCP: return &r.prefrcp;
+    case P_RPREFRCP: return &r.rprefrcp; case P_TREF: return &r.tref; case P_TSTARPR: return &r.tstarpr;
+    case P_QSAT: return &r.qsat; case P_DQSATDT: return &r.dqsatdt; case P_QSATFAC: return &r.qsatfac;
+    case P_GWX: return &r.gwx; case P_GWY: return &r.gwy;
+  }
+  return nullptr;
+}
+
+extern "C" {
+
+int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
+  if (!cfg || !out) return MGPU_ERR_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MGPU_ERR_NO_DEVICE;
+  mgpu_handle* h = new mgpu_handle();
+  h->cfg = *cfg;
+  cudaGetDevice(&h->device);
+  if (cfg->number_q_fields < 0 || cfg->number_q_fields > MGPU_MAX_Q || (cfg->nx % 2) || (cfg->ny % 2) ||
+      (cfg->precision != MGPU_FP64 && cfg->precision != MGPU_FP32_MIXED)) {
+    delete h;
+    return MGPU_ERR_ARGUMENT;
+  }
+  try {
+    build_reference_state(h->cfg, h->rs);
+  } catch (std::exception& e) {
+    std::fprintf(stderr, "mgpu_create: %s\n", e.what());
+    delete h;
+    return MGPU_ERR_ARGUMENT;
+  }
+  h->fp32 = cfg->precision == MGPU_FP32_MIXED;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return MGPU_ERR_CUDA; }
+  // profiles
+  const int stride = cfg->nz + 2;
+  std::vector<double> prof((size_t)P_COUNT * stride, 0.0);
+  for (int id = 0; id < P_COUNT; ++id) {
+    const std::vector<double>* v = prof_vec(h->rs, id);
+    for (int k = 0; k <= cfg->nz && k < (int)v->size(); ++k) prof[(size_t)id * stride + k] = (*v)[k];
+  }
+  int rc = MGPU_OK;
+  auto cleanup = [&](int code) { mgpu_destroy(h); return code; };
+  if (cudaMalloc(&h->prof_d, prof.size() * sizeof(double)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  cudaMemcpy(h->prof_d, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (cudaMalloc(&h->lookup_d, (h->rs.lookup_ustr.size() + 1) * sizeof(double)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  cudaMemcpy(h->lookup_d, h->rs.lookup_ustr.data(), h->rs.lookup_ustr.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (cudaMalloc(&h->divmax_d, sizeof(unsigned long long)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  cudaMemset(h->divmax_d, 0, sizeof(unsigned long long));
+  if (cudaMalloc(&h->xfer, field_elems(h) * sizeof(double)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  if (cudaMalloc(&h->diag_d, 2 * (size_t)cfg->nz * sizeof(double)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  for (cudaEvent_t& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  fill_scalars(h);
+  rc = h->fp32 ? alloc_state<float>(h, h->d32) : alloc_state<double>(h, h->d64);
+  if (rc) return cleanup(rc);
+  if (cfg->solver == MGPU_SOLVER_FFT) {
+    rc = fft_plan_create(h->fft, h->sc, h->rs, h->fp32);
+    if (rc) { std::fprintf(stderr, "mgpu_create: FFT solver needs power-of-two nx, ny\n"); return cleanup(rc); }
+  } else {
+    int st = MGPU_OK;
+    h->iter = iter_create(h->sc, h->rs, h->cfg, h->fp32, &st);
+    if (st) return cleanup(st);
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  *out = h;
+  return MGPU_OK;
+}
+
+int mgpu_destroy(mgpu_handle* h) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void* p : h->allocations) cudaFree(p);
+  h->allocations.clear();
+  if (h->fft.spec) fft_plan_destroy(h->fft);
+  if (h->iter) iter_destroy(h->iter);
+  cudaFree(h->prof_d);
+  cudaFree(h->lookup_d);
+  cudaFree(h->divmax_d);
+  cudaFree(h->xfer);
+  cudaFree(h->diag_d);
+  for (cudaEvent_t& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return MGPU_OK;
+}
+
+void* mgpu_stream(mgpu_handle* h) { return h ? (void*)h->stream : nullptr; }
+int64_t mgpu_launch_count(mgpu_handle* h) { return h ? h->launches : 0; }
+const char* mgpu_last_error(mgpu_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+}  // extern "C"
+
+// ---- field lookup -----------------------------------------------------------------------
+template <typename T>
+static T* field_ptr(mgpu_handle* h, DevState<T>& d, int id) {
+  switch (id) {
+    case MGPU_U: return d.u; case MGPU_V: return d.v; case MGPU_W: return d.w; case MGPU_TH: return d.th;
+    case MGPU_ZU: return d.zu; case MGPU_ZV: return d.zv; case MGPU_ZW: return d.zw; case MGPU_ZTH: return d.zth;
+    case MGPU_P: return d.p; case MGPU_VIS: return d.vis; case MGPU_DIFF: return d.diff;
+    case MGPU_SU: case MGPU_SV: case MGPU_SW: case MGPU_STH: case MGPU_SAVU: case MGPU_SAVV: case MGPU_SAVW:
+      if (alloc_component_fields<T>(h, d)) return nullptr;
+      switch (id) {
+        case MGPU_SU: return d.su; case MGPU_SV: return d.sv; case MGPU_SW: return d.sw; case MGPU_STH: return d.sth;
+        case MGPU_SAVU: return d.savu; case MGPU_SAVV: return d.savv; default: return d.savw;
+      }
+    default: break;
+  }
+  int nq = h->cfg.number_q_fields;
+  if (id >= MGPU_Q0 && id < MGPU_Q0 + nq) return d.q[id - MGPU_Q0];
+  if (id >= MGPU_ZQ0 && id < MGPU_ZQ0 + nq) return d.zq[id - MGPU_ZQ0];
+  if (id >= MGPU_SQ0 && id < MGPU_SQ0 + nq) {
+    if (alloc_component_fields<T>(h, d)) return nullptr;
+    return d.sq[id - MGPU_SQ0];
+  }
+  return nullptr;
+}
+
+// layout conversion kernels between the FP64 staging buffer and a device field
+template <typename T>
+__global__ void k_from_monc(const double* __restrict__ src, T* __restrict__ dst, int nx, int ny, int nz) {
+  // src: (nz, ny+4, nx+4) z fastest; dst: [nz][ny][nx]
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nx * ny * nz;
+  if (t >= n) return;
+  int i = (int)(t % nx);
+  long long r = t / nx;
+  int j = (int)(r % ny);
+  int k = (int)(r / ny);
+  long long s = (long long)k + (long long)nz * ((long long)(j + 2) + (long long)(ny + 4) * (i + 2));
+  dst[t] = (T)src[s];
+}
+
+template <typename T>
+__global__ void k_to_monc(const T* __restrict__ src, double* __restrict__ dst, int nx, int ny, int nz) {
+  // every halo point receives its periodic image
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)(nx + 4) * (ny + 4) * nz;
+  if (t >= n) return;
+  int k = (int)(t % nz);
+  long long r = t / nz;
+  int jj = (int)(r % (ny + 4));
+  int ii = (int)(r / (ny + 4));
+  int j = ((jj - 2) % ny + ny) % ny;
+  int i = ((ii - 2) % nx + nx) % nx;
+  dst[t] = (double)src[(long long)k * nx * ny + (long long)j * nx + i];
+}
+
+template <typename T>
+__global__ void k_convert(const double* __restrict__ src, T* __restrict__ dst, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (T)src[t];
+}
+template <typename T>
+__global__ void k_convert_back(const T* __restrict__ src, double* __restrict__ dst, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (double)src[t];
+}
+
+template <typename T>
+static int upload(mgpu_handle* h, DevState<T>& d, int id, const double* host, int layout) {
+  T* dst = field_ptr<T>(h, d, id);
+  if (!dst) return fail(h, MGPU_ERR_ARGUMENT, "unknown field id");
+  const int nx = h->cfg.nx, ny = h->cfg.ny, nz = h->cfg.nz;
+  const long long n = (long long)nx * ny * nz;
+  if (layout == MGPU_LAYOUT_XFAST) {
+    if (sizeof(T) == sizeof(double)) {
+      CK(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    } else {
+      CK(cudaMemcpyAsync(h->xfer, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      k_convert<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->xfer, dst, n);
+      h->launches++;
+    }
+  } else if (layout == MGPU_LAYOUT_MONC) {
+    long long nm = (long long)(nx + 4) * (ny + 4) * nz;
+    double* stage = nullptr;
+    CK(cudaMallocAsync((void**)&stage, nm * sizeof(double), h->stream));
+    CK(cudaMemcpyAsync(stage, host, nm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    k_from_monc<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(stage, dst, nx, ny, nz);
+    h->launches++;
+    CK(cudaFreeAsync(stage, h->stream));
+  } else {
+    return fail(h, MGPU_ERR_ARGUMENT, "unknown layout");
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+template <typename T>
+static int download(mgpu_handle* h, DevState<T>& d, int id, double* host, int layout) {
+  T* src = field_ptr<T>(h, d, id);
+  if (!src) return fail(h, MGPU_ERR_ARGUMENT, "unknown field id");
+  const int nx = h->cfg.nx, ny = h->cfg.ny, nz = h->cfg.nz;
+  const long long n = (long long)nx * ny * nz;
+  if (layout == MGPU_LAYOUT_XFAST) {
+    if (sizeof(T) == sizeof(double)) {
+      CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    } else {
+      k_convert_back<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(src, h->xfer, n);
+      h->launches++;
+      CK(cudaMemcpyAsync(host, h->xfer, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+  } else if (layout == MGPU_LAYOUT_MONC) {
+    long long nm = (long long)(nx + 4) * (ny + 4) * nz;
+    double* stage = nullptr;
+    CK(cudaMallocAsync((void**)&stage, nm * sizeof(double), h->stream));
+    k_to_monc<T><<<(unsigned)((nm + 255) / 256), 256, 0, h->stream>>>(src, stage, nx, ny, nz);
+    h->launches++;
+    CK(cudaMemcpyAsync(host, stage, nm * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaFreeAsync(stage, h->stream));
+  } else {
+    return fail(h, MGPU_ERR_ARGUMENT, "unknown layout");
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+// ---- timestep driver ----------------------------------------------------------------------
+template <typename T>
+static void swap_scalar_buffers(DevState<T>& d, int nq) {
+  std::swap(d.th, d.th_n);
+  std::swap(d.zth, d.zth_n);
+  for (int n = 0; n < nq; ++n) {
+    std::swap(d.q[n], d.q_n[n]);
+    std::swap(d.zq[n], d.zq_n[n]);
+  }
+}
+
+template <typename T>
+static int pressure_solve(mgpu_handle* h, T* p) {
+  if (h->cfg.solver == MGPU_SOLVER_FFT) {
+    fft_solve<T>(h->fft, h->sc, p, h->stream, &h->launches, h->profiling ? &h->ev[3] : nullptr);
+    return MGPU_OK;
+  }
+  int rc = iter_solve<T>(h->iter, h->sc, p, h->stream, &h->launches, &h->solver_iterations, &h->solver_residual);
+  if (rc == MGPU_ERR_NOT_CONVERGED) return MGPU_OK;  // MONC only warns (iterativesolver.F90:240-242)
+  return rc;
+}
+
+// With profiling on, events ev[0..2] bracket subgrid / dynamics / pressure source, ev[3..8]
+// the five FFT kernels (or ev[3], ev[8] the iterative solve) and ev[8..9] pstep + swap.
+static void collect_stage_times(mgpu_handle* h) {
+  cudaEventSynchronize(h->ev[9]);
+  float t;
+  auto acc = [&](int stage, int a, int b) {
+    if (cudaEventElapsedTime(&t, h->ev[a], h->ev[b]) == cudaSuccess) { h->stage_ms[stage] += t; h->stage_n[stage] += 1; }
+  };
+  acc(0, 0, 1);
+  acc(1, 1, 2);
+  acc(2, 2, 3);
+  if (h->cfg.solver == MGPU_SOLVER_FFT)
+    for (int q = 0; q < 5; ++q) acc(3 + q, 3 + q, 4 + q);
+  else
+    acc(9, 3, 8);
+  acc(8, 8, 9);
+}
+
+template <typename T>
+static int step_once(mgpu_handle* h, DevState<T>& d) {
+  h->sc.forward = (h->timestep == 1) ? 1 : 0;  // steppingdirection.F90:44-48
+  auto mark = [&](int q) { if (h->profiling) cudaEventRecord(h->ev[q], h->stream); };
+  mark(0);
+  launch_fused_subgrid<T>(h->sc, d, h->stream);
+  mark(1);
+  launch_fused_dynamics<T>(h->sc, d, h->stream);
+  mark(2);
+  swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
+  launch_fused_pressure_source<T>(h->sc, d, h->stream);
+  h->launches += 3;
+  if (h->cfg.solver != MGPU_SOLVER_FFT) mark(3);
+  int rc = pressure_solve<T>(h, d.p);
+  if (rc) return rc;
+  if (h->cfg.solver != MGPU_SOLVER_FFT) mark(8);
+  launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+  mark(9);
+  h->launches += 1;
+  h->timestep += 1;
+  if (h->profiling) collect_stage_times(h);
+  return MGPU_OK;
+}
+
+template <typename T>
+static int component(mgpu_handle* h, DevState<T>& d, int cid) {
+  h->sc.forward = (h->timestep == 1) ? 1 : 0;
+  int rc = alloc_component_fields<T>(h, d);
+  if (rc) return rc;
+  switch (cid) {
+    case MGPU_C_STEPPING_DIRECTION: return MGPU_OK;
+    case MGPU_C_HALO_SWAPPER: return MGPU_OK;  // periodic indexing in every kernel replaces the swap
+    case MGPU_C_FFTSOLVER:
+      if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model configured for the iterative solver");
+      fft_solve<T>(h->fft, h->sc, d.p, h->stream, &h->launches);
+      break;
+    case MGPU_C_ITERATIVESOLVER:
+      if (h->cfg.solver != MGPU_SOLVER_ITERATIVE) return fail(h, MGPU_ERR_UNSUPPORTED, "model configured for the FFT solver");
+      rc = pressure_solve<T>(h, d.p);
+      if (rc) return fail(h, rc, "iterative solve failed");
+      break;
+    case MGPU_C_DIVERR:
+      CK(cudaMemsetAsync(h->divmax_d, 0, sizeof(unsigned long long), h->stream));
+      rc = launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
+      if (rc) return fail(h, rc, "component failed");
+      {
+        unsigned long long bits = 0;
+        CK(cudaMemcpyAsync(&bits, h->divmax_d, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        double v;
+        std::memcpy(&v, &bits, sizeof(v));
+        if (v > h->global_divmax) h->global_divmax = v;
+      }
+      break;
+    default:
+      rc = launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
+      if (rc) return fail(h, rc, "unknown or unsupported component");
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+extern "C" {
+
+int mgpu_upload_field(mgpu_handle* h, int32_t id, const double* host, int32_t layout) {
+  if (!h || !host) return MGPU_ERR_ARGUMENT;
+  return h->fp32 ? upload<float>(h, h->d32, id, host, layout) : upload<double>(h, h->d64, id, host, layout);
+}
+
+int mgpu_download_field(mgpu_handle* h, int32_t id, double* host, int32_t layout) {
+  if (!h || !host) return MGPU_ERR_ARGUMENT;
+  return h->fp32 ? download<float>(h, h->d32, id, host, layout) : download<double>(h, h->d64, id, host, layout);
+}
+
+int mgpu_get_profile(mgpu_handle* h, const char* name, double* out, int32_t* n) {
+  if (!h || !name) return MGPU_ERR_ARGUMENT;
+  const std::vector<double>* v = profile_by_name(h->rs, name);
+  if (!v) return fail(h, MGPU_ERR_ARGUMENT, std::string("unknown profile ") + name);
+  if (n) *n = h->cfg.nz;
+  if (out)
+    for (int k = 1; k <= h->cfg.nz; ++k) out[k - 1] = (*v)[k];
+  return MGPU_OK;
+}
+
+int mgpu_step(mgpu_handle* h, int32_t nsteps) {
+  if (!h || nsteps < 0) return MGPU_ERR_ARGUMENT;
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = h->fp32 ? step_once<float>(h, h->d32) : step_once<double>(h, h->d64);
+    if (rc) return rc;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return MGPU_OK;
+}
+
+int mgpu_component_timestep(mgpu_handle* h, int32_t cid) {
+  if (!h || cid < 0 || cid >= MGPU_C_COUNT) return MGPU_ERR_ARGUMENT;
+  return h->fp32 ? component<float>(h, h->d32, cid) : component<double>(h, h->d64, cid);
+}
+
+int mgpu_set_timestep(mgpu_handle* h, int32_t ts) {
+  if (!h || ts < 1) return MGPU_ERR_ARGUMENT;
+  h->timestep = ts;
+  return MGPU_OK;
+}
+
+int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out) {
+  if (!h || !out) return MGPU_ERR_ARGUMENT;
+  out->global_divmax = h->global_divmax;
+  out->solver_iterations = h->solver_iterations;
+  out->solver_residual = h->solver_residual;
+  out->timestep = h->timestep;
+  return MGPU_OK;
+}
+
+int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  const int nz = h->cfg.nz;
+  if (h->fp32) launch_diagnostics<float>(h->sc, h->d32.th, h->d32.w, h->diag_d, h->diag_d + nz, h->stream);
+  else launch_diagnostics<double>(h->sc, h->d64.th, h->d64.w, h->diag_d, h->diag_d + nz, h->stream);
+  h->launches += 1;
+  if (mean_theta) CK(cudaMemcpyAsync(mean_theta, h->diag_d, nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (mean_w2) CK(cudaMemcpyAsync(mean_w2, h->diag_d + nz, nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+int mgpu_set_profiling(mgpu_handle* h, int32_t on) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  h->profiling = on != 0;
+  for (int q = 0; q < MGPU_NSTAGES; ++q) { h->stage_ms[q] = 0.0; h->stage_n[q] = 0; }
+  return MGPU_OK;
+}
+
+int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  for (int q = 0; q < MGPU_NSTAGES; ++q) {
+    if (ms_total) ms_total[q] = h->stage_ms[q];
+    if (launches) launches[q] = h->stage_n[q];
+  }
+  return MGPU_OK;
+}
+
+int mgpu_mean_profile(mgpu_handle* h, int32_t id, double* out) {
+  if (!h || !out) return MGPU_ERR_ARGUMENT;
+  // horizontal means via a download; diagnostics only, not on the timed path
+  std::vector<double> buf(field_elems(h));
+  int rc = mgpu_download_field(h, id, buf.data(), MGPU_LAYOUT_XFAST);
+  if (rc) return rc;
+  const size_t plane = (size_t)h->cfg.nx * h->cfg.ny;
+  for (int k = 0; k < h->cfg.nz; ++k) {
+    double s = 0.0;
+    for (size_t t = 0; t < plane; ++t) s += buf[k * plane + t];
+    out[k] = s / (double)plane;
+  }
+  return MGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,63 @@
+// Device state and kernel launchers of the dynamical core.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mgpu_internal.h"
+
+namespace mgpu {
+
+// Device field pointers ([nz][ny][nx], x fastest).  The *_n fields receive the fused
+// dynamics kernel's stepped values; s* and sav* are only allocated for component calls.
+template <typename T>
+struct DevState {
+  T *u, *v, *w, *th, *zu, *zv, *zw, *zth, *p, *vis, *diff;
+  T *su, *sv, *sw, *sth, *savu, *savv, *savw;
+  T *zu_n, *zv_n, *zw_n, *th_n, *zth_n;
+  T* q[MGPU_MAX_Q];
+  T* zq[MGPU_MAX_Q];
+  T* sq[MGPU_MAX_Q];
+  T* q_n[MGPU_MAX_Q];
+  T* zq_n[MGPU_MAX_Q];
+};
+
+template <typename T>
+int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st, unsigned long long* divmax,
+                     int64_t* launches);
+template <typename T> void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st);
+template <typename T> void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st);
+template <typename T> void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st);
+template <typename T> void launch_fused_pstep_swap(const Scalars& s, DevState<T>& d, cudaStream_t st);
+
+// Spectral pressure solve (fftsolver): p (levels 1..nz) -> p.
+struct FftPlanDev {
+  int nx = 0, ny = 0, nz = 0, nxh = 0;
+  void* spec = nullptr;            // complex [nz][ny][nxh], same precision as p
+  double* b1 = nullptr;            // [nz+1][ny/2+1][nxh] Thomas pivots 1/(b - czh*b1), FP64
+  double2* s1 = nullptr;           // forward-elimination values of the Thomas solve, FP64
+  double* twx = nullptr;           // e^{-2 pi i p / nx}, p < nx/2 (complex FP64)
+  double* twy = nullptr;
+  float* twx_f = nullptr;          // the same twiddles rounded to FP32
+  float* twy_f = nullptr;
+};
+int fft_plan_create(FftPlanDev& plan, const Scalars& s, const RefState& rs, bool fp32);
+void fft_plan_destroy(FftPlanDev& plan);
+// evs: NULL, or 6 events recorded before, between and after the five kernels
+template <typename T>
+void fft_solve(const FftPlanDev& plan, const Scalars& s, T* p, cudaStream_t st, int64_t* launches,
+               cudaEvent_t* evs = nullptr);
+
+template <typename T>
+void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st);
+
+// BiCGStab pressure solve (iterativesolver)
+struct IterSolverDev;
+IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status);
+void iter_destroy(IterSolverDev* it);
+template <typename T>
+int iter_solve(IterSolverDev* it, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, int* iterations,
+               double* residual);
+
+}  // namespace mgpu

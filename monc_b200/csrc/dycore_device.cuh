@@ -1,0 +1,612 @@
+// Device functions of the dynamical core: one function per MONC component, evaluated at a
+// single grid point of an x-fastest [nz][ny][nx] field with periodic horizontal indexing.
+//
+// The same functions serve the per-component kernels (drop-in replacements of MONC's column
+// callbacks) and the fused step kernels.  Expression trees follow the Fortran so that the FP64
+// instantiation reproduces MONC's rounding; T = float gives the FP32 stencil path.
+// Vertical indices k are MONC's 1-based levels; horizontal indices i, j are 0-based and may lie
+// up to 2 points outside [0, n) (wrapped periodically).
+#pragma once
+
+#include "mgpu_internal.h"
+
+namespace mgpu {
+
+struct Geo {
+  int nx, ny, nz;
+  long long plane;
+  __device__ __forceinline__ int wi(int i) const { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
+  __device__ __forceinline__ int wj(int j) const { return j < 0 ? j + ny : (j >= ny ? j - ny : j); }
+  __device__ __forceinline__ long long at(int k, int j, int i) const {
+    return (long long)(k - 1) * plane + (long long)wj(j) * nx + wi(i);
+  }
+};
+
+// read-only field view bound to a geometry
+template <typename T>
+struct View {
+  const T* __restrict__ p;
+  Geo g;
+  __device__ __forceinline__ T operator()(int k, int j, int i) const { return __ldg(p + g.at(k, j, i)); }
+};
+
+// profile accessor (FP64 in memory, converted to the compute type)
+template <typename T>
+struct Prof {
+  const double* __restrict__ base;
+  int stride;
+  __device__ __forceinline__ T operator()(int id, int k) const { return (T)__ldg(base + id * stride + k); }
+};
+
+template <typename T> __device__ __forceinline__ T tsign(T a, T b) { return copysign(fabs(a), b); }
+template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }  // Fortran MAX
+template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
+template <typename T> __device__ __forceinline__ T sqr(T a) { return a * a; }
+template <typename T> __device__ __forceinline__ T cub(T a) { return a * a * a; }
+
+// ------------------------------------------------------------------------------------------
+// lower_bc, prescribed surface fluxes (lowerbc.F90:221-305, 601-768; look :645-666)
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ T lookup_ustr(const Scalars& s, T vel) {
+  T posn = (T)1.0 + (T)(float)(s.lookup_entries - 1) * log(vel / (T)s.velmin) * (T)s.aloginv;
+  int ip = (int)posn;
+  if (ip >= 1) {
+    if (ip < s.lookup_entries) {
+      T a = (T)__ldg(s.lookup + ip), b = (T)__ldg(s.lookup + ip + 1);
+      return a + (posn - (T)(float)ip) * (b - a);
+    }
+    return vel * (T)s.cneut;
+  }
+  return pow(vel, -(T)s.convective_limit) * (T)s.cfc;
+}
+
+// Level-1 eddy coefficients and scalar ghost value of one column.
+//   zu_state : current_state%zu (always), zu_a/zv_a: u,v on the forward step else zu,zv,
+//   th_a     : th on the forward step else zth (level 2 read, level 1 written by the caller).
+template <typename T>
+__device__ void lower_bc_column(const Scalars& s, const Prof<T>& P, const View<T>& zu_state, const View<T>& zu_a,
+                                const View<T>& zv_a, const View<T>& th_a, const View<T>* qv_a, int j, int i,
+                                T& vis1, T& diff1, T& th1, T& qv1) {
+  T hv = sqr((T)0.5 * (zu_state(2, j, i) + zu_a(2, j, i - 1)) + (T)s.ugal);
+  hv = hv + sqr((T)0.5 * (zv_a(2, j, i) + zv_a(2, j - 1, i)) + (T)s.vgal);
+  hv = sqrt(hv) + (T)s.smallp;
+  const T fbuoy = (T)s.fbuoy, vk = (T)s.vk, czn = (T)s.czn, zn2 = (T)s.zn2;
+  T v1, d1;
+  bool set_scalars = true;
+  if (fbuoy > (T)0.0) {
+    // convective surface layer (lowerbc.F90:601-633)
+    T ustr = lookup_ustr<T>(s, hv);
+    v1 = czn * sqr(ustr) / hv;
+    d1 = (vk * czn * ustr / (T)s.alphah) /
+         ((T)s.zlogth - (T)2. * log(((T)1. + sqrt((T)1. + (T)s.gammah * vk * fbuoy * (zn2 + (T)s.z0) / cub(ustr))) /
+                                    ((T)1. + sqrt((T)1. + (T)s.gammah * vk * fbuoy * (T)s.z0th / cub(ustr)))));
+  } else if (fbuoy == (T)0.0) {
+    // neutral (lowerbc.F90:672-702)
+    T ustr = hv * (T)s.vk_on_zlogm;
+    v1 = czn * sqr(ustr) / hv;
+    d1 = v1 * (T)s.zlogm / ((T)s.alphah * (T)s.zlogth);
+  } else {
+    // stable surface layer (lowerbc.F90:708-768)
+    T ustr = hv * (T)s.vk_on_zlogm;
+    if ((fbuoy - (T)1.E-9) < (T)-4.0 * sqr(vk) * cub(hv) / ((T)27.0 * (T)s.betam * zn2 * sqr((T)s.zlogm))) {
+      v1 = (T)0.0;
+      d1 = (T)0.0;
+      set_scalars = false;
+    } else {
+      ustr = ustr / (T)3.0 *
+             ((T)1.0 - (T)2.0 * cos((acos((T)-27.0 * (T)s.betam * vk * zn2 * fbuoy / ((T)s.zlogm * (T)2.0 * cub(ustr)) - (T)1.0) +
+                                     (T)2.0 * (T)s.pi) / (T)3.0));
+      v1 = czn * sqr(ustr) / hv;
+      d1 = v1 * ((T)s.zlogm - (T)s.betam * zn2 * vk * fbuoy / cub(ustr)) /
+           ((T)s.alphah * (T)s.zlogth - (T)s.betah * vk * fbuoy * (zn2 + (T)s.z0 - (T)s.z0th) / cub(ustr));
+    }
+  }
+  v1 = tmin<T>(v1, (T)s.max_diff_or_visc);
+  d1 = tmin<T>(d1, (T)s.max_diff_or_visc);
+  vis1 = v1;
+  diff1 = d1;
+  if (set_scalars) {
+    th1 = ((T)s.surface_temperature_flux * P(P_DZN, 2) / d1) + th_a(2, j, i) - P(P_THREF, 1) + P(P_THREF, 2);
+    qv1 = qv_a ? (*qv_a)(2, j, i) + (T)s.surface_vapour_flux * P(P_DZN, 2) / d1 : (T)0;
+  } else {
+    th1 = th_a(2, j, i);
+    qv1 = qv_a ? (*qv_a)(2, j, i) : (T)0;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// smagorinsky (smagorinsky.F90:180-304 setfri + dry Ri, :316-402 moist Ri, :487-696 strain)
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ T half_squared_strain(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V,
+                                 const View<T>& W, int k, int j, int i) {
+  const T cx = (T)s.cx, cy = (T)s.cy, cx2 = (T)s.cx2, cy2 = (T)s.cy2;
+  const T rdzn1 = P(P_RDZN, k + 1);
+  T ssq11 = cx2 * (sqr(U(k + 1, j, i) - U(k + 1, j, i - 1)) + sqr(U(k, j, i) - U(k, j, i - 1)));
+  T ssq22 = cy2 * (sqr(V(k + 1, j, i) - V(k + 1, j - 1, i)) + sqr(V(k, j, i) - V(k, j - 1, i)));
+  T ssq33 = sqr((W(k, j, i) - W(k - 1, j, i)) * P(P_RDZ, k)) + sqr((W(k + 1, j, i) - W(k, j, i)) * P(P_RDZ, k + 1));
+  T ssq13 = (sqr((U(k + 1, j, i) - U(k, j, i)) * rdzn1 + (W(k, j, i + 1) - W(k, j, i)) * cx) +
+             sqr((U(k + 1, j, i - 1) - U(k, j, i - 1)) * rdzn1 + (W(k, j, i) - W(k, j, i - 1)) * cx)) * (T)0.5;
+  T ssq23 = (sqr((W(k, j, i) - W(k, j - 1, i)) * cy + (V(k + 1, j - 1, i) - V(k, j - 1, i)) * rdzn1) +
+             sqr((W(k, j + 1, i) - W(k, j, i)) * cy + (V(k + 1, j, i) - V(k, j, i)) * rdzn1)) * (T)0.5;
+  T ssq12 =
+      (((sqr((U(k, j, i - 1) - U(k, j - 1, i - 1)) * cy + (V(k, j - 1, i) - V(k, j - 1, i - 1)) * cx) +
+         sqr((U(k, j + 1, i - 1) - U(k, j, i - 1)) * cy + (V(k, j, i) - V(k, j, i - 1)) * cx)) +
+        (sqr((U(k, j, i) - U(k, j - 1, i)) * cy + (V(k, j - 1, i + 1) - V(k, j - 1, i)) * cx) +
+         sqr((U(k, j + 1, i) - U(k, j, i)) * cy + (V(k, j, i + 1) - V(k, j, i)) * cx))) +
+       ((sqr((U(k + 1, j, i - 1) - U(k + 1, j - 1, i - 1)) * cy + (V(k + 1, j - 1, i) - V(k + 1, j - 1, i - 1)) * cx) +
+         sqr((U(k + 1, j + 1, i - 1) - U(k + 1, j, i - 1)) * cy + (V(k + 1, j, i) - V(k + 1, j, i - 1)) * cx)) +
+        (sqr((U(k + 1, j, i) - U(k + 1, j - 1, i)) * cy + (V(k + 1, j - 1, i + 1) - V(k + 1, j - 1, i)) * cx) +
+         sqr((U(k + 1, j + 1, i) - U(k + 1, j, i)) * cy + (V(k + 1, j, i + 1) - V(k + 1, j, i)) * cx)))) *
+      (T)0.125;
+  return ssq11 + ssq22 + ssq33 + ssq13 + ssq23 + ssq12 + (T)s.smallp;
+}
+
+// moist_ri_2 for one level (RICHARDSON_NUMBER_CALCULATION = 2)
+template <typename T>
+__device__ T moist_ri(const Scalars& s, const Prof<T>& P, T ssq, const View<T>& TH, const View<T>& QV,
+                      const View<T>& QL, int k, int j, int i) {
+  T tmpinv = (T)1.0 / ssq;
+  T scltmp = P(P_RDZN, k + 1) * P(P_BUOY_CO, k);
+  const T rl = (T)s.rlvap_over_cp, eps = (T)s.eps;
+  const T qsat = P(P_QSAT, k), dq = P(P_DQSATDT, k), rpr = P(P_RPREFRCP, k), tst = P(P_TSTARPR, k), fac = P(P_QSATFAC, k);
+  const T pr = P(P_PREFRCP, k), thr = P(P_THREF, k), thr1 = P(P_THREF, k + 1), tref = P(P_TREF, k);
+  T qt_k = QV(k, j, i) + QL(k, j, i);
+  T qt_kp1 = QV(k + 1, j, i) + QL(k + 1, j, i);
+  T thlpr_k = TH(k, j, i) - rl * QL(k, j, i) * pr;
+  T thlpr_kp1 = TH(k + 1, j, i) - rl * QL(k + 1, j, i) * pr;
+  T qlli = tmax<T>((T)0.0, (qt_k - (qsat + dq * (rpr * thlpr_k - tst))) * fac);
+  T qlui = tmax<T>((T)0.0, (qt_kp1 - (qsat + dq * (rpr * (thlpr_kp1 + thr1) - tst - tref))) * fac);
+  T thvli = thlpr_k + thr + (rl * pr - (T)s.thcona) * qlli;
+  T thvui = thlpr_kp1 + thr1 + (rl * pr - (T)s.thconap1) * qlui;
+  T dth = (thlpr_kp1 - thlpr_k + P(P_DTHREF, k));
+  T thlpr_un = thlpr_kp1 - eps * dth;
+  T thlpr_ln = thlpr_k + eps * dth;
+  T qtun = qt_kp1 - eps * (qt_kp1 - qt_k);
+  T qtln = qt_k + eps * (qt_kp1 - qt_k);
+  T qlln = tmax<T>((T)0.0, (qtln - (qsat + dq * (rpr * thlpr_ln - tst))) * fac);
+  T qlun = tmax<T>((T)0.0, (qtun - (qsat + dq * (rpr * (thlpr_un + thr1) - tst - tref))) * fac);
+  T thvln = thlpr_ln + thr + (rl * pr - (T)s.thcona) * qlln;
+  T thvun = thlpr_un + thr1 + (rl * pr - (T)s.thconap1) * qlun;
+  return scltmp * tmpinv * ((T)s.thconb * (qt_kp1 - qt_k) + ((thvln - thvli) - (thvun - thvui)) * (T)s.repsh);
+}
+
+// vis/diff at level 2 <= k <= nz-1 from the strain rate and Richardson number
+template <typename T>
+__device__ void smagorinsky_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V,
+                                  const View<T>& W, const View<T>& THcur, const View<T>& THarg, const View<T>* QV,
+                                  const View<T>* QL, int k, int j, int i, T& vis, T& diff) {
+  T ssq = half_squared_strain<T>(s, P, U, V, W, k, j, i);
+  T ri = (T)0.0;
+  if (!s.passive_th) {
+    if (!s.passive_q) ri = moist_ri<T>(s, P, ssq, THarg, *QV, *QL, k, j, i);
+    else  // the dry branch reads current_state%th in both stepping modes
+      ri = (P(P_DTHREF, k) + THcur(k + 1, j, i) - THcur(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
+  }
+  T vs, df;
+  if (ri <= (T)0.0) {
+    vs = sqrt((T)1.0 - (T)s.subc * ri);
+    df = (T)s.suba * sqrt((T)1. - (T)s.subb * ri);
+  } else if (ri > (T)0.0 && ri < (T)s.ric) {
+    T t = (T)1. - ri * (T)s.ricinv;
+    t = t * t;
+    T rifac = t * t;
+    vs = rifac * ((T)1. - (T)s.subh * ri);
+    df = rifac * (T)s.suba * ((T)1. - (T)s.subg * ri);
+  } else {
+    vs = (T)0.0;
+    df = (T)0.0;
+  }
+  T sctmp = P(P_RNEUTML_SQ, k) * sqrt(ssq);
+  vis = vs * sctmp;
+  diff = df * sctmp;
+}
+
+// ------------------------------------------------------------------------------------------
+// pw_advection advect_flow_fields (pwadvection.F90:466-610): assigned sources, 2<=k<=nz
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ void pw_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+                         int k, int j, int i, T& su, T& sv, T& sw) {
+  const T tcx = (T)s.tcx, tcy = (T)s.tcy;
+  const T u0 = U(k, j, i), v0 = V(k, j, i);
+  if (k < s.nz) {
+    const T w0 = W(k, j, i);
+    T a = tcx * (U(k, j, i - 1) * (u0 + U(k, j, i - 1)) - U(k, j, i + 1) * (u0 + U(k, j, i + 1)));
+    a = a + tcy * (U(k, j - 1, i) * (V(k, j - 1, i) + V(k, j - 1, i + 1)) - U(k, j + 1, i) * (v0 + V(k, j, i + 1)));
+    a = a + (P(P_TZC1, k) * U(k - 1, j, i) * (W(k - 1, j, i) + W(k - 1, j, i + 1)) -
+             P(P_TZC2, k) * U(k + 1, j, i) * (w0 + W(k, j, i + 1)));
+    su = a;
+    T b = tcy * (V(k, j - 1, i) * (v0 + V(k, j - 1, i)) - V(k, j + 1, i) * (v0 + V(k, j + 1, i)));
+    b = b + tcx * (V(k, j, i - 1) * (U(k, j, i - 1) + U(k, j + 1, i - 1)) - V(k, j, i + 1) * (u0 + U(k, j + 1, i)));
+    b = b + (P(P_TZC1, k) * V(k - 1, j, i) * (W(k - 1, j, i) + W(k - 1, j + 1, i)) -
+             P(P_TZC2, k) * V(k + 1, j, i) * (w0 + W(k, j + 1, i)));
+    sv = b;
+    T c = (P(P_TZD1, k) * W(k - 1, j, i) * (w0 + W(k - 1, j, i)) - P(P_TZD2, k) * W(k + 1, j, i) * (w0 + W(k + 1, j, i)));
+    c = c + tcx * (W(k, j, i - 1) * (U(k, j, i - 1) + U(k + 1, j, i - 1)) - W(k, j, i + 1) * (u0 + U(k + 1, j, i)));
+    c = c + tcy * (W(k, j - 1, i) * (V(k, j - 1, i) + V(k + 1, j - 1, i)) - W(k, j + 1, i) * (v0 + V(k + 1, j, i)));
+    sw = c;
+  } else {
+    T a = tcx * (U(k, j, i - 1) * (u0 + U(k, j, i - 1)) - U(k, j, i + 1) * (u0 + U(k, j, i + 1)));
+    a = a + tcy * (U(k, j - 1, i) * (V(k, j - 1, i) + V(k, j - 1, i + 1)) - U(k, j + 1, i) * (v0 + V(k, j, i + 1)));
+    a = a + P(P_TZC1, k) * U(k - 1, j, i) * (W(k - 1, j, i) + W(k - 1, j, i + 1));
+    su = a;
+    T b = tcy * (V(k, j - 1, i) * (v0 + V(k, j - 1, i)) - V(k, j + 1, i) * (v0 + V(k, j + 1, i)));
+    b = b + tcx * (V(k, j, i - 1) * (U(k, j, i - 1) + U(k, j + 1, i - 1)) - V(k, j, i + 1) * (u0 + U(k, j + 1, i)));
+    b = b + P(P_TZC1, k) * V(k - 1, j, i) * (W(k - 1, j, i) + W(k - 1, j + 1, i));
+    sv = b;
+    sw = (T)0.0;  // sw(nz) is left at its cleared value
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// viscosity (viscosity.F90:293-498): increments of su, sv (2<=k<=nz) and sw (2<=k<=nz-1)
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct Tau13 {
+  T t13, t13m1, t23, t23m1;
+};
+
+template <typename T>
+__device__ Tau13<T> tau_13_23(const Scalars& s, const Prof<T>& P, const View<T>& ZU, const View<T>& ZV,
+                              const View<T>& ZW, const View<T>& VIS, int k, int j, int i) {
+  Tau13<T> t;
+  if (k >= s.nz) { t.t13 = t.t13m1 = t.t23 = t.t23m1 = (T)0.0; return t; }
+  const T cx = (T)s.cx, cy = (T)s.cy, rdzn = P(P_RDZN, k + 1), rho = P(P_RHO, k);
+  T vis13 = (T)0.5 * (VIS(k, j, i) + VIS(k, j, i + 1));
+  T a = (ZU(k + 1, j, i) - ZU(k, j, i)) * rdzn;
+  a = a + (ZW(k, j, i + 1) - ZW(k, j, i)) * cx;
+  t.t13 = a * rho * vis13;
+  vis13 = (T)0.5 * (VIS(k, j, i - 1) + VIS(k, j, i));
+  a = (ZU(k + 1, j, i - 1) - ZU(k, j, i - 1)) * rdzn;
+  a = a + (ZW(k, j, i) - ZW(k, j, i - 1)) * cx;
+  t.t13m1 = a * rho * vis13;
+  T vis23 = (T)0.5 * (VIS(k, j, i) + VIS(k, j + 1, i));
+  a = (ZW(k, j + 1, i) - ZW(k, j, i)) * cy;
+  a = a + (ZV(k + 1, j, i) - ZV(k, j, i)) * rdzn;
+  t.t23 = a * rho * vis23;
+  vis23 = (T)0.5 * (VIS(k, j - 1, i) + VIS(k, j, i));
+  a = (ZW(k, j, i) - ZW(k, j - 1, i)) * cy;
+  a = a + (ZV(k + 1, j - 1, i) - ZV(k, j - 1, i)) * rdzn;
+  t.t23m1 = a * rho * vis23;
+  return t;
+}
+
+template <typename T>
+__device__ T tau33_at(const Scalars& s, const Prof<T>& P, const View<T>& ZW, const View<T>& VIS, int k, int j, int i) {
+  if (k <= 1) return (T)0.0;
+  T visonp2 = P(P_RHON, k) * (VIS(k, j, i) + VIS(k - 1, j, i));
+  return visonp2 * (ZW(k, j, i) - ZW(k - 1, j, i)) * P(P_RDZ, k);
+}
+
+template <typename T>
+__device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const View<T>& ZU, const View<T>& ZV,
+                                const View<T>& ZW, const View<T>& ZU_state, const View<T>& VIS, int k, int j, int i,
+                                T& du, T& dv, T& dw) {
+  const T cx = (T)s.cx, cy = (T)s.cy, rhon = P(P_RHON, k);
+  // horizontal stresses at level k (k >= 2)
+  T vistmp = VIS(k, j, i) + VIS(k, j + 1, i) + VIS(k - 1, j, i) + VIS(k - 1, j + 1, i);
+  T vis12 = (T)0.125 * (vistmp + VIS(k, j, i + 1) + VIS(k, j + 1, i + 1) + VIS(k - 1, j, i + 1) + VIS(k - 1, j + 1, i + 1));
+  T tau12 = (ZU(k, j + 1, i) - ZU(k, j, i)) * cy;
+  tau12 = tau12 + (ZV(k, j, i + 1) - ZV(k, j, i)) * cx;
+  tau12 = tau12 * rhon * vis12;
+  T vis12a = (T)0.125 * (vistmp + VIS(k, j, i - 1) + VIS(k, j + 1, i - 1) + VIS(k - 1, j, i - 1) + VIS(k - 1, j + 1, i - 1));
+  T tau12m1 = (ZU(k, j + 1, i - 1) - ZU(k, j, i - 1)) * cy;
+  tau12m1 = tau12m1 + (ZV(k, j, i) - ZV(k, j, i - 1)) * cx;
+  tau12m1 = tau12m1 * rhon * vis12a;
+  vistmp = VIS(k, j - 1, i) + VIS(k, j, i) + VIS(k - 1, j - 1, i) + VIS(k - 1, j, i);
+  vis12 = (T)0.125 * (vistmp + VIS(k, j - 1, i + 1) + VIS(k, j, i + 1) + VIS(k - 1, j - 1, i + 1) + VIS(k - 1, j, i + 1));
+  T tau12_ym1 = (ZU(k, j, i) - ZU(k, j - 1, i)) * cy;
+  tau12_ym1 = tau12_ym1 + (ZV(k, j - 1, i + 1) - ZV(k, j - 1, i)) * cx;
+  tau12_ym1 = tau12_ym1 * rhon * vis12;
+  T visonp2 = rhon * (VIS(k, j, i) + VIS(k - 1, j, i));
+  T tau11 = visonp2 * (ZU(k, j, i) - ZU(k, j, i - 1)) * cx;
+  T tau22 = visonp2 * (ZV(k, j, i) - ZV(k, j - 1, i)) * cy;
+  visonp2 = rhon * (VIS(k, j + 1, i) + VIS(k - 1, j + 1, i));
+  T tau22_yp1 = visonp2 * (ZV(k, j + 1, i) - ZV(k, j, i)) * cy;
+  T visonp2a = rhon * (VIS(k, j, i + 1) + VIS(k - 1, j, i + 1));
+  T tau11p1 = visonp2a * (ZU_state(k, j, i + 1) - ZU(k, j, i)) * cx;  // reads current_state%zu at x+1
+  Tau13<T> t0 = tau_13_23<T>(s, P, ZU, ZV, ZW, VIS, k, j, i);
+  Tau13<T> tm = tau_13_23<T>(s, P, ZU, ZV, ZW, VIS, k - 1, j, i);
+  du = ((tau11p1 - tau11) * cx + (tau12 - tau12_ym1) * cy + (t0.t13 - tm.t13) * P(P_RDZ, k)) / rhon;
+  dv = ((tau12 - tau12m1) * cx + (tau22_yp1 - tau22) * cy + (t0.t23 - tm.t23) * P(P_RDZ, k)) / rhon;
+  if (k < s.nz) {
+    T t33p = tau33_at<T>(s, P, ZW, VIS, k + 1, j, i);
+    T t33 = tau33_at<T>(s, P, ZW, VIS, k, j, i);
+    dw = ((t0.t13 - t0.t13m1) * cx + (t0.t23 - t0.t23m1) * cy + (t33p - t33) * P(P_RDZN, k + 1)) / P(P_RHO, k);
+  } else {
+    dw = (T)0.0;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// coriolis (coriolis.F90:243-258), buoyancy (buoyancy.F90:229-262)
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ void coriolis_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, int k, int j,
+                               int i, T& su, T& sv) {
+  const T f = (T)s.fcoriol;
+  su = su + f * ((T)0.25 * (V(k, j, i) + V(k, j, i + 1) + V(k, j - 1, i) + V(k, j - 1, i + 1)) + (T)s.vgal - P(P_GWY, k));
+  sv = sv - f * ((T)0.25 * (U(k, j, i) + U(k, j, i - 1) + U(k, j + 1, i) + U(k, j + 1, i - 1)) + (T)s.ugal - P(P_GWX, k));
+}
+
+template <typename T>
+__device__ T buoyancy_point(const Scalars& s, const Prof<T>& P, const View<T>& TH, const View<T>* Q, int k, int j,
+                            int i, T sw) {
+  if (!s.passive_th) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (TH(k, j, i) + TH(k + 1, j, i));
+  if (!s.passive_q) {
+    const T g2 = (T)(0.5 * s.G);
+    for (int n = 0; n < s.nq; ++n) sw = sw + g2 * (T)(n == 0 ? s.cq0 : 0.0) * (Q[n](k, j, i) + Q[n](k + 1, j, i));
+  }
+  return sw;
+}
+
+// ------------------------------------------------------------------------------------------
+// TVD advection: ULTIMATE-QUICKEST face values (ultimateflux.F90) and their divergence
+// (tvdadvection.F90:911-960).  dt is 2*dtm in both stepping modes.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, T fdels, T fd, T fc, T fu, T fgt1, T fgt2,
+                                        T curv_term) {
+  const T r6 = (T)(1.0 / 6.0);
+  T cflmod = fabs(data_value * c * dt);
+  T hrcfl = (T)1.0 / (sum_cfl_out + (T)1.e-30);
+  T hcfl = (T)0.5 * cflmod;
+  T cflcoef = r6 * ((T)1.0 - cflmod * cflmod);
+  T rfdels = (T)1.0 / (fdels + (T)1.e-30);
+  T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * curv_term - fgt1 - fgt2;
+  T fnfs = (ffs - fu) * rfdels;
+  T fncs = (fc - fu) * rfdels;
+  T fnrefs = fncs * hrcfl;
+  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+  return ftemp * fdels + fu;
+}
+
+// face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx
+template <typename T>
+__device__ T tvd_face_x(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+                        const View<T>& ZF, T dt, int k, int j, int i) {
+  const int nz = s.nz;
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  const int kp1 = k + 1 < nz ? k + 1 : nz;
+  const int kp0 = kp1 - 1;
+  const T u0 = U(k, j, i);
+  T sm = tsign<T>((T).5, u0);
+  T advpos = (T)0.5 + sm, advneg = (T)0.5 - sm;
+  T fu = ZF(k, j, i - 1) * advpos + ZF(k, j, i + 2) * advneg;
+  T fc = ZF(k, j, i) * advpos + ZF(k, j, i + 1) * advneg;
+  T fd = ZF(k, j, i + 1) * advpos + ZF(k, j, i) * advneg;
+  T fdels = fd - fu;
+  T fcurvs = fd - (T)2.0 * fc + fu;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
+  T sum;
+  if (u0 > (T)0.0) {
+    sum = (T)0.0;
+    sum = sum + P(P_RDZ, k) * (tmax<T>((T)0.0, W(k, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
+    sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
+    sum = sum + cx * (u0 + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
+    sum = sum * dt;
+  } else {
+    sum = (T)0.0;
+    sum = sum + P(P_RDZ, k) * (tmax<T>((T)0.0, W(k, j, i + 1)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i + 1))));
+    sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i + 1)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i + 1))));
+    sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i + 1)) - u0);
+    sum = sum * dt;
+  }
+  // gradient term in z (calculate_gradient_term_in_z with two source columns)
+  T fgt1;
+  {
+    T sf = (T)0.125 * (W(k, j, i) + W(k - 1, j, i) + W(k, j, i + 1) + W(k - 1, j, i + 1));
+    bool pos = !signbit(sf);
+    int ksu = pos ? k - 1 : kp1;
+    int ksl = pos ? k : kp0;
+    T ts = ZF(ksl, j, i) - ZF(ksu, j, i);
+    ts = ts * advpos + (ZF(ksl, j, i + 1) - ZF(ksu, j, i + 1)) * advneg;
+    fgt1 = fabs(sf) * P(P_RDZ, k) * dt * ts;
+  }
+  // gradient term in y with two v columns
+  T fgt2;
+  {
+    T sf = (T)0.125 * (V(k, j, i + 1) + V(k, j, i) + V(k, j - 1, i + 1) + V(k, j - 1, i));
+    int jsu = signbit(sf) ? j + 1 : j - 1;
+    T t1 = ZF(k, jsu, i) * advpos;
+    T t2 = ZF(k, jsu, i + 1) * advneg;
+    t1 = t1 + t2;
+    fgt2 = fabs(sf) * cy * dt * (fc - t1);
+  }
+  return limit_face<T>(u0, cx, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs);
+}
+
+// face y+1/2 of cell (k, j, i): flux_y(k) of ultflx
+template <typename T>
+__device__ T tvd_face_y(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+                        const View<T>& ZF, T dt, int k, int j, int i) {
+  const int nz = s.nz;
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  const int kp1 = k + 1 < nz ? k + 1 : nz;
+  const int kp0 = kp1 - 1;
+  const T v0 = V(k, j, i);
+  T sm = tsign<T>((T)0.5, v0);
+  T advpos = (T)0.5 + sm, advneg = (T)0.5 - sm;
+  int jo = signbit(v0) ? 1 : 0;  // jofset = nint(advneg)
+  T fu = ZF(k, j - 1, i) * advpos + ZF(k, j + 2, i) * advneg;
+  T fc = ZF(k, j, i) * advpos + ZF(k, j + 1, i) * advneg;
+  T fd = ZF(k, j + 1, i) * advpos + ZF(k, j, i) * advneg;
+  T fdels = fd - fu;
+  T fcurvs = fd - (T)2.0 * fc + fu;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
+  T sum = (T)0.0;
+  sum = sum + P(P_RDZ, k) * (tmax<T>((T)0.0, W(k, j + jo, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j + jo, i))));
+  sum = sum + cy * (tmax<T>((T)0.0, V(k, j + jo, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1 + jo, i))));
+  sum = sum + cx * (tmax<T>((T)0.0, U(k, j + jo, i)) + fabs(tmin<T>((T)0.0, U(k, j + jo, i - 1))));
+  sum = sum * dt;
+  T fgt1;
+  {
+    T sf = (T)0.125 * (W(k, j, i) + W(k - 1, j, i) + W(k, j + 1, i) + W(k - 1, j + 1, i));
+    bool pos = !signbit(sf);
+    int ksu = pos ? k - 1 : kp1;
+    int ksl = pos ? k : kp0;
+    T ts = ZF(ksl, j + jo, i) - ZF(ksu, j + jo, i);
+    fgt1 = fabs(sf) * P(P_RDZ, k) * dt * ts;
+  }
+  T fgt2;
+  {
+    T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k, j + 1, i - 1) + U(k, j + 1, i));
+    T posuf = (T)0.5 + tsign<T>((T).5, sf);
+    fgt2 = fabs(sf) * cx * dt * (fc - (ZF(k, j + jo, i + 1) * ((T)1. - posuf) + ZF(k, j + jo, i - 1) * posuf));
+  }
+  return limit_face<T>(v0, cy, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs);
+}
+
+// flux_z(k+1): face above level k (2 <= k <= nz-1); the top routine handles k = nz-1
+template <typename T>
+__device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+                        const View<T>& ZF, T dt, int k, int j, int i) {
+  const int nz = s.nz;
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  const T w0 = W(k, j, i);
+  T fu, fc, fd, rdu, rdc, sum, fgt1, fgt2;
+  int kf;  // level of the upwind-side values used by the gradient terms
+  if (k == nz - 1) {
+    bool up = w0 >= (T)0.0;
+    if (up) { fu = ZF(k - 1, j, i); fc = ZF(k, j, i); fd = ZF(k + 1, j, i); }
+    else { fu = (T)2.0 * ZF(k + 1, j, i) - ZF(k, j, i); fc = ZF(k + 1, j, i); fd = ZF(k, j, i); }
+    T fcurvs = fd - (T)2.0 * fc + fu;
+    T fdels = fd - fu;
+    if (fabs(fcurvs) >= fabs(fdels)) return fc;
+    if (up) {
+      sum = (T)0.0;
+      sum = sum + P(P_RDZ, k) * (w0 + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
+      sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
+      sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i)) + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
+      sum = sum * dt;
+      kf = k;
+      rdu = P(P_RDZN, k);
+      rdc = P(P_RDZ, k);
+    } else {
+      sum = (T)0.0;
+      sum = sum + (-w0 * P(P_RDZ, nz < k + 1 ? nz : k + 1));
+      sum = sum + cy * (tmax<T>((T)0.0, V(k + 1, j, i)) + fabs(tmin<T>((T)0.0, V(k + 1, j - 1, i))));
+      sum = sum + cx * (tmax<T>((T)0.0, U(k + 1, j, i)) + fabs(tmin<T>((T)0.0, U(k + 1, j, i - 1))));
+      sum = sum * dt;
+      kf = k + 1;
+      rdu = P(P_RDZN, nz);
+      rdc = P(P_RDZ, nz < k + 1 ? nz : k + 1);
+    }
+    {
+      T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
+      int jsu = signbit(sf) ? j + 1 : j - 1;
+      fgt1 = fabs(sf) * cy * dt * (fc - ZF(kf, jsu, i));
+    }
+    {
+      T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k + 1, j, i - 1) + U(k + 1, j, i));
+      T posuf = (T)0.5 + tsign<T>((T).5, sf);
+      fgt2 = fabs(sf) * cx * dt * (fc - (ZF(kf, j, i + 1) * ((T)1. - posuf) + ZF(kf, j, i - 1) * posuf));
+    }
+    // calculate_flux_in_w
+    T dd = P(P_DZN, k + 1), rdd = P(P_RDZN, k + 1);
+    T cflmod = fabs(w0 * rdd * dt);
+    T hrcfl = (T)1.0 / (sum + (T)1.e-30);
+    T hcfl = (T)0.5 * cflmod;
+    T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
+    T rfdels = (T)1.0 / (fdels + (T)1.e-30);
+    T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
+    T fnfs = (ffs - fu) * rfdels;
+    T fncs = (fc - fu) * rfdels;
+    T fnrefs = fncs * hrcfl;
+    T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+    return ftemp * fdels + fu;
+  }
+  // middle of the column
+  T sm = tsign<T>((T).5, w0);
+  T advpos = (T)0.5 + sm, advneg = (T)0.5 - sm;
+  int ko = signbit(w0) ? 1 : 0;  // kofset
+  fu = ZF(k - 1, j, i) * advpos + ZF(k + 2, j, i) * advneg;
+  fc = ZF(k + ko, j, i);
+  fd = ZF(k + 1, j, i) * advpos + ZF(k, j, i) * advneg;
+  T fcurvs = fd - (T)2.0 * fc + fu;
+  T fdels = fd - fu;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
+  sum = (T)0.0;
+  sum = sum + P(P_RDZ, k + ko) * (tmax<T>((T)0.0, W(k + ko, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1 + ko, j, i))));
+  sum = sum + cy * (tmax<T>((T)0.0, V(k + ko, j, i)) + fabs(tmin<T>((T)0.0, V(k + ko, j - 1, i))));
+  sum = sum + cx * (tmax<T>((T)0.0, U(k + ko, j, i)) + fabs(tmin<T>((T)0.0, U(k + ko, j, i - 1))));
+  sum = sum * dt;
+  {
+    T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
+    int jsu = signbit(sf) ? j + 1 : j - 1;
+    fgt1 = fabs(sf) * cy * dt * (fc - ZF(k + ko, jsu, i));
+  }
+  {
+    T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k + 1, j, i - 1) + U(k + 1, j, i));
+    T posuf = (T)0.5 + tsign<T>((T).5, sf);
+    fgt2 = fabs(sf) * cx * dt * (fc - (ZF(k + ko, j, i + 1) * ((T)1. - posuf) + ZF(k + ko, j, i - 1) * posuf));
+  }
+  rdu = P(P_RDZN, k) * advpos + P(P_RDZN, k + 2) * advneg;
+  rdc = P(P_RDZ, k) * advpos + P(P_RDZ, k + 1) * advneg;
+  T dd = P(P_DZN, k + 1), rdd = P(P_RDZN, k + 1);
+  T cflmod = fabs(w0 * rdd * dt);
+  T hrcfl = (T)1.0 / (sum + (T)1.e-30);
+  T hcfl = (T)0.5 * cflmod;
+  T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
+  T rfdels = (T)1.0 / (fdels + (T)1.e-30);
+  T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
+  T fnfs = (ffs - fu) * rfdels;
+  T fncs = (fc - fu) * rfdels;
+  T fnrefs = fncs * hrcfl;
+  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+  return ftemp * fdels + fu;
+}
+
+// TVD source of cell (k, j, i), 2 <= k <= nz, from the six face values
+// acc0 is the source value before the callback (MONC accumulates into it below the top level
+// and zeroes it at the top level)
+template <typename T>
+__device__ T tvd_source(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+                        T fx_m, T fx_p, T fy_m, T fy_p, T fz_m, T fz_p, int k, int j, int i, T acc0) {
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  T acc = (k < s.nz) ? acc0 : (T)0.0;
+  if (k < s.nz) {
+    acc = acc + (V(k, j - 1, i) * fy_m - V(k, j, i) * fy_p) * cy;
+    acc = acc + (T)4.0 * (W(k - 1, j, i) * fz_m * P(P_TZC1, k) - W(k, j, i) * fz_p * P(P_TZC2, k));
+    acc = acc + (U(k, j, i - 1) * fx_m - U(k, j, i) * fx_p) * cx;
+  } else {
+    acc = acc + (V(k, j - 1, i) * fy_m - V(k, j, i) * fy_p) * cy;
+    acc = acc + (T)4.0 * P(P_TZC1, k) * W(k - 1, j, i) * fz_m;
+    acc = acc + (U(k, j, i - 1) * fx_m - U(k, j, i) * fx_p) * cx;
+  }
+  return acc;
+}
+
+template <typename T>
+__device__ T tvd_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+                       const View<T>& ZF, int k, int j, int i, T acc0) {
+  const T dt = (T)(s.dtm * 2.0);
+  T fxm = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i - 1);
+  T fxp = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i);
+  T fym = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j - 1, i);
+  T fyp = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j, i);
+  T fzm = (k == 2) ? (T)0.0 : tvd_face_z<T>(s, P, U, V, W, ZF, dt, k - 1, j, i);
+  T fzp = (k < s.nz) ? tvd_face_z<T>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
+  return tvd_source<T>(s, P, U, V, W, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, acc0);
+}
+
+// ------------------------------------------------------------------------------------------
+// diffusion general_diffusion (diffusion.F90:501-545), 2 <= k <= nz
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ T diffusion_point(const Scalars& s, const Prof<T>& P, const View<T>& F, const View<T>& D, int k, int j, int i) {
+  const T f0 = F(k, j, i), d0 = D(k, j, i), dm = D(k - 1, j, i);
+  T term = (T)s.cx2 * (T)0.25 *
+               (((d0 + D(k, j, i - 1)) + (dm + D(k - 1, j, i - 1))) * (F(k, j, i - 1) - f0) -
+                ((D(k, j, i + 1) + d0) + (D(k - 1, j, i + 1) + dm)) * (f0 - F(k, j, i + 1))) +
+           (T)s.cy2 * (T)0.25 *
+               (((d0 + D(k, j - 1, i)) + (dm + D(k - 1, j - 1, i))) * (F(k, j - 1, i) - f0) -
+                ((D(k, j + 1, i) + d0) + (D(k - 1, j + 1, i) + dm)) * (f0 - F(k, j + 1, i))) +
+           (P(P_CZB, k) * dm * (F(k - 1, j, i) - f0));
+  if (k < s.nz) term = term - P(P_CZA, k) * d0 * (f0 - F(k + 1, j, i));
+  return term;
+}
+
+}  // namespace mgpu

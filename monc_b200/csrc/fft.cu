@@ -1,0 +1,437 @@
+// Spectral pressure solve (fftsolver.F90:129-309): horizontal FFTs in shared memory and a
+// column-per-thread FP64 Thomas solve per horizontal wavenumber.
+//
+//   forward x : pairs of real rows packed as one complex row, radix-2 FFT in shared memory,
+//               split into the two half spectra (kx = 0..nx/2)
+//   forward y : complex FFT along y of a tile of kx columns
+//   tridiag   : per (kx, ky) column, b(k) = cos_x + cos_y + czg(k) with the Thomas pivots
+//               precomputed in FP64 on the host exactly as fftsolver.F90:259-293 forms them;
+//               the horizontal-mean mode is integrated upward (fftsolver.F90:294-308)
+//   inverse y, inverse x (imaginary parts of the kx = 0 and kx = nx/2 bins are dropped, as the
+//               Hermitian completion of fftnorth.F90:54-73 drops them)
+// MONC transforms y first and stores real and imaginary parts separately ("real-interleaved",
+// pencilfft.F90:276-332); the solve is linear with real coefficients that depend only on
+// |kx|, |ky|, so this complex half-spectrum form gives the same field up to rounding.
+// Level 1 is transformed too: its non-mean modes pass through unchanged, its mean is zeroed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "dycore.h"
+
+namespace mgpu {
+
+template <typename T> struct Cx;
+template <> struct Cx<double> { typedef double2 t; };
+template <> struct Cx<float> { typedef float2 t; };
+
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+
+static int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
+
+// In-place radix-2 decimation-in-time stages over `nrows` rows held in shared memory in
+// bit-reversed order.  Element e of row r lives at buf[r*rs + e*es].
+template <typename C>
+__device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int es, const C* tw, bool inverse) {
+  const int half_n = n >> 1;
+  const int total = nrows * half_n;
+  for (int s = 1; s <= logn; ++s) {
+    const int half = 1 << (s - 1);
+    const int stride = n >> s;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      int r = b / half_n;
+      int bb = b - r * half_n;
+      int pos = bb & (half - 1);
+      int i0 = ((bb >> (s - 1)) << s) | pos;
+      int i1 = i0 + half;
+      C w = tw[pos * stride];
+      if (inverse) w.y = -w.y;
+      C* row = buf + r * rs;
+      C a = row[i0 * es], c = row[i1 * es];
+      C t = cmul(w, c);
+      row[i1 * es] = csub(a, t);
+      row[i0 * es] = cadd(a, t);
+    }
+    __syncthreads();
+  }
+}
+
+// ---- forward x: real rows (k, j), (k, j+1) -> half spectra ------------------------------
+template <typename T>
+__global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g,
+                            int nx, int ny, int nz, int logn, int rows_per_cta) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* buf = tw + nx / 2;
+  for (int t = threadIdx.x; t < nx / 2; t += blockDim.x) tw[t] = tw_g[t];
+  const int pairs_per_level = ny / 2;
+  const long long pair0 = (long long)blockIdx.x * rows_per_cta;
+  const long long npairs = (long long)nz * pairs_per_level;
+  const int nxh = nx / 2 + 1;
+  for (int t = threadIdx.x; t < rows_per_cta * nx; t += blockDim.x) {
+    int r = t / nx, e = t - r * nx;
+    long long pr = pair0 + r;
+    C z;
+    if (pr < npairs) {
+      int k = (int)(pr / pairs_per_level) + 1;
+      int j = 2 * (int)(pr % pairs_per_level);
+      const T* row = p + (long long)(k - 1) * nx * ny + (long long)j * nx;
+      z.x = row[e];
+      z.y = row[nx + e];
+    } else {
+      z.x = (T)0; z.y = (T)0;
+    }
+    int br = __brev(e) >> (32 - logn);
+    buf[r * nx + br] = z;
+  }
+  __syncthreads();
+  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, nx, 1, tw, false);
+  for (int t = threadIdx.x; t < rows_per_cta * nxh; t += blockDim.x) {
+    int r = t / nxh, m = t - r * nxh;
+    long long pr = pair0 + r;
+    if (pr >= npairs) continue;
+    int k = (int)(pr / pairs_per_level) + 1;
+    int j = 2 * (int)(pr % pairs_per_level);
+    C zm = buf[r * nx + m];
+    C zn = buf[r * nx + ((nx - m) & (nx - 1))];
+    C a, b;
+    a.x = (T)0.5 * (zm.x + zn.x);
+    a.y = (T)0.5 * (zm.y - zn.y);
+    b.x = (T)0.5 * (zm.y + zn.y);
+    b.y = (T)0.5 * (zn.x - zm.x);
+    C* out = spec + (long long)(k - 1) * ny * nxh + (long long)j * nxh;
+    out[m] = a;
+    out[nxh + m] = b;
+  }
+}
+
+// ---- inverse x: half spectra -> real rows (k, j), (k, j+1) -----------------------------
+template <typename T>
+__global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g,
+                            int nx, int ny, int nz, int logn, int rows_per_cta) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* buf = tw + nx / 2;
+  for (int t = threadIdx.x; t < nx / 2; t += blockDim.x) tw[t] = tw_g[t];
+  const int pairs_per_level = ny / 2;
+  const long long pair0 = (long long)blockIdx.x * rows_per_cta;
+  const long long npairs = (long long)nz * pairs_per_level;
+  const int nxh = nx / 2 + 1;
+  for (int t = threadIdx.x; t < rows_per_cta * nxh; t += blockDim.x) {
+    int r = t / nxh, m = t - r * nxh;
+    long long pr = pair0 + r;
+    C a, b;
+    if (pr < npairs) {
+      int k = (int)(pr / pairs_per_level) + 1;
+      int j = 2 * (int)(pr % pairs_per_level);
+      const C* in = spec + (long long)(k - 1) * ny * nxh + (long long)j * nxh;
+      a = in[m];
+      b = in[nxh + m];
+    } else {
+      a.x = a.y = b.x = b.y = (T)0;
+    }
+    if (m == 0 || m == nx / 2) { a.y = (T)0; b.y = (T)0; }
+    C z;
+    z.x = a.x - b.y;
+    z.y = a.y + b.x;
+    buf[r * nx + (__brev(m) >> (32 - logn))] = z;
+    if (m > 0 && m < nx / 2) {
+      C zc;
+      zc.x = a.x + b.y;
+      zc.y = b.x - a.y;
+      int mm = nx - m;
+      buf[r * nx + (__brev(mm) >> (32 - logn))] = zc;
+    }
+  }
+  __syncthreads();
+  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, nx, 1, tw, true);
+  const T sc = (T)(1.0 / (double)nx);
+  for (int t = threadIdx.x; t < rows_per_cta * nx; t += blockDim.x) {
+    int r = t / nx, e = t - r * nx;
+    long long pr = pair0 + r;
+    if (pr >= npairs) continue;
+    int k = (int)(pr / pairs_per_level) + 1;
+    int j = 2 * (int)(pr % pairs_per_level);
+    T* row = p + (long long)(k - 1) * nx * ny + (long long)j * nx;
+    C z = buf[r * nx + e];
+    row[e] = z.x * sc;
+    row[nx + e] = z.y * sc;
+  }
+}
+
+// ---- complex FFT along y on a tile of kx columns ------------------------------------------
+template <typename T>
+__global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g, int nx, int ny, int logn,
+                        int cols, bool inverse) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* buf = tw + ny / 2;
+  for (int t = threadIdx.x; t < ny / 2; t += blockDim.x) tw[t] = tw_g[t];
+  const int nxh = nx / 2 + 1;
+  const int kx0 = blockIdx.x * cols;
+  const int k = blockIdx.y + 1;
+  C* base = spec + (long long)(k - 1) * ny * nxh;
+  for (int t = threadIdx.x; t < cols * ny; t += blockDim.x) {
+    int e = t / cols, c = t - e * cols;
+    C z;
+    if (kx0 + c < nxh) z = base[(long long)e * nxh + kx0 + c];
+    else { z.x = (T)0; z.y = (T)0; }
+    buf[(__brev(e) >> (32 - logn)) * cols + c] = z;
+  }
+  __syncthreads();
+  // rows = columns here: element e of column c at buf[e*cols + c]
+  smem_fft_stages<C>(buf, ny, logn, cols, 1, cols, tw, inverse);
+  const T sc = inverse ? (T)(1.0 / (double)ny) : (T)1.0;
+  for (int t = threadIdx.x; t < cols * ny; t += blockDim.x) {
+    int e = t / cols, c = t - e * cols;
+    if (kx0 + c >= nxh) continue;
+    C z = buf[e * cols + c];
+    z.x = z.x * sc;
+    z.y = z.y * sc;
+    base[(long long)e * nxh + kx0 + c] = z;
+  }
+}
+
+// ---- vertical tridiagonal per (ky, kx) in FP64 ----------------------------------------------
+template <typename T>
+__global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
+                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz) {
+  typedef typename Cx<T>::t C;
+  const int nxh = nx / 2 + 1;
+  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= (long long)ny * nxh) return;
+  int ky = (int)(col / nxh), kx = (int)(col - (long long)ky * nxh);
+  const long long plane = (long long)ny * nxh;
+  const double* czb = prof + P_CZB * prof_stride;
+  const double* cza = prof + P_CZA * prof_stride;
+  const double* czg = prof + P_CZG * prof_stride;
+  C* sp = spec + col;
+  if (kx == 0 && ky == 0) {
+    // horizontal-mean mode: upward recurrence from p(1) = p(2) = 0
+    C v2 = sp[plane];
+    double sr_prev = (double)v2.x, si_prev = (double)v2.y;
+    double pr2 = 0.0, pi2 = 0.0, pr1 = 0.0, pi1 = 0.0;  // p(k-2), p(k-1)
+    C zero;
+    zero.x = (T)0;
+    zero.y = (T)0;
+    sp[0] = zero;  // p(1) = p(2) = 0 for the mean mode
+    sp[plane] = zero;
+    for (int k = 3; k <= nz; ++k) {
+      C vk = sp[(long long)(k - 1) * plane];
+      double pr = (sr_prev - czg[k - 1] * pr1 - czb[k - 1] * pr2) / cza[k - 1];
+      double pi = (si_prev - czg[k - 1] * pi1 - czb[k - 1] * pi2) / cza[k - 1];
+      sr_prev = (double)vk.x;
+      si_prev = (double)vk.y;
+      C o;
+      o.x = (T)pr;
+      o.y = (T)pi;
+      sp[(long long)(k - 1) * plane] = o;
+      pr2 = pr1; pi2 = pi1; pr1 = pr; pi1 = pi;
+    }
+    return;
+  }
+  const int kyi = ky <= ny / 2 ? ky : ny - ky;
+  const long long bstride = (long long)(ny / 2 + 1) * nxh;
+  const double* bcol = b1 + (long long)kyi * nxh + kx;
+  // forward elimination: s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1)
+  C v = sp[plane];
+  double sr = (double)v.x, si = (double)v.y;
+  s1buf[col + plane] = make_double2(sr, si);
+  for (int k = 3; k <= nz; ++k) {
+    C vk = sp[(long long)(k - 1) * plane];
+    double bm = bcol[(long long)(k - 1) * bstride];
+    sr = (double)vk.x - czb[k] * sr * bm;
+    si = (double)vk.y - czb[k] * si * bm;
+    s1buf[col + (long long)(k - 1) * plane] = make_double2(sr, si);
+  }
+  // back substitution
+  double pr = sr * bcol[(long long)nz * bstride];
+  double pi = si * bcol[(long long)nz * bstride];
+  C o;
+  o.x = (T)pr;
+  o.y = (T)pi;
+  sp[(long long)(nz - 1) * plane] = o;
+  for (int k = nz - 1; k >= 2; --k) {
+    double2 s = s1buf[col + (long long)(k - 1) * plane];
+    double bk = bcol[(long long)k * bstride];
+    pr = (s.x - cza[k] * pr) * bk;
+    pi = (s.y - cza[k] * pi) * bk;
+    o.x = (T)pr;
+    o.y = (T)pi;
+    sp[(long long)(k - 1) * plane] = o;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+struct FftSizes {
+  int rows_x, cols_y, logx, logy;
+  size_t smem_x, smem_y;
+};
+
+template <typename T>
+static FftSizes sizes(const FftPlanDev& pl) {
+  FftSizes z;
+  const size_t cs = sizeof(typename Cx<T>::t);
+  z.logx = ilog2(pl.nx);
+  z.logy = ilog2(pl.ny);
+  z.rows_x = (int)std::max<size_t>(1, 32768 / (pl.nx * cs));
+  z.cols_y = (int)std::min<size_t>(16, std::max<size_t>(1, 32768 / (pl.ny * cs)));
+  z.smem_x = cs * (pl.nx / 2 + (size_t)z.rows_x * pl.nx);
+  z.smem_y = cs * (pl.ny / 2 + (size_t)z.cols_y * pl.ny);
+  return z;
+}
+
+int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool fp32) {
+  pl.nx = s.nx;
+  pl.ny = s.ny;
+  pl.nz = s.nz;
+  pl.nxh = s.nx / 2 + 1;
+  auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
+  if (!pow2(s.nx) || !pow2(s.ny) || s.nx > 4096 || s.ny > 4096) return MGPU_ERR_UNSUPPORTED;
+  const size_t plane = (size_t)s.ny * pl.nxh;
+  const size_t cs = fp32 ? sizeof(float2) : sizeof(double2);
+  if (cudaMalloc(&pl.spec, cs * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+  if (cudaMalloc(&pl.s1, sizeof(double2) * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+  // Thomas pivots per (|ky|, kx), built exactly as fftsolver.F90:259-280 and :72-90
+  const int nyh = s.ny / 2 + 1;
+  std::vector<double> b1((size_t)(s.nz + 1) * nyh * pl.nxh, 0.0);
+  const double PI = 4.0 * std::atan(1.0);
+  std::vector<double> cosx(pl.nxh), cosy(nyh);
+  for (int m = 0; m < pl.nxh; ++m) cosx[m] = (2.0 / (rs.dx * rs.dx)) * (std::cos(2.0 * PI * (double)m / (double)s.nx) - 1.0);
+  for (int m = 0; m < nyh; ++m) cosy[m] = (2.0 / (rs.dy * rs.dy)) * (std::cos(2.0 * PI * (double)m / (double)s.ny) - 1.0);
+  for (int ky = 0; ky < nyh; ++ky)
+    for (int kx = 0; kx < pl.nxh; ++kx) {
+      double cij = cosx[kx] + cosy[ky];
+      double b = cij - rs.cza[2];
+      double prev = 1.0 / b;
+      b1[((size_t)2 * nyh + ky) * pl.nxh + kx] = prev;
+      for (int k = 3; k <= s.nz; ++k) {
+        double bk = cij + rs.czg[k];
+        prev = 1.0 / (bk - rs.czh[k] * prev);
+        b1[((size_t)k * nyh + ky) * pl.nxh + kx] = prev;
+      }
+    }
+  if (cudaMalloc(&pl.b1, b1.size() * sizeof(double)) != cudaSuccess) return MGPU_ERR_CUDA;
+  cudaMemcpy(pl.b1, b1.data(), b1.size() * sizeof(double), cudaMemcpyHostToDevice);
+  auto twiddles = [&](int n, double** dd, float** df) {
+    std::vector<double> t(n);
+    std::vector<float> tf(n);
+    for (int q = 0; q < n / 2; ++q) {
+      double a = 2.0 * PI * (double)q / (double)n;
+      t[2 * q] = std::cos(a);
+      t[2 * q + 1] = -std::sin(a);
+      tf[2 * q] = (float)t[2 * q];
+      tf[2 * q + 1] = (float)t[2 * q + 1];
+    }
+    cudaMalloc(dd, n * sizeof(double));
+    cudaMalloc(df, n * sizeof(float));
+    cudaMemcpy(*dd, t.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(*df, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+  };
+  twiddles(s.nx, &pl.twx, &pl.twx_f);
+  twiddles(s.ny, &pl.twy, &pl.twy_f);
+  FftSizes zd = sizes<double>(pl), zf = sizes<float>(pl);
+  size_t mx = std::max(std::max(zd.smem_x, zd.smem_y), std::max(zf.smem_x, zf.smem_y));
+  if (mx > 48 * 1024) {
+    cudaFuncSetAttribute(k_fft_x_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+    cudaFuncSetAttribute(k_fft_x_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+    cudaFuncSetAttribute(k_fft_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+    cudaFuncSetAttribute(k_fft_x_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+    cudaFuncSetAttribute(k_fft_x_inv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+    cudaFuncSetAttribute(k_fft_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+  }
+  return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
+}
+
+void fft_plan_destroy(FftPlanDev& pl) {
+  cudaFree(pl.spec);
+  cudaFree(pl.s1);
+  cudaFree(pl.b1);
+  cudaFree(pl.twx);
+  cudaFree(pl.twy);
+  cudaFree(pl.twx_f);
+  cudaFree(pl.twy_f);
+  pl = FftPlanDev{};
+}
+
+template <typename T>
+void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, cudaEvent_t* evs) {
+  typedef typename Cx<T>::t C;
+  const bool f32 = sizeof(T) == 4;
+  FftSizes z = sizes<T>(pl);
+  C* spec = reinterpret_cast<C*>(pl.spec);
+  const C* twx = reinterpret_cast<const C*>(f32 ? (void*)pl.twx_f : (void*)pl.twx);
+  const C* twy = reinterpret_cast<const C*>(f32 ? (void*)pl.twy_f : (void*)pl.twy);
+  const long long npairs = (long long)s.nz * (s.ny / 2);
+  const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
+  const size_t plane = (size_t)s.ny * pl.nxh;
+  double2* s1 = pl.s1;
+  auto mark = [&](int q) { if (evs) cudaEventRecord(evs[q], st); };
+  mark(0);
+  k_fft_x_fwd<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x);
+  mark(1);
+  dim3 gy((pl.nxh + z.cols_y - 1) / z.cols_y, s.nz);
+  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, s.nx, s.ny, z.logy, z.cols_y, false);
+  mark(2);
+  long long ncol = (long long)plane;
+  k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz);
+  mark(3);
+  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, s.nx, s.ny, z.logy, z.cols_y, true);
+  mark(4);
+  k_fft_x_inv<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x);
+  mark(5);
+  *launches += 5;
+}
+
+template void fft_solve<double>(const FftPlanDev&, const Scalars&, double*, cudaStream_t, int64_t*, cudaEvent_t*);
+template void fft_solve<float>(const FftPlanDev&, const Scalars&, float*, cudaStream_t, int64_t*, cudaEvent_t*);
+
+// ---- horizontal-mean diagnostics: one block per level, FP64 accumulation in a fixed order ----
+template <typename T>
+__global__ void k_diagnostics(const T* __restrict__ th, const T* __restrict__ w, const double* __restrict__ prof,
+                              int prof_stride, long long plane, double* out_th, double* out_w2) {
+  const int k = blockIdx.x + 1;
+  const T* thk = th + (long long)(k - 1) * plane;
+  const T* wk = w + (long long)(k - 1) * plane;
+  double a = 0.0, b = 0.0;
+  for (long long t = threadIdx.x; t < plane; t += blockDim.x) {
+    a += (double)thk[t];
+    double wv = (double)wk[t];
+    b += wv * wv;
+  }
+  __shared__ double sa[256], sb[256];
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+      sa[threadIdx.x] += sa[threadIdx.x + h];
+      sb[threadIdx.x] += sb[threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (out_th) out_th[k - 1] = sa[0] / (double)plane + prof[P_THREF * prof_stride + k];
+    if (out_w2) out_w2[k - 1] = sb[0] / (double)plane;
+  }
+}
+
+template <typename T>
+void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st) {
+  k_diagnostics<T><<<s.nz, 256, 0, st>>>(th, w, s.prof, s.nz + 2, s.plane, out_th, out_w2);
+}
+template void launch_diagnostics<double>(const Scalars&, const double*, const double*, double*, double*, cudaStream_t);
+template void launch_diagnostics<float>(const Scalars&, const float*, const float*, double*, double*, cudaStream_t);
+
+}  // namespace mgpu

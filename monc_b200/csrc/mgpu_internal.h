@@ -1,0 +1,64 @@
+// Internal declarations of libmoncgpu: host-side reference state and device model.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/monc_gpu.h"
+
+namespace mgpu {
+
+// Vertical-grid and reference-state profiles, 1-based like MONC (element [k], k = 1..nz),
+// plus the horizontal-grid scalars.  Built on the host in FP64 (grid.cpp).
+struct RefState {
+  int nz = 0;
+  std::vector<double> z, zn, dz, dzn, rdz, rdzn, rho, rhon, thref, dthref, czb, cza, czg, czh, tzc1, tzc2, tzd1, tzd2;
+  std::vector<double> rneutml, rneutml_sq, buoy_co, prefn, prefrcp, rprefrcp, tref, tstarpr, qsat, dqsatdt, qsatfac;
+  std::vector<double> gwx, gwy;  // geostrophic wind profile
+  double czn = 0, zlogm = 0, zlogth = 0, vk_on_zlogm = 0;
+  double dx = 0, dy = 0, cx = 0, cy = 0, cx2 = 0, cy2 = 0, tcx = 0, tcy = 0;
+  double rmlmax = 0, smallp = 0, rlvap_over_cp = 0, r_over_cp = 0;
+  // surface scheme (setfluxlook / lowerbc)
+  double surface_temperature_flux = 0, surface_vapour_flux = 0, fbuoy = 0;
+  std::vector<double> lookup_ustr;  // 1-based, 80 entries
+  double velmin = 0, velmax = 0, aloginv = 0, cneut = 0, cfc = 0;
+  int lookup_entries = 80;
+  std::vector<double> cq;
+};
+
+// Builds the reference state from a configuration (restates gridmanager.F90:2008-2642,
+// simplesetup.F90:149-266, setfluxlook.F90:63-186).  Throws std::runtime_error on bad input.
+void build_reference_state(const mgpu_config& cfg, RefState& rs);
+const std::vector<double>* profile_by_name(const RefState& rs, const std::string& name);
+
+// Profiles copied to device memory, 1-based (index k), FP64.
+enum ProfileId {
+  P_RDZ = 0, P_RDZN, P_DZN, P_RHO, P_RHON, P_DTHREF, P_CZB, P_CZA, P_CZG, P_CZH, P_TZC1, P_TZC2, P_TZD1, P_TZD2,
+  P_RNEUTML_SQ, P_BUOY_CO, P_THREF, P_PREFRCP, P_RPREFRCP, P_TREF, P_TSTARPR, P_QSAT, P_DQSATDT, P_QSATFAC,
+  P_GWX, P_GWY, P_COUNT
+};
+
+// Scalars every dynamical-core kernel reads (passed by value as a kernel parameter).
+struct Scalars {
+  int nx, ny, nz;
+  long long plane;  // nx*ny
+  double cx, cy, cx2, cy2, tcx, tcy;
+  double dtm, tsmth, ugal, vgal, fcoriol, smallp;
+  double czn, zn2, zlogm, zlogth, vk_on_zlogm, vk, z0, z0th, alphah, betam, betah, gammah, pi;
+  double surface_temperature_flux, surface_vapour_flux, fbuoy, max_diff_or_visc;
+  double velmin, aloginv, cneut, cfc, convective_limit;
+  double subb, subc, subg, subh, suba, ric, ricinv;
+  double eps, repsh, thcona, thconb, thconap1, rlvap_over_cp, G;
+  double cq0;  // cq of the vapour field
+  int lookup_entries;
+  int forward;  // 1 on the first (forward) step
+  int passive_th, passive_q, nq, iqv, iql;
+  int coriolis, surface_bcs, use_vd;
+  const double* prof;      // device: P_COUNT profiles, each (nz+2) long, 1-based
+  const double* lookup;    // device: lookup_ustr, 1-based
+};
+
+}  // namespace mgpu

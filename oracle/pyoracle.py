@@ -1,0 +1,134 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+The oracle is a C++ restatement of MONC's Fortran dynamical-core timestep (monc_oracle.cpp).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module, as the
+checker; the GPU library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libmonc_oracle.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_void_p]
+        L.orc_destroy.argtypes = [C.c_void_p]
+        for name in ("orc_set_field", "orc_get_field", "orc_get_field_monc"):
+            f = getattr(L, name)
+            f.restype = C.c_int
+            f.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_get_profile.restype = C.c_int
+        L.orc_get_profile.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        L.orc_step.restype = C.c_int
+        L.orc_step.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_timestep.restype = C.c_int
+        L.orc_set_timestep.argtypes = [C.c_void_p, C.c_int]
+        L.orc_component.restype = C.c_int
+        L.orc_component.argtypes = [C.c_void_p, C.c_int]
+        L.orc_divmax.restype = C.c_double
+        L.orc_divmax.argtypes = [C.c_void_p]
+        L.orc_solver_iterations.restype = C.c_int
+        L.orc_solver_iterations.argtypes = [C.c_void_p]
+        L.orc_solver_residual.restype = C.c_double
+        L.orc_solver_residual.argtypes = [C.c_void_p]
+        L.orc_fft_c2c.restype = C.c_int
+        L.orc_fft_c2c.argtypes = [C.c_int, C.c_void_p, C.c_int]
+        L.orc_lookup_ustr.restype = C.c_double
+        L.orc_lookup_ustr.argtypes = [C.c_void_p, C.c_double]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """One CPU model instance (MONC layout internally, [nz][ny][nx] arrays at the boundary)."""
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.nx, self.ny, self.nz = cfg.nx, cfg.ny, cfg.nz
+        self.h = lib().orc_create(C.byref(cfg))
+        if not self.h:
+            raise RuntimeError("oracle creation failed")
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set(self, fid: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.nz, self.ny, self.nx)
+        if lib().orc_set_field(self.h, fid, a.ctypes.data) != 0:
+            raise KeyError(fid)
+
+    def get(self, fid: int) -> np.ndarray:
+        a = np.empty((self.nz, self.ny, self.nx), dtype=np.float64)
+        if lib().orc_get_field(self.h, fid, a.ctypes.data) != 0:
+            raise KeyError(fid)
+        return a
+
+    def get_monc(self, fid: int) -> np.ndarray:
+        a = np.empty((self.nx + 4, self.ny + 4, self.nz), dtype=np.float64)
+        if lib().orc_get_field_monc(self.h, fid, a.ctypes.data) != 0:
+            raise KeyError(fid)
+        return a
+
+    def profile(self, name: str) -> np.ndarray:
+        a = np.empty(self.nz, dtype=np.float64)
+        if lib().orc_get_profile(self.h, name.encode(), a.ctypes.data) != 0:
+            raise KeyError(name)
+        return a
+
+    def step(self, n: int = 1):
+        if lib().orc_step(self.h, n) != 0:
+            raise RuntimeError("oracle step failed")
+
+    def set_timestep(self, ts: int):
+        lib().orc_set_timestep(self.h, ts)
+
+    def component(self, cid: int):
+        rc = lib().orc_component(self.h, cid)
+        if rc != 0:
+            raise RuntimeError(f"oracle component {cid} failed ({rc})")
+
+    def divmax(self) -> float:
+        return lib().orc_divmax(self.h)
+
+    def solver_stats(self):
+        return lib().orc_solver_iterations(self.h), lib().orc_solver_residual(self.h)
+
+    def lookup_ustr(self, vel: float) -> float:
+        return lib().orc_lookup_ustr(self.h, vel)
+
+
+def fft_c2c(x: np.ndarray, sign: int) -> np.ndarray:
+    """FFTPACK zfftf (sign=-1) / zfftb (sign=+1) of a complex vector, unnormalised."""
+    n = len(x)
+    buf = np.empty(2 * n, dtype=np.float64)
+    buf[0::2] = x.real
+    buf[1::2] = x.imag
+    if lib().orc_fft_c2c(n, buf.ctypes.data, sign) != 0:
+        raise ValueError("length must be a power of two")
+    return buf[0::2] + 1j * buf[1::2]
