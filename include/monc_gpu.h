@@ -125,6 +125,7 @@ typedef struct mgpu_config {
   double  tolerance;                  /* tolerance */
   int32_t max_iterations;             /* max_iterations */
   int32_t precision;                  /* MGPU_FP64 / MGPU_FP32_MIXED */
+  int32_t reproducible;               /* 1: fused kernels without FMA contraction (bit-reproducible) */
   /* science constants (global_config:355-372) */
   double  von_karman_constant, z0, z0th, alphah, betam, betah, gammam, gammah;
   double  pi, cp, rlvap, r, G, convective_limit, ratio_mol_wts, rlargep;

@@ -21,7 +21,9 @@ UNITS = [
     ("grid.cpp", []),
     ("api.cu", []),
     ("dycore_f64.cu", ["--fmad=false"]),
-    ("dycore_f32.cu", []),
+    ("dycore_f64_fast.cu", []),
+    ("dycore_f32.cu", ["--fmad=false"]),
+    ("dycore_f32_fast.cu", []),
     ("fft.cu", []),
     ("iter.cu", []),
 ]

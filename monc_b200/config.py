@@ -54,6 +54,7 @@ class MgpuConfig(C.Structure):
         ("tolerance", C.c_double),
         ("max_iterations", C.c_int32),
         ("precision", C.c_int32),
+        ("reproducible", C.c_int32),
         ("von_karman_constant", C.c_double), ("z0", C.c_double), ("z0th", C.c_double),
         ("alphah", C.c_double), ("betam", C.c_double), ("betah", C.c_double),
         ("gammam", C.c_double), ("gammah", C.c_double),
@@ -101,6 +102,7 @@ def default_config() -> MgpuConfig:
     c.tolerance = 1.0e-4
     c.max_iterations = 500
     c.precision = FP64
+    c.reproducible = 0
     c.von_karman_constant = 0.4
     c.z0 = 2.0e-3
     c.z0th = 2.0e-4

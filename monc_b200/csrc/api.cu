@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -129,10 +130,17 @@ static void fill_scalars(mgpu_handle* h) {
   s.cq0 = r.cq.empty() ? 0.0 : r.cq[0];
   s.lookup_entries = r.lookup_entries;
   s.forward = 1;
+  {
+    const char* e = std::getenv("MGPU_POINT_DYNAMICS");
+    s.point_dynamics = (e && e[0] == '1') ? 1 : 0;
+  }
   s.passive_th = c.passive_th; s.passive_q = c.passive_q; s.nq = c.number_q_fields;
   s.iqv = 0; s.iql = c.number_q_fields > 1 ? 1 : 0;
   s.coriolis = c.coriolis_enabled; s.surface_bcs = c.use_surface_boundary_conditions;
   s.use_vd = c.use_viscosity_and_diffusion;
+  s.rho_unity = 1;
+  for (int k = 1; k <= c.nz; ++k)
+    if (r.rho[k] != 1.0 || r.rhon[k] != 1.0) s.rho_unity = 0;
   s.prof = h->prof_d;
   s.lookup = h->lookup_d;
 }
@@ -404,18 +412,22 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   h->sc.forward = (h->timestep == 1) ? 1 : 0;  // steppingdirection.F90:44-48
   auto mark = [&](int q) { if (h->profiling) cudaEventRecord(h->ev[q], h->stream); };
   mark(0);
-  launch_fused_subgrid<T>(h->sc, d, h->stream);
+  if (h->cfg.reproducible) exact::launch_fused_subgrid<T>(h->sc, d, h->stream);
+  else fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
   mark(1);
-  launch_fused_dynamics<T>(h->sc, d, h->stream);
+  if (h->cfg.reproducible) exact::launch_fused_dynamics<T>(h->sc, d, h->stream);
+  else fast::launch_fused_dynamics<T>(h->sc, d, h->stream);
   mark(2);
   swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
-  launch_fused_pressure_source<T>(h->sc, d, h->stream);
+  if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
+  else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
   h->launches += 3;
   if (h->cfg.solver != MGPU_SOLVER_FFT) mark(3);
   int rc = pressure_solve<T>(h, d.p);
   if (rc) return rc;
   if (h->cfg.solver != MGPU_SOLVER_FFT) mark(8);
-  launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+  if (h->cfg.reproducible) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+  else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
   mark(9);
   h->launches += 1;
   h->timestep += 1;
@@ -442,7 +454,7 @@ static int component(mgpu_handle* h, DevState<T>& d, int cid) {
       break;
     case MGPU_C_DIVERR:
       CK(cudaMemsetAsync(h->divmax_d, 0, sizeof(unsigned long long), h->stream));
-      rc = launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
+      rc = exact::launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
       if (rc) return fail(h, rc, "component failed");
       {
         unsigned long long bits = 0;
@@ -454,7 +466,7 @@ static int component(mgpu_handle* h, DevState<T>& d, int cid) {
       }
       break;
     default:
-      rc = launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
+      rc = exact::launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
       if (rc) return fail(h, rc, "unknown or unsupported component");
   }
   CK(cudaGetLastError());

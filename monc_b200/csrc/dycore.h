@@ -23,13 +23,19 @@ struct DevState {
   T* zq_n[MGPU_MAX_Q];
 };
 
-template <typename T>
-int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st, unsigned long long* divmax,
-                     int64_t* launches);
-template <typename T> void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st);
-template <typename T> void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st);
-template <typename T> void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st);
-template <typename T> void launch_fused_pstep_swap(const Scalars& s, DevState<T>& d, cudaStream_t st);
+// Kernel launchers, built twice: `exact` compiles every multiply and add separately rounded
+// (MONC's x86-64 arithmetic, bit-reproducible against the CPU oracle), `fast` lets nvcc contract
+// multiply-adds into FMAs.  Component kernels always come from `exact`.
+#define MGPU_DECLARE_LAUNCHERS                                                                            \
+  template <typename T>                                                                                   \
+  int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st, unsigned long long* divmax, \
+                       int64_t* launches);                                                                \
+  template <typename T> void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st);     \
+  template <typename T> void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st);    \
+  template <typename T> void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st); \
+  template <typename T> void launch_fused_pstep_swap(const Scalars& s, DevState<T>& d, cudaStream_t st);
+namespace exact { MGPU_DECLARE_LAUNCHERS }
+namespace fast { MGPU_DECLARE_LAUNCHERS }
 
 // Spectral pressure solve (fftsolver): p (levels 1..nz) -> p.
 struct FftPlanDev {

@@ -42,6 +42,11 @@ template <typename T> __device__ __forceinline__ T tsign(T a, T b) { return copy
 template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }  // Fortran MAX
 template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
 template <typename T> __device__ __forceinline__ T sqr(T a) { return a * a; }
+// 1/x rounded to nearest: the same value IEEE division 1.0/x produces, with a shorter sequence
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+// x / r where r is a reference density; Boussinesq runs have r == 1 exactly and x/1 == x
+template <typename T> __device__ __forceinline__ T div_rho(const Scalars& s, T x, T r) { return s.rho_unity ? x : x / r; }
 template <typename T> __device__ __forceinline__ T cub(T a) { return a * a * a; }
 
 // ------------------------------------------------------------------------------------------
@@ -118,9 +123,9 @@ __device__ void lower_bc_column(const Scalars& s, const Prof<T>& P, const View<T
 // ------------------------------------------------------------------------------------------
 // smagorinsky (smagorinsky.F90:180-304 setfri + dry Ri, :316-402 moist Ri, :487-696 strain)
 // ------------------------------------------------------------------------------------------
-template <typename T>
-__device__ T half_squared_strain(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V,
-                                 const View<T>& W, int k, int j, int i) {
+template <typename T, class A>
+__device__ T half_squared_strain(const Scalars& s, const Prof<T>& P, const A& U, const A& V,
+                                 const A& W, int k, int j, int i) {
   const T cx = (T)s.cx, cy = (T)s.cy, cx2 = (T)s.cx2, cy2 = (T)s.cy2;
   const T rdzn1 = P(P_RDZN, k + 1);
   T ssq11 = cx2 * (sqr(U(k + 1, j, i) - U(k + 1, j, i - 1)) + sqr(U(k, j, i) - U(k, j, i - 1)));
@@ -147,7 +152,7 @@ __device__ T half_squared_strain(const Scalars& s, const Prof<T>& P, const View<
 template <typename T>
 __device__ T moist_ri(const Scalars& s, const Prof<T>& P, T ssq, const View<T>& TH, const View<T>& QV,
                       const View<T>& QL, int k, int j, int i) {
-  T tmpinv = (T)1.0 / ssq;
+  T tmpinv = rcp(ssq);
   T scltmp = P(P_RDZN, k + 1) * P(P_BUOY_CO, k);
   const T rl = (T)s.rlvap_over_cp, eps = (T)s.eps;
   const T qsat = P(P_QSAT, k), dq = P(P_DQSATDT, k), rpr = P(P_RPREFRCP, k), tst = P(P_TSTARPR, k), fac = P(P_QSATFAC, k);
@@ -177,7 +182,7 @@ template <typename T>
 __device__ void smagorinsky_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V,
                                   const View<T>& W, const View<T>& THcur, const View<T>& THarg, const View<T>* QV,
                                   const View<T>* QL, int k, int j, int i, T& vis, T& diff) {
-  T ssq = half_squared_strain<T>(s, P, U, V, W, k, j, i);
+  T ssq = half_squared_strain<T, View<T>>(s, P, U, V, W, k, j, i);
   T ri = (T)0.0;
   if (!s.passive_th) {
     if (!s.passive_q) ri = moist_ri<T>(s, P, ssq, THarg, *QV, *QL, k, j, i);
@@ -206,8 +211,8 @@ __device__ void smagorinsky_point(const Scalars& s, const Prof<T>& P, const View
 // ------------------------------------------------------------------------------------------
 // pw_advection advect_flow_fields (pwadvection.F90:466-610): assigned sources, 2<=k<=nz
 // ------------------------------------------------------------------------------------------
-template <typename T>
-__device__ void pw_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+template <typename T, class A>
+__device__ void pw_point(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
                          int k, int j, int i, T& su, T& sv, T& sw) {
   const T tcx = (T)s.tcx, tcy = (T)s.tcy;
   const T u0 = U(k, j, i), v0 = V(k, j, i);
@@ -248,9 +253,9 @@ struct Tau13 {
   T t13, t13m1, t23, t23m1;
 };
 
-template <typename T>
-__device__ Tau13<T> tau_13_23(const Scalars& s, const Prof<T>& P, const View<T>& ZU, const View<T>& ZV,
-                              const View<T>& ZW, const View<T>& VIS, int k, int j, int i) {
+template <typename T, class A>
+__device__ Tau13<T> tau_13_23(const Scalars& s, const Prof<T>& P, const A& ZU, const A& ZV,
+                              const A& ZW, const A& VIS, int k, int j, int i) {
   Tau13<T> t;
   if (k >= s.nz) { t.t13 = t.t13m1 = t.t23 = t.t23m1 = (T)0.0; return t; }
   const T cx = (T)s.cx, cy = (T)s.cy, rdzn = P(P_RDZN, k + 1), rho = P(P_RHO, k);
@@ -273,16 +278,16 @@ __device__ Tau13<T> tau_13_23(const Scalars& s, const Prof<T>& P, const View<T>&
   return t;
 }
 
-template <typename T>
-__device__ T tau33_at(const Scalars& s, const Prof<T>& P, const View<T>& ZW, const View<T>& VIS, int k, int j, int i) {
+template <typename T, class A>
+__device__ T tau33_at(const Scalars& s, const Prof<T>& P, const A& ZW, const A& VIS, int k, int j, int i) {
   if (k <= 1) return (T)0.0;
   T visonp2 = P(P_RHON, k) * (VIS(k, j, i) + VIS(k - 1, j, i));
   return visonp2 * (ZW(k, j, i) - ZW(k - 1, j, i)) * P(P_RDZ, k);
 }
 
-template <typename T>
-__device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const View<T>& ZU, const View<T>& ZV,
-                                const View<T>& ZW, const View<T>& ZU_state, const View<T>& VIS, int k, int j, int i,
+template <typename T, class A>
+__device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const A& ZU, const A& ZV,
+                                const A& ZW, const A& ZU_state, const A& VIS, int k, int j, int i,
                                 T& du, T& dv, T& dw) {
   const T cx = (T)s.cx, cy = (T)s.cy, rhon = P(P_RHON, k);
   // horizontal stresses at level k (k >= 2)
@@ -307,14 +312,14 @@ __device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const View<T
   T tau22_yp1 = visonp2 * (ZV(k, j + 1, i) - ZV(k, j, i)) * cy;
   T visonp2a = rhon * (VIS(k, j, i + 1) + VIS(k - 1, j, i + 1));
   T tau11p1 = visonp2a * (ZU_state(k, j, i + 1) - ZU(k, j, i)) * cx;  // reads current_state%zu at x+1
-  Tau13<T> t0 = tau_13_23<T>(s, P, ZU, ZV, ZW, VIS, k, j, i);
-  Tau13<T> tm = tau_13_23<T>(s, P, ZU, ZV, ZW, VIS, k - 1, j, i);
-  du = ((tau11p1 - tau11) * cx + (tau12 - tau12_ym1) * cy + (t0.t13 - tm.t13) * P(P_RDZ, k)) / rhon;
-  dv = ((tau12 - tau12m1) * cx + (tau22_yp1 - tau22) * cy + (t0.t23 - tm.t23) * P(P_RDZ, k)) / rhon;
+  Tau13<T> t0 = tau_13_23<T, A>(s, P, ZU, ZV, ZW, VIS, k, j, i);
+  Tau13<T> tm = tau_13_23<T, A>(s, P, ZU, ZV, ZW, VIS, k - 1, j, i);
+  du = div_rho<T>(s, (tau11p1 - tau11) * cx + (tau12 - tau12_ym1) * cy + (t0.t13 - tm.t13) * P(P_RDZ, k), rhon);
+  dv = div_rho<T>(s, (tau12 - tau12m1) * cx + (tau22_yp1 - tau22) * cy + (t0.t23 - tm.t23) * P(P_RDZ, k), rhon);
   if (k < s.nz) {
-    T t33p = tau33_at<T>(s, P, ZW, VIS, k + 1, j, i);
-    T t33 = tau33_at<T>(s, P, ZW, VIS, k, j, i);
-    dw = ((t0.t13 - t0.t13m1) * cx + (t0.t23 - t0.t23m1) * cy + (t33p - t33) * P(P_RDZN, k + 1)) / P(P_RHO, k);
+    T t33p = tau33_at<T, A>(s, P, ZW, VIS, k + 1, j, i);
+    T t33 = tau33_at<T, A>(s, P, ZW, VIS, k, j, i);
+    dw = div_rho<T>(s, (t0.t13 - t0.t13m1) * cx + (t0.t23 - t0.t23m1) * cy + (t33p - t33) * P(P_RDZN, k + 1), P(P_RHO, k));
   } else {
     dw = (T)0.0;
   }
@@ -323,8 +328,8 @@ __device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const View<T
 // ------------------------------------------------------------------------------------------
 // coriolis (coriolis.F90:243-258), buoyancy (buoyancy.F90:229-262)
 // ------------------------------------------------------------------------------------------
-template <typename T>
-__device__ void coriolis_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, int k, int j,
+template <typename T, class A>
+__device__ void coriolis_point(const Scalars& s, const Prof<T>& P, const A& U, const A& V, int k, int j,
                                int i, T& su, T& sv) {
   const T f = (T)s.fcoriol;
   su = su + f * ((T)0.25 * (V(k, j, i) + V(k, j, i + 1) + V(k, j - 1, i) + V(k, j - 1, i + 1)) + (T)s.vgal - P(P_GWY, k));
@@ -351,10 +356,10 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
                                         T curv_term) {
   const T r6 = (T)(1.0 / 6.0);
   T cflmod = fabs(data_value * c * dt);
-  T hrcfl = (T)1.0 / (sum_cfl_out + (T)1.e-30);
+  T hrcfl = rcp(sum_cfl_out + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = r6 * ((T)1.0 - cflmod * cflmod);
-  T rfdels = (T)1.0 / (fdels + (T)1.e-30);
+  T rfdels = rcp(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * curv_term - fgt1 - fgt2;
   T fnfs = (ffs - fu) * rfdels;
   T fncs = (fc - fu) * rfdels;
@@ -364,9 +369,9 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
 }
 
 // face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx
-template <typename T>
-__device__ T tvd_face_x(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
-                        const View<T>& ZF, T dt, int k, int j, int i) {
+template <typename T, class A>
+__device__ T tvd_face_x(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+                        const A& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const int kp1 = k + 1 < nz ? k + 1 : nz;
@@ -419,9 +424,9 @@ __device__ T tvd_face_x(const Scalars& s, const Prof<T>& P, const View<T>& U, co
 }
 
 // face y+1/2 of cell (k, j, i): flux_y(k) of ultflx
-template <typename T>
-__device__ T tvd_face_y(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
-                        const View<T>& ZF, T dt, int k, int j, int i) {
+template <typename T, class A>
+__device__ T tvd_face_y(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+                        const A& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const int kp1 = k + 1 < nz ? k + 1 : nz;
@@ -460,9 +465,9 @@ __device__ T tvd_face_y(const Scalars& s, const Prof<T>& P, const View<T>& U, co
 }
 
 // flux_z(k+1): face above level k (2 <= k <= nz-1); the top routine handles k = nz-1
-template <typename T>
-__device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
-                        const View<T>& ZF, T dt, int k, int j, int i) {
+template <typename T, class A>
+__device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+                        const A& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const T w0 = W(k, j, i);
@@ -507,10 +512,10 @@ __device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const View<T>& U, co
     // calculate_flux_in_w
     T dd = P(P_DZN, k + 1), rdd = P(P_RDZN, k + 1);
     T cflmod = fabs(w0 * rdd * dt);
-    T hrcfl = (T)1.0 / (sum + (T)1.e-30);
+    T hrcfl = rcp(sum + (T)1.e-30);
     T hcfl = (T)0.5 * cflmod;
     T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-    T rfdels = (T)1.0 / (fdels + (T)1.e-30);
+    T rfdels = rcp(fdels + (T)1.e-30);
     T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
     T fnfs = (ffs - fu) * rfdels;
     T fncs = (fc - fu) * rfdels;
@@ -547,10 +552,10 @@ __device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const View<T>& U, co
   rdc = P(P_RDZ, k) * advpos + P(P_RDZ, k + 1) * advneg;
   T dd = P(P_DZN, k + 1), rdd = P(P_RDZN, k + 1);
   T cflmod = fabs(w0 * rdd * dt);
-  T hrcfl = (T)1.0 / (sum + (T)1.e-30);
+  T hrcfl = rcp(sum + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-  T rfdels = (T)1.0 / (fdels + (T)1.e-30);
+  T rfdels = rcp(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
   T fnfs = (ffs - fu) * rfdels;
   T fncs = (fc - fu) * rfdels;
@@ -562,8 +567,8 @@ __device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const View<T>& U, co
 // TVD source of cell (k, j, i), 2 <= k <= nz, from the six face values
 // acc0 is the source value before the callback (MONC accumulates into it below the top level
 // and zeroes it at the top level)
-template <typename T>
-__device__ T tvd_source(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
+template <typename T, class A>
+__device__ T tvd_source(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
                         T fx_m, T fx_p, T fy_m, T fy_p, T fz_m, T fz_p, int k, int j, int i, T acc0) {
   const T cx = (T)s.cx, cy = (T)s.cy;
   T acc = (k < s.nz) ? acc0 : (T)0.0;
@@ -579,24 +584,24 @@ __device__ T tvd_source(const Scalars& s, const Prof<T>& P, const View<T>& U, co
   return acc;
 }
 
-template <typename T>
-__device__ T tvd_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V, const View<T>& W,
-                       const View<T>& ZF, int k, int j, int i, T acc0) {
+template <typename T, class A>
+__device__ T tvd_point(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+                       const A& ZF, int k, int j, int i, T acc0) {
   const T dt = (T)(s.dtm * 2.0);
-  T fxm = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i - 1);
-  T fxp = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i);
-  T fym = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j - 1, i);
-  T fyp = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j, i);
-  T fzm = (k == 2) ? (T)0.0 : tvd_face_z<T>(s, P, U, V, W, ZF, dt, k - 1, j, i);
-  T fzp = (k < s.nz) ? tvd_face_z<T>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
-  return tvd_source<T>(s, P, U, V, W, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, acc0);
+  T fxm = tvd_face_x<T, A>(s, P, U, V, W, ZF, dt, k, j, i - 1);
+  T fxp = tvd_face_x<T, A>(s, P, U, V, W, ZF, dt, k, j, i);
+  T fym = tvd_face_y<T, A>(s, P, U, V, W, ZF, dt, k, j - 1, i);
+  T fyp = tvd_face_y<T, A>(s, P, U, V, W, ZF, dt, k, j, i);
+  T fzm = (k == 2) ? (T)0.0 : tvd_face_z<T, A>(s, P, U, V, W, ZF, dt, k - 1, j, i);
+  T fzp = (k < s.nz) ? tvd_face_z<T, A>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
+  return tvd_source<T, A>(s, P, U, V, W, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, acc0);
 }
 
 // ------------------------------------------------------------------------------------------
 // diffusion general_diffusion (diffusion.F90:501-545), 2 <= k <= nz
 // ------------------------------------------------------------------------------------------
-template <typename T>
-__device__ T diffusion_point(const Scalars& s, const Prof<T>& P, const View<T>& F, const View<T>& D, int k, int j, int i) {
+template <typename T, class A>
+__device__ T diffusion_point(const Scalars& s, const Prof<T>& P, const A& F, const A& D, int k, int j, int i) {
   const T f0 = F(k, j, i), d0 = D(k, j, i), dm = D(k - 1, j, i);
   T term = (T)s.cx2 * (T)0.25 *
                (((d0 + D(k, j, i - 1)) + (dm + D(k - 1, j, i - 1))) * (F(k, j, i - 1) - f0) -

@@ -20,7 +20,12 @@
 #include "dycore.h"
 #include "dycore_device.cuh"
 
+#ifndef KVARIANT
+#define KVARIANT exact
+#endif
+
 namespace mgpu {
+namespace KVARIANT {
 
 static inline dim3 pt_block() { return dim3(32, 8, 1); }
 static inline dim3 pt_grid(const Scalars& s, int kcount) {
@@ -115,7 +120,7 @@ __global__ void k_c_pw(Scalars s, DevState<T> d) {
   Prof<T> P = prof<T>(s);
   View<T> U = view<T>(d.u, s), V = view<T>(d.v, s), W = view<T>(d.w, s);
   T su, sv, sw;
-  pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
+  pw_point<T, View<T>>(s, P, U, V, W, k, j, i, su, sv, sw);
   long long o = lin(s, k, j, i);
   d.su[o] = su;
   d.sv[o] = sv;
@@ -135,11 +140,11 @@ __global__ void k_c_tvd(Scalars s, DevState<T> d, const T* zf_th, T* sth, int n_
   // theta, then each q field (advect_theta, advect_q_fields)
   {
     View<T> ZF = view<T>(fwd ? d.th : d.zth, s);
-    d.sth[o] = tvd_point<T>(s, P, U, V, W, ZF, k, j, i, d.sth[o]);
+    d.sth[o] = tvd_point<T, View<T>>(s, P, U, V, W, ZF, k, j, i, d.sth[o]);
   }
   for (int n = 0; n < s.nq; ++n) {
     View<T> ZF = view<T>(fwd ? d.q[n] : d.zq[n], s);
-    d.sq[n][o] = tvd_point<T>(s, P, U, V, W, ZF, k, j, i, d.sq[n][o]);
+    d.sq[n][o] = tvd_point<T, View<T>>(s, P, U, V, W, ZF, k, j, i, d.sq[n][o]);
   }
   (void)zf_th; (void)sth; (void)n_extra;
 }
@@ -153,8 +158,8 @@ __global__ void k_c_diffusion(Scalars s, DevState<T> d) {
   Prof<T> P = prof<T>(s);
   View<T> D = view<T>(d.diff, s);
   long long o = lin(s, k, j, i);
-  d.sth[o] = d.sth[o] + diffusion_point<T>(s, P, view<T>(d.zth, s), D, k, j, i);
-  for (int n = 0; n < s.nq; ++n) d.sq[n][o] = d.sq[n][o] + diffusion_point<T>(s, P, view<T>(d.zq[n], s), D, k, j, i);
+  d.sth[o] = d.sth[o] + diffusion_point<T, View<T>>(s, P, view<T>(d.zth, s), D, k, j, i);
+  for (int n = 0; n < s.nq; ++n) d.sq[n][o] = d.sq[n][o] + diffusion_point<T, View<T>>(s, P, view<T>(d.zq[n], s), D, k, j, i);
 }
 
 template <typename T>
@@ -167,7 +172,7 @@ __global__ void k_c_viscosity(Scalars s, DevState<T> d) {
   bool fwd = s.forward;
   View<T> ZU = view<T>(fwd ? d.u : d.zu, s), ZV = view<T>(fwd ? d.v : d.zv, s), ZW = view<T>(fwd ? d.w : d.zw, s);
   T du, dv, dw;
-  viscosity_point<T>(s, P, ZU, ZV, ZW, view<T>(d.zu, s), view<T>(d.vis, s), k, j, i, du, dv, dw);
+  viscosity_point<T, View<T>>(s, P, ZU, ZV, ZW, view<T>(d.zu, s), view<T>(d.vis, s), k, j, i, du, dv, dw);
   long long o = lin(s, k, j, i);
   d.su[o] = d.su[o] + du;
   d.sv[o] = d.sv[o] + dv;
@@ -183,7 +188,7 @@ __global__ void k_c_coriolis(Scalars s, DevState<T> d) {
   Prof<T> P = prof<T>(s);
   long long o = lin(s, k, j, i);
   T su = d.su[o], sv = d.sv[o];
-  coriolis_point<T>(s, P, view<T>(d.u, s), view<T>(d.v, s), k, j, i, su, sv);
+  coriolis_point<T, View<T>>(s, P, view<T>(d.u, s), view<T>(d.v, s), k, j, i, su, sv);
   d.su[o] = su;
   d.sv[o] = sv;
 }
@@ -419,27 +424,27 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
   for (int n = 0; n < s.nq; ++n) sq[n] = (T)0.0;
   if (k >= 2) {
     // pw_advection (assigns), viscosity, coriolis, buoyancy: the order MONC adds them in
-    pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
+    pw_point<T, View<T>>(s, P, U, V, W, k, j, i, su, sv, sw);
     if (s.use_vd) {
       View<T> ZU = view<T>(fwd ? d.u : d.zu, s), ZV = view<T>(fwd ? d.v : d.zv, s), ZW = view<T>(fwd ? d.w : d.zw, s);
       T du, dv, dw;
-      viscosity_point<T>(s, P, ZU, ZV, ZW, view<T>(d.zu, s), view<T>(d.vis, s), k, j, i, du, dv, dw);
+      viscosity_point<T, View<T>>(s, P, ZU, ZV, ZW, view<T>(d.zu, s), view<T>(d.vis, s), k, j, i, du, dv, dw);
       su = su + du;
       sv = sv + dv;
       if (k < s.nz) sw = sw + dw;
     }
-    if (s.coriolis) coriolis_point<T>(s, P, U, V, k, j, i, su, sv);
+    if (s.coriolis) coriolis_point<T, View<T>>(s, P, U, V, k, j, i, su, sv);
     if (k < s.nz) {
       View<T> Q[MGPU_MAX_Q];
       for (int n = 0; n < s.nq; ++n) Q[n] = view<T>(d.q[n], s);
       sw = buoyancy_point<T>(s, P, view<T>(d.th, s), Q, k, j, i, sw);
     }
     // tvd_advection then diffusion of theta and q
-    sth = tvd_point<T>(s, P, U, V, W, view<T>(fwd ? d.th : d.zth, s), k, j, i, (T)0.0);
-    if (s.use_vd) sth = sth + diffusion_point<T>(s, P, view<T>(d.zth, s), view<T>(d.diff, s), k, j, i);
+    sth = tvd_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.th : d.zth, s), k, j, i, (T)0.0);
+    if (s.use_vd) sth = sth + diffusion_point<T, View<T>>(s, P, view<T>(d.zth, s), view<T>(d.diff, s), k, j, i);
     for (int n = 0; n < s.nq; ++n) {
-      sq[n] = tvd_point<T>(s, P, U, V, W, view<T>(fwd ? d.q[n] : d.zq[n], s), k, j, i, (T)0.0);
-      if (s.use_vd) sq[n] = sq[n] + diffusion_point<T>(s, P, view<T>(d.zq[n], s), view<T>(d.diff, s), k, j, i);
+      sq[n] = tvd_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.q[n] : d.zq[n], s), k, j, i, (T)0.0);
+      if (s.use_vd) sq[n] = sq[n] + diffusion_point<T, View<T>>(s, P, view<T>(d.zq[n], s), view<T>(d.diff, s), k, j, i);
     }
   }
   // stepfields (source at level 1 is zeroed there) and, for scalars, swap_smooth
@@ -478,6 +483,159 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
   for (int n = 0; n < s.nq; ++n) step_scalar(d.q[n], d.zq[n], sq[n], d.q_n[n], d.zq_n[n], true);
 }
 
+// 2'. Centred-step dynamics, shared-memory tiled.  A CTA owns a TX x TY tile of columns and
+//     marches up the levels.  The planes each level needs (with a 2-point periodic halo) sit in
+//     per-field ring buffers in shared memory, filled one level ahead with cp.async; every TVD
+//     face flux is computed once (x and y faces exchanged through shared memory, the z face
+//     carried in a register from the level below).  Arithmetic is the same device code as the
+//     point kernel, so the results are bit-identical to it.
+namespace tiled {
+constexpr int TX = 32, TY = 8, H = 2;
+constexpr int PW = TX + 2 * H, PH = TY + 2 * H, PLANE = PW * PH;
+constexpr int RZF = 8, R3 = 4;  // ring slots: zth (levels k-1..k+3), other fields (k-1..k+2)
+enum Slot { S_ZF = 0, S_U = S_ZF + RZF, S_V = S_U + R3, S_W = S_V + R3, S_ZU = S_W + R3, S_ZV = S_ZU + R3,
+            S_ZW = S_ZV + R3, S_VIS = S_ZW + R3, S_DIFF = S_VIS + R3, S_TOTAL = S_DIFF + R3 };
+template <typename T>
+constexpr size_t smem_bytes() {
+  return sizeof(T) * ((size_t)S_TOTAL * PLANE + (size_t)TY * (TX + 1) + (size_t)(TY + 1) * TX);
+}
+}  // namespace tiled
+
+template <typename T>
+struct SView {
+  const T* base;
+  int jb, ib;  // global (unwrapped) coordinates of local element (0, 0)
+  int rmask;   // ring slots - 1 (a power of two)
+  __device__ __forceinline__ T operator()(int k, int j, int i) const {
+    return base[((k & rmask) * tiled::PH + (j - jb)) * tiled::PW + (i - ib)];
+  }
+};
+
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, int bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// copy level k of a field (tile + halo, periodic) into ring slot `slot` of that field's planes
+template <typename T>
+__device__ __forceinline__ void stage_plane(T* ring, int rmask, const T* __restrict__ f, const Scalars& s, int k, int j0,
+                                            int i0, int tid) {
+  using namespace tiled;
+  T* dst = ring + (k & rmask) * PLANE;
+  const T* src = f + (long long)(k - 1) * s.plane;
+  for (int e = tid; e < PLANE; e += TX * TY) {
+    int jj = e / PW, ii = e - jj * PW;
+    int gj = j0 - H + jj, gi = i0 - H + ii;
+    gj = gj < 0 ? gj + s.ny : (gj >= s.ny ? gj - s.ny : gj);
+    gi = gi < 0 ? gi + s.nx : (gi >= s.nx ? gi - s.nx : gi);
+    cp_async_elem(dst + e, src + (long long)gj * s.nx + gi, (int)sizeof(T));
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(tiled::TX* tiled::TY, 1) k_f_dynamics_tiled(Scalars s, DevState<T> d) {
+  using namespace tiled;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  T* FX = sm + (size_t)S_TOTAL * PLANE;  // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
+  T* FY = FX + TY * (TX + 1);            // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool inside = (i < s.nx) && (j < s.ny);
+  const int nz = s.nz;
+  Prof<T> P = prof<T>(s);
+  const int jb = j0 - H, ib = i0 - H;
+  const SView<T> ZF{sm + S_ZF * PLANE, jb, ib, RZF - 1};
+  const SView<T> U{sm + S_U * PLANE, jb, ib, R3 - 1}, V{sm + S_V * PLANE, jb, ib, R3 - 1}, W{sm + S_W * PLANE, jb, ib, R3 - 1};
+  const SView<T> ZU{sm + S_ZU * PLANE, jb, ib, R3 - 1}, ZV{sm + S_ZV * PLANE, jb, ib, R3 - 1},
+      ZW{sm + S_ZW * PLANE, jb, ib, R3 - 1};
+  const SView<T> VIS{sm + S_VIS * PLANE, jb, ib, R3 - 1}, DIFF{sm + S_DIFF * PLANE, jb, ib, R3 - 1};
+  // prologue: planes for level 2 (zth 1..4, others 1..3, diff 1..2)
+  for (int kk = 1; kk <= 4 && kk <= nz; ++kk) stage_plane<T>(sm + S_ZF * PLANE, RZF - 1, d.zth, s, kk, j0, i0, tid);
+  for (int kk = 1; kk <= 3 && kk <= nz; ++kk) {
+    stage_plane<T>(sm + S_U * PLANE, R3 - 1, d.u, s, kk, j0, i0, tid);
+    stage_plane<T>(sm + S_V * PLANE, R3 - 1, d.v, s, kk, j0, i0, tid);
+    stage_plane<T>(sm + S_W * PLANE, R3 - 1, d.w, s, kk, j0, i0, tid);
+    stage_plane<T>(sm + S_ZU * PLANE, R3 - 1, d.zu, s, kk, j0, i0, tid);
+    stage_plane<T>(sm + S_ZV * PLANE, R3 - 1, d.zv, s, kk, j0, i0, tid);
+    stage_plane<T>(sm + S_ZW * PLANE, R3 - 1, d.zw, s, kk, j0, i0, tid);
+    stage_plane<T>(sm + S_VIS * PLANE, R3 - 1, d.vis, s, kk, j0, i0, tid);
+  }
+  for (int kk = 1; kk <= 2; ++kk) stage_plane<T>(sm + S_DIFF * PLANE, R3 - 1, d.diff, s, kk, j0, i0, tid);
+  // level 1: sources are zero there (stepfields zeroes them)
+  const T dtm_x2 = (T)(2.0 * s.dtm);
+  const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
+  if (inside) {
+    long long o = lin(s, 1, j, i);
+    d.zu_n[o] = (T)s.ugal + d.zu[o] + dtm_x2 * (T)0.0;
+    d.zv_n[o] = (T)s.vgal + d.zv[o] + dtm_x2 * (T)0.0;
+    d.zw_n[o] = (T)0.0 + d.zw[o] + dtm_x2 * (T)0.0;
+    T fv = d.th[o], zv = d.zth[o];
+    T sm1 = c1 * fv + c2 * zv;
+    T zn = (T)0.0 + zv + dtm_x2 * (T)0.0;
+    d.zth_n[o] = sm1 + (T)s.tsmth * zn;
+    d.th_n[o] = zn;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const T dt = (T)(s.dtm * 2.0);
+  T fz_lo = (T)0.0;  // flux_z(2) = 0
+  View<T> THg = view<T>(d.th, s);
+  for (int k = 2; k <= nz; ++k) {
+    // prefetch the planes level k+1 will add
+    if (k + 3 <= nz) stage_plane<T>(sm + S_ZF * PLANE, RZF - 1, d.zth, s, k + 3, j0, i0, tid);
+    if (k + 2 <= nz) {
+      stage_plane<T>(sm + S_U * PLANE, R3 - 1, d.u, s, k + 2, j0, i0, tid);
+      stage_plane<T>(sm + S_V * PLANE, R3 - 1, d.v, s, k + 2, j0, i0, tid);
+      stage_plane<T>(sm + S_W * PLANE, R3 - 1, d.w, s, k + 2, j0, i0, tid);
+      stage_plane<T>(sm + S_ZU * PLANE, R3 - 1, d.zu, s, k + 2, j0, i0, tid);
+      stage_plane<T>(sm + S_ZV * PLANE, R3 - 1, d.zv, s, k + 2, j0, i0, tid);
+      stage_plane<T>(sm + S_ZW * PLANE, R3 - 1, d.zw, s, k + 2, j0, i0, tid);
+      stage_plane<T>(sm + S_VIS * PLANE, R3 - 1, d.vis, s, k + 2, j0, i0, tid);
+    }
+    if (k + 1 <= nz) stage_plane<T>(sm + S_DIFF * PLANE, R3 - 1, d.diff, s, k + 1, j0, i0, tid);
+    // TVD faces of this level: own x+1/2 and y+1/2 faces, then the tile's low-side faces
+    FX[ty * (TX + 1) + tx + 1] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i);
+    FY[(ty + 1) * TX + tx] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j, i);
+    if (tid < TX) FY[tid] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j0 - 1, i0 + tid);
+    else if (tid < TX + TY) FX[(tid - TX) * (TX + 1)] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1);
+    T fz_hi = (k < nz) ? tvd_face_z<T>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
+    // momentum sources: pw (assigns), viscosity, coriolis, buoyancy
+    T su, sv, sw;
+    pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
+    if (s.use_vd) {
+      T du, dv, dw;
+      viscosity_point<T>(s, P, ZU, ZV, ZW, ZU, VIS, k, j, i, du, dv, dw);
+      su = su + du;
+      sv = sv + dv;
+      if (k < nz) sw = sw + dw;
+    }
+    if (s.coriolis) coriolis_point<T>(s, P, U, V, k, j, i, su, sv);
+    if (k < nz && !s.passive_th && inside) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (THg(k, j, i) + THg(k + 1, j, i));
+    __syncthreads();
+    T sth = tvd_source<T>(s, P, U, V, W, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1], FY[ty * TX + tx],
+                          FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
+    if (s.use_vd) sth = sth + diffusion_point<T>(s, P, ZF, DIFF, k, j, i);
+    fz_lo = fz_hi;
+    if (inside) {
+      long long o = lin(s, k, j, i);
+      d.zu_n[o] = (T)s.ugal + ZU(k, j, i) + dtm_x2 * su;
+      d.zv_n[o] = (T)s.vgal + ZV(k, j, i) + dtm_x2 * sv;
+      d.zw_n[o] = (T)0.0 + ZW(k, j, i) + dtm_x2 * sw;
+      T fv = THg(k, j, i), zv = ZF(k, j, i);
+      T smo = c1 * fv + c2 * zv;
+      T zn = (T)0.0 + zv + dtm_x2 * sth;
+      d.zth_n[o] = smo + (T)s.tsmth * zn;
+      d.th_n[o] = zn;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
 // 3. pressure source from the stepped z-velocities (diverr + psrce)
 template <typename T>
 __global__ void k_f_pressure_source(Scalars s, DevState<T> d) {
@@ -497,63 +655,66 @@ __global__ void k_f_pressure_source(Scalars s, DevState<T> d) {
   d.p[o] = pp * timec;
 }
 
-// 5. pstep + swap_smooth of u, v, w
+// 5. pstep + swap_smooth of u, v, w.  Every input is loaded before the first store so that the
+//    loads of a thread are in flight together (the outputs overwrite u, v, w, zu, zv, zw in place).
 template <typename T>
-__global__ void k_f_pstep_swap(Scalars s, DevState<T> d) {
+__global__ void __launch_bounds__(256) k_f_pstep_swap(Scalars s, DevState<T> d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z + 1;
   if (i >= s.nx || j >= s.ny || k > s.nz) return;
   Prof<T> P = prof<T>(s);
-  View<T> Pv = view<T>(d.p, s);
   const bool fwd = s.forward;
   const T dtmtmp = fwd ? (T)(0.5 * s.dtm) : (T)s.dtm;
-  long long o = lin(s, k, j, i);
+  const long long o = lin(s, k, j, i);
   const bool bc = s.use_vd && s.surface_bcs;
-  auto pu = [&](int kk) {
-    return d.zu_n[lin(s, kk, j, i)] + (T)2.0 * (T)s.cx * dtmtmp * (Pv(kk, j, i) - Pv(kk, j, i + 1));
-  };
-  auto pv = [&](int kk) {
-    return d.zv_n[lin(s, kk, j, i)] + (T)2.0 * (T)s.cy * dtmtmp * (Pv(kk, j, i) - Pv(kk, j + 1, i));
-  };
-  T zu_p, zv_p, zw_p;
-  if (k >= 2) {
-    zu_p = pu(k);
-    zv_p = pv(k);
-  } else if (bc) {
-    zu_p = -pu(2) - (T)2.0 * (T)s.ugal;
-    zv_p = -pv(2) - (T)2.0 * (T)s.vgal;
-  } else {
-    zu_p = pu(2);
-    zv_p = pv(2);
+  const int kp = (k >= 2) ? k : 2;  // level whose pressure gradient sets zu, zv (level 1 mirrors level 2)
+  const long long op = lin(s, kp, j, i);
+  const int ie = (i + 1 == s.nx) ? 0 : i + 1, jn = (j + 1 == s.ny) ? 0 : j + 1;
+  const T* __restrict__ p = d.p;
+  const T p0 = __ldg(p + op);
+  const T pe = __ldg(p + lin(s, kp, j, ie));
+  const T pn = __ldg(p + lin(s, kp, jn, i));
+  const T pz0 = __ldg(p + o);
+  const T pz1 = (k >= 2 && k < s.nz) ? __ldg(p + o + s.plane) : (T)0;
+  const T zun = __ldg(d.zu_n + op), zvn = __ldg(d.zv_n + op), zwn = __ldg(d.zw_n + o);
+  const T u0 = d.u[o], v0 = d.v[o], w0 = d.w[o], zu0 = d.zu[o], zv0 = d.zv[o], zw0 = d.zw[o];
+  T zu_p = zun + (T)2.0 * (T)s.cx * dtmtmp * (p0 - pe);
+  T zv_p = zvn + (T)2.0 * (T)s.cy * dtmtmp * (p0 - pn);
+  if (k == 1) {
+    if (bc) {
+      zu_p = -zu_p - (T)2.0 * (T)s.ugal;
+      zv_p = -zv_p - (T)2.0 * (T)s.vgal;
+    }
   }
-  zw_p = d.zw_n[o];
-  if (k >= 2 && k < s.nz) zw_p = zw_p + (T)2.0 * P(P_RDZN, k + 1) * dtmtmp * (Pv(k, j, i) - Pv(k + 1, j, i));
+  T zw_p = zwn;
+  if (k >= 2 && k < s.nz) zw_p = zw_p + (T)2.0 * P(P_RDZN, k + 1) * dtmtmp * (pz0 - pz1);
+  T nu, nzu, nv, nzv, nw, nzw;
   if (fwd) {
-    auto cl = [&](T* f, T* zf, T fv, T zn) {
-      T ev = fv + zn;
-      T nf = ev * (T)1.0 + fv * (T)-1.0;
-      f[o] = nf;
-      zf[o] = ev - nf;
-    };
-    cl(d.u, d.zu, (T)s.ugal + d.u[o], zu_p);
-    cl(d.v, d.zv, (T)s.vgal + d.v[o], zv_p);
-    cl(d.w, d.zw, d.w[o], zw_p);
+    T ev = ((T)s.ugal + u0) + zu_p;
+    nu = ev * (T)1.0 + ((T)s.ugal + u0) * (T)-1.0;
+    nzu = ev - nu;
+    ev = ((T)s.vgal + v0) + zv_p;
+    nv = ev * (T)1.0 + ((T)s.vgal + v0) * (T)-1.0;
+    nzv = ev - nv;
+    ev = w0 + zw_p;
+    nw = ev * (T)1.0 + w0 * (T)-1.0;
+    nzw = ev - nw;
   } else {
     const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
-    T ev = (T)s.ugal + d.u[o];
-    T sav = d.zu[o] + (T)s.ugal;
-    d.u[o] = zu_p;
-    d.zu[o] = c1 * ev + c2 * (zu_p + sav - (T)s.ugal);
-    ev = (T)s.vgal + d.v[o];
-    sav = d.zv[o] + (T)s.vgal;
-    d.v[o] = zv_p;
-    d.zv[o] = c1 * ev + c2 * (zv_p + sav - (T)s.vgal);
-    ev = d.w[o];
-    sav = d.zw[o] + (T)0.0;
-    d.w[o] = zw_p;
-    d.zw[o] = c1 * ev + c2 * (zw_p + sav);
+    nu = zu_p;
+    nzu = c1 * ((T)s.ugal + u0) + c2 * (zu_p + (zu0 + (T)s.ugal) - (T)s.ugal);
+    nv = zv_p;
+    nzv = c1 * ((T)s.vgal + v0) + c2 * (zv_p + (zv0 + (T)s.vgal) - (T)s.vgal);
+    nw = zw_p;
+    nzw = c1 * w0 + c2 * (zw_p + (zw0 + (T)0.0));
   }
+  d.u[o] = nu;
+  d.zu[o] = nzu;
+  d.v[o] = nv;
+  d.zv[o] = nzv;
+  d.w[o] = nw;
+  d.zw[o] = nzw;
 }
 
 // ==========================================================================================
@@ -600,7 +761,21 @@ void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st) {
 }
 template <typename T>
 void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
-  k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
+  // the tiled kernel covers centred dry steps; the first (forward) step and moist runs use the
+  // point kernel
+  const bool tiled_ok = !s.forward && !s.point_dynamics && s.nq == 0 && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 && s.nz >= 4;
+  if (!tiled_ok) {
+    k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
+    return;
+  }
+  const size_t smem = tiled::smem_bytes<T>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_f_dynamics_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  dim3 grid(s.nx / tiled::TX, s.ny / tiled::TY, 1), block(tiled::TX, tiled::TY, 1);
+  k_f_dynamics_tiled<T><<<grid, block, smem, st>>>(s, d);
 }
 template <typename T>
 void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st) {
@@ -611,4 +786,5 @@ void launch_fused_pstep_swap(const Scalars& s, DevState<T>& d, cudaStream_t st) 
   k_f_pstep_swap<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
 }
 
+}  // namespace KVARIANT
 }  // namespace mgpu

@@ -39,16 +39,21 @@ static int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
 
 // In-place radix-2 decimation-in-time stages over `nrows` rows held in shared memory in
 // bit-reversed order.  Element e of row r lives at buf[r*rs + e*es].
+// rows_fast selects which index consecutive threads walk: the row (when rows are the contiguous
+// dimension in shared memory, es > 1) or the butterfly within a row (es == 1), so that a warp
+// touches consecutive shared-memory words.
 template <typename C>
-__device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int es, const C* tw, bool inverse) {
+__device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int es, const C* tw, bool inverse,
+                                bool rows_fast = false) {
   const int half_n = n >> 1;
   const int total = nrows * half_n;
   for (int s = 1; s <= logn; ++s) {
     const int half = 1 << (s - 1);
     const int stride = n >> s;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      int r = b / half_n;
-      int bb = b - r * half_n;
+      int r, bb;
+      if (rows_fast) { bb = b / nrows; r = b - bb * nrows; }
+      else { r = b / half_n; bb = b - r * half_n; }
       int pos = bb & (half - 1);
       int i0 = ((bb >> (s - 1)) << s) | pos;
       int i1 = i0 + half;
@@ -191,7 +196,7 @@ __global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<
   }
   __syncthreads();
   // rows = columns here: element e of column c at buf[e*cols + c]
-  smem_fft_stages<C>(buf, ny, logn, cols, 1, cols, tw, inverse);
+  smem_fft_stages<C>(buf, ny, logn, cols, 1, cols, tw, inverse, true);
   const T sc = inverse ? (T)(1.0 / (double)ny) : (T)1.0;
   for (int t = threadIdx.x; t < cols * ny; t += blockDim.x) {
     int e = t / cols, c = t - e * cols;
@@ -244,32 +249,55 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   const int kyi = ky <= ny / 2 ? ky : ny - ky;
   const long long bstride = (long long)(ny / 2 + 1) * nxh;
   const double* bcol = b1 + (long long)kyi * nxh + kx;
-  // forward elimination: s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1)
+  // forward elimination s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1), loads batched 8 levels at a time
+  constexpr int B = 8;
   C v = sp[plane];
   double sr = (double)v.x, si = (double)v.y;
   s1buf[col + plane] = make_double2(sr, si);
-  for (int k = 3; k <= nz; ++k) {
-    C vk = sp[(long long)(k - 1) * plane];
-    double bm = bcol[(long long)(k - 1) * bstride];
-    sr = (double)vk.x - czb[k] * sr * bm;
-    si = (double)vk.y - czb[k] * si * bm;
-    s1buf[col + (long long)(k - 1) * plane] = make_double2(sr, si);
+  for (int k0 = 3; k0 <= nz; k0 += B) {
+    C vb[B];
+    double bb[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      int k = k0 + q;
+      if (k <= nz) { vb[q] = sp[(long long)(k - 1) * plane]; bb[q] = __ldg(bcol + (long long)(k - 1) * bstride); }
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      int k = k0 + q;
+      if (k <= nz) {
+        sr = (double)vb[q].x - czb[k] * sr * bb[q];
+        si = (double)vb[q].y - czb[k] * si * bb[q];
+        s1buf[col + (long long)(k - 1) * plane] = make_double2(sr, si);
+      }
+    }
   }
-  // back substitution
-  double pr = sr * bcol[(long long)nz * bstride];
-  double pi = si * bcol[(long long)nz * bstride];
+  // back substitution pt(k) = (s1(k) - cza(k)*pt(k+1))*b1(k)
+  double pr = sr * __ldg(bcol + (long long)nz * bstride);
+  double pi = si * __ldg(bcol + (long long)nz * bstride);
   C o;
   o.x = (T)pr;
   o.y = (T)pi;
   sp[(long long)(nz - 1) * plane] = o;
-  for (int k = nz - 1; k >= 2; --k) {
-    double2 s = s1buf[col + (long long)(k - 1) * plane];
-    double bk = bcol[(long long)k * bstride];
-    pr = (s.x - cza[k] * pr) * bk;
-    pi = (s.y - cza[k] * pi) * bk;
-    o.x = (T)pr;
-    o.y = (T)pi;
-    sp[(long long)(k - 1) * plane] = o;
+  for (int k0 = nz - 1; k0 >= 2; k0 -= B) {
+    double2 sb[B];
+    double bb[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      int k = k0 - q;
+      if (k >= 2) { sb[q] = s1buf[col + (long long)(k - 1) * plane]; bb[q] = __ldg(bcol + (long long)k * bstride); }
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      int k = k0 - q;
+      if (k >= 2) {
+        pr = (sb[q].x - cza[k] * pr) * bb[q];
+        pi = (sb[q].y - cza[k] * pi) * bb[q];
+        o.x = (T)pr;
+        o.y = (T)pi;
+        sp[(long long)(k - 1) * plane] = o;
+      }
+    }
   }
 }
 

@@ -55,6 +55,8 @@ struct Scalars {
   double cq0;  // cq of the vapour field
   int lookup_entries;
   int forward;  // 1 on the first (forward) step
+  int point_dynamics;  // 1: always use the untiled dynamics kernel (MGPU_POINT_DYNAMICS=1)
+  int rho_unity;       // 1 when rho = rhon = 1 on every level (Boussinesq with rhobous = 1)
   int passive_th, passive_q, nq, iqv, iql;
   int coriolis, surface_bcs, use_vd;
   const double* prof;      // device: P_COUNT profiles, each (nz+2) long, 1-based

@@ -25,8 +25,7 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
-            build()
+        build()  # make is a no-op when the library is newer than its sources
         L = C.CDLL(_LIB_PATH)
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_void_p]

@@ -105,8 +105,9 @@ def test_component_fp32_close_to_oracle(gpu_lib, comp):
         assert rel_err(a, b) <= tol, f"{comp}/{f}: FP32 rel err {rel_err(a, b):.3e}"
 
 
-def cbl_pair(n=64, nz=65, precision=cf.FP64, ug=5.0, fcoriol=1e-4, seed=5):
+def cbl_pair(n=64, nz=65, precision=cf.FP64, ug=5.0, fcoriol=1e-4, seed=5, reproducible=0):
     c = cf.dry_cbl_config(n, n, nz, 50.0, 25.0, 1.0, ug=ug, fcoriol=fcoriol, precision=precision)
+    c.reproducible = reproducible
     o = po.Oracle(c)
     zn = o.profile("zn")
     st = ini.dry_cbl_state(n, n, nz, zn, seed=seed, ug=ug)
@@ -121,9 +122,10 @@ def cbl_pair(n=64, nz=65, precision=cf.FP64, ug=5.0, fcoriol=1e-4, seed=5):
     return o, m
 
 
+@pytest.mark.parametrize("reproducible", [0, 1], ids=["fma", "exact"])
 @pytest.mark.parametrize("nsteps", [1, 4])
-def test_fused_steps_fp64_match_oracle(gpu_lib, nsteps):
-    o, m = cbl_pair()
+def test_fused_steps_fp64_match_oracle(gpu_lib, nsteps, reproducible):
+    o, m = cbl_pair(reproducible=reproducible)
     o.step(nsteps)
     m.step(nsteps)
     for f in STATE_FIELDS + ["p", "vis", "diff"]:
@@ -133,9 +135,9 @@ def test_fused_steps_fp64_match_oracle(gpu_lib, nsteps):
 
 def test_component_chain_matches_fused(gpu_lib):
     """MONC's group sequence through the per-component entry points equals the fused step."""
-    o, m_fused = cbl_pair(n=32, nz=24)
+    o, m_fused = cbl_pair(n=32, nz=24, reproducible=1)
     del o
-    o2, m_comp = cbl_pair(n=32, nz=24)
+    o2, m_comp = cbl_pair(n=32, nz=24, reproducible=1)
     del o2
     for _ in range(3):
         m_fused.step(1)
@@ -160,3 +162,30 @@ def test_monc_layout_roundtrip(gpu_lib):
     m2 = api.Model(c)
     m2.upload("th", monc, layout=api.LAYOUT_MONC)
     np.testing.assert_array_equal(m2.download("th"), st["th"])
+
+
+def test_tiled_dynamics_bit_identical_to_point_kernel(gpu_lib, monkeypatch):
+    """The shared-memory tiled dynamics kernel evaluates the same expressions as the point kernel."""
+    outs = []
+    for point in ("1", "0"):
+        monkeypatch.setenv("MGPU_POINT_DYNAMICS", point)
+        o, m = cbl_pair(n=64, nz=40, reproducible=1)
+        m.step(3)
+        outs.append({f: m.download(f) for f in STATE_FIELDS})
+        m.close()
+    for f in STATE_FIELDS:
+        np.testing.assert_array_equal(outs[0][f], outs[1][f], err_msg=f)
+
+
+@pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
+def test_fma_variant_close_to_exact(gpu_lib, precision):
+    """The FMA-contracted kernels differ from the separately rounded ones only at rounding level."""
+    res = []
+    for rep in (1, 0):
+        o, m = cbl_pair(n=64, nz=40, precision=precision, reproducible=rep)
+        m.step(4)
+        res.append({f: m.download(f) for f in STATE_FIELDS})
+        m.close()
+    tol = 1e-12 if precision == cf.FP64 else 1e-4
+    for f in STATE_FIELDS:
+        assert rel_err(res[1][f], res[0][f]) <= tol, f
