@@ -136,6 +136,9 @@ def lib():
     L.mgpu_stage_times.restype = C.c_int
     L.mgpu_reference_profile.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
     L.mgpu_reference_profile.restype = C.c_int
+    L.mgpu_poisson_fft_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mgpu_poisson_fft_noalloc.restype = C.c_int
     L.mgpu_last_error.argtypes = [C.c_void_p]
     L.mgpu_last_error.restype = C.c_char_p
     _lib = L

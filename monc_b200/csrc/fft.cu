@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <vector>
 
 #include "dycore.h"
@@ -463,3 +464,142 @@ template void launch_diagnostics<double>(const Scalars&, const double*, const do
 template void launch_diagnostics<float>(const Scalars&, const float*, const float*, double*, double*, cudaStream_t);
 
 }  // namespace mgpu
+
+// =============================================================================================
+// Poisson solve without device allocation.
+//
+// Callers that cannot allocate device memory -- code running while a CUDA graph is being
+// captured, or a host model whose device memory is owned by another allocator and which may not
+// grow the device footprint during a run -- can still solve for the pressure: the caller passes
+// the right-hand side (overwritten with the solution) and the vertical coefficients, and every
+// piece of working storage (spectra, Thomas scratch, pivots, twiddles) lives in the fixed
+// file-scope array below.  That array is part of the library image: every GPU that loads the
+// library holds MGPU_NOALLOC_SCRATCH_BYTES until the process exits.
+// =============================================================================================
+#include <mutex>
+
+#include "../../include/monc_gpu.h"
+
+namespace mgpu {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MGPU_NOALLOC_SCRATCH_BYTES];
+
+// host-side device address of g_noalloc_scratch, looked up once per device
+static void* noalloc_scratch_address(int* status) {
+  static std::mutex mu;
+  static void* addr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { *status = MGPU_ERR_CUDA; return nullptr; }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) { *status = MGPU_ERR_CUDA; return nullptr; }
+    addr[dev] = p;
+  }
+  *status = MGPU_OK;
+  return addr[dev];
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// twiddles e^{-2 pi i q / n}, q < n/2
+__global__ void k_noalloc_twiddles(double2* tw, int n) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n / 2) return;
+  double sv, cv;
+  sincospi(2.0 * (double)q / (double)n, &sv, &cv);
+  tw[q] = make_double2(cv, -sv);
+}
+
+// Thomas pivots per (|ky|, kx), formed as fftsolver.F90:72-90 and :259-280 form them
+__global__ void k_noalloc_pivots(double* b1, const double* __restrict__ prof, int stride, int nx, int ny, int nz,
+                                 double dx, double dy) {
+  const int nxh = nx / 2 + 1, nyh = ny / 2 + 1;
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= nyh * nxh) return;
+  int ky = col / nxh, kx = col - ky * nxh;
+  const double PI = 4.0 * atan(1.0);
+  double cosx = (2.0 / (dx * dx)) * (cos(2.0 * PI * (double)kx / (double)nx) - 1.0);
+  double cosy = (2.0 / (dy * dy)) * (cos(2.0 * PI * (double)ky / (double)ny) - 1.0);
+  double cij = cosx + cosy;
+  const double* cza = prof + P_CZA * stride;
+  const double* czg = prof + P_CZG * stride;
+  const double* czh = prof + P_CZH * stride;
+  double prev = 1.0 / (cij - cza[2]);
+  b1[((size_t)2 * nyh + ky) * nxh + kx] = prev;
+  for (int k = 3; k <= nz; ++k) {
+    double bk = cij + czg[k];
+    prev = 1.0 / (bk - czh[k] * prev);
+    b1[((size_t)k * nyh + ky) * nxh + kx] = prev;
+  }
+}
+
+}  // namespace mgpu
+
+extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32_t nz, double dx, double dy,
+                                        const double* czb, const double* cza, const double* czg, const double* czh,
+                                        void* stream) {
+  using namespace mgpu;
+  auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
+  if (!p || !czb || !cza || !czg || !czh || !pow2(nx) || !pow2(ny) || nz < 4 || nz > MGPU_MAX_NZ || !(dx > 0) ||
+      !(dy > 0))
+    return MGPU_ERR_ARGUMENT;
+  const int nxh = nx / 2 + 1, nyh = ny / 2 + 1;
+  const size_t plane = (size_t)ny * nxh;
+  const int stride = nz + 2;
+  const size_t b_spec = align256(sizeof(double2) * plane * nz);
+  const size_t b_s1 = align256(sizeof(double2) * plane * nz);
+  const size_t b_b1 = align256(sizeof(double) * (size_t)(nz + 1) * nyh * nxh);
+  const size_t b_twx = align256(sizeof(double2) * (nx / 2));
+  const size_t b_twy = align256(sizeof(double2) * (ny / 2));
+  const size_t b_prof = align256(sizeof(double) * (size_t)P_COUNT * stride);
+  const size_t need = b_spec + b_s1 + b_b1 + b_twx + b_twy + b_prof;
+  if (need > (size_t)MGPU_NOALLOC_SCRATCH_BYTES) {
+    std::fprintf(stderr,
+                 "mgpu_poisson_fft_noalloc: a %d x %d x %d grid needs %zu bytes of scratch, more than the "
+                 "%zu-byte maximum\n",
+                 nx, ny, nz, need, (size_t)MGPU_NOALLOC_SCRATCH_BYTES);
+    return MGPU_ERR_ARGUMENT;
+  }
+  int status = MGPU_OK;
+  unsigned char* base = reinterpret_cast<unsigned char*>(noalloc_scratch_address(&status));
+  if (status != MGPU_OK) return status;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  double2* spec = reinterpret_cast<double2*>(base);
+  double2* s1 = reinterpret_cast<double2*>(base + b_spec);
+  double* b1 = reinterpret_cast<double*>(base + b_spec + b_s1);
+  double2* twx = reinterpret_cast<double2*>(base + b_spec + b_s1 + b_b1);
+  double2* twy = reinterpret_cast<double2*>(base + b_spec + b_s1 + b_b1 + b_twx);
+  double* prof = reinterpret_cast<double*>(base + b_spec + b_s1 + b_b1 + b_twx + b_twy);
+  // vertical coefficients: caller arrays hold level k at element k-1; the kernels index level k
+  const double* src[4] = {czb, cza, czg, czh};
+  const int ids[4] = {P_CZB, P_CZA, P_CZG, P_CZH};
+  for (int q = 0; q < 4; ++q)
+    if (cudaMemcpyAsync(prof + (size_t)ids[q] * stride + 1, src[q], sizeof(double) * nz, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+      return MGPU_ERR_CUDA;
+  k_noalloc_twiddles<<<(nx / 2 + 127) / 128, 128, 0, st>>>(twx, nx);
+  k_noalloc_twiddles<<<(ny / 2 + 127) / 128, 128, 0, st>>>(twy, ny);
+  k_noalloc_pivots<<<(nyh * nxh + 127) / 128, 128, 0, st>>>(b1, prof, stride, nx, ny, nz, dx, dy);
+  // the five solve kernels of fft_solve, on the scratch buffers
+  FftPlanDev pl;
+  pl.nx = nx;
+  pl.ny = ny;
+  pl.nz = nz;
+  pl.nxh = nxh;
+  FftSizes z = sizes<double>(pl);
+  if (z.smem_x > 48 * 1024 || z.smem_y > 48 * 1024) {
+    std::fprintf(stderr, "mgpu_poisson_fft_noalloc: rows of %d or %d points exceed the shared-memory tile\n", nx, ny);
+    return MGPU_ERR_ARGUMENT;
+  }
+  const long long npairs = (long long)nz * (ny / 2);
+  const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
+  dim3 gy((nxh + z.cols_y - 1) / z.cols_y, nz);
+  k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x);
+  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nx, ny, z.logy, z.cols_y, false);
+  k_tridiag<double><<<(unsigned)((plane + 127) / 128), 128, 0, st>>>(spec, s1, b1, prof, stride, nx, ny, nz);
+  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nx, ny, z.logy, z.cols_y, true);
+  k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x);
+  return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
+}
