@@ -146,7 +146,10 @@ void mgpu_config_defaults(mgpu_config* cfg);
 
 /* Create a device-resident model: builds the vertical grid and reference state
  * (replaces gridmanager.F90:2008-2075 + simplesetup.F90:60-126 initialisation callbacks)
- * and allocates every field on the current CUDA device. */
+ * and allocates every field on the current CUDA device.
+ * MGPU_ERR_ARGUMENT (checked on the host before any device call): nx, ny even and >= 4; with the
+ * FFT solver nx and ny powers of two <= 4096; 3 <= nz <= MGPU_MAX_NZ; dtm > 0; known precision and
+ * solver.  MGPU_ERR_NO_DEVICE when no CUDA device is visible. */
 int mgpu_create(const mgpu_config* cfg, mgpu_handle** out);
 
 /* Release every device allocation (the finalisation callbacks). */

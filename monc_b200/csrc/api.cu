@@ -164,16 +164,19 @@ extern "C" {
 int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   if (!cfg || !out) return MGPU_ERR_ARGUMENT;
   *out = nullptr;
+  // host-side checks first, so a bad configuration is reported the same with or without a device
+  auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
+  if (cfg->nx < 4 || cfg->ny < 4 || (cfg->nx % 2) || (cfg->ny % 2) || cfg->nz < 3 || cfg->nz > MGPU_MAX_NZ ||
+      cfg->number_q_fields < 0 || cfg->number_q_fields > MGPU_MAX_Q ||
+      (cfg->precision != MGPU_FP64 && cfg->precision != MGPU_FP32_MIXED) ||
+      (cfg->solver != MGPU_SOLVER_FFT && cfg->solver != MGPU_SOLVER_ITERATIVE) ||
+      (cfg->solver == MGPU_SOLVER_FFT && (!pow2(cfg->nx) || !pow2(cfg->ny))) || !(cfg->dtm > 0.0))
+    return MGPU_ERR_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MGPU_ERR_NO_DEVICE;
   mgpu_handle* h = new mgpu_handle();
   h->cfg = *cfg;
   cudaGetDevice(&h->device);
-  if (cfg->number_q_fields < 0 || cfg->number_q_fields > MGPU_MAX_Q || (cfg->nx % 2) || (cfg->ny % 2) ||
-      (cfg->precision != MGPU_FP64 && cfg->precision != MGPU_FP32_MIXED)) {
-    delete h;
-    return MGPU_ERR_ARGUMENT;
-  }
   try {
     build_reference_state(h->cfg, h->rs);
   } catch (std::exception& e) {
