@@ -67,20 +67,33 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+    def __init__(self, device: int, rank: int):
+        import torch
 
-    def start(self):
+        # nvidia-smi numbers GPUs independently of CUDA_VISIBLE_DEVICES: address the device by UUID
+        try:
+            self.gpu = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+        except Exception:
+            self.gpu = str(device)
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+
+    def start(self, wait_s: float = 10.0):
+        """Start sampling every 100 ms and return once the first sample has been written."""
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < wait_s and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -161,7 +174,7 @@ def run_ours(args):
         model.step(3)
         stages = {k: v[0] / max(v[1], 1) for k, v in model.stage_times().items() if v[1] > 0}
         model.set_profiling(False)
-        clocks = ClockSampler(local)
+        clocks = ClockSampler(local, rank)
         barrier()
         if prec_name == "fp64":
             clocks.start()
@@ -335,7 +348,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     args = ap.parse_args()
