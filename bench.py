@@ -258,6 +258,7 @@ def run_ours(args):
                    "l2": "working set (~1.1 GB of fields) larger than the 126 MB L2; no flush needed"},
         "fp32_mixed": {"value": round(results["fp32_mixed"]["value"], 2),
                        "ms_per_step": round(results["fp32_mixed"]["ms_per_step"], 4),
+                       "stages_ms": {k: round(v, 4) for k, v in results["fp32_mixed"]["stages"].items()},
                        "speedup_vs_fp64": round(r64["ms_per_step"] / results["fp32_mixed"]["ms_per_step"], 3)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),

@@ -134,6 +134,11 @@ static void fill_scalars(mgpu_handle* h) {
     const char* e = std::getenv("MGPU_POINT_DYNAMICS");
     s.point_dynamics = (e && e[0] == '1') ? 1 : 0;
   }
+  {
+    const char* e = std::getenv("MGPU_LEVEL_CHUNKS");
+    s.level_chunks = e ? std::atoi(e) : 0;
+    if (s.level_chunks < 0) s.level_chunks = 0;
+  }
   s.passive_th = c.passive_th; s.passive_q = c.passive_q; s.nq = c.number_q_fields;
   s.iqv = 0; s.iql = c.number_q_fields > 1 ? 1 : 0;
   s.coriolis = c.coriolis_enabled; s.surface_bcs = c.use_surface_boundary_conditions;

@@ -45,8 +45,20 @@ template <typename T> __device__ __forceinline__ T sqr(T a) { return a * a; }
 // 1/x rounded to nearest: the same value IEEE division 1.0/x produces, with a shorter sequence
 __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
 __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+// IEEE division (the instruction `x / r` compiles to) written as PTX, so that the compiler cannot
+// fold `c ? x : x / r` into an unconditional x / (c ? 1 : r)
+__device__ __forceinline__ double div_rn(double x, double r) {
+  double q;
+  asm("div.rn.f64 %0, %1, %2;" : "=d"(q) : "d"(x), "d"(r));
+  return q;
+}
+__device__ __forceinline__ float div_rn(float x, float r) {
+  float q;
+  asm("div.rn.f32 %0, %1, %2;" : "=f"(q) : "f"(x), "f"(r));
+  return q;
+}
 // x / r where r is a reference density; Boussinesq runs have r == 1 exactly and x/1 == x
-template <typename T> __device__ __forceinline__ T div_rho(const Scalars& s, T x, T r) { return s.rho_unity ? x : x / r; }
+template <typename T> __device__ __forceinline__ T div_rho(const Scalars& s, T x, T r) { return s.rho_unity ? x : div_rn(x, r); }
 template <typename T> __device__ __forceinline__ T cub(T a) { return a * a * a; }
 
 // ------------------------------------------------------------------------------------------
@@ -123,8 +135,8 @@ __device__ void lower_bc_column(const Scalars& s, const Prof<T>& P, const View<T
 // ------------------------------------------------------------------------------------------
 // smagorinsky (smagorinsky.F90:180-304 setfri + dry Ri, :316-402 moist Ri, :487-696 strain)
 // ------------------------------------------------------------------------------------------
-template <typename T, class A>
-__device__ T half_squared_strain(const Scalars& s, const Prof<T>& P, const A& U, const A& V,
+template <typename T, class A, class PA>
+__device__ T half_squared_strain(const Scalars& s, const PA& P, const A& U, const A& V,
                                  const A& W, int k, int j, int i) {
   const T cx = (T)s.cx, cy = (T)s.cy, cx2 = (T)s.cx2, cy2 = (T)s.cy2;
   const T rdzn1 = P(P_RDZN, k + 1);
@@ -211,8 +223,8 @@ __device__ void smagorinsky_point(const Scalars& s, const Prof<T>& P, const View
 // ------------------------------------------------------------------------------------------
 // pw_advection advect_flow_fields (pwadvection.F90:466-610): assigned sources, 2<=k<=nz
 // ------------------------------------------------------------------------------------------
-template <typename T, class A>
-__device__ void pw_point(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+template <typename T, class A, class PA>
+__device__ void pw_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                          int k, int j, int i, T& su, T& sv, T& sw) {
   const T tcx = (T)s.tcx, tcy = (T)s.tcy;
   const T u0 = U(k, j, i), v0 = V(k, j, i);
@@ -253,8 +265,8 @@ struct Tau13 {
   T t13, t13m1, t23, t23m1;
 };
 
-template <typename T, class A>
-__device__ Tau13<T> tau_13_23(const Scalars& s, const Prof<T>& P, const A& ZU, const A& ZV,
+template <typename T, class A, class PA>
+__device__ Tau13<T> tau_13_23(const Scalars& s, const PA& P, const A& ZU, const A& ZV,
                               const A& ZW, const A& VIS, int k, int j, int i) {
   Tau13<T> t;
   if (k >= s.nz) { t.t13 = t.t13m1 = t.t23 = t.t23m1 = (T)0.0; return t; }
@@ -278,15 +290,15 @@ __device__ Tau13<T> tau_13_23(const Scalars& s, const Prof<T>& P, const A& ZU, c
   return t;
 }
 
-template <typename T, class A>
-__device__ T tau33_at(const Scalars& s, const Prof<T>& P, const A& ZW, const A& VIS, int k, int j, int i) {
+template <typename T, class A, class PA>
+__device__ T tau33_at(const Scalars& s, const PA& P, const A& ZW, const A& VIS, int k, int j, int i) {
   if (k <= 1) return (T)0.0;
   T visonp2 = P(P_RHON, k) * (VIS(k, j, i) + VIS(k - 1, j, i));
   return visonp2 * (ZW(k, j, i) - ZW(k - 1, j, i)) * P(P_RDZ, k);
 }
 
-template <typename T, class A>
-__device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const A& ZU, const A& ZV,
+template <typename T, class A, class PA>
+__device__ void viscosity_point(const Scalars& s, const PA& P, const A& ZU, const A& ZV,
                                 const A& ZW, const A& ZU_state, const A& VIS, int k, int j, int i,
                                 T& du, T& dv, T& dw) {
   const T cx = (T)s.cx, cy = (T)s.cy, rhon = P(P_RHON, k);
@@ -328,8 +340,8 @@ __device__ void viscosity_point(const Scalars& s, const Prof<T>& P, const A& ZU,
 // ------------------------------------------------------------------------------------------
 // coriolis (coriolis.F90:243-258), buoyancy (buoyancy.F90:229-262)
 // ------------------------------------------------------------------------------------------
-template <typename T, class A>
-__device__ void coriolis_point(const Scalars& s, const Prof<T>& P, const A& U, const A& V, int k, int j,
+template <typename T, class A, class PA>
+__device__ void coriolis_point(const Scalars& s, const PA& P, const A& U, const A& V, int k, int j,
                                int i, T& su, T& sv) {
   const T f = (T)s.fcoriol;
   su = su + f * ((T)0.25 * (V(k, j, i) + V(k, j, i + 1) + V(k, j - 1, i) + V(k, j - 1, i + 1)) + (T)s.vgal - P(P_GWY, k));
@@ -369,9 +381,9 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
 }
 
 // face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx
-template <typename T, class A>
-__device__ T tvd_face_x(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
-                        const A& ZF, T dt, int k, int j, int i) {
+template <typename T, class A, class AF, class PA>
+__device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                        const AF& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const int kp1 = k + 1 < nz ? k + 1 : nz;
@@ -424,9 +436,9 @@ __device__ T tvd_face_x(const Scalars& s, const Prof<T>& P, const A& U, const A&
 }
 
 // face y+1/2 of cell (k, j, i): flux_y(k) of ultflx
-template <typename T, class A>
-__device__ T tvd_face_y(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
-                        const A& ZF, T dt, int k, int j, int i) {
+template <typename T, class A, class AF, class PA>
+__device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                        const AF& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const int kp1 = k + 1 < nz ? k + 1 : nz;
@@ -465,9 +477,9 @@ __device__ T tvd_face_y(const Scalars& s, const Prof<T>& P, const A& U, const A&
 }
 
 // flux_z(k+1): face above level k (2 <= k <= nz-1); the top routine handles k = nz-1
-template <typename T, class A>
-__device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
-                        const A& ZF, T dt, int k, int j, int i) {
+template <typename T, class A, class AF, class PA>
+__device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                        const AF& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const T w0 = W(k, j, i);
@@ -567,8 +579,8 @@ __device__ T tvd_face_z(const Scalars& s, const Prof<T>& P, const A& U, const A&
 // TVD source of cell (k, j, i), 2 <= k <= nz, from the six face values
 // acc0 is the source value before the callback (MONC accumulates into it below the top level
 // and zeroes it at the top level)
-template <typename T, class A>
-__device__ T tvd_source(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+template <typename T, class A, class PA>
+__device__ T tvd_source(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                         T fx_m, T fx_p, T fy_m, T fy_p, T fz_m, T fz_p, int k, int j, int i, T acc0) {
   const T cx = (T)s.cx, cy = (T)s.cy;
   T acc = (k < s.nz) ? acc0 : (T)0.0;
@@ -584,8 +596,8 @@ __device__ T tvd_source(const Scalars& s, const Prof<T>& P, const A& U, const A&
   return acc;
 }
 
-template <typename T, class A>
-__device__ T tvd_point(const Scalars& s, const Prof<T>& P, const A& U, const A& V, const A& W,
+template <typename T, class A, class PA>
+__device__ T tvd_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                        const A& ZF, int k, int j, int i, T acc0) {
   const T dt = (T)(s.dtm * 2.0);
   T fxm = tvd_face_x<T, A>(s, P, U, V, W, ZF, dt, k, j, i - 1);
@@ -600,8 +612,8 @@ __device__ T tvd_point(const Scalars& s, const Prof<T>& P, const A& U, const A& 
 // ------------------------------------------------------------------------------------------
 // diffusion general_diffusion (diffusion.F90:501-545), 2 <= k <= nz
 // ------------------------------------------------------------------------------------------
-template <typename T, class A>
-__device__ T diffusion_point(const Scalars& s, const Prof<T>& P, const A& F, const A& D, int k, int j, int i) {
+template <typename T, class AF, class AD, class PA>
+__device__ T diffusion_point(const Scalars& s, const PA& P, const AF& F, const AD& D, int k, int j, int i) {
   const T f0 = F(k, j, i), d0 = D(k, j, i), dm = D(k - 1, j, i);
   T term = (T)s.cx2 * (T)0.25 *
                (((d0 + D(k, j, i - 1)) + (dm + D(k - 1, j, i - 1))) * (F(k, j, i - 1) - f0) -

@@ -483,127 +483,189 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
   for (int n = 0; n < s.nq; ++n) step_scalar(d.q[n], d.zq[n], sq[n], d.q_n[n], d.zq_n[n], true);
 }
 
-// 2'. Centred-step dynamics, shared-memory tiled.  A CTA owns a TX x TY tile of columns and
-//     marches up the levels.  The planes each level needs (with a 2-point periodic halo) sit in
-//     per-field ring buffers in shared memory, filled one level ahead with cp.async; every TVD
-//     face flux is computed once (x and y faces exchanged through shared memory, the z face
-//     carried in a register from the level below).  Arithmetic is the same device code as the
-//     point kernel, so the results are bit-identical to it.
+// 2'. Centred-step dynamics, shared-memory tiled, as two kernels that each march up the levels
+//     of a TX x TY tile of columns:
+//       k_f_momentum_tiled : pw_advection + viscosity + coriolis + buoyancy + stepfields of u, v, w
+//       k_f_scalar_tiled   : tvd_advection + diffusion + stepfields + swap_smooth pre-smoothing of th
+//     The planes each level needs (with a periodic halo of 2 points in y and one 16-byte chunk
+//     in x) sit in per-field ring buffers in shared memory, filled one level ahead with 16-byte
+//     cp.async copies whose source offsets each thread computes once.  Every TVD face flux is
+//     computed once: x and y faces go through shared memory, the z face is carried in a
+//     register from the level below.  The arithmetic is the device code the point kernel
+//     runs, so the results are bit-identical to it.
 namespace tiled {
-constexpr int TX = 32, TY = 8, H = 2;
-constexpr int PW = TX + 2 * H, PH = TY + 2 * H, PLANE = PW * PH;
-constexpr int RZF = 8, R3 = 4;  // ring slots: zth (levels k-1..k+3), other fields (k-1..k+2)
-enum Slot { S_ZF = 0, S_U = S_ZF + RZF, S_V = S_U + R3, S_W = S_V + R3, S_ZU = S_W + R3, S_ZV = S_ZU + R3,
-            S_ZW = S_ZV + R3, S_VIS = S_ZW + R3, S_DIFF = S_VIS + R3, S_TOTAL = S_DIFF + R3 };
+constexpr int TX = 32, TY = 8, HY = 2, NT = TX * TY;
 template <typename T>
-constexpr size_t smem_bytes() {
-  return sizeof(T) * ((size_t)S_TOTAL * PLANE + (size_t)TY * (TX + 1) + (size_t)(TY + 1) * TX);
+struct G {
+  static constexpr int V = 16 / (int)sizeof(T);  // elements per 16-byte chunk = x halo width
+  static constexpr int PW = TX + 2 * V, PH = TY + 2 * HY, PLANE = PW * PH;
+  static constexpr int CPR = PW / V;   // chunks per plane row
+  static constexpr int NCH = CPR * PH;  // chunks per plane (<= NT)
+  static_assert(NCH <= NT, "one chunk per thread and plane");
+  static_assert((PLANE * sizeof(T)) % 16 == 0, "planes start on 16-byte boundaries");
+};
+constexpr int RM = 4;              // momentum rings: levels k-1..k+1 live, k+2 in flight
+constexpr int RF = 4, RZF = 8;     // scalar kernel: u, v, w and diff rings; the scalar's ring (k-1..k+3)
+constexpr int RP = 8;              // profile ring: levels k-1..k+2 live, k+3 staged
+// resident CTAs per SM the register budget is sized for (FP64: 2 x 256 threads x <= 128 registers)
+template <typename T>
+constexpr int min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
+constexpr int M_PLANES = 7 * RM;   // u v w zu zv zw vis
+constexpr int S_PLANES = 4 * RF + RZF;  // u v w diff + scalar
+template <typename T>
+constexpr size_t momentum_smem() { return sizeof(T) * ((size_t)M_PLANES * G<T>::PLANE + (size_t)RP * P_COUNT); }
+template <typename T>
+constexpr size_t scalar_smem() {
+  return sizeof(T) * ((size_t)S_PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
+                      (size_t)(TY + 1) * TX);
 }
 }  // namespace tiled
 
+// Centred ring view: the thread's own point at levels kc-1 .. kc+2 through four slot pointers.
+// Every access the device functions make at k +- const, j +- const, i +- const folds to one
+// shared-memory load with an immediate offset; data-dependent levels select among the four.
 template <typename T>
-struct SView {
-  const T* base;
-  int jb, ib;  // global (unwrapped) coordinates of local element (0, 0)
-  int rmask;   // ring slots - 1 (a power of two)
+struct CRing {
+  const T* pm;
+  const T* p0;
+  const T* p1;
+  const T* p2;
+  int kc, jc, ic;
+  __device__ __forceinline__ const T* lvl(int dk) const { return dk <= -1 ? pm : (dk == 0 ? p0 : (dk == 1 ? p1 : p2)); }
   __device__ __forceinline__ T operator()(int k, int j, int i) const {
-    return base[((k & rmask) * tiled::PH + (j - jb)) * tiled::PW + (i - ib)];
+    return lvl(k - kc)[(j - jc) * tiled::G<T>::PW + (i - ic)];
   }
 };
 
-__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, int bytes) {
+// profile values of levels kc-1 .. kc+2, staged per level in shared memory (P_COUNT per level)
+template <typename T>
+struct CProf {
+  const T* pm;
+  const T* p0;
+  const T* p1;
+  const T* p2;
+  int kc;
+  __device__ __forceinline__ T operator()(int id, int k) const {
+    const int dk = k - kc;
+    return (dk <= -1 ? pm : (dk == 0 ? p0 : (dk == 1 ? p1 : p2)))[id];
+  }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// copy level k of a field (tile + halo, periodic) into ring slot `slot` of that field's planes
+// One thread's share of staging a plane: a single 16-byte chunk.  The x halo is one whole
+// chunk on each side and nx is a multiple of the chunk, so no chunk straddles the periodic wrap.
 template <typename T>
-__device__ __forceinline__ void stage_plane(T* ring, int rmask, const T* __restrict__ f, const Scalars& s, int k, int j0,
-                                            int i0, int tid) {
-  using namespace tiled;
-  T* dst = ring + (k & rmask) * PLANE;
-  const T* src = f + (long long)(k - 1) * s.plane;
-  for (int e = tid; e < PLANE; e += TX * TY) {
-    int jj = e / PW, ii = e - jj * PW;
-    int gj = j0 - H + jj, gi = i0 - H + ii;
+struct Stager {
+  int soff;       // element offset of the chunk inside a plane
+  long long goff; // element offset of the chunk inside a global level
+  bool on;
+  __device__ void init(const Scalars& s, int j0, int i0, int tid) {
+    using Gt = tiled::G<T>;
+    on = tid < Gt::NCH;
+    const int c = on ? tid : 0;
+    const int row = c / Gt::CPR, cc = c - row * Gt::CPR;
+    soff = row * Gt::PW + cc * Gt::V;
+    int gj = j0 - tiled::HY + row, gi = i0 - Gt::V + cc * Gt::V;
     gj = gj < 0 ? gj + s.ny : (gj >= s.ny ? gj - s.ny : gj);
     gi = gi < 0 ? gi + s.nx : (gi >= s.nx ? gi - s.nx : gi);
-    cp_async_elem(dst + e, src + (long long)gj * s.nx + gi, (int)sizeof(T));
+    goff = (long long)gj * s.nx + gi;
   }
+  // copy level k of field f into slot (k mod R) of the ring at `ring`
+  template <int R>
+  __device__ __forceinline__ void stage(T* ring, const T* __restrict__ f, long long plane, int k) const {
+    if (on) cp_async16(ring + (k & (R - 1)) * tiled::G<T>::PLANE + soff, f + (long long)(k - 1) * plane + goff);
+  }
+};
+
+// profile ring: RP levels x P_COUNT values, converted to the compute type when staged
+template <typename T>
+__device__ __forceinline__ T load_profile(const Scalars& s, int id, int k) {
+  return (T)__ldg(s.prof + id * (s.nz + 2) + k);
+}
+template <typename T>
+__device__ __forceinline__ CProf<T> cprof(const T* ring, int k) {
+  using namespace tiled;
+  return CProf<T>{ring + ((k - 1) & (RP - 1)) * P_COUNT, ring + (k & (RP - 1)) * P_COUNT,
+                  ring + ((k + 1) & (RP - 1)) * P_COUNT, ring + ((k + 2) & (RP - 1)) * P_COUNT, k};
+}
+// the four centred slot pointers of a ring of R planes for level k at plane offset `co`
+template <typename T, int R>
+__device__ __forceinline__ CRing<T> cring(const T* ring, int k, int co, int j, int i) {
+  using Gt = tiled::G<T>;
+  return CRing<T>{ring + ((k - 1) & (R - 1)) * Gt::PLANE + co, ring + (k & (R - 1)) * Gt::PLANE + co,
+                  ring + ((k + 1) & (R - 1)) * Gt::PLANE + co, ring + ((k + 2) & (R - 1)) * Gt::PLANE + co, k, j, i};
 }
 
+// Each CTA runs the levels kb..ke of its tile, kb = 2 + blockIdx.z * kchunk: splitting the level
+// range gives enough CTAs to fill every SM on grids with few tiles.
 template <typename T>
-__global__ void __launch_bounds__(tiled::TX* tiled::TY, 1) k_f_dynamics_tiled(Scalars s, DevState<T> d) {
+__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_tiled(Scalars s, DevState<T> d,
+                                                                                      int kchunk) {
   using namespace tiled;
+  using Gt = G<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
-  T* FX = sm + (size_t)S_TOTAL * PLANE;  // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
-  T* FY = FX + TY * (TX + 1);            // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
-  const bool inside = (i < s.nx) && (j < s.ny);
   const int nz = s.nz;
-  Prof<T> P = prof<T>(s);
-  const int jb = j0 - H, ib = i0 - H;
-  const SView<T> ZF{sm + S_ZF * PLANE, jb, ib, RZF - 1};
-  const SView<T> U{sm + S_U * PLANE, jb, ib, R3 - 1}, V{sm + S_V * PLANE, jb, ib, R3 - 1}, W{sm + S_W * PLANE, jb, ib, R3 - 1};
-  const SView<T> ZU{sm + S_ZU * PLANE, jb, ib, R3 - 1}, ZV{sm + S_ZV * PLANE, jb, ib, R3 - 1},
-      ZW{sm + S_ZW * PLANE, jb, ib, R3 - 1};
-  const SView<T> VIS{sm + S_VIS * PLANE, jb, ib, R3 - 1}, DIFF{sm + S_DIFF * PLANE, jb, ib, R3 - 1};
-  // prologue: planes for level 2 (zth 1..4, others 1..3, diff 1..2)
-  for (int kk = 1; kk <= 4 && kk <= nz; ++kk) stage_plane<T>(sm + S_ZF * PLANE, RZF - 1, d.zth, s, kk, j0, i0, tid);
-  for (int kk = 1; kk <= 3 && kk <= nz; ++kk) {
-    stage_plane<T>(sm + S_U * PLANE, R3 - 1, d.u, s, kk, j0, i0, tid);
-    stage_plane<T>(sm + S_V * PLANE, R3 - 1, d.v, s, kk, j0, i0, tid);
-    stage_plane<T>(sm + S_W * PLANE, R3 - 1, d.w, s, kk, j0, i0, tid);
-    stage_plane<T>(sm + S_ZU * PLANE, R3 - 1, d.zu, s, kk, j0, i0, tid);
-    stage_plane<T>(sm + S_ZV * PLANE, R3 - 1, d.zv, s, kk, j0, i0, tid);
-    stage_plane<T>(sm + S_ZW * PLANE, R3 - 1, d.zw, s, kk, j0, i0, tid);
-    stage_plane<T>(sm + S_VIS * PLANE, R3 - 1, d.vis, s, kk, j0, i0, tid);
-  }
-  for (int kk = 1; kk <= 2; ++kk) stage_plane<T>(sm + S_DIFF * PLANE, R3 - 1, d.diff, s, kk, j0, i0, tid);
-  // level 1: sources are zero there (stepfields zeroes them)
+  const int kb = 2 + (int)blockIdx.z * kchunk;
+  const int ke = min(nz, kb + kchunk - 1);
+  const long long plane = s.plane;
+  constexpr int FS = RM * Gt::PLANE;  // field stride inside the shared ring block
+  T* rU = sm;
+  T* rV = rU + FS;
+  T* rW = rV + FS;
+  T* rZU = rW + FS;
+  T* rZV = rZU + FS;
+  T* rZW = rZV + FS;
+  T* rVIS = rZW + FS;
+  T* rP = rVIS + FS;  // profile ring
+  const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  Stager<T> sg;
+  sg.init(s, j0, i0, tid);
+  auto stage_level = [&](int kk) {
+    sg.template stage<RM>(rU, d.u, plane, kk);
+    sg.template stage<RM>(rV, d.v, plane, kk);
+    sg.template stage<RM>(rW, d.w, plane, kk);
+    sg.template stage<RM>(rZU, d.zu, plane, kk);
+    sg.template stage<RM>(rZV, d.zv, plane, kk);
+    sg.template stage<RM>(rZW, d.zw, plane, kk);
+    sg.template stage<RM>(rVIS, d.vis, plane, kk);
+  };
+  // level k reads levels k-1 .. k+1 of every ring and profiles k-1 .. k+2
+  for (int kk = kb - 1; kk <= kb + 1 && kk <= nz; ++kk) stage_level(kk);
+  if (tid < P_COUNT)
+    for (int kk = kb - 1; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
   const T dtm_x2 = (T)(2.0 * s.dtm);
-  const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
-  if (inside) {
-    long long o = lin(s, 1, j, i);
+  if (kb == 2) {
+    // level 1: the sources are zero there (stepfields zeroes them)
+    const long long o = lin(s, 1, j, i);
     d.zu_n[o] = (T)s.ugal + d.zu[o] + dtm_x2 * (T)0.0;
     d.zv_n[o] = (T)s.vgal + d.zv[o] + dtm_x2 * (T)0.0;
     d.zw_n[o] = (T)0.0 + d.zw[o] + dtm_x2 * (T)0.0;
-    T fv = d.th[o], zv = d.zth[o];
-    T sm1 = c1 * fv + c2 * zv;
-    T zn = (T)0.0 + zv + dtm_x2 * (T)0.0;
-    d.zth_n[o] = sm1 + (T)s.tsmth * zn;
-    d.th_n[o] = zn;
   }
+  const T* __restrict__ th = d.th;
+  T th_hi = th[lin(s, kb, j, i)];
   cp_async_wait_all();
   __syncthreads();
-  const T dt = (T)(s.dtm * 2.0);
-  T fz_lo = (T)0.0;  // flux_z(2) = 0
-  View<T> THg = view<T>(d.th, s);
-  for (int k = 2; k <= nz; ++k) {
-    // prefetch the planes level k+1 will add
-    if (k + 3 <= nz) stage_plane<T>(sm + S_ZF * PLANE, RZF - 1, d.zth, s, k + 3, j0, i0, tid);
-    if (k + 2 <= nz) {
-      stage_plane<T>(sm + S_U * PLANE, R3 - 1, d.u, s, k + 2, j0, i0, tid);
-      stage_plane<T>(sm + S_V * PLANE, R3 - 1, d.v, s, k + 2, j0, i0, tid);
-      stage_plane<T>(sm + S_W * PLANE, R3 - 1, d.w, s, k + 2, j0, i0, tid);
-      stage_plane<T>(sm + S_ZU * PLANE, R3 - 1, d.zu, s, k + 2, j0, i0, tid);
-      stage_plane<T>(sm + S_ZV * PLANE, R3 - 1, d.zv, s, k + 2, j0, i0, tid);
-      stage_plane<T>(sm + S_ZW * PLANE, R3 - 1, d.zw, s, k + 2, j0, i0, tid);
-      stage_plane<T>(sm + S_VIS * PLANE, R3 - 1, d.vis, s, k + 2, j0, i0, tid);
-    }
-    if (k + 1 <= nz) stage_plane<T>(sm + S_DIFF * PLANE, R3 - 1, d.diff, s, k + 1, j0, i0, tid);
-    // TVD faces of this level: own x+1/2 and y+1/2 faces, then the tile's low-side faces
-    FX[ty * (TX + 1) + tx + 1] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i);
-    FY[(ty + 1) * TX + tx] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j, i);
-    if (tid < TX) FY[tid] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j0 - 1, i0 + tid);
-    else if (tid < TX + TY) FX[(tid - TX) * (TX + 1)] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1);
-    T fz_hi = (k < nz) ? tvd_face_z<T>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
-    // momentum sources: pw (assigns), viscosity, coriolis, buoyancy
+  for (int k = kb; k <= ke; ++k) {
+    if (k + 2 <= min(nz, ke + 1)) stage_level(k + 2);
+    const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
+    T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
+    const long long o = lin(s, k, j, i);
+    const T th_lo = th_hi;
+    if (k < nz) th_hi = __ldg(th + o + plane);
+    const CProf<T> P = cprof<T>(rP, k);
+    const CRing<T> U = cring<T, RM>(rU, k, co, j, i), V = cring<T, RM>(rV, k, co, j, i),
+                   W = cring<T, RM>(rW, k, co, j, i);
+    const CRing<T> ZU = cring<T, RM>(rZU, k, co, j, i), ZV = cring<T, RM>(rZV, k, co, j, i),
+                   ZW = cring<T, RM>(rZW, k, co, j, i), VIS = cring<T, RM>(rVIS, k, co, j, i);
     T su, sv, sw;
     pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
     if (s.use_vd) {
@@ -614,23 +676,112 @@ __global__ void __launch_bounds__(tiled::TX* tiled::TY, 1) k_f_dynamics_tiled(Sc
       if (k < nz) sw = sw + dw;
     }
     if (s.coriolis) coriolis_point<T>(s, P, U, V, k, j, i, su, sv);
-    if (k < nz && !s.passive_th && inside) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (THg(k, j, i) + THg(k + 1, j, i));
+    if (k < nz && !s.passive_th) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (th_lo + th_hi);
+    d.zu_n[o] = (T)s.ugal + ZU(k, j, i) + dtm_x2 * su;
+    d.zv_n[o] = (T)s.vgal + ZV(k, j, i) + dtm_x2 * sv;
+    d.zw_n[o] = (T)0.0 + ZW(k, j, i) + dtm_x2 * sw;
+    if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_tiled(Scalars s, DevState<T> d,
+                                                                                    int kchunk) {
+  using namespace tiled;
+  using Gt = G<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int nz = s.nz;
+  const int kb = 2 + (int)blockIdx.z * kchunk;
+  const int ke = min(nz, kb + kchunk - 1);
+  const long long plane = s.plane;
+  constexpr int FS = RF * Gt::PLANE;
+  T* rU = sm;
+  T* rV = rU + FS;
+  T* rW = rV + FS;
+  T* rD = rW + FS;
+  T* rF = rD + FS;
+  T* rP = rF + RZF * Gt::PLANE;  // profile ring
+  T* FX = rP + RP * P_COUNT;     // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
+  T* FY = FX + TY * (TX + 1);    // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
+  const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  Stager<T> sg;
+  sg.init(s, j0, i0, tid);
+  // level k reads the scalar at k-1 .. k+2, u v w at k-1 .. k+1, diff at k-1 .. k and profiles
+  // at k-1 .. k+2; a chunk above level 2 also needs the z face below it (level kb-1).
+  const int k0 = kb == 2 ? 1 : kb - 2;
+  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<RZF>(rF, d.zth, plane, kk);
+  for (int kk = k0; kk <= kb + 1 && kk <= nz; ++kk) {
+    sg.template stage<RF>(rU, d.u, plane, kk);
+    sg.template stage<RF>(rV, d.v, plane, kk);
+    sg.template stage<RF>(rW, d.w, plane, kk);
+  }
+  for (int kk = kb - 1; kk <= kb; ++kk) sg.template stage<RF>(rD, d.diff, plane, kk);
+  if (tid < P_COUNT)
+    for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
+  const T dtm_x2 = (T)(2.0 * s.dtm);
+  const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
+  const T* __restrict__ th = d.th;
+  if (kb == 2) {
+    // level 1: zero source
+    const long long o = lin(s, 1, j, i);
+    T fv = th[o], zv = d.zth[o];
+    T sm1 = c1 * fv + c2 * zv;
+    T zn = (T)0.0 + zv + dtm_x2 * (T)0.0;
+    d.zth_n[o] = sm1 + (T)s.tsmth * zn;
+    d.th_n[o] = zn;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const T dt = (T)(s.dtm * 2.0);
+  T fz_lo = (T)0.0;  // flux_z(2) = 0
+  if (kb > 2) {
+    const int kz = kb - 1;
+    const CProf<T> P = cprof<T>(rP, kz);
+    const CRing<T> U = cring<T, RF>(rU, kz, co, j, i), V = cring<T, RF>(rV, kz, co, j, i),
+                   W = cring<T, RF>(rW, kz, co, j, i);
+    const CRing<T> ZF = cring<T, RZF>(rF, kz, co, j, i);
+    fz_lo = tvd_face_z<T>(s, P, U, V, W, ZF, dt, kz, j, i);
+    __syncthreads();  // level kb-2 of the u, v, w rings is overwritten by the first prefetch
+  }
+  for (int k = kb; k <= ke; ++k) {
+    if (k + 3 <= min(nz, ke + 2)) sg.template stage<RZF>(rF, d.zth, plane, k + 3);
+    if (k + 2 <= min(nz, ke + 1)) {
+      sg.template stage<RF>(rU, d.u, plane, k + 2);
+      sg.template stage<RF>(rV, d.v, plane, k + 2);
+      sg.template stage<RF>(rW, d.w, plane, k + 2);
+    }
+    if (k + 1 <= min(nz, ke)) sg.template stage<RF>(rD, d.diff, plane, k + 1);
+    const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
+    T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
+    const long long o = lin(s, k, j, i);
+    const T fv = __ldg(th + o);
+    const CProf<T> P = cprof<T>(rP, k);
+    const CRing<T> U = cring<T, RF>(rU, k, co, j, i), V = cring<T, RF>(rV, k, co, j, i),
+                   W = cring<T, RF>(rW, k, co, j, i), DIFF = cring<T, RF>(rD, k, co, j, i);
+    const CRing<T> ZF = cring<T, RZF>(rF, k, co, j, i);
+    // TVD faces of this level: own x+1/2 and y+1/2 faces, then the tile's low-side faces
+    FX[ty * (TX + 1) + tx + 1] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i);
+    FY[(ty + 1) * TX + tx] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j, i);
+    if (tid < TX) FY[tid] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j0 - 1, i0 + tid);
+    else if (tid < TX + TY) FX[(tid - TX) * (TX + 1)] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1);
+    T fz_hi = (k < nz) ? tvd_face_z<T>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
     __syncthreads();
     T sth = tvd_source<T>(s, P, U, V, W, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1], FY[ty * TX + tx],
                           FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
     if (s.use_vd) sth = sth + diffusion_point<T>(s, P, ZF, DIFF, k, j, i);
     fz_lo = fz_hi;
-    if (inside) {
-      long long o = lin(s, k, j, i);
-      d.zu_n[o] = (T)s.ugal + ZU(k, j, i) + dtm_x2 * su;
-      d.zv_n[o] = (T)s.vgal + ZV(k, j, i) + dtm_x2 * sv;
-      d.zw_n[o] = (T)0.0 + ZW(k, j, i) + dtm_x2 * sw;
-      T fv = THg(k, j, i), zv = ZF(k, j, i);
-      T smo = c1 * fv + c2 * zv;
-      T zn = (T)0.0 + zv + dtm_x2 * sth;
-      d.zth_n[o] = smo + (T)s.tsmth * zn;
-      d.th_n[o] = zn;
-    }
+    T zv = ZF(k, j, i);
+    T smo = c1 * fv + c2 * zv;
+    T zn = (T)0.0 + zv + dtm_x2 * sth;
+    d.zth_n[o] = smo + (T)s.tsmth * zn;
+    d.th_n[o] = zn;
+    if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
     cp_async_wait_all();
     __syncthreads();
   }
@@ -759,23 +910,55 @@ template <typename T>
 void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st) {
   k_f_subgrid<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
 }
+// Number of level chunks for a grid of `tiles` tiles: the count (chunks of at least 8 levels) whose
+// CTAs fill the resident slots most evenly; each extra chunk costs a few staged levels.
+static inline int choose_level_chunks(int tiles, int slots, int levels) {
+  int best = 1;
+  double best_score = -1.0;
+  for (int n = 1; n <= 16 && levels / n >= 8; ++n) {
+    const long long ctas = (long long)tiles * n;
+    const long long waves = (ctas + slots - 1) / slots;
+    const double score = (double)ctas / (double)(waves * slots) - 0.01 * n;
+    if (score > best_score + 1e-9) { best_score = score; best = n; }
+  }
+  return best;
+}
+
 template <typename T>
 void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
-  // the tiled kernel covers centred dry steps; the first (forward) step and moist runs use the
+  // the tiled kernels cover centred dry steps; the first (forward) step and moist runs use the
   // point kernel
-  const bool tiled_ok = !s.forward && !s.point_dynamics && s.nq == 0 && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 && s.nz >= 4;
+  const bool tiled_ok = !s.forward && !s.point_dynamics && s.nq == 0 && (s.nx % tiled::TX) == 0 &&
+                        (s.ny % tiled::TY) == 0 && s.nz >= 4;
   if (!tiled_ok) {
     k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
     return;
   }
-  const size_t smem = tiled::smem_bytes<T>();
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_f_dynamics_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
+  const size_t sm_m = tiled::momentum_smem<T>(), sm_s = tiled::scalar_smem<T>();
+  static int occ_m = 0, occ_s = 0, nsm = 0;
+  if (!nsm) {
+    cudaFuncSetAttribute(k_f_momentum_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_m);
+    cudaFuncSetAttribute(k_f_scalar_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_s);
+    cudaFuncSetAttribute(k_f_momentum_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_f_scalar_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_f_momentum_tiled<T>, tiled::NT, sm_m);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_f_scalar_tiled<T>, tiled::NT, sm_s);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (occ_m < 1) occ_m = 1;
+    if (occ_s < 1) occ_s = 1;
+    if (nsm < 1) nsm = 1;
   }
-  dim3 grid(s.nx / tiled::TX, s.ny / tiled::TY, 1), block(tiled::TX, tiled::TY, 1);
-  k_f_dynamics_tiled<T><<<grid, block, smem, st>>>(s, d);
+  const int tiles = (s.nx / tiled::TX) * (s.ny / tiled::TY), levels = s.nz - 1;
+  const int nc_s = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ_s * nsm, levels);
+  const int nc_m = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ_m * nsm, levels);
+  const int kc_s = (levels + nc_s - 1) / nc_s, kc_m = (levels + nc_m - 1) / nc_m;
+  dim3 block(tiled::TX, tiled::TY, 1);
+  dim3 grid_s(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_s - 1) / kc_s);
+  dim3 grid_m(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_m - 1) / kc_m);
+  k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s);
+  k_f_momentum_tiled<T><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
 }
 template <typename T>
 void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st) {

@@ -56,6 +56,8 @@ struct Scalars {
   int lookup_entries;
   int forward;  // 1 on the first (forward) step
   int point_dynamics;  // 1: always use the untiled dynamics kernel (MGPU_POINT_DYNAMICS=1)
+  int level_chunks;    // level chunks of the tiled dynamics kernels; 0 = chosen from the occupancy
+                       // (MGPU_LEVEL_CHUNKS=n fixes it)
   int rho_unity;       // 1 when rho = rhon = 1 on every level (Boussinesq with rhobous = 1)
   int passive_th, passive_q, nq, iqv, iql;
   int coriolis, surface_bcs, use_vd;

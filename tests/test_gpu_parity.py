@@ -164,17 +164,22 @@ def test_monc_layout_roundtrip(gpu_lib):
     np.testing.assert_array_equal(m2.download("th"), st["th"])
 
 
-def test_tiled_dynamics_bit_identical_to_point_kernel(gpu_lib, monkeypatch):
-    """The shared-memory tiled dynamics kernel evaluates the same expressions as the point kernel."""
+@pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
+def test_tiled_dynamics_bit_identical_to_point_kernel(gpu_lib, monkeypatch, precision):
+    """The shared-memory tiled dynamics kernels evaluate the same expressions as the point kernel,
+    for any split of the levels into chunks (auto, whole column, 3, 5 and 20 chunks of 39 levels;
+    the last split ends in a one-level chunk)."""
     outs = []
-    for point in ("1", "0"):
+    for point, chunks in (("1", "0"), ("0", "0"), ("0", "1"), ("0", "3"), ("0", "5"), ("0", "20")):
         monkeypatch.setenv("MGPU_POINT_DYNAMICS", point)
-        o, m = cbl_pair(n=64, nz=40, reproducible=1)
+        monkeypatch.setenv("MGPU_LEVEL_CHUNKS", chunks)
+        o, m = cbl_pair(n=64, nz=40, precision=precision, reproducible=1)
         m.step(3)
         outs.append({f: m.download(f) for f in STATE_FIELDS})
         m.close()
-    for f in STATE_FIELDS:
-        np.testing.assert_array_equal(outs[0][f], outs[1][f], err_msg=f)
+    for n, res in enumerate(outs[1:], 1):
+        for f in STATE_FIELDS:
+            np.testing.assert_array_equal(outs[0][f], res[f], err_msg=f"{f} (setting {n})")
 
 
 @pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
