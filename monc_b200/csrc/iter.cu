@@ -1,20 +1,569 @@
-// BiCGStab pressure solve (iterativesolver.F90): not yet available on this path.
+// Iterative pressure solve: preconditioned BiCGStab on MONC's 7-point Poisson operator
+// (iterativesolver.F90:140-248 bicgstab, :329-380 precond, :400-493 calc_Ax, :500-553 inner
+// products, :559-602 set_matrix_for_poisson).
+//
+// One BiCGStab iteration is five kernels over the resident work arrays:
+//   k_bicg_direction  : t = r - bet*omg*v; s = M^-1 t; pp = s + bet*pp   (pp = M^-1 r on it 1)
+//   k_bicg_apply_dot  : v = A pp,  nrm = <cr, v>, alf = rho / nrm
+//   k_bicg_half_step  : s = r - alf*v,  cs = M^-1 s
+//   k_bicg_apply_dots : t = A cs,  tt, ts, ss,  omg = ts / tt,  err
+//   k_bicg_update     : x += alf*pp + omg*cs,  r = s - omg*t,  rho = <r, cr>,  convergence
+// M^-1 is MONC's column LU solve of the vertical part (preconditioner_iterations = 0).  Dot
+// products accumulate in FP64 whatever the work precision: warp shuffles, one partial per block,
+// and the last block to finish sums the partials in a fixed order (deterministic) and updates the
+// solver scalars, which stay in device memory.  Every kernel returns at once when the solve has
+// converged, so the host launches iterations in batches and reads the state back once a batch.
+//
+// The FP32-mixed model solves in FP64 by iterative refinement: r = b - A x in FP64, an FP32
+// BiCGStab solve of A e = r, x += e, until the FP64 residual meets the tolerance.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
 #include "dycore.h"
 
 namespace mgpu {
 
-struct IterSolverDev {
-  int dummy;
+struct IterScalars {
+  double rho, rho_prev, nrm, alf, omg, err, sc_err, tol, shift;
+  int it, done, it_done, pad;
+  unsigned int counter;
 };
 
-IterSolverDev* iter_create(const Scalars&, const RefState&, const mgpu_config&, bool, int* status) {
-  *status = MGPU_ERR_UNSUPPORTED;
-  return nullptr;
+namespace {
+
+constexpr int BX = 32, BY = 8, NTH = BX * BY;
+constexpr int NCOEF = 6;  // A_u, A_d, A_p, lu_d, lu_u, vol = rhon*dz, each nz+2 long (1-based)
+
+struct Geom {
+  int nx, ny, nz;
+  long long plane;
+  double A_n, A_e;
+  const double* coef;  // [NCOEF][nz+2]
+  __device__ __forceinline__ double au(int k) const { return coef[k]; }
+  __device__ __forceinline__ double ad(int k) const { return coef[(nz + 2) + k]; }
+  __device__ __forceinline__ double ap(int k) const { return coef[2 * (nz + 2) + k]; }
+  __device__ __forceinline__ double lud(int k) const { return coef[3 * (nz + 2) + k]; }
+  __device__ __forceinline__ double luu(int k) const { return coef[4 * (nz + 2) + k]; }
+  __device__ __forceinline__ double vol(int k) const { return coef[5 * (nz + 2) + k]; }
+  __device__ __forceinline__ long long at(int k, int j, int i) const { return (long long)(k - 1) * plane + (long long)j * nx + i; }
+};
+
+template <int NV>
+__device__ __forceinline__ void block_partials(double (&v)[NV], double* partials, int nblocks, int bid) {
+  __shared__ double sh[NV][NTH / 32];
+  const int tid = threadIdx.y * BX + threadIdx.x, lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q)
+    for (int off = 16; off; off >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], off);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sh[q][wid] = v[q];
+  __syncthreads();
+  if (tid == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double a = 0.0;
+      for (int w = 0; w < NTH / 32; ++w) a += sh[q][w];
+      partials[(long long)q * nblocks + bid] = a;
+    }
 }
-void iter_destroy(IterSolverDev* it) { delete it; }
+
+// True in thread 0 of the last block to finish; `out` then holds the sums over all blocks.
+template <int NV>
+__device__ bool last_block_sums(IterScalars* st, const double* partials, int nblocks, double (&out)[NV]) {
+  __shared__ bool am_last;
+  __shared__ double sh[NV][NTH / 32];
+  const int tid = threadIdx.y * BX + threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) am_last = atomicAdd(&st->counter, 1u) == (unsigned)nblocks - 1u;
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double v[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double a = 0.0;
+    for (int b = tid; b < nblocks; b += NTH) a += __ldcg(partials + (long long)q * nblocks + b);
+    v[q] = a;
+  }
+#pragma unroll
+  for (int q = 0; q < NV; ++q)
+    for (int off = 16; off; off >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], off);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sh[q][wid] = v[q];
+  __syncthreads();
+  if (tid != 0) return false;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double a = 0.0;
+    for (int w = 0; w < NTH / 32; ++w) a += sh[q][w];
+    out[q] = a;
+  }
+  st->counter = 0u;
+  return true;
+}
+
+// (A x)(k, j, i) for 2 <= k <= nz (calc_Ax, non-symmetric form used by BiCGStab)
+template <typename W>
+__device__ __forceinline__ W apply_A(const Geom& g, const W* __restrict__ x, int k, int j, int i) {
+  const int ie = i + 1 == g.nx ? 0 : i + 1, iw = i == 0 ? g.nx - 1 : i - 1;
+  const int jn = j + 1 == g.ny ? 0 : j + 1, js = j == 0 ? g.ny - 1 : j - 1;
+  const long long o = g.at(k, j, i);
+  const W xc = x[o];
+  W h = (W)g.A_n * (x[g.at(k, j, ie)] + x[g.at(k, j, iw)]) + (W)g.A_e * (x[g.at(k, jn, i)] + x[g.at(k, js, i)]);
+  if (k == 2) return h + (W)g.au(k) * x[o + g.plane] + (W)g.ap(k) * xc;
+  if (k < g.nz) return h + (W)g.au(k) * x[o + g.plane] + (W)g.ad(k) * x[o - g.plane] + (W)g.ap(k) * xc;
+  return h + (W)g.ad(k) * x[o - g.plane] + (W)g.ap(k) * xc;
+}
+
+__device__ __forceinline__ int block_id() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+
+// r = b - A x, cr = r; sums <r, r> and <b, b>; initial scalars
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_bicg_init(Geom g, const W* __restrict__ x, const W* __restrict__ b, W* r, W* cr,
+                                                    double* partials, int nblocks, IterScalars* st, double sc_floor) {
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double v[2] = {0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W rv = b[o] - apply_A<W>(g, x, k, j, i);
+    r[o] = rv;
+    cr[o] = rv;
+    v[0] = (double)rv * (double)rv;
+    v[1] = (double)b[o] * (double)b[o];
+  }
+  block_partials<2>(v, partials, nblocks, block_id());
+  double s[2];
+  if (last_block_sums<2>(st, partials, nblocks, s)) {
+    st->sc_err = fmax(sqrt(s[1]), sc_floor);
+    st->rho = s[0];
+    st->rho_prev = 1.0;
+    st->nrm = 1.0;
+    st->alf = 1.0;
+    st->omg = 1.0;
+    st->err = sqrt(s[0]) / st->sc_err;
+    st->it = 1;
+    st->it_done = 0;
+    st->done = st->err < st->tol ? 1 : 0;
+  }
+}
+
+// column LU solve of the vertical operator: out = M^-1 in (precond); `tmp` holds the forward sweep
+template <typename W, class In>
+__device__ __forceinline__ void column_precond(const Geom& g, In in, W* tmp, int j, int i) {
+  long long o = g.at(2, j, i);
+  W sp = in(o) * (W)g.lud(2);
+  tmp[o] = sp;
+  for (int k = 3; k <= g.nz; ++k) {
+    o += g.plane;
+    sp = (in(o) - (W)g.ad(k) * sp) * (W)g.lud(k);
+    tmp[o] = sp;
+  }
+}
+
+// iteration step 1: search direction pp
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_bicg_direction(Geom g, const W* __restrict__ r, const W* __restrict__ v, W* pp,
+                                                         W* tmp, const IterScalars* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const bool first = st->it == 1;
+  const double bet_d = (st->rho / st->rho_prev) * (st->alf / st->omg);
+  const W bet = (W)bet_d, bo = (W)(bet_d * st->omg);
+  if (first) column_precond<W>(g, [&](long long o) { return r[o]; }, tmp, j, i);
+  else column_precond<W>(g, [&](long long o) { return r[o] - bo * v[o]; }, tmp, j, i);
+  // back substitution, then pp = s + bet*pp
+  long long o = g.at(g.nz, j, i);
+  W sk = tmp[o];
+  pp[o] = first ? sk : sk + bet * pp[o];
+  for (int k = g.nz - 1; k >= 2; --k) {
+    o -= g.plane;
+    sk = tmp[o] - (W)g.luu(k) * sk;
+    pp[o] = first ? sk : sk + bet * pp[o];
+  }
+}
+
+// iteration step 2: v = A pp, alf = rho / <cr, v>
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_bicg_apply_dot(Geom g, const W* __restrict__ pp, const W* __restrict__ cr, W* v,
+                                                         double* partials, int nblocks, IterScalars* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double a[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W vv = apply_A<W>(g, pp, k, j, i);
+    v[o] = vv;
+    a[0] = (double)cr[o] * (double)vv;
+  }
+  block_partials<1>(a, partials, nblocks, block_id());
+  double s[1];
+  if (last_block_sums<1>(st, partials, nblocks, s)) {
+    st->nrm = s[0];
+    st->alf = st->rho / s[0];
+  }
+}
+
+// iteration step 3: s = r - alf*v, cs = M^-1 s
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_bicg_half_step(Geom g, const W* __restrict__ r, const W* __restrict__ v, W* s_,
+                                                         W* cs, W* tmp, const IterScalars* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const W alf = (W)st->alf;
+  column_precond<W>(g, [&](long long o) {
+    const W sv = r[o] - alf * v[o];
+    s_[o] = sv;
+    return sv;
+  }, tmp, j, i);
+  long long o = g.at(g.nz, j, i);
+  W ck = tmp[o];
+  cs[o] = ck;
+  for (int k = g.nz - 1; k >= 2; --k) {
+    o -= g.plane;
+    ck = tmp[o] - (W)g.luu(k) * ck;
+    cs[o] = ck;
+  }
+}
+
+// iteration step 4: t = A cs; tt, ts, ss; omg, err
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_bicg_apply_dots(Geom g, const W* __restrict__ cs, const W* __restrict__ s_, W* t,
+                                                          double* partials, int nblocks, IterScalars* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double a[3] = {0.0, 0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W tv = apply_A<W>(g, cs, k, j, i);
+    t[o] = tv;
+    const double td = (double)tv, sd = (double)s_[o];
+    a[0] = td * td;
+    a[1] = td * sd;
+    a[2] = sd * sd;
+  }
+  block_partials<3>(a, partials, nblocks, block_id());
+  double s[3];
+  if (last_block_sums<3>(st, partials, nblocks, s)) {
+    const double omg = s[1] / s[0];
+    st->omg = omg;
+    st->err = sqrt(s[2] - 2 * omg * s[1] + omg * omg * s[0]) / st->sc_err;
+  }
+}
+
+// iteration step 5: x += alf*pp + omg*cs, r = s - omg*t, rho = <r, cr>, convergence test
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __restrict__ pp, const W* __restrict__ cs,
+                                                      const W* __restrict__ s_, const W* __restrict__ t, W* r,
+                                                      const W* __restrict__ cr, double* partials, int nblocks,
+                                                      IterScalars* st, int max_it) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double a[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W alf = (W)st->alf, omg = (W)st->omg;
+    x[o] = x[o] + alf * pp[o] + omg * cs[o];
+    const W rv = s_[o] - omg * t[o];
+    r[o] = rv;
+    a[0] = (double)rv * (double)cr[o];
+  }
+  block_partials<1>(a, partials, nblocks, block_id());
+  double s[1];
+  if (last_block_sums<1>(st, partials, nblocks, s)) {
+    st->rho_prev = st->rho;
+    st->rho = s[0];
+    st->it_done = st->it;
+    st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
+    st->it += 1;
+  }
+}
+
+// FP64 residual of the refinement: r = b - A x (levels 2..nz) with <r, r>, <b, b>
+__global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* __restrict__ x, const double* __restrict__ b,
+                                                          double* r, float* r32, double* partials, int nblocks,
+                                                          IterScalars* st) {
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double v[2] = {0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const double rv = b[o] - apply_A<double>(g, x, k, j, i);
+    r[o] = rv;
+    r32[o] = (float)rv;
+    v[0] = rv * rv;
+    v[1] = b[o] * b[o];
+  }
+  block_partials<2>(v, partials, nblocks, block_id());
+  double s[2];
+  if (last_block_sums<2>(st, partials, nblocks, s)) {
+    st->sc_err = fmax(sqrt(s[1]), 0.0001);
+    st->rho = s[0];
+    st->err = sqrt(s[0]) / st->sc_err;
+    st->done = st->err < st->tol ? 1 : 0;
+  }
+}
+
+// The horizontal-mean problem is singular: sum_k rhon(k) dz(k) sum_ij (A x)(k, j, i) = 0 for any x.
+// A right-hand side rounded to FP32 carries an incompatible part of that size, which an FP32
+// solve cannot remove; the refinement takes it out of b first (a constant shift of levels 2..nz).
+__global__ void __launch_bounds__(NTH) k_compat_sum(Geom g, const double* __restrict__ b, double* partials, int nblocks,
+                                                     IterScalars* st) {
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double v[1] = {0.0};
+  if (i < g.nx && j < g.ny) v[0] = g.vol(k) * b[g.at(k, j, i)];
+  block_partials<1>(v, partials, nblocks, block_id());
+  double s[1];
+  if (last_block_sums<1>(st, partials, nblocks, s)) {
+    double w = 0.0;
+    for (int kk = 2; kk <= g.nz; ++kk) w += g.vol(kk);
+    st->shift = s[0] / (w * (double)g.nx * (double)g.ny);
+  }
+}
+__global__ void k_compat_shift(Geom g, double* b, const IterScalars* st) {
+  const double c = st->shift;
+  const long long n = (long long)g.nz * g.plane;
+  for (long long q = g.plane + blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = b[q] - c;
+}
+
+template <typename A, typename B>
+__global__ void k_convert_levels(const A* __restrict__ a, B* b, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = (B)a[q];
+}
+__global__ void k_add_correction(double* x, const float* __restrict__ e, long long plane, long long n, double sign) {
+  for (long long q = plane + blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    x[q] = x[q] + sign * (double)e[q];
+}
+
+template <typename W>
+struct Work {
+  W *x, *b, *r, *cr, *pp, *v, *t, *s, *cs, *tmp;
+};
+
+}  // namespace
+
+struct IterSolverDev {
+  Geom g;
+  bool fp32 = false;
+  int max_it = 0;
+  double tol = 0.0;
+  double* coef = nullptr;
+  double* partials = nullptr;
+  int nblocks = 0;
+  IterScalars* st = nullptr;
+  IterScalars* st_host = nullptr;
+  Work<double> w64{};
+  Work<float> w32{};
+  double* r64 = nullptr;  // refinement residual (FP32-mixed model)
+  std::vector<void*> allocs;
+  dim3 grid_pt, grid_col, block;
+};
+
+static int dev_alloc(IterSolverDev* it, void** p, size_t bytes) {
+  if (cudaMalloc(p, bytes) != cudaSuccess) return MGPU_ERR_CUDA;
+  cudaMemset(*p, 0, bytes);
+  it->allocs.push_back(*p);
+  return MGPU_OK;
+}
+
+IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status) {
+  *status = MGPU_OK;
+  if (cfg.solver_type != MGPU_ITER_BICGSTAB) {
+    std::fprintf(stderr, "iterative solver: only BiCGStab is available\n");
+    *status = MGPU_ERR_UNSUPPORTED;
+    return nullptr;
+  }
+  auto* it = new IterSolverDev();
+  const int nz = s.nz;
+  it->fp32 = fp32;
+  it->max_it = cfg.max_iterations > 0 ? cfg.max_iterations : 1;
+  it->tol = cfg.tolerance;
+  // set_matrix_for_poisson (iterativesolver.F90:559-602), BiCGStab form (A_vol = 1)
+  const double A_n = rs.cx * rs.cx, A_e = rs.cy * rs.cy;
+  const double concat = A_n + A_n + A_e + A_e;
+  std::vector<double> c((size_t)NCOEF * (nz + 2), 0.0);
+  double* Au = c.data();
+  double* Ad = Au + (nz + 2);
+  double* Ap = Ad + (nz + 2);
+  double* lud = Ap + (nz + 2);
+  double* luu = lud + (nz + 2);
+  double* vol = luu + (nz + 2);
+  for (int k = 2; k <= nz; ++k) vol[k] = rs.rhon[k] * rs.dz[k];
+  for (int k = 2; k <= nz; ++k) {
+    const double d_sc = rs.rdz[k] / rs.rhon[k];
+    Au[k] = (k == nz) ? 0.0 : rs.rho[k] * rs.rdzn[k + 1];
+    Ad[k] = (k == 2) ? 0.0 : rs.rho[k - 1] * rs.rdzn[k];
+    Ap[k] = d_sc * (-(Au[k] + Ad[k])) - concat * 1.0;
+    Au[k] = d_sc * Au[k];
+    Ad[k] = d_sc * Ad[k];
+  }
+  lud[2] = 1.0 / Ap[2];
+  luu[2] = lud[2] * Au[2];
+  for (int k = 3; k <= nz; ++k) {
+    lud[k] = 1.0 / (Ap[k] - Ad[k] * luu[k - 1]);
+    luu[k] = Au[k] * lud[k];
+  }
+  auto fail = [&](int code) {
+    iter_destroy(it);
+    *status = code;
+    return (IterSolverDev*)nullptr;
+  };
+  if (dev_alloc(it, (void**)&it->coef, c.size() * sizeof(double))) return fail(MGPU_ERR_CUDA);
+  cudaMemcpy(it->coef, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice);
+  it->g = Geom{s.nx, s.ny, nz, s.plane, A_n, A_e, it->coef};
+  it->block = dim3(BX, BY, 1);
+  it->grid_col = dim3((s.nx + BX - 1) / BX, (s.ny + BY - 1) / BY, 1);
+  it->grid_pt = dim3(it->grid_col.x, it->grid_col.y, nz - 1);
+  it->nblocks = (int)(it->grid_pt.x * it->grid_pt.y * it->grid_pt.z);
+  if (dev_alloc(it, (void**)&it->partials, sizeof(double) * 3 * (size_t)it->nblocks)) return fail(MGPU_ERR_CUDA);
+  if (dev_alloc(it, (void**)&it->st, sizeof(IterScalars))) return fail(MGPU_ERR_CUDA);
+  if (cudaMallocHost((void**)&it->st_host, sizeof(IterScalars)) != cudaSuccess) return fail(MGPU_ERR_CUDA);
+  const size_t n = (size_t)nz * s.plane;
+  // FP64 arrays: the solve itself (FP64 model) or the refinement's x, b, r (FP32-mixed model)
+  double** f64[] = {&it->w64.x, &it->w64.b, &it->w64.r, &it->w64.cr, &it->w64.pp, &it->w64.v,
+                    &it->w64.t, &it->w64.s, &it->w64.cs, &it->w64.tmp};
+  const int n64 = fp32 ? 2 : 10;
+  for (int q = 0; q < n64; ++q)
+    if (dev_alloc(it, (void**)f64[q], n * sizeof(double))) return fail(MGPU_ERR_CUDA);
+  if (fp32) {
+    if (dev_alloc(it, (void**)&it->r64, n * sizeof(double))) return fail(MGPU_ERR_CUDA);
+    float** f32[] = {&it->w32.x, &it->w32.b, &it->w32.r, &it->w32.cr, &it->w32.pp, &it->w32.v,
+                     &it->w32.t, &it->w32.s, &it->w32.cs, &it->w32.tmp};
+    for (float** pp : f32)
+      if (dev_alloc(it, (void**)pp, n * sizeof(float))) return fail(MGPU_ERR_CUDA);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(MGPU_ERR_CUDA);
+  return it;
+}
+
+void iter_destroy(IterSolverDev* it) {
+  if (!it) return;
+  for (void* p : it->allocs) cudaFree(p);
+  if (it->st_host) cudaFreeHost(it->st_host);
+  delete it;
+}
+
+// BiCGStab on work arrays w (x is the initial guess and the result); returns the iterations done
+template <typename W>
+static int run_bicgstab(IterSolverDev* it, Work<W>& w, double tol, double sc_floor, cudaStream_t st, int64_t* launches,
+                        int* iterations, double* residual) {
+  IterScalars init{};
+  init.tol = tol;
+  it->st_host[0] = init;
+  if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return MGPU_ERR_CUDA;
+  const Geom& g = it->g;
+  k_bicg_init<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, w.cr, it->partials, it->nblocks, it->st, sc_floor);
+  *launches += 1;
+  constexpr int BATCH = 4;
+  for (int done = 0; done < it->max_it;) {
+    // the first batch checks convergence of the initial guess after one iteration's launches
+    for (int q = 0; q < BATCH; ++q) {
+      k_bicg_direction<W><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.pp, w.tmp, it->st);
+      k_bicg_apply_dot<W><<<it->grid_pt, it->block, 0, st>>>(g, w.pp, w.cr, w.v, it->partials, it->nblocks, it->st);
+      k_bicg_half_step<W><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.s, w.cs, w.tmp, it->st);
+      k_bicg_apply_dots<W><<<it->grid_pt, it->block, 0, st>>>(g, w.cs, w.s, w.t, it->partials, it->nblocks, it->st);
+      k_bicg_update<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.pp, w.cs, w.s, w.t, w.r, w.cr, it->partials,
+                                                          it->nblocks, it->st, it->max_it);
+      *launches += 5;
+    }
+    done += BATCH;
+    if (cudaMemcpyAsync(it->st_host, it->st, sizeof(IterScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MGPU_ERR_CUDA;
+    if (it->st_host->done) break;
+  }
+  if (cudaGetLastError() != cudaSuccess) return MGPU_ERR_CUDA;
+  *iterations = it->st_host->it_done;
+  *residual = it->st_host->err;
+  return it->st_host->err < tol ? MGPU_OK : MGPU_ERR_NOT_CONVERGED;
+}
+
+static int solve_fp64(IterSolverDev* it, const Scalars& s, double* p, cudaStream_t st, int64_t* launches,
+                      int* iterations, double* residual) {
+  if (!it || it->fp32) return MGPU_ERR_ARGUMENT;
+  // psource = p; the initial guess is the previous solution (iterativesolver.F90:95-106)
+  const size_t bytes = (size_t)s.nz * s.plane * sizeof(double);
+  if (cudaMemcpyAsync(it->w64.b, p, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
+  int rc = run_bicgstab<double>(it, it->w64, it->tol, 0.0001, st, launches, iterations, residual);
+  if (rc != MGPU_OK && rc != MGPU_ERR_NOT_CONVERGED) return rc;
+  // p = x, level 1 included (the solution keeps the previous solve's level 1)
+  if (cudaMemcpyAsync(p, it->w64.x, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
+  return rc;
+}
+
+static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream_t st, int64_t* launches,
+                       int* iterations, double* residual) {
+  if (!it || !it->fp32) return MGPU_ERR_ARGUMENT;
+  const long long n = (long long)s.nz * s.plane;
+  const Geom& g = it->g;
+  double* x64 = it->w64.x;
+  double* b64 = it->w64.b;
+  k_convert_levels<float, double><<<592, 256, 0, st>>>(p, b64, n);
+  {
+    IterScalars init{};
+    it->st_host[0] = init;
+    if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+  }
+  k_compat_sum<<<it->grid_pt, it->block, 0, st>>>(g, b64, it->partials, it->nblocks, it->st);
+  k_compat_shift<<<592, 256, 0, st>>>(g, b64, it->st);
+  *launches += 3;
+  int total = 0;
+  double err = 0.0, prev_err = 0.0;
+  constexpr int MAX_REFINE = 8;
+  int rc = MGPU_ERR_NOT_CONVERGED;
+  for (int outer = 0; outer < MAX_REFINE; ++outer) {
+    IterScalars init{};
+    init.tol = it->tol;
+    it->st_host[0] = init;
+    if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+    k_refine_residual<<<it->grid_pt, it->block, 0, st>>>(g, x64, b64, it->r64, it->w32.b, it->partials, it->nblocks,
+                                                        it->st);
+    *launches += 1;
+    if (cudaMemcpyAsync(it->st_host, it->st, sizeof(IterScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MGPU_ERR_CUDA;
+    err = it->st_host->err;
+    if (it->st_host->done) { rc = MGPU_OK; break; }
+    if (outer > 0 && !(err < prev_err)) {
+      // the last correction did not reduce the FP64 residual: take it back and stop
+      k_add_correction<<<592, 256, 0, st>>>(x64, it->w32.x, s.plane, n, -1.0);
+      *launches += 1;
+      err = prev_err;
+      break;
+    }
+    prev_err = err;
+    // FP32 correction solve A e = r, from e = 0, to a relative residual of 1e-5
+    if (cudaMemsetAsync(it->w32.x, 0, (size_t)n * sizeof(float), st) != cudaSuccess) return MGPU_ERR_CUDA;
+    int its = 0;
+    double inner = 0.0;
+    int irc = run_bicgstab<float>(it, it->w32, 1e-5, 1e-300, st, launches, &its, &inner);
+    if (irc != MGPU_OK && irc != MGPU_ERR_NOT_CONVERGED) return irc;
+    total += its;
+    k_add_correction<<<592, 256, 0, st>>>(x64, it->w32.x, s.plane, n, 1.0);
+    *launches += 1;
+  }
+  k_convert_levels<double, float><<<592, 256, 0, st>>>(x64, p, n);
+  *launches += 1;
+  if (cudaGetLastError() != cudaSuccess) return MGPU_ERR_CUDA;
+  *iterations = total;
+  *residual = err;
+  return rc;
+}
+
 template <typename T>
-int iter_solve(IterSolverDev*, const Scalars&, T*, cudaStream_t, int64_t*, int*, double*) {
-  return MGPU_ERR_UNSUPPORTED;
+int iter_solve(IterSolverDev* it, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, int* iterations,
+               double* residual) {
+  if constexpr (sizeof(T) == 8) return solve_fp64(it, s, p, st, launches, iterations, residual);
+  else return solve_mixed(it, s, p, st, launches, iterations, residual);
 }
 template int iter_solve<double>(IterSolverDev*, const Scalars&, double*, cudaStream_t, int64_t*, int*, double*);
 template int iter_solve<float>(IterSolverDev*, const Scalars&, float*, cudaStream_t, int64_t*, int*, double*);
