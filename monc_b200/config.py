@@ -160,6 +160,23 @@ def dry_cbl_config(nx: int, ny: int, nz: int, dx: float, dz: float, dtm: float,
     return c
 
 
+def moist_config(nx: int, ny: int, z, dx: float, dtm: float, shf_wm2: float = 0.0, lhf_wm2: float = 0.0,
+                 thref0: float = 289.0, cs: float = 0.23, max_height_cloud: float = 20000.0,
+                 n_tracers: int = 0, precision: int = FP64, solver: int = SOLVER_FFT) -> MgpuConfig:
+    """Moist layer on explicit w-levels z: q fields vapour (0) and liquid (1), plus n_tracers
+    passive q fields, saturation adjustment by simplecloud, moist Richardson number in the
+    Smagorinsky closure, surface fluxes in W m-2 (setfluxlook.F90:84-92)."""
+    c = dry_cbl_config(nx, ny, len(z), dx, 1.0, dtm, cs=cs, thref0=thref0, precision=precision, solver=solver)
+    set_explicit_levels(c, z)
+    c.passive_q = 0
+    c.number_q_fields = 2 + n_tracers
+    c.simplecloud_enabled = 1
+    c.max_height_cloud = max_height_cloud
+    c.surface_sensible_heat_flux = shf_wm2
+    c.surface_latent_heat_flux = lhf_wm2
+    return c
+
+
 def stretched_levels(nz: int, dz_bottom: float, dz_top: float, ztop: float | None = None):
     """w-level heights with spacing growing geometrically from dz_bottom to dz_top.
 

@@ -127,7 +127,9 @@ static void fill_scalars(mgpu_handle* h) {
   s.eps = 0.01; s.repsh = 0.5 / 0.01;
   s.thcona = c.ratio_mol_wts * c.thref0; s.thconb = s.thcona - c.thref0; s.thconap1 = s.thcona;
   s.rlvap_over_cp = r.rlvap_over_cp; s.G = c.G;
-  s.cq0 = r.cq.empty() ? 0.0 : r.cq[0];
+  for (int n = 0; n < MGPU_MAX_Q; ++n) s.cq[n] = n < (int)r.cq.size() ? r.cq[n] : 0.0;
+  s.simplecloud = c.simplecloud_enabled;
+  s.k_cloudmax = r.k_cloudmax;
   s.lookup_entries = r.lookup_entries;
   s.forward = 1;
   {
@@ -159,7 +161,7 @@ static const std::vector<double>* prof_vec(const RefState& r, int id) {
     case P_BUOY_CO: return &r.buoy_co; case P_THREF: return &r.thref; case P_PREFRCP: return &r.prefrcp;
     case P_RPREFRCP: return &r.rprefrcp; case P_TREF: return &r.tref; case P_TSTARPR: return &r.tstarpr;
     case P_QSAT: return &r.qsat; case P_DQSATDT: return &r.dqsatdt; case P_QSATFAC: return &r.qsatfac;
-    case P_GWX: return &r.gwx; case P_GWY: return &r.gwy;
+    case P_GWX: return &r.gwx; case P_GWY: return &r.gwy; case P_PREFN: return &r.prefn;
   }
   return nullptr;
 }

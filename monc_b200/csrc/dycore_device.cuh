@@ -354,9 +354,58 @@ __device__ T buoyancy_point(const Scalars& s, const Prof<T>& P, const View<T>& T
   if (!s.passive_th) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (TH(k, j, i) + TH(k + 1, j, i));
   if (!s.passive_q) {
     const T g2 = (T)(0.5 * s.G);
-    for (int n = 0; n < s.nq; ++n) sw = sw + g2 * (T)(n == 0 ? s.cq0 : 0.0) * (Q[n](k, j, i) + Q[n](k + 1, j, i));
+    for (int n = 0; n < s.nq; ++n) sw = sw + g2 * (T)s.cq[n] * (Q[n](k, j, i) + Q[n](k + 1, j, i));
   }
   return sw;
+}
+
+// ------------------------------------------------------------------------------------------
+// simplecloud saturation adjustment (simplecloud.F90:262-379, saturation.F90 qsaturation and
+// dqwsatdt), one point 2 <= k <= nz.  q_v, q_l, th are the state (forward step) or z-fields;
+// zq_l is always the z-field (the evaporation branch tests scalar_stepping, which is centred).
+// Above k_cloudmax the Fortran reuses one_over_exner from the last adjusted level.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T qsaturation(T temperature, T pressure) {
+  const T tk0c = (T)273.15, qsa1 = (T)3.8, qsa2 = (T)-17.2693882, qsa3 = (T)35.86, qsa4 = (T)6.109;
+  return qsa1 / (pressure * exp(qsa2 * (temperature - tk0c) / (temperature - qsa3)) - qsa4);
+}
+template <typename T>
+__device__ __forceinline__ T dqwsatdt(T qs, T temperature) {
+  const T tk0c = (T)273.15, qsa1 = (T)3.8, qsa2 = (T)-17.2693882, qsa3 = (T)35.86, qsa4 = (T)6.109;
+  return -qsa2 * (tk0c - qsa3) * ((T)1.0 + qsa4 * qs / qsa1) * qs * pow(temperature - qsa3, (T)-2.0);
+}
+
+template <typename T, class PA>
+__device__ void simplecloud_point(const Scalars& s, const PA& P, int k, T q_v, T q_l, T th, T zq_l, T& sth, T& sqv,
+                                  T& sql) {
+  const T dtm = s.forward ? (T)s.dtm : (T)(s.dtm * 2.0);
+  const T rl = (T)s.rlvap_over_cp;
+  if (k <= s.k_cloudmax) {
+    const T exner = P(P_RPREFRCP, k), one_over_exner = P(P_PREFRCP, k);
+    const T Pmb = P(P_PREFN, k) / (T)100.;
+    const T qv = q_v + sqv * dtm;
+    const T qc = q_l + sql * dtm;
+    const T tk = (th + sth * dtm + P(P_THREF, k)) * exner;
+    const T qs = qsaturation<T>(tk, Pmb);
+    if (qv > qs || qc > (T)0.0) {
+      const T dqsdT = dqwsatdt<T>(qs, tk);
+      const T qsatfac = (T)1.0 / ((T)1.0 + rl * dqsdT);
+      const T dmass = tmax<T>(-qc, (qv - qs) * qsatfac) / dtm;
+      sqv = sqv - dmass;
+      sql = sql + dmass;
+      sth = sth + rl * dmass * one_over_exner;
+    }
+  } else {
+    const T one_over_exner = s.k_cloudmax >= 2 ? P(P_PREFRCP, s.k_cloudmax) : (T)0.0;
+    const T qc = zq_l + sql * dtm;
+    if (qc > (T)0.0) {
+      const T dmass = -qc / dtm;
+      sqv = sqv - dmass;
+      sql = sql + dmass;
+      sth = sth + rl * dmass * one_over_exner;
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -218,6 +218,25 @@ __global__ void k_c_set_consistent_lowbc(Scalars s, DevState<T> d) {
   for (int n = 0; n < s.nq; ++n) d.sq[n][o1] = d.sq[n][o2];
 }
 
+// simplecloud: saturation adjustment of sth, sq(vapour), sq(liquid), levels 2..nz
+template <typename T>
+__global__ void k_c_simplecloud(Scalars s, DevState<T> d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z + 2;
+  if (i >= s.nx || j >= s.ny || k > s.nz) return;
+  Prof<T> P = prof<T>(s);
+  const long long o = lin(s, k, j, i);
+  const bool fwd = s.forward;
+  const int iv = s.iqv, il = s.iql;
+  T sth = d.sth[o], sqv = d.sq[iv][o], sql = d.sq[il][o];
+  simplecloud_point<T>(s, P, k, (fwd ? d.q[iv] : d.zq[iv])[o], (fwd ? d.q[il] : d.zq[il])[o], (fwd ? d.th : d.zth)[o],
+                       d.zq[il][o], sth, sqv, sql);
+  d.sth[o] = sth;
+  d.sq[iv][o] = sqv;
+  d.sq[il][o] = sql;
+}
+
 // diverr: p from the divergence of the (z-)velocities; |p| max into *divmax (bit pattern)
 template <typename T>
 __global__ void k_c_diverr(Scalars s, DevState<T> d, unsigned long long* divmax) {
@@ -445,6 +464,11 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
     for (int n = 0; n < s.nq; ++n) {
       sq[n] = tvd_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.q[n] : d.zq[n], s), k, j, i, (T)0.0);
       if (s.use_vd) sq[n] = sq[n] + diffusion_point<T, View<T>>(s, P, view<T>(d.zq[n], s), view<T>(d.diff, s), k, j, i);
+    }
+    if (s.simplecloud) {
+      const int iv = s.iqv, il = s.iql;
+      simplecloud_point<T>(s, P, k, (fwd ? d.q[iv] : d.zq[iv])[o], (fwd ? d.q[il] : d.zq[il])[o], (fwd ? d.th : d.zth)[o],
+                           d.zq[il][o], sth, sq[iv], sq[il]);
     }
   }
   // stepfields (source at level 1 is zeroed there) and, for scalars, swap_smooth
@@ -887,6 +911,10 @@ int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st,
     case MGPU_C_CORIOLIS: k_c_coriolis<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
     case MGPU_C_BUOYANCY: k_c_buoyancy<T><<<pt_grid(s, s.nz - 2), b, 0, st>>>(s, d); break;
     case MGPU_C_SET_CONSISTENT_LOWBC: k_c_set_consistent_lowbc<T><<<gcol, b, 0, st>>>(s, d); break;
+    case MGPU_C_SIMPLECLOUD:
+      if (!s.simplecloud) return MGPU_ERR_UNSUPPORTED;
+      k_c_simplecloud<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d);
+      break;
     case MGPU_C_DIVERR: k_c_diverr<T><<<pt_grid(s, s.nz), b, 0, st>>>(s, d, divmax); break;
     case MGPU_C_PSRCE: k_c_psrce<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
     case MGPU_C_STEPFIELDS: k_c_stepfields<T><<<pt_grid(s, s.nz), b, 0, st>>>(s, d); break;

@@ -216,6 +216,15 @@ void build_reference_state(const mgpu_config& c, RefState& rs) {
   // water loading coefficient of the vapour field (setfluxlook.F90:70-76)
   rs.cq.assign(std::max(c.number_q_fields, 1), 0.0);
   if (!c.passive_q && c.number_q_fields > 0) rs.cq[0] = c.ratio_mol_wts - 1.0;
+  if (c.simplecloud_enabled) {
+    // simplecloud.F90:230-248
+    if (c.number_q_fields < 2) throw std::runtime_error("simplecloud needs the vapour and liquid q fields");
+    rs.cq[1] = -1.0;
+    int k = 2;
+    for (; k <= c.nz - 1; ++k)
+      if (rs.zn[k] > c.max_height_cloud) break;
+    rs.k_cloudmax = k - 1;
+  }
   // prescribed surface fluxes and the Monin-Obukhov u* table (setfluxlook.F90:78-99, 150-186)
   rs.lookup_ustr.assign(rs.lookup_entries + 1, 0.0);
   if (c.use_surface_boundary_conditions) {

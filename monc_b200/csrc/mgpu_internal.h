@@ -27,6 +27,7 @@ struct RefState {
   double velmin = 0, velmax = 0, aloginv = 0, cneut = 0, cfc = 0;
   int lookup_entries = 80;
   std::vector<double> cq;
+  int k_cloudmax = 0;  // simplecloud: highest level of saturation adjustment
 };
 
 // Builds the reference state from a configuration (restates gridmanager.F90:2008-2642,
@@ -38,7 +39,7 @@ const std::vector<double>* profile_by_name(const RefState& rs, const std::string
 enum ProfileId {
   P_RDZ = 0, P_RDZN, P_DZN, P_RHO, P_RHON, P_DTHREF, P_CZB, P_CZA, P_CZG, P_CZH, P_TZC1, P_TZC2, P_TZD1, P_TZD2,
   P_RNEUTML_SQ, P_BUOY_CO, P_THREF, P_PREFRCP, P_RPREFRCP, P_TREF, P_TSTARPR, P_QSAT, P_DQSATDT, P_QSATFAC,
-  P_GWX, P_GWY, P_COUNT
+  P_GWX, P_GWY, P_PREFN, P_COUNT
 };
 
 // Scalars every dynamical-core kernel reads (passed by value as a kernel parameter).
@@ -52,7 +53,8 @@ struct Scalars {
   double velmin, aloginv, cneut, cfc, convective_limit;
   double subb, subc, subg, subh, suba, ric, ricinv;
   double eps, repsh, thcona, thconb, thconap1, rlvap_over_cp, G;
-  double cq0;  // cq of the vapour field
+  double cq[MGPU_MAX_Q];  // buoyancy loading of each q field
+  int simplecloud, k_cloudmax;
   int lookup_entries;
   int forward;  // 1 on the first (forward) step
   int point_dynamics;  // 1: always use the untiled dynamics kernel (MGPU_POINT_DYNAMICS=1)

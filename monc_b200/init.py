@@ -87,3 +87,28 @@ def random_flow_state(nx, ny, nz, seed=7, amp_uv=2.0, amp_w=0.5, amp_th=0.5, ug=
     st["zw"] = zw
     st["zth"] = th + uniform_noise(shape, seed, 7, 0.1 * amp_th)
     return st
+
+
+def moist_layer_state(nx, ny, nz, zn, seed=1, theta_below=289.0, theta_above=297.5, inversion=840.0,
+                      lapse=0.00365, qt_below=9e-3, qt_above=1.5e-3, thref0=289.0, noise_levels=8,
+                      noise_amp=0.1, ug=0.0, n_tracers=0):
+    """Stratocumulus-like layer: theta (as theta' = theta - thref0) well mixed below `inversion`
+    and `theta_above` + lapse*(z - inversion) above it; total water as vapour (q0) with no
+    liquid (q1) -- the saturation adjustment forms the cloud in the first steps; uniform theta
+    noise on the lowest levels; passive tracers (q2...) log-normal near the surface."""
+    shape = (nz, ny, nx)
+    th_prof = np.where(zn > inversion, theta_above + lapse * (zn - inversion), theta_below) - thref0
+    th = np.broadcast_to(th_prof[:, None, None], shape).copy()
+    noise = uniform_noise(shape, seed, 3, noise_amp)
+    th[1:1 + noise_levels] += noise[1:1 + noise_levels]
+    th[0] = th[1]
+    qv = np.broadcast_to(np.where(zn > inversion, qt_above, qt_below)[:, None, None], shape).copy()
+    st = {"u": np.full(shape, float(ug)), "v": np.zeros(shape), "w": np.zeros(shape), "th": th,
+          "q0": qv, "q1": np.zeros(shape)}
+    for t in range(n_tracers):
+        g = uniform_noise(shape, seed, 40 + t, 1.0)
+        src = np.exp(0.5 * g) * np.exp(-zn / 200.0)[:, None, None]
+        st[f"q{2 + t}"] = src
+    for name in list(st):
+        st["z" + name] = st[name].copy()
+    return st

@@ -64,6 +64,7 @@ struct Model {
   std::vector<Field> q, zq, sq;
   std::vector<double> cq;
   int iqv = 0, iql = 0;  // 0-based indices of vapour / liquid (q_indices)
+  int k_cloudmax = 0;    // simplecloud: highest level of saturation adjustment
   // time stepping
   int timestep = 1, start_timestep = 1, field_stepping = FORWARD_STEPPING;
   int scalar_stepping = CENTRED_STEPPING, momentum_stepping = CENTRED_STEPPING;
@@ -1012,6 +1013,59 @@ static void set_consistent_lowbc_column(Model& m) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// simplecloud (simplecloud.F90:262-379) with saturation.F90 qsaturation / dqwsatdt
+// ---------------------------------------------------------------------------------------------
+static double qsaturation_(double temperature, double pressure) {
+  const double tk0c = 273.15, qsa1 = 3.8, qsa2 = -17.2693882, qsa3 = 35.86, qsa4 = 6.109;
+  return qsa1 / (pressure * std::exp(qsa2 * (temperature - tk0c) / (temperature - qsa3)) - qsa4);
+}
+static double dqwsatdt_(double qs, double temperature) {
+  const double tk0c = 273.15, qsa1 = 3.8, qsa2 = -17.2693882, qsa3 = 35.86, qsa4 = 6.109;
+  return -qsa2 * (tk0c - qsa3) * (1.0 + qsa4 * qs / qsa1) * qs * std::pow(temperature - qsa3, -2.0);
+}
+
+static void simplecloud_column(Model& m) {
+  if (m.halo_column) return;
+  const int y = m.col_y, x = m.col_x, iqv = m.iqv, iql = m.iql;
+  const bool fwd = m.field_stepping == FORWARD_STEPPING;
+  double dtm = m.dtm * 2.0;
+  if (fwd) dtm = m.dtm;
+  Field& q_v = fwd ? m.q[iqv] : m.zq[iqv];
+  Field& q_l = fwd ? m.q[iql] : m.zq[iql];
+  Field& th = fwd ? m.th : m.zth;
+  double exner = 0.0, one_over_exner = 0.0;
+  for (int k = 2; k <= m.k_cloudmax; ++k) {
+    exner = m.rprefrcp(k);
+    one_over_exner = m.prefrcp(k);
+    const double Pmb = m.prefn(k) / 100.;
+    const double qv = q_v(k, y, x) + m.sq[iqv](k, y, x) * dtm;
+    const double qc = q_l(k, y, x) + m.sq[iql](k, y, x) * dtm;
+    const double TdegK = (th(k, y, x) + m.sth(k, y, x) * dtm + m.thref(k)) * exner;
+    const double qs = qsaturation_(TdegK, Pmb);
+    if (qv > qs || qc > 0.0) {
+      const double dqsdT = dqwsatdt_(qs, TdegK);
+      const double qsatfac = 1.0 / (1.0 + m.rlvap_over_cp * dqsdT);
+      const double dmass = fmax_(-qc, (qv - qs) * qsatfac) / dtm;
+      m.sq[iqv](k, y, x) = m.sq[iqv](k, y, x) - dmass;
+      m.sq[iql](k, y, x) = m.sq[iql](k, y, x) + dmass;
+      m.sth(k, y, x) = m.sth(k, y, x) + m.rlvap_over_cp * dmass * one_over_exner;
+    }
+  }
+  // above k_cloudmax any cloud evaporates; the branch tests scalar_stepping (always centred) and
+  // one_over_exner keeps its value from the last level of the loop above
+  for (int k = m.k_cloudmax + 1; k <= m.nz; ++k) {
+    const bool sfwd = m.scalar_stepping == FORWARD_STEPPING;
+    const double qc = (sfwd ? m.q[iql] : m.zq[iql])(k, y, x) + m.sq[iql](k, y, x) * dtm;
+    if (qc > 0.0) {
+      const double dmass = -qc / dtm;
+      m.sq[iqv](k, y, x) = m.sq[iqv](k, y, x) - dmass;
+      m.sq[iql](k, y, x) = m.sq[iql](k, y, x) + dmass;
+      m.sth(k, y, x) = m.sth(k, y, x) + m.rlvap_over_cp * dmass * one_over_exner;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // diverr (diverr.F90:44-175) and psrce (pressuresource.F90:61-238)
 // ---------------------------------------------------------------------------------------------
 static void diverr_column(Model& m) {
@@ -1334,8 +1388,13 @@ static void timestep(Model& m) {
   // subgrid
   column_group(m, {lower_bc_column, smagorinsky_column});
   // dynamics
-  column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
-                   buoyancy_column, set_consistent_lowbc_column, diverr_column, psrce_column, stepfields_column});
+  if (m.cfg.simplecloud_enabled)
+    column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
+                     buoyancy_column, set_consistent_lowbc_column, simplecloud_column, diverr_column, psrce_column,
+                     stepfields_column});
+  else
+    column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
+                     buoyancy_column, set_consistent_lowbc_column, diverr_column, psrce_column, stepfields_column});
   // solver
   if (m.cfg.solver == MGPU_SOLVER_FFT) fftsolver(m);
   else iterative_solver(m);
@@ -1403,6 +1462,15 @@ static Model* create(const mgpu_config* cfg) {
   m.iqv = 0; m.iql = nq > 1 ? 1 : 0;
   m.cq.assign(std::max(nq, 1), 0.0);
   if (!cfg->passive_q && nq > 0) m.cq[m.iqv] = m.ratio_mol_wts - 1.0;  // setfluxlook.F90:95
+  if (cfg->simplecloud_enabled) {
+    // simplecloud.F90:230-248: liquid loading, and the highest level below max_height_cloud
+    if (nq < 2) throw std::runtime_error("simplecloud needs the vapour and liquid q fields");
+    m.cq[m.iql] = -1.0;
+    int k = 2;
+    for (; k <= nz - 1; ++k)
+      if (m.zn(k) > cfg->max_height_cloud) break;
+    m.k_cloudmax = k - 1;
+  }
   m.tvd_th.alloc(nz, nyh);
   m.flux_x.assign(nz + 2, 0.0); m.flux_y.assign(nz + 2, 0.0); m.flux_z.assign(nz + 2, 0.0);
   m.send_x.assign((size_t)(nz - 1) * m.ny, 0.0); m.recv_x = m.send_x;
@@ -1676,6 +1744,7 @@ int orc_component(void* h, int cid) {
       case MGPU_C_CORIOLIS: column_group(m, {coriolis_column}); break;
       case MGPU_C_BUOYANCY: column_group(m, {buoyancy_column}); break;
       case MGPU_C_SET_CONSISTENT_LOWBC: column_group(m, {set_consistent_lowbc_column}); break;
+      case MGPU_C_SIMPLECLOUD: if (!m.cfg.simplecloud_enabled) return -5; column_group(m, {simplecloud_column}); break;
       case MGPU_C_DIVERR: column_group(m, {diverr_column}); break;
       // psrce with the deferred first-row/column faces the solver callbacks add (fftsolver.F90:215-250)
       case MGPU_C_PSRCE: column_group(m, {psrce_column}); complete_psrce(m); break;
