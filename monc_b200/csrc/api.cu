@@ -79,11 +79,16 @@ static int alloc_state(mgpu_handle* h, DevState<T>& d) {
     if (rc) return rc;
   }
   for (int n = 0; n < h->cfg.number_q_fields; ++n) {
-    T** qq[] = {&d.q[n], &d.zq[n], &d.q_n[n], &d.zq_n[n]};
+    T** qq[] = {&d.q[n], &d.zq[n], &d.q_n[n], &d.zq_n[n], &d.sq[n]};
     for (T** pp : qq) {
       int rc = alloc_field<T>(h, pp);
       if (rc) return rc;
     }
+  }
+  // the moist centred step passes the scalar sources through memory (tiled kernels, one per scalar)
+  if (h->cfg.number_q_fields > 0) {
+    int rc = alloc_field<T>(h, &d.sth);
+    if (rc) return rc;
   }
   return MGPU_OK;
 }
@@ -93,11 +98,8 @@ static int alloc_component_fields(mgpu_handle* h, DevState<T>& d) {
   if (h->component_fields) return MGPU_OK;
   T** extra[] = {&d.su, &d.sv, &d.sw, &d.sth, &d.savu, &d.savv, &d.savw};
   for (T** pp : extra) {
+    if (*pp) continue;
     int rc = alloc_field<T>(h, pp);
-    if (rc) return rc;
-  }
-  for (int n = 0; n < h->cfg.number_q_fields; ++n) {
-    int rc = alloc_field<T>(h, &d.sq[n]);
     if (rc) return rc;
   }
   h->component_fields = true;
@@ -425,13 +427,13 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   if (h->cfg.reproducible) exact::launch_fused_subgrid<T>(h->sc, d, h->stream);
   else fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
   mark(1);
-  if (h->cfg.reproducible) exact::launch_fused_dynamics<T>(h->sc, d, h->stream);
-  else fast::launch_fused_dynamics<T>(h->sc, d, h->stream);
+  if (h->cfg.reproducible) h->launches += exact::launch_fused_dynamics<T>(h->sc, d, h->stream);
+  else h->launches += fast::launch_fused_dynamics<T>(h->sc, d, h->stream);
   mark(2);
   swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
   if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
   else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
-  h->launches += 3;
+  h->launches += 2;
   if (h->cfg.solver != MGPU_SOLVER_FFT) mark(3);
   int rc = pressure_solve<T>(h, d.p);
   if (rc) return rc;

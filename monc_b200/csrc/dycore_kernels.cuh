@@ -701,6 +701,10 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
     }
     if (s.coriolis) coriolis_point<T>(s, P, U, V, k, j, i, su, sv);
     if (k < nz && !s.passive_th) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (th_lo + th_hi);
+    if (k < nz && !s.passive_q) {
+      const T g2 = (T)(0.5 * s.G);
+      for (int n = 0; n < s.nq; ++n) sw = sw + g2 * (T)s.cq[n] * (__ldg(d.q[n] + o) + __ldg(d.q[n] + o + plane));
+    }
     d.zu_n[o] = (T)s.ugal + ZU(k, j, i) + dtm_x2 * su;
     d.zv_n[o] = (T)s.vgal + ZV(k, j, i) + dtm_x2 * sv;
     d.zw_n[o] = (T)0.0 + ZW(k, j, i) + dtm_x2 * sw;
@@ -710,9 +714,22 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
   }
 }
 
+// One scalar of the centred step: `zf` is advected and diffused; with `src` null the kernel also
+// steps it (stepfields + the Robert pre-smoothing of swap_smooth, with the negative clip for q
+// fields) into out_f / out_zf, otherwise it writes the source (levels 2..nz) for the cloud step.
+template <typename T>
+struct ScalarJob {
+  const T* f;   // state field (th or q)
+  const T* zf;  // z-field (zth or zq)
+  T* out_f;
+  T* out_zf;
+  T* src;
+  int clip;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_tiled(Scalars s, DevState<T> d,
-                                                                                    int kchunk) {
+                                                                                    int kchunk, ScalarJob<T> job) {
   using namespace tiled;
   using Gt = G<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -739,7 +756,7 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
   // level k reads the scalar at k-1 .. k+2, u v w at k-1 .. k+1, diff at k-1 .. k and profiles
   // at k-1 .. k+2; a chunk above level 2 also needs the z face below it (level kb-1).
   const int k0 = kb == 2 ? 1 : kb - 2;
-  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<RZF>(rF, d.zth, plane, kk);
+  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<RZF>(rF, job.zf, plane, kk);
   for (int kk = k0; kk <= kb + 1 && kk <= nz; ++kk) {
     sg.template stage<RF>(rU, d.u, plane, kk);
     sg.template stage<RF>(rV, d.v, plane, kk);
@@ -750,15 +767,20 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
   const T dtm_x2 = (T)(2.0 * s.dtm);
   const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
-  const T* __restrict__ th = d.th;
+  const T* __restrict__ th = job.f;
   if (kb == 2) {
     // level 1: zero source
     const long long o = lin(s, 1, j, i);
-    T fv = th[o], zv = d.zth[o];
-    T sm1 = c1 * fv + c2 * zv;
-    T zn = (T)0.0 + zv + dtm_x2 * (T)0.0;
-    d.zth_n[o] = sm1 + (T)s.tsmth * zn;
-    d.th_n[o] = zn;
+    if (job.src) {
+      job.src[o] = (T)0.0;
+    } else {
+      T fv = th[o], zv = job.zf[o];
+      T sm1 = c1 * fv + c2 * zv;
+      T zn = (T)0.0 + zv + dtm_x2 * (T)0.0;
+      if (job.clip && zn < (T)0.0) zn = (T)0.0;
+      job.out_zf[o] = sm1 + (T)s.tsmth * zn;
+      job.out_f[o] = zn;
+    }
   }
   cp_async_wait_all();
   __syncthreads();
@@ -774,7 +796,7 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     __syncthreads();  // level kb-2 of the u, v, w rings is overwritten by the first prefetch
   }
   for (int k = kb; k <= ke; ++k) {
-    if (k + 3 <= min(nz, ke + 2)) sg.template stage<RZF>(rF, d.zth, plane, k + 3);
+    if (k + 3 <= min(nz, ke + 2)) sg.template stage<RZF>(rF, job.zf, plane, k + 3);
     if (k + 2 <= min(nz, ke + 1)) {
       sg.template stage<RF>(rU, d.u, plane, k + 2);
       sg.template stage<RF>(rV, d.v, plane, k + 2);
@@ -784,7 +806,7 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
     T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
     const long long o = lin(s, k, j, i);
-    const T fv = __ldg(th + o);
+    const T fv = job.src ? (T)0.0 : __ldg(th + o);
     const CProf<T> P = cprof<T>(rP, k);
     const CRing<T> U = cring<T, RF>(rU, k, co, j, i), V = cring<T, RF>(rV, k, co, j, i),
                    W = cring<T, RF>(rW, k, co, j, i), DIFF = cring<T, RF>(rD, k, co, j, i);
@@ -800,15 +822,52 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
                           FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
     if (s.use_vd) sth = sth + diffusion_point<T>(s, P, ZF, DIFF, k, j, i);
     fz_lo = fz_hi;
-    T zv = ZF(k, j, i);
-    T smo = c1 * fv + c2 * zv;
-    T zn = (T)0.0 + zv + dtm_x2 * sth;
-    d.zth_n[o] = smo + (T)s.tsmth * zn;
-    d.th_n[o] = zn;
+    if (job.src) {
+      job.src[o] = sth;
+    } else {
+      T zv = ZF(k, j, i);
+      T smo = c1 * fv + c2 * zv;
+      T zn = (T)0.0 + zv + dtm_x2 * sth;
+      if (job.clip && zn < (T)0.0) zn = (T)0.0;
+      job.out_zf[o] = smo + (T)s.tsmth * zn;
+      job.out_f[o] = zn;
+    }
     if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
     cp_async_wait_all();
     __syncthreads();
   }
+}
+
+// Moist centred step after the tiled scalar kernels have written the advective + diffusive
+// sources: simplecloud (when enabled), then stepfields with the Robert pre-smoothing of
+// swap_smooth for theta and every q field (negative q clipped), as the point kernel does.
+template <typename T>
+__global__ void __launch_bounds__(256) k_f_cloud_step(Scalars s, DevState<T> d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z + 1;
+  if (i >= s.nx || j >= s.ny || k > s.nz) return;
+  const long long o = lin(s, k, j, i);
+  T sth = k >= 2 ? d.sth[o] : (T)0.0;
+  T sq[MGPU_MAX_Q];
+  for (int n = 0; n < s.nq; ++n) sq[n] = k >= 2 ? d.sq[n][o] : (T)0.0;
+  if (s.simplecloud && k >= 2) {
+    Prof<T> P = prof<T>(s);
+    const int iv = s.iqv, il = s.iql;
+    simplecloud_point<T>(s, P, k, d.zq[iv][o], d.zq[il][o], d.zth[o], d.zq[il][o], sth, sq[iv], sq[il]);
+  }
+  const T dtm_x2 = (T)(2.0 * s.dtm);
+  const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
+  auto step = [&](const T* f, const T* zf, T src, T* f_out, T* zf_out, bool clip) {
+    T fv = f[o], zv = zf[o];
+    T sm = c1 * fv + c2 * zv;
+    T zn = (T)0.0 + zv + dtm_x2 * src;
+    if (clip && zn < (T)0.0) zn = (T)0.0;
+    zf_out[o] = sm + (T)s.tsmth * zn;
+    f_out[o] = zn;
+  };
+  step(d.th, d.zth, sth, d.th_n, d.zth_n, false);
+  for (int n = 0; n < s.nq; ++n) step(d.q[n], d.zq[n], sq[n], d.q_n[n], d.zq_n[n], true);
 }
 
 // 3. pressure source from the stepped z-velocities (diverr + psrce)
@@ -952,15 +1011,17 @@ static inline int choose_level_chunks(int tiles, int slots, int levels) {
   return best;
 }
 
+// returns the number of kernels launched
 template <typename T>
-void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
+int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
   // the tiled kernels cover centred dry steps; the first (forward) step and moist runs use the
   // point kernel
-  const bool tiled_ok = !s.forward && !s.point_dynamics && s.nq == 0 && (s.nx % tiled::TX) == 0 &&
-                        (s.ny % tiled::TY) == 0 && s.nz >= 4;
+  const bool moist = s.nq > 0;
+  const bool tiled_ok = !s.forward && !s.point_dynamics && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 &&
+                        s.nz >= 4 && (!moist || (d.sth && d.sq[s.nq - 1]));
   if (!tiled_ok) {
     k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
-    return;
+    return 1;
   }
   const size_t sm_m = tiled::momentum_smem<T>(), sm_s = tiled::scalar_smem<T>();
   static int occ_m = 0, occ_s = 0, nsm = 0;
@@ -985,8 +1046,17 @@ void launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
   dim3 block(tiled::TX, tiled::TY, 1);
   dim3 grid_s(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_s - 1) / kc_s);
   dim3 grid_m(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_m - 1) / kc_m);
-  k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s);
+  if (!moist) {
+    k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, d.th_n, d.zth_n, nullptr, 0});
+  } else {
+    // one launch per scalar writing its source, then saturation adjustment and stepping
+    k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, nullptr, nullptr, d.sth, 0});
+    for (int n = 0; n < s.nq; ++n)
+      k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.q[n], d.zq[n], nullptr, nullptr, d.sq[n], 1});
+    k_f_cloud_step<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
+  }
   k_f_momentum_tiled<T><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
+  return moist ? s.nq + 3 : 2;
 }
 template <typename T>
 void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st) {

@@ -21,10 +21,11 @@ def rel_err(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def moist_pair(precision=cf.FP64, n_tracers=0, max_height_cloud=700.0):
+def moist_pair(precision=cf.FP64, n_tracers=0, max_height_cloud=700.0, reproducible=0):
     z = cf.stretched_levels(NZ, 20.0, 60.0, ztop=1000.0)
     c = cf.moist_config(NX, NY, z, 35.0, 0.3, shf_wm2=10.0, lhf_wm2=50.0, max_height_cloud=max_height_cloud,
                         n_tracers=n_tracers, precision=precision)
+    c.reproducible = reproducible
     o = po.Oracle(c)
     m = api.Model(c)
     st = ini.moist_layer_state(NX, NY, NZ, o.profile("zn"), seed=2, n_tracers=n_tracers)
@@ -82,3 +83,19 @@ def test_moist_fp32_mixed_tracks_fp64(gpu_lib):
         m.close()
     for a, b in zip(res[1], res[0]):
         assert np.abs(a - b).max() <= 1e-4 * max(np.abs(b).max(), 1e-3)
+
+
+@pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
+def test_moist_tiled_bit_identical_to_point_kernel(gpu_lib, monkeypatch, precision):
+    """The per-scalar tiled kernels plus the cloud step reproduce the point kernel bit for bit."""
+    outs = []
+    for point, chunks in (("1", "0"), ("0", "0"), ("0", "3")):
+        monkeypatch.setenv("MGPU_POINT_DYNAMICS", point)
+        monkeypatch.setenv("MGPU_LEVEL_CHUNKS", chunks)
+        o, m = moist_pair(precision=precision, n_tracers=1, reproducible=1)
+        m.step(4)
+        outs.append({f: m.download(f) for f in FIELDS + ["q2", "zq2"]})
+        m.close()
+    for res in outs[1:]:
+        for f in outs[0]:
+            np.testing.assert_array_equal(outs[0][f], res[f], err_msg=f)
