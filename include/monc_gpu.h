@@ -198,8 +198,9 @@ int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2);
 
 /* Per-stage device timing of mgpu_step (CUDA events on the handle's stream).  Stage order:
  * 0 subgrid, 1 dynamics, 2 pressure source, 3 fft x forward, 4 fft y forward, 5 tridiagonal,
- * 6 fft y inverse, 7 fft x inverse, 8 pstep + swap_smooth, 9 iterative solve. */
-#define MGPU_NSTAGES 10
+ * 6 fft y inverse, 7 fft x inverse, 8 pstep + swap_smooth, 9 iterative solve, 10 the momentum
+ * kernel of the dynamics stage alone (stage 1 minus stage 10 is the scalar kernels). */
+#define MGPU_NSTAGES 11
 int mgpu_set_profiling(mgpu_handle* h, int32_t on);
 int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches);
 

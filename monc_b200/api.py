@@ -42,7 +42,7 @@ FIELDS = {
 Q0, ZQ0, SQ0 = 32, 48, 64
 
 STAGES = ["subgrid", "dynamics", "pressure_source", "fft_x_fwd", "fft_y_fwd", "tridiag", "fft_y_inv",
-          "fft_x_inv", "pstep_swap", "iterative"]
+          "fft_x_inv", "pstep_swap", "iterative", "dynamics_momentum"]
 
 # registered MONC component names -> mgpu_component_id
 COMPONENTS = {
@@ -257,8 +257,8 @@ class Model:
         self._check(lib().mgpu_set_profiling(self.h, 1 if on else 0), "set_profiling")
 
     def stage_times(self) -> dict:
-        ms = np.zeros(10, dtype=np.float64)
-        n = np.zeros(10, dtype=np.int64)
+        ms = np.zeros(len(STAGES), dtype=np.float64)
+        n = np.zeros(len(STAGES), dtype=np.int64)
         self._check(lib().mgpu_stage_times(self.h, ms.ctypes.data, n.ctypes.data), "stage_times")
         return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(STAGES)}
 

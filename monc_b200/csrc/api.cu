@@ -411,6 +411,7 @@ static void collect_stage_times(mgpu_handle* h) {
   };
   acc(0, 0, 1);
   acc(1, 1, 2);
+  acc(10, 10, 2);
   acc(2, 2, 3);
   if (h->cfg.solver == MGPU_SOLVER_FFT)
     for (int q = 0; q < 5; ++q) acc(3 + q, 3 + q, 4 + q);
@@ -427,8 +428,9 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   if (h->cfg.reproducible) exact::launch_fused_subgrid<T>(h->sc, d, h->stream);
   else fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
   mark(1);
-  if (h->cfg.reproducible) h->launches += exact::launch_fused_dynamics<T>(h->sc, d, h->stream);
-  else h->launches += fast::launch_fused_dynamics<T>(h->sc, d, h->stream);
+  cudaEvent_t mid = h->profiling ? h->ev[10] : nullptr;
+  if (h->cfg.reproducible) h->launches += exact::launch_fused_dynamics<T>(h->sc, d, h->stream, mid);
+  else h->launches += fast::launch_fused_dynamics<T>(h->sc, d, h->stream, mid);
   mark(2);
   swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
   if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);

@@ -1011,9 +1011,9 @@ static inline int choose_level_chunks(int tiles, int slots, int levels) {
   return best;
 }
 
-// returns the number of kernels launched
+// returns the number of kernels launched; `mid` (may be null) is recorded before the momentum kernel
 template <typename T>
-int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
+int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cudaEvent_t mid) {
   // the tiled kernels cover centred dry steps; the first (forward) step and moist runs use the
   // point kernel
   const bool moist = s.nq > 0;
@@ -1021,6 +1021,7 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
                         s.nz >= 4 && (!moist || (d.sth && d.sq[s.nq - 1]));
   if (!tiled_ok) {
     k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
+    if (mid) cudaEventRecord(mid, st);
     return 1;
   }
   const size_t sm_m = tiled::momentum_smem<T>(), sm_s = tiled::scalar_smem<T>();
@@ -1055,6 +1056,7 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st) {
       k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.q[n], d.zq[n], nullptr, nullptr, d.sq[n], 1});
     k_f_cloud_step<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
   }
+  if (mid) cudaEventRecord(mid, st);
   k_f_momentum_tiled<T><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
   return moist ? s.nq + 3 : 2;
 }
