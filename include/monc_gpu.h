@@ -228,6 +228,29 @@ int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32_t nz, doub
                              const double* czb, const double* cza, const double* czg, const double* czh,
                              void* stream);
 
+/* Tangent-linear and adjoint runs of the dry FP64 model with the FFT solver (no counterpart in
+ * the reference, which has no adjoint).  The derivative is that of the discrete step as
+ * computed, with the TVD limiter branches, the Richardson-number regimes and max/min choices of
+ * the forward evaluation.  Tangents and adjoints of the state fields u v w th zu zv zw zth
+ * (ids 0..7) move through mgpu_upload_field / mgpu_download_field with the ids below (XFAST
+ * layout). */
+#define MGPU_TANGENT0 1024 /* MGPU_TANGENT0 + id: tangent of state field id */
+#define MGPU_ADJOINT0 2048 /* MGPU_ADJOINT0 + id: adjoint of state field id */
+
+/* Transpose (adjoint) of the FFT pressure solve applied to p in place: the same transforms with
+ * the transposed tridiagonal and the transposed horizontal-mean recurrence. */
+int mgpu_fftsolver_adjoint(mgpu_handle* h);
+
+/* Advance the state and its tangent nsteps steps; d_rmlmax is the tangent of the Smagorinsky
+ * mixing length rmlmax (= Cs * dx). */
+int mgpu_tl_step(mgpu_handle* h, int32_t nsteps, double d_rmlmax);
+
+/* Adjoint of nsteps steps from the current state.  On entry the adjoint fields hold dJ/d(state
+ * after nsteps); on return they hold dJ/d(current state), *rmlmax_bar holds dJ/d rmlmax, and the
+ * model state is the state after nsteps.  The forward sweep stores a checkpoint every
+ * checkpoint_interval steps; the reverse sweep recomputes each segment from its checkpoint. */
+int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval, double* rmlmax_bar);
+
 const char* mgpu_last_error(mgpu_handle* h);
 
 #ifdef __cplusplus

@@ -40,6 +40,8 @@ FIELDS = {
     "savu": 15, "savv": 16, "savw": 17,
 }
 Q0, ZQ0, SQ0 = 32, 48, 64
+TANGENT0, ADJOINT0 = 1024, 2048  # + id of a state field (u v w th zu zv zw zth = 0..7)
+STATE_FIELDS = ["u", "v", "w", "th", "zu", "zv", "zw", "zth"]
 
 STAGES = ["subgrid", "dynamics", "pressure_source", "fft_x_fwd", "fft_y_fwd", "tridiag", "fft_y_inv",
           "fft_x_inv", "pstep_swap", "iterative", "dynamics_momentum"]
@@ -139,6 +141,12 @@ def lib():
     L.mgpu_poisson_fft_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.mgpu_poisson_fft_noalloc.restype = C.c_int
+    L.mgpu_fftsolver_adjoint.argtypes = [C.c_void_p]
+    L.mgpu_fftsolver_adjoint.restype = C.c_int
+    L.mgpu_tl_step.argtypes = [C.c_void_p, C.c_int32, C.c_double]
+    L.mgpu_tl_step.restype = C.c_int
+    L.mgpu_adjoint_run.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+    L.mgpu_adjoint_run.restype = C.c_int
     L.mgpu_last_error.argtypes = [C.c_void_p]
     L.mgpu_last_error.restype = C.c_char_p
     _lib = L
@@ -151,6 +159,9 @@ def field_id(name_or_id) -> int:
     name = str(name_or_id)
     if name in FIELDS:
         return FIELDS[name]
+    for prefix, base in (("tl:", TANGENT0), ("adj:", ADJOINT0)):
+        if name.startswith(prefix) and name[len(prefix):] in STATE_FIELDS:
+            return base + FIELDS[name[len(prefix):]]
     for prefix, base in (("zq", ZQ0), ("sq", SQ0), ("q", Q0)):
         if name.startswith(prefix) and name[len(prefix):].isdigit():
             return base + int(name[len(prefix):])
@@ -235,6 +246,22 @@ class Model:
 
     def set_timestep(self, ts: int):
         self._check(lib().mgpu_set_timestep(self.h, ts), "set_timestep")
+
+    def fftsolver_adjoint(self):
+        """Apply the transpose of the FFT pressure solve to p in place."""
+        self._check(lib().mgpu_fftsolver_adjoint(self.h), "fftsolver_adjoint")
+
+    def tl_step(self, n: int = 1, d_rmlmax: float = 0.0):
+        """Advance the state and its tangent (fields "tl:u" ...) n steps (dry FP64 models)."""
+        self._check(lib().mgpu_tl_step(self.h, n, d_rmlmax), "tl_step")
+
+    def adjoint_run(self, n: int, checkpoint_interval: int = 25) -> float:
+        """Adjoint of n steps from the current state: fields "adj:u" ... hold dJ/d(state after n
+        steps) on entry and dJ/d(current state) on return; the state ends n steps on.  Returns
+        dJ/d rmlmax."""
+        out = C.c_double(0.0)
+        self._check(lib().mgpu_adjoint_run(self.h, n, checkpoint_interval, C.byref(out)), "adjoint_run")
+        return out.value
 
     def reductions(self) -> Reductions:
         r = Reductions()

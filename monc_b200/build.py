@@ -26,6 +26,7 @@ UNITS = [
     ("dycore_f32_fast.cu", []),
     ("fft.cu", []),
     ("iter.cu", []),
+    ("tlad.cu", []),
 ]
 
 

@@ -15,6 +15,22 @@
 
 using namespace mgpu;
 
+// Tangent-linear and adjoint work arrays (dry FP64 models)
+struct AdWork {
+  DevState<double> t{};          // tangents of the state and of the step's intermediates
+  double* adj[2][8] = {};        // adjoints of u v w th zu zv zw zth: adj[cur] is the current one
+  int cur = 0;
+  double* inter[6] = {};         // adjoints of vis, diff, zu_n, zv_n, zw_n, p
+  double* prof_bar = nullptr;    // adjoint of rneutml_sq per level
+  double* drsq = nullptr;        // d rneutml_sq / d rmlmax per level (device)
+  std::vector<double> drsq_h;
+  int* overflow = nullptr;
+  std::vector<double*> ckpt, seg;  // checkpoint states and the states of one segment (8 arrays each)
+  double* final_state[8] = {};
+  std::vector<void*> allocs;
+  bool tl = false, adj_ok = false;
+};
+
 struct mgpu_handle {
   mgpu_config cfg;
   RefState rs;
@@ -40,6 +56,7 @@ struct mgpu_handle {
   double* diag_d = nullptr;  // 2*nz FP64 diagnostics
   bool profiling = false;
   cudaEvent_t ev[16] = {};
+  struct AdWork* ad = nullptr;  // tangent-linear / adjoint arrays, allocated on first use
   double stage_ms[MGPU_NSTAGES] = {};
   int64_t stage_n[MGPU_NSTAGES] = {};
   std::string err;
@@ -233,6 +250,11 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
 int mgpu_destroy(mgpu_handle* h) {
   if (!h) return MGPU_ERR_ARGUMENT;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->ad) {
+    for (void* p : h->ad->allocs) cudaFree(p);
+    delete h->ad;
+    h->ad = nullptr;
+  }
   for (void* p : h->allocations) cudaFree(p);
   h->allocations.clear();
   if (h->fft.spec) fft_plan_destroy(h->fft);
@@ -255,6 +277,79 @@ const char* mgpu_last_error(mgpu_handle* h) { return h ? h->err.c_str() : "null 
 
 }  // extern "C"
 
+// ---- tangent-linear / adjoint work arrays ------------------------------------------------
+static void state_ptrs(DevState<double>& d, double* out[8]) {
+  double* p[8] = {d.u, d.v, d.w, d.th, d.zu, d.zv, d.zw, d.zth};
+  for (int q = 0; q < 8; ++q) out[q] = p[q];
+}
+
+static int ad_alloc(mgpu_handle* h, double** p, size_t n) {
+  if (cudaMalloc((void**)p, n * sizeof(double)) != cudaSuccess) return fail(h, MGPU_ERR_CUDA, "cudaMalloc (adjoint work)");
+  cudaMemsetAsync(*p, 0, n * sizeof(double), h->stream);
+  h->ad->allocs.push_back(*p);
+  return MGPU_OK;
+}
+
+static int ad_supported(mgpu_handle* h) {
+  if (h->fp32 || h->cfg.number_q_fields > 0 || h->cfg.solver != MGPU_SOLVER_FFT)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs need a dry FP64 model with the FFT solver");
+  return MGPU_OK;
+}
+
+// d rneutml_sq / d rmlmax: rneutml_sq = 1 / (1/(vk (z+z0))^2 + 1/rmlmax^2) (gridmanager.F90:2298-2310)
+static int ensure_drsq(mgpu_handle* h) {
+  AdWork* a = h->ad;
+  if (a->drsq) return MGPU_OK;
+  const int nz = h->cfg.nz;
+  a->drsq_h.assign(nz + 2, 0.0);
+  const double rm = h->rs.rmlmax;
+  for (int k = 2; k <= nz - 1; ++k) {
+    const double r2 = h->rs.rneutml_sq[k];
+    a->drsq_h[k] = 2.0 * r2 * r2 / (rm * rm * rm);
+  }
+  if (ad_alloc(h, &a->drsq, nz + 2)) return MGPU_ERR_CUDA;
+  if (cudaMemcpy(a->drsq, a->drsq_h.data(), (nz + 2) * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(h, MGPU_ERR_CUDA, "cudaMemcpy (drsq)");
+  return MGPU_OK;
+}
+
+static int ensure_tl(mgpu_handle* h) {
+  if (int rc = ad_supported(h)) return rc;
+  if (!h->ad) h->ad = new AdWork();
+  AdWork* a = h->ad;
+  if (a->tl) return MGPU_OK;
+  const size_t n = field_elems(h);
+  double** f[] = {&a->t.u, &a->t.v, &a->t.w, &a->t.th, &a->t.zu, &a->t.zv, &a->t.zw, &a->t.zth, &a->t.p,
+                  &a->t.vis, &a->t.diff, &a->t.zu_n, &a->t.zv_n, &a->t.zw_n, &a->t.th_n, &a->t.zth_n};
+  for (double** pp : f)
+    if (ad_alloc(h, pp, n)) return MGPU_ERR_CUDA;
+  if (ensure_drsq(h)) return MGPU_ERR_CUDA;
+  a->tl = true;
+  return MGPU_OK;
+}
+
+static int ensure_adj(mgpu_handle* h) {
+  if (int rc = ad_supported(h)) return rc;
+  if (!h->ad) h->ad = new AdWork();
+  AdWork* a = h->ad;
+  if (a->adj_ok) return MGPU_OK;
+  const size_t n = field_elems(h);
+  for (int c = 0; c < 2; ++c)
+    for (int q = 0; q < 8; ++q)
+      if (ad_alloc(h, &a->adj[c][q], n)) return MGPU_ERR_CUDA;
+  for (int q = 0; q < 6; ++q)
+    if (ad_alloc(h, &a->inter[q], n)) return MGPU_ERR_CUDA;
+  for (int q = 0; q < 8; ++q)
+    if (ad_alloc(h, &a->final_state[q], n)) return MGPU_ERR_CUDA;
+  if (ad_alloc(h, &a->prof_bar, h->cfg.nz + 2)) return MGPU_ERR_CUDA;
+  double* ov = nullptr;
+  if (ad_alloc(h, &ov, 1)) return MGPU_ERR_CUDA;
+  a->overflow = reinterpret_cast<int*>(ov);
+  if (ensure_drsq(h)) return MGPU_ERR_CUDA;
+  a->adj_ok = true;
+  return MGPU_OK;
+}
+
 // ---- field lookup -----------------------------------------------------------------------
 template <typename T>
 static T* field_ptr(mgpu_handle* h, DevState<T>& d, int id) {
@@ -276,6 +371,16 @@ static T* field_ptr(mgpu_handle* h, DevState<T>& d, int id) {
   if (id >= MGPU_SQ0 && id < MGPU_SQ0 + nq) {
     if (alloc_component_fields<T>(h, d)) return nullptr;
     return d.sq[id - MGPU_SQ0];
+  }
+  if (sizeof(T) == sizeof(double) && id >= MGPU_TANGENT0 && id < MGPU_TANGENT0 + 8) {
+    if (ensure_tl(h)) return nullptr;
+    double* t[8];
+    state_ptrs(h->ad->t, t);
+    return reinterpret_cast<T*>(t[id - MGPU_TANGENT0]);
+  }
+  if (sizeof(T) == sizeof(double) && id >= MGPU_ADJOINT0 && id < MGPU_ADJOINT0 + 8) {
+    if (ensure_adj(h)) return nullptr;
+    return reinterpret_cast<T*>(h->ad->adj[h->ad->cur][id - MGPU_ADJOINT0]);
   }
   return nullptr;
 }
@@ -449,6 +554,158 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   return MGPU_OK;
 }
 
+// ---- tangent-linear and adjoint drivers (dry FP64) ----------------------------------------
+static void launch_subgrid(mgpu_handle* h, DevState<double>& d) {
+  if (h->cfg.reproducible) exact::launch_fused_subgrid<double>(h->sc, d, h->stream);
+  else fast::launch_fused_subgrid<double>(h->sc, d, h->stream);
+}
+static int launch_dynamics(mgpu_handle* h, DevState<double>& d) {
+  return h->cfg.reproducible ? exact::launch_fused_dynamics<double>(h->sc, d, h->stream, nullptr)
+                             : fast::launch_fused_dynamics<double>(h->sc, d, h->stream, nullptr);
+}
+static void launch_pressure_source(mgpu_handle* h, DevState<double>& d) {
+  if (h->cfg.reproducible) exact::launch_fused_pressure_source<double>(h->sc, d, h->stream);
+  else fast::launch_fused_pressure_source<double>(h->sc, d, h->stream);
+}
+static void launch_pstep_swap(mgpu_handle* h, DevState<double>& d) {
+  if (h->cfg.reproducible) exact::launch_fused_pstep_swap<double>(h->sc, d, h->stream);
+  else fast::launch_fused_pstep_swap<double>(h->sc, d, h->stream);
+}
+
+// one step of the state and of its tangent (each tangent pass runs before the forward pass that
+// overwrites its inputs)
+static int tl_step_once(mgpu_handle* h, double dpar) {
+  DevState<double>& d = h->d64;
+  DevState<double>& t = h->ad->t;
+  const double* drsq = h->ad->drsq;
+  h->sc.forward = (h->timestep == 1) ? 1 : 0;
+  tl_pass(0, h->sc, d, t, drsq, dpar, h->stream);
+  launch_subgrid(h, d);
+  tl_pass(1, h->sc, d, t, drsq, dpar, h->stream);
+  h->launches += 3 + launch_dynamics(h, d);
+  swap_scalar_buffers<double>(d, 0);
+  std::swap(t.th, t.th_n);
+  std::swap(t.zth, t.zth_n);
+  tl_pass(2, h->sc, d, t, drsq, dpar, h->stream);
+  launch_pressure_source(h, d);
+  fft_solve<double>(h->fft, h->sc, t.p, h->stream, &h->launches);
+  int rc = pressure_solve<double>(h, d.p);
+  if (rc) return rc;
+  tl_pass(3, h->sc, d, t, drsq, dpar, h->stream);
+  launch_pstep_swap(h, d);
+  h->launches += 4;
+  h->timestep += 1;
+  return MGPU_OK;
+}
+
+static void copy_state(mgpu_handle* h, double* const* dst, double* const* src) {
+  const size_t bytes = field_elems(h) * sizeof(double);
+  for (int q = 0; q < 8; ++q) cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyDeviceToDevice, h->stream);
+}
+
+// the adjoint of one step from state X (already in h->d64): adjoints of the next state in
+// adj[cur] become adjoints of X in adj[1-cur]
+static int adjoint_step(mgpu_handle* h) {
+  AdWork* a = h->ad;
+  DevState<double>& d = h->d64;
+  h->sc.forward = (h->timestep == 1) ? 1 : 0;
+  // recompute the step's intermediates: post-subgrid state, vis, diff, zu_n..zth_n, p
+  launch_subgrid(h, d);
+  h->launches += 3 + launch_dynamics(h, d);
+  launch_pressure_source(h, d);
+  int rc = pressure_solve<double>(h, d.p);
+  if (rc) return rc;
+  double* const* B = a->adj[a->cur];
+  double* const* A = a->adj[1 - a->cur];
+  const size_t bytes = field_elems(h) * sizeof(double);
+  for (int q = 0; q < 8; ++q) CK(cudaMemsetAsync(A[q], 0, bytes, h->stream));
+  for (int q = 0; q < 6; ++q) CK(cudaMemsetAsync(a->inter[q], 0, bytes, h->stream));
+  double* tg[F_COUNT];
+  for (int q = 0; q < 8; ++q) tg[F_U + q] = A[q];
+  tg[F_VIS] = a->inter[0];
+  tg[F_DIFF] = a->inter[1];
+  tg[F_ZUN] = a->inter[2];
+  tg[F_ZVN] = a->inter[3];
+  tg[F_ZWN] = a->inter[4];
+  tg[F_P] = a->inter[5];
+  tg[F_PROF] = a->prof_bar;
+  const double* seed[8];
+  for (int q = 0; q < 8; ++q) seed[q] = B[q];
+  adj_pass(4, h->sc, d, tg, seed, a->overflow, h->stream);  // pstep + swap_smooth
+  fft_solve<double>(h->fft, h->sc, a->inter[5], h->stream, &h->launches, nullptr, true);
+  adj_pass(3, h->sc, d, tg, seed, a->overflow, h->stream);  // pressure source
+  adj_pass(1, h->sc, d, tg, seed, a->overflow, h->stream);  // momentum
+  adj_pass(2, h->sc, d, tg, seed, a->overflow, h->stream);  // scalars
+  adj_pass(0, h->sc, d, tg, seed, a->overflow, h->stream);  // subgrid
+  h->launches += 5;
+  a->cur = 1 - a->cur;
+  return MGPU_OK;
+}
+
+static int adjoint_run(mgpu_handle* h, int nsteps, int interval, double* rmlmax_bar) {
+  AdWork* a = h->ad;
+  DevState<double>& d = h->d64;
+  const size_t n = field_elems(h);
+  const int t0 = h->timestep;
+  const int nck = (nsteps + interval - 1) / interval;
+  while ((int)a->ckpt.size() < 8 * nck) {
+    double* p = nullptr;
+    if (ad_alloc(h, &p, n)) return MGPU_ERR_CUDA;
+    a->ckpt.push_back(p);
+  }
+  while ((int)a->seg.size() < 8 * interval) {
+    double* p = nullptr;
+    if (ad_alloc(h, &p, n)) return MGPU_ERR_CUDA;
+    a->seg.push_back(p);
+  }
+  double* X[8];
+  // forward sweep, saving a checkpoint every `interval` steps
+  for (int st = 0; st < nsteps; ++st) {
+    state_ptrs(d, X);
+    if (st % interval == 0) copy_state(h, &a->ckpt[8 * (st / interval)], X);
+    int rc = step_once<double>(h, d);
+    if (rc) return rc;
+  }
+  state_ptrs(d, X);
+  copy_state(h, a->final_state, X);
+  CK(cudaMemsetAsync(a->prof_bar, 0, (h->cfg.nz + 2) * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(a->overflow, 0, sizeof(int), h->stream));
+  // reverse sweep, one checkpoint segment at a time
+  for (int c = nck - 1; c >= 0; --c) {
+    const int s0 = c * interval, s1 = std::min(nsteps, s0 + interval);
+    state_ptrs(d, X);
+    copy_state(h, X, &a->ckpt[8 * c]);
+    h->timestep = t0 + s0;
+    for (int st = s0; st < s1; ++st) {
+      state_ptrs(d, X);
+      copy_state(h, &a->seg[8 * (st - s0)], X);
+      int rc = step_once<double>(h, d);
+      if (rc) return rc;
+    }
+    for (int st = s1 - 1; st >= s0; --st) {
+      state_ptrs(d, X);
+      copy_state(h, X, &a->seg[8 * (st - s0)]);
+      h->timestep = t0 + st;
+      int rc = adjoint_step(h);
+      if (rc) return rc;
+    }
+  }
+  state_ptrs(d, X);
+  copy_state(h, X, a->final_state);
+  h->timestep = t0 + nsteps;
+  int ovf = 0;
+  std::vector<double> pb(h->cfg.nz + 2);
+  CK(cudaMemcpyAsync(&ovf, a->overflow, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(pb.data(), a->prof_bar, pb.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  if (ovf) return fail(h, MGPU_ERR_UNSUPPORTED, "adjoint tape capacity exceeded");
+  double acc = 0.0;
+  for (int k = 1; k <= h->cfg.nz; ++k) acc += pb[k] * a->drsq_h[k];
+  if (rmlmax_bar) *rmlmax_bar = acc;
+  return MGPU_OK;
+}
+
 template <typename T>
 static int component(mgpu_handle* h, DevState<T>& d, int cid) {
   h->sc.forward = (h->timestep == 1) ? 1 : 0;
@@ -567,6 +824,32 @@ int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches) {
     if (launches) launches[q] = h->stage_n[q];
   }
   return MGPU_OK;
+}
+
+int mgpu_fftsolver_adjoint(mgpu_handle* h) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model configured for the iterative solver");
+  if (h->fp32) fft_solve<float>(h->fft, h->sc, h->d32.p, h->stream, &h->launches, nullptr, true);
+  else fft_solve<double>(h->fft, h->sc, h->d64.p, h->stream, &h->launches, nullptr, true);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return MGPU_OK;
+}
+
+int mgpu_tl_step(mgpu_handle* h, int32_t nsteps, double d_rmlmax) {
+  if (!h || nsteps < 0) return MGPU_ERR_ARGUMENT;
+  if (int rc = ensure_tl(h)) return rc;
+  for (int q = 0; q < nsteps; ++q)
+    if (int rc = tl_step_once(h, d_rmlmax)) return rc;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return MGPU_OK;
+}
+
+int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval, double* rmlmax_bar) {
+  if (!h || nsteps < 1 || checkpoint_interval < 1) return MGPU_ERR_ARGUMENT;
+  if (int rc = ensure_adj(h)) return rc;
+  return adjoint_run(h, nsteps, checkpoint_interval, rmlmax_bar);
 }
 
 int mgpu_mean_profile(mgpu_handle* h, int32_t id, double* out) {

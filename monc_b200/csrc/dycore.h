@@ -50,10 +50,11 @@ struct FftPlanDev {
 };
 int fft_plan_create(FftPlanDev& plan, const Scalars& s, const RefState& rs, bool fp32);
 void fft_plan_destroy(FftPlanDev& plan);
-// evs: NULL, or 6 events recorded before, between and after the five kernels
+// evs: NULL, or 6 events recorded before, between and after the five kernels.  transpose: apply
+// the transpose of the solve (the adjoint of the pressure solve) instead.
 template <typename T>
 void fft_solve(const FftPlanDev& plan, const Scalars& s, T* p, cudaStream_t st, int64_t* launches,
-               cudaEvent_t* evs = nullptr);
+               cudaEvent_t* evs = nullptr, bool transpose = false);
 
 template <typename T>
 void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st);
@@ -65,5 +66,17 @@ void iter_destroy(IterSolverDev* it);
 template <typename T>
 int iter_solve(IterSolverDev* it, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, int* iterations,
                double* residual);
+
+// Tangent-linear and adjoint passes of the dry FP64 step (tlad.cu).  Adjoint arrays are indexed
+// by these ids; F_FACE0.. are tape-internal (TVD face values).
+enum AdField { F_U, F_V, F_W, F_TH, F_ZU, F_ZV, F_ZW, F_ZTH, F_VIS, F_DIFF, F_ZUN, F_ZVN, F_ZWN, F_P, F_PROF, F_COUNT,
+               F_FACE0 = 64 };
+// pass 0 subgrid, 1 dynamics, 2 pressure source, 3 pstep + swap_smooth; t holds the tangents
+void tl_pass(int pass, const Scalars& s, const DevState<double>& d, const DevState<double>& t, const double* drsq,
+             double dpar, cudaStream_t st);
+// pass 0 subgrid, 1 momentum, 2 scalars, 3 pressure source, 4 pstep + swap_smooth; seed[0..7] are
+// the adjoints of the next state (u v w th zu zv zw zth), tg[F_*] the adjoint arrays added into
+void adj_pass(int pass, const Scalars& s, const DevState<double>& d, double* const* tg, const double* const* seed,
+              int* overflow, cudaStream_t st);
 
 }  // namespace mgpu

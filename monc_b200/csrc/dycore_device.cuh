@@ -81,10 +81,9 @@ __device__ T lookup_ustr(const Scalars& s, T vel) {
 // Level-1 eddy coefficients and scalar ghost value of one column.
 //   zu_state : current_state%zu (always), zu_a/zv_a: u,v on the forward step else zu,zv,
 //   th_a     : th on the forward step else zth (level 2 read, level 1 written by the caller).
-template <typename T>
-__device__ void lower_bc_column(const Scalars& s, const Prof<T>& P, const View<T>& zu_state, const View<T>& zu_a,
-                                const View<T>& zv_a, const View<T>& th_a, const View<T>* qv_a, int j, int i,
-                                T& vis1, T& diff1, T& th1, T& qv1) {
+template <typename T, class A, class PA>
+__device__ void lower_bc_column(const Scalars& s, const PA& P, const A& zu_state, const A& zu_a, const A& zv_a,
+                                const A& th_a, const A* qv_a, int j, int i, T& vis1, T& diff1, T& th1, T& qv1) {
   T hv = sqr((T)0.5 * (zu_state(2, j, i) + zu_a(2, j, i - 1)) + (T)s.ugal);
   hv = hv + sqr((T)0.5 * (zv_a(2, j, i) + zv_a(2, j - 1, i)) + (T)s.vgal);
   hv = sqrt(hv) + (T)s.smallp;
@@ -161,9 +160,8 @@ __device__ T half_squared_strain(const Scalars& s, const PA& P, const A& U, cons
 }
 
 // moist_ri_2 for one level (RICHARDSON_NUMBER_CALCULATION = 2)
-template <typename T>
-__device__ T moist_ri(const Scalars& s, const Prof<T>& P, T ssq, const View<T>& TH, const View<T>& QV,
-                      const View<T>& QL, int k, int j, int i) {
+template <typename T, class A, class PA>
+__device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A& QV, const A& QL, int k, int j, int i) {
   T tmpinv = rcp(ssq);
   T scltmp = P(P_RDZN, k + 1) * P(P_BUOY_CO, k);
   const T rl = (T)s.rlvap_over_cp, eps = (T)s.eps;
@@ -190,14 +188,13 @@ __device__ T moist_ri(const Scalars& s, const Prof<T>& P, T ssq, const View<T>& 
 }
 
 // vis/diff at level 2 <= k <= nz-1 from the strain rate and Richardson number
-template <typename T>
-__device__ void smagorinsky_point(const Scalars& s, const Prof<T>& P, const View<T>& U, const View<T>& V,
-                                  const View<T>& W, const View<T>& THcur, const View<T>& THarg, const View<T>* QV,
-                                  const View<T>* QL, int k, int j, int i, T& vis, T& diff) {
-  T ssq = half_squared_strain<T, View<T>>(s, P, U, V, W, k, j, i);
+template <typename T, class A, class PA>
+__device__ void smagorinsky_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const A& THcur,
+                                  const A& THarg, const A* QV, const A* QL, int k, int j, int i, T& vis, T& diff) {
+  T ssq = half_squared_strain<T, A>(s, P, U, V, W, k, j, i);
   T ri = (T)0.0;
   if (!s.passive_th) {
-    if (!s.passive_q) ri = moist_ri<T>(s, P, ssq, THarg, *QV, *QL, k, j, i);
+    if (!s.passive_q) ri = moist_ri<T, A>(s, P, ssq, THarg, *QV, *QL, k, j, i);
     else  // the dry branch reads current_state%th in both stepping modes
       ri = (P(P_DTHREF, k) + THcur(k + 1, j, i) - THcur(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
   }

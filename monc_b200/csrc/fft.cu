@@ -212,7 +212,7 @@ __global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<
 // ---- vertical tridiagonal per (ky, kx) in FP64 ----------------------------------------------
 template <typename T>
 __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
-                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz) {
+                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose) {
   typedef typename Cx<T>::t C;
   const int nxh = nx / 2 + 1;
   long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -223,6 +223,35 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   const double* cza = prof + P_CZA * prof_stride;
   const double* czg = prof + P_CZG * prof_stride;
   C* sp = spec + col;
+  if (transpose && kx == 0 && ky == 0) {
+    // transpose of the mean-mode recurrence below: the rows r = 2..nz-1 of
+    // cza(r) p(r+1) + czg(r) p(r) + czb(r) p(r-1) = b(r), p(1) = p(2) = 0, solved from the top
+    double zr1 = 0.0, zi1 = 0.0, zr2 = 0.0, zi2 = 0.0;  // z(u), z(u+1)
+    C ynext = sp[(long long)(nz - 1) * plane];           // y(nz)
+    for (int u = nz; u >= 3; --u) {
+      const C yu = ynext;
+      if (u >= 4) ynext = sp[(long long)(u - 2) * plane];  // y(u-1), read before z(u-1) overwrites it
+      double yr = (double)yu.x, yi = (double)yu.y;
+      if (u <= nz - 1) { yr -= czg[u] * zr1; yi -= czg[u] * zi1; }
+      if (u + 1 <= nz - 1) { yr -= czb[u + 1] * zr2; yi -= czb[u + 1] * zi2; }
+      const double zr = yr / cza[u - 1], zi = yi / cza[u - 1];  // z(u-1)
+      zr2 = zr1; zi2 = zi1; zr1 = zr; zi1 = zi;
+      C o;
+      o.x = (T)zr;
+      o.y = (T)zi;
+      sp[(long long)(u - 2) * plane] = o;
+    }
+    C zero;
+    zero.x = (T)0;
+    zero.y = (T)0;
+    sp[0] = zero;
+    sp[(long long)(nz - 1) * plane] = zero;
+    return;
+  }
+  // the transposed tridiagonal has the same pivots (they depend on czb(k)*cza(k-1) only) with
+  // the off-diagonals exchanged: cza(k-1) below the diagonal, czb(k+1) above it
+  const double* lo = transpose ? cza - 1 : czb;  // lo[k]: coefficient of s(k-1) in row k
+  const double* up = transpose ? czb + 1 : cza;  // up[k]: coefficient of p(k+1) in row k
   if (kx == 0 && ky == 0) {
     // horizontal-mean mode: upward recurrence from p(1) = p(2) = 0
     C v2 = sp[plane];
@@ -267,8 +296,8 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
     for (int q = 0; q < B; ++q) {
       int k = k0 + q;
       if (k <= nz) {
-        sr = (double)vb[q].x - czb[k] * sr * bb[q];
-        si = (double)vb[q].y - czb[k] * si * bb[q];
+        sr = (double)vb[q].x - lo[k] * sr * bb[q];
+        si = (double)vb[q].y - lo[k] * si * bb[q];
         s1buf[col + (long long)(k - 1) * plane] = make_double2(sr, si);
       }
     }
@@ -292,8 +321,8 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
     for (int q = 0; q < B; ++q) {
       int k = k0 - q;
       if (k >= 2) {
-        pr = (sb[q].x - cza[k] * pr) * bb[q];
-        pi = (sb[q].y - cza[k] * pi) * bb[q];
+        pr = (sb[q].x - up[k] * pr) * bb[q];
+        pi = (sb[q].y - up[k] * pi) * bb[q];
         o.x = (T)pr;
         o.y = (T)pi;
         sp[(long long)(k - 1) * plane] = o;
@@ -395,7 +424,8 @@ void fft_plan_destroy(FftPlanDev& pl) {
 }
 
 template <typename T>
-void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, cudaEvent_t* evs) {
+void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, cudaEvent_t* evs,
+               bool transpose) {
   typedef typename Cx<T>::t C;
   const bool f32 = sizeof(T) == 4;
   FftSizes z = sizes<T>(pl);
@@ -414,7 +444,8 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, s.nx, s.ny, z.logy, z.cols_y, false);
   mark(2);
   long long ncol = (long long)plane;
-  k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz);
+  k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
+                                                               transpose ? 1 : 0);
   mark(3);
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, s.nx, s.ny, z.logy, z.cols_y, true);
   mark(4);
@@ -423,8 +454,8 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   *launches += 5;
 }
 
-template void fft_solve<double>(const FftPlanDev&, const Scalars&, double*, cudaStream_t, int64_t*, cudaEvent_t*);
-template void fft_solve<float>(const FftPlanDev&, const Scalars&, float*, cudaStream_t, int64_t*, cudaEvent_t*);
+template void fft_solve<double>(const FftPlanDev&, const Scalars&, double*, cudaStream_t, int64_t*, cudaEvent_t*, bool);
+template void fft_solve<float>(const FftPlanDev&, const Scalars&, float*, cudaStream_t, int64_t*, cudaEvent_t*, bool);
 
 // ---- horizontal-mean diagnostics: one block per level, FP64 accumulation in a fixed order ----
 template <typename T>
@@ -598,7 +629,7 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   dim3 gy((nxh + z.cols_y - 1) / z.cols_y, nz);
   k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x);
   k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nx, ny, z.logy, z.cols_y, false);
-  k_tridiag<double><<<(unsigned)((plane + 127) / 128), 128, 0, st>>>(spec, s1, b1, prof, stride, nx, ny, nz);
+  k_tridiag<double><<<(unsigned)((plane + 127) / 128), 128, 0, st>>>(spec, s1, b1, prof, stride, nx, ny, nz, 0);
   k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nx, ny, z.logy, z.cols_y, true);
   k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x);
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
