@@ -6,7 +6,7 @@
 //          derivative of the seeded outputs with respect to every leaf (an input read).
 // Comparisons act on values, so a branch (the TVD limiter's, the Richardson-number regimes,
 // max/min) is frozen at the branch the forward evaluation takes.  Derivatives of |x| and
-// copysign at x = 0 take the branch that x >= 0 selects.
+// copysign at x = 0 take the branch that x >= 0 selects; sqrt'(0) is taken as 0.
 #pragma once
 
 #include <cmath>
@@ -44,9 +44,11 @@ __device__ __forceinline__ Dual copysign(Dual a, Dual b) {
   return Dual(r, ::signbit(a.v) != ::signbit(b.v) ? -a.d : a.d);
 }
 __device__ __forceinline__ bool signbit(Dual a) { return ::signbit(a.v); }
+// at exactly 0 (a wind speed of a flow at rest) the derivative of sqrt is taken as 0, the
+// subgradient of |(u, v)| at the origin
 __device__ __forceinline__ Dual sqrt(Dual a) {
   const double r = ::sqrt(a.v);
-  return Dual(r, a.d / (2.0 * r));
+  return Dual(r, r > 0.0 ? a.d / (2.0 * r) : 0.0);
 }
 __device__ __forceinline__ Dual log(Dual a) { return Dual(::log(a.v), a.d / a.v); }
 __device__ __forceinline__ Dual exp(Dual a) {
@@ -150,7 +152,7 @@ __device__ __forceinline__ TV copysign(TV a, TV b) {
 __device__ __forceinline__ bool signbit(TV a) { return ::signbit(a.v); }
 __device__ __forceinline__ TV sqrt(TV a) {
   const double r = ::sqrt(a.v);
-  return mk1(r, a, 0.5 / r);
+  return mk1(r, a, r > 0.0 ? 0.5 / r : 0.0);
 }
 __device__ __forceinline__ TV log(TV a) { return mk1(::log(a.v), a, 1.0 / a.v); }
 __device__ __forceinline__ TV exp(TV a) {
