@@ -54,6 +54,7 @@ struct mgpu_handle {
   int64_t launches = 0;
   double* xfer = nullptr;  // device staging buffer (FP64 field) for uploads/downloads
   double* diag_d = nullptr;  // 2*nz FP64 diagnostics
+  double* bmean_d = nullptr; // FP32-mixed: horizontal means of th and q per level (1+nq rows of nz+2)
   bool profiling = false;
   cudaEvent_t ev[16] = {};
   struct AdWork* ad = nullptr;  // tangent-linear / adjoint arrays, allocated on first use
@@ -181,6 +182,7 @@ static const std::vector<double>* prof_vec(const RefState& r, int id) {
     case P_RPREFRCP: return &r.rprefrcp; case P_TREF: return &r.tref; case P_TSTARPR: return &r.tstarpr;
     case P_QSAT: return &r.qsat; case P_DQSATDT: return &r.dqsatdt; case P_QSATFAC: return &r.qsatfac;
     case P_GWX: return &r.gwx; case P_GWY: return &r.gwy; case P_PREFN: return &r.prefn;
+    case P_TOFF: return &r.moist_toff; case P_TC0: return &r.tc0;
   }
   return nullptr;
 }
@@ -229,6 +231,9 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   cudaMemset(h->divmax_d, 0, sizeof(unsigned long long));
   if (cudaMalloc(&h->xfer, field_elems(h) * sizeof(double)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
   if (cudaMalloc(&h->diag_d, 2 * (size_t)cfg->nz * sizeof(double)) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
+  if (cudaMalloc(&h->bmean_d, (size_t)(1 + MGPU_MAX_Q) * (cfg->nz + 2) * sizeof(double)) != cudaSuccess)
+    return cleanup(MGPU_ERR_CUDA);
+  cudaMemset(h->bmean_d, 0, (size_t)(1 + MGPU_MAX_Q) * (cfg->nz + 2) * sizeof(double));
   for (cudaEvent_t& e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
   fill_scalars(h);
@@ -264,6 +269,7 @@ int mgpu_destroy(mgpu_handle* h) {
   cudaFree(h->divmax_d);
   cudaFree(h->xfer);
   cudaFree(h->diag_d);
+  cudaFree(h->bmean_d);
   for (cudaEvent_t& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -534,8 +540,15 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   else fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
   mark(1);
   cudaEvent_t mid = h->profiling ? h->ev[10] : nullptr;
+  if (sizeof(T) == 4) {
+    // FP32-mixed: take the horizontal-mean buoyancy out (see buoyancy_point)
+    launch_level_means<T>(h->sc, d.th, d.q, h->cfg.number_q_fields, h->bmean_d, h->stream);
+    h->sc.bmean = h->bmean_d;
+    h->launches += 1;
+  }
   if (h->cfg.reproducible) h->launches += exact::launch_fused_dynamics<T>(h->sc, d, h->stream, mid);
   else h->launches += fast::launch_fused_dynamics<T>(h->sc, d, h->stream, mid);
+  h->sc.bmean = nullptr;
   mark(2);
   swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
   if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);

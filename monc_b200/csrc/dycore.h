@@ -56,6 +56,10 @@ template <typename T>
 void fft_solve(const FftPlanDev& plan, const Scalars& s, T* p, cudaStream_t st, int64_t* launches,
                cudaEvent_t* evs = nullptr, bool transpose = false);
 
+// horizontal means of th (row 0) and q[0..nq-1] (rows 1..nq) per level into out[row*(nz+2) + k]
+template <typename T>
+void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st);
+
 template <typename T>
 void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st);
 

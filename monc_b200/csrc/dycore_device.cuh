@@ -60,6 +60,11 @@ __device__ __forceinline__ float div_rn(float x, float r) {
 // x / r where r is a reference density; Boussinesq runs have r == 1 exactly and x/1 == x
 template <typename T> __device__ __forceinline__ T div_rho(const Scalars& s, T x, T r) { return s.rho_unity ? x : div_rn(x, r); }
 template <typename T> __device__ __forceinline__ T cub(T a) { return a * a * a; }
+// 1/(fdels + 1e-30) of the TVD limiter.  In FP32 an advected perturbation of order 1e-30 can
+// cancel the 1e-30 exactly and make the reciprocal infinite (then 0*inf = NaN downstream); the
+// FP32 path returns 1e30 there.  FP64 keeps MONC's expression unchanged.
+template <typename T> __device__ __forceinline__ T rcp_limiter(T x) { return rcp(x); }
+__device__ __forceinline__ float rcp_limiter(float x) { return x == 0.0f ? 1.0e30f : rcp(x); }
 
 // ------------------------------------------------------------------------------------------
 // lower_bc, prescribed surface fluxes (lowerbc.F90:221-305, 601-768; look :645-666)
@@ -171,6 +176,25 @@ __device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A
   T qt_kp1 = QV(k + 1, j, i) + QL(k + 1, j, i);
   T thlpr_k = TH(k, j, i) - rl * QL(k, j, i) * pr;
   T thlpr_kp1 = TH(k + 1, j, i) - rl * QL(k + 1, j, i) * pr;
+  if constexpr (sizeof(T) == 4) {
+    // FP32: the same quantities with the reference-state offsets (thref ~ 290 K) cancelled
+    // analytically -- thv(ln) - thv(li) = eps dth + (rl pr - thcona)(ql(ln) - ql(li)) -- and the
+    // temperature offset rpr thref(k+1) - tstarpr - tref taken from an FP64 profile
+    const T toff = P(P_TOFF, k);
+    T dth = (thlpr_kp1 - thlpr_k + P(P_DTHREF, k));
+    T qtun = qt_kp1 - eps * (qt_kp1 - qt_k);
+    T qtln = qt_k + eps * (qt_kp1 - qt_k);
+    T qlli = tmax<T>((T)0.0, (qt_k - (qsat + dq * (rpr * thlpr_k - tst))) * fac);
+    T qlui = tmax<T>((T)0.0, (qt_kp1 - (qsat + dq * (rpr * thlpr_kp1 + toff))) * fac);
+    T qlln = tmax<T>((T)0.0, (qtln - (qsat + dq * (rpr * (thlpr_k + eps * dth) - tst))) * fac);
+    T qlun = tmax<T>((T)0.0, (qtun - (qsat + dq * (rpr * (thlpr_kp1 - eps * dth) + toff))) * fac);
+    T dl = eps * dth + (rl * pr - (T)s.thcona) * (qlln - qlli);
+    T du = -eps * dth + (rl * pr - (T)s.thconap1) * (qlun - qlui);
+    (void)thr;
+    (void)thr1;
+    (void)tref;
+    return scltmp * tmpinv * ((T)s.thconb * (qt_kp1 - qt_k) + (dl - du) * (T)s.repsh);
+  }
   T qlli = tmax<T>((T)0.0, (qt_k - (qsat + dq * (rpr * thlpr_k - tst))) * fac);
   T qlui = tmax<T>((T)0.0, (qt_kp1 - (qsat + dq * (rpr * (thlpr_kp1 + thr1) - tst - tref))) * fac);
   T thvli = thlpr_k + thr + (rl * pr - (T)s.thcona) * qlli;
@@ -348,10 +372,22 @@ __device__ void coriolis_point(const Scalars& s, const PA& P, const A& U, const 
 template <typename T>
 __device__ T buoyancy_point(const Scalars& s, const Prof<T>& P, const View<T>& TH, const View<T>* Q, int k, int j,
                             int i, T sw) {
-  if (!s.passive_th) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (TH(k, j, i) + TH(k + 1, j, i));
+  // with s.bmean the horizontal means are taken out first: a horizontally uniform part of sw only
+  // moves the mean pressure, which the projection removes again (the projected mean w is zero)
+  const int st = s.nz + 2;
+  if (!s.passive_th) {
+    if (s.bmean) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * ((TH(k, j, i) - (T)s.bmean[k]) + (TH(k + 1, j, i) - (T)s.bmean[k + 1]));
+    else sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (TH(k, j, i) + TH(k + 1, j, i));
+  }
   if (!s.passive_q) {
     const T g2 = (T)(0.5 * s.G);
-    for (int n = 0; n < s.nq; ++n) sw = sw + g2 * (T)s.cq[n] * (Q[n](k, j, i) + Q[n](k + 1, j, i));
+    for (int n = 0; n < s.nq; ++n) {
+      if (s.bmean)
+        sw = sw + g2 * (T)s.cq[n] * ((Q[n](k, j, i) - (T)s.bmean[(1 + n) * st + k]) +
+                                    (Q[n](k + 1, j, i) - (T)s.bmean[(1 + n) * st + k + 1]));
+      else
+        sw = sw + g2 * (T)s.cq[n] * (Q[n](k, j, i) + Q[n](k + 1, j, i));
+    }
   }
   return sw;
 }
@@ -383,10 +419,21 @@ __device__ void simplecloud_point(const Scalars& s, const PA& P, int k, T q_v, T
     const T Pmb = P(P_PREFN, k) / (T)100.;
     const T qv = q_v + sqv * dtm;
     const T qc = q_l + sql * dtm;
-    const T tk = (th + sth * dtm + P(P_THREF, k)) * exner;
-    const T qs = qsaturation<T>(tk, Pmb);
+    T qs, dqsdT_ = (T)0.0;
+    if constexpr (sizeof(T) == 4) {
+      // FP32: the temperature as its departure from 273.15 K, built from an FP64 reference
+      // offset, so that exp() and the pole of Tetens' formula see it without cancellation
+      const T tc = (th + sth * dtm) * exner + P(P_TC0, k);
+      const T tq = tc + (T)(273.15 - 35.86);  // temperature - qsa3
+      qs = (T)3.8 / (Pmb * exp((T)-17.2693882 * tc / tq) - (T)6.109);
+      dqsdT_ = (T)17.2693882 * (T)(273.15 - 35.86) * ((T)1.0 + (T)6.109 * qs / (T)3.8) * qs / (tq * tq);
+    } else {
+      const T tk = (th + sth * dtm + P(P_THREF, k)) * exner;
+      qs = qsaturation<T>(tk, Pmb);
+      dqsdT_ = dqwsatdt<T>(qs, tk);
+    }
     if (qv > qs || qc > (T)0.0) {
-      const T dqsdT = dqwsatdt<T>(qs, tk);
+      const T dqsdT = dqsdT_;
       const T qsatfac = (T)1.0 / ((T)1.0 + rl * dqsdT);
       const T dmass = tmax<T>(-qc, (qv - qs) * qsatfac) / dtm;
       sqv = sqv - dmass;
@@ -417,7 +464,7 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
   T hrcfl = rcp(sum_cfl_out + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = r6 * ((T)1.0 - cflmod * cflmod);
-  T rfdels = rcp(fdels + (T)1.e-30);
+  T rfdels = rcp_limiter(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * curv_term - fgt1 - fgt2;
   T fnfs = (ffs - fu) * rfdels;
   T fncs = (fc - fu) * rfdels;
@@ -573,7 +620,7 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
     T hrcfl = rcp(sum + (T)1.e-30);
     T hcfl = (T)0.5 * cflmod;
     T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-    T rfdels = rcp(fdels + (T)1.e-30);
+    T rfdels = rcp_limiter(fdels + (T)1.e-30);
     T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
     T fnfs = (ffs - fu) * rfdels;
     T fncs = (fc - fu) * rfdels;
@@ -613,7 +660,7 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
   T hrcfl = rcp(sum + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-  T rfdels = rcp(fdels + (T)1.e-30);
+  T rfdels = rcp_limiter(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
   T fnfs = (ffs - fu) * rfdels;
   T fncs = (fc - fu) * rfdels;

@@ -700,10 +700,21 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
       if (k < nz) sw = sw + dw;
     }
     if (s.coriolis) coriolis_point<T>(s, P, U, V, k, j, i, su, sv);
-    if (k < nz && !s.passive_th) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (th_lo + th_hi);
+    // as buoyancy_point, with the horizontal means removed when s.bmean is set
+    if (k < nz && !s.passive_th) {
+      if (s.bmean) sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * ((th_lo - (T)s.bmean[k]) + (th_hi - (T)s.bmean[k + 1]));
+      else sw = sw + ((T)0.5 * P(P_BUOY_CO, k)) * (th_lo + th_hi);
+    }
     if (k < nz && !s.passive_q) {
       const T g2 = (T)(0.5 * s.G);
-      for (int n = 0; n < s.nq; ++n) sw = sw + g2 * (T)s.cq[n] * (__ldg(d.q[n] + o) + __ldg(d.q[n] + o + plane));
+      const int st = nz + 2;
+      for (int n = 0; n < s.nq; ++n) {
+        if (s.bmean)
+          sw = sw + g2 * (T)s.cq[n] * ((__ldg(d.q[n] + o) - (T)s.bmean[(1 + n) * st + k]) +
+                                      (__ldg(d.q[n] + o + plane) - (T)s.bmean[(1 + n) * st + k + 1]));
+        else
+          sw = sw + g2 * (T)s.cq[n] * (__ldg(d.q[n] + o) + __ldg(d.q[n] + o + plane));
+      }
     }
     d.zu_n[o] = (T)s.ugal + ZU(k, j, i) + dtm_x2 * su;
     d.zv_n[o] = (T)s.vgal + ZV(k, j, i) + dtm_x2 * sv;

@@ -492,6 +492,36 @@ void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_t
   k_diagnostics<T><<<s.nz, 256, 0, st>>>(th, w, s.prof, s.nz + 2, s.plane, out_th, out_w2);
 }
 template void launch_diagnostics<double>(const Scalars&, const double*, const double*, double*, double*, cudaStream_t);
+
+// ---- horizontal means of th and the q fields per level (FP64 sums in a fixed order) ----------
+template <typename T>
+struct MeanFields {
+  const T* f[1 + MGPU_MAX_Q];
+};
+template <typename T>
+__global__ void k_level_means(MeanFields<T> mf, long long plane, int stride, double* out) {
+  const int k = blockIdx.x + 1, row = blockIdx.y;
+  const T* fk = mf.f[row] + (long long)(k - 1) * plane;
+  double a = 0.0;
+  for (long long t = threadIdx.x; t < plane; t += blockDim.x) a += (double)fk[t];
+  __shared__ double sa[256];
+  sa[threadIdx.x] = a;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) sa[threadIdx.x] += sa[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[(long long)row * stride + k] = sa[0] / (double)plane;
+}
+template <typename T>
+void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st) {
+  MeanFields<T> mf{};
+  mf.f[0] = th;
+  for (int n = 0; n < nq; ++n) mf.f[1 + n] = q[n];
+  k_level_means<T><<<dim3(s.nz, 1 + nq), 256, 0, st>>>(mf, s.plane, s.nz + 2, out);
+}
+template void launch_level_means<double>(const Scalars&, const double*, double* const*, int, double*, cudaStream_t);
+template void launch_level_means<float>(const Scalars&, const float*, float* const*, int, double*, cudaStream_t);
 template void launch_diagnostics<float>(const Scalars&, const float*, const float*, double*, double*, cudaStream_t);
 
 }  // namespace mgpu

@@ -115,7 +115,8 @@ void build_reference_state(const mgpu_config& c, RefState& rs) {
   std::vector<double>* all[] = {&rs.z, &rs.zn, &rs.dz, &rs.dzn, &rs.rdz, &rs.rdzn, &rs.rho, &rs.rhon, &rs.thref,
                                 &rs.dthref, &rs.czb, &rs.cza, &rs.czg, &rs.czh, &rs.tzc1, &rs.tzc2, &rs.tzd1, &rs.tzd2,
                                 &rs.rneutml, &rs.rneutml_sq, &rs.buoy_co, &rs.prefn, &rs.prefrcp, &rs.rprefrcp,
-                                &rs.tref, &rs.tstarpr, &rs.qsat, &rs.dqsatdt, &rs.qsatfac, &rs.gwx, &rs.gwy};
+                                &rs.tref, &rs.tstarpr, &rs.qsat, &rs.dqsatdt, &rs.qsatfac, &rs.gwx, &rs.gwy,
+                                &rs.moist_toff, &rs.tc0};
   for (auto* v : all) v->assign(n + 2, 0.0);
   rs.smallp = (double)1.0e-14f;  // MONC declares smallp in FP64 but initialises it from a single literal
   rs.rlvap_over_cp = c.rlvap / c.cp;
@@ -189,6 +190,10 @@ void build_reference_state(const mgpu_config& c, RefState& rs) {
                       (2.0 * 1.0);
       rs.qsatfac[k] = 1.0 / (1.0 + rs.rlvap_over_cp * rs.dqsatdt[k]);
     }
+    // FP64 offsets for the FP32-mixed moist terms: temperature minus 273.15 K of the reference
+    // state, and rprefrcp(k) thref(k+1) - tstarpr(k) - tref(k) of the moist Richardson number
+    for (int k = 1; k <= n; ++k) rs.tc0[k] = rs.thref[k] * rs.rprefrcp[k] - 273.15;
+    for (int k = 1; k <= n - 1; ++k) rs.moist_toff[k] = rs.rprefrcp[k] * rs.thref[k + 1] - rs.tstarpr[k] - rs.tref[k];
   }
   // neutral mixing length (gridmanager.F90:2298-2310)
   for (int k = 2; k <= n - 1; ++k) {

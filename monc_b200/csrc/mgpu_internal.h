@@ -18,6 +18,7 @@ struct RefState {
   std::vector<double> z, zn, dz, dzn, rdz, rdzn, rho, rhon, thref, dthref, czb, cza, czg, czh, tzc1, tzc2, tzd1, tzd2;
   std::vector<double> rneutml, rneutml_sq, buoy_co, prefn, prefrcp, rprefrcp, tref, tstarpr, qsat, dqsatdt, qsatfac;
   std::vector<double> gwx, gwy;  // geostrophic wind profile
+  std::vector<double> moist_toff, tc0;  // FP64 offsets of the FP32-mixed moist terms (grid.cpp)
   double czn = 0, zlogm = 0, zlogth = 0, vk_on_zlogm = 0;
   double dx = 0, dy = 0, cx = 0, cy = 0, cx2 = 0, cy2 = 0, tcx = 0, tcy = 0;
   double rmlmax = 0, smallp = 0, rlvap_over_cp = 0, r_over_cp = 0;
@@ -39,7 +40,7 @@ const std::vector<double>* profile_by_name(const RefState& rs, const std::string
 enum ProfileId {
   P_RDZ = 0, P_RDZN, P_DZN, P_RHO, P_RHON, P_DTHREF, P_CZB, P_CZA, P_CZG, P_CZH, P_TZC1, P_TZC2, P_TZD1, P_TZD2,
   P_RNEUTML_SQ, P_BUOY_CO, P_THREF, P_PREFRCP, P_RPREFRCP, P_TREF, P_TSTARPR, P_QSAT, P_DQSATDT, P_QSATFAC,
-  P_GWX, P_GWY, P_PREFN, P_COUNT
+  P_GWX, P_GWY, P_PREFN, P_TOFF, P_TC0, P_COUNT
 };
 
 // Scalars every dynamical-core kernel reads (passed by value as a kernel parameter).
@@ -64,6 +65,8 @@ struct Scalars {
   int passive_th, passive_q, nq, iqv, iql;
   int coriolis, surface_bcs, use_vd;
   const double* prof;      // device: P_COUNT profiles, each (nz+2) long, 1-based
+  const double* bmean;     // FP32-mixed fused step: horizontal means of th (row 0) and q(n) (row 1+n) per
+                           // level, (nz+2) per row, removed from the buoyancy; null elsewhere
   const double* lookup;    // device: lookup_ustr, 1-based
 };
 
