@@ -30,7 +30,7 @@ struct DevState {
   template <typename T>                                                                                   \
   int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st, unsigned long long* divmax, \
                        int64_t* launches);                                                                \
-  template <typename T> void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st);     \
+  template <typename T> int launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st);      \
   template <typename T> int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cudaEvent_t mid); \
   template <typename T> void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st); \
   template <typename T> void launch_fused_pstep_swap(const Scalars& s, DevState<T>& d, cudaStream_t st);

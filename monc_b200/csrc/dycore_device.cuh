@@ -212,13 +212,13 @@ __device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A
 }
 
 // vis/diff at level 2 <= k <= nz-1 from the strain rate and Richardson number
-template <typename T, class A, class PA>
-__device__ void smagorinsky_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const A& THcur,
-                                  const A& THarg, const A* QV, const A* QL, int k, int j, int i, T& vis, T& diff) {
+template <typename T, class A, class PA, class AT>
+__device__ void smagorinsky_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const AT& THcur,
+                                  const AT& THarg, const AT* QV, const AT* QL, int k, int j, int i, T& vis, T& diff) {
   T ssq = half_squared_strain<T, A>(s, P, U, V, W, k, j, i);
   T ri = (T)0.0;
   if (!s.passive_th) {
-    if (!s.passive_q) ri = moist_ri<T, A>(s, P, ssq, THarg, *QV, *QL, k, j, i);
+    if (!s.passive_q) ri = moist_ri<T, AT>(s, P, ssq, THarg, *QV, *QL, k, j, i);
     else  // the dry branch reads current_state%th in both stepping modes
       ri = (P(P_DTHREF, k) + THcur(k + 1, j, i) - THcur(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
   }

@@ -5,7 +5,7 @@
 
 namespace mgpu {
 namespace fast {
-template void launch_fused_subgrid<float>(const Scalars&, DevState<float>&, cudaStream_t);
+template int launch_fused_subgrid<float>(const Scalars&, DevState<float>&, cudaStream_t);
 template int launch_fused_dynamics<float>(const Scalars&, DevState<float>&, cudaStream_t, cudaEvent_t);
 template void launch_fused_pressure_source<float>(const Scalars&, DevState<float>&, cudaStream_t);
 template void launch_fused_pstep_swap<float>(const Scalars&, DevState<float>&, cudaStream_t);

@@ -8,7 +8,7 @@
 namespace mgpu {
 namespace exact {
 template int launch_component<double>(int, const Scalars&, DevState<double>&, cudaStream_t, unsigned long long*, int64_t*);
-template void launch_fused_subgrid<double>(const Scalars&, DevState<double>&, cudaStream_t);
+template int launch_fused_subgrid<double>(const Scalars&, DevState<double>&, cudaStream_t);
 template int launch_fused_dynamics<double>(const Scalars&, DevState<double>&, cudaStream_t, cudaEvent_t);
 template void launch_fused_pressure_source<double>(const Scalars&, DevState<double>&, cudaStream_t);
 template void launch_fused_pstep_swap<double>(const Scalars&, DevState<double>&, cudaStream_t);

@@ -5,7 +5,7 @@
 
 namespace mgpu {
 namespace fast {
-template void launch_fused_subgrid<double>(const Scalars&, DevState<double>&, cudaStream_t);
+template int launch_fused_subgrid<double>(const Scalars&, DevState<double>&, cudaStream_t);
 template int launch_fused_dynamics<double>(const Scalars&, DevState<double>&, cudaStream_t, cudaEvent_t);
 template void launch_fused_pressure_source<double>(const Scalars&, DevState<double>&, cudaStream_t);
 template void launch_fused_pstep_swap<double>(const Scalars&, DevState<double>&, cudaStream_t);

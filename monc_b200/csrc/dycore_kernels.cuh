@@ -537,6 +537,8 @@ constexpr int min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
 constexpr int M_PLANES = 7 * RM;   // u v w zu zv zw vis
 constexpr int S_PLANES = 4 * RF + RZF;  // u v w diff + scalar
 template <typename T>
+constexpr size_t smag_smem() { return sizeof(T) * ((size_t)3 * RM * G<T>::PLANE + (size_t)RP * P_COUNT); }
+template <typename T>
 constexpr size_t momentum_smem() { return sizeof(T) * ((size_t)M_PLANES * G<T>::PLANE + (size_t)RP * P_COUNT); }
 template <typename T>
 constexpr size_t scalar_smem() {
@@ -881,6 +883,77 @@ __global__ void __launch_bounds__(256) k_f_cloud_step(Scalars s, DevState<T> d) 
   for (int n = 0; n < s.nq; ++n) step(d.q[n], d.zq[n], sq[n], d.q_n[n], d.zq_n[n], true);
 }
 
+// Smagorinsky of levels kb..ke (2 <= k <= nz-1) of a tile, shared-memory tiled like the
+// dynamics kernels: u, v, w (the z-fields on centred steps) in rings of four planes, profiles in a
+// ring, the Richardson-number inputs (th, q) read at the column itself.  The chunk holding level
+// nz-1 also zeroes vis and diff at the top level.  Level 1 (lower_bc) is k_c_lower_bc.
+template <typename T>
+__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_smag_tiled(Scalars s, DevState<T> d,
+                                                                                  int kchunk) {
+  using namespace tiled;
+  using Gt = G<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int nz = s.nz;
+  const int kb = 2 + (int)blockIdx.z * kchunk;
+  const int ke = min(nz - 1, kb + kchunk - 1);
+  const long long plane = s.plane;
+  const bool fwd = s.forward;
+  constexpr int FS = RM * Gt::PLANE;
+  T* rU = sm;
+  T* rV = rU + FS;
+  T* rW = rV + FS;
+  T* rP = rW + FS;
+  const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  const T* gu = fwd ? d.u : d.zu;
+  const T* gv = fwd ? d.v : d.zv;
+  const T* gw = fwd ? d.w : d.zw;
+  Stager<T> sg;
+  sg.init(s, j0, i0, tid);
+  auto stage_level = [&](int kk) {
+    sg.template stage<RM>(rU, gu, plane, kk);
+    sg.template stage<RM>(rV, gv, plane, kk);
+    sg.template stage<RM>(rW, gw, plane, kk);
+  };
+  for (int kk = kb - 1; kk <= kb + 1 && kk <= nz; ++kk) stage_level(kk);
+  if (tid < P_COUNT)
+    for (int kk = kb - 1; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
+  const View<T> THc = view<T>(d.th, s), THa = view<T>(fwd ? d.th : d.zth, s);
+  View<T> QV, QL;
+  const bool moist = !s.passive_q && s.nq > 1;
+  if (moist) {
+    QV = view<T>(fwd ? d.q[s.iqv] : d.zq[s.iqv], s);
+    QL = view<T>(fwd ? d.q[s.iql] : d.zq[s.iql], s);
+  }
+  if (ke == nz - 1) {
+    const long long o = lin(s, nz, j, i);
+    d.vis[o] = (T)0.0;
+    d.diff[o] = (T)0.0;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int k = kb; k <= ke; ++k) {
+    if (k + 2 <= min(nz, ke + 1)) stage_level(k + 2);
+    const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
+    T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
+    const CProf<T> P = cprof<T>(rP, k);
+    const CRing<T> U = cring<T, RM>(rU, k, co, j, i), V = cring<T, RM>(rV, k, co, j, i),
+                   W = cring<T, RM>(rW, k, co, j, i);
+    T vis, diff;
+    smagorinsky_point<T>(s, P, U, V, W, THc, THa, moist ? &QV : (const View<T>*)nullptr,
+                         moist ? &QL : (const View<T>*)nullptr, k, j, i, vis, diff);
+    const long long o = lin(s, k, j, i);
+    d.vis[o] = vis;
+    d.diff[o] = diff;
+    if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
 // 3. pressure source from the stepped z-velocities (diverr + psrce)
 template <typename T>
 __global__ void k_f_pressure_source(Scalars s, DevState<T> d) {
@@ -1004,10 +1077,6 @@ int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st,
   return MGPU_OK;
 }
 
-template <typename T>
-void launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st) {
-  k_f_subgrid<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
-}
 // Number of level chunks for a grid of `tiles` tiles: the count (chunks of at least 8 levels) whose
 // CTAs fill the resident slots most evenly; each extra chunk costs a few staged levels.
 static inline int choose_level_chunks(int tiles, int slots, int levels) {
@@ -1023,6 +1092,37 @@ static inline int choose_level_chunks(int tiles, int slots, int levels) {
 }
 
 // returns the number of kernels launched; `mid` (may be null) is recorded before the momentum kernel
+// returns the number of kernels launched
+template <typename T>
+int launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st) {
+  // measured on B200: the tiled Smagorinsky pays in FP32 (0.18 -> 0.13 ms at 256x256x128) but
+  // not in FP64, where the point kernel is as fast (0.20 ms), so FP64 keeps the point kernel
+  const bool tiled_ok = sizeof(T) == 4 && !s.point_dynamics && (s.nx % tiled::TX) == 0 &&
+                        (s.ny % tiled::TY) == 0 && s.nz >= 4;
+  if (!tiled_ok) {
+    k_f_subgrid<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
+    return 1;
+  }
+  const size_t smem = tiled::smag_smem<T>();
+  static int occ = 0, nsm = 0;
+  if (!nsm) {
+    cudaFuncSetAttribute(k_f_smag_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_f_smag_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_f_smag_tiled<T>, tiled::NT, smem);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (occ < 1) occ = 1;
+    if (nsm < 1) nsm = 1;
+  }
+  k_c_lower_bc<T><<<dim3((s.nx + 31) / 32, (s.ny + 7) / 8, 1), pt_block(), 0, st>>>(s, d);
+  const int tiles = (s.nx / tiled::TX) * (s.ny / tiled::TY), levels = s.nz - 2;
+  const int nc = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ * nsm, levels);
+  const int kc = (levels + nc - 1) / nc;
+  dim3 grid(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc - 1) / kc);
+  k_f_smag_tiled<T><<<grid, dim3(tiled::TX, tiled::TY, 1), smem, st>>>(s, d, kc);
+  return 2;
+}
 template <typename T>
 int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cudaEvent_t mid) {
   // the tiled kernels cover centred dry steps; the first (forward) step and moist runs use the

@@ -43,9 +43,15 @@ static int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
 // rows_fast selects which index consecutive threads walk: the row (when rows are the contiguous
 // dimension in shared memory, es > 1) or the butterfly within a row (es == 1), so that a warp
 // touches consecutive shared-memory words.
+// Rows stored contiguously (es == 1) are padded with one element after every 32 (pidx): a
+// bit-reversed scatter of 16-byte elements then spreads a quarter-warp over all eight bank groups
+// instead of one.
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 5); }
+__host__ __device__ __forceinline__ int padded_row(int n) { return n + (n >> 5); }
+
 template <typename C>
 __device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int es, const C* tw, bool inverse,
-                                bool rows_fast = false) {
+                                bool rows_fast = false, bool padded = false) {
   const int half_n = n >> 1;
   const int total = nrows * half_n;
   for (int s = 1; s <= logn; ++s) {
@@ -61,10 +67,11 @@ __device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int 
       C w = tw[pos * stride];
       if (inverse) w.y = -w.y;
       C* row = buf + r * rs;
-      C a = row[i0 * es], c = row[i1 * es];
+      const int a0 = padded ? pidx(i0) : i0 * es, a1 = padded ? pidx(i1) : i1 * es;
+      C a = row[a0], c = row[a1];
       C t = cmul(w, c);
-      row[i1 * es] = csub(a, t);
-      row[i0 * es] = cadd(a, t);
+      row[a1] = csub(a, t);
+      row[a0] = cadd(a, t);
     }
     __syncthreads();
   }
@@ -83,6 +90,7 @@ __global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restri
   const long long pair0 = (long long)blockIdx.x * rows_per_cta;
   const long long npairs = (long long)nz * pairs_per_level;
   const int nxh = nx / 2 + 1;
+  const int prow = padded_row(nx);
   for (int t = threadIdx.x; t < rows_per_cta * nx; t += blockDim.x) {
     int r = t / nx, e = t - r * nx;
     long long pr = pair0 + r;
@@ -97,18 +105,18 @@ __global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restri
       z.x = (T)0; z.y = (T)0;
     }
     int br = __brev(e) >> (32 - logn);
-    buf[r * nx + br] = z;
+    buf[r * prow + pidx(br)] = z;
   }
   __syncthreads();
-  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, nx, 1, tw, false);
+  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, prow, 1, tw, false, false, true);
   for (int t = threadIdx.x; t < rows_per_cta * nxh; t += blockDim.x) {
     int r = t / nxh, m = t - r * nxh;
     long long pr = pair0 + r;
     if (pr >= npairs) continue;
     int k = (int)(pr / pairs_per_level) + 1;
     int j = 2 * (int)(pr % pairs_per_level);
-    C zm = buf[r * nx + m];
-    C zn = buf[r * nx + ((nx - m) & (nx - 1))];
+    C zm = buf[r * prow + pidx(m)];
+    C zn = buf[r * prow + pidx((nx - m) & (nx - 1))];
     C a, b;
     a.x = (T)0.5 * (zm.x + zn.x);
     a.y = (T)0.5 * (zm.y - zn.y);
@@ -133,6 +141,7 @@ __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restri
   const long long pair0 = (long long)blockIdx.x * rows_per_cta;
   const long long npairs = (long long)nz * pairs_per_level;
   const int nxh = nx / 2 + 1;
+  const int prow = padded_row(nx);
   for (int t = threadIdx.x; t < rows_per_cta * nxh; t += blockDim.x) {
     int r = t / nxh, m = t - r * nxh;
     long long pr = pair0 + r;
@@ -150,17 +159,17 @@ __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restri
     C z;
     z.x = a.x - b.y;
     z.y = a.y + b.x;
-    buf[r * nx + (__brev(m) >> (32 - logn))] = z;
+    buf[r * prow + pidx(__brev(m) >> (32 - logn))] = z;
     if (m > 0 && m < nx / 2) {
       C zc;
       zc.x = a.x + b.y;
       zc.y = b.x - a.y;
       int mm = nx - m;
-      buf[r * nx + (__brev(mm) >> (32 - logn))] = zc;
+      buf[r * prow + pidx(__brev(mm) >> (32 - logn))] = zc;
     }
   }
   __syncthreads();
-  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, nx, 1, tw, true);
+  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, prow, 1, tw, true, false, true);
   const T sc = (T)(1.0 / (double)nx);
   for (int t = threadIdx.x; t < rows_per_cta * nx; t += blockDim.x) {
     int r = t / nx, e = t - r * nx;
@@ -169,7 +178,7 @@ __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restri
     int k = (int)(pr / pairs_per_level) + 1;
     int j = 2 * (int)(pr % pairs_per_level);
     T* row = p + (long long)(k - 1) * nx * ny + (long long)j * nx;
-    C z = buf[r * nx + e];
+    C z = buf[r * prow + pidx(e)];
     row[e] = z.x * sc;
     row[nx + e] = z.y * sc;
   }
@@ -345,7 +354,7 @@ static FftSizes sizes(const FftPlanDev& pl) {
   z.logy = ilog2(pl.ny);
   z.rows_x = (int)std::max<size_t>(1, 32768 / (pl.nx * cs));
   z.cols_y = (int)std::min<size_t>(16, std::max<size_t>(1, 32768 / (pl.ny * cs)));
-  z.smem_x = cs * (pl.nx / 2 + (size_t)z.rows_x * pl.nx);
+  z.smem_x = cs * (pl.nx / 2 + (size_t)z.rows_x * padded_row(pl.nx));
   z.smem_y = cs * (pl.ny / 2 + (size_t)z.cols_y * pl.ny);
   return z;
 }
