@@ -230,6 +230,14 @@ def run_ours(args):
            "note": "initial state (8 FP64 fields, pinned host) uploaded in the timed region and "
                    "amortised over the steps; per-step read-back of the mean theta and w'^2 profiles"}
 
+    # the metric's second part: adjoint/forward time ratio on the differentiation window (dry CBL
+    # 128x128x96, 300 steps, checkpoint every 25), and FP32-mixed vs FP64 on the moist layer;
+    # single-GPU runs only (every rank would repeat the same work)
+    extra = {}
+    if world == 1 and not args.skip_extra:
+        extra["adjoint"] = adjoint_ratio()
+        extra["precision_moist"] = precision_moist()
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -288,7 +296,46 @@ def run_ours(args):
         "clocks": r64["clocks"],
         "finite": r64["finite"],
     }
+    out.update(extra)
     print(json.dumps(out), flush=True)
+
+
+def adjoint_ratio():
+    """Forward window and its adjoint (objective: resolved TKE below 1 km at the last step), CUDA
+    events on the model's stream."""
+    import argparse as _ap
+
+    from monc_b200 import api, gradcheck as gc
+
+    a = _ap.Namespace(nx=128, ny=128, nz=96, dx=50.0, dz=20.0, dt=1.0, ug=0.0, fcoriol=0.0, seed=1)
+    cfg, zn, dz, base = gc.setup(a)
+    steps, interval = 300, 25
+    fin, _, _ = gc.timed_window(cfg, base, steps)
+    lev = (zn <= 1000.0) & (np.arange(a.nz) >= 1)
+    seed = {f: np.zeros_like(base["th"]) for f in api.STATE_FIELDS}
+    for f in ("u", "v", "w"):
+        pert = fin[f] - fin[f].mean(axis=(1, 2), keepdims=True)
+        seed[f] = pert / (a.nx * a.ny) * (dz * lev)[:, None, None]
+    _, fwd_ms, adj_ms = gc.timed_window(cfg, base, steps, seed, interval)
+    return {"window": "dry CBL 128x128x96, dx=50 m, dz=20 m, dt=1 s, 300 steps, FP64, checkpoint every 25 steps",
+            "forward_ms": round(fwd_ms, 3), "adjoint_ms": round(adj_ms, 3),
+            "adjoint_forward_ratio": round(adj_ms / fwd_ms, 2)}
+
+
+def precision_moist():
+    """FP32-mixed vs FP64 on the moist stratocumulus-like layer (512x512x160, 500 steps)."""
+    import argparse as _ap
+
+    from monc_b200 import config as cf, precision as pr
+
+    a = _ap.Namespace(nx=512, ny=512, nz=160, dx=35.0, dz_bottom=5.0, dz_top=20.0, dt=0.3, steps=500, seed=1,
+                      noise_levels=10, solver="fft", tolerance=1e-12)
+    ms64, th64, w64, qv64, _ = pr.run(a, cf.FP64)
+    ms32, th32, w32, qv32, _ = pr.run(a, cf.FP32_MIXED)
+    return {"case": "moist layer 512x512x160, dx=35 m, dz 5->20 m, dt=0.3 s, simplecloud, 500 steps",
+            "fp64_ms_per_step": round(ms64, 4), "fp32_mixed_ms_per_step": round(ms32, 4),
+            "speedup": round(ms64 / ms32, 3), "rel_err_mean_theta": pr.rel(th32, th64),
+            "rel_err_mean_w2": pr.rel(w32, w64), "rel_err_mean_qv": pr.rel(qv32, qv64)}
 
 
 def _oracle_run(seed_steps):
@@ -367,6 +414,8 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--skip-extra", action="store_true",
+                    help="skip the adjoint-ratio and moist-precision measurements (single-GPU runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
