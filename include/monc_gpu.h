@@ -44,6 +44,7 @@ extern "C" {
 /* pressure solvers (fftsolver / iterativesolver components) */
 #define MGPU_SOLVER_FFT        0
 #define MGPU_SOLVER_ITERATIVE  1
+#define MGPU_SOLVER_EXTERNAL   2  /* one y-slab of a decomposed domain: the caller drives the solve */
 
 /* iterative solver types (iterativesolver.F90 solver_type) */
 #define MGPU_ITER_BICGSTAB 0
@@ -149,7 +150,9 @@ void mgpu_config_defaults(mgpu_config* cfg);
  * and allocates every field on the current CUDA device.
  * MGPU_ERR_ARGUMENT (checked on the host before any device call): nx, ny even and >= 4; with the
  * FFT solver nx and ny powers of two <= 4096; 3 <= nz <= MGPU_MAX_NZ; dtm > 0; known precision and
- * solver.  MGPU_ERR_NO_DEVICE when no CUDA device is visible. */
+ * solver.  MGPU_ERR_NO_DEVICE when no CUDA device is visible.  A model with solver
+ * MGPU_SOLVER_EXTERNAL is one slab of a decomposed domain (see mgpu_slab_init below); mgpu_step
+ * refuses it. */
 int mgpu_create(const mgpu_config* cfg, mgpu_handle** out);
 
 /* Release every device allocation (the finalisation callbacks). */
@@ -250,6 +253,80 @@ int mgpu_tl_step(mgpu_handle* h, int32_t nsteps, double d_rmlmax);
  * model state is the state after nsteps.  The forward sweep stores a checkpoint every
  * checkpoint_interval steps; the reverse sweep recomputes each segment from its checkpoint. */
 int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval, double* rmlmax_bar);
+
+/* ---- y-slab domain decomposition ---------------------------------------------------------
+ *
+ * The horizontal domain split into y-slabs, one per GPU (MONC splits it into 2-D blocks,
+ * decomposition.F90:57-123; slabs keep whole x rows, so the x halo stays periodic inside each
+ * model and only y rows move).  Each rank creates a model with solver MGPU_SOLVER_EXTERNAL and
+ * ny = nyl + 2*halo rows: its nyl interior rows of the global ny_global, with `halo` rows of the
+ * neighbouring slabs below and above (halo >= 3 covers the step's stencils: the TVD and
+ * viscosity stencils reach 2 rows, the pressure source 1 more).  A step is then
+ *
+ *   halo exchange of MGPU_HALO_STATE (depth halo)
+ *   mgpu_step_phase(SUBGRID)
+ *   FP32-mixed only: mgpu_slab_level_means, average the means over the slabs
+ *   mgpu_step_phase(DYNAMICS)                   dynamics, scalar swap, pressure source
+ *   mgpu_slab_fft_x(forward)                    x-FFT of the interior rows into kx blocks
+ *   all-to-all: block q of every slab to rank q (perform_forward_3dfft, pencilfft.F90:126-138)
+ *   mgpu_slab_solve_columns                     y-FFT, vertical solve, inverse y-FFT
+ *   all-to-all back (perform_backwards_3dfft, pencilfft.F90:147-159)
+ *   mgpu_slab_fft_x(inverse)                    pressure on the interior rows
+ *   halo exchange of MGPU_HALO_PRESSURE (depth >= 1)
+ *   mgpu_step_phase(PSTEP)                      pressure step, swap_smooth, timestep + 1
+ *
+ * which replaces the halo_swapper component (haloswapper.F90:62-71 over
+ * halocommunication.F90:109-163) and fftsolver's pencil transposes.  All buffers are device
+ * memory of the model's precision (double for MGPU_FP64, float for MGPU_FP32_MIXED; spectra are
+ * interleaved complex of that type) and all work is queued on mgpu_stream(h).  The decomposed
+ * step computes each interior point with the operations of the single-domain step; with
+ * reproducible = 1 an FP64 decomposed run equals the single-domain run bit for bit. */
+
+/* Set the slab geometry: ny_global (power of two) rows in all, `halo` rows each side, at most
+ * max_cols kx columns per mgpu_slab_solve_columns call.  Builds the pivots and twiddles of the
+ * (nx, ny_global) solve.  Needs ny - 2*halo even, >= max(halo, 2). */
+int mgpu_slab_init(mgpu_handle* h, int32_t ny_global, int32_t halo, int32_t max_cols);
+
+#define MGPU_PHASE_SUBGRID   0
+#define MGPU_PHASE_DYNAMICS  1
+#define MGPU_PHASE_PSTEP     2
+int mgpu_step_phase(mgpu_handle* h, int32_t phase);
+
+/* Halo rows.  Sets: MGPU_HALO_STATE = u v w th zu zv zw zth, then q(n), zq(n) for each q field;
+ * MGPU_HALO_PRESSURE = p.  Buffers lo and hi are [nfields][nz][depth][nx] (nfields from
+ * mgpu_halo_fields).  Pack copies the first `depth` interior rows into lo (for the slab below)
+ * and the last `depth` into hi (for the slab above); unpack writes lo (received from the slab
+ * below) into the rows just under the interior and hi (from the slab above) into the rows just
+ * over it.  One kernel launch each. */
+#define MGPU_HALO_STATE     0
+#define MGPU_HALO_PRESSURE  1
+int mgpu_halo_fields(mgpu_handle* h, int32_t set);
+int mgpu_halo_pack(mgpu_handle* h, int32_t set, int32_t depth, void* d_lo, void* d_hi);
+int mgpu_halo_unpack(mgpu_handle* h, int32_t set, int32_t depth, const void* d_lo, const void* d_hi);
+
+/* FP32-mixed: means of th and of each q field per level over the slab's interior rows into
+ * d_means (device FP64 [1 + number_q_fields][nz + 2], level k at column k).  The next dynamics
+ * phase reads d_means as the domain means, so the caller averages it over the slabs in place
+ * (equal slabs: the mean of the slab means) before that phase. */
+int mgpu_slab_level_means(mgpu_handle* h, double* d_means);
+
+/* x-FFT (fftsolver.F90:50-309 transforms, x pass) between the interior rows of p and d_spec,
+ * which is split into nblocks (<= nx/2+1) blocks of consecutive wavenumbers dealt out as evenly
+ * as possible: with b = (nx/2+1) / nblocks and r = (nx/2+1) % nblocks, block q has width
+ * w_q = b + (q < r), first wavenumber k0_q = q*b + min(q, r), is [nz][nyl][w_q] complex and starts
+ * at element k0_q*nz*nyl -- exactly the send buffer of an all-to-all that gives rank q the
+ * wavenumbers of block q.  inverse = 1 runs the inverse transform from d_spec back into p's
+ * interior rows. */
+int mgpu_slab_fft_x(mgpu_handle* h, void* d_spec, int32_t nblocks, int32_t inverse);
+
+/* The rest of the solve on the global wavenumbers kx0 .. kx0+nkx-1 (nkx <= max_cols): forward
+ * y-FFT over all ny_global rows, the vertical tridiagonal solve per (kx, ky) (fftsolver.F90:
+ * 259-309; transpose = 1 applies its transpose, as mgpu_fftsolver_adjoint does), inverse y-FFT.
+ * d_spec holds the rows in blocks of row_block rows: block b is [nz][row_block][nkx] complex and
+ * starts at element b*nz*row_block*nkx -- the receive buffer of the all-to-all, block b coming
+ * from the slab with rows b*row_block .. (b+1)*row_block-1. */
+int mgpu_slab_solve_columns(mgpu_handle* h, void* d_spec, int32_t kx0, int32_t nkx, int32_t row_block,
+                            int32_t transpose);
 
 const char* mgpu_last_error(mgpu_handle* h);
 

@@ -149,6 +149,22 @@ def lib():
     L.mgpu_adjoint_run.restype = C.c_int
     L.mgpu_last_error.argtypes = [C.c_void_p]
     L.mgpu_last_error.restype = C.c_char_p
+    L.mgpu_slab_init.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
+    L.mgpu_slab_init.restype = C.c_int
+    L.mgpu_step_phase.argtypes = [C.c_void_p, C.c_int32]
+    L.mgpu_step_phase.restype = C.c_int
+    L.mgpu_halo_fields.argtypes = [C.c_void_p, C.c_int32]
+    L.mgpu_halo_fields.restype = C.c_int
+    for name in ("mgpu_halo_pack", "mgpu_halo_unpack"):
+        f = getattr(L, name)
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+    L.mgpu_slab_level_means.argtypes = [C.c_void_p, C.c_void_p]
+    L.mgpu_slab_level_means.restype = C.c_int
+    L.mgpu_slab_fft_x.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
+    L.mgpu_slab_fft_x.restype = C.c_int
+    L.mgpu_slab_solve_columns.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+    L.mgpu_slab_solve_columns.restype = C.c_int
     _lib = L
     return _lib
 
@@ -288,6 +304,35 @@ class Model:
         n = np.zeros(len(STAGES), dtype=np.int64)
         self._check(lib().mgpu_stage_times(self.h, ms.ctypes.data, n.ctypes.data), "stage_times")
         return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(STAGES)}
+
+    # -- one y-slab of a decomposed domain (solver SOLVER_EXTERNAL); buffers are device addresses
+    def slab_init(self, ny_global: int, halo: int, max_cols: int):
+        self._check(lib().mgpu_slab_init(self.h, ny_global, halo, max_cols), "slab_init")
+
+    def step_phase(self, phase: int):
+        self._check(lib().mgpu_step_phase(self.h, phase), f"step_phase {phase}")
+
+    def halo_fields(self, halo_set: int) -> int:
+        n = lib().mgpu_halo_fields(self.h, halo_set)
+        if n < 0:
+            self._check(n, "halo_fields")
+        return n
+
+    def halo_pack(self, halo_set: int, depth: int, lo: int, hi: int):
+        self._check(lib().mgpu_halo_pack(self.h, halo_set, depth, lo, hi), "halo_pack")
+
+    def halo_unpack(self, halo_set: int, depth: int, lo: int, hi: int):
+        self._check(lib().mgpu_halo_unpack(self.h, halo_set, depth, lo, hi), "halo_unpack")
+
+    def slab_level_means(self, means: int):
+        self._check(lib().mgpu_slab_level_means(self.h, means), "slab_level_means")
+
+    def slab_fft_x(self, spec: int, nblocks: int, inverse: bool):
+        self._check(lib().mgpu_slab_fft_x(self.h, spec, nblocks, 1 if inverse else 0), "slab_fft_x")
+
+    def slab_solve_columns(self, spec: int, kx0: int, nkx: int, row_block: int, transpose: bool = False):
+        self._check(lib().mgpu_slab_solve_columns(self.h, spec, kx0, nkx, row_block, 1 if transpose else 0),
+                    "slab_solve_columns")
 
     @property
     def stream(self) -> int:

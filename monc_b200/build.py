@@ -27,6 +27,7 @@ UNITS = [
     ("fft.cu", []),
     ("iter.cu", []),
     ("tlad.cu", []),
+    ("slab.cu", []),
 ]
 
 

@@ -18,6 +18,9 @@ FP64 = 0
 FP32_MIXED = 1
 SOLVER_FFT = 0
 SOLVER_ITERATIVE = 1
+SOLVER_EXTERNAL = 2  # one y-slab of a decomposed domain; the slab driver runs the pressure solve
+PHASE_SUBGRID, PHASE_DYNAMICS, PHASE_PSTEP = 0, 1, 2
+HALO_STATE, HALO_PRESSURE = 0, 1
 ITER_BICGSTAB = 0
 ITER_CG = 1
 

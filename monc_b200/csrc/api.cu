@@ -60,6 +60,10 @@ struct mgpu_handle {
   struct AdWork* ad = nullptr;  // tangent-linear / adjoint arrays, allocated on first use
   double stage_ms[MGPU_NSTAGES] = {};
   int64_t stage_n[MGPU_NSTAGES] = {};
+  // y-slab of a decomposed domain (solver MGPU_SOLVER_EXTERNAL, set up by mgpu_slab_init)
+  int slab_halo = 0, slab_ny_global = 0, slab_cols = 0;
+  FftPlanDev slab;
+  const double* bmean_ext = nullptr;  // FP32-mixed: the domain level means for the next dynamics phase
   std::string err;
 };
 
@@ -197,7 +201,7 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   if (cfg->nx < 4 || cfg->ny < 4 || (cfg->nx % 2) || (cfg->ny % 2) || cfg->nz < 3 || cfg->nz > MGPU_MAX_NZ ||
       cfg->number_q_fields < 0 || cfg->number_q_fields > MGPU_MAX_Q ||
       (cfg->precision != MGPU_FP64 && cfg->precision != MGPU_FP32_MIXED) ||
-      (cfg->solver != MGPU_SOLVER_FFT && cfg->solver != MGPU_SOLVER_ITERATIVE) ||
+      (cfg->solver != MGPU_SOLVER_FFT && cfg->solver != MGPU_SOLVER_ITERATIVE && cfg->solver != MGPU_SOLVER_EXTERNAL) ||
       (cfg->solver == MGPU_SOLVER_FFT && (!pow2(cfg->nx) || !pow2(cfg->ny))) || !(cfg->dtm > 0.0))
     return MGPU_ERR_ARGUMENT;
   int ndev = 0;
@@ -242,7 +246,7 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   if (cfg->solver == MGPU_SOLVER_FFT) {
     rc = fft_plan_create(h->fft, h->sc, h->rs, h->fp32);
     if (rc) { std::fprintf(stderr, "mgpu_create: FFT solver needs power-of-two nx, ny\n"); return cleanup(rc); }
-  } else {
+  } else if (cfg->solver == MGPU_SOLVER_ITERATIVE) {
     int st = MGPU_OK;
     h->iter = iter_create(h->sc, h->rs, h->cfg, h->fp32, &st);
     if (st) return cleanup(st);
@@ -263,6 +267,7 @@ int mgpu_destroy(mgpu_handle* h) {
   for (void* p : h->allocations) cudaFree(p);
   h->allocations.clear();
   if (h->fft.spec) fft_plan_destroy(h->fft);
+  if (h->slab.b1) fft_plan_destroy(h->slab);
   if (h->iter) iter_destroy(h->iter);
   cudaFree(h->prof_d);
   cudaFree(h->lookup_d);
@@ -728,11 +733,12 @@ static int component(mgpu_handle* h, DevState<T>& d, int cid) {
     case MGPU_C_STEPPING_DIRECTION: return MGPU_OK;
     case MGPU_C_HALO_SWAPPER: return MGPU_OK;  // periodic indexing in every kernel replaces the swap
     case MGPU_C_FFTSOLVER:
-      if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model configured for the iterative solver");
+      if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model not configured for the FFT solver");
       fft_solve<T>(h->fft, h->sc, d.p, h->stream, &h->launches);
       break;
     case MGPU_C_ITERATIVESOLVER:
-      if (h->cfg.solver != MGPU_SOLVER_ITERATIVE) return fail(h, MGPU_ERR_UNSUPPORTED, "model configured for the FFT solver");
+      if (h->cfg.solver != MGPU_SOLVER_ITERATIVE)
+        return fail(h, MGPU_ERR_UNSUPPORTED, "model not configured for the iterative solver");
       rc = pressure_solve<T>(h, d.p);
       if (rc) return fail(h, rc, "iterative solve failed");
       break;
@@ -782,6 +788,8 @@ int mgpu_get_profile(mgpu_handle* h, const char* name, double* out, int32_t* n) 
 
 int mgpu_step(mgpu_handle* h, int32_t nsteps) {
   if (!h || nsteps < 0) return MGPU_ERR_ARGUMENT;
+  if (h->cfg.solver == MGPU_SOLVER_EXTERNAL)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "the pressure solve of this model is external: step it with mgpu_step_phase");
   for (int s = 0; s < nsteps; ++s) {
     int rc = h->fp32 ? step_once<float>(h, h->d32) : step_once<double>(h, h->d64);
     if (rc) return rc;
@@ -841,7 +849,7 @@ int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches) {
 
 int mgpu_fftsolver_adjoint(mgpu_handle* h) {
   if (!h) return MGPU_ERR_ARGUMENT;
-  if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model configured for the iterative solver");
+  if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model not configured for the FFT solver");
   if (h->fp32) fft_solve<float>(h->fft, h->sc, h->d32.p, h->stream, &h->launches, nullptr, true);
   else fft_solve<double>(h->fft, h->sc, h->d64.p, h->stream, &h->launches, nullptr, true);
   cudaError_t e = cudaGetLastError();
@@ -863,6 +871,171 @@ int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval
   if (!h || nsteps < 1 || checkpoint_interval < 1) return MGPU_ERR_ARGUMENT;
   if (int rc = ensure_adj(h)) return rc;
   return adjoint_run(h, nsteps, checkpoint_interval, rmlmax_bar);
+}
+
+}  // extern "C"
+
+// ---- y-slab decomposition ----------------------------------------------------------------
+template <typename T>
+static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
+  h->sc.forward = (h->timestep == 1) ? 1 : 0;  // steppingdirection.F90:44-48
+  const bool exact_k = h->cfg.reproducible != 0;
+  switch (phase) {
+    case MGPU_PHASE_SUBGRID:
+      h->launches += exact_k ? exact::launch_fused_subgrid<T>(h->sc, d, h->stream)
+                             : fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
+      return MGPU_OK;
+    case MGPU_PHASE_DYNAMICS:
+      if (sizeof(T) == 4) {
+        if (!h->bmean_ext)
+          return fail(h, MGPU_ERR_ARGUMENT, "FP32-mixed slab: mgpu_slab_level_means must precede each dynamics phase");
+        h->sc.bmean = h->bmean_ext;
+      }
+      h->launches += exact_k ? exact::launch_fused_dynamics<T>(h->sc, d, h->stream, nullptr)
+                             : fast::launch_fused_dynamics<T>(h->sc, d, h->stream, nullptr);
+      h->sc.bmean = nullptr;
+      h->bmean_ext = nullptr;
+      swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
+      if (exact_k) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
+      else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
+      h->launches += 1;
+      return MGPU_OK;
+    case MGPU_PHASE_PSTEP:
+      if (exact_k) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+      else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+      h->launches += 1;
+      h->timestep += 1;
+      return MGPU_OK;
+  }
+  return fail(h, MGPU_ERR_ARGUMENT, "unknown step phase");
+}
+
+template <typename T>
+static int halo_set(mgpu_handle* h, DevState<T>& d, int set, T** f) {
+  int n = 0;
+  if (set == MGPU_HALO_STATE) {
+    T* st[8] = {d.u, d.v, d.w, d.th, d.zu, d.zv, d.zw, d.zth};
+    for (T* p : st) f[n++] = p;
+    for (int q = 0; q < h->cfg.number_q_fields; ++q) {
+      f[n++] = d.q[q];
+      f[n++] = d.zq[q];
+    }
+    return n;
+  }
+  if (set == MGPU_HALO_PRESSURE) {
+    f[n++] = d.p;
+    return n;
+  }
+  return -1;
+}
+
+template <typename T>
+static int halo_rows(mgpu_handle* h, DevState<T>& d, int set, int depth, void* lo, void* hi, bool unpack) {
+  T* f[8 + 2 * MGPU_MAX_Q];
+  const int n = halo_set<T>(h, d, set, f);
+  if (n < 0) return fail(h, MGPU_ERR_ARGUMENT, "unknown halo set");
+  const int H = h->slab_halo, ny = h->cfg.ny;
+  // pack the first and last `depth` interior rows; unpack into the rows just outside them
+  const int r_lo = unpack ? H - depth : H, r_hi = unpack ? ny - H : ny - H - depth;
+  launch_halo_rows<T>(h->sc, f, n, depth, r_lo, r_hi, static_cast<T*>(lo), static_cast<T*>(hi), unpack, h->stream);
+  h->launches += 1;
+  return MGPU_OK;
+}
+
+static int check_launch(mgpu_handle* h) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return MGPU_OK;
+}
+
+extern "C" {
+
+int mgpu_slab_init(mgpu_handle* h, int32_t ny_global, int32_t halo, int32_t max_cols) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  if (h->cfg.solver != MGPU_SOLVER_EXTERNAL)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "a slab model is created with solver MGPU_SOLVER_EXTERNAL");
+  if (h->slab.b1) return fail(h, MGPU_ERR_ARGUMENT, "slab already initialised");
+  const int nyl = h->cfg.ny - 2 * halo, nxh = h->cfg.nx / 2 + 1;
+  auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
+  if (halo < 1 || nyl < 2 || nyl < halo || (nyl % 2) || !pow2(h->cfg.nx) || !pow2(ny_global) || nyl > ny_global ||
+      max_cols < 1 || max_cols > nxh)
+    return fail(h, MGPU_ERR_ARGUMENT,
+                "slab needs halo >= 1, an even number of interior rows (ny - 2*halo) >= max(halo, 2) and <= ny_global, "
+                "power-of-two nx and ny_global, and 1 <= max_cols <= nx/2+1");
+  int rc = fft_slab_plan_create(h->slab, h->sc, h->rs, ny_global, max_cols);
+  if (rc) {
+    fft_plan_destroy(h->slab);
+    return fail(h, rc, "slab plan");
+  }
+  h->slab_halo = halo;
+  h->slab_ny_global = ny_global;
+  h->slab_cols = max_cols;
+  return MGPU_OK;
+}
+
+int mgpu_step_phase(mgpu_handle* h, int32_t phase) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  if (h->cfg.solver != MGPU_SOLVER_EXTERNAL)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "phases are for models with an external pressure solve");
+  int rc = h->fp32 ? step_phase<float>(h, h->d32, phase) : step_phase<double>(h, h->d64, phase);
+  return rc ? rc : check_launch(h);
+}
+
+int mgpu_halo_fields(mgpu_handle* h, int32_t set) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  if (set == MGPU_HALO_STATE) return 8 + 2 * h->cfg.number_q_fields;
+  if (set == MGPU_HALO_PRESSURE) return 1;
+  return fail(h, MGPU_ERR_ARGUMENT, "unknown halo set");
+}
+
+static int halo_entry(mgpu_handle* h, int32_t set, int32_t depth, void* lo, void* hi, bool unpack) {
+  if (!h || !lo || !hi) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (depth < 1 || depth > h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "halo depth out of range");
+  int rc = h->fp32 ? halo_rows<float>(h, h->d32, set, depth, lo, hi, unpack)
+                   : halo_rows<double>(h, h->d64, set, depth, lo, hi, unpack);
+  return rc ? rc : check_launch(h);
+}
+
+int mgpu_halo_pack(mgpu_handle* h, int32_t set, int32_t depth, void* d_lo, void* d_hi) {
+  return halo_entry(h, set, depth, d_lo, d_hi, false);
+}
+
+int mgpu_halo_unpack(mgpu_handle* h, int32_t set, int32_t depth, const void* d_lo, const void* d_hi) {
+  return halo_entry(h, set, depth, const_cast<void*>(d_lo), const_cast<void*>(d_hi), true);
+}
+
+int mgpu_slab_level_means(mgpu_handle* h, double* d_means) {
+  if (!h || !d_means) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (h->fp32) launch_level_means<float>(h->sc, h->d32.th, h->d32.q, h->cfg.number_q_fields, d_means, h->stream, h->slab_halo);
+  else launch_level_means<double>(h->sc, h->d64.th, h->d64.q, h->cfg.number_q_fields, d_means, h->stream, h->slab_halo);
+  h->launches += 1;
+  h->bmean_ext = d_means;
+  return check_launch(h);
+}
+
+int mgpu_slab_fft_x(mgpu_handle* h, void* d_spec, int32_t nblocks, int32_t inverse) {
+  if (!h || !d_spec) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (nblocks < 1 || nblocks > h->cfg.nx / 2 + 1) return fail(h, MGPU_ERR_ARGUMENT, "nblocks out of range");
+  if (h->fp32) slab_fft_x<float>(h->slab, h->sc, h->d32.p, h->slab_halo, nblocks, d_spec, inverse != 0, h->stream, &h->launches);
+  else slab_fft_x<double>(h->slab, h->sc, h->d64.p, h->slab_halo, nblocks, d_spec, inverse != 0, h->stream, &h->launches);
+  return check_launch(h);
+}
+
+int mgpu_slab_solve_columns(mgpu_handle* h, void* d_spec, int32_t kx0, int32_t nkx, int32_t row_block,
+                            int32_t transpose) {
+  if (!h || !d_spec) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (kx0 < 0 || nkx < 1 || nkx > h->slab_cols || kx0 + nkx > h->cfg.nx / 2 + 1 || row_block < 1 ||
+      h->slab_ny_global % row_block)
+    return fail(h, MGPU_ERR_ARGUMENT, "column block or row block out of range");
+  if (h->fp32)
+    slab_solve_columns<float>(h->slab, h->sc, d_spec, kx0, nkx, row_block, transpose != 0, h->stream, &h->launches);
+  else
+    slab_solve_columns<double>(h->slab, h->sc, d_spec, kx0, nkx, row_block, transpose != 0, h->stream, &h->launches);
+  return check_launch(h);
 }
 
 int mgpu_mean_profile(mgpu_handle* h, int32_t id, double* out) {

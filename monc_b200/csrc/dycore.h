@@ -56,9 +56,31 @@ template <typename T>
 void fft_solve(const FftPlanDev& plan, const Scalars& s, T* p, cudaStream_t st, int64_t* launches,
                cudaEvent_t* evs = nullptr, bool transpose = false);
 
-// horizontal means of th (row 0) and q[0..nq-1] (rows 1..nq) per level into out[row*(nz+2) + k]
+// horizontal means of th (row 0) and q[0..nq-1] (rows 1..nq) per level into out[row*(nz+2) + k],
+// over the rows halo .. ny-halo-1 (all rows for halo 0)
 template <typename T>
-void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st);
+void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st,
+                        int halo = 0);
+
+// y-slab decomposition.  A slab plan holds the pivots and twiddles of the global grid (nx,
+// ny_global) and Thomas scratch for max_cols kx columns; the spectra are the caller's.
+int fft_slab_plan_create(FftPlanDev& plan, const Scalars& s, const RefState& rs, int ny_global, int max_cols);
+// x-FFT between the slab's interior rows halo .. ny-halo-1 of p and a spectrum split into nblk
+// blocks of consecutive wavenumbers, the first (nx/2+1) % nblk one wider than the rest: block q
+// covers k0_q .. k0_q+w_q-1, is [nz][ny-2*halo][w_q] and starts at k0_q*nz*(ny-2*halo)
+template <typename T>
+void slab_fft_x(const FftPlanDev& plan, const Scalars& s, T* p, int halo, int nblk, void* spec, bool inverse,
+                cudaStream_t st, int64_t* launches);
+// forward y-FFT, vertical solve (or its transpose) and inverse y-FFT of the global wavenumbers
+// kx0 .. kx0+nkx-1 over all plan.ny rows, held in row blocks of rpb rows: block b is [nz][rpb][nkx]
+template <typename T>
+void slab_solve_columns(const FftPlanDev& plan, const Scalars& s, void* spec, int kx0, int nkx, int rpb, bool transpose,
+                        cudaStream_t st, int64_t* launches);
+// rows [r_lo, r_lo+depth) and [r_hi, r_hi+depth) of every level of the n fields f[] to (pack) or
+// from (unpack) the buffers lo and hi, each [n][nz][depth][nx]
+template <typename T>
+void launch_halo_rows(const Scalars& s, T* const* f, int n, int depth, int r_lo, int r_hi, T* lo, T* hi, bool unpack,
+                      cudaStream_t st);
 
 template <typename T>
 void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st);

@@ -19,6 +19,8 @@
 #include <cstdio>
 #include <vector>
 
+#include <mutex>
+
 #include "dycore.h"
 
 namespace mgpu {
@@ -77,10 +79,36 @@ __device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int 
   }
 }
 
+// Offset of wavenumber m of row j, level k in an x-spectrum split into nblk blocks of
+// consecutive wavenumbers: the nxh wavenumbers are dealt out as evenly as possible, the first
+// nxh % nblk blocks one wider.  Block q covers k0_q .. k0_q+w_q-1, is [nz][ny][w_q] and starts at
+// k0_q*nz*ny, so the blocks lie end to end.  *w receives w_q (the row stride inside the block).
+__device__ __forceinline__ long long spec_x_offset(int m, int nxh, int nblk, int ny, int nz, int k, int j, int* w) {
+  int k0 = 0, c = m, wq = nxh;
+  if (nblk > 1) {
+    const int b = nxh / nblk, rem = nxh - b * nblk, split = rem * (b + 1);
+    if (m < split) {
+      const int q = m / (b + 1);
+      k0 = q * (b + 1);
+      wq = b + 1;
+    } else {
+      const int q = (m - split) / b;
+      k0 = split + q * b;
+      wq = b;
+    }
+    c = m - k0;
+  }
+  *w = wq;
+  return (long long)k0 * nz * ny + ((long long)(k - 1) * ny + j) * wq + c;
+}
+
 // ---- forward x: real rows (k, j), (k, j+1) -> half spectra ------------------------------
 template <typename T>
+// ny rows of each level are transformed: rows p_row0 .. p_row0+ny-1 of p, which holds p_rows rows
+// per level (a y-slab with halo rows has p_rows > ny).  The spectrum is split into nblk blocks of
+// consecutive wavenumbers (see spec_x_offset); nblk = 1 gives the plain [nz][ny][nx/2+1] layout.
 __global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g,
-                            int nx, int ny, int nz, int logn, int rows_per_cta) {
+                            int nx, int ny, int nz, int logn, int rows_per_cta, int p_rows, int p_row0, int nblk) {
   typedef typename Cx<T>::t C;
   extern __shared__ unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
@@ -98,7 +126,7 @@ __global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restri
     if (pr < npairs) {
       int k = (int)(pr / pairs_per_level) + 1;
       int j = 2 * (int)(pr % pairs_per_level);
-      const T* row = p + (long long)(k - 1) * nx * ny + (long long)j * nx;
+      const T* row = p + (long long)(k - 1) * nx * p_rows + (long long)(p_row0 + j) * nx;
       z.x = row[e];
       z.y = row[nx + e];
     } else {
@@ -122,16 +150,18 @@ __global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restri
     a.y = (T)0.5 * (zm.y - zn.y);
     b.x = (T)0.5 * (zm.y + zn.y);
     b.y = (T)0.5 * (zn.x - zm.x);
-    C* out = spec + (long long)(k - 1) * ny * nxh + (long long)j * nxh;
-    out[m] = a;
-    out[nxh + m] = b;
+    int w;
+    C* out = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, j, &w);
+    out[0] = a;
+    out[w] = b;
   }
 }
 
 // ---- inverse x: half spectra -> real rows (k, j), (k, j+1) -----------------------------
 template <typename T>
+// the inverse of k_fft_x_fwd, with the same row window and spectrum blocks
 __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g,
-                            int nx, int ny, int nz, int logn, int rows_per_cta) {
+                            int nx, int ny, int nz, int logn, int rows_per_cta, int p_rows, int p_row0, int nblk) {
   typedef typename Cx<T>::t C;
   extern __shared__ unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
@@ -149,9 +179,10 @@ __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restri
     if (pr < npairs) {
       int k = (int)(pr / pairs_per_level) + 1;
       int j = 2 * (int)(pr % pairs_per_level);
-      const C* in = spec + (long long)(k - 1) * ny * nxh + (long long)j * nxh;
-      a = in[m];
-      b = in[nxh + m];
+      int w;
+      const C* in = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, j, &w);
+      a = in[0];
+      b = in[w];
     } else {
       a.x = a.y = b.x = b.y = (T)0;
     }
@@ -177,7 +208,7 @@ __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restri
     if (pr >= npairs) continue;
     int k = (int)(pr / pairs_per_level) + 1;
     int j = 2 * (int)(pr % pairs_per_level);
-    T* row = p + (long long)(k - 1) * nx * ny + (long long)j * nx;
+    T* row = p + (long long)(k - 1) * nx * p_rows + (long long)(p_row0 + j) * nx;
     C z = buf[r * prow + pidx(e)];
     row[e] = z.x * sc;
     row[nx + e] = z.y * sc;
@@ -185,22 +216,30 @@ __global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restri
 }
 
 // ---- complex FFT along y on a tile of kx columns ------------------------------------------
+// The spectrum holds ncols kx columns per row (nx/2+1, or one block of them after a transpose) and
+// its ny rows in blocks of rpb rows: block b is [nz][rpb][ncols] and starts at b*nz*rpb*ncols.
+// rpb = ny gives the plain [nz][ny][ncols] layout.
+__device__ __forceinline__ long long spec_row(int e, int k, int rpb, int ncols, int nz) {
+  const int b = e < rpb ? 0 : e / rpb;
+  return ((long long)b * nz + (k - 1)) * rpb * ncols + (long long)(e - b * rpb) * ncols;
+}
+
 template <typename T>
-__global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g, int nx, int ny, int logn,
-                        int cols, bool inverse) {
+__global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g, int ncols, int ny, int logn,
+                        int cols, bool inverse, int nz, int rpb) {
   typedef typename Cx<T>::t C;
   extern __shared__ unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* buf = tw + ny / 2;
   for (int t = threadIdx.x; t < ny / 2; t += blockDim.x) tw[t] = tw_g[t];
-  const int nxh = nx / 2 + 1;
+  const int nxh = ncols;
   const int kx0 = blockIdx.x * cols;
   const int k = blockIdx.y + 1;
-  C* base = spec + (long long)(k - 1) * ny * nxh;
+  C* base = spec + kx0;
   for (int t = threadIdx.x; t < cols * ny; t += blockDim.x) {
     int e = t / cols, c = t - e * cols;
     C z;
-    if (kx0 + c < nxh) z = base[(long long)e * nxh + kx0 + c];
+    if (kx0 + c < nxh) z = base[spec_row(e, k, rpb, ncols, nz) + c];
     else { z.x = (T)0; z.y = (T)0; }
     buf[(__brev(e) >> (32 - logn)) * cols + c] = z;
   }
@@ -214,32 +253,37 @@ __global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<
     C z = buf[e * cols + c];
     z.x = z.x * sc;
     z.y = z.y * sc;
-    base[(long long)e * nxh + kx0 + c] = z;
+    base[spec_row(e, k, rpb, ncols, nz) + c] = z;
   }
 }
 
 // ---- vertical tridiagonal per (ky, kx) in FP64 ----------------------------------------------
 template <typename T>
+// The spectrum holds ncols kx columns per row, the global wavenumbers kx0 .. kx0+ncols-1 (all
+// nx/2+1 of them, or one rank's block after a transpose), and its rows in blocks of rpb as in
+// k_fft_y.  s1buf is [nz][ny][ncols] whatever the spectrum layout.
 __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
-                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose) {
+                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose,
+                          int ncols, int kx0, int rpb) {
   typedef typename Cx<T>::t C;
   const int nxh = nx / 2 + 1;
   long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= (long long)ny * nxh) return;
-  int ky = (int)(col / nxh), kx = (int)(col - (long long)ky * nxh);
-  const long long plane = (long long)ny * nxh;
+  if (col >= (long long)ny * ncols) return;
+  const int ky = (int)(col / ncols), c = (int)(col - (long long)ky * ncols), kx = kx0 + c;
+  const long long plane = (long long)ny * ncols;      // level stride of s1buf
+  const long long lstride = (long long)rpb * ncols;   // level stride of the spectrum
   const double* czb = prof + P_CZB * prof_stride;
   const double* cza = prof + P_CZA * prof_stride;
   const double* czg = prof + P_CZG * prof_stride;
-  C* sp = spec + col;
+  C* sp = spec + spec_row(ky, 1, rpb, ncols, nz) + c;
   if (transpose && kx == 0 && ky == 0) {
     // transpose of the mean-mode recurrence below: the rows r = 2..nz-1 of
     // cza(r) p(r+1) + czg(r) p(r) + czb(r) p(r-1) = b(r), p(1) = p(2) = 0, solved from the top
     double zr1 = 0.0, zi1 = 0.0, zr2 = 0.0, zi2 = 0.0;  // z(u), z(u+1)
-    C ynext = sp[(long long)(nz - 1) * plane];           // y(nz)
+    C ynext = sp[(long long)(nz - 1) * lstride];           // y(nz)
     for (int u = nz; u >= 3; --u) {
       const C yu = ynext;
-      if (u >= 4) ynext = sp[(long long)(u - 2) * plane];  // y(u-1), read before z(u-1) overwrites it
+      if (u >= 4) ynext = sp[(long long)(u - 2) * lstride];  // y(u-1), read before z(u-1) overwrites it
       double yr = (double)yu.x, yi = (double)yu.y;
       if (u <= nz - 1) { yr -= czg[u] * zr1; yi -= czg[u] * zi1; }
       if (u + 1 <= nz - 1) { yr -= czb[u + 1] * zr2; yi -= czb[u + 1] * zi2; }
@@ -248,13 +292,13 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
       C o;
       o.x = (T)zr;
       o.y = (T)zi;
-      sp[(long long)(u - 2) * plane] = o;
+      sp[(long long)(u - 2) * lstride] = o;
     }
     C zero;
     zero.x = (T)0;
     zero.y = (T)0;
     sp[0] = zero;
-    sp[(long long)(nz - 1) * plane] = zero;
+    sp[(long long)(nz - 1) * lstride] = zero;
     return;
   }
   // the transposed tridiagonal has the same pivots (they depend on czb(k)*cza(k-1) only) with
@@ -263,16 +307,16 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   const double* up = transpose ? czb + 1 : cza;  // up[k]: coefficient of p(k+1) in row k
   if (kx == 0 && ky == 0) {
     // horizontal-mean mode: upward recurrence from p(1) = p(2) = 0
-    C v2 = sp[plane];
+    C v2 = sp[lstride];
     double sr_prev = (double)v2.x, si_prev = (double)v2.y;
     double pr2 = 0.0, pi2 = 0.0, pr1 = 0.0, pi1 = 0.0;  // p(k-2), p(k-1)
     C zero;
     zero.x = (T)0;
     zero.y = (T)0;
     sp[0] = zero;  // p(1) = p(2) = 0 for the mean mode
-    sp[plane] = zero;
+    sp[lstride] = zero;
     for (int k = 3; k <= nz; ++k) {
-      C vk = sp[(long long)(k - 1) * plane];
+      C vk = sp[(long long)(k - 1) * lstride];
       double pr = (sr_prev - czg[k - 1] * pr1 - czb[k - 1] * pr2) / cza[k - 1];
       double pi = (si_prev - czg[k - 1] * pi1 - czb[k - 1] * pi2) / cza[k - 1];
       sr_prev = (double)vk.x;
@@ -280,7 +324,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
       C o;
       o.x = (T)pr;
       o.y = (T)pi;
-      sp[(long long)(k - 1) * plane] = o;
+      sp[(long long)(k - 1) * lstride] = o;
       pr2 = pr1; pi2 = pi1; pr1 = pr; pi1 = pi;
     }
     return;
@@ -290,7 +334,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   const double* bcol = b1 + (long long)kyi * nxh + kx;
   // forward elimination s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1), loads batched 8 levels at a time
   constexpr int B = 8;
-  C v = sp[plane];
+  C v = sp[lstride];
   double sr = (double)v.x, si = (double)v.y;
   s1buf[col + plane] = make_double2(sr, si);
   for (int k0 = 3; k0 <= nz; k0 += B) {
@@ -299,7 +343,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
 #pragma unroll
     for (int q = 0; q < B; ++q) {
       int k = k0 + q;
-      if (k <= nz) { vb[q] = sp[(long long)(k - 1) * plane]; bb[q] = __ldg(bcol + (long long)(k - 1) * bstride); }
+      if (k <= nz) { vb[q] = sp[(long long)(k - 1) * lstride]; bb[q] = __ldg(bcol + (long long)(k - 1) * bstride); }
     }
 #pragma unroll
     for (int q = 0; q < B; ++q) {
@@ -317,7 +361,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   C o;
   o.x = (T)pr;
   o.y = (T)pi;
-  sp[(long long)(nz - 1) * plane] = o;
+  sp[(long long)(nz - 1) * lstride] = o;
   for (int k0 = nz - 1; k0 >= 2; k0 -= B) {
     double2 sb[B];
     double bb[B];
@@ -334,7 +378,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
         pi = (sb[q].y - up[k] * pi) * bb[q];
         o.x = (T)pr;
         o.y = (T)pi;
-        sp[(long long)(k - 1) * plane] = o;
+        sp[(long long)(k - 1) * lstride] = o;
       }
     }
   }
@@ -359,31 +403,22 @@ static FftSizes sizes(const FftPlanDev& pl) {
   return z;
 }
 
-int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool fp32) {
-  pl.nx = s.nx;
-  pl.ny = s.ny;
-  pl.nz = s.nz;
-  pl.nxh = s.nx / 2 + 1;
-  auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
-  if (!pow2(s.nx) || !pow2(s.ny) || s.nx > 4096 || s.ny > 4096) return MGPU_ERR_UNSUPPORTED;
-  const size_t plane = (size_t)s.ny * pl.nxh;
-  const size_t cs = fp32 ? sizeof(float2) : sizeof(double2);
-  if (cudaMalloc(&pl.spec, cs * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
-  if (cudaMalloc(&pl.s1, sizeof(double2) * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+// Pivots and twiddles of the (pl.nx, pl.ny, pl.nz) grid; pl.spec and pl.s1 are left to the caller.
+static int plan_tables(FftPlanDev& pl, const RefState& rs) {
   // Thomas pivots per (|ky|, kx), built exactly as fftsolver.F90:259-280 and :72-90
-  const int nyh = s.ny / 2 + 1;
-  std::vector<double> b1((size_t)(s.nz + 1) * nyh * pl.nxh, 0.0);
+  const int nyh = pl.ny / 2 + 1;
+  std::vector<double> b1((size_t)(pl.nz + 1) * nyh * pl.nxh, 0.0);
   const double PI = 4.0 * std::atan(1.0);
   std::vector<double> cosx(pl.nxh), cosy(nyh);
-  for (int m = 0; m < pl.nxh; ++m) cosx[m] = (2.0 / (rs.dx * rs.dx)) * (std::cos(2.0 * PI * (double)m / (double)s.nx) - 1.0);
-  for (int m = 0; m < nyh; ++m) cosy[m] = (2.0 / (rs.dy * rs.dy)) * (std::cos(2.0 * PI * (double)m / (double)s.ny) - 1.0);
+  for (int m = 0; m < pl.nxh; ++m) cosx[m] = (2.0 / (rs.dx * rs.dx)) * (std::cos(2.0 * PI * (double)m / (double)pl.nx) - 1.0);
+  for (int m = 0; m < nyh; ++m) cosy[m] = (2.0 / (rs.dy * rs.dy)) * (std::cos(2.0 * PI * (double)m / (double)pl.ny) - 1.0);
   for (int ky = 0; ky < nyh; ++ky)
     for (int kx = 0; kx < pl.nxh; ++kx) {
       double cij = cosx[kx] + cosy[ky];
       double b = cij - rs.cza[2];
       double prev = 1.0 / b;
       b1[((size_t)2 * nyh + ky) * pl.nxh + kx] = prev;
-      for (int k = 3; k <= s.nz; ++k) {
+      for (int k = 3; k <= pl.nz; ++k) {
         double bk = cij + rs.czg[k];
         prev = 1.0 / (bk - rs.czh[k] * prev);
         b1[((size_t)k * nyh + ky) * pl.nxh + kx] = prev;
@@ -406,11 +441,17 @@ int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool f
     cudaMemcpy(*dd, t.data(), n * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(*df, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice);
   };
-  twiddles(s.nx, &pl.twx, &pl.twx_f);
-  twiddles(s.ny, &pl.twy, &pl.twy_f);
+  twiddles(pl.nx, &pl.twx, &pl.twx_f);
+  twiddles(pl.ny, &pl.twy, &pl.twy_f);
   FftSizes zd = sizes<double>(pl), zf = sizes<float>(pl);
   size_t mx = std::max(std::max(zd.smem_x, zd.smem_y), std::max(zf.smem_x, zf.smem_y));
-  if (mx > 48 * 1024) {
+  // the attribute belongs to the kernel, not to the plan: only ever raise it, so that a smaller
+  // plan created later does not cut the limit an earlier, larger one needs
+  static std::mutex mu;
+  static size_t raised = 48 * 1024;
+  std::lock_guard<std::mutex> lock(mu);
+  if (mx > raised) {
+    raised = mx;
     cudaFuncSetAttribute(k_fft_x_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
     cudaFuncSetAttribute(k_fft_x_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
     cudaFuncSetAttribute(k_fft_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
@@ -419,6 +460,32 @@ int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool f
     cudaFuncSetAttribute(k_fft_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
   }
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
+}
+
+int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool fp32) {
+  pl.nx = s.nx;
+  pl.ny = s.ny;
+  pl.nz = s.nz;
+  pl.nxh = s.nx / 2 + 1;
+  auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
+  if (!pow2(s.nx) || !pow2(s.ny) || s.nx > 4096 || s.ny > 4096) return MGPU_ERR_UNSUPPORTED;
+  const size_t plane = (size_t)s.ny * pl.nxh;
+  const size_t cs = fp32 ? sizeof(float2) : sizeof(double2);
+  if (cudaMalloc(&pl.spec, cs * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+  if (cudaMalloc(&pl.s1, sizeof(double2) * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+  return plan_tables(pl, rs);
+}
+
+int fft_slab_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, int ny_global, int max_cols) {
+  pl.nx = s.nx;
+  pl.ny = ny_global;
+  pl.nz = s.nz;
+  pl.nxh = s.nx / 2 + 1;
+  auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
+  if (!pow2(s.nx) || !pow2(ny_global) || s.nx > 4096 || ny_global > 4096 || max_cols < 1 || max_cols > pl.nxh)
+    return MGPU_ERR_UNSUPPORTED;
+  if (cudaMalloc(&pl.s1, sizeof(double2) * (size_t)ny_global * max_cols * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+  return plan_tables(pl, rs);
 }
 
 void fft_plan_destroy(FftPlanDev& pl) {
@@ -447,24 +514,67 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   double2* s1 = pl.s1;
   auto mark = [&](int q) { if (evs) cudaEventRecord(evs[q], st); };
   mark(0);
-  k_fft_x_fwd<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x);
+  k_fft_x_fwd<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x, s.ny, 0, 1);
   mark(1);
   dim3 gy((pl.nxh + z.cols_y - 1) / z.cols_y, s.nz);
-  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, s.nx, s.ny, z.logy, z.cols_y, false);
+  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, false, s.nz, s.ny);
   mark(2);
   long long ncol = (long long)plane;
   k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
-                                                               transpose ? 1 : 0);
+                                                               transpose ? 1 : 0, pl.nxh, 0, s.ny);
   mark(3);
-  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, s.nx, s.ny, z.logy, z.cols_y, true);
+  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, true, s.nz, s.ny);
   mark(4);
-  k_fft_x_inv<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x);
+  k_fft_x_inv<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x, s.ny, 0, 1);
   mark(5);
   *launches += 5;
 }
 
 template void fft_solve<double>(const FftPlanDev&, const Scalars&, double*, cudaStream_t, int64_t*, cudaEvent_t*, bool);
 template void fft_solve<float>(const FftPlanDev&, const Scalars&, float*, cudaStream_t, int64_t*, cudaEvent_t*, bool);
+
+// ---- y-slab decomposition: the solve split at the two transposes -------------------------
+template <typename T>
+void slab_fft_x(const FftPlanDev& pl, const Scalars& s, T* p, int halo, int nblk, void* spec, bool inverse,
+                cudaStream_t st, int64_t* launches) {
+  typedef typename Cx<T>::t C;
+  const bool f32 = sizeof(T) == 4;
+  FftSizes z = sizes<T>(pl);
+  const C* twx = reinterpret_cast<const C*>(f32 ? (void*)pl.twx_f : (void*)pl.twx);
+  C* sp = reinterpret_cast<C*>(spec);
+  const int nyl = s.ny - 2 * halo;
+  const long long npairs = (long long)s.nz * (nyl / 2);
+  const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
+  if (!inverse)
+    k_fft_x_fwd<T><<<gx, 256, z.smem_x, st>>>(p, sp, twx, s.nx, nyl, s.nz, z.logx, z.rows_x, s.ny, halo, nblk);
+  else
+    k_fft_x_inv<T><<<gx, 256, z.smem_x, st>>>(p, sp, twx, s.nx, nyl, s.nz, z.logx, z.rows_x, s.ny, halo, nblk);
+  *launches += 1;
+}
+
+template <typename T>
+void slab_solve_columns(const FftPlanDev& pl, const Scalars& s, void* spec, int kx0, int nkx, int rpb, bool transpose,
+                        cudaStream_t st, int64_t* launches) {
+  typedef typename Cx<T>::t C;
+  const bool f32 = sizeof(T) == 4;
+  FftSizes z = sizes<T>(pl);
+  const C* twy = reinterpret_cast<const C*>(f32 ? (void*)pl.twy_f : (void*)pl.twy);
+  C* sp = reinterpret_cast<C*>(spec);
+  dim3 gy((nkx + z.cols_y - 1) / z.cols_y, s.nz);
+  const long long ncol = (long long)pl.ny * nkx;
+  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, false, s.nz, rpb);
+  k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(sp, pl.s1, pl.b1, s.prof, s.nz + 2, pl.nx, pl.ny, s.nz,
+                                                               transpose ? 1 : 0, nkx, kx0, rpb);
+  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, true, s.nz, rpb);
+  *launches += 3;
+}
+
+template void slab_fft_x<double>(const FftPlanDev&, const Scalars&, double*, int, int, void*, bool, cudaStream_t, int64_t*);
+template void slab_fft_x<float>(const FftPlanDev&, const Scalars&, float*, int, int, void*, bool, cudaStream_t, int64_t*);
+template void slab_solve_columns<double>(const FftPlanDev&, const Scalars&, void*, int, int, int, bool, cudaStream_t,
+                                         int64_t*);
+template void slab_solve_columns<float>(const FftPlanDev&, const Scalars&, void*, int, int, int, bool, cudaStream_t,
+                                        int64_t*);
 
 // ---- horizontal-mean diagnostics: one block per level, FP64 accumulation in a fixed order ----
 template <typename T>
@@ -508,11 +618,13 @@ struct MeanFields {
   const T* f[1 + MGPU_MAX_Q];
 };
 template <typename T>
-__global__ void k_level_means(MeanFields<T> mf, long long plane, int stride, double* out) {
+// the mean over `count` points of each level starting `off` points into the level
+__global__ void k_level_means(MeanFields<T> mf, long long plane, long long off, long long count, int stride,
+                              double* out) {
   const int k = blockIdx.x + 1, row = blockIdx.y;
-  const T* fk = mf.f[row] + (long long)(k - 1) * plane;
+  const T* fk = mf.f[row] + (long long)(k - 1) * plane + off;
   double a = 0.0;
-  for (long long t = threadIdx.x; t < plane; t += blockDim.x) a += (double)fk[t];
+  for (long long t = threadIdx.x; t < count; t += blockDim.x) a += (double)fk[t];
   __shared__ double sa[256];
   sa[threadIdx.x] = a;
   __syncthreads();
@@ -520,17 +632,18 @@ __global__ void k_level_means(MeanFields<T> mf, long long plane, int stride, dou
     if ((int)threadIdx.x < h) sa[threadIdx.x] += sa[threadIdx.x + h];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[(long long)row * stride + k] = sa[0] / (double)plane;
+  if (threadIdx.x == 0) out[(long long)row * stride + k] = sa[0] / (double)count;
 }
 template <typename T>
-void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st) {
+void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st, int halo) {
   MeanFields<T> mf{};
   mf.f[0] = th;
   for (int n = 0; n < nq; ++n) mf.f[1 + n] = q[n];
-  k_level_means<T><<<dim3(s.nz, 1 + nq), 256, 0, st>>>(mf, s.plane, s.nz + 2, out);
+  k_level_means<T><<<dim3(s.nz, 1 + nq), 256, 0, st>>>(mf, s.plane, (long long)halo * s.nx,
+                                                       (long long)(s.ny - 2 * halo) * s.nx, s.nz + 2, out);
 }
-template void launch_level_means<double>(const Scalars&, const double*, double* const*, int, double*, cudaStream_t);
-template void launch_level_means<float>(const Scalars&, const float*, float* const*, int, double*, cudaStream_t);
+template void launch_level_means<double>(const Scalars&, const double*, double* const*, int, double*, cudaStream_t, int);
+template void launch_level_means<float>(const Scalars&, const float*, float* const*, int, double*, cudaStream_t, int);
 template void launch_diagnostics<float>(const Scalars&, const float*, const float*, double*, double*, cudaStream_t);
 
 }  // namespace mgpu
@@ -546,7 +659,6 @@ template void launch_diagnostics<float>(const Scalars&, const float*, const floa
 // file-scope array below.  That array is part of the library image: every GPU that loads the
 // library holds MGPU_NOALLOC_SCRATCH_BYTES until the process exits.
 // =============================================================================================
-#include <mutex>
 
 #include "../../include/monc_gpu.h"
 
@@ -666,10 +778,10 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   const long long npairs = (long long)nz * (ny / 2);
   const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
   dim3 gy((nxh + z.cols_y - 1) / z.cols_y, nz);
-  k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x);
-  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nx, ny, z.logy, z.cols_y, false);
-  k_tridiag<double><<<(unsigned)((plane + 127) / 128), 128, 0, st>>>(spec, s1, b1, prof, stride, nx, ny, nz, 0);
-  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nx, ny, z.logy, z.cols_y, true);
-  k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x);
+  k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
+  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, false, nz, ny);
+  k_tridiag<double><<<(unsigned)((plane + 127) / 128), 128, 0, st>>>(spec, s1, b1, prof, stride, nx, ny, nz, 0, nxh, 0, ny);
+  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, true, nz, ny);
+  k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
 }

@@ -1,0 +1,318 @@
+"""Y-slab domain decomposition of the dynamical core: one slab of the horizontal domain per GPU.
+
+MONC decomposes the horizontal domain into 2-D blocks of whole columns (decomposition.F90:57-123),
+swaps halos of depth 2 with its neighbours before the dynamics (haloswapper.F90:62-71 over
+halocommunication.F90:109-163) and solves the pressure on pencils reached by all-to-all
+transposes (pencilfft.F90:126-159).  Here the domain is split along y only, so every slab keeps
+whole x rows (x stays periodic inside each model) and the FFT solve needs one transpose each way:
+
+    per step, on every slab
+      halo exchange of the state (u v w th zu zv zw zth q zq), `halo` rows each side
+      subgrid phase
+      FP32-mixed: level means of th and q over the slab, averaged over all slabs
+      dynamics phase (dynamics, scalar swap, pressure source)
+      x-FFT of the interior rows, written straight into per-destination kx blocks
+      all-to-all: rank q receives kx block q of every slab (all rows of its wavenumbers)
+      y-FFT, tridiagonal solve, inverse y-FFT on those columns
+      all-to-all back, inverse x-FFT into the interior rows of p
+      halo exchange of p (1 row each side: the pressure gradient reaches row j+1)
+      pstep phase (pressure step, swap_smooth)
+
+`halo` = 4 rows covers the step's stencil reach: 2 rows for TVD advection and the viscous and
+diffusive fluxes, 1 more for the pressure source, which reads the stepped velocities at j-1.
+Halo rows are recomputed by every phase (with the slab's own periodic wrap) and hold stale
+values until the next exchange; the interior rows never read them beyond that reach.
+
+The exchanges go through a communicator object: `TorchComm` (one slab per process over
+torch.distributed, NCCL between GPUs) or `LoopbackComm` (every slab in this process on one
+device, each exchange a set of device copies made after all queued work has finished; the
+slabs never wait on each other inside a kernel).  With `reproducible` set, an FP64 decomposed
+run reproduces the single-domain run bit for bit: each interior point is computed by the same
+operations on the same values, the x-FFT pairs the same rows (slab heights are even) and the y
+transforms and tridiagonal solves see the same columns.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+from . import api
+from . import config as cf
+
+
+def kx_blocks(nxh: int, nranks: int) -> list[tuple[int, int]]:
+    """Split the nxh = nx/2+1 x-wavenumbers over nranks as mgpu_slab_fft_x does: as evenly as
+    possible, the first nxh % nranks blocks one wider.  Returns [(first wavenumber, width)]."""
+    if nranks > nxh:
+        raise ValueError(f"{nxh} x-wavenumbers cannot be split into {nranks} non-empty blocks")
+    b, r = divmod(nxh, nranks)
+    return [(q * b + min(q, r), b + (1 if q < r else 0)) for q in range(nranks)]
+
+
+@dataclass(frozen=True)
+class SlabGeometry:
+    """Sizes of a y-slab decomposition of an nx x ny x nz domain over nranks slabs."""
+    nx: int
+    ny: int
+    nz: int
+    nranks: int
+    halo: int = 4
+
+    def __post_init__(self):
+        if self.ny % self.nranks:
+            raise ValueError(f"ny={self.ny} is not a multiple of {self.nranks} slabs")
+        nyl = self.ny // self.nranks
+        if nyl % 2 or nyl < max(self.halo, 2):
+            raise ValueError(f"slabs of {nyl} rows: need an even number >= max(halo={self.halo}, 2)")
+        kx_blocks(self.nx // 2 + 1, self.nranks)
+
+    @property
+    def nyl(self) -> int:
+        return self.ny // self.nranks
+
+    @property
+    def nxh(self) -> int:
+        return self.nx // 2 + 1
+
+    @property
+    def blocks(self) -> list[tuple[int, int]]:
+        return kx_blocks(self.nxh, self.nranks)
+
+    def y0(self, rank: int) -> int:
+        return rank * self.nyl
+
+    def rows(self, rank: int) -> np.ndarray:
+        """Global rows held by a slab model, halo rows included (periodic)."""
+        return np.arange(self.y0(rank) - self.halo, self.y0(rank) + self.nyl + self.halo) % self.ny
+
+    # element offsets (complex elements) of the all-to-all blocks
+    def xblock(self, q: int) -> tuple[int, int]:
+        """Block q of a slab's x-spectrum: (offset, length)."""
+        k0, w = self.blocks[q]
+        return k0 * self.nz * self.nyl, self.nz * self.nyl * w
+
+    def tblock(self, rank: int, r: int) -> tuple[int, int]:
+        """Block r (rows of slab r) of rank's transposed spectrum: (offset, length)."""
+        n = self.nz * self.nyl * self.blocks[rank][1]
+        return r * n, n
+
+
+# ---- communicators ------------------------------------------------------------------------
+class LoopbackComm:
+    """Every slab in this process.  Lists passed to the exchanges hold one entry per slab."""
+
+    def __init__(self, nranks: int):
+        self.size = nranks
+        self.local_ranks = list(range(nranks))
+
+    @staticmethod
+    def _sync(t: torch.Tensor):
+        if t.is_cuda:
+            torch.cuda.synchronize(t.device)
+
+    def halo_exchange(self, send_lo, send_hi, recv_lo, recv_hi):
+        """recv_lo[r] <- send_hi[r-1], recv_hi[r] <- send_lo[r+1] (periodic)."""
+        R = self.size
+        self._sync(send_lo[0])
+        for r in range(R):
+            recv_lo[r].copy_(send_hi[(r - 1) % R])
+            recv_hi[r].copy_(send_lo[(r + 1) % R])
+        self._sync(send_lo[0])
+
+    def all_to_all(self, send, recv):
+        """recv[q][r] <- send[r][q] for every pair of slabs."""
+        self._sync(send[0][0])
+        for r in range(self.size):
+            for q in range(self.size):
+                recv[q][r].copy_(send[r][q])
+        self._sync(send[0][0])
+
+    def allreduce_mean(self, bufs):
+        self._sync(bufs[0])
+        total = bufs[0].clone()
+        for b in bufs[1:]:
+            total += b
+        total /= self.size
+        for b in bufs:
+            b.copy_(total)
+        self._sync(bufs[0])
+
+    def gather_rows(self, parts):
+        return parts
+
+
+class TorchComm:
+    """One slab per process over torch.distributed; collectives run on `stream` (the model's)."""
+
+    def __init__(self, group=None):
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.size = dist.get_world_size(group)
+        self.local_ranks = [self.rank]
+        self.stream = None
+
+    def _ctx(self):
+        if self.stream is None:
+            import contextlib
+            return contextlib.nullcontext()
+        return torch.cuda.stream(self.stream)
+
+    def _peer(self, r: int) -> int:
+        return dist.get_global_rank(self.group, r) if self.group is not None else r
+
+    def halo_exchange(self, send_lo, send_hi, recv_lo, recv_hi):
+        R, r = self.size, self.rank
+        with self._ctx():
+            if R == 1:
+                recv_lo[0].copy_(send_hi[0])
+                recv_hi[0].copy_(send_lo[0])
+                return
+            prev, nxt = self._peer((r - 1) % R), self._peer((r + 1) % R)
+            # the same order on every rank: with two slabs prev == nxt and the two messages each
+            # way are matched by order (NCCL) or by tag (gloo)
+            ops = [dist.P2POp(dist.isend, send_lo[0], prev, self.group, 1),
+                   dist.P2POp(dist.isend, send_hi[0], nxt, self.group, 2),
+                   dist.P2POp(dist.irecv, recv_hi[0], nxt, self.group, 1),
+                   dist.P2POp(dist.irecv, recv_lo[0], prev, self.group, 2)]
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+
+    def all_to_all(self, send, recv):
+        R, me = self.size, self.rank
+        with self._ctx():
+            recv[0][me].copy_(send[0][me])
+            if R == 1:
+                return
+            ops = []
+            for q in range(R):
+                if q != me:
+                    ops.append(dist.P2POp(dist.isend, send[0][q], self._peer(q), self.group, 3))
+                    ops.append(dist.P2POp(dist.irecv, recv[0][q], self._peer(q), self.group, 3))
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+
+    def allreduce_mean(self, bufs):
+        with self._ctx():
+            dist.all_reduce(bufs[0], group=self.group)
+            bufs[0].div_(self.size)
+
+    def gather_rows(self, parts):
+        with self._ctx():
+            out = [torch.empty_like(parts[0]) for _ in range(self.size)]
+            dist.all_gather(out, parts[0].contiguous(), group=self.group)
+        return out
+
+
+# ---- the decomposed model -------------------------------------------------------------------
+class _Slab:
+    def __init__(self, rank: int, model: api.Model, geo: SlabGeometry, dtype, device):
+        self.rank = rank
+        self.m = model
+        g = geo
+        # spectra are interleaved complex: 2 reals per element
+        self.spec_x = torch.zeros(2 * g.nz * g.nyl * g.nxh, dtype=dtype, device=device)
+        self.spec_t = torch.zeros(2 * g.nz * g.ny * g.blocks[rank][1], dtype=dtype, device=device)
+        nf = model.halo_fields(cf.HALO_STATE)
+        # send below, send above, received from below, received from above
+        self.state_bufs = [torch.zeros(nf * g.nz * g.halo * g.nx, dtype=dtype, device=device) for _ in range(4)]
+        self.p_bufs = [torch.zeros(g.nz * g.nx, dtype=dtype, device=device) for _ in range(4)]
+        self.means = torch.zeros((1 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
+
+        def cview(buf, off, n):
+            return buf[2 * off:2 * (off + n)]
+        self.x_blocks = [cview(self.spec_x, *g.xblock(q)) for q in range(g.nranks)]
+        self.t_blocks = [cview(self.spec_t, *g.tblock(rank, r)) for r in range(g.nranks)]
+
+
+class SlabDomain:
+    """A periodic domain of cfg's size split into y-slabs over comm's ranks.
+
+    The slabs local to this process (all of them under LoopbackComm) are models created with
+    solver SOLVER_EXTERNAL on `device`.  Fields move in and out as global [nz][ny][nx] arrays."""
+
+    def __init__(self, cfg: cf.MgpuConfig, comm, halo: int = 4, device=None):
+        self.cfg = cfg
+        self.comm = comm
+        self.geo = SlabGeometry(cfg.nx, cfg.ny, cfg.nz, comm.size, halo)
+        g = self.geo
+        self.fp32 = cfg.precision == cf.FP32_MIXED
+        dtype = torch.float32 if self.fp32 else torch.float64
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.slabs: list[_Slab] = []
+        for r in comm.local_ranks:
+            c = cf.MgpuConfig.from_buffer_copy(cfg)
+            c.ny = g.nyl + 2 * halo
+            c.solver = cf.SOLVER_EXTERNAL
+            m = api.Model(c)
+            m.slab_init(g.ny, halo, max(w for _, w in g.blocks))
+            self.slabs.append(_Slab(r, m, g, dtype, self.device))
+        if isinstance(comm, TorchComm) and self.device.type == "cuda":
+            comm.stream = torch.cuda.ExternalStream(self.slabs[0].m.stream, device=self.device)
+
+    def close(self):
+        for s in self.slabs:
+            s.m.close()
+        self.slabs = []
+
+    # -- fields
+    def upload(self, name, arr: np.ndarray):
+        a = np.asarray(arr, dtype=np.float64).reshape(self.geo.nz, self.geo.ny, self.geo.nx)
+        for s in self.slabs:
+            s.m.upload(name, np.ascontiguousarray(a[:, self.geo.rows(s.rank), :]))
+
+    def set_state(self, state: dict):
+        for k, v in state.items():
+            self.upload(k, v)
+
+    def download(self, name) -> np.ndarray:
+        g = self.geo
+        parts = [torch.from_numpy(s.m.download(name)[:, g.halo:g.halo + g.nyl, :].copy()) for s in self.slabs]
+        if isinstance(self.comm, TorchComm):
+            dev = self.device if dist.get_backend(self.comm.group) == "nccl" else torch.device("cpu")
+            parts = [p.to(dev) for p in self.comm.gather_rows([parts[0].to(dev)])]
+        return np.concatenate([p.cpu().numpy() for p in parts], axis=1)
+
+    def set_timestep(self, ts: int):
+        for s in self.slabs:
+            s.m.set_timestep(ts)
+
+    # -- stepping
+    def _exchange(self, halo_set: int, depth: int):
+        bufs = [s.state_bufs if halo_set == cf.HALO_STATE else s.p_bufs for s in self.slabs]
+        for s, b in zip(self.slabs, bufs):
+            s.m.halo_pack(halo_set, depth, b[0].data_ptr(), b[1].data_ptr())
+        self.comm.halo_exchange([b[0] for b in bufs], [b[1] for b in bufs], [b[2] for b in bufs],
+                                [b[3] for b in bufs])
+        for s, b in zip(self.slabs, bufs):
+            s.m.halo_unpack(halo_set, depth, b[2].data_ptr(), b[3].data_ptr())
+
+    def step(self, n: int = 1):
+        g = self.geo
+        for _ in range(n):
+            self._exchange(cf.HALO_STATE, g.halo)
+            for s in self.slabs:
+                s.m.step_phase(cf.PHASE_SUBGRID)
+            if self.fp32:
+                for s in self.slabs:
+                    s.m.slab_level_means(s.means.data_ptr())
+                self.comm.allreduce_mean([s.means for s in self.slabs])
+            for s in self.slabs:
+                s.m.step_phase(cf.PHASE_DYNAMICS)
+                s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, False)
+            self.comm.all_to_all([s.x_blocks for s in self.slabs], [s.t_blocks for s in self.slabs])
+            for s in self.slabs:
+                k0, w = g.blocks[s.rank]
+                s.m.slab_solve_columns(s.spec_t.data_ptr(), k0, w, g.nyl)
+            self.comm.all_to_all([s.t_blocks for s in self.slabs], [s.x_blocks for s in self.slabs])
+            for s in self.slabs:
+                s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, True)
+            self._exchange(cf.HALO_PRESSURE, 1)
+            for s in self.slabs:
+                s.m.step_phase(cf.PHASE_PSTEP)
+
+    def synchronize(self):
+        for s in self.slabs:
+            torch.cuda.ExternalStream(s.m.stream, device=self.device).synchronize()

@@ -1,0 +1,227 @@
+"""The y-slab decomposed step on one GPU: every slab a separate model with an external pressure
+solve, exchanged through the loopback communicator (device copies between the slabs' buffers
+after all queued work has finished; no kernel waits on another slab).
+
+* FP64 with reproducible arithmetic: 2 and 4 slabs reproduce the single-domain model bit for
+  bit, dry and moist, on the forward and centred steps; and both agree with the CPU oracle.
+* Default (contracted) FP64 arithmetic and FP32-mixed: the decomposed run tracks the
+  single-domain run (FP32-mixed differs by the order in which the level means are summed).
+* The slab entry points themselves: halo rows, the transposed column solve, argument checks.
+"""
+import numpy as np
+import pytest
+import torch
+
+from monc_b200 import api, config as cf, decomposition as dc, init as ini
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ = 64, 64, 24
+STATE = ["u", "v", "w", "th", "zu", "zv", "zw", "zth"]
+
+
+def dry_config(precision=cf.FP64, reproducible=1):
+    c = cf.dry_cbl_config(NX, NY, NZ, 50.0, 25.0, 0.5, ug=5.0, fcoriol=1e-4, precision=precision)
+    c.reproducible = reproducible
+    return c
+
+
+def dry_state(seed=4):
+    return ini.random_flow_state(NX, NY, NZ, seed=seed, amp_uv=1.0, amp_w=0.3, amp_th=0.5, ug=5.0)
+
+
+def run_single(cfg, state, nsteps, fields):
+    m = api.Model(cfg)
+    m.set_state(state)
+    m.step(nsteps)
+    out = {f: m.download(f) for f in fields}
+    m.close()
+    return out
+
+
+def run_slabs(cfg, state, nsteps, nranks, fields, halo=4):
+    d = dc.SlabDomain(cfg, dc.LoopbackComm(nranks), halo=halo)
+    d.set_state(state)
+    d.step(nsteps)
+    out = {f: d.download(f) for f in fields}
+    d.close()
+    return out
+
+
+@pytest.mark.parametrize("nranks", [2, 4])
+@pytest.mark.parametrize("nsteps", [1, 3])
+def test_dry_fp64_slabs_bit_identical(gpu_lib, nranks, nsteps):
+    cfg, st = dry_config(), dry_state()
+    ref = run_single(cfg, st, nsteps, STATE + ["p"])
+    got = run_slabs(cfg, st, nsteps, nranks, STATE + ["p"])
+    for f in STATE + ["p"]:
+        np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
+
+
+def test_dry_fp64_slabs_match_oracle(gpu_lib):
+    cfg, st = dry_config(), dry_state(seed=7)
+    o = po.Oracle(cfg)
+    for name, arr in st.items():
+        o.set(api.FIELDS[name], arr)
+    o.step(2)
+    got = run_slabs(cfg, st, 2, 4, STATE)
+    for f in STATE:
+        ref = o.get(api.FIELDS[f])
+        assert np.abs(got[f] - ref).max() <= 1e-10 * np.abs(ref).max(), f
+
+
+def moist_setup(precision=cf.FP64):
+    z = cf.stretched_levels(NZ, 20.0, 60.0, ztop=1000.0)
+    c = cf.moist_config(NX, NY, z, 35.0, 0.3, shf_wm2=10.0, lhf_wm2=50.0, max_height_cloud=700.0, n_tracers=1,
+                        precision=precision)
+    c.reproducible = 1
+    zn = api.reference_profile(c, "zn")
+    st = ini.moist_layer_state(NX, NY, NZ, zn, seed=2, n_tracers=1)
+    flow = ini.random_flow_state(NX, NY, NZ, seed=5, amp_uv=0.5, amp_w=0.2)
+    for k in ("u", "v", "w", "zu", "zv", "zw"):
+        st[k] = flow[k]
+    return c, st
+
+
+def test_moist_fp64_slabs_bit_identical(gpu_lib):
+    cfg, st = moist_setup()
+    fields = STATE + ["q0", "q1", "q2", "zq0", "zq1", "zq2", "p"]
+    ref = run_single(cfg, st, 3, fields)
+    got = run_slabs(cfg, st, 3, 2, fields)
+    for f in fields:
+        np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
+    assert ref["q1"].max() > 0
+
+
+def test_contracted_fp64_slabs_match(gpu_lib):
+    cfg, st = dry_config(reproducible=0), dry_state()
+    ref = run_single(cfg, st, 3, STATE)
+    got = run_slabs(cfg, st, 3, 4, STATE)
+    for f in STATE:
+        assert np.abs(got[f] - ref[f]).max() <= 1e-12 * np.abs(ref[f]).max(), f
+
+
+def test_fp32_mixed_slabs_track_single_domain(gpu_lib):
+    cfg, st = moist_setup(precision=cf.FP32_MIXED)
+    fields = ["th", "w", "q0", "q1"]
+    ref = run_single(cfg, st, 5, fields)
+    got = run_slabs(cfg, st, 5, 4, fields)
+    for f in fields:
+        scale = np.abs(ref[f]).max()
+        assert np.abs(got[f] - ref[f]).max() <= 1e-5 * scale, f
+        assert np.abs(got[f].mean(axis=(1, 2)) - ref[f].mean(axis=(1, 2))).max() <= 1e-6 * scale, f
+
+
+def test_halo_rows_pack_and_unpack(gpu_lib):
+    """Pack takes the first and last `depth` interior rows, unpack writes the rows just outside."""
+    halo, nyl = 4, 16
+    c = dry_config()
+    c.ny = nyl + 2 * halo
+    c.solver = cf.SOLVER_EXTERNAL
+    m = api.Model(c)
+    m.slab_init(NY, halo, NX // 2 + 1)
+    fields = {f: ini.uniform_noise((NZ, c.ny, NX), 3, n, 1.0) for n, f in enumerate(STATE)}
+    for f, a in fields.items():
+        m.upload(f, a)
+    nf = m.halo_fields(cf.HALO_STATE)
+    assert nf == 8
+    for depth in (1, 3, halo):
+        lo = torch.zeros(nf * NZ * depth * NX, dtype=torch.float64, device="cuda")
+        hi = torch.zeros_like(lo)
+        m.halo_pack(cf.HALO_STATE, depth, lo.data_ptr(), hi.data_ptr())
+        torch.cuda.synchronize()
+        for n, f in enumerate(STATE):
+            blo = lo.view(nf, NZ, depth, NX)[n].cpu().numpy()
+            bhi = hi.view(nf, NZ, depth, NX)[n].cpu().numpy()
+            np.testing.assert_array_equal(blo, fields[f][:, halo:halo + depth])
+            np.testing.assert_array_equal(bhi, fields[f][:, c.ny - halo - depth:c.ny - halo])
+        # unpack marked buffers and check the rows they land in, and that nothing else moved
+        lo.fill_(7.0)
+        hi.fill_(-7.0)
+        m.halo_unpack(cf.HALO_STATE, depth, lo.data_ptr(), hi.data_ptr())
+        torch.cuda.synchronize()
+        for f in STATE:
+            a = m.download(f)
+            expect = fields[f].copy()
+            expect[:, halo - depth:halo] = 7.0
+            expect[:, c.ny - halo:c.ny - halo + depth] = -7.0
+            np.testing.assert_array_equal(a, expect)
+            m.upload(f, fields[f])
+    m.close()
+
+
+@pytest.mark.parametrize("nranks", [1, 2, 4])
+def test_slab_solve_and_its_transpose_match_fftsolver(gpu_lib, nranks):
+    """x-FFT + all-to-all + column solve + all-to-all + inverse x-FFT over the slabs equals the
+    fftsolver component on the whole domain, bit for bit, for the solve and for its transpose."""
+    rhs = ini.uniform_noise((NZ, NY, NX), 11, 1, 1e-3)
+    rhs[0] = 0.0
+    for transpose in (False, True):
+        ref_m = api.Model(dry_config())
+        ref_m.upload("p", rhs)
+        if transpose:
+            ref_m.fftsolver_adjoint()
+        else:
+            ref_m.component("fftsolver")
+        ref = ref_m.download("p")
+        ref_m.close()
+        d = dc.SlabDomain(dry_config(), dc.LoopbackComm(nranks))
+        d.upload("p", rhs)
+        g = d.geo
+        for s in d.slabs:
+            s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, False)
+        d.comm.all_to_all([s.x_blocks for s in d.slabs], [s.t_blocks for s in d.slabs])
+        for s in d.slabs:
+            k0, w = g.blocks[s.rank]
+            s.m.slab_solve_columns(s.spec_t.data_ptr(), k0, w, g.nyl, transpose)
+        d.comm.all_to_all([s.t_blocks for s in d.slabs], [s.x_blocks for s in d.slabs])
+        for s in d.slabs:
+            s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, True)
+        torch.cuda.synchronize()
+        got = d.download("p")
+        d.close()
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_slab_entry_points_check_arguments(gpu_lib):
+    c = dry_config()
+    c.ny = 24
+    c.solver = cf.SOLVER_EXTERNAL
+    m = api.Model(c)
+    with pytest.raises(api.MgpuError):
+        m.step(1)  # the pressure solve is external
+    with pytest.raises(api.MgpuError):
+        m.halo_pack(cf.HALO_STATE, 1, 1, 1)  # before slab_init
+    with pytest.raises(api.MgpuError):
+        m.slab_init(64, 12, 8)  # no interior rows left
+    with pytest.raises(api.MgpuError):
+        m.slab_init(48, 4, 8)  # ny_global not a power of two
+    m.slab_init(64, 4, 9)
+    buf = torch.zeros(8 * NZ * 4 * NX, dtype=torch.float64, device="cuda")
+    with pytest.raises(api.MgpuError):
+        m.halo_pack(cf.HALO_STATE, 5, buf.data_ptr(), buf.data_ptr())  # deeper than the halo
+    with pytest.raises(api.MgpuError):
+        m.halo_pack(7, 1, buf.data_ptr(), buf.data_ptr())  # unknown set
+    with pytest.raises(api.MgpuError):
+        m.slab_solve_columns(buf.data_ptr(), 0, 10, 16)  # more columns than slab_init allowed
+    with pytest.raises(api.MgpuError):
+        m.slab_solve_columns(buf.data_ptr(), 30, 5, 16)  # past nx/2+1
+    with pytest.raises(api.MgpuError):
+        m.slab_fft_x(buf.data_ptr(), NX // 2 + 2, False)  # more blocks than wavenumbers
+    m.close()
+    c32 = dry_config(precision=cf.FP32_MIXED)
+    c32.ny = 24
+    c32.solver = cf.SOLVER_EXTERNAL
+    m = api.Model(c32)
+    m.slab_init(64, 4, 9)
+    m.step_phase(cf.PHASE_SUBGRID)
+    with pytest.raises(api.MgpuError):
+        m.step_phase(cf.PHASE_DYNAMICS)  # FP32-mixed needs the domain level means first
+    m.close()
+    plain = api.Model(dry_config())
+    with pytest.raises(api.MgpuError):
+        plain.step_phase(cf.PHASE_SUBGRID)
+    with pytest.raises(api.MgpuError):
+        plain.slab_init(64, 4, 9)
+    plain.close()
