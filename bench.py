@@ -10,8 +10,13 @@ step is part of the warm-up, timed steps are centred leapfrog steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs one independent model per GPU (replicas, weak scaling); every rank's steps are
-timed on its own stream with CUDA events between barriers and the slowest rank is reported.
+N > 1 (one process per GPU under torchrun) decomposes a 256 x (256*N) x 128 domain into N
+y-slabs of the single-GPU grid (weak scaling): each step exchanges 4 halo rows of the state and
+1 of the pressure with the neighbouring slabs and transposes the pressure spectrum with two
+all-to-alls, all over NCCL (monc_b200/decomposition.py).  The initial state is the single-GPU
+one repeated in y.  Every rank's steps are timed on its model's stream with CUDA events between
+barriers and the slowest rank is reported.  --replicas runs N independent single-GPU models
+instead.
 `--impl reference` times the CPU restatement of MONC's Fortran (oracle/), the only runnable
 form of the reference here (no Fortran compiler on this machine or the GPU machine).
 """
@@ -133,6 +138,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def slab_state(cfg, geo, rank):
+    """Rows of a slab (halo rows included) of the single-GPU initial state repeated in y."""
+    st = initial_state(cfg)
+    rows = geo.rows(rank) % NY
+    return {k: np.ascontiguousarray(v[:, rows, :]) for k, v in st.items()}
+
+
+def decomposed_domain(prec, world, rank, pinned_torch=None):
+    """The 256 x (256*world) x 128 domain split into one y-slab per rank over NCCL."""
+    from monc_b200 import decomposition as dc
+
+    cfg = make_config(prec)
+    cfg.ny = NY * world
+    d = dc.SlabDomain(cfg, dc.TorchComm(), halo=4)
+    st = slab_state(make_config(prec), d.geo, rank)
+    if pinned_torch is not None:
+        pinned = {}
+        for k, v in st.items():
+            t = pinned_torch.empty(v.shape, dtype=pinned_torch.float64, pin_memory=True)
+            t.numpy()[...] = v
+            pinned[k] = t.numpy()
+        st = pinned
+    for k, v in st.items():
+        d.upload_local(k, [v])
+    return d, st
+
+
 def time_steps(model, steps, torch):
     stream = torch.cuda.ExternalStream(model.stream)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -154,11 +186,16 @@ def run_ours(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     if not torch.cuda.is_available():
         raise SystemExit("bench.py: no CUDA device")
     torch.cuda.set_device(local)
+    decomposed = (world > 1 and not args.replicas) or args.decomposed
+    if world > 1 or decomposed:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        dist.init_process_group("nccl", rank=rank, world_size=world,
+                                timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
     npts = NX * NY * NZ
 
     def barrier():
@@ -184,18 +221,36 @@ def run_ours(args):
         model.step(3)
         stages = {k: v[0] / max(v[1], 1) for k, v in model.stage_times().items() if v[1] > 0}
         model.set_profiling(False)
+        if decomposed:
+            # the timed run is the decomposed domain; the single-domain model only gave the stages
+            model.close()
+            model, _ = decomposed_domain(prec, world, rank)
+            model.step(args.warmup)
         clocks = ClockSampler(local, rank)
         barrier()
         if prec_name == "fp64":
             clocks.start()
-        l0 = model.launches
-        ms = time_steps(model, args.steps, torch)
-        launches = model.launches - l0
+        if decomposed:
+            s0 = model.slabs[0].m
+            l0 = s0.launches
+            stream = torch.cuda.ExternalStream(s0.stream)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            model.step(args.steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            launches = s0.launches - l0
+        else:
+            l0 = model.launches
+            ms = time_steps(model, args.steps, torch)
+            launches = model.launches - l0
         barrier()
         ck = clocks.stop() if prec_name == "fp64" else None
         ms = max_over_ranks(ms)
         per_step = ms / args.steps
-        th, w2 = model.diagnostics()
+        th, w2 = (model.slabs[0].m if decomposed else model).diagnostics()
         finite = bool(np.isfinite(th).all() and np.isfinite(w2).all())
         results[prec_name] = {"ms_per_step": per_step, "value": world * npts / (per_step * 1e-3) / 1e6,
                               "stages": stages, "launches": launches, "clocks": ck, "finite": finite}
@@ -204,31 +259,39 @@ def run_ours(args):
     # end to end through the C ABI: host-resident initial state (pinned) uploaded inside the timed
     # region, K steps, each followed by a device->host read of the mean theta and w'^2 profiles
     cfg = make_config(cf.FP64)
-    state = initial_state(cfg)
-    pinned = {}
-    for k, v in state.items():
-        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = v
-        pinned[k] = t.numpy()
-    model = api.Model(cfg)
-    model.set_state(pinned)
+    if decomposed:
+        model, pinned = decomposed_domain(cf.FP64, world, rank, pinned_torch=torch)
+        upload = lambda st: [model.upload_local(k, [v]) for k, v in st.items()]  # noqa: E731
+        local_model = model.slabs[0].m
+    else:
+        state = initial_state(cfg)
+        pinned = {}
+        for k, v in state.items():
+            t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = v
+            pinned[k] = t.numpy()
+        model = api.Model(cfg)
+        model.set_state(pinned)
+        upload = model.set_state
+        local_model = model
     model.step(args.warmup)
     th = np.empty(NZ)
     w2 = np.empty(NZ)
     barrier()
     t0 = time.perf_counter()
-    model.set_state(pinned)
+    upload(pinned)
     for _ in range(args.steps):
         model.step(1)
-        model.diagnostics(th, w2)
+        local_model.diagnostics(th, w2)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     model.close()
-    h2d = sum(v.nbytes for v in state.values()) / args.steps
+    h2d = sum(v.nbytes for v in pinned.values()) / args.steps
     e2e = {"value": world * npts * args.steps / e2e_s / 1e6, "unit": "Mpoint-steps/s",
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 2 * NZ * 8,
-           "note": "initial state (8 FP64 fields, pinned host) uploaded in the timed region and "
-                   "amortised over the steps; per-step read-back of the mean theta and w'^2 profiles"}
+           "note": "initial state (8 FP64 fields, pinned host; each rank its slab) uploaded in the timed "
+                   "region and amortised over the steps; per-step read-back of the mean theta and w'^2 "
+                   "profiles"}
 
     # the metric's second part: adjoint/forward time ratio on the differentiation window (dry CBL
     # 128x128x96, 300 steps, checkpoint every 25), and FP32-mixed vs FP64 on the moist layer;
@@ -238,7 +301,7 @@ def run_ours(args):
         extra["adjoint"] = adjoint_ratio()
         extra["precision_moist"] = precision_moist()
 
-    if world > 1:
+    if dist.is_initialized():
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
@@ -275,9 +338,14 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded initial state; no dataset involved)",
-        "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "precision": "fp64",
-                   "solver": "fft", "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "working set (~1.1 GB of fields) larger than the 126 MB L2; no flush needed"},
+        "config": {"workload": WORKLOAD if not decomposed else
+                   f"dry CBL {NX}x{NY * world}x{NZ} in {world} y-slabs of {NX}x{NY}x{NZ} (halo 4 rows, "
+                   "NCCL halo exchange + all-to-all FFT transposes), dx=dy=25 m, dz=15 m, u_g=5 m/s, f=1e-4, "
+                   "dt=0.5 s, FFT solver",
+                   "nx": NX, "ny": NY * world if decomposed else NY, "nz": NZ, "precision": "fp64",
+                   "solver": "fft",
+                   "parallelism": f"y-slabs x{world}" if decomposed else ("replicas" if world > 1 else "single"),
+                   "l2": "working set (~1.1 GB of fields per GPU) larger than the 126 MB L2; no flush needed"},
         "fp32_mixed": {"value": round(results["fp32_mixed"]["value"], 2),
                        "ms_per_step": round(results["fp32_mixed"]["ms_per_step"], 4),
                        "stages_ms": {k: round(v, 4) for k, v in results["fp32_mixed"]["stages"].items()},
@@ -414,6 +482,10 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: independent single-GPU models instead of the decomposed domain")
+    ap.add_argument("--decomposed", action="store_true",
+                    help="run the decomposed domain even on one GPU (one slab; exercises the NCCL path)")
     ap.add_argument("--skip-extra", action="store_true",
                     help="skip the adjoint-ratio and moist-precision measurements (single-GPU runs)")
     args = ap.parse_args()

@@ -267,6 +267,12 @@ class SlabDomain:
         for k, v in state.items():
             self.upload(k, v)
 
+    def upload_local(self, name, arrays):
+        """Upload each local slab's rows directly: arrays[i] is [nz][nyl + 2*halo][nx] for the i-th
+        local slab (the rows SlabGeometry.rows gives), so no process builds the global field."""
+        for s, a in zip(self.slabs, arrays):
+            s.m.upload(name, a)
+
     def download(self, name) -> np.ndarray:
         g = self.geo
         parts = [torch.from_numpy(s.m.download(name)[:, g.halo:g.halo + g.nyl, :].copy()) for s in self.slabs]

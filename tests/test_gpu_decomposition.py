@@ -8,6 +8,11 @@ after all queued work has finished; no kernel waits on another slab).
   single-domain run (FP32-mixed differs by the order in which the level means are summed).
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
+import os
+import subprocess
+import sys
+import textwrap
+
 import numpy as np
 import pytest
 import torch
@@ -225,3 +230,44 @@ def test_slab_entry_points_check_arguments(gpu_lib):
     with pytest.raises(api.MgpuError):
         plain.slab_init(64, 4, 9)
     plain.close()
+
+
+NCCL_ONE_RANK = textwrap.dedent("""
+    import datetime, os, sys
+    import numpy as np, torch, torch.distributed as dist
+    sys.path.insert(0, os.getcwd())
+    from monc_b200 import api, config as cf, decomposition as dc, init as ini
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    c = cf.dry_cbl_config(64, 64, 24, 50.0, 25.0, 0.5, ug=5.0, fcoriol=1e-4, precision=int(sys.argv[1]))
+    c.reproducible = 1
+    st = ini.random_flow_state(64, 64, 24, seed=4, amp_uv=1.0, amp_w=0.3, amp_th=0.5, ug=5.0)
+    m = api.Model(c)
+    m.set_state(st)
+    m.step(3)
+    d = dc.SlabDomain(c, dc.TorchComm(), halo=4)
+    d.set_state(st)
+    d.step(3)
+    for f in ("u", "v", "w", "th", "zu", "zv", "zw", "zth"):
+        a, b = d.download(f), m.download(f)
+        err = np.abs(a - b).max() / np.abs(b).max()
+        assert err <= (0.0 if c.precision == cf.FP64 else 1e-5), (f, err)
+    d.close()
+    m.close()
+    dist.destroy_process_group()
+    print("SLAB-NCCL-OK")
+""")
+
+
+@pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32_mixed"])
+def test_torch_comm_over_nccl_single_rank(gpu_lib, precision):
+    """The torch.distributed communicator on NCCL with one rank (the model's stream as the
+    collectives' stream, all-to-all and halo exchange as local copies, the FP32 level-mean
+    all-reduce through NCCL) reproduces the single-domain model; run in a child process so the
+    process group does not outlive the test."""
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(29600 + precision))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", NCCL_ONE_RANK, str(precision)], cwd=root, env=env,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "SLAB-NCCL-OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
