@@ -258,32 +258,24 @@ __global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<
 }
 
 // ---- vertical tridiagonal per (ky, kx) in FP64 ----------------------------------------------
+// The horizontal-mean mode (kx = ky = 0) of one column, held at col[0], col[1], ... (level k at
+// col[k-1]): p(1) = p(2) = 0 and an upward recurrence, or with transpose the transposed recurrence
+// from the top.
 template <typename T>
-// The spectrum holds ncols kx columns per row, the global wavenumbers kx0 .. kx0+ncols-1 (all
-// nx/2+1 of them, or one rank's block after a transpose), and its rows in blocks of rpb as in
-// k_fft_y.  s1buf is [nz][ny][ncols] whatever the spectrum layout.
-__global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
-                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose,
-                          int ncols, int kx0, int rpb) {
+__device__ void mean_mode_column(typename Cx<T>::t* col, int nz, const double* czb, const double* cza,
+                                 const double* czg, int transpose) {
   typedef typename Cx<T>::t C;
-  const int nxh = nx / 2 + 1;
-  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= (long long)ny * ncols) return;
-  const int ky = (int)(col / ncols), c = (int)(col - (long long)ky * ncols), kx = kx0 + c;
-  const long long plane = (long long)ny * ncols;      // level stride of s1buf
-  const long long lstride = (long long)rpb * ncols;   // level stride of the spectrum
-  const double* czb = prof + P_CZB * prof_stride;
-  const double* cza = prof + P_CZA * prof_stride;
-  const double* czg = prof + P_CZG * prof_stride;
-  C* sp = spec + spec_row(ky, 1, rpb, ncols, nz) + c;
-  if (transpose && kx == 0 && ky == 0) {
-    // transpose of the mean-mode recurrence below: the rows r = 2..nz-1 of
-    // cza(r) p(r+1) + czg(r) p(r) + czb(r) p(r-1) = b(r), p(1) = p(2) = 0, solved from the top
+  C zero;
+  zero.x = (T)0;
+  zero.y = (T)0;
+  if (transpose) {
+    // the rows r = 2..nz-1 of cza(r) p(r+1) + czg(r) p(r) + czb(r) p(r-1) = b(r), p(1) = p(2) = 0,
+    // transposed and solved from the top
     double zr1 = 0.0, zi1 = 0.0, zr2 = 0.0, zi2 = 0.0;  // z(u), z(u+1)
-    C ynext = sp[(long long)(nz - 1) * lstride];           // y(nz)
+    C ynext = col[nz - 1];                              // y(nz)
     for (int u = nz; u >= 3; --u) {
       const C yu = ynext;
-      if (u >= 4) ynext = sp[(long long)(u - 2) * lstride];  // y(u-1), read before z(u-1) overwrites it
+      if (u >= 4) ynext = col[u - 2];  // y(u-1), read before z(u-1) overwrites it
       double yr = (double)yu.x, yi = (double)yu.y;
       if (u <= nz - 1) { yr -= czg[u] * zr1; yi -= czg[u] * zi1; }
       if (u + 1 <= nz - 1) { yr -= czb[u + 1] * zr2; yi -= czb[u + 1] * zi2; }
@@ -292,43 +284,67 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
       C o;
       o.x = (T)zr;
       o.y = (T)zi;
-      sp[(long long)(u - 2) * lstride] = o;
+      col[u - 2] = o;
     }
-    C zero;
-    zero.x = (T)0;
-    zero.y = (T)0;
-    sp[0] = zero;
-    sp[(long long)(nz - 1) * lstride] = zero;
+    col[0] = zero;
+    col[nz - 1] = zero;
     return;
   }
+  C v2 = col[1];
+  double sr_prev = (double)v2.x, si_prev = (double)v2.y;
+  double pr2 = 0.0, pi2 = 0.0, pr1 = 0.0, pi1 = 0.0;  // p(k-2), p(k-1)
+  col[0] = zero;  // p(1) = p(2) = 0 for the mean mode
+  col[1] = zero;
+  for (int k = 3; k <= nz; ++k) {
+    C vk = col[k - 1];
+    double pr = (sr_prev - czg[k - 1] * pr1 - czb[k - 1] * pr2) / cza[k - 1];
+    double pi = (si_prev - czg[k - 1] * pi1 - czb[k - 1] * pi2) / cza[k - 1];
+    sr_prev = (double)vk.x;
+    si_prev = (double)vk.y;
+    C o;
+    o.x = (T)pr;
+    o.y = (T)pi;
+    col[k - 1] = o;
+    pr2 = pr1; pi2 = pi1; pr1 = pr; pi1 = pi;
+  }
+}
+
+template <typename T>
+// The spectrum holds ncols kx columns per row, the global wavenumbers kx0 .. kx0+ncols-1 (all
+// nx/2+1 of them, or one rank's block after a transpose), and its rows in blocks of rpb as in
+// k_fft_y.  s1buf is [nz][ny][ncols] whatever the spectrum layout.  One thread per column; when
+// the block holds kx = 0 (kx0 == 0) the launch has one extra block, the last, for the mean mode.
+__global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
+                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose,
+                          int ncols, int kx0, int rpb) {
+  typedef typename Cx<T>::t C;
+  const int nxh = nx / 2 + 1;
+  const long long lstride = (long long)rpb * ncols;   // level stride of the spectrum
+  const double* czb = prof + P_CZB * prof_stride;
+  const double* cza = prof + P_CZA * prof_stride;
+  const double* czg = prof + P_CZG * prof_stride;
+  if (kx0 == 0 && blockIdx.x == gridDim.x - 1) {
+    // the mean mode is one sequential recurrence over the levels: stage its column (row 0,
+    // column 0 of every level) in shared memory so that no step of it waits on a global load
+    extern __shared__ unsigned char smem_raw[];
+    C* colv = reinterpret_cast<C*>(smem_raw);
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) colv[k] = spec[(long long)k * lstride];
+    __syncthreads();
+    if (threadIdx.x == 0) mean_mode_column<T>(colv, nz, czb, cza, czg, transpose);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) spec[(long long)k * lstride] = colv[k];
+    return;
+  }
+  long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= (long long)ny * ncols) return;
+  const int ky = (int)(col / ncols), c = (int)(col - (long long)ky * ncols), kx = kx0 + c;
+  if (kx == 0 && ky == 0) return;  // the mean-mode block's column
+  const long long plane = (long long)ny * ncols;      // level stride of s1buf
+  C* sp = spec + spec_row(ky, 1, rpb, ncols, nz) + c;
   // the transposed tridiagonal has the same pivots (they depend on czb(k)*cza(k-1) only) with
   // the off-diagonals exchanged: cza(k-1) below the diagonal, czb(k+1) above it
   const double* lo = transpose ? cza - 1 : czb;  // lo[k]: coefficient of s(k-1) in row k
   const double* up = transpose ? czb + 1 : cza;  // up[k]: coefficient of p(k+1) in row k
-  if (kx == 0 && ky == 0) {
-    // horizontal-mean mode: upward recurrence from p(1) = p(2) = 0
-    C v2 = sp[lstride];
-    double sr_prev = (double)v2.x, si_prev = (double)v2.y;
-    double pr2 = 0.0, pi2 = 0.0, pr1 = 0.0, pi1 = 0.0;  // p(k-2), p(k-1)
-    C zero;
-    zero.x = (T)0;
-    zero.y = (T)0;
-    sp[0] = zero;  // p(1) = p(2) = 0 for the mean mode
-    sp[lstride] = zero;
-    for (int k = 3; k <= nz; ++k) {
-      C vk = sp[(long long)(k - 1) * lstride];
-      double pr = (sr_prev - czg[k - 1] * pr1 - czb[k - 1] * pr2) / cza[k - 1];
-      double pi = (si_prev - czg[k - 1] * pi1 - czb[k - 1] * pi2) / cza[k - 1];
-      sr_prev = (double)vk.x;
-      si_prev = (double)vk.y;
-      C o;
-      o.x = (T)pr;
-      o.y = (T)pi;
-      sp[(long long)(k - 1) * lstride] = o;
-      pr2 = pr1; pi2 = pi1; pr1 = pr; pi1 = pi;
-    }
-    return;
-  }
   const int kyi = ky <= ny / 2 ? ky : ny - ky;
   const long long bstride = (long long)(ny / 2 + 1) * nxh;
   const double* bcol = b1 + (long long)kyi * nxh + kx;
@@ -520,7 +536,7 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, false, s.nz, s.ny);
   mark(2);
   long long ncol = (long long)plane;
-  k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
+  k_tridiag<T><<<(unsigned)((ncol + 127) / 128 + 1), 128, s.nz * sizeof(C), st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
                                                                transpose ? 1 : 0, pl.nxh, 0, s.ny);
   mark(3);
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, true, s.nz, s.ny);
@@ -563,7 +579,8 @@ void slab_solve_columns(const FftPlanDev& pl, const Scalars& s, void* spec, int 
   dim3 gy((nkx + z.cols_y - 1) / z.cols_y, s.nz);
   const long long ncol = (long long)pl.ny * nkx;
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, false, s.nz, rpb);
-  k_tridiag<T><<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(sp, pl.s1, pl.b1, s.prof, s.nz + 2, pl.nx, pl.ny, s.nz,
+  k_tridiag<T><<<(unsigned)((ncol + 127) / 128 + (kx0 == 0 ? 1 : 0)), 128, s.nz * sizeof(C), st>>>(
+      sp, pl.s1, pl.b1, s.prof, s.nz + 2, pl.nx, pl.ny, s.nz,
                                                                transpose ? 1 : 0, nkx, kx0, rpb);
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, true, s.nz, rpb);
   *launches += 3;
@@ -780,7 +797,8 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   dim3 gy((nxh + z.cols_y - 1) / z.cols_y, nz);
   k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
   k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, false, nz, ny);
-  k_tridiag<double><<<(unsigned)((plane + 127) / 128), 128, 0, st>>>(spec, s1, b1, prof, stride, nx, ny, nz, 0, nxh, 0, ny);
+  k_tridiag<double><<<(unsigned)((plane + 127) / 128 + 1), 128, nz * sizeof(double2), st>>>(spec, s1, b1, prof, stride, nx,
+                                                                                          ny, nz, 0, nxh, 0, ny);
   k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, true, nz, ny);
   k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
