@@ -257,6 +257,47 @@ __global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<
   }
 }
 
+// ---- cp.async staging (each thread copies and later reads its own shared-memory slots) -------
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(double2* dst, const double2* src) { cp_async_16(dst, src); }
+__device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src) { cp_async_8(dst, src); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// tridiagonal launch shape: TRI_TB columns (threads) per block, TRI_KC levels per staged chunk
+constexpr int TRI_TB = 128, TRI_KC = 16;
+constexpr size_t TRI_SMEM = (size_t)2 * TRI_KC * TRI_TB * (sizeof(double2) + sizeof(double));
+template <typename C>
+static size_t tri_smem_bytes(int nz) { return std::max(TRI_SMEM, (size_t)nz * sizeof(C)); }
+template <typename T>
+__global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
+                          const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose,
+                          int ncols, int kx0, int rpb);
+// the staging buffers exceed the default 48 KB of dynamic shared memory: raise the limit once per
+// device (the largest column, nz = MGPU_MAX_NZ levels for the mean mode, stays below TRI_SMEM)
+static void ensure_tri_attr() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  cudaFuncSetAttribute(k_tridiag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM);
+  cudaFuncSetAttribute(k_tridiag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM);
+  done[dev] = true;
+}
+__device__ __forceinline__ unsigned char* tri_smem() {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  return smem_raw;
+}
+
 // ---- vertical tridiagonal per (ky, kx) in FP64 ----------------------------------------------
 // The horizontal-mean mode (kx = ky = 0) of one column, held at col[0], col[1], ... (level k at
 // col[k-1]): p(1) = p(2) = 0 and an upward recurrence, or with transpose the transposed recurrence
@@ -326,8 +367,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   if (kx0 == 0 && blockIdx.x == gridDim.x - 1) {
     // the mean mode is one sequential recurrence over the levels: stage its column (row 0,
     // column 0 of every level) in shared memory so that no step of it waits on a global load
-    extern __shared__ unsigned char smem_raw[];
-    C* colv = reinterpret_cast<C*>(smem_raw);
+    C* colv = reinterpret_cast<C*>(tri_smem());
     for (int k = threadIdx.x; k < nz; k += blockDim.x) colv[k] = spec[(long long)k * lstride];
     __syncthreads();
     if (threadIdx.x == 0) mean_mode_column<T>(colv, nz, czb, cza, czg, transpose);
@@ -348,56 +388,87 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   const int kyi = ky <= ny / 2 ? ky : ny - ky;
   const long long bstride = (long long)(ny / 2 + 1) * nxh;
   const double* bcol = b1 + (long long)kyi * nxh + kx;
-  // forward elimination s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1), loads batched 8 levels at a time
-  constexpr int B = 8;
+  // Every level a thread needs (spectrum or s1, and the pivot) is staged in shared memory by
+  // cp.async, TRI_KC levels per chunk, the next chunk in flight while this one is used.  Each
+  // thread copies and reads only its own slots, so no block barrier is involved.
+  // Slots are 16 bytes whatever the spectrum type, so that a thread's forward slots (spectrum)
+  // and backward slots (s1) are the same bytes and no thread's slot overlaps another's.
+  unsigned char* raw = tri_smem();
+  double2* sbuf = reinterpret_cast<double2*>(raw);    // [2][TRI_KC][TRI_TB] 16-byte slots
+  double* bbuf = reinterpret_cast<double*>(raw + (size_t)2 * TRI_KC * TRI_TB * sizeof(double2));
+  const int t = threadIdx.x;
+  auto slot = [&](int ch, int q) { return ((ch & 1) * TRI_KC + q) * TRI_TB + t; };
+  auto fslot = [&](int ch, int q) { return reinterpret_cast<C*>(sbuf + slot(ch, q)); };
+  // forward elimination s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1) for k = 3..nz
   C v = sp[lstride];
   double sr = (double)v.x, si = (double)v.y;
   s1buf[col + plane] = make_double2(sr, si);
-  for (int k0 = 3; k0 <= nz; k0 += B) {
-    C vb[B];
-    double bb[B];
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      int k = k0 + q;
-      if (k <= nz) { vb[q] = sp[(long long)(k - 1) * lstride]; bb[q] = __ldg(bcol + (long long)(k - 1) * bstride); }
-    }
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      int k = k0 + q;
+  const int nch = (nz - 2 + TRI_KC - 1) / TRI_KC;
+  auto issue_fwd = [&](int ch) {
+    for (int q = 0; q < TRI_KC; ++q) {
+      const int k = 3 + ch * TRI_KC + q;
       if (k <= nz) {
-        sr = (double)vb[q].x - lo[k] * sr * bb[q];
-        si = (double)vb[q].y - lo[k] * si * bb[q];
+        cp_async_elem(fslot(ch, q), sp + (long long)(k - 1) * lstride);
+        cp_async_8(bbuf + slot(ch, q), bcol + (long long)(k - 1) * bstride);
+      }
+    }
+    cp_async_commit();
+  };
+  issue_fwd(0);
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) issue_fwd(ch + 1);
+    else cp_async_commit();
+    cp_async_wait_1();
+#pragma unroll 4
+    for (int q = 0; q < TRI_KC; ++q) {
+      const int k = 3 + ch * TRI_KC + q;
+      if (k <= nz) {
+        const C vq = *fslot(ch, q);
+        const double bq = bbuf[slot(ch, q)];
+        sr = (double)vq.x - lo[k] * sr * bq;
+        si = (double)vq.y - lo[k] * si * bq;
         s1buf[col + (long long)(k - 1) * plane] = make_double2(sr, si);
       }
     }
   }
-  // back substitution pt(k) = (s1(k) - cza(k)*pt(k+1))*b1(k)
+  cp_async_wait_0();
+  // back substitution pt(k) = (s1(k) - cza(k)*pt(k+1))*b1(k) for k = nz-1 down to 2
   double pr = sr * __ldg(bcol + (long long)nz * bstride);
   double pi = si * __ldg(bcol + (long long)nz * bstride);
   C o;
   o.x = (T)pr;
   o.y = (T)pi;
   sp[(long long)(nz - 1) * lstride] = o;
-  for (int k0 = nz - 1; k0 >= 2; k0 -= B) {
-    double2 sb[B];
-    double bb[B];
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      int k = k0 - q;
-      if (k >= 2) { sb[q] = s1buf[col + (long long)(k - 1) * plane]; bb[q] = __ldg(bcol + (long long)k * bstride); }
-    }
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      int k = k0 - q;
+  auto issue_bwd = [&](int ch) {
+    for (int q = 0; q < TRI_KC; ++q) {
+      const int k = nz - 1 - ch * TRI_KC - q;
       if (k >= 2) {
-        pr = (sb[q].x - up[k] * pr) * bb[q];
-        pi = (sb[q].y - up[k] * pi) * bb[q];
+        cp_async_16(sbuf + slot(ch, q), s1buf + col + (long long)(k - 1) * plane);
+        cp_async_8(bbuf + slot(ch, q), bcol + (long long)k * bstride);
+      }
+    }
+    cp_async_commit();
+  };
+  issue_bwd(0);
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) issue_bwd(ch + 1);
+    else cp_async_commit();
+    cp_async_wait_1();
+#pragma unroll 4
+    for (int q = 0; q < TRI_KC; ++q) {
+      const int k = nz - 1 - ch * TRI_KC - q;
+      if (k >= 2) {
+        const double2 sq = sbuf[slot(ch, q)];
+        const double bq = bbuf[slot(ch, q)];
+        pr = (sq.x - up[k] * pr) * bq;
+        pi = (sq.y - up[k] * pi) * bq;
         o.x = (T)pr;
         o.y = (T)pi;
         sp[(long long)(k - 1) * lstride] = o;
       }
     }
   }
+  cp_async_wait_0();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -536,7 +607,9 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, false, s.nz, s.ny);
   mark(2);
   long long ncol = (long long)plane;
-  k_tridiag<T><<<(unsigned)((ncol + 127) / 128 + 1), 128, s.nz * sizeof(C), st>>>(spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
+  ensure_tri_attr();
+  k_tridiag<T><<<(unsigned)((ncol + TRI_TB - 1) / TRI_TB + 1), TRI_TB, tri_smem_bytes<C>(s.nz), st>>>(
+      spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
                                                                transpose ? 1 : 0, pl.nxh, 0, s.ny);
   mark(3);
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, true, s.nz, s.ny);
@@ -579,7 +652,8 @@ void slab_solve_columns(const FftPlanDev& pl, const Scalars& s, void* spec, int 
   dim3 gy((nkx + z.cols_y - 1) / z.cols_y, s.nz);
   const long long ncol = (long long)pl.ny * nkx;
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, false, s.nz, rpb);
-  k_tridiag<T><<<(unsigned)((ncol + 127) / 128 + (kx0 == 0 ? 1 : 0)), 128, s.nz * sizeof(C), st>>>(
+  ensure_tri_attr();
+  k_tridiag<T><<<(unsigned)((ncol + TRI_TB - 1) / TRI_TB + (kx0 == 0 ? 1 : 0)), TRI_TB, tri_smem_bytes<C>(s.nz), st>>>(
       sp, pl.s1, pl.b1, s.prof, s.nz + 2, pl.nx, pl.ny, s.nz,
                                                                transpose ? 1 : 0, nkx, kx0, rpb);
   k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, true, s.nz, rpb);
@@ -797,8 +871,9 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   dim3 gy((nxh + z.cols_y - 1) / z.cols_y, nz);
   k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
   k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, false, nz, ny);
-  k_tridiag<double><<<(unsigned)((plane + 127) / 128 + 1), 128, nz * sizeof(double2), st>>>(spec, s1, b1, prof, stride, nx,
-                                                                                          ny, nz, 0, nxh, 0, ny);
+  ensure_tri_attr();
+  k_tridiag<double><<<(unsigned)((plane + TRI_TB - 1) / TRI_TB + 1), TRI_TB, tri_smem_bytes<double2>(nz), st>>>(
+      spec, s1, b1, prof, stride, nx, ny, nz, 0, nxh, 0, ny);
   k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, true, nz, ny);
   k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
