@@ -40,43 +40,156 @@ template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a
 
 static int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
 
-// In-place radix-2 decimation-in-time stages over `nrows` rows held in shared memory in
-// bit-reversed order.  Element e of row r lives at buf[r*rs + e*es].
-// rows_fast selects which index consecutive threads walk: the row (when rows are the contiguous
-// dimension in shared memory, es > 1) or the butterfly within a row (es == 1), so that a warp
-// touches consecutive shared-memory words.
-// Rows stored contiguously (es == 1) are padded with one element after every 32 (pidx): a
-// bit-reversed scatter of 16-byte elements then spreads a quarter-warp over all eight bank groups
-// instead of one.
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 5); }
-__host__ __device__ __forceinline__ int padded_row(int n) { return n + (n >> 5); }
+// ---- line FFTs: Stockham autosort passes, radix 16 in registers -----------------------------
+// An N-point complex transform (N = 2^LOGN) of one line is done by G = N/E threads holding E =
+// min(N, 16) points each.  Pass p has radix R_p (16, the last pass 2^(LOGN mod 4) when LOGN is
+// not a multiple of 4) and span NS_p = R_0*...*R_{p-1}: a thread's butterflies are jb = j + G*b,
+// b < E/R_p, each on the points x[jb + r*N/R_p] (r < R_p), multiplied by W_{NS*R}^{(jb mod NS)*r},
+// transformed by an R_p-point DFT in registers and stored to y[(jb/NS)*NS*R + jb mod NS + r*NS]
+// (the self-sorting Stockham form: the output of the last pass is in natural order).  The first
+// pass reads the line from wherever the caller's accessor points (global memory or shared
+// memory), passes in between go through a padded shared-memory copy of the line, and the last
+// pass hands each result to the caller's accessor.  W_N^m = e^{-2 pi i m / N} (forward) or its
+// conjugate (inverse); inverse transforms are unscaled.
+template <int LOGN>
+struct LineShape {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int E = N < 16 ? N : 16;
+  static constexpr int G = N / E;
+  static constexpr int P = (LOGN + 3) / 4;
+  static constexpr int RL = 1 << (LOGN - 4 * (P - 1));   // radix of the last pass
+  static constexpr int R(int p) { return p < P - 1 ? 16 : RL; }
+  static constexpr int NS(int p) { return p == 0 ? 1 : (p == 1 ? R(0) : R(0) * R(1)); }
+  static constexpr int LPL = N + N / 16 + 1;  // padded line length in shared memory (elements)
+};
+// shared-memory index of point i of a line: one element of padding after every 16, so that the
+// first pass's stores (stride 16 between threads) fall in different banks
+__device__ __forceinline__ int lpad(int i) { return i + (i >> 4); }
 
-template <typename C>
-__device__ void smem_fft_stages(C* buf, int n, int logn, int nrows, int rs, int es, const C* tw, bool inverse,
-                                bool rows_fast = false, bool padded = false) {
-  const int half_n = n >> 1;
-  const int total = nrows * half_n;
-  for (int s = 1; s <= logn; ++s) {
-    const int half = 1 << (s - 1);
-    const int stride = n >> s;
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      int r, bb;
-      if (rows_fast) { bb = b / nrows; r = b - bb * nrows; }
-      else { r = b / half_n; bb = b - r * half_n; }
-      int pos = bb & (half - 1);
-      int i0 = ((bb >> (s - 1)) << s) | pos;
-      int i1 = i0 + half;
-      C w = tw[pos * stride];
-      if (inverse) w.y = -w.y;
-      C* row = buf + r * rs;
-      const int a0 = padded ? pidx(i0) : i0 * es, a1 = padded ? pidx(i1) : i1 * es;
-      C a = row[a0], c = row[a1];
-      C t = cmul(w, c);
-      row[a1] = csub(a, t);
-      row[a0] = cadd(a, t);
-    }
-    __syncthreads();
+__host__ __device__ constexpr int brev_c(int i, int r) {
+  int o = 0;
+  for (int b = 1; b < r; b <<= 1) { o = (o << 1) | (i & 1); i >>= 1; }
+  return o;
+}
+
+// b * W16^t (t < 8), conjugated twiddle when INV; t is a constant after unrolling
+template <typename C, bool INV>
+__device__ __forceinline__ C mul_w16(C b, int t) {
+  typedef decltype(b.x) T;
+  const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173, r2 = (T)0.70710678118654752440;
+  if (t == 0) return b;
+  C o;
+  if (t == 4) {  // W16^4 = -i
+    if (!INV) { o.x = b.y; o.y = -b.x; } else { o.x = -b.y; o.y = b.x; }
+    return o;
   }
+  T wr, wi;
+  switch (t) {
+    case 1: wr = c1; wi = -s1; break;
+    case 2: wr = r2; wi = -r2; break;
+    case 3: wr = s1; wi = -c1; break;
+    case 5: wr = -s1; wi = -c1; break;
+    case 6: wr = -r2; wi = -r2; break;
+    default: wr = -c1; wi = -s1; break;
+  }
+  if (INV) wi = -wi;
+  o.x = b.x * wr - b.y * wi;
+  o.y = b.x * wi + b.y * wr;
+  return o;
+}
+
+// R-point DFT (R <= 16) of u[0..R-1] in registers, natural order in and out (radix-2 DIT)
+template <typename C, int R, bool INV>
+__device__ __forceinline__ void dft_reg(C* u) {
+  C w[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) w[i] = u[brev_c(i, R)];
+#pragma unroll
+  for (int h = 1; h < R; h <<= 1)
+#pragma unroll
+    for (int s = 0; s < R; s += 2 * h)
+#pragma unroll
+      for (int q = 0; q < h; ++q) {
+        const C a = w[s + q];
+        const C b = mul_w16<C, INV>(w[s + q + h], q * (R / (2 * h)) * (16 / R));
+        w[s + q] = cadd(a, b);
+        w[s + q + h] = csub(a, b);
+      }
+#pragma unroll
+  for (int i = 0; i < R; ++i) u[i] = w[i];
+}
+
+template <typename C, bool INV>
+__device__ __forceinline__ C mul_tw(C a, C w) {
+  if (INV) w.y = -w.y;
+  return cmul(a, w);
+}
+
+template <int N, int G, int E, int R, class In, class C>
+__device__ __forceinline__ void pass_load(int j, In in, C* v) {
+#pragma unroll
+  for (int b = 0; b < E / R; ++b)
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b * R + r] = in(j + G * b + r * (N / R));
+}
+
+template <int N, int G, int E, int R, int NS, bool INV, class Out, class C>
+__device__ __forceinline__ void pass_compute_store(int j, const C* __restrict__ tw, C* v, Out out) {
+#pragma unroll
+  for (int b = 0; b < E / R; ++b) {
+    const int jb = j + G * b, k = jb & (NS - 1);
+    C* u = v + b * R;
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) u[r] = mul_tw<C, INV>(u[r], __ldg(tw + k * r * (N / (NS * R))));
+    }
+    dft_reg<C, R, INV>(u);
+    const int base = (jb / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out(base + r * NS, u[r]);
+  }
+}
+
+// The transform of one line by its G threads (thread j of the line).  in(i) returns point i of
+// the input, out(i, z) receives point i of the result.  IN_SMEM / OUT_SMEM say that in / out
+// touch this line's shared-memory copy `line`, so that the pass separates them from its own
+// shared-memory traffic with barriers.  Every thread of the block must call it.
+template <typename C, int LOGN, bool INV, bool IN_SMEM, bool OUT_SMEM, class In, class Out>
+__device__ __forceinline__ void line_fft(int j, C* line, const C* __restrict__ tw, In in, Out out) {
+  typedef LineShape<LOGN> S;
+  constexpr int N = S::N, G = S::G, E = S::E, P = S::P;
+  C v[E];
+  auto sm_in = [&](int i) { return line[lpad(i)]; };
+  auto sm_out = [&](int i, C z) { line[lpad(i)] = z; };
+  pass_load<N, G, E, S::R(0)>(j, in, v);
+  if constexpr (P == 1) {
+    if (IN_SMEM && OUT_SMEM) __syncthreads();
+    pass_compute_store<N, G, E, S::R(0), 1, INV>(j, tw, v, out);
+  } else {
+    if (IN_SMEM) __syncthreads();
+    pass_compute_store<N, G, E, S::R(0), 1, INV>(j, tw, v, sm_out);
+    __syncthreads();
+    pass_load<N, G, E, S::R(1)>(j, sm_in, v);
+    if constexpr (P == 2) {
+      if (OUT_SMEM) __syncthreads();
+      pass_compute_store<N, G, E, S::R(1), S::NS(1), INV>(j, tw, v, out);
+    } else {
+      __syncthreads();
+      pass_compute_store<N, G, E, S::R(1), S::NS(1), INV>(j, tw, v, sm_out);
+      __syncthreads();
+      pass_load<N, G, E, S::R(2)>(j, sm_in, v);
+      if (OUT_SMEM) __syncthreads();
+      pass_compute_store<N, G, E, S::R(2), S::NS(2), INV>(j, tw, v, out);
+    }
+  }
+}
+
+// threads per block and lines per block of the line-FFT kernels
+__host__ __device__ constexpr int line_block(int logn) {
+  return ((1 << logn) / ((1 << logn) < 16 ? (1 << logn) : 16)) > 128 ? ((1 << logn) / 16) : 128;
+}
+__host__ __device__ constexpr int line_lines(int logn) {
+  return line_block(logn) / ((1 << logn) / ((1 << logn) < 16 ? (1 << logn) : 16));
 }
 
 // Offset of wavenumber m of row j, level k in an x-spectrum split into nblk blocks of
@@ -103,116 +216,99 @@ __device__ __forceinline__ long long spec_x_offset(int m, int nxh, int nblk, int
 }
 
 // ---- forward x: real rows (k, j), (k, j+1) -> half spectra ------------------------------
-template <typename T>
 // ny rows of each level are transformed: rows p_row0 .. p_row0+ny-1 of p, which holds p_rows rows
-// per level (a y-slab with halo rows has p_rows > ny).  The spectrum is split into nblk blocks of
-// consecutive wavenumbers (see spec_x_offset); nblk = 1 gives the plain [nz][ny][nx/2+1] layout.
-__global__ void k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g,
-                            int nx, int ny, int nz, int logn, int rows_per_cta, int p_rows, int p_row0, int nblk) {
+// per level (a y-slab with halo rows has p_rows > ny).  Two real rows are packed as the real and
+// imaginary parts of one complex line and separated after the transform.  The spectrum is split
+// into nblk blocks of consecutive wavenumbers (see spec_x_offset); nblk = 1 gives the plain
+// [nz][ny][nx/2+1] layout.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(line_block(LOGN)) k_fft_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restrict__ spec,
+                                                              const typename Cx<T>::t* __restrict__ tw, int ny, int nz,
+                                                              int p_rows, int p_row0, int nblk) {
   typedef typename Cx<T>::t C;
-  extern __shared__ unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  C* buf = tw + nx / 2;
-  for (int t = threadIdx.x; t < nx / 2; t += blockDim.x) tw[t] = tw_g[t];
-  const int pairs_per_level = ny / 2;
-  const long long pair0 = (long long)blockIdx.x * rows_per_cta;
-  const long long npairs = (long long)nz * pairs_per_level;
-  const int nxh = nx / 2 + 1;
-  const int prow = padded_row(nx);
-  for (int t = threadIdx.x; t < rows_per_cta * nx; t += blockDim.x) {
-    int r = t / nx, e = t - r * nx;
-    long long pr = pair0 + r;
+  typedef LineShape<LOGN> S;
+  constexpr int N = S::N, G = S::G, L = line_lines(LOGN);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int line = threadIdx.x / G, j = threadIdx.x - line * G;
+  C* buf = reinterpret_cast<C*>(smem_raw) + line * S::LPL;
+  const int pairs = ny / 2;
+  const long long pr = (long long)blockIdx.x * L + line;
+  const bool ok = pr < (long long)nz * pairs;
+  const int k = ok ? (int)(pr / pairs) + 1 : 1, jr = ok ? 2 * (int)(pr % pairs) : 0;
+  const T* row = p + ((long long)(k - 1) * p_rows + p_row0 + jr) * N;
+  auto in = [&](int e) {
     C z;
-    if (pr < npairs) {
-      int k = (int)(pr / pairs_per_level) + 1;
-      int j = 2 * (int)(pr % pairs_per_level);
-      const T* row = p + (long long)(k - 1) * nx * p_rows + (long long)(p_row0 + j) * nx;
-      z.x = row[e];
-      z.y = row[nx + e];
-    } else {
-      z.x = (T)0; z.y = (T)0;
-    }
-    int br = __brev(e) >> (32 - logn);
-    buf[r * prow + pidx(br)] = z;
-  }
+    if (ok) { z.x = row[e]; z.y = row[N + e]; } else { z.x = (T)0; z.y = (T)0; }
+    return z;
+  };
+  auto out = [&](int i, C z) { buf[lpad(i)] = z; };
+  line_fft<C, LOGN, false, false, true>(j, buf, tw, in, out);
   __syncthreads();
-  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, prow, 1, tw, false, false, true);
-  for (int t = threadIdx.x; t < rows_per_cta * nxh; t += blockDim.x) {
-    int r = t / nxh, m = t - r * nxh;
-    long long pr = pair0 + r;
-    if (pr >= npairs) continue;
-    int k = (int)(pr / pairs_per_level) + 1;
-    int j = 2 * (int)(pr % pairs_per_level);
-    C zm = buf[r * prow + pidx(m)];
-    C zn = buf[r * prow + pidx((nx - m) & (nx - 1))];
+  if (!ok) return;
+  constexpr int nxh = N / 2 + 1;
+  for (int m = j; m < nxh; m += G) {
+    const C zm = buf[lpad(m)];
+    const C zn = buf[lpad((N - m) & (N - 1))];
     C a, b;
     a.x = (T)0.5 * (zm.x + zn.x);
     a.y = (T)0.5 * (zm.y - zn.y);
     b.x = (T)0.5 * (zm.y + zn.y);
     b.y = (T)0.5 * (zn.x - zm.x);
     int w;
-    C* out = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, j, &w);
-    out[0] = a;
-    out[w] = b;
+    C* o = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, jr, &w);
+    o[0] = a;
+    o[w] = b;
   }
 }
 
 // ---- inverse x: half spectra -> real rows (k, j), (k, j+1) -----------------------------
-template <typename T>
-// the inverse of k_fft_x_fwd, with the same row window and spectrum blocks
-__global__ void k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g,
-                            int nx, int ny, int nz, int logn, int rows_per_cta, int p_rows, int p_row0, int nblk) {
+// the inverse of k_fft_x_fwd, with the same row window and spectrum blocks; the imaginary parts
+// of the kx = 0 and kx = nx/2 bins are dropped (the Hermitian completion of fftnorth.F90:54-73)
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(line_block(LOGN)) k_fft_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restrict__ spec,
+                                                              const typename Cx<T>::t* __restrict__ tw, int ny, int nz,
+                                                              int p_rows, int p_row0, int nblk) {
   typedef typename Cx<T>::t C;
-  extern __shared__ unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  C* buf = tw + nx / 2;
-  for (int t = threadIdx.x; t < nx / 2; t += blockDim.x) tw[t] = tw_g[t];
-  const int pairs_per_level = ny / 2;
-  const long long pair0 = (long long)blockIdx.x * rows_per_cta;
-  const long long npairs = (long long)nz * pairs_per_level;
-  const int nxh = nx / 2 + 1;
-  const int prow = padded_row(nx);
-  for (int t = threadIdx.x; t < rows_per_cta * nxh; t += blockDim.x) {
-    int r = t / nxh, m = t - r * nxh;
-    long long pr = pair0 + r;
+  typedef LineShape<LOGN> S;
+  constexpr int N = S::N, G = S::G, L = line_lines(LOGN);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int line = threadIdx.x / G, j = threadIdx.x - line * G;
+  C* buf = reinterpret_cast<C*>(smem_raw) + line * S::LPL;
+  const int pairs = ny / 2;
+  const long long pr = (long long)blockIdx.x * L + line;
+  const bool ok = pr < (long long)nz * pairs;
+  const int k = ok ? (int)(pr / pairs) + 1 : 1, jr = ok ? 2 * (int)(pr % pairs) : 0;
+  constexpr int nxh = N / 2 + 1;
+  for (int m = j; m < nxh; m += G) {
     C a, b;
-    if (pr < npairs) {
-      int k = (int)(pr / pairs_per_level) + 1;
-      int j = 2 * (int)(pr % pairs_per_level);
+    if (ok) {
       int w;
-      const C* in = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, j, &w);
+      const C* in = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, jr, &w);
       a = in[0];
       b = in[w];
     } else {
       a.x = a.y = b.x = b.y = (T)0;
     }
-    if (m == 0 || m == nx / 2) { a.y = (T)0; b.y = (T)0; }
+    if (m == 0 || m == N / 2) { a.y = (T)0; b.y = (T)0; }
     C z;
     z.x = a.x - b.y;
     z.y = a.y + b.x;
-    buf[r * prow + pidx(__brev(m) >> (32 - logn))] = z;
-    if (m > 0 && m < nx / 2) {
+    buf[lpad(m)] = z;
+    if (m > 0 && m < N / 2) {
       C zc;
       zc.x = a.x + b.y;
       zc.y = b.x - a.y;
-      int mm = nx - m;
-      buf[r * prow + pidx(__brev(mm) >> (32 - logn))] = zc;
+      buf[lpad(N - m)] = zc;
     }
   }
   __syncthreads();
-  smem_fft_stages<C>(buf, nx, logn, rows_per_cta, prow, 1, tw, true, false, true);
-  const T sc = (T)(1.0 / (double)nx);
-  for (int t = threadIdx.x; t < rows_per_cta * nx; t += blockDim.x) {
-    int r = t / nx, e = t - r * nx;
-    long long pr = pair0 + r;
-    if (pr >= npairs) continue;
-    int k = (int)(pr / pairs_per_level) + 1;
-    int j = 2 * (int)(pr % pairs_per_level);
-    T* row = p + (long long)(k - 1) * nx * p_rows + (long long)(p_row0 + j) * nx;
-    C z = buf[r * prow + pidx(e)];
-    row[e] = z.x * sc;
-    row[nx + e] = z.y * sc;
-  }
+  T* row = p + ((long long)(k - 1) * p_rows + p_row0 + jr) * N;
+  const T sc = (T)(1.0 / (double)N);
+  auto in = [&](int i) { return buf[lpad(i)]; };
+  auto out = [&](int e, C z) {
+    if (ok) { row[e] = z.x * sc; row[N + e] = z.y * sc; }
+  };
+  line_fft<C, LOGN, true, true, false>(j, buf, tw, in, out);
 }
 
 // ---- complex FFT along y on a tile of kx columns ------------------------------------------
@@ -224,36 +320,105 @@ __device__ __forceinline__ long long spec_row(int e, int k, int rpb, int ncols, 
   return ((long long)b * nz + (k - 1)) * rpb * ncols + (long long)(e - b * rpb) * ncols;
 }
 
-template <typename T>
-__global__ void k_fft_y(typename Cx<T>::t* __restrict__ spec, const typename Cx<T>::t* tw_g, int ncols, int ny, int logn,
-                        int cols, bool inverse, int nz, int rpb) {
+// One block per (tile of kx columns, level); consecutive threads take consecutive columns, so
+// the first pass's loads and the last pass's stores are coalesced across the tile.  The inverse
+// transform is scaled by 1/ny.
+template <typename T, int LOGN, bool INV>
+__global__ void __launch_bounds__(line_block(LOGN)) k_fft_y(typename Cx<T>::t* __restrict__ spec,
+                                                          const typename Cx<T>::t* __restrict__ tw, int ncols, int nz,
+                                                          int rpb) {
   typedef typename Cx<T>::t C;
-  extern __shared__ unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  C* buf = tw + ny / 2;
-  for (int t = threadIdx.x; t < ny / 2; t += blockDim.x) tw[t] = tw_g[t];
-  const int nxh = ncols;
-  const int kx0 = blockIdx.x * cols;
-  const int k = blockIdx.y + 1;
-  C* base = spec + kx0;
-  for (int t = threadIdx.x; t < cols * ny; t += blockDim.x) {
-    int e = t / cols, c = t - e * cols;
+  typedef LineShape<LOGN> S;
+  constexpr int N = S::N, COLS = line_lines(LOGN);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = threadIdx.x % COLS, j = threadIdx.x / COLS;
+  C* buf = reinterpret_cast<C*>(smem_raw) + c * S::LPL;
+  const int kx = blockIdx.x * COLS + c, k = blockIdx.y + 1;
+  const bool ok = kx < ncols;
+  C* col = spec + kx;
+  auto in = [&](int e) {
     C z;
-    if (kx0 + c < nxh) z = base[spec_row(e, k, rpb, ncols, nz) + c];
+    if (ok) z = col[spec_row(e, k, rpb, ncols, nz)];
     else { z.x = (T)0; z.y = (T)0; }
-    buf[(__brev(e) >> (32 - logn)) * cols + c] = z;
+    return z;
+  };
+  const T sc = INV ? (T)(1.0 / (double)N) : (T)1.0;
+  auto out = [&](int e, C z) {
+    if (!ok) return;
+    if (INV) { z.x = z.x * sc; z.y = z.y * sc; }
+    col[spec_row(e, k, rpb, ncols, nz)] = z;
+  };
+  line_fft<C, LOGN, INV, false, false>(j, buf, tw, in, out);
+}
+
+// ---- launches: one kernel instantiation per transform length (4 .. 4096 points) ----------------
+template <typename T>
+static size_t line_smem(int logn) {
+  return (size_t)line_lines(logn) * ((1 << logn) + (1 << logn) / 16 + 1) * sizeof(typename Cx<T>::t);
+}
+
+#define MGPU_LOGN_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+
+// the largest line needs more than the default 48 KB of dynamic shared memory: raise the limit
+// of every line kernel once per device
+template <typename T>
+static void ensure_line_attr() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+#define MGPU_SET_ATTR(L)                                                                                  \
+  cudaFuncSetAttribute(k_fft_x_fwd<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
+  cudaFuncSetAttribute(k_fft_x_inv<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
+  cudaFuncSetAttribute(k_fft_y<T, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
+  cudaFuncSetAttribute(k_fft_y<T, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L));
+  MGPU_LOGN_CASES(MGPU_SET_ATTR)
+#undef MGPU_SET_ATTR
+  done[dev] = true;
+}
+
+// x-FFT of `pairs_total` row pairs (nz levels of ny rows), forward or inverse
+template <typename T>
+static void launch_fft_x(bool inverse, int logn, T* p, typename Cx<T>::t* spec, const typename Cx<T>::t* tw, int ny,
+                         int nz, int p_rows, int p_row0, int nblk, cudaStream_t st) {
+  ensure_line_attr<T>();
+  const long long pairs = (long long)nz * (ny / 2);
+  const int L = line_lines(logn);
+  const unsigned grid = (unsigned)((pairs + L - 1) / L);
+  const int block = line_block(logn);
+  const size_t smem = line_smem<T>(logn);
+  switch (logn) {
+#define MGPU_X_CASE(LG)                                                                                     \
+  case LG:                                                                                                  \
+    if (inverse) k_fft_x_inv<T, LG><<<grid, block, smem, st>>>(p, spec, tw, ny, nz, p_rows, p_row0, nblk);  \
+    else k_fft_x_fwd<T, LG><<<grid, block, smem, st>>>(p, spec, tw, ny, nz, p_rows, p_row0, nblk);          \
+    break;
+    MGPU_LOGN_CASES(MGPU_X_CASE)
+#undef MGPU_X_CASE
+    default: break;
   }
-  __syncthreads();
-  // rows = columns here: element e of column c at buf[e*cols + c]
-  smem_fft_stages<C>(buf, ny, logn, cols, 1, cols, tw, inverse, true);
-  const T sc = inverse ? (T)(1.0 / (double)ny) : (T)1.0;
-  for (int t = threadIdx.x; t < cols * ny; t += blockDim.x) {
-    int e = t / cols, c = t - e * cols;
-    if (kx0 + c >= nxh) continue;
-    C z = buf[e * cols + c];
-    z.x = z.x * sc;
-    z.y = z.y * sc;
-    base[spec_row(e, k, rpb, ncols, nz) + c] = z;
+}
+
+// y-FFT of ncols columns of 2^logn rows on each of nz levels (rows in blocks of rpb)
+template <typename T>
+static void launch_fft_y(bool inverse, int logn, typename Cx<T>::t* spec, const typename Cx<T>::t* tw, int ncols, int nz,
+                         int rpb, cudaStream_t st) {
+  ensure_line_attr<T>();
+  const int cols = line_lines(logn);
+  dim3 grid((unsigned)((ncols + cols - 1) / cols), (unsigned)nz);
+  const int block = line_block(logn);
+  const size_t smem = line_smem<T>(logn);
+  switch (logn) {
+#define MGPU_Y_CASE(LG)                                                                        \
+  case LG:                                                                                     \
+    if (inverse) k_fft_y<T, LG, true><<<grid, block, smem, st>>>(spec, tw, ncols, nz, rpb);    \
+    else k_fft_y<T, LG, false><<<grid, block, smem, st>>>(spec, tw, ncols, nz, rpb);           \
+    break;
+    MGPU_LOGN_CASES(MGPU_Y_CASE)
+#undef MGPU_Y_CASE
+    default: break;
   }
 }
 
@@ -471,25 +636,6 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   cp_async_wait_0();
 }
 
-// ---------------------------------------------------------------------------------------------
-struct FftSizes {
-  int rows_x, cols_y, logx, logy;
-  size_t smem_x, smem_y;
-};
-
-template <typename T>
-static FftSizes sizes(const FftPlanDev& pl) {
-  FftSizes z;
-  const size_t cs = sizeof(typename Cx<T>::t);
-  z.logx = ilog2(pl.nx);
-  z.logy = ilog2(pl.ny);
-  z.rows_x = (int)std::max<size_t>(1, 32768 / (pl.nx * cs));
-  z.cols_y = (int)std::min<size_t>(16, std::max<size_t>(1, 32768 / (pl.ny * cs)));
-  z.smem_x = cs * (pl.nx / 2 + (size_t)z.rows_x * padded_row(pl.nx));
-  z.smem_y = cs * (pl.ny / 2 + (size_t)z.cols_y * pl.ny);
-  return z;
-}
-
 // Pivots and twiddles of the (pl.nx, pl.ny, pl.nz) grid; pl.spec and pl.s1 are left to the caller.
 static int plan_tables(FftPlanDev& pl, const RefState& rs) {
   // Thomas pivots per (|ky|, kx), built exactly as fftsolver.F90:259-280 and :72-90
@@ -513,39 +659,24 @@ static int plan_tables(FftPlanDev& pl, const RefState& rs) {
     }
   if (cudaMalloc(&pl.b1, b1.size() * sizeof(double)) != cudaSuccess) return MGPU_ERR_CUDA;
   cudaMemcpy(pl.b1, b1.data(), b1.size() * sizeof(double), cudaMemcpyHostToDevice);
+  // twiddles W_n^q = e^{-2 pi i q / n}, q < n (interleaved complex), and the same rounded to FP32
   auto twiddles = [&](int n, double** dd, float** df) {
-    std::vector<double> t(n);
-    std::vector<float> tf(n);
-    for (int q = 0; q < n / 2; ++q) {
+    std::vector<double> t(2 * (size_t)n);
+    std::vector<float> tf(2 * (size_t)n);
+    for (int q = 0; q < n; ++q) {
       double a = 2.0 * PI * (double)q / (double)n;
       t[2 * q] = std::cos(a);
       t[2 * q + 1] = -std::sin(a);
       tf[2 * q] = (float)t[2 * q];
       tf[2 * q + 1] = (float)t[2 * q + 1];
     }
-    cudaMalloc(dd, n * sizeof(double));
-    cudaMalloc(df, n * sizeof(float));
-    cudaMemcpy(*dd, t.data(), n * sizeof(double), cudaMemcpyHostToDevice);
-    cudaMemcpy(*df, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMalloc(dd, 2 * (size_t)n * sizeof(double));
+    cudaMalloc(df, 2 * (size_t)n * sizeof(float));
+    cudaMemcpy(*dd, t.data(), 2 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(*df, tf.data(), 2 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
   };
   twiddles(pl.nx, &pl.twx, &pl.twx_f);
   twiddles(pl.ny, &pl.twy, &pl.twy_f);
-  FftSizes zd = sizes<double>(pl), zf = sizes<float>(pl);
-  size_t mx = std::max(std::max(zd.smem_x, zd.smem_y), std::max(zf.smem_x, zf.smem_y));
-  // the attribute belongs to the kernel, not to the plan: only ever raise it, so that a smaller
-  // plan created later does not cut the limit an earlier, larger one needs
-  static std::mutex mu;
-  static size_t raised = 48 * 1024;
-  std::lock_guard<std::mutex> lock(mu);
-  if (mx > raised) {
-    raised = mx;
-    cudaFuncSetAttribute(k_fft_x_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    cudaFuncSetAttribute(k_fft_x_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    cudaFuncSetAttribute(k_fft_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    cudaFuncSetAttribute(k_fft_x_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    cudaFuncSetAttribute(k_fft_x_inv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    cudaFuncSetAttribute(k_fft_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-  }
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
 }
 
@@ -591,30 +722,26 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
                bool transpose) {
   typedef typename Cx<T>::t C;
   const bool f32 = sizeof(T) == 4;
-  FftSizes z = sizes<T>(pl);
   C* spec = reinterpret_cast<C*>(pl.spec);
   const C* twx = reinterpret_cast<const C*>(f32 ? (void*)pl.twx_f : (void*)pl.twx);
   const C* twy = reinterpret_cast<const C*>(f32 ? (void*)pl.twy_f : (void*)pl.twy);
-  const long long npairs = (long long)s.nz * (s.ny / 2);
-  const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
+  const int logx = ilog2(s.nx), logy = ilog2(s.ny);
   const size_t plane = (size_t)s.ny * pl.nxh;
   double2* s1 = pl.s1;
   auto mark = [&](int q) { if (evs) cudaEventRecord(evs[q], st); };
   mark(0);
-  k_fft_x_fwd<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x, s.ny, 0, 1);
+  launch_fft_x<T>(false, logx, p, spec, twx, s.ny, s.nz, s.ny, 0, 1, st);
   mark(1);
-  dim3 gy((pl.nxh + z.cols_y - 1) / z.cols_y, s.nz);
-  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, false, s.nz, s.ny);
+  launch_fft_y<T>(false, logy, spec, twy, pl.nxh, s.nz, s.ny, st);
   mark(2);
   long long ncol = (long long)plane;
   ensure_tri_attr();
   k_tridiag<T><<<(unsigned)((ncol + TRI_TB - 1) / TRI_TB + 1), TRI_TB, tri_smem_bytes<C>(s.nz), st>>>(
-      spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz,
-                                                               transpose ? 1 : 0, pl.nxh, 0, s.ny);
+      spec, s1, pl.b1, s.prof, s.nz + 2, s.nx, s.ny, s.nz, transpose ? 1 : 0, pl.nxh, 0, s.ny);
   mark(3);
-  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(spec, twy, pl.nxh, s.ny, z.logy, z.cols_y, true, s.nz, s.ny);
+  launch_fft_y<T>(true, logy, spec, twy, pl.nxh, s.nz, s.ny, st);
   mark(4);
-  k_fft_x_inv<T><<<gx, 256, z.smem_x, st>>>(p, spec, twx, s.nx, s.ny, s.nz, z.logx, z.rows_x, s.ny, 0, 1);
+  launch_fft_x<T>(true, logx, p, spec, twx, s.ny, s.nz, s.ny, 0, 1, st);
   mark(5);
   *launches += 5;
 }
@@ -628,16 +755,10 @@ void slab_fft_x(const FftPlanDev& pl, const Scalars& s, T* p, int halo, int nblk
                 cudaStream_t st, int64_t* launches) {
   typedef typename Cx<T>::t C;
   const bool f32 = sizeof(T) == 4;
-  FftSizes z = sizes<T>(pl);
   const C* twx = reinterpret_cast<const C*>(f32 ? (void*)pl.twx_f : (void*)pl.twx);
   C* sp = reinterpret_cast<C*>(spec);
   const int nyl = s.ny - 2 * halo;
-  const long long npairs = (long long)s.nz * (nyl / 2);
-  const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
-  if (!inverse)
-    k_fft_x_fwd<T><<<gx, 256, z.smem_x, st>>>(p, sp, twx, s.nx, nyl, s.nz, z.logx, z.rows_x, s.ny, halo, nblk);
-  else
-    k_fft_x_inv<T><<<gx, 256, z.smem_x, st>>>(p, sp, twx, s.nx, nyl, s.nz, z.logx, z.rows_x, s.ny, halo, nblk);
+  launch_fft_x<T>(inverse, ilog2(s.nx), p, sp, twx, nyl, s.nz, s.ny, halo, nblk, st);
   *launches += 1;
 }
 
@@ -646,17 +767,15 @@ void slab_solve_columns(const FftPlanDev& pl, const Scalars& s, void* spec, int 
                         cudaStream_t st, int64_t* launches) {
   typedef typename Cx<T>::t C;
   const bool f32 = sizeof(T) == 4;
-  FftSizes z = sizes<T>(pl);
   const C* twy = reinterpret_cast<const C*>(f32 ? (void*)pl.twy_f : (void*)pl.twy);
   C* sp = reinterpret_cast<C*>(spec);
-  dim3 gy((nkx + z.cols_y - 1) / z.cols_y, s.nz);
+  const int logy = ilog2(pl.ny);
   const long long ncol = (long long)pl.ny * nkx;
-  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, false, s.nz, rpb);
+  launch_fft_y<T>(false, logy, sp, twy, nkx, s.nz, rpb, st);
   ensure_tri_attr();
   k_tridiag<T><<<(unsigned)((ncol + TRI_TB - 1) / TRI_TB + (kx0 == 0 ? 1 : 0)), TRI_TB, tri_smem_bytes<C>(s.nz), st>>>(
-      sp, pl.s1, pl.b1, s.prof, s.nz + 2, pl.nx, pl.ny, s.nz,
-                                                               transpose ? 1 : 0, nkx, kx0, rpb);
-  k_fft_y<T><<<gy, 256, z.smem_y, st>>>(sp, twy, nkx, pl.ny, z.logy, z.cols_y, true, s.nz, rpb);
+      sp, pl.s1, pl.b1, s.prof, s.nz + 2, pl.nx, pl.ny, s.nz, transpose ? 1 : 0, nkx, kx0, rpb);
+  launch_fft_y<T>(true, logy, sp, twy, nkx, s.nz, rpb, st);
   *launches += 3;
 }
 
@@ -776,10 +895,10 @@ static void* noalloc_scratch_address(int* status) {
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// twiddles e^{-2 pi i q / n}, q < n/2
+// twiddles e^{-2 pi i q / n}, q < n
 __global__ void k_noalloc_twiddles(double2* tw, int n) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n / 2) return;
+  if (q >= n) return;
   double sv, cv;
   sincospi(2.0 * (double)q / (double)n, &sv, &cv);
   tw[q] = make_double2(cv, -sv);
@@ -824,8 +943,8 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   const size_t b_spec = align256(sizeof(double2) * plane * nz);
   const size_t b_s1 = align256(sizeof(double2) * plane * nz);
   const size_t b_b1 = align256(sizeof(double) * (size_t)(nz + 1) * nyh * nxh);
-  const size_t b_twx = align256(sizeof(double2) * (nx / 2));
-  const size_t b_twy = align256(sizeof(double2) * (ny / 2));
+  const size_t b_twx = align256(sizeof(double2) * nx);
+  const size_t b_twy = align256(sizeof(double2) * ny);
   const size_t b_prof = align256(sizeof(double) * (size_t)P_COUNT * stride);
   const size_t need = b_spec + b_s1 + b_b1 + b_twx + b_twy + b_prof;
   if (need > (size_t)MGPU_NOALLOC_SCRATCH_BYTES) {
@@ -852,29 +971,16 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
     if (cudaMemcpyAsync(prof + (size_t)ids[q] * stride + 1, src[q], sizeof(double) * nz, cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
       return MGPU_ERR_CUDA;
-  k_noalloc_twiddles<<<(nx / 2 + 127) / 128, 128, 0, st>>>(twx, nx);
-  k_noalloc_twiddles<<<(ny / 2 + 127) / 128, 128, 0, st>>>(twy, ny);
+  k_noalloc_twiddles<<<(nx + 127) / 128, 128, 0, st>>>(twx, nx);
+  k_noalloc_twiddles<<<(ny + 127) / 128, 128, 0, st>>>(twy, ny);
   k_noalloc_pivots<<<(nyh * nxh + 127) / 128, 128, 0, st>>>(b1, prof, stride, nx, ny, nz, dx, dy);
   // the five solve kernels of fft_solve, on the scratch buffers
-  FftPlanDev pl;
-  pl.nx = nx;
-  pl.ny = ny;
-  pl.nz = nz;
-  pl.nxh = nxh;
-  FftSizes z = sizes<double>(pl);
-  if (z.smem_x > 48 * 1024 || z.smem_y > 48 * 1024) {
-    std::fprintf(stderr, "mgpu_poisson_fft_noalloc: rows of %d or %d points exceed the shared-memory tile\n", nx, ny);
-    return MGPU_ERR_ARGUMENT;
-  }
-  const long long npairs = (long long)nz * (ny / 2);
-  const int gx = (int)((npairs + z.rows_x - 1) / z.rows_x);
-  dim3 gy((nxh + z.cols_y - 1) / z.cols_y, nz);
-  k_fft_x_fwd<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
-  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, false, nz, ny);
+  launch_fft_x<double>(false, ilog2(nx), p, spec, twx, ny, nz, ny, 0, 1, st);
+  launch_fft_y<double>(false, ilog2(ny), spec, twy, nxh, nz, ny, st);
   ensure_tri_attr();
   k_tridiag<double><<<(unsigned)((plane + TRI_TB - 1) / TRI_TB + 1), TRI_TB, tri_smem_bytes<double2>(nz), st>>>(
       spec, s1, b1, prof, stride, nx, ny, nz, 0, nxh, 0, ny);
-  k_fft_y<double><<<gy, 256, z.smem_y, st>>>(spec, twy, nxh, ny, z.logy, z.cols_y, true, nz, ny);
-  k_fft_x_inv<double><<<gx, 256, z.smem_x, st>>>(p, spec, twx, nx, ny, nz, z.logx, z.rows_x, ny, 0, 1);
+  launch_fft_y<double>(true, ilog2(ny), spec, twy, nxh, nz, ny, st);
+  launch_fft_x<double>(true, ilog2(nx), p, spec, twx, ny, nz, ny, 0, 1, st);
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
 }
