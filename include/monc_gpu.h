@@ -36,6 +36,7 @@ extern "C" {
 #define MGPU_ERR_TIMEOUT       -4   /* a bounded device-side wait gave up */
 #define MGPU_ERR_UNSUPPORTED   -5   /* option not implemented on this path */
 #define MGPU_ERR_NO_DEVICE     -6   /* no CUDA device visible */
+#define MGPU_ERR_CFL           -7   /* cfltest: the new timestep fell below cfl_dtmmin (MONC stops) */
 
 /* precision modes */
 #define MGPU_FP64        0  /* every field and every operation in FP64 (MONC's DEFAULT_PRECISION) */
@@ -130,6 +131,14 @@ typedef struct mgpu_config {
   /* science constants (global_config:355-372) */
   double  von_karman_constant, z0, z0th, alphah, betam, betah, gammam, gammah;
   double  pi, cp, rlvap, r, G, convective_limit, ratio_mol_wts, rlargep;
+  /* cfltest (cfltest.F90:44-58, global_config:19,113,137-143): adaptive dtm from the advective and
+   * viscous Courant numbers, evaluated every cfl_frequency steps inside mgpu_step.  cfl_enabled = 0
+   * keeps dtm fixed. */
+  int32_t cfl_enabled;                /* cfltest_enabled */
+  int32_t cfl_frequency;              /* cfl_frequency */
+  double  cfl_tollerance, cfl_cvismax, cfl_cvelmax; /* cfl_tollerance, cfl_cvismax, cfl_cvelmax */
+  double  cfl_dtmmax, cfl_dtmmin, cfl_rincmax;      /* cfl_dtmmax, cfl_dtmmin, cfl_rincmax */
+  int32_t l_constant_dtm;             /* l_constant_dtm */
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */
@@ -138,6 +147,14 @@ typedef struct mgpu_reductions {
   int32_t solver_iterations;          /* iterations of the last iterative solve */
   double  solver_residual;            /* relative residual of the last iterative solve */
   int32_t timestep;                   /* next MONC timestep number (1 = first, forward) */
+  /* cfltest state after the last step (cfltest.F90:62-128, 135-191) */
+  double  dtm;                        /* timestep of the last step */
+  double  dtm_new;                    /* timestep of the next step */
+  double  absolute_new_dtm;           /* target of the last CFL evaluation */
+  double  cvel, cvis, cfl_number;     /* Courant numbers of the last evaluation (scaled by dtm) */
+  double  cvel_x, cvel_y, cvel_z;     /* their advective parts before the dtm scaling */
+  int32_t cfl_evaluations;            /* CFL evaluations so far */
+  int32_t last_cfl_timestep;          /* timestep of the last evaluation */
 } mgpu_reductions;
 
 typedef struct mgpu_handle mgpu_handle;
@@ -184,6 +201,13 @@ int mgpu_component_timestep(mgpu_handle* h, int32_t component_id);
 int mgpu_set_timestep(mgpu_handle* h, int32_t timestep);
 
 int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out);
+
+/* The flow and viscosity extrema cfltest reads, gathered on the device from the current fields
+ * (replaces stepfields.F90:372-393 determine_local_flow_minmax and smagorinsky.F90:143-173
+ * update_viscous_number, for a CPU cfltest driving GPU-resident fields): out[0..5] = min zu, max zu,
+ * min zv, max zv (levels 2..nz), max over k = 2..nz-1 of |zw| rdzn(k+1), max over k = 2..nz-1 of
+ * max(vis, diff) (rdzn(k+1)^2 + cx2 + cy2).  Synchronous; reads back 48 bytes. */
+int mgpu_cfl_gather(mgpu_handle* h, double* out);
 
 /* Horizontal-mean profile of a field (meanprofiles.F90:155-293 style sum / (nx*ny)). */
 int mgpu_mean_profile(mgpu_handle* h, int32_t field_id, double* out);

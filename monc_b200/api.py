@@ -30,6 +30,7 @@ ERR_NOT_CONVERGED = -3
 ERR_TIMEOUT = -4
 ERR_UNSUPPORTED = -5
 ERR_NO_DEVICE = -6
+ERR_CFL = -7
 
 LAYOUT_XFAST = 0
 LAYOUT_MONC = 1
@@ -89,7 +90,11 @@ class MgpuError(RuntimeError):
 
 class Reductions(C.Structure):
     _fields_ = [("global_divmax", C.c_double), ("solver_iterations", C.c_int32),
-                ("solver_residual", C.c_double), ("timestep", C.c_int32)]
+                ("solver_residual", C.c_double), ("timestep", C.c_int32),
+                ("dtm", C.c_double), ("dtm_new", C.c_double), ("absolute_new_dtm", C.c_double),
+                ("cvel", C.c_double), ("cvis", C.c_double), ("cfl_number", C.c_double),
+                ("cvel_x", C.c_double), ("cvel_y", C.c_double), ("cvel_z", C.c_double),
+                ("cfl_evaluations", C.c_int32), ("last_cfl_timestep", C.c_int32)]
 
 
 _lib = None
@@ -124,6 +129,8 @@ def lib():
     L.mgpu_set_timestep.restype = C.c_int
     L.mgpu_get_reductions.argtypes = [C.c_void_p, C.c_void_p]
     L.mgpu_get_reductions.restype = C.c_int
+    L.mgpu_cfl_gather.argtypes = [C.c_void_p, C.c_void_p]
+    L.mgpu_cfl_gather.restype = C.c_int
     L.mgpu_mean_profile.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.mgpu_mean_profile.restype = C.c_int
     L.mgpu_stream.argtypes = [C.c_void_p]
@@ -283,6 +290,13 @@ class Model:
         r = Reductions()
         self._check(lib().mgpu_get_reductions(self.h, C.byref(r)), "reductions")
         return r
+
+    def cfl_gather(self) -> np.ndarray:
+        """cfltest's extrema from the current fields: min zu, max zu, min zv, max zv,
+        max |zw| rdzn(k+1), max max(vis, diff) (rdzn(k+1)^2 + cx2 + cy2)."""
+        out = np.zeros(6, dtype=np.float64)
+        self._check(lib().mgpu_cfl_gather(self.h, out.ctypes.data), "cfl_gather")
+        return out
 
     def mean_profile(self, name) -> np.ndarray:
         out = np.empty(self.nz, dtype=np.float64)

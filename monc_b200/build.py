@@ -28,6 +28,7 @@ UNITS = [
     ("iter.cu", []),
     ("tlad.cu", []),
     ("slab.cu", []),
+    ("cfl.cu", []),
 ]
 
 

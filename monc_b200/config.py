@@ -64,6 +64,10 @@ class MgpuConfig(C.Structure):
         ("pi", C.c_double), ("cp", C.c_double), ("rlvap", C.c_double), ("r", C.c_double),
         ("G", C.c_double), ("convective_limit", C.c_double), ("ratio_mol_wts", C.c_double),
         ("rlargep", C.c_double),
+        ("cfl_enabled", C.c_int32), ("cfl_frequency", C.c_int32),
+        ("cfl_tollerance", C.c_double), ("cfl_cvismax", C.c_double), ("cfl_cvelmax", C.c_double),
+        ("cfl_dtmmax", C.c_double), ("cfl_dtmmin", C.c_double), ("cfl_rincmax", C.c_double),
+        ("l_constant_dtm", C.c_int32),
     ]
 
 
@@ -122,6 +126,15 @@ def default_config() -> MgpuConfig:
     c.convective_limit = -0.5
     c.ratio_mol_wts = 1.608
     c.rlargep = 1.0e37
+    c.cfl_enabled = 1
+    c.cfl_frequency = 10
+    c.cfl_tollerance = 0.1
+    c.cfl_cvismax = 0.2
+    c.cfl_cvelmax = 0.2
+    c.cfl_dtmmax = 100.0
+    c.cfl_dtmmin = 0.0001
+    c.cfl_rincmax = 0.05
+    c.l_constant_dtm = 0
     return c
 
 
@@ -134,6 +147,7 @@ def dry_cbl_config(nx: int, ny: int, nz: int, dx: float, dz: float, dtm: float,
     The surface sensible heat flux is given kinematically (K m/s); MONC takes W m-2 and divides
     by rho(1)*cp (setfluxlook.F90:84-85), so the W m-2 value passed is shf_kms*rhobous*cp.
     Cs maps to MONC's rmlmax = Cs*max(dx,dy) (simplesetup.F90:234 uses 0.23 as the default).
+    The timestep is fixed (cfltest off), as the benchmark cases run; enable_cfl() turns it on.
     """
     c = default_config()
     c.nx, c.ny, c.nz = nx, ny, nz
@@ -160,6 +174,19 @@ def dry_cbl_config(nx: int, ny: int, nz: int, dx: float, dz: float, dtm: float,
         c.surface_geostrophic_wind_x = ug
     c.precision = precision
     c.solver = solver
+    c.cfl_enabled = 0
+    return c
+
+
+def enable_cfl(c: MgpuConfig, frequency: int = 10, dtmmax: float = 100.0, dtmmin: float = 1e-4,
+               rincmax: float = 0.05, tollerance: float = 0.1, cvismax: float = 0.2, cvelmax: float = 0.2,
+               constant_dtm: bool = False) -> MgpuConfig:
+    """Switch on cfltest with MONC's option names (global_config:137-143 defaults)."""
+    c.cfl_enabled = 1
+    c.cfl_frequency = frequency
+    c.cfl_dtmmax, c.cfl_dtmmin, c.cfl_rincmax = dtmmax, dtmmin, rincmax
+    c.cfl_tollerance, c.cfl_cvismax, c.cfl_cvelmax = tollerance, cvismax, cvelmax
+    c.l_constant_dtm = 1 if constant_dtm else 0
     return c
 
 

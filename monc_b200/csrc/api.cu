@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -64,6 +65,17 @@ struct mgpu_handle {
   int slab_halo = 0, slab_ny_global = 0, slab_cols = 0;
   FftPlanDev slab;
   const double* bmean_ext = nullptr;  // FP32-mixed: the domain level means for the next dynamics phase
+  // cfltest (cfltest.F90:62-191) when cfg.cfl_enabled: state carried between steps
+  struct {
+    int last_cfl_timestep = 0, evaluations = 0;
+    bool update_dtm = false;
+    double dtm_new = 0.0, absolute_new_dtm = 0.0, dtm_last = 0.0;
+    double cvel = 0.0, cvis = 0.0, cfl_number = 0.0, cvel_x = 0.0, cvel_y = 0.0, cvel_z = 0.0;
+    double* part_d = nullptr;  // CFL_BLOCKS*6 block partials
+    double* out_d = nullptr;   // 6 reduced values
+    double* out_h = nullptr;   // the same, pinned host copy
+    cudaEvent_t ev = nullptr;  // recorded after the copy to out_h
+  } cfl;
   std::string err;
 };
 
@@ -204,6 +216,9 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
       (cfg->solver != MGPU_SOLVER_FFT && cfg->solver != MGPU_SOLVER_ITERATIVE && cfg->solver != MGPU_SOLVER_EXTERNAL) ||
       (cfg->solver == MGPU_SOLVER_FFT && (!pow2(cfg->nx) || !pow2(cfg->ny))) || !(cfg->dtm > 0.0))
     return MGPU_ERR_ARGUMENT;
+  if (cfg->cfl_enabled && (cfg->cfl_frequency < 1 || !(cfg->cfl_cvismax > 0.0) || !(cfg->cfl_cvelmax > 0.0) ||
+                           !(cfg->cfl_dtmmax > 0.0) || cfg->cfl_rincmax < 0.0 || cfg->solver == MGPU_SOLVER_EXTERNAL))
+    return MGPU_ERR_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MGPU_ERR_NO_DEVICE;
   mgpu_handle* h = new mgpu_handle();
@@ -241,6 +256,14 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   for (cudaEvent_t& e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
   fill_scalars(h);
+  h->cfl.dtm_last = cfg->dtm;
+  h->cfl.dtm_new = cfg->dtm;
+  h->cfl.absolute_new_dtm = cfg->dtm;
+  if (cudaMalloc(&h->cfl.part_d, (size_t)CFL_BLOCKS * 6 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->cfl.out_d, 6 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&h->cfl.out_h, 6 * sizeof(double)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->cfl.ev, cudaEventDisableTiming) != cudaSuccess)
+    return cleanup(MGPU_ERR_CUDA);
   rc = h->fp32 ? alloc_state<float>(h, h->d32) : alloc_state<double>(h, h->d64);
   if (rc) return cleanup(rc);
   if (cfg->solver == MGPU_SOLVER_FFT) {
@@ -275,6 +298,10 @@ int mgpu_destroy(mgpu_handle* h) {
   cudaFree(h->xfer);
   cudaFree(h->diag_d);
   cudaFree(h->bmean_d);
+  cudaFree(h->cfl.part_d);
+  cudaFree(h->cfl.out_d);
+  if (h->cfl.out_h) cudaFreeHost(h->cfl.out_h);
+  if (h->cfl.ev) cudaEventDestroy(h->cfl.ev);
   for (cudaEvent_t& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -302,6 +329,8 @@ static int ad_alloc(mgpu_handle* h, double** p, size_t n) {
 }
 
 static int ad_supported(mgpu_handle* h) {
+  if (h->cfg.cfl_enabled)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs hold dtm fixed: disable cfltest");
   if (h->fp32 || h->cfg.number_q_fields > 0 || h->cfg.solver != MGPU_SOLVER_FFT)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs need a dry FP64 model with the FFT solver");
   return MGPU_OK;
@@ -536,13 +565,76 @@ static void collect_stage_times(mgpu_handle* h) {
   acc(8, 8, 9);
 }
 
+// cfltest's evaluation test (cfltest.F90:80-82; the same test gates the gathers in
+// stepfields.F90:249-256 and smagorinsky.F90:151-153): every step up to cfl_frequency, then every
+// cfl_frequency steps (start_timestep = 1, no reconfiguration offset)
+static bool cfl_evaluation_step(const mgpu_handle* h, int n) {
+  const int f = h->cfg.cfl_frequency;
+  return n % f == 1 || n - 1 <= f || n >= h->cfl.last_cfl_timestep + f;
+}
+
+// cfltest's timestep callback (cfltest.F90:62-128) and update_dtm_based_on_absolute (:135-191), on
+// the host: `evaluate` when this step gathered the extrema into cfl.out_h.  The new dtm takes
+// effect at the start of the next step (monc.F90:313).  Galilean transformation is off
+// (global_config:268): ugal = vgal = 0.  The output-time alignment of time_basis runs is not on
+// this path.
+static int cfltest_callback(mgpu_handle* h, bool evaluate) {
+  auto& c = h->cfl;
+  const mgpu_config& g = h->cfg;
+  const double dtm = h->sc.dtm;
+  c.dtm_last = dtm;
+  c.update_dtm = false;
+  if (evaluate) {
+    if (cudaEventSynchronize(c.ev) != cudaSuccess) return fail(h, MGPU_ERR_CUDA, "cfltest read-back");
+    const double* r = c.out_h;
+    c.last_cfl_timestep = h->timestep;
+    c.evaluations += 1;
+    const double ugal = 0.0, vgal = 0.0;
+    const double zumin = r[0] + ugal, zumax = r[1] + ugal, zvmin = r[2] + vgal, zvmax = r[3] + vgal;
+    c.cvel_z = r[4];
+    c.cvel_x = std::max(std::fabs(zumax - ugal), std::fabs(zumin - ugal));
+    c.cvel_y = std::max(std::fabs(zvmax - vgal), std::fabs(zvmin - vgal));
+    c.cvel = (c.cvel_x * h->sc.cx + c.cvel_y * h->sc.cy + c.cvel_z) * dtm;
+    c.cvis = r[5] * (dtm * 4);
+    c.cfl_number = c.cvis / g.cfl_cvismax + c.cvel / g.cfl_cvelmax;
+    c.absolute_new_dtm = dtm;
+    if (c.cfl_number > 0.0 &&
+        (c.cfl_number < (1.0 - g.cfl_tollerance) || c.cfl_number > (1.0 + g.cfl_tollerance)))
+      c.absolute_new_dtm = dtm / c.cfl_number;
+  }
+  if (dtm != c.absolute_new_dtm && (dtm != g.cfl_dtmmax || c.absolute_new_dtm < g.cfl_dtmmax)) {
+    c.update_dtm = true;
+    c.dtm_new = std::min(std::min(dtm * (1.0 + g.cfl_rincmax), c.absolute_new_dtm), g.cfl_dtmmax);
+    if (c.dtm_new < g.cfl_dtmmin && !g.l_constant_dtm)
+      return fail(h, MGPU_ERR_CFL, "cfltest: timestep too small, dtm_new=" + std::to_string(c.dtm_new) +
+                                       " < cfl_dtmmin=" + std::to_string(g.cfl_dtmmin));
+  }
+  if (g.l_constant_dtm) {
+    h->sc.dtm = g.dtm;
+    c.dtm_new = g.dtm;
+    c.update_dtm = false;
+  }
+  return MGPU_OK;
+}
+
 template <typename T>
 static int step_once(mgpu_handle* h, DevState<T>& d) {
+  const bool cfl = h->cfg.cfl_enabled != 0;
+  if (cfl && h->cfl.update_dtm) h->sc.dtm = h->cfl.dtm_new;  // monc.F90:313
+  const bool cfl_gather = cfl && cfl_evaluation_step(h, h->timestep);
   h->sc.forward = (h->timestep == 1) ? 1 : 0;  // steppingdirection.F90:44-48
   auto mark = [&](int q) { if (h->profiling) cudaEventRecord(h->ev[q], h->stream); };
   mark(0);
   if (h->cfg.reproducible) h->launches += exact::launch_fused_subgrid<T>(h->sc, d, h->stream);
   else h->launches += fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
+  if (cfl_gather) {
+    // the extrema of the pre-step zu, zv, zw and of this step's vis, diff (zu..zw change only in
+    // the pressure step at the end of the step)
+    h->launches += launch_cfl_gather<T>(h->sc, d, h->cfg.use_viscosity_and_diffusion != 0, h->cfl.part_d,
+                                        h->cfl.out_d, h->stream);
+    cudaMemcpyAsync(h->cfl.out_h, h->cfl.out_d, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaEventRecord(h->cfl.ev, h->stream);
+  }
   mark(1);
   cudaEvent_t mid = h->profiling ? h->ev[10] : nullptr;
   if (sizeof(T) == 4) {
@@ -567,6 +659,11 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
   mark(9);
   h->launches += 1;
+  if (cfl) {
+    // cfltest runs in the solver group; it only sets the next step's dtm
+    int rc = cfltest_callback(h, cfl_gather);
+    if (rc) return rc;
+  }
   h->timestep += 1;
   if (h->profiling) collect_stage_times(h);
   return MGPU_OK;
@@ -816,6 +913,17 @@ int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out) {
   out->solver_iterations = h->solver_iterations;
   out->solver_residual = h->solver_residual;
   out->timestep = h->timestep;
+  out->dtm = h->cfl.dtm_last;
+  out->dtm_new = h->cfl.update_dtm ? h->cfl.dtm_new : h->sc.dtm;
+  out->absolute_new_dtm = h->cfl.absolute_new_dtm;
+  out->cvel = h->cfl.cvel;
+  out->cvis = h->cfl.cvis;
+  out->cfl_number = h->cfl.cfl_number;
+  out->cvel_x = h->cfl.cvel_x;
+  out->cvel_y = h->cfl.cvel_y;
+  out->cvel_z = h->cfl.cvel_z;
+  out->cfl_evaluations = h->cfl.evaluations;
+  out->last_cfl_timestep = h->cfl.last_cfl_timestep;
   return MGPU_OK;
 }
 
@@ -1036,6 +1144,17 @@ int mgpu_slab_solve_columns(mgpu_handle* h, void* d_spec, int32_t kx0, int32_t n
   else
     slab_solve_columns<double>(h->slab, h->sc, d_spec, kx0, nkx, row_block, transpose != 0, h->stream, &h->launches);
   return check_launch(h);
+}
+
+int mgpu_cfl_gather(mgpu_handle* h, double* out) {
+  if (!h || !out) return MGPU_ERR_ARGUMENT;
+  const bool vd = h->cfg.use_viscosity_and_diffusion != 0;
+  if (h->fp32) h->launches += launch_cfl_gather<float>(h->sc, h->d32, vd, h->cfl.part_d, h->cfl.out_d, h->stream);
+  else h->launches += launch_cfl_gather<double>(h->sc, h->d64, vd, h->cfl.part_d, h->cfl.out_d, h->stream);
+  if (cudaMemcpyAsync(out, h->cfl.out_d, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return fail(h, MGPU_ERR_CUDA, "cfl gather");
+  return MGPU_OK;
 }
 
 int mgpu_mean_profile(mgpu_handle* h, int32_t id, double* out) {

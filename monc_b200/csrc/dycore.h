@@ -85,6 +85,14 @@ void launch_halo_rows(const Scalars& s, T* const* f, int n, int depth, int r_lo,
 template <typename T>
 void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st);
 
+// cfltest's reductions of the current zu, zv, zw (and vis, diff when with_vis) into out[0..5]:
+// min zu, max zu, min zv, max zv (levels 2..nz), max |zw| rdzn(k+1), max max(vis, diff) (rdzn(k+1)^2
+// + cx2 + cy2) (levels 2..nz-1).  part holds CFL_BLOCKS*6 doubles.  Returns the launch count.
+constexpr int CFL_BLOCKS = 296;
+template <typename T>
+int launch_cfl_gather(const Scalars& s, const DevState<T>& d, bool with_vis, double* part, double* out,
+                      cudaStream_t st);
+
 // BiCGStab pressure solve (iterativesolver)
 struct IterSolverDev;
 IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status);

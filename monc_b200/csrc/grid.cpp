@@ -56,6 +56,15 @@ extern "C" void mgpu_config_defaults(mgpu_config* c) {
   c->convective_limit = -0.5;
   c->ratio_mol_wts = 1.608;
   c->rlargep = 1.0e37;
+  c->cfl_enabled = 1;
+  c->cfl_frequency = 10;
+  c->cfl_tollerance = 0.1;
+  c->cfl_cvismax = 0.2;
+  c->cfl_cvelmax = 0.2;
+  c->cfl_dtmmax = 100.0;
+  c->cfl_dtmmin = 0.0001;
+  c->cfl_rincmax = 0.05;
+  c->l_constant_dtm = 0;
 }
 
 // w-level heights: piecewise-linear kgd/hgd grid smoothed nsmth times

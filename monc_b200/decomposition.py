@@ -234,6 +234,9 @@ class SlabDomain:
     solver SOLVER_EXTERNAL on `device`.  Fields move in and out as global [nz][ny][nx] arrays."""
 
     def __init__(self, cfg: cf.MgpuConfig, comm, halo: int = 4, device=None):
+        if cfg.cfl_enabled:
+            raise ValueError("cfltest on a decomposed domain needs its extrema reduced across the slabs; "
+                             "run the slabs at a fixed dtm (cfl_enabled = 0)")
         self.cfg = cfg
         self.comm = comm
         self.geo = SlabGeometry(cfg.nx, cfg.ny, cfg.nz, comm.size, halo)

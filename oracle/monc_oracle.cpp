@@ -95,6 +95,15 @@ struct Model {
   std::vector<double> A_u, A_d, A_p, A_lu_d, A_lu_u, A_vol;
   Field psource, prev_p;
   bool first_run = true;
+  // cfltest (cfltest.F90:23-28, state.F90:104-117) and the gathers feeding it
+  bool determine_flow_minmax = false;
+  int last_cfl_timestep = 0, cfl_evaluations = 0;
+  bool update_dtm = false;
+  double dtm_new = 0.0, absolute_new_dtm = 0.0, dtm_last = 0.0, cfl_number = 0.0;
+  double cvis = 0.0, cvis_last = 0.0, cvel = 0.0, cvel_x = 0.0, cvel_y = 0.0, cvel_z = 0.0;
+  double local_zumin = 0.0, local_zumax = 0.0, local_zvmin = 0.0, local_zvmax = 0.0, local_cvel_z = 0.0;
+  std::vector<double> abswmax;  // 1-based k
+  int cfl_error = 0;
 };
 
 static inline double& PT(Model& m, int k, int j, int i) {
@@ -512,6 +521,21 @@ static void moist_ri_2(Model& m, const std::vector<double>& ssq, Field& TH, std:
   }
 }
 
+// cfltest's evaluation test (cfltest.F90:80-82, stepfields.F90:249-256, smagorinsky.F90:151-153)
+static bool cfl_step(const Model& m) {
+  const int n = m.timestep, f = m.cfg.cfl_frequency;
+  return n % f == 1 || n - m.start_timestep <= f || n >= m.last_cfl_timestep + f;
+}
+
+// smagorinsky.F90:143-173 (non-IB)
+static void update_viscous_number(Model& m) {
+  if (!cfl_step(m)) return;
+  int y = m.col_y, x = m.col_x;
+  for (int k = 2; k <= m.nz - 1; ++k)
+    m.cvis = std::max(m.cvis, std::max(m.vis(k, y, x), m.diff(k, y, x)) *
+                                  (m.rdzn(k + 1) * m.rdzn(k + 1) + m.cx2 + m.cy2));
+}
+
 static void smagorinsky_column(Model& m) {
   int y = m.col_y, x = m.col_x;
   if (!m.halo_column) {
@@ -552,6 +576,7 @@ static void smagorinsky_column(Model& m) {
     }
     m.vis(m.nz, y, x) = 0.0;
     m.diff(m.nz, y, x) = 0.0;
+    if (m.cfg.cfl_enabled) update_viscous_number(m);
   }
   if (m.last_col) {  // non-blocking halo swap of vis and diff, completed before first use
     periodic_wrap(m, m.diff, 2, true);
@@ -1172,9 +1197,34 @@ static void clip_slice(Model& m, int yl, int xp, int yp, Field& f) {
   if (yl == m.ye) clip(yl);
 }
 
+// stepfields.F90:397-406
+static void reset_local_minmax_values(Model& m) {
+  m.local_zumin = m.rlargep;
+  m.local_zumax = -m.rlargep;
+  m.local_zvmin = m.rlargep;
+  m.local_zvmax = -m.rlargep;
+  m.abswmax.assign(m.nz + 1, -m.rlargep);
+}
+
+// stepfields.F90:372-393, before the column is stepped
+static void determine_local_flow_minmax(Model& m, int y, int x) {
+  for (int k = 2; k <= m.nz; ++k) {
+    m.local_zumax = std::max(m.local_zumax, m.zu(k, y, x));
+    m.local_zumin = std::min(m.local_zumin, m.zu(k, y, x));
+    m.local_zvmax = std::max(m.local_zvmax, m.zv(k, y, x));
+    m.local_zvmin = std::min(m.local_zvmin, m.zv(k, y, x));
+    if (k < m.nz) m.abswmax[k] = std::max(m.abswmax[k], std::fabs(m.zw(k, y, x)));
+  }
+}
+
 static void stepfields_column(Model& m) {
   int x = m.col_x, y = m.col_y;
+  if (m.cfg.cfl_enabled && m.first_col) {  // stepfields.F90:249-256
+    m.determine_flow_minmax = cfl_step(m);
+    if (m.determine_flow_minmax) reset_local_minmax_values(m);
+  }
   if (!m.halo_column) {
+    if (m.cfg.cfl_enabled && m.determine_flow_minmax) determine_local_flow_minmax(m, y, x);
     int xp = x - 2, yp = y - 1;
     double c1 = 1.0 - 2.0 * m.tsmth, c2 = m.tsmth;
     step_single_field(m, x, y, xp, yp, m.u, m.zu, m.su, true, m.ugal, c1, c2, false, &m.savu);
@@ -1380,7 +1430,56 @@ static void column_group(Model& m, const std::vector<ColumnFn>& fns) {
 void iterative_solver(Model& m);  // defined below
 void iterative_solver_solve(Model& m);
 
+// cfltest timestep callback (cfltest.F90:62-128) with update_dtm_based_on_absolute (:135-191) on
+// normal steps, single rank (the global reductions of :193-222 are the local values), Galilean
+// transformation off (global_config:268)
+static void cfltest(Model& m) {
+  const mgpu_config& g = m.cfg;
+  m.update_dtm = false;
+  m.dtm_last = m.dtm;
+  if (cfl_step(m)) {
+    m.last_cfl_timestep = m.timestep;
+    m.cfl_evaluations += 1;
+    m.cvel = 0.0;
+    m.cvel_x = 0.0;
+    m.cvel_y = 0.0;
+    m.cvel_z = 0.0;
+    // perform_cfl_and_galilean_transformation_calculation (:231-266)
+    m.local_zumin = m.local_zumin + m.ugal;
+    m.local_zumax = m.local_zumax + m.ugal;
+    m.local_zvmin = m.local_zvmin + m.vgal;
+    m.local_zvmax = m.local_zvmax + m.vgal;
+    m.local_cvel_z = m.cvel_z;
+    for (int k = 2; k <= m.nz - 1; ++k) m.local_cvel_z = std::max(m.local_cvel_z, m.abswmax[k] * m.rdzn(k + 1));
+    m.ugal = 0.0;
+    m.vgal = 0.0;
+    m.cvel_z = m.local_cvel_z;
+    m.cvel_x = std::max(std::fabs(m.local_zumax - m.ugal), std::fabs(m.local_zumin - m.ugal));
+    m.cvel_y = std::max(std::fabs(m.local_zvmax - m.vgal), std::fabs(m.local_zvmin - m.vgal));
+    m.cvel = (m.cvel_x * m.cx + m.cvel_y * m.cy + m.cvel_z) * m.dtm;
+    m.cvis = m.cvis * (m.dtm * 4);
+    m.cvis_last = m.cvis;
+    m.cfl_number = m.cvis / g.cfl_cvismax + m.cvel / g.cfl_cvelmax;
+    m.absolute_new_dtm = m.dtm;
+    if (m.cfl_number > 0.0)
+      if (m.cfl_number < (1.0 - g.cfl_tollerance) || m.cfl_number > (1.0 + g.cfl_tollerance))
+        m.absolute_new_dtm = m.dtm / m.cfl_number;
+  }
+  if (m.dtm != m.absolute_new_dtm && (m.dtm != g.cfl_dtmmax || m.absolute_new_dtm < g.cfl_dtmmax)) {
+    m.update_dtm = true;
+    m.dtm_new = std::min(std::min(m.dtm * (1.0 + g.cfl_rincmax), m.absolute_new_dtm), g.cfl_dtmmax);
+    if (m.dtm_new < g.cfl_dtmmin && !g.l_constant_dtm) m.cfl_error = 1;  // MONC stops (LOG_ERROR)
+  }
+  if (g.l_constant_dtm) {
+    m.dtm = g.dtm;
+    m.dtm_new = m.dtm;
+    m.update_dtm = false;
+  }
+  m.cvis = 0.0;
+}
+
 static void timestep(Model& m) {
+  if (m.cfg.cfl_enabled && m.update_dtm) m.dtm = m.dtm_new;  // monc.F90:313
   // start: clearsourceterms, stepping_direction, halo_swapper, setfluxlook (no per-step work)
   clearsourceterms(m);
   stepping_direction(m);
@@ -1398,6 +1497,7 @@ static void timestep(Model& m) {
   // solver
   if (m.cfg.solver == MGPU_SOLVER_FFT) fftsolver(m);
   else iterative_solver(m);
+  if (m.cfg.cfl_enabled) cfltest(m);
   // pressure-terms
   column_group(m, {pstep_column, swap_smooth_column});
   m.timestep += 1;
@@ -1451,6 +1551,11 @@ static Model* create(const mgpu_config* cfg) {
   m.r_over_cp = m.r / m.cp;
   m.dtm = cfg->dtm;
   m.tsmth = 1e-2;
+  m.dtm_last = m.dtm;
+  m.absolute_new_dtm = m.dtm;
+  m.dtm_new = m.dtm;
+  m.abswmax.assign(cfg->nz + 1, 0.0);
+  if (cfg->cfl_enabled) reset_local_minmax_values(m);  // stepfields.F90:99-100 (initialisation)
   build_grid(m);
   int nz = m.nz, nyh = m.nyh, nxh = m.nxh;
   Field* fl[] = {&m.u, &m.v, &m.w, &m.zu, &m.zv, &m.zw, &m.p, &m.su, &m.sv, &m.sw, &m.savu, &m.savv, &m.savw, &m.vis, &m.diff};
@@ -1710,11 +1815,27 @@ int orc_get_profile(void* h, const char* name, double* dst) {
 int orc_step(void* h, int nsteps) {
   Model& m = *(Model*)h;
   try {
-    for (int s = 0; s < nsteps; ++s) timestep(m);
+    for (int s = 0; s < nsteps; ++s) {
+      timestep(m);
+      if (m.cfl_error) return MGPU_ERR_CFL;
+    }
   } catch (std::exception& e) {
     std::fprintf(stderr, "orc_step: %s\n", e.what());
     return -1;
   }
+  return 0;
+}
+
+// cfltest state: out[0..8] = dtm of the last step, dtm of the next step, absolute_new_dtm, cvel,
+// cvis, cfl_number, cvel_x, cvel_y, cvel_z; iout[0..1] = evaluations, last_cfl_timestep
+int orc_cfl_state(void* h, double* out, int* iout) {
+  Model& m = *(Model*)h;
+  const double next = m.update_dtm ? m.dtm_new : m.dtm;
+  const double v[9] = {m.dtm_last, next, m.absolute_new_dtm, m.cvel, m.cvis_last, m.cfl_number,
+                       m.cvel_x, m.cvel_y, m.cvel_z};
+  for (int q = 0; q < 9; ++q) out[q] = v[q];
+  iout[0] = m.cfl_evaluations;
+  iout[1] = m.last_cfl_timestep;
   return 0;
 }
 

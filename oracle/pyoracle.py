@@ -52,8 +52,17 @@ def lib():
         L.orc_fft_c2c.argtypes = [C.c_int, C.c_void_p, C.c_int]
         L.orc_lookup_ustr.restype = C.c_double
         L.orc_lookup_ustr.argtypes = [C.c_void_p, C.c_double]
+        L.orc_cfl_state.restype = C.c_int
+        L.orc_cfl_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
+
+
+CFL_TOO_SMALL = -7  # MGPU_ERR_CFL
+
+
+class CflError(RuntimeError):
+    pass
 
 
 class Oracle:
@@ -101,8 +110,21 @@ class Oracle:
         return a
 
     def step(self, n: int = 1):
-        if lib().orc_step(self.h, n) != 0:
+        rc = lib().orc_step(self.h, n)
+        if rc == CFL_TOO_SMALL:
+            raise CflError("cfltest: the new timestep fell below cfl_dtmmin")
+        if rc != 0:
             raise RuntimeError("oracle step failed")
+
+    def cfl_state(self) -> dict:
+        """cfltest's state after the last step (the mgpu_reductions fields of the same names)."""
+        v = np.zeros(9)
+        i = np.zeros(2, dtype=np.int32)
+        lib().orc_cfl_state(self.h, v.ctypes.data, i.ctypes.data)
+        keys = ["dtm", "dtm_new", "absolute_new_dtm", "cvel", "cvis", "cfl_number", "cvel_x", "cvel_y", "cvel_z"]
+        out = dict(zip(keys, (float(x) for x in v)))
+        out["cfl_evaluations"], out["last_cfl_timestep"] = int(i[0]), int(i[1])
+        return out
 
     def set_timestep(self, ts: int):
         lib().orc_set_timestep(self.h, ts)
