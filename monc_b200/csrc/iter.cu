@@ -1,6 +1,6 @@
-// Iterative pressure solve: preconditioned BiCGStab on MONC's 7-point Poisson operator
-// (iterativesolver.F90:140-248 bicgstab, :329-380 precond, :400-493 calc_Ax, :500-553 inner
-// products, :559-602 set_matrix_for_poisson).
+// Iterative pressure solve: preconditioned BiCGStab or conjugate gradients on MONC's 7-point
+// Poisson operator (iterativesolver.F90:140-248 bicgstab, :255-321 cg_solver, :329-380 precond,
+// :400-493 calc_Ax, :500-553 inner products, :559-602 set_matrix_for_poisson).
 //
 // One BiCGStab iteration is five kernels over the resident work arrays:
 //   k_bicg_direction  : t = r - bet*omg*v; s = M^-1 t; pp = s + bet*pp   (pp = M^-1 r on it 1)
@@ -8,6 +8,12 @@
 //   k_bicg_half_step  : s = r - alf*v,  cs = M^-1 s
 //   k_bicg_apply_dots : t = A cs,  tt, ts, ss,  omg = ts / tt,  err
 //   k_bicg_update     : x += alf*pp + omg*cs,  r = s - omg*t,  rho = <r, cr>,  convergence
+// One CG iteration (solver_type MGPU_ITER_CG, MONC's symm_prob: the symmetric form of the operator,
+// A_vol = dz, and a right-hand side scaled by A_vol) is three kernels:
+//   k_cg_precond      : z = M^-1 r,  <z, r>,  bet = <z, r> / rho,  rho = <z, r>
+//   k_cg_apply        : p' = z + bet*p (each point computes its neighbours' p' itself, so p' goes to
+//                       a second buffer and no point waits for another),  Ap',  alf = rho / <p', Ap'>
+//   k_cg_update       : x += alf*p',  r -= alf*Ap',  err = |r| / sc_err,  convergence
 // M^-1 is MONC's column LU solve of the vertical part (preconditioner_iterations = 0).  Dot
 // products accumulate in FP64 whatever the work precision: warp shuffles, one partial per block,
 // and the last block to finish sums the partials in a fixed order (deterministic) and updates the
@@ -25,7 +31,7 @@
 namespace mgpu {
 
 struct IterScalars {
-  double rho, rho_prev, nrm, alf, omg, err, sc_err, tol, shift;
+  double rho, rho_prev, nrm, alf, omg, err, sc_err, tol, shift, bet;
   int it, done, it_done, pad;
   unsigned int counter;
 };
@@ -33,10 +39,12 @@ struct IterScalars {
 namespace {
 
 constexpr int BX = 32, BY = 8, NTH = BX * BY;
-constexpr int NCOEF = 6;  // A_u, A_d, A_p, lu_d, lu_u, vol = rhon*dz, each nz+2 long (1-based)
+// A_u, A_d, A_p, lu_d, lu_u, vol = rhon*dz, A_vol (dz for the symmetric form, else 1), each nz+2
+// long (1-based)
+constexpr int NCOEF = 7;
 
 struct Geom {
-  int nx, ny, nz;
+  int nx, ny, nz, symm;
   long long plane;
   double A_n, A_e;
   const double* coef;  // [NCOEF][nz+2]
@@ -46,6 +54,7 @@ struct Geom {
   __device__ __forceinline__ double lud(int k) const { return coef[3 * (nz + 2) + k]; }
   __device__ __forceinline__ double luu(int k) const { return coef[4 * (nz + 2) + k]; }
   __device__ __forceinline__ double vol(int k) const { return coef[5 * (nz + 2) + k]; }
+  __device__ __forceinline__ double avol(int k) const { return coef[6 * (nz + 2) + k]; }
   __device__ __forceinline__ long long at(int k, int j, int i) const { return (long long)(k - 1) * plane + (long long)j * nx + i; }
 };
 
@@ -106,17 +115,23 @@ __device__ bool last_block_sums(IterScalars* st, const double* partials, int nbl
   return true;
 }
 
-// (A x)(k, j, i) for 2 <= k <= nz (calc_Ax, non-symmetric form used by BiCGStab)
-template <typename W>
-__device__ __forceinline__ W apply_A(const Geom& g, const W* __restrict__ x, int k, int j, int i) {
+// (A x)(k, j, i) for 2 <= k <= nz (calc_Ax); x(o) gives the value at offset o.  The symmetric
+// form scales the horizontal part by A_vol(k).
+template <typename W, class X>
+__device__ __forceinline__ W apply_A_fn(const Geom& g, X x, int k, int j, int i) {
   const int ie = i + 1 == g.nx ? 0 : i + 1, iw = i == 0 ? g.nx - 1 : i - 1;
   const int jn = j + 1 == g.ny ? 0 : j + 1, js = j == 0 ? g.ny - 1 : j - 1;
   const long long o = g.at(k, j, i);
-  const W xc = x[o];
-  W h = (W)g.A_n * (x[g.at(k, j, ie)] + x[g.at(k, j, iw)]) + (W)g.A_e * (x[g.at(k, jn, i)] + x[g.at(k, js, i)]);
-  if (k == 2) return h + (W)g.au(k) * x[o + g.plane] + (W)g.ap(k) * xc;
-  if (k < g.nz) return h + (W)g.au(k) * x[o + g.plane] + (W)g.ad(k) * x[o - g.plane] + (W)g.ap(k) * xc;
-  return h + (W)g.ad(k) * x[o - g.plane] + (W)g.ap(k) * xc;
+  const W xc = x(o);
+  W h = (W)g.A_n * (x(g.at(k, j, ie)) + x(g.at(k, j, iw))) + (W)g.A_e * (x(g.at(k, jn, i)) + x(g.at(k, js, i)));
+  if (g.symm) h = (W)g.avol(k) * h;
+  if (k == 2) return h + (W)g.au(k) * x(o + g.plane) + (W)g.ap(k) * xc;
+  if (k < g.nz) return h + (W)g.au(k) * x(o + g.plane) + (W)g.ad(k) * x(o - g.plane) + (W)g.ap(k) * xc;
+  return h + (W)g.ad(k) * x(o - g.plane) + (W)g.ap(k) * xc;
+}
+template <typename W>
+__device__ __forceinline__ W apply_A(const Geom& g, const W* __restrict__ x, int k, int j, int i) {
+  return apply_A_fn<W>(g, [&](long long o) { return x[o]; }, k, j, i);
 }
 
 __device__ __forceinline__ int block_id() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
@@ -284,6 +299,126 @@ __global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __re
   }
 }
 
+
+// ---- conjugate gradients (cg_solver, symmetric form) -------------------------------------------
+// r = b*A_vol - A x (b*A_vol when scale_rhs, else b), sc_err = max(|b*A_vol|, sc_floor); MONC's
+// loop runs at least one iteration, so the solve is never marked done here
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_cg_init(Geom g, const W* __restrict__ x, const W* __restrict__ b, W* r,
+                                                  double* partials, int nblocks, IterScalars* st, double sc_floor,
+                                                  int scale_rhs) {
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double v[2] = {0.0, 0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W bv = scale_rhs ? b[o] * (W)g.avol(k) : b[o];
+    const W rv = bv - apply_A<W>(g, x, k, j, i);
+    r[o] = rv;
+    v[0] = (double)bv * (double)bv;
+    v[1] = (double)rv * (double)rv;
+  }
+  block_partials<2>(v, partials, nblocks, block_id());
+  double s[2];
+  if (last_block_sums<2>(st, partials, nblocks, s)) {
+    st->sc_err = fmax(sqrt(s[0]), sc_floor);
+    st->err = sqrt(s[1]) / st->sc_err;
+    st->rho = 0.0;
+    st->alf = 0.0;
+    st->bet = 0.0;
+    st->it = 1;
+    st->it_done = 0;
+    st->done = 0;
+  }
+}
+
+// z = M^-1 r per column, <z, r>; bet = <z, r> / rho and rho = <z, r> (iteration 1: rho = <z, r>)
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_cg_precond(Geom g, const W* __restrict__ r, W* z, W* tmp, double* partials,
+                                                     int nblocks, IterScalars* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  double a[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    column_precond<W>(g, [&](long long o) { return r[o]; }, tmp, j, i);
+    long long o = g.at(g.nz, j, i);
+    W zk = tmp[o];
+    z[o] = zk;
+    a[0] = (double)zk * (double)r[o];
+    for (int k = g.nz - 1; k >= 2; --k) {
+      o -= g.plane;
+      zk = tmp[o] - (W)g.luu(k) * zk;
+      z[o] = zk;
+      a[0] += (double)zk * (double)r[o];
+    }
+  }
+  block_partials<1>(a, partials, nblocks, block_id());
+  double s[1];
+  if (last_block_sums<1>(st, partials, nblocks, s)) {
+    if (st->it == 1) {
+      st->bet = 0.0;
+    } else {
+      st->bet = s[0] / st->rho;
+    }
+    st->rho = s[0];
+    st->alf = s[0];
+  }
+}
+
+// p' = z + bet*p (p' = z on iteration 1) into p_new, Ap' into Ax, alf = rho / <p', Ap'>.  Every
+// point forms p' at its stencil neighbours from z and the old p itself, with the same rounding as
+// the neighbour's own store, so the kernel needs no second pass.
+template <typename W>
+__device__ __forceinline__ W axpy_rn(W a, W x, W y) {
+  if constexpr (sizeof(W) == 8) return __dadd_rn(y, __dmul_rn(a, x));
+  else return __fadd_rn(y, __fmul_rn(a, x));
+}
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_cg_apply(Geom g, const W* __restrict__ z, const W* __restrict__ p_old,
+                                                   W* p_new, W* Ax, double* partials, int nblocks, IterScalars* st) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const bool first = st->it == 1;
+  const W bet = (W)st->bet;
+  auto pn = [&](long long o) { return first ? z[o] : axpy_rn<W>(bet, p_old[o], z[o]); };
+  double a[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W pc = pn(o);
+    p_new[o] = pc;
+    const W av = apply_A_fn<W>(g, pn, k, j, i);
+    Ax[o] = av;
+    a[0] = (double)pc * (double)av;
+  }
+  block_partials<1>(a, partials, nblocks, block_id());
+  double s[1];
+  if (last_block_sums<1>(st, partials, nblocks, s)) st->alf = st->alf / s[0];
+}
+
+// x += alf*p', r -= alf*Ap', err = |r| / sc_err, convergence
+template <typename W>
+__global__ void __launch_bounds__(NTH) k_cg_update(Geom g, W* x, const W* __restrict__ p, const W* __restrict__ Ax, W* r,
+                                                    double* partials, int nblocks, IterScalars* st, int max_it) {
+  if (st->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  double a[1] = {0.0};
+  if (i < g.nx && j < g.ny) {
+    const long long o = g.at(k, j, i);
+    const W alf = (W)st->alf;
+    x[o] = x[o] + alf * p[o];
+    const W rv = r[o] - alf * Ax[o];
+    r[o] = rv;
+    a[0] = (double)rv * (double)rv;
+  }
+  block_partials<1>(a, partials, nblocks, block_id());
+  double s[1];
+  if (last_block_sums<1>(st, partials, nblocks, s)) {
+    st->err = sqrt(s[0]) / st->sc_err;
+    st->it_done = st->it;
+    st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
+    st->it += 1;
+  }
+}
+
 // FP64 residual of the refinement: r = b - A x (levels 2..nz) with <r, r>, <b, b>
 __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* __restrict__ x, const double* __restrict__ b,
                                                           double* r, float* r32, double* partials, int nblocks,
@@ -292,11 +427,12 @@ __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* _
   double v[2] = {0.0, 0.0};
   if (i < g.nx && j < g.ny) {
     const long long o = g.at(k, j, i);
-    const double rv = b[o] - apply_A<double>(g, x, k, j, i);
+    const double bv = g.symm ? b[o] * g.avol(k) : b[o];
+    const double rv = bv - apply_A<double>(g, x, k, j, i);
     r[o] = rv;
     r32[o] = (float)rv;
     v[0] = rv * rv;
-    v[1] = b[o] * b[o];
+    v[1] = bv * bv;
   }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
@@ -351,6 +487,7 @@ struct Work {
 struct IterSolverDev {
   Geom g;
   bool fp32 = false;
+  bool symm = false;  // conjugate gradients on the symmetric form (MGPU_ITER_CG)
   int max_it = 0;
   double tol = 0.0;
   double* coef = nullptr;
@@ -374,17 +511,19 @@ static int dev_alloc(IterSolverDev* it, void** p, size_t bytes) {
 
 IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status) {
   *status = MGPU_OK;
-  if (cfg.solver_type != MGPU_ITER_BICGSTAB) {
-    std::fprintf(stderr, "iterative solver: only BiCGStab is available\n");
+  if (cfg.solver_type != MGPU_ITER_BICGSTAB && cfg.solver_type != MGPU_ITER_CG) {
+    std::fprintf(stderr, "iterative solver: unknown solver_type %d\n", cfg.solver_type);
     *status = MGPU_ERR_UNSUPPORTED;
     return nullptr;
   }
   auto* it = new IterSolverDev();
   const int nz = s.nz;
   it->fp32 = fp32;
+  it->symm = cfg.solver_type == MGPU_ITER_CG;
   it->max_it = cfg.max_iterations > 0 ? cfg.max_iterations : 1;
   it->tol = cfg.tolerance;
-  // set_matrix_for_poisson (iterativesolver.F90:559-602), BiCGStab form (A_vol = 1)
+  // set_matrix_for_poisson (iterativesolver.F90:559-602): BiCGStab form (A_vol = 1,
+  // d_sc = rdz/rhon) or, for conjugate gradients, the symmetric form (A_vol = dz, d_sc = 1/rhon)
   const double A_n = rs.cx * rs.cx, A_e = rs.cy * rs.cy;
   const double concat = A_n + A_n + A_e + A_e;
   std::vector<double> c((size_t)NCOEF * (nz + 2), 0.0);
@@ -394,12 +533,14 @@ IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_conf
   double* lud = Ap + (nz + 2);
   double* luu = lud + (nz + 2);
   double* vol = luu + (nz + 2);
+  double* avol = vol + (nz + 2);
   for (int k = 2; k <= nz; ++k) vol[k] = rs.rhon[k] * rs.dz[k];
   for (int k = 2; k <= nz; ++k) {
-    const double d_sc = rs.rdz[k] / rs.rhon[k];
+    avol[k] = it->symm ? rs.dz[k] : 1.0;
+    const double d_sc = it->symm ? 1.0 / rs.rhon[k] : rs.rdz[k] / rs.rhon[k];
     Au[k] = (k == nz) ? 0.0 : rs.rho[k] * rs.rdzn[k + 1];
     Ad[k] = (k == 2) ? 0.0 : rs.rho[k - 1] * rs.rdzn[k];
-    Ap[k] = d_sc * (-(Au[k] + Ad[k])) - concat * 1.0;
+    Ap[k] = d_sc * (-(Au[k] + Ad[k])) - concat * avol[k];
     Au[k] = d_sc * Au[k];
     Ad[k] = d_sc * Ad[k];
   }
@@ -416,7 +557,7 @@ IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_conf
   };
   if (dev_alloc(it, (void**)&it->coef, c.size() * sizeof(double))) return fail(MGPU_ERR_CUDA);
   cudaMemcpy(it->coef, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice);
-  it->g = Geom{s.nx, s.ny, nz, s.plane, A_n, A_e, it->coef};
+  it->g = Geom{s.nx, s.ny, nz, it->symm ? 1 : 0, s.plane, A_n, A_e, it->coef};
   it->block = dim3(BX, BY, 1);
   it->grid_col = dim3((s.nx + BX - 1) / BX, (s.ny + BY - 1) / BY, 1);
   it->grid_pt = dim3(it->grid_col.x, it->grid_col.y, nz - 1);
@@ -485,13 +626,54 @@ static int run_bicgstab(IterSolverDev* it, Work<W>& w, double tol, double sc_flo
   return it->st_host->err < tol ? MGPU_OK : MGPU_ERR_NOT_CONVERGED;
 }
 
+// conjugate gradients on work arrays w: x (initial guess, result), b, r, z in s, p in pp / cs
+// (alternating), A p in v, column scratch in tmp
+template <typename W>
+static int run_cg(IterSolverDev* it, Work<W>& w, double tol, double sc_floor, bool scale_rhs, cudaStream_t st,
+                  int64_t* launches, int* iterations, double* residual) {
+  IterScalars init{};
+  init.tol = tol;
+  it->st_host[0] = init;
+  if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return MGPU_ERR_CUDA;
+  const Geom& g = it->g;
+  const int ncol = (int)(it->grid_col.x * it->grid_col.y);
+  k_cg_init<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, it->partials, it->nblocks, it->st, sc_floor,
+                                                   scale_rhs ? 1 : 0);
+  *launches += 1;
+  W* pbuf[2] = {w.pp, w.cs};
+  int n = 0;
+  constexpr int BATCH = 4;
+  for (int done = 0; done < it->max_it;) {
+    for (int q = 0; q < BATCH; ++q, ++n) {
+      W* p_old = pbuf[n & 1];
+      W* p_new = pbuf[(n + 1) & 1];
+      k_cg_precond<W><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.s, w.tmp, it->partials, ncol, it->st);
+      k_cg_apply<W><<<it->grid_pt, it->block, 0, st>>>(g, w.s, p_old, p_new, w.v, it->partials, it->nblocks, it->st);
+      k_cg_update<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, p_new, w.v, w.r, it->partials, it->nblocks, it->st,
+                                                        it->max_it);
+      *launches += 3;
+    }
+    done += BATCH;
+    if (cudaMemcpyAsync(it->st_host, it->st, sizeof(IterScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MGPU_ERR_CUDA;
+    if (it->st_host->done) break;
+  }
+  if (cudaGetLastError() != cudaSuccess) return MGPU_ERR_CUDA;
+  *iterations = it->st_host->it_done;
+  *residual = it->st_host->err;
+  return it->st_host->err < tol ? MGPU_OK : MGPU_ERR_NOT_CONVERGED;
+}
+
 static int solve_fp64(IterSolverDev* it, const Scalars& s, double* p, cudaStream_t st, int64_t* launches,
                       int* iterations, double* residual) {
   if (!it || it->fp32) return MGPU_ERR_ARGUMENT;
   // psource = p; the initial guess is the previous solution (iterativesolver.F90:95-106)
   const size_t bytes = (size_t)s.nz * s.plane * sizeof(double);
   if (cudaMemcpyAsync(it->w64.b, p, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
-  int rc = run_bicgstab<double>(it, it->w64, it->tol, 0.0001, st, launches, iterations, residual);
+  int rc = it->symm ? run_cg<double>(it, it->w64, it->tol, 0.0001, true, st, launches, iterations, residual)
+                    : run_bicgstab<double>(it, it->w64, it->tol, 0.0001, st, launches, iterations, residual);
   if (rc != MGPU_OK && rc != MGPU_ERR_NOT_CONVERGED) return rc;
   // p = x, level 1 included (the solution keeps the previous solve's level 1)
   if (cudaMemcpyAsync(p, it->w64.x, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
@@ -545,7 +727,8 @@ static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream
     if (cudaMemsetAsync(it->w32.x, 0, (size_t)n * sizeof(float), st) != cudaSuccess) return MGPU_ERR_CUDA;
     int its = 0;
     double inner = 0.0;
-    int irc = run_bicgstab<float>(it, it->w32, 1e-5, 1e-300, st, launches, &its, &inner);
+    int irc = it->symm ? run_cg<float>(it, it->w32, 1e-5, 1e-300, false, st, launches, &its, &inner)
+                       : run_bicgstab<float>(it, it->w32, 1e-5, 1e-300, st, launches, &its, &inner);
     if (irc != MGPU_OK && irc != MGPU_ERR_NOT_CONVERGED) return irc;
     total += its;
     k_add_correction<<<592, 256, 0, st>>>(x64, it->w32.x, s.plane, n, 1.0);

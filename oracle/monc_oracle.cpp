@@ -1747,13 +1747,67 @@ static void bicgstab(Model& m, Field& x, Field& b) {
   m.last_residual = err;
 }
 
+// cg_solver (iterativesolver.F90:255-321): preconditioned conjugate gradients on the symmetric
+// form of the operator (symm_prob: A_vol = dz), right-hand side scaled by A_vol; the loop always
+// runs at least one iteration and tests convergence after the update
+static void cg_solver(Model& m, Field& x, Field& b) {
+  const int nz = m.nz;
+  Field Ax, r, z, p;
+  Field* ws[] = {&Ax, &r, &z, &p};
+  for (Field* f : ws) f->alloc(nz, m.nyh, m.nxh);
+  const double tolerance = m.cfg.tolerance;
+  for (int i = m.xs; i <= m.xe; ++i)
+    for (int j = m.ys; j <= m.ye; ++j) {
+      r(1, j, i) = 0.0;
+      for (int k = 2; k <= nz; ++k) r(k, j, i) = b(k, j, i) * m.A_vol[k];
+    }
+  calc_Ax(m, x, Ax);
+  double sc_err = std::sqrt(inner_prod(m, r, r));
+  sc_err = fmax_(sc_err, 0.0001);
+  for (int i = m.xs; i <= m.xe; ++i)
+    for (int j = m.ys; j <= m.ye; ++j)
+      for (int k = 1; k <= nz; ++k) r(k, j, i) = r(k, j, i) - Ax(k, j, i);
+  double err = std::sqrt(inner_prod(m, r, r)) / sc_err;  // init_err
+  double rho = 0.0, alf = 0.0;
+  int it_done = 0;
+  for (int it = 1; it <= m.cfg.max_iterations; ++it) {
+    it_done = it;
+    if (it == 1) {
+      precond(m, p, r);
+      rho = inner_prod(m, p, r);
+      alf = rho;
+    } else {
+      precond(m, z, r);
+      alf = inner_prod(m, z, r);
+      const double bet = alf / rho;
+      rho = alf;
+      for (int i = m.xs; i <= m.xe; ++i)
+        for (int j = m.ys; j <= m.ye; ++j)
+          for (int k = 1; k <= nz; ++k) p(k, j, i) = z(k, j, i) + bet * p(k, j, i);
+    }
+    calc_Ax(m, p, Ax);
+    alf = alf / inner_prod(m, p, Ax);
+    for (int i = m.xs; i <= m.xe; ++i)
+      for (int j = m.ys; j <= m.ye; ++j)
+        for (int k = 1; k <= nz; ++k) {
+          x(k, j, i) = x(k, j, i) + alf * p(k, j, i);
+          r(k, j, i) = r(k, j, i) - alf * Ax(k, j, i);
+        }
+    err = std::sqrt(inner_prod(m, r, r)) / sc_err;
+    if (err < tolerance) break;
+  }
+  periodic_wrap(m, x, 1, false);
+  m.last_iterations = it_done;
+  m.last_residual = err;
+}
+
 void iterative_solver_solve(Model& m) {
   periodic_wrap(m, m.p, 1, false);
   m.psource.d = m.p.d;
   if (m.first_run) { periodic_wrap(m, m.prev_p, 1, false); m.first_run = false; }
   m.p.d = m.prev_p.d;
-  if (m.cfg.solver_type == MGPU_ITER_CG) throw std::runtime_error("oracle: cg_solver is not restated");
-  bicgstab(m, m.p, m.psource);
+  if (m.cfg.solver_type == MGPU_ITER_CG) cg_solver(m, m.p, m.psource);
+  else bicgstab(m, m.p, m.psource);
   m.prev_p.d = m.p.d;
 }
 

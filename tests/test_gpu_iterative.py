@@ -1,4 +1,5 @@
-"""GPU BiCGStab pressure solve (iterativesolver) against the CPU oracle and the FFT solve.
+"""GPU iterative pressure solves (iterativesolver: BiCGStab, and cg_solver on the symmetric form
+of the operator) against the CPU oracle and the FFT solve.
 
 The GPU solver accumulates its inner products in a different order (block partials) and
 contracts multiply-adds, so its iterates differ from the oracle's at rounding level.  With a
@@ -21,10 +22,14 @@ def rel_err(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def config(solver=cf.SOLVER_ITERATIVE, precision=cf.FP64, tol=1e-4, max_it=500):
+TYPES = pytest.mark.parametrize("stype", [cf.ITER_BICGSTAB, cf.ITER_CG], ids=["bicgstab", "cg"])
+
+
+def config(solver=cf.SOLVER_ITERATIVE, precision=cf.FP64, tol=1e-4, max_it=500, stype=cf.ITER_BICGSTAB):
     c = cf.dry_cbl_config(NX, NY, NZ, 50.0, 25.0, 0.5, ug=5.0, fcoriol=1e-4, precision=precision, solver=solver)
     c.tolerance = tol
     c.max_iterations = max_it
+    c.solver_type = stype
     return c
 
 
@@ -37,11 +42,12 @@ def rhs(seed=3):
     return b
 
 
+@TYPES
 @pytest.mark.parametrize("iterations", [1, 2, 5, 12])
-def test_bicgstab_iterates_match_oracle(gpu_lib, iterations):
+def test_iterates_match_oracle(gpu_lib, iterations, stype):
     """With the tolerance out of reach, both solvers run exactly `iterations` iterations; the
     iterates then agree to rounding (different dot-product order, contracted multiply-adds)."""
-    c = config(tol=1e-30, max_it=iterations)
+    c = config(tol=1e-30, max_it=iterations, stype=stype)
     o = po.Oracle(c)
     m = api.Model(c)
     b = rhs()
@@ -57,11 +63,12 @@ def test_bicgstab_iterates_match_oracle(gpu_lib, iterations):
     m.close()
 
 
+@TYPES
 @pytest.mark.parametrize("tol", [1e-4, 1e-10])
-def test_bicgstab_converges_like_oracle(gpu_lib, tol):
+def test_converges_like_oracle(gpu_lib, tol, stype):
     """To a tolerance, the iteration counts agree within one (the stopping test sits on a
     rounding-level residual) and both solutions meet it."""
-    c = config(tol=tol)
+    c = config(tol=tol, stype=stype)
     o = po.Oracle(c)
     m = api.Model(c)
     b = rhs()
@@ -77,9 +84,10 @@ def test_bicgstab_converges_like_oracle(gpu_lib, tol):
     m.close()
 
 
-def test_bicgstab_warm_start_matches_oracle(gpu_lib):
+@TYPES
+def test_warm_start_matches_oracle(gpu_lib, stype):
     """The second solve starts from the first solution (MONC keeps prev_p)."""
-    c = config(tol=1e-30, max_it=6)
+    c = config(tol=1e-30, max_it=6, stype=stype)
     o = po.Oracle(c)
     m = api.Model(c)
     for seed in (3, 4):
@@ -92,12 +100,13 @@ def test_bicgstab_warm_start_matches_oracle(gpu_lib):
     m.close()
 
 
+@TYPES
 @pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32_mixed_refined"])
-def test_bicgstab_agrees_with_fft_solve(gpu_lib, precision):
+def test_agrees_with_fft_solve(gpu_lib, precision, stype):
     b = rhs(5)
     out = {}
     for solver in (cf.SOLVER_FFT, cf.SOLVER_ITERATIVE):
-        m = api.Model(config(solver=solver, precision=precision, tol=1e-11))
+        m = api.Model(config(solver=solver, precision=precision, tol=1e-11, stype=stype))
         m.upload("p", b)
         m.component("fftsolver" if solver == cf.SOLVER_FFT else "iterativesolver")
         out[solver] = m.download("p")[1:]
@@ -111,9 +120,10 @@ def test_bicgstab_agrees_with_fft_solve(gpu_lib, precision):
     assert np.abs(d).max() <= tol * np.abs(out[cf.SOLVER_FFT]).max()
 
 
-def test_fused_step_with_bicgstab_matches_oracle(gpu_lib):
+@TYPES
+def test_fused_step_matches_oracle(gpu_lib, stype):
     """Three fused steps with a fixed number of solver iterations per step."""
-    c = config(tol=1e-30, max_it=8)
+    c = config(tol=1e-30, max_it=8, stype=stype)
     o = po.Oracle(c)
     m = api.Model(c)
     st = ini.random_flow_state(NX, NY, NZ, seed=6, ug=5.0)
@@ -127,10 +137,11 @@ def test_fused_step_with_bicgstab_matches_oracle(gpu_lib):
     m.close()
 
 
-def test_bicgstab_reports_non_convergence(gpu_lib):
+@TYPES
+def test_reports_non_convergence(gpu_lib, stype):
     """At max_iterations the solve stops, the step still succeeds (MONC only warns) and the
     residual reported is above the tolerance."""
-    c = config(tol=1e-14, max_it=2)
+    c = config(tol=1e-14, max_it=2, stype=stype)
     m = api.Model(c)
     m.upload("p", rhs())
     m.component("iterativesolver")

@@ -171,10 +171,12 @@ def test_oracle_is_deterministic():
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
-def test_bicgstab_agrees_with_fft_solve():
-    """The oracle's BiCGStab and FFT solves of one right-hand side agree (the discrete operators
-    are the same).  The right-hand side has zero horizontal mean on every level, as the divergence
-    of a periodic flow has; the horizontal-mean problem is singular otherwise."""
+@pytest.mark.parametrize("stype", [cf.ITER_BICGSTAB, cf.ITER_CG], ids=["bicgstab", "cg"])
+def test_iterative_solvers_agree_with_fft_solve(stype):
+    """The oracle's BiCGStab / conjugate-gradient and FFT solves of one right-hand side agree (the
+    discrete operators are the same; CG solves the symmetric form, rows scaled by dz).  The
+    right-hand side has zero horizontal mean on every level, as the divergence of a periodic flow
+    has; the horizontal-mean problem is singular otherwise."""
     n, nz = 16, 12
     b = ini.uniform_noise((nz, n, n), 3, 9, 1e-3)
     b -= b.mean(axis=(1, 2), keepdims=True)
@@ -182,6 +184,7 @@ def test_bicgstab_agrees_with_fft_solve():
     out = []
     for solver in (cf.SOLVER_FFT, cf.SOLVER_ITERATIVE):
         c = cf.dry_cbl_config(n, n, nz, 50.0, 25.0, 1.0, solver=solver)
+        c.solver_type = stype
         c.tolerance = 1e-12
         o = po.Oracle(c)
         o.set(F["p"], b)
