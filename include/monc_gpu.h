@@ -47,6 +47,10 @@ extern "C" {
 #define MGPU_SOLVER_ITERATIVE  1
 #define MGPU_SOLVER_EXTERNAL   2  /* one y-slab of a decomposed domain: the caller drives the solve */
 
+/* advection of the flow fields (advection_flow_fields, pwadvection.F90 / tvdadvection.F90:603-908) */
+#define MGPU_ADVECT_PW   0  /* Piacsek-Williams centred flux form (the benchmark configurations) */
+#define MGPU_ADVECT_TVD  1  /* TVD (ULTIMATE-QUICKEST) on the dual grids of u, v, w */
+
 /* iterative solver types (iterativesolver.F90 solver_type) */
 #define MGPU_ITER_BICGSTAB 0
 #define MGPU_ITER_CG       1
@@ -139,6 +143,7 @@ typedef struct mgpu_config {
   double  cfl_tollerance, cfl_cvismax, cfl_cvelmax; /* cfl_tollerance, cfl_cvismax, cfl_cvelmax */
   double  cfl_dtmmax, cfl_dtmmin, cfl_rincmax;      /* cfl_dtmmax, cfl_dtmmin, cfl_rincmax */
   int32_t l_constant_dtm;             /* l_constant_dtm */
+  int32_t advection_flow_fields;      /* MGPU_ADVECT_PW / MGPU_ADVECT_TVD (MONC's "any" would advect twice) */
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */

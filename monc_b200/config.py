@@ -16,6 +16,7 @@ MAX_Q = 8
 
 FP64 = 0
 FP32_MIXED = 1
+ADVECT_PW, ADVECT_TVD = 0, 1
 SOLVER_FFT = 0
 SOLVER_ITERATIVE = 1
 SOLVER_EXTERNAL = 2  # one y-slab of a decomposed domain; the slab driver runs the pressure solve
@@ -68,6 +69,7 @@ class MgpuConfig(C.Structure):
         ("cfl_tollerance", C.c_double), ("cfl_cvismax", C.c_double), ("cfl_cvelmax", C.c_double),
         ("cfl_dtmmax", C.c_double), ("cfl_dtmmin", C.c_double), ("cfl_rincmax", C.c_double),
         ("l_constant_dtm", C.c_int32),
+        ("advection_flow_fields", C.c_int32),
     ]
 
 
@@ -135,6 +137,7 @@ def default_config() -> MgpuConfig:
     c.cfl_dtmmin = 0.0001
     c.cfl_rincmax = 0.05
     c.l_constant_dtm = 0
+    c.advection_flow_fields = ADVECT_PW
     return c
 
 

@@ -181,6 +181,7 @@ static void fill_scalars(mgpu_handle* h) {
   s.iqv = 0; s.iql = c.number_q_fields > 1 ? 1 : 0;
   s.coriolis = c.coriolis_enabled; s.surface_bcs = c.use_surface_boundary_conditions;
   s.use_vd = c.use_viscosity_and_diffusion;
+  s.tvd_flow = c.advection_flow_fields == MGPU_ADVECT_TVD ? 1 : 0;
   s.rho_unity = 1;
   for (int k = 1; k <= c.nz; ++k)
     if (r.rho[k] != 1.0 || r.rhon[k] != 1.0) s.rho_unity = 0;
@@ -198,7 +199,7 @@ static const std::vector<double>* prof_vec(const RefState& r, int id) {
     case P_RPREFRCP: return &r.rprefrcp; case P_TREF: return &r.tref; case P_TSTARPR: return &r.tstarpr;
     case P_QSAT: return &r.qsat; case P_DQSATDT: return &r.dqsatdt; case P_QSATFAC: return &r.qsatfac;
     case P_GWX: return &r.gwx; case P_GWY: return &r.gwy; case P_PREFN: return &r.prefn;
-    case P_TOFF: return &r.moist_toff; case P_TC0: return &r.tc0;
+    case P_TOFF: return &r.moist_toff; case P_TC0: return &r.tc0; case P_DZ: return &r.dz;
   }
   return nullptr;
 }
@@ -329,6 +330,8 @@ static int ad_alloc(mgpu_handle* h, double** p, size_t n) {
 }
 
 static int ad_supported(mgpu_handle* h) {
+  if (h->cfg.advection_flow_fields != MGPU_ADVECT_PW)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the PW advection of the flow");
   if (h->cfg.cfl_enabled)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs hold dtm fixed: disable cfltest");
   if (h->fp32 || h->cfg.number_q_fields > 0 || h->cfg.solver != MGPU_SOLVER_FFT)

@@ -455,7 +455,17 @@ __device__ void simplecloud_point(const Scalars& s, const PA& P, int k, T q_v, T
 // ------------------------------------------------------------------------------------------
 // TVD advection: ULTIMATE-QUICKEST face values (ultimateflux.F90) and their divergence
 // (tvdadvection.F90:911-960).  dt is 2*dtm in both stepping modes.
+//
+// The vertical metrics ultflx is called with (tvdadvection.F90:722-908): scalars, u and v take
+// rdz, rdzn, dzn and kdof = 0; w takes rdzn, rdz, dz and kdof = 1, which shifts the rdz of the
+// gradient and central terms up one level.
 // ------------------------------------------------------------------------------------------
+struct TvdMetricScalar {
+  static constexpr int RDZ = P_RDZ, RDZN = P_RDZN, DZN = P_DZN, KDOF = 0, TZ1 = P_TZC1, TZ2 = P_TZC2;
+};
+struct TvdMetricW {
+  static constexpr int RDZ = P_RDZN, RDZN = P_RDZ, DZN = P_DZ, KDOF = 1, TZ1 = P_TZD1, TZ2 = P_TZD2;
+};
 template <typename T>
 __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, T fdels, T fd, T fc, T fu, T fgt1, T fgt2,
                                         T curv_term) {
@@ -474,7 +484,7 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
 }
 
 // face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx
-template <typename T, class A, class AF, class PA>
+template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
 __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                         const AF& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
@@ -493,13 +503,13 @@ __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, c
   T sum;
   if (u0 > (T)0.0) {
     sum = (T)0.0;
-    sum = sum + P(P_RDZ, k) * (tmax<T>((T)0.0, W(k, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
+    sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
     sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
     sum = sum + cx * (u0 + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
     sum = sum * dt;
   } else {
     sum = (T)0.0;
-    sum = sum + P(P_RDZ, k) * (tmax<T>((T)0.0, W(k, j, i + 1)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i + 1))));
+    sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j, i + 1)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i + 1))));
     sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i + 1)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i + 1))));
     sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i + 1)) - u0);
     sum = sum * dt;
@@ -513,7 +523,7 @@ __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, c
     int ksl = pos ? k : kp0;
     T ts = ZF(ksl, j, i) - ZF(ksu, j, i);
     ts = ts * advpos + (ZF(ksl, j, i + 1) - ZF(ksu, j, i + 1)) * advneg;
-    fgt1 = fabs(sf) * P(P_RDZ, k) * dt * ts;
+    fgt1 = fabs(sf) * P(M::RDZ, k + M::KDOF) * dt * ts;
   }
   // gradient term in y with two v columns
   T fgt2;
@@ -529,7 +539,7 @@ __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, c
 }
 
 // face y+1/2 of cell (k, j, i): flux_y(k) of ultflx
-template <typename T, class A, class AF, class PA>
+template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
 __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                         const AF& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
@@ -547,7 +557,7 @@ __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fcurvs = fd - (T)2.0 * fc + fu;
   if (fabs(fcurvs) >= fabs(fdels)) return fc;
   T sum = (T)0.0;
-  sum = sum + P(P_RDZ, k) * (tmax<T>((T)0.0, W(k, j + jo, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j + jo, i))));
+  sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j + jo, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j + jo, i))));
   sum = sum + cy * (tmax<T>((T)0.0, V(k, j + jo, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1 + jo, i))));
   sum = sum + cx * (tmax<T>((T)0.0, U(k, j + jo, i)) + fabs(tmin<T>((T)0.0, U(k, j + jo, i - 1))));
   sum = sum * dt;
@@ -558,7 +568,7 @@ __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, c
     int ksu = pos ? k - 1 : kp1;
     int ksl = pos ? k : kp0;
     T ts = ZF(ksl, j + jo, i) - ZF(ksu, j + jo, i);
-    fgt1 = fabs(sf) * P(P_RDZ, k) * dt * ts;
+    fgt1 = fabs(sf) * P(M::RDZ, k + M::KDOF) * dt * ts;
   }
   T fgt2;
   {
@@ -570,7 +580,7 @@ __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, c
 }
 
 // flux_z(k+1): face above level k (2 <= k <= nz-1); the top routine handles k = nz-1
-template <typename T, class A, class AF, class PA>
+template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
 __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                         const AF& ZF, T dt, int k, int j, int i) {
   const int nz = s.nz;
@@ -587,22 +597,22 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
     if (fabs(fcurvs) >= fabs(fdels)) return fc;
     if (up) {
       sum = (T)0.0;
-      sum = sum + P(P_RDZ, k) * (w0 + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
+      sum = sum + P(M::RDZ, k + M::KDOF) * (w0 + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
       sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
       sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i)) + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
       sum = sum * dt;
       kf = k;
-      rdu = P(P_RDZN, k);
-      rdc = P(P_RDZ, k);
+      rdu = P(M::RDZN, k);
+      rdc = P(M::RDZ, k + M::KDOF);
     } else {
       sum = (T)0.0;
-      sum = sum + (-w0 * P(P_RDZ, nz < k + 1 ? nz : k + 1));
+      sum = sum + (-w0 * P(M::RDZ, nz < k + 1 + M::KDOF ? nz : k + 1 + M::KDOF));
       sum = sum + cy * (tmax<T>((T)0.0, V(k + 1, j, i)) + fabs(tmin<T>((T)0.0, V(k + 1, j - 1, i))));
       sum = sum + cx * (tmax<T>((T)0.0, U(k + 1, j, i)) + fabs(tmin<T>((T)0.0, U(k + 1, j, i - 1))));
       sum = sum * dt;
       kf = k + 1;
-      rdu = P(P_RDZN, nz);
-      rdc = P(P_RDZ, nz < k + 1 ? nz : k + 1);
+      rdu = P(M::RDZN, nz);
+      rdc = P(M::RDZ, nz < k + 1 + M::KDOF ? nz : k + 1 + M::KDOF);
     }
     {
       T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
@@ -615,7 +625,7 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
       fgt2 = fabs(sf) * cx * dt * (fc - (ZF(kf, j, i + 1) * ((T)1. - posuf) + ZF(kf, j, i - 1) * posuf));
     }
     // calculate_flux_in_w
-    T dd = P(P_DZN, k + 1), rdd = P(P_RDZN, k + 1);
+    T dd = P(M::DZN, k + 1), rdd = P(M::RDZN, k + 1);
     T cflmod = fabs(w0 * rdd * dt);
     T hrcfl = rcp(sum + (T)1.e-30);
     T hcfl = (T)0.5 * cflmod;
@@ -639,7 +649,7 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fdels = fd - fu;
   if (fabs(fcurvs) >= fabs(fdels)) return fc;
   sum = (T)0.0;
-  sum = sum + P(P_RDZ, k + ko) * (tmax<T>((T)0.0, W(k + ko, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1 + ko, j, i))));
+  sum = sum + P(M::RDZ, k + ko) * (tmax<T>((T)0.0, W(k + ko, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1 + ko, j, i))));
   sum = sum + cy * (tmax<T>((T)0.0, V(k + ko, j, i)) + fabs(tmin<T>((T)0.0, V(k + ko, j - 1, i))));
   sum = sum + cx * (tmax<T>((T)0.0, U(k + ko, j, i)) + fabs(tmin<T>((T)0.0, U(k + ko, j, i - 1))));
   sum = sum * dt;
@@ -653,9 +663,9 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
     T posuf = (T)0.5 + tsign<T>((T).5, sf);
     fgt2 = fabs(sf) * cx * dt * (fc - (ZF(k + ko, j, i + 1) * ((T)1. - posuf) + ZF(k + ko, j, i - 1) * posuf));
   }
-  rdu = P(P_RDZN, k) * advpos + P(P_RDZN, k + 2) * advneg;
-  rdc = P(P_RDZ, k) * advpos + P(P_RDZ, k + 1) * advneg;
-  T dd = P(P_DZN, k + 1), rdd = P(P_RDZN, k + 1);
+  rdu = P(M::RDZN, k) * advpos + P(M::RDZN, k + 2) * advneg;
+  rdc = P(M::RDZ, k + M::KDOF) * advpos + P(M::RDZ, k + 1 + M::KDOF) * advneg;
+  T dd = P(M::DZN, k + 1), rdd = P(M::RDZN, k + 1);
   T cflmod = fabs(w0 * rdd * dt);
   T hrcfl = rcp(sum + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
@@ -672,18 +682,18 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
 // TVD source of cell (k, j, i), 2 <= k <= nz, from the six face values
 // acc0 is the source value before the callback (MONC accumulates into it below the top level
 // and zeroes it at the top level)
-template <typename T, class A, class PA>
+template <typename T, class A, class PA, class M = TvdMetricScalar>
 __device__ T tvd_source(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                         T fx_m, T fx_p, T fy_m, T fy_p, T fz_m, T fz_p, int k, int j, int i, T acc0) {
   const T cx = (T)s.cx, cy = (T)s.cy;
   T acc = (k < s.nz) ? acc0 : (T)0.0;
   if (k < s.nz) {
     acc = acc + (V(k, j - 1, i) * fy_m - V(k, j, i) * fy_p) * cy;
-    acc = acc + (T)4.0 * (W(k - 1, j, i) * fz_m * P(P_TZC1, k) - W(k, j, i) * fz_p * P(P_TZC2, k));
+    acc = acc + (T)4.0 * (W(k - 1, j, i) * fz_m * P(M::TZ1, k) - W(k, j, i) * fz_p * P(M::TZ2, k));
     acc = acc + (U(k, j, i - 1) * fx_m - U(k, j, i) * fx_p) * cx;
   } else {
     acc = acc + (V(k, j - 1, i) * fy_m - V(k, j, i) * fy_p) * cy;
-    acc = acc + (T)4.0 * P(P_TZC1, k) * W(k - 1, j, i) * fz_m;
+    acc = acc + (T)4.0 * P(M::TZ1, k) * W(k - 1, j, i) * fz_m;
     acc = acc + (U(k, j, i - 1) * fx_m - U(k, j, i) * fx_p) * cx;
   }
   return acc;
@@ -700,6 +710,130 @@ __device__ T tvd_point(const Scalars& s, const PA& P, const A& U, const A& V, co
   T fzm = (k == 2) ? (T)0.0 : tvd_face_z<T, A>(s, P, U, V, W, ZF, dt, k - 1, j, i);
   T fzp = (k < s.nz) ? tvd_face_z<T, A>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
   return tvd_source<T, A>(s, P, U, V, W, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, acc0);
+}
+
+// ------------------------------------------------------------------------------------------
+// TVD advection of the flow fields (tvdadvection.F90:603-908, advection_flow_fields = tvd)
+// ------------------------------------------------------------------------------------------
+// The advecting flow of u, v or w: interpolate_to_dual (stencil.F90:87-169) averages each flow
+// component with its neighbour one point along the direction in which the advected field sits on
+// the primal grid -- x for u, y for v, z for w (simplesetup.F90:70-85) -- and keeps the top level
+// as it is for w.  MONC also keeps the value where that neighbour lies outside its local arrays,
+// the outermost halo column or row; the faces of interior points never read those.
+template <typename T, class A, int DIM>
+struct DualFlow {
+  A a;
+  int nz;
+  __device__ __forceinline__ T operator()(int k, int j, int i) const {
+    if (DIM == 0) return (T)0.5 * (a(k, j, i) + a(k, j, i + 1));
+    if (DIM == 1) return (T)0.5 * (a(k, j, i) + a(k, j + 1, i));
+    return k == nz ? a(k, j, i) : (T)0.5 * (a(k, j, i) + a(k + 1, j, i));
+  }
+};
+
+// flux_z(2) of w's advection: handle_vertical_fluxes_bottomofcolumn (ultimateflux.F90:307-412),
+// the face above level 1 (only w's metrics reach it: kmin = 1)
+template <typename T, class A, class AF, class PA, class M>
+__device__ T tvd_face_z_bottom(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const AF& ZF, T dt,
+                               int j, int i) {
+  const int k = 1;
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  const T w0 = W(k, j, i);
+  const bool up = w0 >= (T)0.0;
+  T fu, fc, fd;
+  if (up) { fu = ZF(1, j, i); fc = ZF(k, j, i); fd = ZF(k + 1, j, i); }
+  else { fu = ZF(k + 2, j, i); fc = ZF(k + 1, j, i); fd = ZF(k, j, i); }
+  T fcurvs = fd - (T)2.0 * fc + fu;
+  T fdels = fd - fu;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
+  T sum, rdu, rdc;
+  const int kf = up ? k : k + 1;  // level of the values the gradient terms take
+  if (up) {
+    sum = (T)0.0;
+    sum = sum + w0 * P(M::RDZ, k + M::KDOF);
+    sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
+    sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i)) + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
+    sum = sum * dt;
+    rdu = P(M::RDZN, 2);
+    rdc = P(M::RDZ, k + M::KDOF);
+  } else {
+    sum = (T)0.0;
+    sum = sum + P(M::RDZ, k + 1 + M::KDOF) * (tmax<T>((T)0.0, W(k + 1, j, i)) - w0);
+    sum = sum + cy * (tmax<T>((T)0.0, V(k + 1, j, i)) + fabs(tmin<T>((T)0.0, V(k + 1, j - 1, i))));
+    sum = sum + cx * (tmax<T>((T)0.0, U(k + 1, j, i)) + fabs(tmin<T>((T)0.0, U(k + 1, j, i - 1))));
+    sum = sum * dt;
+    rdu = P(M::RDZN, k + 2);
+    rdc = P(M::RDZ, k + 1 + M::KDOF);
+  }
+  T fgt1, fgt2;
+  {
+    T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
+    int jsu = signbit(sf) ? j + 1 : j - 1;
+    fgt1 = fabs(sf) * cy * dt * (fc - ZF(kf, jsu, i));
+  }
+  {
+    T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k + 1, j, i - 1) + U(k + 1, j, i));
+    T posuf = (T)0.5 + tsign<T>((T).5, sf);
+    fgt2 = fabs(sf) * cx * dt * (fc - (ZF(kf, j, i + 1) * ((T)1. - posuf) + ZF(kf, j, i - 1) * posuf));
+  }
+  T dd = P(M::DZN, k + 1), rdd = P(M::RDZN, k + 1);
+  T cflmod = fabs(w0 * rdd * dt);
+  T hrcfl = rcp(sum + (T)1.e-30);
+  T hcfl = (T)0.5 * cflmod;
+  T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
+  T rfdels = rcp_limiter(fdels + (T)1.e-30);
+  T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
+  T fnfs = (ffs - fu) * rfdels;
+  T fncs = (fc - fu) * rfdels;
+  T fnrefs = fncs * hrcfl;
+  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+  return ftemp * fdels + fu;
+}
+
+// TVD sources of u, v (2 <= k <= nz) and w (2 <= k <= nz-1) at (k, j, i), added to su_in, sv_in,
+// sw_in as differentiate_face_values adds them (u and v restart from 0 at the top level; w has no
+// top-level source).  U, V, W are the current flow fields, ZU, ZV, ZW the advected ones.
+template <typename T, class A, class PA>
+__device__ void tvd_flow_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const A& ZU,
+                               const A& ZV, const A& ZW, int k, int j, int i, T su_in, T sv_in, T sw_in, T& su, T& sv,
+                               T& sw) {
+  const T dt = (T)(s.dtm * 2.0);  // momentum_stepping is always centred (steppingdirection.F90:32)
+  const int nz = s.nz;
+  {
+    typedef DualFlow<T, A, 0> F;
+    const F IU{U, nz}, IV{V, nz}, IW{W, nz};
+    T fxm = tvd_face_x<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZU, dt, k, j, i - 1);
+    T fxp = tvd_face_x<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZU, dt, k, j, i);
+    T fym = tvd_face_y<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZU, dt, k, j - 1, i);
+    T fyp = tvd_face_y<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZU, dt, k, j, i);
+    T fzm = (k == 2) ? (T)0.0 : tvd_face_z<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZU, dt, k - 1, j, i);
+    T fzp = (k < nz) ? tvd_face_z<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZU, dt, k, j, i) : (T)0.0;
+    su = tvd_source<T, F, PA, TvdMetricScalar>(s, P, IU, IV, IW, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, su_in);
+  }
+  {
+    typedef DualFlow<T, A, 1> F;
+    const F IU{U, nz}, IV{V, nz}, IW{W, nz};
+    T fxm = tvd_face_x<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZV, dt, k, j, i - 1);
+    T fxp = tvd_face_x<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZV, dt, k, j, i);
+    T fym = tvd_face_y<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZV, dt, k, j - 1, i);
+    T fyp = tvd_face_y<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZV, dt, k, j, i);
+    T fzm = (k == 2) ? (T)0.0 : tvd_face_z<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZV, dt, k - 1, j, i);
+    T fzp = (k < nz) ? tvd_face_z<T, F, A, PA, TvdMetricScalar>(s, P, IU, IV, IW, ZV, dt, k, j, i) : (T)0.0;
+    sv = tvd_source<T, F, PA, TvdMetricScalar>(s, P, IU, IV, IW, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, sv_in);
+  }
+  sw = sw_in;
+  if (k <= nz - 1) {
+    typedef DualFlow<T, A, 2> F;
+    const F IU{U, nz}, IV{V, nz}, IW{W, nz};
+    T fxm = tvd_face_x<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k, j, i - 1);
+    T fxp = tvd_face_x<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k, j, i);
+    T fym = tvd_face_y<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k, j - 1, i);
+    T fyp = tvd_face_y<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k, j, i);
+    T fzm = (k == 2) ? tvd_face_z_bottom<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, j, i)
+                     : tvd_face_z<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k - 1, j, i);
+    T fzp = tvd_face_z<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k, j, i);
+    sw = tvd_source<T, F, PA, TvdMetricW>(s, P, IU, IV, IW, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, sw_in);
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -117,6 +117,7 @@ __global__ void k_c_pw(Scalars s, DevState<T> d) {
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z + 2;
   if (i >= s.nx || j >= s.ny || k > s.nz) return;
+  if (s.tvd_flow) return;  // the flow is advected by tvd_advection (advect_flow is false here)
   Prof<T> P = prof<T>(s);
   View<T> U = view<T>(d.u, s), V = view<T>(d.v, s), W = view<T>(d.w, s);
   T su, sv, sw;
@@ -137,7 +138,16 @@ __global__ void k_c_tvd(Scalars s, DevState<T> d, const T* zf_th, T* sth, int n_
   View<T> U = view<T>(d.u, s), V = view<T>(d.v, s), W = view<T>(d.w, s);
   long long o = lin(s, k, j, i);
   bool fwd = s.forward;
-  // theta, then each q field (advect_theta, advect_q_fields)
+  // the flow fields (advect_flow_fields), then theta, then each q field (advect_theta, advect_q_fields)
+  if (s.tvd_flow) {
+    T su, sv, sw;
+    tvd_flow_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.u : d.zu, s), view<T>(fwd ? d.v : d.zv, s),
+                               view<T>(fwd ? d.w : d.zw, s), k, j, i, d.su[o], d.sv[o], k < s.nz ? d.sw[o] : (T)0.0,
+                               su, sv, sw);
+    d.su[o] = su;
+    d.sv[o] = sv;
+    if (k < s.nz) d.sw[o] = sw;
+  }
   {
     View<T> ZF = view<T>(fwd ? d.th : d.zth, s);
     d.sth[o] = tvd_point<T, View<T>>(s, P, U, V, W, ZF, k, j, i, d.sth[o]);
@@ -442,8 +452,13 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
   T sq[MGPU_MAX_Q];
   for (int n = 0; n < s.nq; ++n) sq[n] = (T)0.0;
   if (k >= 2) {
-    // pw_advection (assigns), viscosity, coriolis, buoyancy: the order MONC adds them in
-    pw_point<T, View<T>>(s, P, U, V, W, k, j, i, su, sv, sw);
+    // pw_advection (assigns) or the TVD advection of the flow (adds to the cleared sources),
+    // viscosity, coriolis, buoyancy: the order MONC adds them in
+    if (s.tvd_flow)
+      tvd_flow_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.u : d.zu, s), view<T>(fwd ? d.v : d.zv, s),
+                                 view<T>(fwd ? d.w : d.zw, s), k, j, i, (T)0.0, (T)0.0, (T)0.0, su, sv, sw);
+    else
+      pw_point<T, View<T>>(s, P, U, V, W, k, j, i, su, sv, sw);
     if (s.use_vd) {
       View<T> ZU = view<T>(fwd ? d.u : d.zu, s), ZV = view<T>(fwd ? d.v : d.zv, s), ZW = view<T>(fwd ? d.w : d.zw, s);
       T du, dv, dw;
@@ -1128,7 +1143,7 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
   // the tiled kernels cover centred dry steps; the first (forward) step and moist runs use the
   // point kernel
   const bool moist = s.nq > 0;
-  const bool tiled_ok = !s.forward && !s.point_dynamics && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 &&
+  const bool tiled_ok = !s.forward && !s.point_dynamics && !s.tvd_flow && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 &&
                         s.nz >= 4 && (!moist || (d.sth && d.sq[s.nq - 1]));
   if (!tiled_ok) {
     k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);

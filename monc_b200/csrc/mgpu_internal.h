@@ -40,7 +40,7 @@ const std::vector<double>* profile_by_name(const RefState& rs, const std::string
 enum ProfileId {
   P_RDZ = 0, P_RDZN, P_DZN, P_RHO, P_RHON, P_DTHREF, P_CZB, P_CZA, P_CZG, P_CZH, P_TZC1, P_TZC2, P_TZD1, P_TZD2,
   P_RNEUTML_SQ, P_BUOY_CO, P_THREF, P_PREFRCP, P_RPREFRCP, P_TREF, P_TSTARPR, P_QSAT, P_DQSATDT, P_QSATFAC,
-  P_GWX, P_GWY, P_PREFN, P_TOFF, P_TC0, P_COUNT
+  P_GWX, P_GWY, P_PREFN, P_TOFF, P_TC0, P_DZ, P_COUNT
 };
 
 // Scalars every dynamical-core kernel reads (passed by value as a kernel parameter).
@@ -64,6 +64,7 @@ struct Scalars {
   int rho_unity;       // 1 when rho = rhon = 1 on every level (Boussinesq with rhobous = 1)
   int passive_th, passive_q, nq, iqv, iql;
   int coriolis, surface_bcs, use_vd;
+  int tvd_flow;            // 1: u, v, w advected by TVD (advection_flow_fields = tvd) instead of PW
   const double* prof;      // device: P_COUNT profiles, each (nz+2) long, 1-based
   const double* bmean;     // FP32-mixed fused step: horizontal means of th (row 0) and q(n) (row 1+n) per
                            // level, (nz+2) per row, removed from the buoyancy; null elsewhere

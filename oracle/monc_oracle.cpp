@@ -82,6 +82,8 @@ struct Model {
   std::vector<double> flux_x, flux_y, flux_z;
   TvdFieldState tvd_th;
   std::vector<TvdFieldState> tvd_q;
+  TvdFieldState tvd_u, tvd_v, tvd_w;  // TVD momentum advection (advection_flow_fields = tvd)
+  Field iflow[3][3];                  // [advected u, v, w][interpolated u, v, w]
   // psrce buffers (pressuresource.F90)
   std::vector<double> send_x, send_y, recv_x, recv_y;  // (nz-1, ny) / (nz-1, nx), 1-based (k-1, idx)
   // fft solver
@@ -589,6 +591,7 @@ static void smagorinsky_column(Model& m) {
 // ---------------------------------------------------------------------------------------------
 static void pw_advection_column(Model& m) {
   if (m.halo_column) return;
+  if (m.cfg.advection_flow_fields == MGPU_ADVECT_TVD) return;  // advect_flow is false (pwadvection.F90)
   int y = m.col_y, x = m.col_x;
   Field &U = m.u, &V = m.v, &W = m.w;
   const double tcx = m.tcx, tcy = m.tcy;
@@ -625,11 +628,21 @@ static void pw_advection_column(Model& m) {
 // ---------------------------------------------------------------------------------------------
 static const double r6 = 1.0 / 6.0;
 
-static double flux_in_w(Model& m, int k, double data_value, double dt, double sum_cfl_out, double rdc, double fdels,
-                        double fd, double fc, double fu, double rdu, double fgt1, double fgt2) {
-  double dd = m.dzn(k + 1);
-  double rdd = m.rdzn(k + 1);
-  double cflmod = std::fabs(data_value * m.rdzn(k + 1) * dt);
+// The vertical metrics ultflx is called with (tvdadvection.F90:722-908): scalars, u and v use
+// rdz, rdzn, dzn with kdof = 0 over k = 2..nz; w uses rdzn, rdz, dz with kdof = 1 over
+// k = 1..nz-1 (its bottom face from handle_vertical_fluxes_bottomofcolumn)
+struct TvdMetrics {
+  const Prof* rdz;
+  const Prof* rdzn;
+  const Prof* dzn;
+  int kdof, kmin, kmax;
+};
+
+static double flux_in_w(const TvdMetrics& M, int k, double data_value, double dt, double sum_cfl_out, double rdc,
+                        double fdels, double fd, double fc, double fu, double rdu, double fgt1, double fgt2) {
+  double dd = (*M.dzn)(k + 1);
+  double rdd = (*M.rdzn)(k + 1);
+  double cflmod = std::fabs(data_value * (*M.rdzn)(k + 1) * dt);
   double hrcfl = 1.0 / (sum_cfl_out + 1.e-30);
   double hcfl = 0.5 * cflmod;
   double cflcoef = r6 * (1.0 - cflmod * cflmod) * (dd * dd * rdc);
@@ -658,15 +671,15 @@ static double flux_in_xy(double data_value, double c, double dt, double sum_cfl_
 }
 
 // calculate_gradient_term_in_z
-static double grad_z(Model& m, int k, const double* col1, const double* col2, double dt, double advneg, double advpos,
-                     int kdof, int kp0, int kp1, const double* src1, const double* src2) {
+static double grad_z(const TvdMetrics& M, int k, const double* col1, const double* col2, double dt, double advneg,
+                     double advpos, int kdof, int kp0, int kp1, const double* src1, const double* src2) {
   double specific_face = 0.125 * (col1[k] + col1[k - 1] + col2[k] + col2[k - 1]);
   int kposwf = (int)std::lround(0.5 + sign_(0.5, specific_face));
   int ksu = kp1 * (1 - kposwf) + (k - 1) * kposwf;
   int ksl = kp0 * (1 - kposwf) + k * kposwf;
   double temp_src = src1[ksl] - src1[ksu];
   if (src2) temp_src = temp_src * advpos + (src2[ksl] - src2[ksu]) * advneg;
-  return std::fabs(specific_face) * m.rdz(k + kdof) * dt * temp_src;
+  return std::fabs(specific_face) * (*M.rdz)(k + kdof) * dt * temp_src;
 }
 
 // calculate_gradient_term_in_x
@@ -680,11 +693,58 @@ static double grad_x(int k, const double* c1, const double* c2, const double* c3
 // nint(sign(1.0, x)): +1 unless the sign bit of x is set (SIGN honours -0.0)
 static inline int nint_sign1(double x) { return std::signbit(x) ? -1 : 1; }
 
-static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& zf, int kdof, double dt,
+static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& zf, const TvdMetrics& M, double dt,
                    std::vector<double>& flux_y, std::vector<double>& flux_z, std::vector<double>& flux_x,
                    double* flux_previous_x) {
   const int nz = m.nz;
+  const int kdof = M.kdof;
   const double cx = m.cx, cy = m.cy;
+  auto rdz = [&](int k) { return (*M.rdz)(k); };
+  auto rdzn = [&](int k) { return (*M.rdzn)(k); };
+  // ---- handle_vertical_fluxes: bottom of column (kmin = 1, w only: flux_z(2))
+  if (M.kmin == 1) {
+    const int k = 1;
+    double fu, fc, fd;
+    if (W(k, y, x) >= 0.0) { fu = zf(1, y, x); fc = zf(k, y, x); fd = zf(k + 1, y, x); }
+    else { fu = zf(k + 2, y, x); fc = zf(k + 1, y, x); fd = zf(k, y, x); }
+    double fcurvs = fd - 2.0 * fc + fu;
+    double fdels = fd - fu;
+    if (std::fabs(fcurvs) >= std::fabs(fdels)) {
+      flux_z[k + 1] = fc;
+    } else {
+      double sum_cfl_out, fgt1, fgt2, rdu, rdc;
+      if (W(k, y, x) >= 0.0) {
+        sum_cfl_out = 0.0;
+        sum_cfl_out = sum_cfl_out + W(k, y, x) * rdz(k + kdof);
+        sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k, y, x)) + std::fabs(fmin_(0.0, V(k, y - 1, x))));
+        sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k, y, x)) + std::fabs(fmin_(0.0, U(k, y, x - 1))));
+        sum_cfl_out = sum_cfl_out * dt;
+        {
+          double sf = 0.125 * (V(k, y - 1, x) + V(k, y, x) + V(k + 1, y - 1, x) + V(k + 1, y, x));
+          int jsu = y - nint_sign1(sf);
+          fgt1 = std::fabs(sf) * cy * dt * (fc - zf(k, jsu, x));
+        }
+        fgt2 = grad_x(k, U.col(y, x - 1), U.col(y, x), U.col(y, x - 1), U.col(y, x), cx, dt, fc, zf(k, y, x + 1), zf(k, y, x - 1), 1);
+        rdu = rdzn(2);
+        rdc = rdz(k + kdof);
+      } else {
+        sum_cfl_out = 0.0;
+        sum_cfl_out = sum_cfl_out + rdz(k + 1 + kdof) * (fmax_(0.0, W(k + 1, y, x)) - W(k, y, x));
+        sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k + 1, y, x)) + std::fabs(fmin_(0.0, V(k + 1, y - 1, x))));
+        sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k + 1, y, x)) + std::fabs(fmin_(0.0, U(k + 1, y, x - 1))));
+        sum_cfl_out = sum_cfl_out * dt;
+        {
+          double sf = 0.125 * (V(k, y - 1, x) + V(k, y, x) + V(k + 1, y - 1, x) + V(k + 1, y, x));
+          int jsu = y - nint_sign1(sf);
+          fgt1 = std::fabs(sf) * cy * dt * (fc - zf(k + 1, jsu, x));
+        }
+        fgt2 = grad_x(k, U.col(y, x - 1), U.col(y, x), U.col(y, x - 1), U.col(y, x), cx, dt, fc, zf(k + 1, y, x + 1), zf(k + 1, y, x - 1), 1);
+        rdu = rdzn(k + 2);
+        rdc = rdz(k + 1 + kdof);
+      }
+      flux_z[k + 1] = flux_in_w(M, k, W(k, y, x), dt, sum_cfl_out, rdc, fdels, fd, fc, fu, rdu, fgt1, fgt2);
+    }
+  }
   // ---- handle_vertical_fluxes: top of column (k = nz-1)
   {
     int k = nz - 1;
@@ -700,7 +760,7 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
       double sum_cfl_out, fgt1, fgt2, rdu, rdc;
       if (W(k, y, x) >= 0.0) {
         sum_cfl_out = 0.0;
-        sum_cfl_out = sum_cfl_out + m.rdz(k + kdof) * (W(k, y, x) + std::fabs(fmin_(0.0, W(k - 1, y, x))));
+        sum_cfl_out = sum_cfl_out + rdz(k + kdof) * (W(k, y, x) + std::fabs(fmin_(0.0, W(k - 1, y, x))));
         sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k, y, x)) + std::fabs(fmin_(0.0, V(k, y - 1, x))));
         sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k, y, x)) + std::fabs(fmin_(0.0, U(k, y, x - 1))));
         sum_cfl_out = sum_cfl_out * dt;
@@ -711,11 +771,11 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
           fgt1 = std::fabs(sf) * cy * dt * (fc - zf(k, jsu, x));
         }
         fgt2 = grad_x(k, U.col(y, x - 1), U.col(y, x), U.col(y, x - 1), U.col(y, x), cx, dt, fc, zf(k, y, x + 1), zf(k, y, x - 1), 1);
-        rdu = m.rdzn(k);
-        rdc = m.rdz(k + kdof);
+        rdu = rdzn(k);
+        rdc = rdz(k + kdof);
       } else {
         sum_cfl_out = 0.0;
-        sum_cfl_out = sum_cfl_out + (-W(k, y, x) * m.rdz(std::min(nz, k + 1 + kdof)));
+        sum_cfl_out = sum_cfl_out + (-W(k, y, x) * rdz(std::min(nz, k + 1 + kdof)));
         sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k + 1, y, x)) + std::fabs(fmin_(0.0, V(k + 1, y - 1, x))));
         sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k + 1, y, x)) + std::fabs(fmin_(0.0, U(k + 1, y, x - 1))));
         sum_cfl_out = sum_cfl_out * dt;
@@ -725,10 +785,10 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
           fgt1 = std::fabs(sf) * cy * dt * (fc - zf(k + 1, jsu, x));
         }
         fgt2 = grad_x(k, U.col(y, x - 1), U.col(y, x), U.col(y, x - 1), U.col(y, x), cx, dt, fc, zf(k + 1, y, x + 1), zf(k + 1, y, x - 1), 1);
-        rdu = m.rdzn(nz);
-        rdc = m.rdz(std::min(nz, k + 1 + kdof));
+        rdu = rdzn(nz);
+        rdc = rdz(std::min(nz, k + 1 + kdof));
       }
-      flux_z[k + 1] = flux_in_w(m, k, W(k, y, x), dt, sum_cfl_out, rdc, fdels, fd, fc, fu, rdu, fgt1, fgt2);
+      flux_z[k + 1] = flux_in_w(M, k, W(k, y, x), dt, sum_cfl_out, rdc, fdels, fd, fc, fu, rdu, fgt1, fgt2);
     }
   }
   // ---- middle of column (k = 2 .. nz-2 -> flux_z(k+1))
@@ -745,7 +805,7 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
       flux_z[k + 1] = fc;
     } else {
       double sum_cfl_out = 0.0;
-      sum_cfl_out = sum_cfl_out + m.rdz(k + kofset) * (fmax_(0.0, W(k + kofset, y, x)) + std::fabs(fmin_(0.0, W(k - 1 + kofset, y, x))));
+      sum_cfl_out = sum_cfl_out + rdz(k + kofset) * (fmax_(0.0, W(k + kofset, y, x)) + std::fabs(fmin_(0.0, W(k - 1 + kofset, y, x))));
       sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k + kofset, y, x)) + std::fabs(fmin_(0.0, V(k + kofset, y - 1, x))));
       sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k + kofset, y, x)) + std::fabs(fmin_(0.0, U(k + kofset, y, x - 1))));
       sum_cfl_out = sum_cfl_out * dt;
@@ -757,15 +817,15 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
       }
       double fgt2 = grad_x(k, U.col(y, x - 1), U.col(y, x), U.col(y, x - 1), U.col(y, x), cx, dt, fc,
                            zf(k + kofset, y, x + 1), zf(k + kofset, y, x - 1), 1);
-      double rdu = m.rdzn(k) * advpos + m.rdzn(k + 2) * advneg;
-      double rdc = m.rdz(k + kdof) * advpos + m.rdz(k + 1 + kdof) * advneg;
-      flux_z[k + 1] = flux_in_w(m, k, W(k, y, x), dt, sum_cfl_out, rdc, fdels, fd, fc, fu, rdu, fgt1, fgt2);
+      double rdu = rdzn(k) * advpos + rdzn(k + 2) * advneg;
+      double rdc = rdz(k + kdof) * advpos + rdz(k + 1 + kdof) * advneg;
+      flux_z[k + 1] = flux_in_w(M, k, W(k, y, x), dt, sum_cfl_out, rdc, fdels, fd, fc, fu, rdu, fgt1, fgt2);
     }
   }
-  flux_z[2] = 0.0;  // kmin > 1
+  if (M.kmin > 1) flux_z[2] = 0.0;
   // ---- y direction (skipped on the last interior row of the last y-process)
   if (y != m.ye) {
-    for (int k = 2; k <= nz; ++k) {
+    for (int k = 2; k <= M.kmax; ++k) {
       int kp1 = std::min(k + 1, nz);
       int kp0 = kp1 - 1;
       double sm = sign_(0.5, V(k, y, x));
@@ -781,11 +841,11 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
         flux_y[k] = fc;
       } else {
         double sum_cfl_out = 0.0;
-        sum_cfl_out = sum_cfl_out + m.rdz(k) * (fmax_(0.0, W(k, y + jofset, x)) + std::fabs(fmin_(0.0, W(k - 1, y + jofset, x))));
+        sum_cfl_out = sum_cfl_out + rdz(k) * (fmax_(0.0, W(k, y + jofset, x)) + std::fabs(fmin_(0.0, W(k - 1, y + jofset, x))));
         sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k, y + jofset, x)) + std::fabs(fmin_(0.0, V(k, y - 1 + jofset + jperiod, x))));
         sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k, y + jofset, x)) + std::fabs(fmin_(0.0, U(k, y + jofset, x - 1))));
         sum_cfl_out = sum_cfl_out * dt;
-        double fgt1 = grad_z(m, k, W.col(y, x), W.col(y + 1, x), dt, advneg, advpos, kdof, kp0, kp1, zf.col(y + jofset, x), nullptr);
+        double fgt1 = grad_z(M, k, W.col(y, x), W.col(y + 1, x), dt, advneg, advpos, kdof, kp0, kp1, zf.col(y + jofset, x), nullptr);
         double fgt2 = grad_x(k, U.col(y, x - 1), U.col(y, x), U.col(y + 1, x - 1), U.col(y + 1, x), cx, dt, fc,
                              zf(k, y + jofset, x + 1), zf(k, y + jofset, x - 1), 0);
         flux_y[k] = flux_in_xy(V(k, y, x), cy, dt, sum_cfl_out, fdels, fd, fc, fu, fgt1, fgt2, fcurvs);
@@ -794,7 +854,7 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
   }
   // ---- x direction: flux_x <- previous (face x-1/2); compute face x+1/2 into flux_previous_x
   for (int k = 1; k <= nz; ++k) flux_x[k] = flux_previous_x[k];
-  for (int k = 2; k <= nz; ++k) {
+  for (int k = 2; k <= M.kmax; ++k) {
     int kp1 = std::min(k + 1, nz);
     int kp0 = kp1 - 1;
     double sm = sign_(.5, U(k, y, x));
@@ -810,18 +870,18 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
       double sum_cfl_out;
       if (U(k, y, x) > 0.0) {
         sum_cfl_out = 0.0;
-        sum_cfl_out = sum_cfl_out + m.rdz(k) * (fmax_(0.0, W(k, y, x)) + std::fabs(fmin_(0.0, W(k - 1, y, x))));
+        sum_cfl_out = sum_cfl_out + rdz(k) * (fmax_(0.0, W(k, y, x)) + std::fabs(fmin_(0.0, W(k - 1, y, x))));
         sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k, y, x)) + std::fabs(fmin_(0.0, V(k, y - 1, x))));
         sum_cfl_out = sum_cfl_out + cx * (U(k, y, x) + std::fabs(fmin_(0.0, U(k, y, x - 1))));
         sum_cfl_out = sum_cfl_out * dt;
       } else {
         sum_cfl_out = 0.0;
-        sum_cfl_out = sum_cfl_out + m.rdz(k) * (fmax_(0.0, W(k, y, x + 1)) + std::fabs(fmin_(0.0, W(k - 1, y, x + 1))));
+        sum_cfl_out = sum_cfl_out + rdz(k) * (fmax_(0.0, W(k, y, x + 1)) + std::fabs(fmin_(0.0, W(k - 1, y, x + 1))));
         sum_cfl_out = sum_cfl_out + cy * (fmax_(0.0, V(k, y, x + 1)) + std::fabs(fmin_(0.0, V(k, y - 1, x + 1))));
         sum_cfl_out = sum_cfl_out + cx * (fmax_(0.0, U(k, y, x + 1)) - U(k, y, x));
         sum_cfl_out = sum_cfl_out * dt;
       }
-      double fgt1 = grad_z(m, k, W.col(y, x), W.col(y, x + 1), dt, advneg, advpos, kdof, kp0, kp1, zf.col(y, x), zf.col(y, x + 1));
+      double fgt1 = grad_z(M, k, W.col(y, x), W.col(y, x + 1), dt, advneg, advpos, kdof, kp0, kp1, zf.col(y, x), zf.col(y, x + 1));
       double fgt2;
       {
         // calculate_gradient_term_in_y with data_two: v at (y, x+1) and (y, x)
@@ -838,33 +898,79 @@ static void ultflx(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& 
 }
 
 static void differentiate_face_values(Model& m, int y, int x, Field& U, Field& V, Field& W, Field& S,
-                                      const std::vector<double>& fyp, const double* fxp) {
+                                      const std::vector<double>& fyp, const double* fxp, const Prof& tz1,
+                                      const Prof& tz2, bool differentiate_top) {
   const double cx = m.cx, cy = m.cy;
   for (int k = 2; k <= m.nz - 1; ++k) {
     double& s = S(k, y, x);
     s = s + (V(k, y - 1, x) * fyp[k] - V(k, y, x) * m.flux_y[k]) * cy;
-    s = s + 4.0 * (W(k - 1, y, x) * m.flux_z[k] * m.tzc1(k) - W(k, y, x) * m.flux_z[k + 1] * m.tzc2(k));
+    s = s + 4.0 * (W(k - 1, y, x) * m.flux_z[k] * tz1(k) - W(k, y, x) * m.flux_z[k + 1] * tz2(k));
     s = s + (U(k, y, x - 1) * m.flux_x[k] - U(k, y, x) * fxp[k]) * cx;
   }
+  if (!differentiate_top) return;
   int k = m.nz;
   double& s = S(k, y, x);
   s = 0.0;
   s = s + (V(k, y - 1, x) * fyp[k] - V(k, y, x) * m.flux_y[k]) * cy;
-  s = s + 4.0 * m.tzc1(k) * W(k - 1, y, x) * m.flux_z[k];
+  s = s + 4.0 * tz1(k) * W(k - 1, y, x) * m.flux_z[k];
   s = s + (U(k, y, x - 1) * m.flux_x[k] - U(k, y, x) * fxp[k]) * cx;
 }
 
 static void advect_scalar_field(Model& m, double dt, Field& zqf, Field& qf, Field& sf, TvdFieldState& st) {
   int y = m.col_y, x = m.col_x;
   Field& src = (m.field_stepping == FORWARD_STEPPING) ? qf : zqf;
-  ultflx(m, y, x, m.u, m.v, m.w, src, 0, dt, m.flux_y, m.flux_z, m.flux_x, st.fpx_col(y));
+  const TvdMetrics M{&m.rdz, &m.rdzn, &m.dzn, 0, 2, m.nz};
+  ultflx(m, y, x, m.u, m.v, m.w, src, M, dt, m.flux_y, m.flux_z, m.flux_x, st.fpx_col(y));
   if (y == m.ye) {  // complete_y_flux_wrap_recv_if_required (serial: local copy)
     for (int k = 1; k <= m.nz; ++k) m.flux_y[k] = st.fyb[k];
   }
-  if (!m.halo_column) differentiate_face_values(m, y, x, m.u, m.v, m.w, sf, st.fpy, st.fpx_col(y));
+  if (!m.halo_column)
+    differentiate_face_values(m, y, x, m.u, m.v, m.w, sf, st.fpy, st.fpx_col(y), m.tzc1, m.tzc2, true);
   if (y < m.ye)
     for (int k = 1; k <= m.nz; ++k) st.fpy[k] = m.flux_y[k];
   if (y == m.ys - 1)  // register_y_flux_wrap_send_if_required
+    for (int k = 1; k <= m.nz; ++k) st.fyb[k] = m.flux_y[k];
+}
+
+// interpolate_to_dual (stencil.F90:87-169) for the advection of field c (0 u, 1 v, 2 w): u, v, w
+// averaged with their neighbour one point along the direction in which c is on the primal grid
+// (x for u, y for v, z for w; simplesetup.F90:70-85), left as they are where that neighbour is
+// outside the local arrays and, for z, at the top level.  MONC caches these per column as it
+// sweeps; stepfields lags two columns behind, so every cached value is a pre-step one and
+// computing them all before the sweep gives the same numbers.
+static void interpolate_flow(Model& m, int c) {
+  Field* src[3] = {&m.u, &m.v, &m.w};
+  for (int f = 0; f < 3; ++f) {
+    Field& in = *src[f];
+    Field& out = m.iflow[c][f];
+    for (int i = 1; i <= m.nxh; ++i)
+      for (int j = 1; j <= m.nyh; ++j)
+        for (int k = 1; k <= m.nz; ++k) {
+          const int jj = c == 1 ? j + 1 : j, ii = c == 0 ? i + 1 : i, kk = c == 2 ? k + 1 : k;
+          if (jj > m.nyh || ii > m.nxh || (c == 2 && k == m.nz)) out(k, j, i) = in(k, j, i);
+          else out(k, j, i) = 0.5 * (in(k, j, i) + in(kk, jj, ii));
+        }
+  }
+}
+
+// advect_u / advect_v / advect_w (tvdadvection.F90:765-908): field c advected by the interpolated
+// flow; w with the swapped vertical metrics and kdof = 1, its sources on levels 2..nz-1 only
+static void advect_flow_field(Model& m, int c, double dt, Field& f, Field& zf, Field& sf, TvdFieldState& st) {
+  int y = m.col_y, x = m.col_x;
+  Field& src = (m.field_stepping == FORWARD_STEPPING) ? f : zf;
+  Field &IU = m.iflow[c][0], &IV = m.iflow[c][1], &IW = m.iflow[c][2];
+  const TvdMetrics M = c == 2 ? TvdMetrics{&m.rdzn, &m.rdz, &m.dz, 1, 1, m.nz - 1}
+                              : TvdMetrics{&m.rdz, &m.rdzn, &m.dzn, 0, 2, m.nz};
+  ultflx(m, y, x, IU, IV, IW, src, M, dt, m.flux_y, m.flux_z, m.flux_x, st.fpx_col(y));
+  if (y == m.ye)
+    for (int k = 1; k <= m.nz; ++k) m.flux_y[k] = st.fyb[k];
+  if (!m.halo_column) {
+    if (c == 2) differentiate_face_values(m, y, x, IU, IV, IW, sf, st.fpy, st.fpx_col(y), m.tzd1, m.tzd2, false);
+    else differentiate_face_values(m, y, x, IU, IV, IW, sf, st.fpy, st.fpx_col(y), m.tzc1, m.tzc2, true);
+  }
+  if (y < m.ye)
+    for (int k = 1; k <= m.nz; ++k) st.fpy[k] = m.flux_y[k];
+  if (y == m.ys - 1)
     for (int k = 1; k <= m.nz; ++k) st.fyb[k] = m.flux_y[k];
 }
 
@@ -873,6 +979,14 @@ static void tvd_advection_column(Model& m) {
   if (m.halo_column) {
     bool keep = (y == 2 && x <= m.xe && x >= m.xs - 1) || (x == 2 && y >= m.ys && y <= m.ye);
     if (!keep) return;
+  }
+  if (m.cfg.advection_flow_fields == MGPU_ADVECT_TVD) {
+    // advect_flow_fields (tvdadvection.F90:603-646): momentum_stepping is always centred
+    // (steppingdirection.F90:32), so dt = 2 dtm
+    const double dtf = m.dtm * 2.0;
+    advect_flow_field(m, 0, dtf, m.u, m.zu, m.su, m.tvd_u);
+    advect_flow_field(m, 1, dtf, m.v, m.zv, m.sv, m.tvd_v);
+    advect_flow_field(m, 2, dtf, m.w, m.zw, m.sw, m.tvd_w);
   }
   double dt = m.dtm * 2.0;  // scalar_stepping is always CENTRED_STEPPING (steppingdirection.F90:29-33)
   if (m.th.active) advect_scalar_field(m, dt, m.zth, m.th, m.sth, m.tvd_th);
@@ -1487,6 +1601,8 @@ static void timestep(Model& m) {
   // subgrid
   column_group(m, {lower_bc_column, smagorinsky_column});
   // dynamics
+  if (m.cfg.advection_flow_fields == MGPU_ADVECT_TVD)
+    for (int c = 0; c < 3; ++c) interpolate_flow(m, c);
   if (m.cfg.simplecloud_enabled)
     column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
                      buoyancy_column, set_consistent_lowbc_column, simplecloud_column, diverr_column, psrce_column,
@@ -1577,6 +1693,13 @@ static Model* create(const mgpu_config* cfg) {
     m.k_cloudmax = k - 1;
   }
   m.tvd_th.alloc(nz, nyh);
+  if (cfg->advection_flow_fields == MGPU_ADVECT_TVD) {
+    m.tvd_u.alloc(nz, nyh);
+    m.tvd_v.alloc(nz, nyh);
+    m.tvd_w.alloc(nz, nyh);
+    for (auto& row : m.iflow)
+      for (Field& f : row) f.alloc(nz, nyh, nxh);
+  }
   m.flux_x.assign(nz + 2, 0.0); m.flux_y.assign(nz + 2, 0.0); m.flux_z.assign(nz + 2, 0.0);
   m.send_x.assign((size_t)(nz - 1) * m.ny, 0.0); m.recv_x = m.send_x;
   m.send_y.assign((size_t)(nz - 1) * m.nx, 0.0); m.recv_y = m.send_y;
@@ -1913,7 +2036,11 @@ int orc_component(void* h, int cid) {
       case MGPU_C_LOWER_BC: column_group(m, {lower_bc_column}); break;
       case MGPU_C_SMAGORINSKY: column_group(m, {smagorinsky_column}); break;
       case MGPU_C_PW_ADVECTION: column_group(m, {pw_advection_column}); break;
-      case MGPU_C_TVD_ADVECTION: column_group(m, {tvd_advection_column}); break;
+      case MGPU_C_TVD_ADVECTION:
+        if (m.cfg.advection_flow_fields == MGPU_ADVECT_TVD)
+          for (int c = 0; c < 3; ++c) interpolate_flow(m, c);
+        column_group(m, {tvd_advection_column});
+        break;
       case MGPU_C_DIFFUSION: column_group(m, {diffusion_column}); break;
       case MGPU_C_VISCOSITY: column_group(m, {viscosity_column}); break;
       case MGPU_C_CORIOLIS: column_group(m, {coriolis_column}); break;
