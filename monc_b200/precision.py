@@ -32,9 +32,11 @@ def build(a, precision):
     return c, st
 
 
-def run(a, precision, reproducible=0):
+def run(a, precision, reproducible=0, round_state=False):
     c, st = build(a, precision)
     c.reproducible = reproducible
+    if round_state:  # the initial state as the FP32-mixed model holds it
+        st = {k: v.astype(np.float32).astype(np.float64) for k, v in st.items()}
     m = api.Model(c)
     m.set_state(st)
     m.step(1)  # the forward step
@@ -79,6 +81,9 @@ def main(argv=None):
     # control: the same FP64 model with separately rounded multiply-adds; the difference shows how
     # far rounding-level changes alone grow in this developing convection
     _, thr, wr, qvr, _ = run(a, cf.FP64, reproducible=1) if a.control else (None, th64, w64, qv64, None)
+    # second control: FP64 throughout, from the initial state rounded to FP32 -- how far the
+    # rounding of the initial fields alone carries the flow, whatever the arithmetic
+    _, thi, wi, qvi, _ = run(a, cf.FP64, round_state=True) if a.control else (None, th64, w64, qv64, None)
     zmax = float(cf.stretched_levels(a.nz, a.dz_bottom, a.dz_top)[-1])
     print(json.dumps({
         "case": f"moist layer {a.nx}x{a.ny}x{a.nz}, dx={a.dx} m, dz {a.dz_bottom}->{a.dz_top} m (top {zmax:.0f} m), "
@@ -96,6 +101,8 @@ def main(argv=None):
         "rel_err_mean_ql": rel(ql32, ql64),
         "fp64_fma_vs_separate_rounding": {"rel_err_mean_theta": rel(thr, th64), "rel_err_mean_w2": rel(wr, w64),
                                            "rel_err_mean_qv": rel(qvr, qv64)},
+        "fp64_from_fp32_rounded_initial_state": {"rel_err_mean_theta": rel(thi, th64), "rel_err_mean_w2": rel(wi, w64),
+                                                 "rel_err_mean_qv": rel(qvi, qv64)},
     }))
 
 
