@@ -128,7 +128,13 @@ __device__ void lower_bc_column(const Scalars& s, const PA& P, const A& zu_state
   vis1 = v1;
   diff1 = d1;
   if (set_scalars) {
-    th1 = ((T)s.surface_temperature_flux * P(P_DZN, 2) / d1) + th_a(2, j, i) - P(P_THREF, 1) + P(P_THREF, 2);
+    if constexpr (sizeof(T) == 4) {
+      // FP32: thref(2) - thref(1) as the FP64 profile difference.  MONC's order, th(2) - thref(1)
+      // + thref(2), rounds th(2) to the spacing of thref (~290 K, ulp 3e-5 K) and turns the ghost
+      // value into a staircase of th(2) that drives the surface-layer buoyancy every step
+      th1 = th_a(2, j, i) + (((T)s.surface_temperature_flux * P(P_DZN, 2) / d1) + P(P_DTHREF, 1));
+    } else
+      th1 = ((T)s.surface_temperature_flux * P(P_DZN, 2) / d1) + th_a(2, j, i) - P(P_THREF, 1) + P(P_THREF, 2);
     qv1 = qv_a ? (*qv_a)(2, j, i) + (T)s.surface_vapour_flux * P(P_DZN, 2) / d1 : (T)0;
   } else {
     th1 = th_a(2, j, i);

@@ -85,6 +85,22 @@ def test_moist_fp32_mixed_tracks_fp64(gpu_lib):
         assert np.abs(a - b).max() <= 1e-4 * max(np.abs(b).max(), 1e-3)
 
 
+@pytest.mark.parametrize("timestep", [1, 2], ids=["forward", "centred"])
+def test_fp32_surface_ghost_theta_keeps_the_perturbation(gpu_lib, timestep):
+    """lower_bc's ghost value theta(1) = theta(2) + flux dzn / diff + thref(2) - thref(1) in FP32
+    carries theta(2) and the flux term (up to 1.4 K here) at FP32 precision, within 2e-6 K, not at
+    the spacing of thref = 289 K (3e-5 K) that MONC's order of the sum would round theta(2) to."""
+    out = []
+    for prec in (cf.FP64, cf.FP32_MIXED):
+        _, m = moist_pair(precision=prec)
+        m.set_timestep(timestep)
+        m.component("lower_bc")
+        out.append(m.download("th" if timestep == 1 else "zth")[0])
+        m.close()
+    assert np.abs(out[0]).max() > 1e-3  # the perturbation and the surface flux term are there
+    assert np.abs(out[1] - out[0]).max() <= 2e-6
+
+
 @pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
 def test_moist_tiled_bit_identical_to_point_kernel(gpu_lib, monkeypatch, precision):
     """The per-scalar tiled kernels plus the cloud step reproduce the point kernel bit for bit."""
