@@ -144,6 +144,8 @@ typedef struct mgpu_config {
   double  cfl_dtmmax, cfl_dtmmin, cfl_rincmax;      /* cfl_dtmmax, cfl_dtmmin, cfl_rincmax */
   int32_t l_constant_dtm;             /* l_constant_dtm */
   int32_t advection_flow_fields;      /* MGPU_ADVECT_PW / MGPU_ADVECT_TVD (MONC's "any" would advect twice) */
+  int32_t adjoint_taped;              /* 1: adjoint passes on the operator-overloading tape (the check
+                                         path); 0: the hand-written adjoint kernels */
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */

@@ -27,6 +27,7 @@ UNITS = [
     ("fft.cu", []),
     ("iter.cu", []),
     ("tlad.cu", []),
+    ("adjoint.cu", []),
     ("slab.cu", []),
     ("cfl.cu", []),
 ]

@@ -70,6 +70,7 @@ class MgpuConfig(C.Structure):
         ("cfl_dtmmax", C.c_double), ("cfl_dtmmin", C.c_double), ("cfl_rincmax", C.c_double),
         ("l_constant_dtm", C.c_int32),
         ("advection_flow_fields", C.c_int32),
+        ("adjoint_taped", C.c_int32),
     ]
 
 

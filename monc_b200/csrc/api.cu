@@ -749,12 +749,20 @@ static int adjoint_step(mgpu_handle* h) {
   tg[F_PROF] = a->prof_bar;
   const double* seed[8];
   for (int q = 0; q < 8; ++q) seed[q] = B[q];
-  adj_pass(4, h->sc, d, tg, seed, a->overflow, h->stream);  // pstep + swap_smooth
+  auto pass = [&](int q) {
+    if (h->cfg.adjoint_taped) {
+      adj_pass(q, h->sc, d, tg, seed, a->overflow, h->stream);
+      return;
+    }
+    if (q == 0) adj_lower_bc(h->sc, d, tg, seed, a->overflow, h->stream);
+    if (!hadj_pass(q, h->sc, d, tg, seed, h->stream)) adj_pass(q, h->sc, d, tg, seed, a->overflow, h->stream);
+  };
+  pass(4);  // pstep + swap_smooth
   fft_solve<double>(h->fft, h->sc, a->inter[5], h->stream, &h->launches, nullptr, true);
-  adj_pass(3, h->sc, d, tg, seed, a->overflow, h->stream);  // pressure source
-  adj_pass(1, h->sc, d, tg, seed, a->overflow, h->stream);  // momentum
-  adj_pass(2, h->sc, d, tg, seed, a->overflow, h->stream);  // scalars
-  adj_pass(0, h->sc, d, tg, seed, a->overflow, h->stream);  // subgrid
+  pass(3);  // pressure source
+  pass(1);  // momentum
+  pass(2);  // scalars
+  pass(0);  // subgrid
   h->launches += 5;
   a->cur = 1 - a->cur;
   return MGPU_OK;

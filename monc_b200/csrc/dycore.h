@@ -112,5 +112,12 @@ void tl_pass(int pass, const Scalars& s, const DevState<double>& d, const DevSta
 // the adjoints of the next state (u v w th zu zv zw zth), tg[F_*] the adjoint arrays added into
 void adj_pass(int pass, const Scalars& s, const DevState<double>& d, double* const* tg, const double* const* seed,
               int* overflow, cudaStream_t st);
+// the subgrid pass's adjoint on level 1 only (lower_bc), on the tape
+void adj_lower_bc(const Scalars& s, const DevState<double>& d, double* const* tg, const double* const* seed,
+                  int* overflow, cudaStream_t st);
+// the hand-written adjoint of the same pass (adjoint.cu; the subgrid pass covers levels 2..nz, with
+// level 1 left to adj_lower_bc); false when the pass has none
+bool hadj_pass(int pass, const Scalars& s, const DevState<double>& d, double* const* tg, const double* const* seed,
+               cudaStream_t st);
 
 }  // namespace mgpu

@@ -66,6 +66,7 @@ extern "C" void mgpu_config_defaults(mgpu_config* c) {
   c->cfl_rincmax = 0.05;
   c->l_constant_dtm = 0;
   c->advection_flow_fields = MGPU_ADVECT_PW;
+  c->adjoint_taped = 0;
 }
 
 // w-level heights: piecewise-linear kgd/hgd grid smoothed nsmth times

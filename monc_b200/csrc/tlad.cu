@@ -467,6 +467,18 @@ __global__ void __launch_bounds__(128) k_adj_subgrid(Scalars s, AdjArgs a) {
 static dim3 ad_grid(const Scalars& s) { return dim3((s.nx + 31) / 32, (s.ny + 3) / 4, s.nz); }
 static dim3 ad_block() { return dim3(32, 4, 1); }
 
+void adj_lower_bc(const Scalars& s, const DevState<double>& d, double* const* tg, const double* const* seed,
+                  int* overflow, cudaStream_t st) {
+  tlad::AdjArgs a;
+  a.d = d;
+  for (int f = 0; f < F_COUNT; ++f) a.tg[f] = tg[f];
+  for (int q = 0; q < 8; ++q) a.seed[q] = seed[q];
+  a.overflow = overflow;
+  dim3 grid = ad_grid(s);
+  grid.z = 1;  // k = 1 only
+  tlad::k_adj_subgrid<<<grid, ad_block(), 0, st>>>(s, a);
+}
+
 void tl_pass(int pass, const Scalars& s, const DevState<double>& d, const DevState<double>& t, const double* drsq,
              double dpar, cudaStream_t st) {
   tlad::TlArgs a{d, t, drsq, dpar};
