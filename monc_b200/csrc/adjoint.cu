@@ -955,56 +955,79 @@ __device__ void adj_strain(const Scalars& s, const Prof<double>& P, const View<d
   }
 }
 
+// sum of v over the block (all of whose threads lie on one level), added to *dst by one thread
+__device__ __forceinline__ void block_add(double v, double* dst) {
+  __shared__ double part[4];
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+  if (lane == 0) part[warp] = v;
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    const double t = (part[0] + part[1]) + (part[2] + part[3]);
+    if (t != 0.0) atomicAdd(dst, t);
+  }
+}
+
+// one block of 32 x 4 threads per (x, y) tile of one level: the rneutml_sq adjoint of the level is
+// summed over the block before its single atomic (every point of a level adds to the same entry)
 __global__ void __launch_bounds__(128) k_hadj_smagorinsky(Scalars s, Args a) {
-  HADJ_POINT_INDEX
-  if (k < 2 || k >= s.nz) return;
-  const double vb = a.tg[F_VIS][o], db = a.tg[F_DIFF][o];
-  if (vb == 0.0 && db == 0.0) return;
-  const Geo g = geo(s);
-  const Prof<double> P{s.prof, s.nz + 2};
-  const Scatter S{a.tg, g};
-  const DevState<double>& d = a.d;
-  const bool fwd = s.forward;
-  const View<double> U{fwd ? d.u : d.zu, g}, V{fwd ? d.v : d.zv, g}, W{fwd ? d.w : d.zw, g}, TH{d.th, g};
-  const VelAdj f = fwd ? VelAdj{F_U, F_V, F_W} : VelAdj{F_ZU, F_ZV, F_ZW};
-  // forward
-  const double ssq = half_squared_strain<double>(s, P, U, V, W, k, j, i);
-  double ri = 0.0;
-  if (!s.passive_th)
-    ri = (P(P_DTHREF, k) + TH(k + 1, j, i) - TH(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
-  double vs = 0.0, df = 0.0, ri_vs = 0.0, ri_df = 0.0;  // the stability functions and their ri-derivatives
-  if (ri <= 0.0) {
-    const double x1 = 1.0 - s.subc * ri, x2 = 1.0 - s.subb * ri;
-    vs = sqrt(x1);
-    const double r2 = sqrt(x2);
-    df = s.suba * r2;
-    ri_vs = vs > 0.0 ? -s.subc * 0.5 / vs : 0.0;
-    ri_df = r2 > 0.0 ? -s.subb * s.suba * 0.5 / r2 : 0.0;
-  } else if (ri > 0.0 && ri < s.ric) {
-    const double t1 = 1. - ri * s.ricinv;
-    const double t = t1 * t1;
-    const double rifac = t * t;
-    const double ev = 1. - s.subh * ri, ed = 1. - s.subg * ri;
-    vs = rifac * ev;
-    df = rifac * s.suba * ed;
-    const double rifac_ri = 2.0 * t * 2.0 * t1 * (-s.ricinv);
-    ri_vs = rifac_ri * ev - rifac * s.subh;
-    ri_df = rifac_ri * s.suba * ed - rifac * s.suba * s.subg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z + 1;
+  if (k < 2 || k >= s.nz) return;  // uniform over the block
+  double prof_c = 0.0;
+  if (i < s.nx && j < s.ny) {
+    const long long o = (long long)(k - 1) * s.plane + (long long)j * s.nx + i;
+    const double vb = a.tg[F_VIS][o], db = a.tg[F_DIFF][o];
+    if (vb != 0.0 || db != 0.0) {
+      const Geo g = geo(s);
+      const Prof<double> P{s.prof, s.nz + 2};
+      const Scatter S{a.tg, g};
+      const DevState<double>& d = a.d;
+      const bool fwd = s.forward;
+      const View<double> U{fwd ? d.u : d.zu, g}, V{fwd ? d.v : d.zv, g}, W{fwd ? d.w : d.zw, g}, TH{d.th, g};
+      const VelAdj f = fwd ? VelAdj{F_U, F_V, F_W} : VelAdj{F_ZU, F_ZV, F_ZW};
+      // forward
+      const double ssq = half_squared_strain<double>(s, P, U, V, W, k, j, i);
+      double ri = 0.0;
+      if (!s.passive_th)
+        ri = (P(P_DTHREF, k) + TH(k + 1, j, i) - TH(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
+      double vs = 0.0, df = 0.0, ri_vs = 0.0, ri_df = 0.0;  // stability functions and their ri-derivatives
+      if (ri <= 0.0) {
+        const double x1 = 1.0 - s.subc * ri, x2 = 1.0 - s.subb * ri;
+        vs = sqrt(x1);
+        const double r2 = sqrt(x2);
+        df = s.suba * r2;
+        ri_vs = vs > 0.0 ? -s.subc * 0.5 / vs : 0.0;
+        ri_df = r2 > 0.0 ? -s.subb * s.suba * 0.5 / r2 : 0.0;
+      } else if (ri > 0.0 && ri < s.ric) {
+        const double t1 = 1. - ri * s.ricinv;
+        const double t = t1 * t1;
+        const double rifac = t * t;
+        const double ev = 1. - s.subh * ri, ed = 1. - s.subg * ri;
+        vs = rifac * ev;
+        df = rifac * s.suba * ed;
+        const double rifac_ri = 2.0 * t * 2.0 * t1 * (-s.ricinv);
+        ri_vs = rifac_ri * ev - rifac * s.subh;
+        ri_df = rifac_ri * s.suba * ed - rifac * s.suba * s.subg;
+      }
+      const double rsq = P(P_RNEUTML_SQ, k), sq = sqrt(ssq);
+      const double sctmp = rsq * sq;
+      // reverse: vis = vs sctmp, diff = df sctmp, sctmp = rneutml_sq sqrt(ssq)
+      const double sct_b = vb * vs + db * df;
+      prof_c = sct_b * sq;
+      double ssq_b = sq > 0.0 ? sct_b * rsq * 0.5 / sq : 0.0;
+      const double ri_b = (vb * ri_vs + db * ri_df) * sctmp;
+      if (!s.passive_th && ri_b != 0.0) {
+        const double nb = ri_b * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
+        S(F_TH, k + 1, j, i, nb);
+        S(F_TH, k, j, i, -nb);
+        ssq_b -= ri_b * ri / ssq;
+      }
+      adj_strain(s, P, U, V, W, S, f, k, j, i, ssq_b);
+    }
   }
-  const double rsq = P(P_RNEUTML_SQ, k), sq = sqrt(ssq);
-  const double sctmp = rsq * sq;
-  // reverse: vis = vs sctmp, diff = df sctmp, sctmp = rneutml_sq sqrt(ssq)
-  const double sct_b = vb * vs + db * df;
-  atomicAdd(a.tg[F_PROF] + k, sct_b * sq);
-  double ssq_b = sq > 0.0 ? sct_b * rsq * 0.5 / sq : 0.0;
-  const double ri_b = (vb * ri_vs + db * ri_df) * sctmp;
-  if (!s.passive_th && ri_b != 0.0) {
-    const double nb = ri_b * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
-    S(F_TH, k + 1, j, i, nb);
-    S(F_TH, k, j, i, -nb);
-    ssq_b -= ri_b * ri / ssq;
-  }
-  adj_strain(s, P, U, V, W, S, f, k, j, i, ssq_b);
+  block_add(prof_c, a.tg[F_PROF] + k);
 }
 }  // namespace hadj
 
