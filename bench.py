@@ -386,6 +386,7 @@ def adjoint_ratio():
         seed[f] = pert / (a.nx * a.ny) * (dz * lev)[:, None, None]
     _, fwd_ms, adj_ms = gc.timed_window(cfg, base, steps, seed, interval)
     return {"window": "dry CBL 128x128x96, dx=50 m, dz=20 m, dt=1 s, 300 steps, FP64, checkpoint every 25 steps",
+            "timing": "second run of each from the same state; the first allocates the work buffers",
             "forward_ms": round(fwd_ms, 3), "adjoint_ms": round(adj_ms, 3),
             "adjoint_forward_ratio": round(adj_ms / fwd_ms, 2)}
 

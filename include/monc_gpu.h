@@ -51,6 +51,12 @@ extern "C" {
 #define MGPU_ADVECT_PW   0  /* Piacsek-Williams centred flux form (the benchmark configurations) */
 #define MGPU_ADVECT_TVD  1  /* TVD (ULTIMATE-QUICKEST) on the dual grids of u, v, w */
 
+/* subsidence input (forcing.F90:40-41, subsidence_input_type): the f_subs_pl nodes are a
+ * divergence (w_subs = -div z) or the subsidence velocity itself */
+#define MGPU_SUBS_DIVERGENCE 0
+#define MGPU_SUBS_VELOCITY   1
+#define MGPU_MAX_SUBS_NODES  32
+
 /* iterative solver types (iterativesolver.F90 solver_type) */
 #define MGPU_ITER_BICGSTAB 0
 #define MGPU_ITER_CG       1
@@ -94,6 +100,9 @@ enum mgpu_component_id {
   MGPU_C_ITERATIVESOLVER,       /* iterativesolver.F90:87-602 */
   MGPU_C_PSTEP,                 /* pstep.F90:310-469 */
   MGPU_C_SWAP_SMOOTH,           /* swapsmooth.F90:45-289 */
+  MGPU_C_MEAN_PROFILES,         /* meanprofiles.F90:95-216: olzubar, olzvbar, olzthbar, olzqbar */
+  MGPU_C_DAMPING,               /* damping.F90:301-409 */
+  MGPU_C_FORCING,               /* forcing.F90:918-1166: subsidence of u, v, theta and q */
   MGPU_C_COUNT
 };
 
@@ -146,6 +155,20 @@ typedef struct mgpu_config {
   int32_t advection_flow_fields;      /* MGPU_ADVECT_PW / MGPU_ADVECT_TVD (MONC's "any" would advect twice) */
   int32_t adjoint_taped;              /* 1: adjoint passes on the operator-overloading tape (the check
                                          path); 0: the hand-written adjoint kernels */
+  /* damping (damping.F90:124-148, global_config:157-159): Newtonian relaxation of u, v, theta and q
+   * towards their horizontal means, and of w towards 0, above zdmp; dmpco = dmptim (exp((zn -
+   * zdmp)/hdmp) - 1).  Needs the mean profiles, which the library keeps on the device. */
+  int32_t damping_enabled;            /* damping_enabled */
+  double  dmptim, zdmp, hdmp;         /* dmptim, zdmp, hdmp */
+  /* forcing: subsidence (forcing.F90:447-1166, global_config:313-317).  w_subs is the piecewise-
+   * linear interpolation (interpolation.F90:15-58) of the n_subs_pl nodes onto the w levels z. */
+  int32_t l_subs_pl_theta;            /* subsidence of u, v and theta */
+  int32_t l_subs_pl_q;                /* subsidence of the q fields */
+  int32_t subsidence_input_type;      /* MGPU_SUBS_DIVERGENCE / MGPU_SUBS_VELOCITY */
+  int32_t subsidence_local_theta;     /* 1: theta (and u, v) gradients of the column, 0: of the mean profiles */
+  int32_t subsidence_local_q;         /* the same for q */
+  int32_t n_subs_pl;                  /* nodes in z_subs_pl / f_subs_pl (<= MGPU_MAX_SUBS_NODES) */
+  double  z_subs_pl[MGPU_MAX_SUBS_NODES], f_subs_pl[MGPU_MAX_SUBS_NODES];
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */
@@ -229,6 +252,12 @@ int64_t mgpu_launch_count(mgpu_handle* h);
  * mean of w squared per level (the domain-mean theta and w'^2 profiles used to judge runs);
  * either pointer may be NULL.  Reads back 8*nz bytes per non-NULL pointer. */
 int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2);
+
+/* The mean profiles damping and forcing read (meanprofiles.F90:95-216, global_grid vertical
+ * olzubar, olzvbar, olzthbar, olzqbar): out receives (3 + number_q_fields) rows of nz values,
+ * k = 1..nz.  mgpu_step refreshes them in the solver group of each step when damping or
+ * non-local subsidence is on; MGPU_C_MEAN_PROFILES refreshes them from zu, zv, zth, zq. */
+int mgpu_mean_profiles(mgpu_handle* h, double* out);
 
 /* Per-stage device timing of mgpu_step (CUDA events on the handle's stream).  Stage order:
  * 0 subgrid, 1 dynamics, 2 pressure source, 3 fft x forward, 4 fft y forward, 5 tridiagonal,

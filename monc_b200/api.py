@@ -69,15 +69,18 @@ COMPONENTS = {
     "iterativesolver": 17,
     "pstep": 18,
     "swap_smooth": 19,
+    "mean_profiles": 20,
+    "damping": 21,
+    "forcing": 22,
 }
 
 # MONC's default group layout of these components (global_config:77-92)
 GROUPS = {
     "start": ["clearsourceterms", "stepping_direction", "halo_swapper"],
     "subgrid": ["lower_bc", "smagorinsky"],
-    "dynamics": ["pw_advection", "tvd_advection", "diffusion", "viscosity", "coriolis", "buoyancy",
-                 "set_consistent_lowbc", "simplecloud", "diverr", "psrce", "stepfields"],
-    "solver": ["fftsolver", "iterativesolver"],
+    "dynamics": ["pw_advection", "tvd_advection", "diffusion", "viscosity", "coriolis", "buoyancy", "damping",
+                 "forcing", "set_consistent_lowbc", "simplecloud", "diverr", "psrce", "stepfields"],
+    "solver": ["mean_profiles", "fftsolver", "iterativesolver"],
     "pressure-terms": ["pstep", "swap_smooth"],
 }
 
@@ -139,6 +142,8 @@ def lib():
     L.mgpu_launch_count.restype = C.c_int64
     L.mgpu_diagnostics.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.mgpu_diagnostics.restype = C.c_int
+    L.mgpu_mean_profiles.argtypes = [C.c_void_p, C.c_void_p]
+    L.mgpu_mean_profiles.restype = C.c_int
     L.mgpu_set_profiling.argtypes = [C.c_void_p, C.c_int32]
     L.mgpu_set_profiling.restype = C.c_int
     L.mgpu_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -303,6 +308,15 @@ class Model:
         self._check(lib().mgpu_mean_profile(self.h, field_id(name), out.ctypes.data), "mean_profile")
         return out
 
+    def mean_profiles(self) -> dict:
+        """The mean profiles damping and forcing read: olzubar, olzvbar, olzthbar and olzqbar(n)
+        (meanprofiles.F90), as refreshed by the last step or mean_profiles component."""
+        rows = 3 + self.cfg.number_q_fields
+        out = np.empty((rows, self.nz), dtype=np.float64)
+        self._check(lib().mgpu_mean_profiles(self.h, out.ctypes.data), "mean_profiles")
+        names = ["olzubar", "olzvbar", "olzthbar"] + [f"olzqbar{n}" for n in range(self.cfg.number_q_fields)]
+        return dict(zip(names, out))
+
     def diagnostics(self, out_th: np.ndarray | None = None, out_w2: np.ndarray | None = None):
         """Device-computed horizontal means: theta (incl. thref) and w**2 per level."""
         th = out_th if out_th is not None else np.empty(self.nz, dtype=np.float64)
@@ -392,6 +406,13 @@ def run_groups(model: Model, groups=("start", "subgrid", "dynamics", "solver", "
             if name == "simplecloud" and not model.cfg.simplecloud_enabled:
                 continue
             if name == "coriolis" and not model.cfg.coriolis_enabled:
+                continue
+            if name == "damping" and not model.cfg.damping_enabled:
+                continue
+            if name == "forcing" and not (model.cfg.l_subs_pl_theta or model.cfg.l_subs_pl_q):
+                continue
+            if name == "mean_profiles" and not (model.cfg.damping_enabled or model.cfg.l_subs_pl_theta
+                                                or model.cfg.l_subs_pl_q):
                 continue
             model.component(name)
     ts = model.reductions().timestep

@@ -30,6 +30,7 @@ UNITS = [
     ("adjoint.cu", []),
     ("slab.cu", []),
     ("cfl.cu", []),
+    ("forcing.cu", []),
 ]
 
 

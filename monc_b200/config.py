@@ -24,6 +24,8 @@ PHASE_SUBGRID, PHASE_DYNAMICS, PHASE_PSTEP = 0, 1, 2
 HALO_STATE, HALO_PRESSURE = 0, 1
 ITER_BICGSTAB = 0
 ITER_CG = 1
+SUBS_DIVERGENCE, SUBS_VELOCITY = 0, 1  # subsidence_input_type (forcing.F90:40-41)
+MAX_SUBS_NODES = 32
 
 
 class MgpuConfig(C.Structure):
@@ -71,6 +73,13 @@ class MgpuConfig(C.Structure):
         ("l_constant_dtm", C.c_int32),
         ("advection_flow_fields", C.c_int32),
         ("adjoint_taped", C.c_int32),
+        ("damping_enabled", C.c_int32),
+        ("dmptim", C.c_double), ("zdmp", C.c_double), ("hdmp", C.c_double),
+        ("l_subs_pl_theta", C.c_int32), ("l_subs_pl_q", C.c_int32),
+        ("subsidence_input_type", C.c_int32),
+        ("subsidence_local_theta", C.c_int32), ("subsidence_local_q", C.c_int32),
+        ("n_subs_pl", C.c_int32),
+        ("z_subs_pl", C.c_double * MAX_SUBS_NODES), ("f_subs_pl", C.c_double * MAX_SUBS_NODES),
     ]
 
 
@@ -139,6 +148,12 @@ def default_config() -> MgpuConfig:
     c.cfl_rincmax = 0.05
     c.l_constant_dtm = 0
     c.advection_flow_fields = ADVECT_PW
+    c.damping_enabled = 0
+    c.dmptim = c.zdmp = c.hdmp = 0.0
+    c.l_subs_pl_theta = c.l_subs_pl_q = 0
+    c.subsidence_input_type = SUBS_VELOCITY
+    c.subsidence_local_theta = c.subsidence_local_q = 1
+    c.n_subs_pl = 0
     return c
 
 
@@ -191,6 +206,35 @@ def enable_cfl(c: MgpuConfig, frequency: int = 10, dtmmax: float = 100.0, dtmmin
     c.cfl_dtmmax, c.cfl_dtmmin, c.cfl_rincmax = dtmmax, dtmmin, rincmax
     c.cfl_tollerance, c.cfl_cvismax, c.cfl_cvelmax = tollerance, cvismax, cvelmax
     c.l_constant_dtm = 1 if constant_dtm else 0
+    return c
+
+
+def enable_damping(c: MgpuConfig, dmptim: float, zdmp: float, hdmp: float) -> MgpuConfig:
+    """Switch on the damping layer with MONC's option names (damping.F90:124-148): relaxation at
+    rate dmptim (exp((z - zdmp)/hdmp) - 1) above zdmp towards the mean profiles."""
+    c.damping_enabled = 1
+    c.dmptim, c.zdmp, c.hdmp = dmptim, zdmp, hdmp
+    return c
+
+
+def enable_subsidence(c: MgpuConfig, z_nodes, f_nodes, input_type: int = None, theta: bool = True,
+                      q: bool = False, local_theta: bool = False, local_q: bool = False) -> MgpuConfig:
+    """Subsidence forcing with MONC's option names (forcing.F90:447-582, global_config:313-317):
+    w_subs interpolated from the (z_subs_pl, f_subs_pl) nodes, a velocity or, with
+    input_type = SUBS_DIVERGENCE, a divergence (w_subs = -div z); applied to u, v and theta
+    (l_subs_pl_theta) and the q fields (l_subs_pl_q), with the column's gradients (local) or those
+    of the mean profiles."""
+    if len(z_nodes) != len(f_nodes) or not 1 <= len(z_nodes) <= MAX_SUBS_NODES:
+        raise ValueError(f"z_subs_pl and f_subs_pl need the same length, 1..{MAX_SUBS_NODES}")
+    c.l_subs_pl_theta = 1 if theta else 0
+    c.l_subs_pl_q = 1 if q else 0
+    c.subsidence_input_type = SUBS_VELOCITY if input_type is None else input_type
+    c.subsidence_local_theta = 1 if local_theta else 0
+    c.subsidence_local_q = 1 if local_q else 0
+    c.n_subs_pl = len(z_nodes)
+    for n, (z, f) in enumerate(zip(z_nodes, f_nodes)):
+        c.z_subs_pl[n] = z
+        c.f_subs_pl[n] = f
     return c
 
 

@@ -56,6 +56,8 @@ struct mgpu_handle {
   double* xfer = nullptr;  // device staging buffer (FP64 field) for uploads/downloads
   double* diag_d = nullptr;  // 2*nz FP64 diagnostics
   double* bmean_d = nullptr; // FP32-mixed: horizontal means of th and q per level (1+nq rows of nz+2)
+  double* olz_d = nullptr;       // mean profiles olzubar, olzvbar, olzthbar, olzqbar (3+MGPU_MAX_Q rows of nz+2)
+  double* subs_tend_d = nullptr; // mean-profile subsidence tendencies, the same rows
   bool profiling = false;
   cudaEvent_t ev[16] = {};
   struct AdWork* ad = nullptr;  // tangent-linear / adjoint arrays, allocated on first use
@@ -187,6 +189,32 @@ static void fill_scalars(mgpu_handle* h) {
     if (r.rho[k] != 1.0 || r.rhon[k] != 1.0) s.rho_unity = 0;
   s.prof = h->prof_d;
   s.lookup = h->lookup_d;
+  s.damping = s.subs_th = s.subs_q = 0;  // set per step (forcing_flags)
+  s.kdmpmin = r.kdmpmin;
+  s.subs_local_th = c.subsidence_local_theta;
+  s.subs_local_q = c.subsidence_local_q;
+  s.olz = h->olz_d;
+  s.subs_tend = h->subs_tend_d;
+}
+
+// damping and forcing act from timestep 3 (damping.F90:329-330, forcing.F90:974-975)
+static void forcing_flags(mgpu_handle* h) {
+  const mgpu_config& c = h->cfg;
+  const bool on = h->timestep >= 3;
+  h->sc.damping = (c.damping_enabled && on) ? 1 : 0;
+  h->sc.subs_th = (c.l_subs_pl_theta && on) ? 1 : 0;
+  h->sc.subs_q = (c.l_subs_pl_q && c.number_q_fields > 0 && on) ? 1 : 0;
+}
+// the mean profiles are refreshed every step when damping or mean-profile subsidence reads them
+static bool needs_mean_profiles(const mgpu_config& c) {
+  return c.damping_enabled || (c.l_subs_pl_theta && !c.subsidence_local_theta) ||
+         (c.l_subs_pl_q && !c.subsidence_local_q && c.number_q_fields > 0);
+}
+// the mean-profile subsidence tendencies of this step, from the mean profiles of the last
+static int subsidence_tendencies(mgpu_handle* h) {
+  const bool ft = h->sc.subs_th && !h->sc.subs_local_th, q = h->sc.subs_q && !h->sc.subs_local_q;
+  if (!ft && !q) return 0;
+  return launch_subsidence_tendencies(h->sc, h->olz_d, h->subs_tend_d, ft, q, h->stream);
 }
 
 static const std::vector<double>* prof_vec(const RefState& r, int id) {
@@ -200,6 +228,7 @@ static const std::vector<double>* prof_vec(const RefState& r, int id) {
     case P_QSAT: return &r.qsat; case P_DQSATDT: return &r.dqsatdt; case P_QSATFAC: return &r.qsatfac;
     case P_GWX: return &r.gwx; case P_GWY: return &r.gwy; case P_PREFN: return &r.prefn;
     case P_TOFF: return &r.moist_toff; case P_TC0: return &r.tc0; case P_DZ: return &r.dz;
+    case P_DMPCO: return &r.dmpco; case P_DMPCOZ: return &r.dmpcoz; case P_WSUBS: return &r.w_subs;
   }
   return nullptr;
 }
@@ -254,6 +283,13 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   if (cudaMalloc(&h->bmean_d, (size_t)(1 + MGPU_MAX_Q) * (cfg->nz + 2) * sizeof(double)) != cudaSuccess)
     return cleanup(MGPU_ERR_CUDA);
   cudaMemset(h->bmean_d, 0, (size_t)(1 + MGPU_MAX_Q) * (cfg->nz + 2) * sizeof(double));
+  {
+    const size_t nb = (size_t)(3 + MGPU_MAX_Q) * (cfg->nz + 2) * sizeof(double);
+    if (cudaMalloc(&h->olz_d, nb) != cudaSuccess || cudaMalloc(&h->subs_tend_d, nb) != cudaSuccess)
+      return cleanup(MGPU_ERR_CUDA);
+    cudaMemset(h->olz_d, 0, nb);
+    cudaMemset(h->subs_tend_d, 0, nb);
+  }
   for (cudaEvent_t& e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
   fill_scalars(h);
@@ -299,6 +335,8 @@ int mgpu_destroy(mgpu_handle* h) {
   cudaFree(h->xfer);
   cudaFree(h->diag_d);
   cudaFree(h->bmean_d);
+  cudaFree(h->olz_d);
+  cudaFree(h->subs_tend_d);
   cudaFree(h->cfl.part_d);
   cudaFree(h->cfl.out_d);
   if (h->cfl.out_h) cudaFreeHost(h->cfl.out_h);
@@ -334,6 +372,8 @@ static int ad_supported(mgpu_handle* h) {
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the PW advection of the flow");
   if (h->cfg.cfl_enabled)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs hold dtm fixed: disable cfltest");
+  if (h->cfg.damping_enabled || h->cfg.l_subs_pl_theta || h->cfg.l_subs_pl_q)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the step without damping and forcing");
   if (h->fp32 || h->cfg.number_q_fields > 0 || h->cfg.solver != MGPU_SOLVER_FFT)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs need a dry FP64 model with the FFT solver");
   return MGPU_OK;
@@ -626,8 +666,10 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   if (cfl && h->cfl.update_dtm) h->sc.dtm = h->cfl.dtm_new;  // monc.F90:313
   const bool cfl_gather = cfl && cfl_evaluation_step(h, h->timestep);
   h->sc.forward = (h->timestep == 1) ? 1 : 0;  // steppingdirection.F90:44-48
+  forcing_flags(h);
   auto mark = [&](int q) { if (h->profiling) cudaEventRecord(h->ev[q], h->stream); };
   mark(0);
+  h->launches += subsidence_tendencies(h);
   if (h->cfg.reproducible) h->launches += exact::launch_fused_subgrid<T>(h->sc, d, h->stream);
   else h->launches += fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
   if (cfl_gather) {
@@ -651,6 +693,9 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   h->sc.bmean = nullptr;
   mark(2);
   swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
+  // mean_profiles (solver group): the stepped zu, zv and the new theta, q before the pressure step
+  if (needs_mean_profiles(h->cfg))
+    h->launches += launch_mean_profiles<T>(h->sc, d.zu_n, d.zv_n, d.th, d.q, h->olz_d, h->stream);
   if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
   else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
   h->launches += 1;
@@ -727,12 +772,17 @@ static int adjoint_step(mgpu_handle* h) {
   AdWork* a = h->ad;
   DevState<double>& d = h->d64;
   h->sc.forward = (h->timestep == 1) ? 1 : 0;
-  // recompute the step's intermediates: post-subgrid state, vis, diff, zu_n..zth_n, p
+  // recompute the step's intermediates.  The hand-written passes read only the step's input state
+  // (with lower_bc's th(1) or zth(1)) and vis, diff: the pressure step and source are linear and
+  // read no values, so the subgrid pass is all there is to recompute.  The tape re-evaluates every
+  // pass on its values: post-subgrid state, vis, diff, zu_n..zth_n and p.
   launch_subgrid(h, d);
-  h->launches += 3 + launch_dynamics(h, d);
-  launch_pressure_source(h, d);
-  int rc = pressure_solve<double>(h, d.p);
-  if (rc) return rc;
+  if (h->cfg.adjoint_taped) {
+    h->launches += 3 + launch_dynamics(h, d);
+    launch_pressure_source(h, d);
+    int rc = pressure_solve<double>(h, d.p);
+    if (rc) return rc;
+  }
   double* const* B = a->adj[a->cur];
   double* const* A = a->adj[1 - a->cur];
   const size_t bytes = field_elems(h) * sizeof(double);
@@ -802,9 +852,11 @@ static int adjoint_run(mgpu_handle* h, int nsteps, int interval, double* rmlmax_
     state_ptrs(d, X);
     copy_state(h, X, &a->ckpt[8 * c]);
     h->timestep = t0 + s0;
+    // the input states of steps s0 .. s1-1; the last step's own result is not needed
     for (int st = s0; st < s1; ++st) {
       state_ptrs(d, X);
       copy_state(h, &a->seg[8 * (st - s0)], X);
+      if (st == s1 - 1) break;
       int rc = step_once<double>(h, d);
       if (rc) return rc;
     }
@@ -835,10 +887,19 @@ static int adjoint_run(mgpu_handle* h, int nsteps, int interval, double* rmlmax_
 template <typename T>
 static int component(mgpu_handle* h, DevState<T>& d, int cid) {
   h->sc.forward = (h->timestep == 1) ? 1 : 0;
+  forcing_flags(h);
   int rc = alloc_component_fields<T>(h, d);
   if (rc) return rc;
   switch (cid) {
     case MGPU_C_STEPPING_DIRECTION: return MGPU_OK;
+    case MGPU_C_MEAN_PROFILES:
+      h->launches += launch_mean_profiles<T>(h->sc, d.zu, d.zv, d.zth, d.zq, h->olz_d, h->stream);
+      break;
+    case MGPU_C_FORCING:
+      h->launches += subsidence_tendencies(h);
+      rc = exact::launch_component<T>(cid, h->sc, d, h->stream, h->divmax_d, &h->launches);
+      if (rc) return fail(h, rc, "component failed");
+      break;
     case MGPU_C_HALO_SWAPPER: return MGPU_OK;  // periodic indexing in every kernel replaces the swap
     case MGPU_C_FFTSOLVER:
       if (h->cfg.solver != MGPU_SOLVER_FFT) return fail(h, MGPU_ERR_UNSUPPORTED, "model not configured for the FFT solver");
@@ -935,6 +996,17 @@ int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out) {
   out->cvel_z = h->cfl.cvel_z;
   out->cfl_evaluations = h->cfl.evaluations;
   out->last_cfl_timestep = h->cfl.last_cfl_timestep;
+  return MGPU_OK;
+}
+
+int mgpu_mean_profiles(mgpu_handle* h, double* out) {
+  if (!h || !out) return MGPU_ERR_ARGUMENT;
+  const int nz = h->cfg.nz, rows = 3 + h->cfg.number_q_fields;
+  std::vector<double> buf((size_t)rows * (nz + 2));
+  CK(cudaMemcpyAsync(buf.data(), h->olz_d, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int r = 0; r < rows; ++r)
+    for (int k = 1; k <= nz; ++k) out[(size_t)r * nz + k - 1] = buf[(size_t)r * (nz + 2) + k];
   return MGPU_OK;
 }
 
@@ -1074,6 +1146,9 @@ int mgpu_slab_init(mgpu_handle* h, int32_t ny_global, int32_t halo, int32_t max_
   if (h->cfg.solver != MGPU_SOLVER_EXTERNAL)
     return fail(h, MGPU_ERR_UNSUPPORTED, "a slab model is created with solver MGPU_SOLVER_EXTERNAL");
   if (h->slab.b1) return fail(h, MGPU_ERR_ARGUMENT, "slab already initialised");
+  if (h->cfg.damping_enabled || h->cfg.l_subs_pl_theta || h->cfg.l_subs_pl_q)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "damping and subsidence on y-slabs are not supported (the mean profiles "
+                                         "would need a reduction across the slabs)");
   const int nyl = h->cfg.ny - 2 * halo, nxh = h->cfg.nx / 2 + 1;
   auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
   if (halo < 1 || nyl < 2 || nyl < halo || (nyl % 2) || !pow2(h->cfg.nx) || !pow2(ny_global) || nyl > ny_global ||

@@ -93,6 +93,14 @@ template <typename T>
 int launch_cfl_gather(const Scalars& s, const DevState<T>& d, bool with_vis, double* part, double* out,
                       cudaStream_t st);
 
+// mean profiles (olzubar, olzvbar, olzthbar, olzqbar) of zu, zv, th and q into olz (rows of nz+2),
+// and the mean-profile subsidence tendencies (forcing.cu)
+template <typename T>
+int launch_mean_profiles(const Scalars& s, const T* zu, const T* zv, const T* th, const T* const* q, double* olz,
+                         cudaStream_t st);
+int launch_subsidence_tendencies(const Scalars& s, const double* olz, double* tend, bool flow_theta, bool q,
+                                 cudaStream_t st);
+
 // BiCGStab pressure solve (iterativesolver)
 struct IterSolverDev;
 IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status);

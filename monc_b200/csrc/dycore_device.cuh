@@ -399,6 +399,78 @@ __device__ T buoyancy_point(const Scalars& s, const Prof<T>& P, const View<T>& T
 }
 
 // ------------------------------------------------------------------------------------------
+// damping (damping.F90:367-404), levels kdmpmin..nz (w: ..nz-1): Newtonian relaxation of zu, zv
+// towards the mean profiles (in the Galilean frame), of zw towards 0, of scalars towards theirs
+// ------------------------------------------------------------------------------------------
+template <typename T, class PA>
+__device__ __forceinline__ void damping_flow_point(const Scalars& s, const PA& P, int k, T zu, T zv, T zw, T& su,
+                                                   T& sv, T& sw) {
+  if (k < s.kdmpmin) return;
+  const int st = s.nz + 2;
+  su = su - P(P_DMPCO, k) * (zu - (T)(s.olz[k] - s.ugal));
+  sv = sv - P(P_DMPCO, k) * (zv - (T)(s.olz[st + k] - s.vgal));
+  if (k <= s.nz - 1) sw = sw - P(P_DMPCOZ, k) * zw;
+}
+
+// row 2 of s.olz for theta, 3 + n for q(n)
+template <typename T, class PA>
+__device__ __forceinline__ T damping_scalar_point(const Scalars& s, const PA& P, int k, T zf, int row, T sf) {
+  if (k < s.kdmpmin) return sf;
+  return sf - P(P_DMPCO, k) * (zf - (T)s.olz[row * (s.nz + 2) + k]);
+}
+
+// ------------------------------------------------------------------------------------------
+// forcing: subsidence (forcing.F90:1052-1166), levels 2..nz.  With subsidence_local_* the
+// gradients are the column's; otherwise every column gets the mean-profile tendencies in
+// s.subs_tend (k_subsidence_tendencies).
+// ------------------------------------------------------------------------------------------
+template <typename T, class A, class PA>
+__device__ __forceinline__ void subsidence_flow_point(const Scalars& s, const PA& P, const A& ZU, const A& ZV, int k,
+                                                      int j, int i, T& su, T& sv) {
+  if (!s.subs_local_th) {
+    su = su - (T)s.subs_tend[k];
+    sv = sv - (T)s.subs_tend[(s.nz + 2) + k];
+    return;
+  }
+  T usub, vsub;
+  if (k < s.nz) {
+    usub = (T)2.0 * (P(P_WSUBS, k - 1) * P(P_TZC1, k) * (ZU(k, j, i) - ZU(k - 1, j, i)) +
+                     P(P_WSUBS, k) * P(P_TZC2, k) * (ZU(k + 1, j, i) - ZU(k, j, i)));
+    vsub = (T)2.0 * (P(P_WSUBS, k - 1) * P(P_TZC1, k) * (ZV(k, j, i) - ZV(k - 1, j, i)) +
+                     P(P_WSUBS, k) * P(P_TZC2, k) * (ZV(k + 1, j, i) - ZV(k, j, i)));
+  } else {
+    usub = (T)2.0 * (P(P_WSUBS, k - 1) * P(P_TZC1, k) * (ZU(k, j, i) - ZU(k - 1, j, i)));
+    vsub = (T)2.0 * (P(P_WSUBS, k - 1) * P(P_TZC1, k) * (ZV(k, j, i) - ZV(k - 1, j, i)));
+  }
+  su = su - usub;
+  sv = sv - vsub;
+}
+
+template <typename T, class A, class PA>
+__device__ __forceinline__ T subsidence_theta_point(const Scalars& s, const PA& P, const A& ZTH, int k, int j, int i,
+                                                    T sth) {
+  if (!s.subs_local_th) return sth - (T)s.subs_tend[2 * (s.nz + 2) + k];
+  const int ka = k < s.nz ? k + 1 : k, kb = ka - 1;  // the upper and lower level of the difference
+  T thsub;
+  if constexpr (sizeof(T) == 4) {
+    // FP32: (zth + thref) differenced as dzth + dthref; thref (~290 K) would round zth to its
+    // 3e-5 K spacing
+    thsub = P(P_WSUBS, k) * ((ZTH(ka, j, i) - ZTH(kb, j, i)) + P(P_DTHREF, kb)) * P(P_RDZN, ka);
+  } else {
+    thsub = P(P_WSUBS, k) * ((ZTH(ka, j, i) + P(P_THREF, ka)) - (ZTH(kb, j, i) + P(P_THREF, kb))) * P(P_RDZN, ka);
+  }
+  return sth - thsub;
+}
+
+template <typename T, class A, class PA>
+__device__ __forceinline__ T subsidence_q_point(const Scalars& s, const PA& P, const A& ZQ, int n, int k, int j, int i,
+                                                T sq) {
+  if (!s.subs_local_q) return sq - (T)s.subs_tend[(3 + n) * (s.nz + 2) + k];
+  const int ka = k < s.nz ? k + 1 : k, kb = ka - 1;
+  return sq - P(P_WSUBS, k) * (ZQ(ka, j, i) - ZQ(kb, j, i)) * P(P_RDZN, ka);
+}
+
+// ------------------------------------------------------------------------------------------
 // simplecloud saturation adjustment (simplecloud.F90:262-379, saturation.F90 qsaturation and
 // dqwsatdt), one point 2 <= k <= nz.  q_v, q_l, th are the state (forward step) or z-fields;
 // zq_l is always the z-field (the evaporation branch tests scalar_stepping, which is centred).

@@ -216,6 +216,44 @@ __global__ void k_c_buoyancy(Scalars s, DevState<T> d) {
   d.sw[o] = buoyancy_point<T>(s, P, view<T>(d.th, s), Q, k, j, i, d.sw[o]);
 }
 
+// damping (damping.F90:301-409) over the levels kdmpmin..nz of every column
+template <typename T>
+__global__ void k_c_damping(Scalars s, DevState<T> d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z + 1;
+  if (i >= s.nx || j >= s.ny || k > s.nz || k < s.kdmpmin) return;
+  Prof<T> P = prof<T>(s);
+  long long o = lin(s, k, j, i);
+  T su = d.su[o], sv = d.sv[o], sw = d.sw[o];
+  damping_flow_point<T>(s, P, k, d.zu[o], d.zv[o], d.zw[o], su, sv, sw);
+  d.su[o] = su;
+  d.sv[o] = sv;
+  d.sw[o] = sw;
+  if (!s.passive_th) d.sth[o] = damping_scalar_point<T>(s, P, k, d.zth[o], 2, d.sth[o]);
+  for (int n = 0; n < s.nq; ++n) d.sq[n][o] = damping_scalar_point<T>(s, P, k, d.zq[n][o], 3 + n, d.sq[n][o]);
+}
+
+// forcing's subsidence (forcing.F90:1032-1166): u, v and theta, then q, levels 2..nz
+template <typename T>
+__global__ void k_c_forcing(Scalars s, DevState<T> d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z + 1;
+  if (i >= s.nx || j >= s.ny || k > s.nz || k < 2) return;
+  Prof<T> P = prof<T>(s);
+  long long o = lin(s, k, j, i);
+  if (s.subs_th) {
+    T su = d.su[o], sv = d.sv[o];
+    subsidence_flow_point<T>(s, P, view<T>(d.zu, s), view<T>(d.zv, s), k, j, i, su, sv);
+    d.su[o] = su;
+    d.sv[o] = sv;
+    d.sth[o] = subsidence_theta_point<T>(s, P, view<T>(d.zth, s), k, j, i, d.sth[o]);
+  }
+  if (s.subs_q)
+    for (int n = 0; n < s.nq; ++n) d.sq[n][o] = subsidence_q_point<T>(s, P, view<T>(d.zq[n], s), n, k, j, i, d.sq[n][o]);
+}
+
 template <typename T>
 __global__ void k_c_set_consistent_lowbc(Scalars s, DevState<T> d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -473,12 +511,19 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
       for (int n = 0; n < s.nq; ++n) Q[n] = view<T>(d.q[n], s);
       sw = buoyancy_point<T>(s, P, view<T>(d.th, s), Q, k, j, i, sw);
     }
-    // tvd_advection then diffusion of theta and q
+    // damping, then forcing's subsidence (both from timestep 3, so the z-fields are zu, zv, zw)
+    if (s.damping) damping_flow_point<T>(s, P, k, d.zu[o], d.zv[o], d.zw[o], su, sv, sw);
+    if (s.subs_th) subsidence_flow_point<T>(s, P, view<T>(d.zu, s), view<T>(d.zv, s), k, j, i, su, sv);
+    // tvd_advection then diffusion of theta and q, then their damping and subsidence
     sth = tvd_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.th : d.zth, s), k, j, i, (T)0.0);
     if (s.use_vd) sth = sth + diffusion_point<T, View<T>>(s, P, view<T>(d.zth, s), view<T>(d.diff, s), k, j, i);
+    if (s.damping && !s.passive_th) sth = damping_scalar_point<T>(s, P, k, d.zth[o], 2, sth);
+    if (s.subs_th) sth = subsidence_theta_point<T>(s, P, view<T>(d.zth, s), k, j, i, sth);
     for (int n = 0; n < s.nq; ++n) {
       sq[n] = tvd_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.q[n] : d.zq[n], s), k, j, i, (T)0.0);
       if (s.use_vd) sq[n] = sq[n] + diffusion_point<T, View<T>>(s, P, view<T>(d.zq[n], s), view<T>(d.diff, s), k, j, i);
+      if (s.damping) sq[n] = damping_scalar_point<T>(s, P, k, d.zq[n][o], 3 + n, sq[n]);
+      if (s.subs_q) sq[n] = subsidence_q_point<T>(s, P, view<T>(d.zq[n], s), n, k, j, i, sq[n]);
     }
     if (s.simplecloud) {
       const int iv = s.iqv, il = s.iql;
@@ -733,6 +778,8 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
           sw = sw + g2 * (T)s.cq[n] * (__ldg(d.q[n] + o) + __ldg(d.q[n] + o + plane));
       }
     }
+    if (s.damping) damping_flow_point<T>(s, P, k, ZU(k, j, i), ZV(k, j, i), ZW(k, j, i), su, sv, sw);
+    if (s.subs_th) subsidence_flow_point<T>(s, P, ZU, ZV, k, j, i, su, sv);
     d.zu_n[o] = (T)s.ugal + ZU(k, j, i) + dtm_x2 * su;
     d.zv_n[o] = (T)s.vgal + ZV(k, j, i) + dtm_x2 * sv;
     d.zw_n[o] = (T)0.0 + ZW(k, j, i) + dtm_x2 * sw;
@@ -753,6 +800,7 @@ struct ScalarJob {
   T* out_zf;
   T* src;
   int clip;
+  int row;  // the field's row in the mean profiles: 2 for theta, 3 + n for q(n)
 };
 
 template <typename T>
@@ -849,6 +897,11 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     T sth = tvd_source<T>(s, P, U, V, W, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1], FY[ty * TX + tx],
                           FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
     if (s.use_vd) sth = sth + diffusion_point<T>(s, P, ZF, DIFF, k, j, i);
+    // damping, then forcing's subsidence (the dynamics group's order)
+    if (s.damping && (job.row > 2 || !s.passive_th)) sth = damping_scalar_point<T>(s, P, k, ZF(k, j, i), job.row, sth);
+    if (job.row == 2 ? s.subs_th : s.subs_q)
+      sth = job.row == 2 ? subsidence_theta_point<T>(s, P, ZF, k, j, i, sth)
+                         : subsidence_q_point<T>(s, P, ZF, job.row - 3, k, j, i, sth);
     fz_lo = fz_hi;
     if (job.src) {
       job.src[o] = sth;
@@ -1069,6 +1122,8 @@ int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st,
     case MGPU_C_CORIOLIS: k_c_coriolis<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
     case MGPU_C_BUOYANCY: k_c_buoyancy<T><<<pt_grid(s, s.nz - 2), b, 0, st>>>(s, d); break;
     case MGPU_C_SET_CONSISTENT_LOWBC: k_c_set_consistent_lowbc<T><<<gcol, b, 0, st>>>(s, d); break;
+    case MGPU_C_DAMPING: if (s.damping) k_c_damping<T><<<pt_grid(s, s.nz), b, 0, st>>>(s, d); break;
+    case MGPU_C_FORCING: if (s.subs_th || s.subs_q) k_c_forcing<T><<<pt_grid(s, s.nz), b, 0, st>>>(s, d); break;
     case MGPU_C_SIMPLECLOUD:
       if (!s.simplecloud) return MGPU_ERR_UNSUPPORTED;
       k_c_simplecloud<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d);
@@ -1174,12 +1229,12 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
   dim3 grid_s(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_s - 1) / kc_s);
   dim3 grid_m(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_m - 1) / kc_m);
   if (!moist) {
-    k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, d.th_n, d.zth_n, nullptr, 0});
+    k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, d.th_n, d.zth_n, nullptr, 0, 2});
   } else {
     // one launch per scalar writing its source, then saturation adjustment and stepping
-    k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, nullptr, nullptr, d.sth, 0});
+    k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, nullptr, nullptr, d.sth, 0, 2});
     for (int n = 0; n < s.nq; ++n)
-      k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.q[n], d.zq[n], nullptr, nullptr, d.sq[n], 1});
+      k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.q[n], d.zq[n], nullptr, nullptr, d.sq[n], 1, 3 + n});
     k_f_cloud_step<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
   }
   if (mid) cudaEventRecord(mid, st);

@@ -67,6 +67,17 @@ extern "C" void mgpu_config_defaults(mgpu_config* c) {
   c->l_constant_dtm = 0;
   c->advection_flow_fields = MGPU_ADVECT_PW;
   c->adjoint_taped = 0;
+  c->damping_enabled = 0;
+  c->dmptim = 0.0;
+  c->zdmp = 0.0;
+  c->hdmp = 0.0;
+  c->l_subs_pl_theta = 0;
+  c->l_subs_pl_q = 0;
+  c->subsidence_input_type = MGPU_SUBS_VELOCITY;
+  c->subsidence_local_theta = 1;
+  c->subsidence_local_q = 1;
+  c->n_subs_pl = 0;
+  for (int q = 0; q < MGPU_MAX_SUBS_NODES; ++q) c->z_subs_pl[q] = c->f_subs_pl[q] = 0.0;
 }
 
 // w-level heights: piecewise-linear kgd/hgd grid smoothed nsmth times
@@ -117,6 +128,8 @@ static double qsaturation(double temperature, double pressure) {
   const double tk0c = 273.15, qsa1 = 3.8, qsa2 = -17.2693882, qsa3 = 35.86, qsa4 = 6.109;
   return qsa1 / (pressure * std::exp(qsa2 * (temperature - tk0c) / (temperature - qsa3)) - qsa4);
 }
+
+static void damping_and_subsidence(const mgpu_config& c, RefState& rs);
 
 void build_reference_state(const mgpu_config& c, RefState& rs) {
   const int n = c.nz;
@@ -275,6 +288,52 @@ void build_reference_state(const mgpu_config& c, RefState& rs) {
       rs.cfc = rs.lookup_ustr[1] * std::pow(vel[1], c.convective_limit);
     }
   }
+  damping_and_subsidence(c, rs);
+}
+
+// piecewise_linear_1d (interpolation.F90:15-58): linear between the nodes, the first node's value
+// below it, the last node's value at exactly its height.  MONC leaves the levels above the last
+// node unset; here they stay 0.
+static void piecewise_linear_1d(const double* zvals, const double* vals, int nnodes, const std::vector<double>& zgrid,
+                                int n, std::vector<double>& field) {
+  std::vector<double> init(nnodes + 2), zng(nnodes + 2);
+  const double verylow = -1.0e5;
+  init[1] = vals[0];
+  zng[1] = verylow;
+  for (int nn = 2; nn <= nnodes + 1; ++nn) {
+    init[nn] = vals[nn - 2];
+    zng[nn] = zvals[nn - 2];
+  }
+  for (int nn = 1; nn <= nnodes; ++nn)
+    for (int k = 1; k <= n; ++k)
+      if (zng[nn] <= zgrid[k] && zgrid[k] < zng[nn + 1])
+        field[k] = init[nn] + (init[nn + 1] - init[nn]) * (zgrid[k] - zng[nn]) / (zng[nn + 1] - zng[nn]);
+  if (zgrid[n] == zng[nnodes + 1]) field[n] = init[nnodes + 1];
+}
+
+// damping coefficients (damping.F90:124-148) and the subsidence velocity (forcing.F90:568-582)
+static void damping_and_subsidence(const mgpu_config& c, RefState& rs) {
+  const int n = c.nz;
+  rs.dmpco.assign(n + 2, 0.0);
+  rs.dmpcoz.assign(n + 2, 0.0);
+  rs.w_subs.assign(n + 2, 0.0);
+  rs.kdmpmin = n + 1;  // no level damped
+  if (c.damping_enabled) {
+    if (!(c.hdmp > 0.0)) throw std::runtime_error("damping needs hdmp > 0");
+    for (int k = n; k >= 1; --k) {
+      rs.kdmpmin = k;
+      if (rs.zn[k] >= c.zdmp) rs.dmpco[k] = c.dmptim * (std::exp((rs.zn[k] - c.zdmp) / c.hdmp) - 1.0);
+      if (rs.z[k] >= c.zdmp) rs.dmpcoz[k] = c.dmptim * (std::exp((rs.z[k] - c.zdmp) / c.hdmp) - 1.0);
+      if (rs.zn[k] < c.zdmp) break;
+    }
+  }
+  if (c.l_subs_pl_theta || c.l_subs_pl_q) {
+    if (c.n_subs_pl < 1 || c.n_subs_pl > MGPU_MAX_SUBS_NODES)
+      throw std::runtime_error("subsidence needs 1..MGPU_MAX_SUBS_NODES nodes in z_subs_pl / f_subs_pl");
+    piecewise_linear_1d(c.z_subs_pl, c.f_subs_pl, c.n_subs_pl, rs.z, n, rs.w_subs);
+    if (c.subsidence_input_type == MGPU_SUBS_DIVERGENCE)
+      for (int k = 1; k <= n; ++k) rs.w_subs[k] = -1.0 * rs.w_subs[k] * rs.z[k];
+  }
 }
 
 const std::vector<double>* profile_by_name(const RefState& rs, const std::string& nm) {
@@ -286,7 +345,8 @@ const std::vector<double>* profile_by_name(const RefState& rs, const std::string
                        {"tzd2", &rs.tzd2}, {"rneutml", &rs.rneutml}, {"rneutml_sq", &rs.rneutml_sq},
                        {"buoy_co", &rs.buoy_co}, {"prefn", &rs.prefn}, {"prefrcp", &rs.prefrcp},
                        {"rprefrcp", &rs.rprefrcp}, {"tref", &rs.tref}, {"qsat", &rs.qsat},
-                       {"dqsatdt", &rs.dqsatdt}, {"qsatfac", &rs.qsatfac}};
+                       {"dqsatdt", &rs.dqsatdt}, {"qsatfac", &rs.qsatfac}, {"dmpco", &rs.dmpco},
+                       {"dmpcoz", &rs.dmpcoz}, {"w_subs", &rs.w_subs}};
   for (const Entry& e : tab)
     if (nm == e.name) return e.v;
   return nullptr;

@@ -29,6 +29,9 @@ struct RefState {
   int lookup_entries = 80;
   std::vector<double> cq;
   int k_cloudmax = 0;  // simplecloud: highest level of saturation adjustment
+  // damping (damping.F90:124-148) and subsidence (forcing.F90:568-582)
+  std::vector<double> dmpco, dmpcoz, w_subs;
+  int kdmpmin = 0;
 };
 
 // Builds the reference state from a configuration (restates gridmanager.F90:2008-2642,
@@ -40,7 +43,7 @@ const std::vector<double>* profile_by_name(const RefState& rs, const std::string
 enum ProfileId {
   P_RDZ = 0, P_RDZN, P_DZN, P_RHO, P_RHON, P_DTHREF, P_CZB, P_CZA, P_CZG, P_CZH, P_TZC1, P_TZC2, P_TZD1, P_TZD2,
   P_RNEUTML_SQ, P_BUOY_CO, P_THREF, P_PREFRCP, P_RPREFRCP, P_TREF, P_TSTARPR, P_QSAT, P_DQSATDT, P_QSATFAC,
-  P_GWX, P_GWY, P_PREFN, P_TOFF, P_TC0, P_DZ, P_COUNT
+  P_GWX, P_GWY, P_PREFN, P_TOFF, P_TC0, P_DZ, P_DMPCO, P_DMPCOZ, P_WSUBS, P_COUNT
 };
 
 // Scalars every dynamical-core kernel reads (passed by value as a kernel parameter).
@@ -69,6 +72,13 @@ struct Scalars {
   const double* bmean;     // FP32-mixed fused step: horizontal means of th (row 0) and q(n) (row 1+n) per
                            // level, (nz+2) per row, removed from the buoyancy; null elsewhere
   const double* lookup;    // device: lookup_ustr, 1-based
+  // damping and subsidence (damping.F90, forcing.F90); the flags are set per step (MONC applies
+  // both from timestep 3)
+  int damping, kdmpmin;
+  int subs_th, subs_q;             // subsidence of u, v and theta / of the q fields this step
+  int subs_local_th, subs_local_q; // 1: gradients of the column; 0: the tendencies in subs_tend
+  const double* olz;       // device: olzubar, olzvbar, olzthbar, olzqbar(n) rows, (nz+2) each
+  const double* subs_tend; // device: mean-profile subsidence tendencies usub, vsub, thsub, qsub(n) rows
 };
 
 }  // namespace mgpu

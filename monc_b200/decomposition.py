@@ -237,6 +237,9 @@ class SlabDomain:
         if cfg.cfl_enabled:
             raise ValueError("cfltest on a decomposed domain needs its extrema reduced across the slabs; "
                              "run the slabs at a fixed dtm (cfl_enabled = 0)")
+        if cfg.damping_enabled or cfg.l_subs_pl_theta or cfg.l_subs_pl_q:
+            raise ValueError("damping and subsidence on a decomposed domain need the mean profiles reduced "
+                             "across the slabs; not supported")
         self.cfg = cfg
         self.comm = comm
         self.geo = SlabGeometry(cfg.nx, cfg.ny, cfg.nz, comm.size, halo)

@@ -106,6 +106,11 @@ struct Model {
   double local_zumin = 0.0, local_zumax = 0.0, local_zvmin = 0.0, local_zvmax = 0.0, local_cvel_z = 0.0;
   std::vector<double> abswmax;  // 1-based k
   int cfl_error = 0;
+  // damping (damping.F90:19-21, grids.F90 dmpco/dmpcoz/kdmpmin), subsidence velocity (forcing.F90)
+  // and the mean profiles they read (meanprofiles.F90, grids.F90 olz*bar)
+  Prof dmpco, dmpcoz, w_subs, olzubar, olzvbar, olzthbar;
+  std::vector<Prof> olzqbar;
+  int kdmpmin = 0;
 };
 
 static inline double& PT(Model& m, int k, int j, int i) {
@@ -1529,6 +1534,133 @@ static void swap_smooth_column(Model& m) {
 // ---------------------------------------------------------------------------------------------
 typedef void (*ColumnFn)(Model&);
 
+// ---------------------------------------------------------------------------------------------
+// damping (damping.F90:124-148 init, :301-409 timestep), mean_profiles (meanprofiles.F90:95-216,
+// no immersed boundary), forcing's subsidence (forcing.F90:568-582 init, :918-1166 timestep)
+// ---------------------------------------------------------------------------------------------
+// interpolation.F90:15-58; the levels above the last node are left at 0 (MONC leaves them unset)
+static void piecewise_linear_1d(const double* zvals, const double* vals, int nnodes, const Prof& zgrid, int nlev,
+                                Prof& field) {
+  std::vector<double> initgd(nnodes + 2), zngd(nnodes + 2);
+  double verylow = -1.0e5;
+  initgd[1] = vals[0];
+  zngd[1] = verylow;
+  for (int nn = 2; nn <= nnodes + 1; ++nn) {
+    initgd[nn] = vals[nn - 2];
+    zngd[nn] = zvals[nn - 2];
+  }
+  for (int nn = 1; nn <= nnodes; ++nn)
+    for (int k = 1; k <= nlev; ++k)
+      if (zngd[nn] <= zgrid(k) && zgrid(k) < zngd[nn + 1])
+        field(k) = initgd[nn] + (initgd[nn + 1] - initgd[nn]) * (zgrid(k) - zngd[nn]) / (zngd[nn + 1] - zngd[nn]);
+  if (zgrid(nlev) == zngd[nnodes + 1]) field(nlev) = initgd[nnodes + 1];
+}
+
+static void damping_and_forcing_init(Model& m) {
+  const mgpu_config& c = m.cfg;
+  const int nz = m.nz;
+  m.dmpco.alloc(nz); m.dmpcoz.alloc(nz); m.w_subs.alloc(nz);
+  m.olzubar.alloc(nz); m.olzvbar.alloc(nz); m.olzthbar.alloc(nz);
+  m.olzqbar.assign(c.number_q_fields, Prof());
+  for (Prof& p : m.olzqbar) p.alloc(nz);
+  m.kdmpmin = nz + 1;
+  if (c.damping_enabled) {
+    for (int k = nz; k >= 1; --k) {
+      m.kdmpmin = k;
+      if (m.zn(k) >= c.zdmp) m.dmpco(k) = c.dmptim * (std::exp((m.zn(k) - c.zdmp) / c.hdmp) - 1.0);
+      if (m.z(k) >= c.zdmp) m.dmpcoz(k) = c.dmptim * (std::exp((m.z(k) - c.zdmp) / c.hdmp) - 1.0);
+      if (m.zn(k) < c.zdmp) break;
+    }
+  }
+  if (c.l_subs_pl_theta || c.l_subs_pl_q) {
+    piecewise_linear_1d(c.z_subs_pl, c.f_subs_pl, c.n_subs_pl, m.z, nz, m.w_subs);
+    if (c.subsidence_input_type == MGPU_SUBS_DIVERGENCE)
+      for (int k = 1; k <= nz; ++k) m.w_subs(k) = -1.0 * m.w_subs(k) * m.z(k);
+  }
+}
+
+static bool mean_profiles_enabled(const Model& m) {
+  const mgpu_config& c = m.cfg;
+  return c.damping_enabled || c.l_subs_pl_theta || c.l_subs_pl_q;
+}
+
+// calculate_mean_profiles: sums of zu, zv, zth, zq over the interior of each level (one rank)
+// times rnhpts = 1 / real(nx ny), real() at default (single) precision
+static void mean_profiles(Model& m) {
+  const double rnhpts = 1.0 / (double)(float)((long long)m.nx * m.ny);
+  auto mean = [&](const Field& f, Prof& out) {
+    for (int k = 1; k <= m.nz; ++k) {
+      double sum = 0.0;
+      for (int x = m.xs; x <= m.xe; ++x)
+        for (int y = m.ys; y <= m.ye; ++y) sum += f(k, y, x);
+      out(k) = sum * rnhpts;
+    }
+  };
+  mean(m.zu, m.olzubar);
+  mean(m.zv, m.olzvbar);
+  mean(m.zth, m.olzthbar);
+  for (int n = 0; n < m.cfg.number_q_fields; ++n) mean(m.zq[n], m.olzqbar[n]);
+}
+
+static void damping_column(Model& m) {
+  if (!m.cfg.damping_enabled) return;
+  if (m.halo_column || m.timestep < 3) return;
+  const int y = m.col_y, x = m.col_x;
+  for (int k = m.kdmpmin; k <= m.nz; ++k) {
+    m.su(k, y, x) = m.su(k, y, x) - m.dmpco(k) * (m.zu(k, y, x) - (m.olzubar(k) - m.ugal));
+    m.sv(k, y, x) = m.sv(k, y, x) - m.dmpco(k) * (m.zv(k, y, x) - (m.olzvbar(k) - m.vgal));
+    if (!m.cfg.passive_th) m.sth(k, y, x) = m.sth(k, y, x) - m.dmpco(k) * (m.zth(k, y, x) - m.olzthbar(k));
+    for (int n = 0; n < m.cfg.number_q_fields; ++n)
+      m.sq[n](k, y, x) = m.sq[n](k, y, x) - m.dmpco(k) * (m.zq[n](k, y, x) - m.olzqbar[n](k));
+  }
+  for (int k = m.kdmpmin; k <= m.nz - 1; ++k) m.sw(k, y, x) = m.sw(k, y, x) - m.dmpcoz(k) * m.zw(k, y, x);
+}
+
+static void forcing_column(Model& m) {
+  const mgpu_config& c = m.cfg;
+  if (!(c.l_subs_pl_theta || c.l_subs_pl_q)) return;
+  if (m.halo_column || m.timestep < 3) return;
+  const int y = m.col_y, x = m.col_x, nz = m.nz;
+  std::vector<double> prof(nz + 2);
+  if (c.l_subs_pl_theta) {
+    // apply_subsidence_to_flow_fields
+    for (int f = 0; f < 2; ++f) {
+      const Field& zf = f == 0 ? m.zu : m.zv;
+      const Prof& bar = f == 0 ? m.olzubar : m.olzvbar;
+      Field& sf = f == 0 ? m.su : m.sv;
+      for (int k = 1; k <= nz; ++k) prof[k] = c.subsidence_local_theta ? zf(k, y, x) : bar(k);
+      for (int k = 2; k <= nz - 1; ++k) {
+        double sub = 2.0 * (m.w_subs(k - 1) * m.tzc1(k) * (prof[k] - prof[k - 1]) +
+                            m.w_subs(k) * m.tzc2(k) * (prof[k + 1] - prof[k]));
+        sf(k, y, x) = sf(k, y, x) - sub;
+      }
+      int k = nz;
+      double sub = 2.0 * (m.w_subs(k - 1) * m.tzc1(k) * (prof[k] - prof[k - 1]));
+      sf(k, y, x) = sf(k, y, x) - sub;
+    }
+    // apply_subsidence_to_theta
+    for (int k = 1; k <= nz; ++k) prof[k] = (c.subsidence_local_theta ? m.zth(k, y, x) : m.olzthbar(k)) + m.thref(k);
+    for (int k = 2; k <= nz - 1; ++k) {
+      double thsub = m.w_subs(k) * (prof[k + 1] - prof[k]) * m.rdzn(k + 1);
+      m.sth(k, y, x) = m.sth(k, y, x) - thsub;
+    }
+    int k = nz;
+    double thsub = m.w_subs(k) * (prof[k] - prof[k - 1]) * m.rdzn(k);
+    m.sth(k, y, x) = m.sth(k, y, x) - thsub;
+  }
+  if (c.l_subs_pl_q)
+    for (int n = 0; n < c.number_q_fields; ++n) {
+      for (int k = 1; k <= nz; ++k) prof[k] = c.subsidence_local_q ? m.zq[n](k, y, x) : m.olzqbar[n](k);
+      for (int k = 2; k <= nz - 1; ++k) {
+        double qsub = m.w_subs(k) * (prof[k + 1] - prof[k]) * m.rdzn(k + 1);
+        m.sq[n](k, y, x) = m.sq[n](k, y, x) - qsub;
+      }
+      int k = nz;
+      double qsub = m.w_subs(k) * (prof[k] - prof[k - 1]) * m.rdzn(k);
+      m.sq[n](k, y, x) = m.sq[n](k, y, x) - qsub;
+    }
+}
+
 static void column_group(Model& m, const std::vector<ColumnFn>& fns) {
   for (int x = 1; x <= m.nxh; ++x)
     for (int y = 1; y <= m.nyh; ++y) {
@@ -1605,12 +1737,14 @@ static void timestep(Model& m) {
     for (int c = 0; c < 3; ++c) interpolate_flow(m, c);
   if (m.cfg.simplecloud_enabled)
     column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
-                     buoyancy_column, set_consistent_lowbc_column, simplecloud_column, diverr_column, psrce_column,
-                     stepfields_column});
+                     buoyancy_column, damping_column, forcing_column, set_consistent_lowbc_column,
+                     simplecloud_column, diverr_column, psrce_column, stepfields_column});
   else
     column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
-                     buoyancy_column, set_consistent_lowbc_column, diverr_column, psrce_column, stepfields_column});
-  // solver
+                     buoyancy_column, damping_column, forcing_column, set_consistent_lowbc_column, diverr_column,
+                     psrce_column, stepfields_column});
+  // solver: mean_profiles, then the pressure solve
+  if (mean_profiles_enabled(m)) mean_profiles(m);
   if (m.cfg.solver == MGPU_SOLVER_FFT) fftsolver(m);
   else iterative_solver(m);
   if (m.cfg.cfl_enabled) cfltest(m);
@@ -1642,7 +1776,9 @@ Prof* profile_by_name(Model& m, const std::string& n) {
       {"cza", &m.cza}, {"czg", &m.czg}, {"czh", &m.czh}, {"tzc1", &m.tzc1}, {"tzc2", &m.tzc2}, {"tzd1", &m.tzd1},
       {"tzd2", &m.tzd2}, {"rneutml", &m.rneutml}, {"rneutml_sq", &m.rneutml_sq}, {"buoy_co", &m.buoy_co},
       {"prefn", &m.prefn}, {"prefrcp", &m.prefrcp}, {"rprefrcp", &m.rprefrcp}, {"tref", &m.tref},
-      {"qsat", &m.qsat}, {"dqsatdt", &m.dqsatdt}, {"qsatfac", &m.qsatfac}};
+      {"qsat", &m.qsat}, {"dqsatdt", &m.dqsatdt}, {"qsatfac", &m.qsatfac}, {"dmpco", &m.dmpco},
+      {"dmpcoz", &m.dmpcoz}, {"w_subs", &m.w_subs}, {"olzubar", &m.olzubar}, {"olzvbar", &m.olzvbar},
+      {"olzthbar", &m.olzthbar}};
   for (auto& t : tab)
     if (n == t.name) return t.p;
   return nullptr;
@@ -1719,6 +1855,7 @@ static Model* create(const mgpu_config* cfg) {
     if (!cfg->passive_q && nq > 0) m.fbuoy = m.fbuoy + m.cq[m.iqv] * m.surface_vapour_flux * m.G;
     set_look(m);
   }
+  damping_and_forcing_init(m);
   if (cfg->solver == MGPU_SOLVER_FFT) fft_init(m);
   else init_iterative(m);
   return mp;
@@ -2055,6 +2192,9 @@ int orc_component(void* h, int cid) {
       case MGPU_C_ITERATIVESOLVER: if (m.A_u.empty()) return -5; iterative_solver_solve(m); break;
       case MGPU_C_PSTEP: column_group(m, {pstep_column}); break;
       case MGPU_C_SWAP_SMOOTH: column_group(m, {swap_smooth_column}); break;
+      case MGPU_C_MEAN_PROFILES: mean_profiles(m); break;
+      case MGPU_C_DAMPING: column_group(m, {damping_column}); break;
+      case MGPU_C_FORCING: column_group(m, {forcing_column}); break;
       default: return -5;
     }
   } catch (std::exception& e) {
@@ -2080,5 +2220,13 @@ int orc_fft_c2c(int n, double* c, int sign) {
 }
 
 double orc_lookup_ustr(void* h, double vel) { return look(*(Model*)h, vel); }
+
+// olzqbar(:, n) of the mean profiles, levels 1..nz
+int orc_mean_q_profile(void* h, int n, double* out) {
+  Model& m = *(Model*)h;
+  if (n < 0 || n >= (int)m.olzqbar.size()) return -1;
+  for (int k = 1; k <= m.nz; ++k) out[k - 1] = m.olzqbar[n](k);
+  return 0;
+}
 
 }  // extern "C"

@@ -52,6 +52,8 @@ def lib():
         L.orc_fft_c2c.argtypes = [C.c_int, C.c_void_p, C.c_int]
         L.orc_lookup_ustr.restype = C.c_double
         L.orc_lookup_ustr.argtypes = [C.c_void_p, C.c_double]
+        L.orc_mean_q_profile.restype = C.c_int
+        L.orc_mean_q_profile.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_cfl_state.restype = C.c_int
         L.orc_cfl_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -102,6 +104,16 @@ class Oracle:
         if lib().orc_get_field_monc(self.h, fid, a.ctypes.data) != 0:
             raise KeyError(fid)
         return a
+
+    def mean_profiles(self) -> dict:
+        """olzubar, olzvbar, olzthbar and olzqbar(n) as the last mean_profiles left them."""
+        out = {n: self.profile(n) for n in ("olzubar", "olzvbar", "olzthbar")}
+        for n in range(self.cfg.number_q_fields):
+            a = np.empty(self.nz, dtype=np.float64)
+            if lib().orc_mean_q_profile(self.h, n, a.ctypes.data) != 0:
+                raise RuntimeError("orc_mean_q_profile")
+            out[f"olzqbar{n}"] = a
+        return out
 
     def profile(self, name: str) -> np.ndarray:
         a = np.empty(self.nz, dtype=np.float64)
