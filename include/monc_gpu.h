@@ -253,6 +253,33 @@ int64_t mgpu_launch_count(mgpu_handle* h);
  * either pointer may be NULL.  Reads back 8*nz bytes per non-NULL pointer. */
 int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2);
 
+/* ---- Checkpoint files (checkpointer: writecheckpoint.F90:42-100, readcheckpoint.F90) ----------
+ * MONC's checkpoint layout (checkpointcommon.F90:11-81 names: options_database, x/y_resolution,
+ * z, zn, thref, olz*bar, q, zq, u_nogal, v_nogal, w, th, p, zu, zv, zw, zth, timestep, time, dtm,
+ * dtm_new, ...) in NetCDF classic format with 64-bit offsets, the format a serial MONC writes and
+ * nf90_open reads.  Fields are stored z fastest as MONC stores them. */
+typedef struct mgpu_checkpoint_meta {
+  int32_t timestep;            /* the last completed step (MONC's current_state%timestep) */
+  int32_t last_cfl_timestep;
+  double  time;                /* model time after that step */
+  double  dtm, dtm_new, absolute_new_dtm, ugal, vgal;
+} mgpu_checkpoint_meta;
+
+/* Write / read a checkpoint of the model's state (all fields, the mean profiles when damping or
+ * subsidence is on, the step count, time and dtm state).  Reading restarts the model at the step
+ * after the checkpointed one; the file's x, y, zn sizes and q fields must match the model's. */
+int mgpu_checkpoint_write(mgpu_handle* h, const char* path);
+int mgpu_checkpoint_read(mgpu_handle* h, const char* path);
+
+/* The same without a GPU, on host arrays: fields[0..8] = u v w th zu zv zw zth p, then q(n) and
+ * zq(n) for n < number_q_fields, each [nz][ny][nx] x fastest; mean = (3 + number_q_fields) rows of
+ * nz (olzubar, olzvbar, olzthbar, olzqbar(n)) or null.  read sets *has_mean when the file holds
+ * the mean profiles. */
+int mgpu_checkpoint_write_host(const mgpu_config* cfg, const char* path, const double* const* fields,
+                               const double* mean, const mgpu_checkpoint_meta* meta);
+int mgpu_checkpoint_read_host(const mgpu_config* cfg, const char* path, double* const* fields, double* mean,
+                              int32_t* has_mean, mgpu_checkpoint_meta* meta);
+
 /* The mean profiles damping and forcing read (meanprofiles.F90:95-216, global_grid vertical
  * olzubar, olzvbar, olzthbar, olzqbar): out receives (3 + number_q_fields) rows of nz values,
  * k = 1..nz.  mgpu_step refreshes them in the solver group of each step when damping or

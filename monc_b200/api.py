@@ -85,6 +85,13 @@ GROUPS = {
 }
 
 
+class CheckpointMeta(C.Structure):
+    """mgpu_checkpoint_meta: the step count, time and dtm state a MONC checkpoint carries."""
+    _fields_ = [("timestep", C.c_int32), ("last_cfl_timestep", C.c_int32), ("time", C.c_double),
+                ("dtm", C.c_double), ("dtm_new", C.c_double), ("absolute_new_dtm", C.c_double),
+                ("ugal", C.c_double), ("vgal", C.c_double)]
+
+
 class MgpuError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"libmoncgpu error {code}: {msg}")
@@ -144,6 +151,15 @@ def lib():
     L.mgpu_diagnostics.restype = C.c_int
     L.mgpu_mean_profiles.argtypes = [C.c_void_p, C.c_void_p]
     L.mgpu_mean_profiles.restype = C.c_int
+    for name in ("mgpu_checkpoint_write", "mgpu_checkpoint_read"):
+        f = getattr(L, name)
+        f.argtypes = [C.c_void_p, C.c_char_p]
+        f.restype = C.c_int
+    L.mgpu_checkpoint_write_host.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mgpu_checkpoint_write_host.restype = C.c_int
+    L.mgpu_checkpoint_read_host.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]
+    L.mgpu_checkpoint_read_host.restype = C.c_int
     L.mgpu_set_profiling.argtypes = [C.c_void_p, C.c_int32]
     L.mgpu_set_profiling.restype = C.c_int
     L.mgpu_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -317,6 +333,14 @@ class Model:
         names = ["olzubar", "olzvbar", "olzthbar"] + [f"olzqbar{n}" for n in range(self.cfg.number_q_fields)]
         return dict(zip(names, out))
 
+    def checkpoint_write(self, path: str):
+        """Write a MONC-layout checkpoint (NetCDF classic) of the model's state."""
+        self._check(lib().mgpu_checkpoint_write(self.h, os.fsencode(path)), "checkpoint_write")
+
+    def checkpoint_read(self, path: str):
+        """Restart from a MONC-layout checkpoint: state, mean profiles, step count, time, dtm."""
+        self._check(lib().mgpu_checkpoint_read(self.h, os.fsencode(path)), "checkpoint_read")
+
     def diagnostics(self, out_th: np.ndarray | None = None, out_w2: np.ndarray | None = None):
         """Device-computed horizontal means: theta (incl. thref) and w**2 per level."""
         th = out_th if out_th is not None else np.empty(self.nz, dtype=np.float64)
@@ -417,3 +441,40 @@ def run_groups(model: Model, groups=("start", "subgrid", "dynamics", "solver", "
             model.component(name)
     ts = model.reductions().timestep
     model.set_timestep(ts + 1)
+
+
+CHECKPOINT_FIELDS = ["u", "v", "w", "th", "zu", "zv", "zw", "zth", "p"]
+
+
+def _checkpoint_names(cfg) -> list:
+    nq = cfg.number_q_fields
+    return CHECKPOINT_FIELDS + [f"q{n}" for n in range(nq)] + [f"zq{n}" for n in range(nq)]
+
+
+def checkpoint_write_host(cfg, path: str, fields: dict, meta: CheckpointMeta, mean: np.ndarray | None = None):
+    """Write a MONC-layout checkpoint from host arrays (no GPU): fields by name, each (nz, ny, nx);
+    mean, when given, (3 + number_q_fields, nz) rows olzubar, olzvbar, olzthbar, olzqbar(n)."""
+    names = _checkpoint_names(cfg)
+    arrs = [np.ascontiguousarray(fields[n], dtype=np.float64) for n in names]
+    ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    m = None if mean is None else np.ascontiguousarray(mean, dtype=np.float64)
+    rc = lib().mgpu_checkpoint_write_host(C.byref(cfg), os.fsencode(path), ptrs,
+                                          None if m is None else m.ctypes.data, C.byref(meta))
+    if rc != OK:
+        raise MgpuError(rc, "mgpu_checkpoint_write_host")
+
+
+def checkpoint_read_host(cfg, path: str):
+    """Read a MONC-layout checkpoint into host arrays: (fields, mean or None, meta)."""
+    names = _checkpoint_names(cfg)
+    shape = (cfg.nz, cfg.ny, cfg.nx)
+    arrs = [np.empty(shape, dtype=np.float64) for _ in names]
+    ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    mean = np.empty((3 + cfg.number_q_fields, cfg.nz), dtype=np.float64)
+    has_mean = C.c_int32(0)
+    meta = CheckpointMeta()
+    rc = lib().mgpu_checkpoint_read_host(C.byref(cfg), os.fsencode(path), ptrs, mean.ctypes.data,
+                                         C.byref(has_mean), C.byref(meta))
+    if rc != OK:
+        raise MgpuError(rc, "mgpu_checkpoint_read_host")
+    return dict(zip(names, arrs)), (mean if has_mean.value else None), meta

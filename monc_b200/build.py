@@ -19,6 +19,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 # (source, extra flags)
 UNITS = [
     ("grid.cpp", []),
+    ("checkpoint.cpp", []),
     ("api.cu", []),
     ("dycore_f64.cu", ["--fmad=false"]),
     ("dycore_f64_fast.cu", []),

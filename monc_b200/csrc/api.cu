@@ -37,6 +37,7 @@ struct mgpu_handle {
   RefState rs;
   Scalars sc;
   int timestep = 1;
+  double time = 0.0;  // model time: the dtm of every completed step
   int device = 0;
   bool fp32 = false;
   cudaStream_t stream = nullptr;
@@ -712,6 +713,7 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
     int rc = cfltest_callback(h, cfl_gather);
     if (rc) return rc;
   }
+  h->time += h->sc.dtm;
   h->timestep += 1;
   if (h->profiling) collect_stage_times(h);
   return MGPU_OK;
@@ -999,6 +1001,88 @@ int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out) {
   return MGPU_OK;
 }
 
+// ---- checkpoints: the host codec (checkpoint.cpp) around downloads / uploads of the state ----
+static int checkpoint_fields(mgpu_handle* h, std::vector<std::vector<double>>& buf, std::vector<int>& ids) {
+  const int nq = h->cfg.number_q_fields;
+  const int base[9] = {MGPU_U, MGPU_V, MGPU_W, MGPU_TH, MGPU_ZU, MGPU_ZV, MGPU_ZW, MGPU_ZTH, MGPU_P};
+  ids.assign(base, base + 9);
+  for (int n = 0; n < nq; ++n) ids.push_back(MGPU_Q0 + n);
+  for (int n = 0; n < nq; ++n) ids.push_back(MGPU_ZQ0 + n);
+  buf.assign(ids.size(), std::vector<double>(field_elems(h)));
+  return MGPU_OK;
+}
+
+int mgpu_checkpoint_write(mgpu_handle* h, const char* path) {
+  if (!h || !path) return MGPU_ERR_ARGUMENT;
+  std::vector<std::vector<double>> buf;
+  std::vector<int> ids;
+  checkpoint_fields(h, buf, ids);
+  std::vector<const double*> ptr;
+  for (size_t q = 0; q < ids.size(); ++q) {
+    int rc = h->fp32 ? download<float>(h, h->d32, ids[q], buf[q].data(), MGPU_LAYOUT_XFAST)
+                     : download<double>(h, h->d64, ids[q], buf[q].data(), MGPU_LAYOUT_XFAST);
+    if (rc) return rc;
+    ptr.push_back(buf[q].data());
+  }
+  std::vector<double> mean;
+  const bool with_mean = needs_mean_profiles(h->cfg);
+  if (with_mean) {
+    mean.resize((size_t)(3 + h->cfg.number_q_fields) * h->cfg.nz);
+    if (int rc = mgpu_mean_profiles(h, mean.data())) return rc;
+  }
+  mgpu_checkpoint_meta meta{};
+  meta.timestep = h->timestep - 1;
+  meta.last_cfl_timestep = h->cfl.last_cfl_timestep;
+  meta.time = h->time;
+  meta.dtm = h->sc.dtm;
+  meta.dtm_new = h->cfl.update_dtm ? h->cfl.dtm_new : h->sc.dtm;
+  meta.absolute_new_dtm = h->cfl.absolute_new_dtm;
+  meta.ugal = h->sc.ugal;
+  meta.vgal = h->sc.vgal;
+  std::string err;
+  int rc = checkpoint_write_host(h->cfg, h->rs, path, ptr.data(), with_mean ? mean.data() : nullptr, meta, err);
+  if (rc) return fail(h, rc, "checkpoint write: " + err);
+  return MGPU_OK;
+}
+
+int mgpu_checkpoint_read(mgpu_handle* h, const char* path) {
+  if (!h || !path) return MGPU_ERR_ARGUMENT;
+  std::vector<std::vector<double>> buf;
+  std::vector<int> ids;
+  checkpoint_fields(h, buf, ids);
+  std::vector<double*> ptr;
+  for (auto& b : buf) ptr.push_back(b.data());
+  std::vector<double> mean((size_t)(3 + h->cfg.number_q_fields) * h->cfg.nz);
+  int has_mean = 0;
+  mgpu_checkpoint_meta meta{};
+  std::string err;
+  int rc = checkpoint_read_host(h->cfg, path, ptr.data(), mean.data(), &has_mean, meta, err);
+  if (rc) return fail(h, rc, "checkpoint read: " + err);
+  for (size_t q = 0; q < ids.size(); ++q) {
+    rc = h->fp32 ? upload<float>(h, h->d32, ids[q], buf[q].data(), MGPU_LAYOUT_XFAST)
+                 : upload<double>(h, h->d64, ids[q], buf[q].data(), MGPU_LAYOUT_XFAST);
+    if (rc) return rc;
+  }
+  if (has_mean) {
+    const int nz = h->cfg.nz;
+    std::vector<double> rows((size_t)(3 + MGPU_MAX_Q) * (nz + 2), 0.0);
+    for (int r = 0; r < 3 + h->cfg.number_q_fields; ++r)
+      for (int k = 1; k <= nz; ++k) rows[(size_t)r * (nz + 2) + k] = mean[(size_t)r * nz + k - 1];
+    CK(cudaMemcpyAsync(h->olz_d, rows.data(), rows.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  // readcheckpoint.F90 load_misc: the run continues at the step after the checkpointed one
+  h->timestep = meta.timestep + 1;
+  h->time = meta.time;
+  h->sc.dtm = meta.dtm;
+  h->cfl.dtm_last = meta.dtm;
+  h->cfl.dtm_new = meta.dtm_new;
+  h->cfl.update_dtm = h->cfg.cfl_enabled && meta.dtm_new != meta.dtm;
+  h->cfl.absolute_new_dtm = meta.absolute_new_dtm;
+  h->cfl.last_cfl_timestep = meta.last_cfl_timestep;
+  return MGPU_OK;
+}
+
 int mgpu_mean_profiles(mgpu_handle* h, double* out) {
   if (!h || !out) return MGPU_ERR_ARGUMENT;
   const int nz = h->cfg.nz, rows = 3 + h->cfg.number_q_fields;
@@ -1095,6 +1179,7 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
       if (exact_k) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
       else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
       h->launches += 1;
+      h->time += h->sc.dtm;
       h->timestep += 1;
       return MGPU_OK;
   }

@@ -39,6 +39,13 @@ struct RefState {
 void build_reference_state(const mgpu_config& cfg, RefState& rs);
 const std::vector<double>* profile_by_name(const RefState& rs, const std::string& name);
 
+// Checkpoint files in MONC's layout (checkpoint.cpp); fields and mean as in mgpu_checkpoint_write_host
+int checkpoint_write_host(const mgpu_config& c, const RefState& rs, const std::string& path,
+                          const double* const* fields, const double* mean, const mgpu_checkpoint_meta& meta,
+                          std::string& err);
+int checkpoint_read_host(const mgpu_config& c, const std::string& path, double* const* fields, double* mean,
+                         int* has_mean, mgpu_checkpoint_meta& meta, std::string& err);
+
 // Profiles copied to device memory, 1-based (index k), FP64.
 enum ProfileId {
   P_RDZ = 0, P_RDZN, P_DZN, P_RHO, P_RHON, P_DTHREF, P_CZB, P_CZA, P_CZG, P_CZH, P_TZC1, P_TZC2, P_TZD1, P_TZD2,
