@@ -300,6 +300,8 @@ def run_ours(args):
     if world == 1 and not args.skip_extra:
         extra["adjoint"] = adjoint_ratio()
         extra["precision_moist"] = precision_moist()
+        if args.large:
+            extra["large_fp32_mixed"] = large_fp32_mixed()
 
     if dist.is_initialized():
         dist.barrier()
@@ -407,6 +409,63 @@ def precision_moist():
             "rel_err_mean_w2": pr.rel(w32, w64), "rel_err_mean_qv": pr.rel(qv32, qv64)}
 
 
+def large_fp32_mixed():
+    """The largest configuration: 1024x1024x200 FP32-mixed, dz 10->50 m to 6 km, vapour, liquid and
+    three passive tracers with log-normal surface sources, 150 / 200 W m-2 surface fluxes, +-0.2 K
+    noise, dt = 0.5 s, 200 steps; CUDA events on the model's stream over steps 2..200."""
+    import torch
+
+    from monc_b200 import api, config as cf, init as ini
+
+    nx = ny = 1024
+    nz, steps = 200, 200
+    z = cf.stretched_levels(nz, 10.0, 50.0, ztop=6000.0)
+    c = cf.moist_config(nx, ny, z, 25.0, 0.5, shf_wm2=150.0, lhf_wm2=200.0, max_height_cloud=5000.0, n_tracers=3,
+                        precision=cf.FP32_MIXED)
+    m = api.Model(c)
+    # the state of init.moist_layer_state, built and uploaded one field at a time (each 1.7 GB on
+    # the host): theta with +-0.2 K noise on the lowest levels, vapour, no liquid, three tracers
+    zn = api.reference_profile(c, "zn")
+    shape = (nz, ny, nx)
+    th_prof = np.where(zn > 840.0, 297.5 + 0.00365 * (zn - 840.0), 289.0) - 289.0
+    f = np.broadcast_to(th_prof[:, None, None], shape).copy()
+    f[1:9] += ini.uniform_noise((8, ny, nx), 5, 3, 0.2)
+    f[0] = f[1]
+    m.upload("th", f)
+    m.upload("zth", f)
+    f[:] = np.where(zn > 840.0, 1.5e-3, 9e-3)[:, None, None]
+    m.upload("q0", f)
+    m.upload("zq0", f)
+    f[:] = 2.0  # a uniform 2 m/s wind: MONC's surface scheme has no windless limit (u* -> 0)
+    m.upload("u", f)
+    m.upload("zu", f)
+    f[:] = 0.0
+    for name in ("v", "w", "zv", "zw", "q1", "zq1"):
+        m.upload(name, f)
+    for t in range(3):
+        for k in range(nz):
+            f[k] = np.exp(0.5 * ini.uniform_noise((1, ny, nx), 5 + k, 40 + t, 1.0)[0]) * np.exp(-zn[k] / 200.0)
+        m.upload(f"q{2 + t}", f)
+        m.upload(f"zq{2 + t}", f)
+    del f
+    m.step(1)
+    stream = torch.cuda.ExternalStream(m.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    m.step(steps - 1)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / (steps - 1)
+    th, w2 = m.diagnostics()
+    finite = bool(np.isfinite(th).all() and np.isfinite(w2).all())
+    m.close()
+    return {"case": "1024x1024x200 FP32-mixed, dx=25 m, dz 10->50 m to 6 km, u = 2 m/s, vapour + liquid + "
+                    "3 tracers, shf 150 / lhf 200 W m-2, dt=0.5 s, 200 steps",
+            "ms_per_step": round(ms, 3), "mpoint_steps_per_s": round(nx * ny * nz / (ms * 1e-3) / 1e6, 1),
+            "finite": finite, "max_mean_w2": float(np.max(w2)) if finite else None}
+
+
 def _oracle_run(seed_steps):
     """One oracle instance on the benchmark grid: forward step + `steps` timed centred steps."""
     steps = seed_steps
@@ -487,6 +546,8 @@ def main():
                     help="N > 1: independent single-GPU models instead of the decomposed domain")
     ap.add_argument("--decomposed", action="store_true",
                     help="run the decomposed domain even on one GPU (one slab; exercises the NCCL path)")
+    ap.add_argument("--large", action="store_true",
+                    help="also run the 1024x1024x200 FP32-mixed case with three tracers (about a minute)")
     ap.add_argument("--skip-extra", action="store_true",
                     help="skip the adjoint-ratio and moist-precision measurements (single-GPU runs)")
     args = ap.parse_args()
