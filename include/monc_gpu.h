@@ -169,6 +169,9 @@ typedef struct mgpu_config {
   int32_t subsidence_local_q;         /* the same for q */
   int32_t n_subs_pl;                  /* nodes in z_subs_pl / f_subs_pl (<= MGPU_MAX_SUBS_NODES) */
   double  z_subs_pl[MGPU_MAX_SUBS_NODES], f_subs_pl[MGPU_MAX_SUBS_NODES];
+  /* profile_diagnostics (profile_diagnostics.F90:311-636): keeps the mean profiles it reads up to
+   * date every step, so that mgpu_profile_diagnostics can be called between steps */
+  int32_t profile_diagnostics_enabled;
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */
@@ -280,11 +283,41 @@ int mgpu_checkpoint_write_host(const mgpu_config* cfg, const char* path, const d
 int mgpu_checkpoint_read_host(const mgpu_config* cfg, const char* path, double* const* fields, double* mean,
                               int32_t* has_mean, mgpu_checkpoint_meta* meta);
 
-/* The mean profiles damping and forcing read (meanprofiles.F90:95-216, global_grid vertical
- * olzubar, olzvbar, olzthbar, olzqbar): out receives (3 + number_q_fields) rows of nz values,
- * k = 1..nz.  mgpu_step refreshes them in the solver group of each step when damping or
- * non-local subsidence is on; MGPU_C_MEAN_PROFILES refreshes them from zu, zv, zth, zq. */
+/* The mean profiles (meanprofiles.F90:95-216, global_grid vertical olzubar, olzvbar, olzthbar,
+ * olzqbar, olubar, olvbar, olthbar): out receives (6 + number_q_fields) rows of nz values,
+ * k = 1..nz: olzubar, olzvbar, olzthbar, olzqbar(n), then olubar, olvbar, olthbar.  They are the
+ * means of the fields as MONC's solver group sees them: the stepped zu, zv, zth, zq before the
+ * pressure step, u + ugal, v + vgal, and theta after stepfields' time smoothing.  mgpu_step
+ * refreshes them every step when damping, subsidence or profile_diagnostics reads them;
+ * MGPU_C_MEAN_PROFILES refreshes them from the component fields. */
 int mgpu_mean_profiles(mgpu_handle* h, double* out);
+
+/* profile_diagnostics (profile_diagnostics.F90:311-636, published as <name>_total_local): the
+ * per-level sums over the domain's columns that MONC's component accumulates in the next step's
+ * dynamics group, from the current state and the mean profiles of the last step.  For PW flow
+ * advection with TVD scalars (the flux terms of TVD flow advection are not provided: error).
+ * Needs profile_diagnostics_enabled.  out receives *nrows rows of nz values, k = 1..nz, in the
+ * order MGPU_PD_U_WIND .. MGPU_PD_RH (the last five only with active q fields). */
+enum mgpu_profile_diagnostic {
+  MGPU_PD_U_WIND = 0,  /* u_wind_total:    sum (u + ugal) */
+  MGPU_PD_V_WIND,      /* v_wind_total:    sum (v + vgal) */
+  MGPU_PD_W_WIND,      /* w_wind_total:    sum w, k >= 2 */
+  MGPU_PD_WW,          /* ww_total:        sum w^2 */
+  MGPU_PD_WWW,         /* www_total:       sum w^3, k >= 2 */
+  MGPU_PD_WWWW,        /* wwww_total:      sum w^4, k >= 2 */
+  MGPU_PD_THETA,       /* theta_total:     sum (th + thref) */
+  MGPU_PD_TH2,         /* th2_total:       sum (th - olthbar)^2 */
+  MGPU_PD_WTHETA_CN,   /* wtheta_cn_total: sum w (th(k) + th(k+1))/2, 2 <= k <= nz-1 */
+  MGPU_PD_UW,          /* uw_total:        sum (u at w points + ugal - mean) w, k <= nz-1 */
+  MGPU_PD_VW,          /* vw_total:        the same for v */
+  MGPU_PD_VAPOUR,      /* vapour_mmr_total */
+  MGPU_PD_LIQUID,      /* liquid_mmr_total */
+  MGPU_PD_WQV_CN,      /* wqv_cn_total:    sum w (qv(k) + qv(k+1))/2, 2 <= k <= nz-1 */
+  MGPU_PD_WQL_CN,      /* wql_cn_total */
+  MGPU_PD_RH,          /* rh_total:        sum qv / qsat(T, p) */
+  MGPU_PD_COUNT
+};
+int mgpu_profile_diagnostics(mgpu_handle* h, double* out, int32_t* nrows);
 
 /* Per-stage device timing of mgpu_step (CUDA events on the handle's stream).  Stage order:
  * 0 subgrid, 1 dynamics, 2 pressure source, 3 fft x forward, 4 fft y forward, 5 tridiagonal,

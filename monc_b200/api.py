@@ -74,6 +74,13 @@ COMPONENTS = {
     "forcing": 22,
 }
 
+# the profile_diagnostics sums mgpu_profile_diagnostics returns, under the names MONC's component
+# publishes them (profile_diagnostics.F90:74-118), in the MGPU_PD_* row order
+PROFILE_DIAGNOSTICS = ["u_wind_total_local", "v_wind_total_local", "w_wind_total_local", "ww_total_local",
+                       "www_total_local", "wwww_total_local", "theta_total_local", "th2_total_local",
+                       "wtheta_cn_total_local", "uw_total_local", "vw_total_local", "vapour_mmr_total_local",
+                       "liquid_mmr_total_local", "wqv_cn_total_local", "wql_cn_total_local", "rh_total_local"]
+
 # MONC's default group layout of these components (global_config:77-92)
 GROUPS = {
     "start": ["clearsourceterms", "stepping_direction", "halo_swapper"],
@@ -151,6 +158,8 @@ def lib():
     L.mgpu_diagnostics.restype = C.c_int
     L.mgpu_mean_profiles.argtypes = [C.c_void_p, C.c_void_p]
     L.mgpu_mean_profiles.restype = C.c_int
+    L.mgpu_profile_diagnostics.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]
+    L.mgpu_profile_diagnostics.restype = C.c_int
     for name in ("mgpu_checkpoint_write", "mgpu_checkpoint_read"):
         f = getattr(L, name)
         f.argtypes = [C.c_void_p, C.c_char_p]
@@ -325,13 +334,22 @@ class Model:
         return out
 
     def mean_profiles(self) -> dict:
-        """The mean profiles damping and forcing read: olzubar, olzvbar, olzthbar and olzqbar(n)
-        (meanprofiles.F90), as refreshed by the last step or mean_profiles component."""
-        rows = 3 + self.cfg.number_q_fields
+        """The mean profiles (meanprofiles.F90): olzubar, olzvbar, olzthbar, olzqbar(n), olubar,
+        olvbar, olthbar, as refreshed by the last step or mean_profiles component."""
+        rows = 6 + self.cfg.number_q_fields
         out = np.empty((rows, self.nz), dtype=np.float64)
         self._check(lib().mgpu_mean_profiles(self.h, out.ctypes.data), "mean_profiles")
-        names = ["olzubar", "olzvbar", "olzthbar"] + [f"olzqbar{n}" for n in range(self.cfg.number_q_fields)]
+        names = (["olzubar", "olzvbar", "olzthbar"] + [f"olzqbar{n}" for n in range(self.cfg.number_q_fields)]
+                 + ["olubar", "olvbar", "olthbar"])
         return dict(zip(names, out))
+
+    def profile_diagnostics(self) -> dict:
+        """MONC's profile_diagnostics sums (<name>_total_local, per level) from the current state,
+        as the component would accumulate them in the next step (needs profile_diagnostics_enabled)."""
+        out = np.empty((len(PROFILE_DIAGNOSTICS), self.nz), dtype=np.float64)
+        rows = C.c_int32(0)
+        self._check(lib().mgpu_profile_diagnostics(self.h, out.ctypes.data, C.byref(rows)), "profile_diagnostics")
+        return dict(zip(PROFILE_DIAGNOSTICS[:rows.value], out[:rows.value]))
 
     def checkpoint_write(self, path: str):
         """Write a MONC-layout checkpoint (NetCDF classic) of the model's state."""
@@ -404,12 +422,25 @@ class ComponentDescriptor:
     initialisation: Optional[Callable] = None
     timestep: Optional[Callable] = None
     finalisation: Optional[Callable] = None
+    published_fields: Optional[list] = None
+    field_value_retrieval: Optional[Callable] = None
 
 
 def component_descriptor(name: str) -> ComponentDescriptor:
     """The descriptor a MONC registry would receive for a GPU drop-in of `name`.
 
-    The callbacks take the `Model` that stands for `current_state`."""
+    The callbacks take the `Model` that stands for `current_state`.  `profile_diagnostics` has
+    no timestep work here: its field_value_retrieval(model, field_name) computes the named sums
+    on the device when the IO server asks for them."""
+    if name == "profile_diagnostics":
+        def retrieve(model: Model, field_name: str) -> np.ndarray:
+            values = model.profile_diagnostics()
+            if field_name not in values:
+                raise KeyError(f"profile_diagnostics publishes no {field_name} for this model")
+            return values[field_name]
+
+        return ComponentDescriptor(name=name, version=0.1, published_fields=list(PROFILE_DIAGNOSTICS),
+                                   field_value_retrieval=retrieve)
     if name not in COMPONENTS:
         raise KeyError(f"no GPU drop-in for component {name}")
 
@@ -436,7 +467,7 @@ def run_groups(model: Model, groups=("start", "subgrid", "dynamics", "solver", "
             if name == "forcing" and not (model.cfg.l_subs_pl_theta or model.cfg.l_subs_pl_q):
                 continue
             if name == "mean_profiles" and not (model.cfg.damping_enabled or model.cfg.l_subs_pl_theta
-                                                or model.cfg.l_subs_pl_q):
+                                                or model.cfg.l_subs_pl_q or model.cfg.profile_diagnostics_enabled):
                 continue
             model.component(name)
     ts = model.reductions().timestep

@@ -80,6 +80,7 @@ class MgpuConfig(C.Structure):
         ("subsidence_local_theta", C.c_int32), ("subsidence_local_q", C.c_int32),
         ("n_subs_pl", C.c_int32),
         ("z_subs_pl", C.c_double * MAX_SUBS_NODES), ("f_subs_pl", C.c_double * MAX_SUBS_NODES),
+        ("profile_diagnostics_enabled", C.c_int32),
     ]
 
 
@@ -154,6 +155,7 @@ def default_config() -> MgpuConfig:
     c.subsidence_input_type = SUBS_VELOCITY
     c.subsidence_local_theta = c.subsidence_local_q = 1
     c.n_subs_pl = 0
+    c.profile_diagnostics_enabled = 0
     return c
 
 

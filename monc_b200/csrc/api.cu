@@ -59,6 +59,8 @@ struct mgpu_handle {
   double* bmean_d = nullptr; // FP32-mixed: horizontal means of th and q per level (1+nq rows of nz+2)
   double* olz_d = nullptr;       // mean profiles olzubar, olzvbar, olzthbar, olzqbar (3+MGPU_MAX_Q rows of nz+2)
   double* subs_tend_d = nullptr; // mean-profile subsidence tendencies, the same rows
+  double* olbar_d = nullptr;     // olubar, olvbar, olthbar (3 rows of nz+2)
+  double* pd_d = nullptr;        // profile_diagnostics sums (MGPU_PD_COUNT rows of nz)
   bool profiling = false;
   cudaEvent_t ev[16] = {};
   struct AdWork* ad = nullptr;  // tangent-linear / adjoint arrays, allocated on first use
@@ -208,7 +210,7 @@ static void forcing_flags(mgpu_handle* h) {
 }
 // the mean profiles are refreshed every step when damping or mean-profile subsidence reads them
 static bool needs_mean_profiles(const mgpu_config& c) {
-  return c.damping_enabled || (c.l_subs_pl_theta && !c.subsidence_local_theta) ||
+  return c.damping_enabled || c.profile_diagnostics_enabled || (c.l_subs_pl_theta && !c.subsidence_local_theta) ||
          (c.l_subs_pl_q && !c.subsidence_local_q && c.number_q_fields > 0);
 }
 // the mean-profile subsidence tendencies of this step, from the mean profiles of the last
@@ -290,6 +292,10 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
       return cleanup(MGPU_ERR_CUDA);
     cudaMemset(h->olz_d, 0, nb);
     cudaMemset(h->subs_tend_d, 0, nb);
+    const size_t nbar = (size_t)3 * (cfg->nz + 2) * sizeof(double), npd = (size_t)MGPU_PD_COUNT * cfg->nz * sizeof(double);
+    if (cudaMalloc(&h->olbar_d, nbar) != cudaSuccess || cudaMalloc(&h->pd_d, npd) != cudaSuccess)
+      return cleanup(MGPU_ERR_CUDA);
+    cudaMemset(h->olbar_d, 0, nbar);
   }
   for (cudaEvent_t& e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return cleanup(MGPU_ERR_CUDA);
@@ -338,6 +344,8 @@ int mgpu_destroy(mgpu_handle* h) {
   cudaFree(h->bmean_d);
   cudaFree(h->olz_d);
   cudaFree(h->subs_tend_d);
+  cudaFree(h->olbar_d);
+  cudaFree(h->pd_d);
   cudaFree(h->cfl.part_d);
   cudaFree(h->cfl.out_d);
   if (h->cfl.out_h) cudaFreeHost(h->cfl.out_h);
@@ -695,8 +703,15 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   mark(2);
   swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
   // mean_profiles (solver group): the stepped zu, zv and the new theta, q before the pressure step
-  if (needs_mean_profiles(h->cfg))
+  if (needs_mean_profiles(h->cfg)) {
     h->launches += launch_mean_profiles<T>(h->sc, d.zu_n, d.zv_n, d.th, d.q, h->olz_d, h->stream);
+    // u + ugal, v + vgal (stepfields.F90 adds the Galilean velocity before the solver group) and
+    // the old theta, time-smoothed on a centred step; the swap left the old th, zth in th_n, zth_n
+    const bool fwd = h->sc.forward != 0;
+    h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th_n, fwd ? nullptr : d.zth_n, h->sc.ugal,
+                                                 h->sc.vgal, 1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d,
+                                                 h->stream);
+  }
   if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
   else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
   h->launches += 1;
@@ -895,7 +910,10 @@ static int component(mgpu_handle* h, DevState<T>& d, int cid) {
   switch (cid) {
     case MGPU_C_STEPPING_DIRECTION: return MGPU_OK;
     case MGPU_C_MEAN_PROFILES:
+      // the component fields already hold u + ugal and the time-smoothed theta, as MONC's do
       h->launches += launch_mean_profiles<T>(h->sc, d.zu, d.zv, d.zth, d.zq, h->olz_d, h->stream);
+      h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th, nullptr, 0.0, 0.0, 1.0, 0.0, h->olbar_d,
+                                                   h->stream);
       break;
     case MGPU_C_FORCING:
       h->launches += subsidence_tendencies(h);
@@ -1027,7 +1045,8 @@ int mgpu_checkpoint_write(mgpu_handle* h, const char* path) {
   std::vector<double> mean;
   const bool with_mean = needs_mean_profiles(h->cfg);
   if (with_mean) {
-    mean.resize((size_t)(3 + h->cfg.number_q_fields) * h->cfg.nz);
+    // the olz*bar rows come first; olubar, olvbar, olthbar follow and are not checkpointed
+    mean.resize((size_t)(6 + h->cfg.number_q_fields) * h->cfg.nz);
     if (int rc = mgpu_mean_profiles(h, mean.data())) return rc;
   }
   mgpu_checkpoint_meta meta{};
@@ -1086,11 +1105,42 @@ int mgpu_checkpoint_read(mgpu_handle* h, const char* path) {
 int mgpu_mean_profiles(mgpu_handle* h, double* out) {
   if (!h || !out) return MGPU_ERR_ARGUMENT;
   const int nz = h->cfg.nz, rows = 3 + h->cfg.number_q_fields;
-  std::vector<double> buf((size_t)rows * (nz + 2));
+  std::vector<double> buf((size_t)rows * (nz + 2)), bar((size_t)3 * (nz + 2));
   CK(cudaMemcpyAsync(buf.data(), h->olz_d, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(bar.data(), h->olbar_d, bar.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   for (int r = 0; r < rows; ++r)
     for (int k = 1; k <= nz; ++k) out[(size_t)r * nz + k - 1] = buf[(size_t)r * (nz + 2) + k];
+  for (int r = 0; r < 3; ++r)
+    for (int k = 1; k <= nz; ++k) out[(size_t)(rows + r) * nz + k - 1] = bar[(size_t)r * (nz + 2) + k];
+  return MGPU_OK;
+}
+
+int mgpu_profile_diagnostics(mgpu_handle* h, double* out, int32_t* nrows) {
+  if (!h || !out) return MGPU_ERR_ARGUMENT;
+  if (!h->cfg.profile_diagnostics_enabled)
+    return fail(h, MGPU_ERR_ARGUMENT, "profile_diagnostics_enabled is off (the mean profiles it reads are not kept)");
+  if (h->cfg.advection_flow_fields != MGPU_ADVECT_PW)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "profile diagnostics of TVD flow advection (its flux diagnostics) are not provided");
+  const int nz = h->cfg.nz, nq = h->cfg.number_q_fields;
+  const bool moist = !h->cfg.passive_q && nq >= 2;
+  const int rows = moist ? MGPU_PD_COUNT : MGPU_PD_VAPOUR;
+  const bool has_mean = needs_mean_profiles(h->cfg);
+  if (h->fp32) {
+    DevState<float>& d = h->d32;
+    h->launches += launch_profile_diagnostics<float>(h->sc, d.u, d.v, d.w, d.th, moist ? d.q[h->sc.iqv] : nullptr,
+                                                     moist ? d.q[h->sc.iql] : nullptr, h->olbar_d, has_mean, h->pd_d,
+                                                     h->stream);
+  } else {
+    DevState<double>& d = h->d64;
+    h->launches += launch_profile_diagnostics<double>(h->sc, d.u, d.v, d.w, d.th, moist ? d.q[h->sc.iqv] : nullptr,
+                                                      moist ? d.q[h->sc.iql] : nullptr, h->olbar_d, has_mean, h->pd_d,
+                                                      h->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, h->pd_d, (size_t)rows * nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (nrows) *nrows = rows;
   return MGPU_OK;
 }
 

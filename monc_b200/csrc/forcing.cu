@@ -1,5 +1,6 @@
-// Mean profiles (meanprofiles.F90) and the mean-profile subsidence tendencies (forcing.F90)
-// the damping and forcing components read.
+// Mean profiles (meanprofiles.F90), the mean-profile subsidence tendencies (forcing.F90) the
+// damping and forcing components read, and the profile_diagnostics sums
+// (profile_diagnostics.F90).
 //
 // MONC's mean_profiles runs in the solver group, after stepfields: olzubar, olzvbar, olzthbar and
 // olzqbar are the horizontal means of the stepped fields before the pressure correction.  In the
@@ -11,18 +12,28 @@
 
 namespace mgpu {
 
+// field q of a mean: c[q] + p[q], or a[q] p[q] + b[q] p2[q] when p2[q] is set (theta after
+// stepfields' time smoothing)
 template <typename T>
 struct MeanFields {
   const T* p[3 + MGPU_MAX_Q];
+  const T* p2[3 + MGPU_MAX_Q];
+  double a[3 + MGPU_MAX_Q], b[3 + MGPU_MAX_Q], c[3 + MGPU_MAX_Q];
 };
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_plane_means(MeanFields<T> f, long long plane, double rnhpts, double* out,
                                                      int stride) {
   const int k = blockIdx.x + 1, q = blockIdx.y;
-  const T* __restrict__ p = f.p[q] + (long long)(k - 1) * plane;
+  const long long base = (long long)(k - 1) * plane;
+  const T* __restrict__ p = f.p[q] + base;
+  const T* __restrict__ p2 = f.p2[q] ? f.p2[q] + base : nullptr;
+  const double a = f.a[q], b = f.b[q], c = f.c[q];
   double acc = 0.0;
-  for (long long t = threadIdx.x; t < plane; t += blockDim.x) acc += (double)__ldg(p + t);
+  if (p2)
+    for (long long t = threadIdx.x; t < plane; t += blockDim.x) acc += a * (double)__ldg(p + t) + b * (double)__ldg(p2 + t);
+  else
+    for (long long t = threadIdx.x; t < plane; t += blockDim.x) acc += c + (double)__ldg(p + t);
   __shared__ double sh[256];
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -39,7 +50,7 @@ static double rnhpts(const Scalars& s) { return 1.0 / (double)(float)((long long
 template <typename T>
 int launch_mean_profiles(const Scalars& s, const T* zu, const T* zv, const T* th, const T* const* q, double* olz,
                          cudaStream_t st) {
-  MeanFields<T> f;
+  MeanFields<T> f{};
   f.p[0] = zu;
   f.p[1] = zv;
   f.p[2] = th;
@@ -51,6 +62,112 @@ template int launch_mean_profiles<float>(const Scalars&, const float*, const flo
                                          double*, cudaStream_t);
 template int launch_mean_profiles<double>(const Scalars&, const double*, const double*, const double*,
                                           const double* const*, double*, cudaStream_t);
+
+// olubar, olvbar, olthbar: the means of ugal + u, vgal + v and of theta, with zth (time
+// smoothing c1 th + c2 zth) when given
+template <typename T>
+int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth, double ugal,
+                               double vgal, double c1, double c2, double* olbar, cudaStream_t st) {
+  MeanFields<T> f{};
+  f.p[0] = u;
+  f.c[0] = ugal;
+  f.p[1] = v;
+  f.c[1] = vgal;
+  f.p[2] = th;
+  f.p2[2] = zth;
+  f.a[2] = c1;
+  f.b[2] = c2;
+  k_plane_means<T><<<dim3(s.nz, 3), 256, 0, st>>>(f, s.plane, rnhpts(s), olbar, s.nz + 2);
+  return 1;
+}
+template int launch_mean_profiles_state<float>(const Scalars&, const float*, const float*, const float*, const float*,
+                                               double, double, double, double, double*, cudaStream_t);
+template int launch_mean_profiles_state<double>(const Scalars&, const double*, const double*, const double*,
+                                                const double*, double, double, double, double, double*, cudaStream_t);
+
+// profile_diagnostics (profile_diagnostics.F90:311-636, PW flow and TVD scalars): one block per
+// level sums the MGPU_PD_* quantities over the plane in FP64, in a fixed order
+template <typename T>
+__global__ void __launch_bounds__(256) k_profile_diagnostics(Scalars s, const T* __restrict__ u,
+                                                             const T* __restrict__ v, const T* __restrict__ w,
+                                                             const T* __restrict__ th, const T* __restrict__ qv,
+                                                             const T* __restrict__ ql, const double* __restrict__ olbar,
+                                                             int has_mean, double* __restrict__ out) {
+  constexpr int NR = MGPU_PD_COUNT;
+  const int k = blockIdx.x + 1, nz = s.nz, st = nz + 2;
+  const Geo g{s.nx, s.ny, s.nz, s.plane};
+  auto P = [&](int id, int kk) { return s.prof[id * st + kk]; };
+  const bool moist = qv != nullptr;
+  double acc[NR];
+  for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+  const double ugal = s.ugal, vgal = s.vgal, thref = P(P_THREF, k);
+  const double thbar = olbar[2 * st + k];
+  const double umean = (k < nz && has_mean) ? 0.5 * (olbar[k] + olbar[k + 1]) : 0.0;
+  const double vmean = (k < nz && has_mean) ? 0.5 * (olbar[st + k] + olbar[st + k + 1]) : 0.0;
+  for (long long t = threadIdx.x; t < s.plane; t += blockDim.x) {
+    const int j = (int)(t / s.nx), i = (int)(t % s.nx);
+    const long long o = g.at(k, j, i);
+    const double w0 = (double)w[o], th0 = (double)th[o];
+    acc[MGPU_PD_U_WIND] += (double)u[o] + ugal;
+    acc[MGPU_PD_V_WIND] += (double)v[o] + vgal;
+    acc[MGPU_PD_WW] += w0 * w0;
+    if (k >= 2) {
+      acc[MGPU_PD_W_WIND] += w0;
+      acc[MGPU_PD_WWW] += w0 * w0 * w0;
+      acc[MGPU_PD_WWWW] += (w0 * w0) * (w0 * w0);
+    }
+    acc[MGPU_PD_THETA] += th0 + thref;
+    const double dth = th0 - thbar;
+    acc[MGPU_PD_TH2] += dth * dth;
+    if (k < nz) {
+      const long long o1 = o + s.plane;
+      if (k >= 2) acc[MGPU_PD_WTHETA_CN] += w0 * (0.5 * (th0 + (double)th[o1]));
+      double up = 0.25 * ((double)u[o] + (double)u[g.at(k, j, i - 1)] + (double)u[o1] + (double)u[g.at(k + 1, j, i - 1)]) + ugal;
+      up = up - umean;
+      acc[MGPU_PD_UW] += up * w0;
+      double vp = 0.25 * ((double)v[o] + (double)v[g.at(k, j - 1, i)] + (double)v[o1] + (double)v[g.at(k + 1, j - 1, i)]) + vgal;
+      vp = vp - vmean;
+      acc[MGPU_PD_VW] += vp * w0;
+    }
+    if (moist) {
+      const double q0 = (double)qv[o], l0 = (double)ql[o];
+      acc[MGPU_PD_VAPOUR] += q0;
+      acc[MGPU_PD_LIQUID] += l0;
+      if (k >= 2 && k < nz) {
+        acc[MGPU_PD_WQV_CN] += 0.5 * (q0 + (double)qv[o + s.plane]) * w0;
+        acc[MGPU_PD_WQL_CN] += 0.5 * (l0 + (double)ql[o + s.plane]) * w0;
+      }
+      const double tk = (th0 + thref) * P(P_RPREFRCP, k), pmb = P(P_PREFN, k) / 100.;
+      acc[MGPU_PD_RH] += q0 / qsaturation<double>(tk, pmb);
+    }
+  }
+  __shared__ double sh[256];
+  const int nrows = moist ? NR : MGPU_PD_VAPOUR;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    if (r >= nrows) break;  // uniform over the block
+    sh[threadIdx.x] = acc[r];
+    __syncthreads();
+    for (int wdt = 128; wdt > 0; wdt >>= 1) {
+      if (threadIdx.x < wdt) sh[threadIdx.x] += sh[threadIdx.x + wdt];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[(size_t)r * nz + k - 1] = sh[0];
+    __syncthreads();
+  }
+}
+
+template <typename T>
+int launch_profile_diagnostics(const Scalars& s, const T* u, const T* v, const T* w, const T* th, const T* qv,
+                               const T* ql, const double* olbar, bool has_mean, double* out, cudaStream_t st) {
+  k_profile_diagnostics<T><<<s.nz, 256, 0, st>>>(s, u, v, w, th, qv, ql, olbar, has_mean ? 1 : 0, out);
+  return 1;
+}
+template int launch_profile_diagnostics<float>(const Scalars&, const float*, const float*, const float*, const float*,
+                                               const float*, const float*, const double*, bool, double*, cudaStream_t);
+template int launch_profile_diagnostics<double>(const Scalars&, const double*, const double*, const double*,
+                                                const double*, const double*, const double*, const double*, bool,
+                                                double*, cudaStream_t);
 
 // subsidence tendencies of the mean profiles (forcing.F90:1052-1166 with the profiles olzubar,
 // olzvbar, olzthbar + thref and olzqbar), levels 2..nz: rows usub, vsub, thsub, qsub(n)

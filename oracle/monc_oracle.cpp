@@ -108,7 +108,7 @@ struct Model {
   int cfl_error = 0;
   // damping (damping.F90:19-21, grids.F90 dmpco/dmpcoz/kdmpmin), subsidence velocity (forcing.F90)
   // and the mean profiles they read (meanprofiles.F90, grids.F90 olz*bar)
-  Prof dmpco, dmpcoz, w_subs, olzubar, olzvbar, olzthbar;
+  Prof dmpco, dmpcoz, w_subs, olzubar, olzvbar, olzthbar, olubar, olvbar, olthbar;
   std::vector<Prof> olzqbar;
   int kdmpmin = 0;
 };
@@ -1561,6 +1561,7 @@ static void damping_and_forcing_init(Model& m) {
   const int nz = m.nz;
   m.dmpco.alloc(nz); m.dmpcoz.alloc(nz); m.w_subs.alloc(nz);
   m.olzubar.alloc(nz); m.olzvbar.alloc(nz); m.olzthbar.alloc(nz);
+  m.olubar.alloc(nz); m.olvbar.alloc(nz); m.olthbar.alloc(nz);
   m.olzqbar.assign(c.number_q_fields, Prof());
   for (Prof& p : m.olzqbar) p.alloc(nz);
   m.kdmpmin = nz + 1;
@@ -1581,7 +1582,7 @@ static void damping_and_forcing_init(Model& m) {
 
 static bool mean_profiles_enabled(const Model& m) {
   const mgpu_config& c = m.cfg;
-  return c.damping_enabled || c.l_subs_pl_theta || c.l_subs_pl_q;
+  return c.damping_enabled || c.l_subs_pl_theta || c.l_subs_pl_q || c.profile_diagnostics_enabled;
 }
 
 // calculate_mean_profiles: sums of zu, zv, zth, zq over the interior of each level (one rank)
@@ -1596,10 +1597,72 @@ static void mean_profiles(Model& m) {
       out(k) = sum * rnhpts;
     }
   };
+  mean(m.u, m.olubar);
   mean(m.zu, m.olzubar);
+  mean(m.v, m.olvbar);
   mean(m.zv, m.olzvbar);
+  mean(m.th, m.olthbar);
   mean(m.zth, m.olzthbar);
   for (int n = 0; n < m.cfg.number_q_fields; ++n) mean(m.zq[n], m.olzqbar[n]);
+}
+
+// profile_diagnostics (profile_diagnostics.F90:311-636) for PW flow and TVD scalars: the column
+// sums over the interior, from the current state and the last mean profiles (what the component
+// accumulates in the next step's dynamics group).  out: MGPU_PD_* rows of nz.
+static int profile_diagnostics(Model& m, double* out) {
+  halo_swapper(m);  // the next step's start group refreshes the halos before the dynamics group
+  const int nz = m.nz, nq = m.cfg.number_q_fields;
+  const bool moist = !m.cfg.passive_q && nq >= 2;
+  const int rows = moist ? MGPU_PD_COUNT : MGPU_PD_VAPOUR;
+  const bool has_mean = mean_profiles_enabled(m);
+  std::vector<double> tot((size_t)MGPU_PD_COUNT * (nz + 1), 0.0);
+  auto T = [&](int r, int k) -> double& { return tot[(size_t)r * (nz + 1) + k]; };
+  for (int x = m.xs; x <= m.xe; ++x)
+    for (int y = m.ys; y <= m.ye; ++y) {
+      for (int k = 1; k <= nz; ++k) {
+        T(MGPU_PD_U_WIND, k) = T(MGPU_PD_U_WIND, k) + (m.u(k, y, x) + m.ugal);
+        T(MGPU_PD_V_WIND, k) = T(MGPU_PD_V_WIND, k) + (m.v(k, y, x) + m.vgal);
+        T(MGPU_PD_WW, k) = T(MGPU_PD_WW, k) + m.w(k, y, x) * m.w(k, y, x);
+      }
+      for (int k = 2; k <= nz; ++k) {
+        const double w = m.w(k, y, x);
+        T(MGPU_PD_WWW, k) = T(MGPU_PD_WWW, k) + w * w * w;
+        T(MGPU_PD_WWWW, k) = T(MGPU_PD_WWWW, k) + (w * w) * (w * w);
+        T(MGPU_PD_W_WIND, k) = T(MGPU_PD_W_WIND, k) + w;
+      }
+      for (int k = 1; k <= nz - 1; ++k) {
+        double up = 0.25 * (m.u(k, y, x) + m.u(k, y, x - 1) + m.u(k + 1, y, x) + m.u(k + 1, y, x - 1)) + m.ugal;
+        if (has_mean) up = up - 0.5 * (m.olubar(k) + m.olubar(k + 1));
+        T(MGPU_PD_UW, k) = T(MGPU_PD_UW, k) + up * m.w(k, y, x);
+        double vp = 0.25 * (m.v(k, y, x) + m.v(k, y - 1, x) + m.v(k + 1, y, x) + m.v(k + 1, y - 1, x)) + m.vgal;
+        if (has_mean) vp = vp - 0.5 * (m.olvbar(k) + m.olvbar(k + 1));
+        T(MGPU_PD_VW, k) = T(MGPU_PD_VW, k) + vp * m.w(k, y, x);
+      }
+      for (int k = 1; k <= nz; ++k) {
+        T(MGPU_PD_THETA, k) = T(MGPU_PD_THETA, k) + (m.th(k, y, x) + m.thref(k));
+        const double d = m.th(k, y, x) - m.olthbar(k);
+        T(MGPU_PD_TH2, k) = T(MGPU_PD_TH2, k) + d * d;
+      }
+      for (int k = 2; k <= nz - 1; ++k)
+        T(MGPU_PD_WTHETA_CN, k) = T(MGPU_PD_WTHETA_CN, k) + m.w(k, y, x) * (0.5 * (m.th(k, y, x) + m.th(k + 1, y, x)));
+      if (moist) {
+        const Field &qv = m.q[m.iqv], &ql = m.q[m.iql];
+        for (int k = 1; k <= nz; ++k) {
+          T(MGPU_PD_VAPOUR, k) = T(MGPU_PD_VAPOUR, k) + qv(k, y, x);
+          T(MGPU_PD_LIQUID, k) = T(MGPU_PD_LIQUID, k) + ql(k, y, x);
+          const double exner = m.rprefrcp(k), pmb = m.prefn(k) / 100.;
+          const double tk = (m.th(k, y, x) + m.thref(k)) * exner;
+          T(MGPU_PD_RH, k) = T(MGPU_PD_RH, k) + qv(k, y, x) / qsaturation_(tk, pmb);
+        }
+        for (int k = 2; k <= nz - 1; ++k) {
+          T(MGPU_PD_WQV_CN, k) = T(MGPU_PD_WQV_CN, k) + 0.5 * (qv(k, y, x) + qv(k + 1, y, x)) * m.w(k, y, x);
+          T(MGPU_PD_WQL_CN, k) = T(MGPU_PD_WQL_CN, k) + 0.5 * (ql(k, y, x) + ql(k + 1, y, x)) * m.w(k, y, x);
+        }
+      }
+    }
+  for (int r = 0; r < rows; ++r)
+    for (int k = 1; k <= nz; ++k) out[(size_t)r * nz + k - 1] = T(r, k);
+  return rows;
 }
 
 static void damping_column(Model& m) {
@@ -1778,7 +1841,7 @@ Prof* profile_by_name(Model& m, const std::string& n) {
       {"prefn", &m.prefn}, {"prefrcp", &m.prefrcp}, {"rprefrcp", &m.rprefrcp}, {"tref", &m.tref},
       {"qsat", &m.qsat}, {"dqsatdt", &m.dqsatdt}, {"qsatfac", &m.qsatfac}, {"dmpco", &m.dmpco},
       {"dmpcoz", &m.dmpcoz}, {"w_subs", &m.w_subs}, {"olzubar", &m.olzubar}, {"olzvbar", &m.olzvbar},
-      {"olzthbar", &m.olzthbar}};
+      {"olzthbar", &m.olzthbar}, {"olubar", &m.olubar}, {"olvbar", &m.olvbar}, {"olthbar", &m.olthbar}};
   for (auto& t : tab)
     if (n == t.name) return t.p;
   return nullptr;
@@ -2220,6 +2283,8 @@ int orc_fft_c2c(int n, double* c, int sign) {
 }
 
 double orc_lookup_ustr(void* h, double vel) { return look(*(Model*)h, vel); }
+
+int orc_profile_diagnostics(void* h, double* out) { return profile_diagnostics(*(Model*)h, out); }
 
 // olzqbar(:, n) of the mean profiles, levels 1..nz
 int orc_mean_q_profile(void* h, int n, double* out) {

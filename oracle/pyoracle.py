@@ -54,6 +54,8 @@ def lib():
         L.orc_lookup_ustr.argtypes = [C.c_void_p, C.c_double]
         L.orc_mean_q_profile.restype = C.c_int
         L.orc_mean_q_profile.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_profile_diagnostics.restype = C.c_int
+        L.orc_profile_diagnostics.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_cfl_state.restype = C.c_int
         L.orc_cfl_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -107,13 +109,20 @@ class Oracle:
 
     def mean_profiles(self) -> dict:
         """olzubar, olzvbar, olzthbar and olzqbar(n) as the last mean_profiles left them."""
-        out = {n: self.profile(n) for n in ("olzubar", "olzvbar", "olzthbar")}
+        out = {n: self.profile(n) for n in ("olzubar", "olzvbar", "olzthbar", "olubar", "olvbar", "olthbar")}
         for n in range(self.cfg.number_q_fields):
             a = np.empty(self.nz, dtype=np.float64)
             if lib().orc_mean_q_profile(self.h, n, a.ctypes.data) != 0:
                 raise RuntimeError("orc_mean_q_profile")
             out[f"olzqbar{n}"] = a
         return out
+
+    def profile_diagnostics(self) -> dict:
+        """profile_diagnostics sums from the current state (MGPU_PD_* rows), by MONC's names."""
+        from monc_b200.api import PROFILE_DIAGNOSTICS
+        out = np.empty((len(PROFILE_DIAGNOSTICS), self.nz), dtype=np.float64)
+        rows = lib().orc_profile_diagnostics(self.h, out.ctypes.data)
+        return dict(zip(PROFILE_DIAGNOSTICS[:rows], out[:rows]))
 
     def profile(self, name: str) -> np.ndarray:
         a = np.empty(self.nz, dtype=np.float64)
