@@ -430,6 +430,14 @@ int mgpu_halo_unpack(mgpu_handle* h, int32_t set, int32_t depth, const void* d_l
  * (equal slabs: the mean of the slab means) before that phase. */
 int mgpu_slab_level_means(mgpu_handle* h, double* d_means);
 
+/* The mean profiles of a slab (mgpu_mean_profiles' rows; damping, subsidence and
+ * profile_diagnostics read them).  The dynamics phase leaves this slab's means; the driver
+ * fetches them into d_buf (put = 0: (6 + number_q_fields) rows of nz + 2 doubles on the device,
+ * olz*bar rows then olubar, olvbar, olthbar), averages them over the slabs (all slabs hold the
+ * same number of rows: the average is the domain mean) and puts the result back (put = 1)
+ * before the next dynamics phase. */
+int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put);
+
 /* x-FFT (fftsolver.F90:50-309 transforms, x pass) between the interior rows of p and d_spec,
  * which is split into nblocks (<= nx/2+1) blocks of consecutive wavenumbers dealt out as evenly
  * as possible: with b = (nx/2+1) / nblocks and r = (nx/2+1) % nblocks, block q has width

@@ -198,6 +198,8 @@ def lib():
         f.restype = C.c_int
     L.mgpu_slab_level_means.argtypes = [C.c_void_p, C.c_void_p]
     L.mgpu_slab_level_means.restype = C.c_int
+    L.mgpu_slab_mean_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    L.mgpu_slab_mean_profiles.restype = C.c_int
     L.mgpu_slab_fft_x.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
     L.mgpu_slab_fft_x.restype = C.c_int
     L.mgpu_slab_solve_columns.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
@@ -396,6 +398,9 @@ class Model:
 
     def slab_level_means(self, means: int):
         self._check(lib().mgpu_slab_level_means(self.h, means), "slab_level_means")
+
+    def slab_mean_profiles(self, buf: int, put: bool):
+        self._check(lib().mgpu_slab_mean_profiles(self.h, buf, 1 if put else 0), "slab_mean_profiles")
 
     def slab_fft_x(self, spec: int, nblocks: int, inverse: bool):
         self._check(lib().mgpu_slab_fft_x(self.h, spec, nblocks, 1 if inverse else 0), "slab_fft_x")

@@ -1130,12 +1130,12 @@ int mgpu_profile_diagnostics(mgpu_handle* h, double* out, int32_t* nrows) {
     DevState<float>& d = h->d32;
     h->launches += launch_profile_diagnostics<float>(h->sc, d.u, d.v, d.w, d.th, moist ? d.q[h->sc.iqv] : nullptr,
                                                      moist ? d.q[h->sc.iql] : nullptr, h->olbar_d, has_mean, h->pd_d,
-                                                     h->stream);
+                                                     h->stream, h->slab_halo);
   } else {
     DevState<double>& d = h->d64;
     h->launches += launch_profile_diagnostics<double>(h->sc, d.u, d.v, d.w, d.th, moist ? d.q[h->sc.iqv] : nullptr,
                                                       moist ? d.q[h->sc.iql] : nullptr, h->olbar_d, has_mean, h->pd_d,
-                                                      h->stream);
+                                                      h->stream, h->slab_halo);
   }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, h->pd_d, (size_t)rows * nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1211,6 +1211,8 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
                              : fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
       return MGPU_OK;
     case MGPU_PHASE_DYNAMICS:
+      forcing_flags(h);
+      h->launches += subsidence_tendencies(h);
       if (sizeof(T) == 4) {
         if (!h->bmean_ext)
           return fail(h, MGPU_ERR_ARGUMENT, "FP32-mixed slab: mgpu_slab_level_means must precede each dynamics phase");
@@ -1221,6 +1223,14 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
       h->sc.bmean = nullptr;
       h->bmean_ext = nullptr;
       swap_scalar_buffers<T>(d, h->cfg.number_q_fields);
+      if (needs_mean_profiles(h->cfg)) {
+        // this slab's means; the driver averages them across the slabs (mgpu_slab_mean_profiles)
+        const bool fwd = h->sc.forward != 0;
+        h->launches += launch_mean_profiles<T>(h->sc, d.zu_n, d.zv_n, d.th, d.q, h->olz_d, h->stream, h->slab_halo);
+        h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th_n, fwd ? nullptr : d.zth_n, h->sc.ugal,
+                                                     h->sc.vgal, 1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d,
+                                                     h->stream, h->slab_halo);
+      }
       if (exact_k) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
       else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
       h->launches += 1;
@@ -1281,9 +1291,6 @@ int mgpu_slab_init(mgpu_handle* h, int32_t ny_global, int32_t halo, int32_t max_
   if (h->cfg.solver != MGPU_SOLVER_EXTERNAL)
     return fail(h, MGPU_ERR_UNSUPPORTED, "a slab model is created with solver MGPU_SOLVER_EXTERNAL");
   if (h->slab.b1) return fail(h, MGPU_ERR_ARGUMENT, "slab already initialised");
-  if (h->cfg.damping_enabled || h->cfg.l_subs_pl_theta || h->cfg.l_subs_pl_q)
-    return fail(h, MGPU_ERR_UNSUPPORTED, "damping and subsidence on y-slabs are not supported (the mean profiles "
-                                         "would need a reduction across the slabs)");
   const int nyl = h->cfg.ny - 2 * halo, nxh = h->cfg.nx / 2 + 1;
   auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
   if (halo < 1 || nyl < 2 || nyl < halo || (nyl % 2) || !pow2(h->cfg.nx) || !pow2(ny_global) || nyl > ny_global ||
@@ -1342,6 +1349,23 @@ int mgpu_slab_level_means(mgpu_handle* h, double* d_means) {
   h->launches += 1;
   h->bmean_ext = d_means;
   return check_launch(h);
+}
+
+int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put) {
+  if (!h || !d_buf) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (!needs_mean_profiles(h->cfg))
+    return fail(h, MGPU_ERR_ARGUMENT, "no mean profiles are kept (no damping, mean-profile subsidence or profile diagnostics)");
+  const size_t row = (size_t)(h->cfg.nz + 2) * sizeof(double);
+  const size_t nz_rows = (size_t)(3 + h->cfg.number_q_fields) * row, bar = 3 * row;
+  if (put) {
+    CK(cudaMemcpyAsync(h->olz_d, d_buf, nz_rows, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->olbar_d, (const char*)d_buf + nz_rows, bar, cudaMemcpyDeviceToDevice, h->stream));
+  } else {
+    CK(cudaMemcpyAsync(d_buf, h->olz_d, nz_rows, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync((char*)d_buf + nz_rows, h->olbar_d, bar, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return MGPU_OK;
 }
 
 int mgpu_slab_fft_x(mgpu_handle* h, void* d_spec, int32_t nblocks, int32_t inverse) {

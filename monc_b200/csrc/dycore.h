@@ -97,17 +97,19 @@ int launch_cfl_gather(const Scalars& s, const DevState<T>& d, bool with_vis, dou
 // and the mean-profile subsidence tendencies (forcing.cu)
 template <typename T>
 int launch_mean_profiles(const Scalars& s, const T* zu, const T* zv, const T* th, const T* const* q, double* olz,
-                         cudaStream_t st);
+                         cudaStream_t st, int halo = 0);
 int launch_subsidence_tendencies(const Scalars& s, const double* olz, double* tend, bool flow_theta, bool q,
                                  cudaStream_t st);
 // olubar, olvbar, olthbar from u, v and theta (zth given: theta after time smoothing c1 th + c2 zth)
 template <typename T>
 int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth, double ugal,
-                               double vgal, double c1, double c2, double* olbar, cudaStream_t st);
-// profile_diagnostics sums into out (MGPU_PD_* rows of nz); qv, ql null for a dry model
+                               double vgal, double c1, double c2, double* olbar, cudaStream_t st, int halo = 0);
+// profile_diagnostics sums into out (MGPU_PD_* rows of nz); qv, ql null for a dry model.  With halo
+// > 0 (a y-slab) the means and sums run over the interior rows halo .. ny-1-halo
 template <typename T>
 int launch_profile_diagnostics(const Scalars& s, const T* u, const T* v, const T* w, const T* th, const T* qv,
-                               const T* ql, const double* olbar, bool has_mean, double* out, cudaStream_t st);
+                               const T* ql, const double* olbar, bool has_mean, double* out, cudaStream_t st,
+                               int halo = 0);
 
 // BiCGStab pressure solve (iterativesolver)
 struct IterSolverDev;

@@ -21,19 +21,20 @@ struct MeanFields {
   double a[3 + MGPU_MAX_Q], b[3 + MGPU_MAX_Q], c[3 + MGPU_MAX_Q];
 };
 
+// the level sums run over count points from row offset off of each plane (a slab's interior rows)
 template <typename T>
-__global__ void __launch_bounds__(256) k_plane_means(MeanFields<T> f, long long plane, double rnhpts, double* out,
-                                                     int stride) {
+__global__ void __launch_bounds__(256) k_plane_means(MeanFields<T> f, long long plane, long long off, long long count,
+                                                     double rnhpts, double* out, int stride) {
   const int k = blockIdx.x + 1, q = blockIdx.y;
-  const long long base = (long long)(k - 1) * plane;
+  const long long base = (long long)(k - 1) * plane + off;
   const T* __restrict__ p = f.p[q] + base;
   const T* __restrict__ p2 = f.p2[q] ? f.p2[q] + base : nullptr;
   const double a = f.a[q], b = f.b[q], c = f.c[q];
   double acc = 0.0;
   if (p2)
-    for (long long t = threadIdx.x; t < plane; t += blockDim.x) acc += a * (double)__ldg(p + t) + b * (double)__ldg(p2 + t);
+    for (long long t = threadIdx.x; t < count; t += blockDim.x) acc += a * (double)__ldg(p + t) + b * (double)__ldg(p2 + t);
   else
-    for (long long t = threadIdx.x; t < plane; t += blockDim.x) acc += c + (double)__ldg(p + t);
+    for (long long t = threadIdx.x; t < count; t += blockDim.x) acc += c + (double)__ldg(p + t);
   __shared__ double sh[256];
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -44,30 +45,34 @@ __global__ void __launch_bounds__(256) k_plane_means(MeanFields<T> f, long long 
   if (threadIdx.x == 0) out[q * stride + k] = sh[0] * rnhpts;
 }
 
-// rnhpts of meanprofiles.F90:44: the point count converted at default (single) precision
-static double rnhpts(const Scalars& s) { return 1.0 / (double)(float)((long long)s.nx * s.ny); }
+// rnhpts of meanprofiles.F90:44: the point count converted at default (single) precision; a
+// slab (halo rows above and below) averages its interior rows, which the slabs' driver averages
+// again across the slabs (all slabs hold the same number of rows)
+static long long interior(const Scalars& s, int halo) { return (long long)s.nx * (s.ny - 2 * halo); }
+static double rnhpts(const Scalars& s, int halo) { return 1.0 / (double)(float)interior(s, halo); }
 
 template <typename T>
 int launch_mean_profiles(const Scalars& s, const T* zu, const T* zv, const T* th, const T* const* q, double* olz,
-                         cudaStream_t st) {
+                         cudaStream_t st, int halo) {
   MeanFields<T> f{};
   f.p[0] = zu;
   f.p[1] = zv;
   f.p[2] = th;
   for (int n = 0; n < s.nq; ++n) f.p[3 + n] = q[n];
-  k_plane_means<T><<<dim3(s.nz, 3 + s.nq), 256, 0, st>>>(f, s.plane, rnhpts(s), olz, s.nz + 2);
+  k_plane_means<T><<<dim3(s.nz, 3 + s.nq), 256, 0, st>>>(f, s.plane, (long long)halo * s.nx, interior(s, halo),
+                                                         rnhpts(s, halo), olz, s.nz + 2);
   return 1;
 }
 template int launch_mean_profiles<float>(const Scalars&, const float*, const float*, const float*, const float* const*,
-                                         double*, cudaStream_t);
+                                         double*, cudaStream_t, int);
 template int launch_mean_profiles<double>(const Scalars&, const double*, const double*, const double*,
-                                          const double* const*, double*, cudaStream_t);
+                                          const double* const*, double*, cudaStream_t, int);
 
 // olubar, olvbar, olthbar: the means of ugal + u, vgal + v and of theta, with zth (time
 // smoothing c1 th + c2 zth) when given
 template <typename T>
 int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth, double ugal,
-                               double vgal, double c1, double c2, double* olbar, cudaStream_t st) {
+                               double vgal, double c1, double c2, double* olbar, cudaStream_t st, int halo) {
   MeanFields<T> f{};
   f.p[0] = u;
   f.c[0] = ugal;
@@ -77,13 +82,15 @@ int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T
   f.p2[2] = zth;
   f.a[2] = c1;
   f.b[2] = c2;
-  k_plane_means<T><<<dim3(s.nz, 3), 256, 0, st>>>(f, s.plane, rnhpts(s), olbar, s.nz + 2);
+  k_plane_means<T><<<dim3(s.nz, 3), 256, 0, st>>>(f, s.plane, (long long)halo * s.nx, interior(s, halo),
+                                                  rnhpts(s, halo), olbar, s.nz + 2);
   return 1;
 }
 template int launch_mean_profiles_state<float>(const Scalars&, const float*, const float*, const float*, const float*,
-                                               double, double, double, double, double*, cudaStream_t);
+                                               double, double, double, double, double*, cudaStream_t, int);
 template int launch_mean_profiles_state<double>(const Scalars&, const double*, const double*, const double*,
-                                                const double*, double, double, double, double, double*, cudaStream_t);
+                                                const double*, double, double, double, double, double*, cudaStream_t,
+                                                int);
 
 // profile_diagnostics (profile_diagnostics.F90:311-636, PW flow and TVD scalars): one block per
 // level sums the MGPU_PD_* quantities over the plane in FP64, in a fixed order
@@ -92,7 +99,7 @@ __global__ void __launch_bounds__(256) k_profile_diagnostics(Scalars s, const T*
                                                              const T* __restrict__ v, const T* __restrict__ w,
                                                              const T* __restrict__ th, const T* __restrict__ qv,
                                                              const T* __restrict__ ql, const double* __restrict__ olbar,
-                                                             int has_mean, double* __restrict__ out) {
+                                                             int has_mean, int halo, double* __restrict__ out) {
   constexpr int NR = MGPU_PD_COUNT;
   const int k = blockIdx.x + 1, nz = s.nz, st = nz + 2;
   const Geo g{s.nx, s.ny, s.nz, s.plane};
@@ -104,8 +111,9 @@ __global__ void __launch_bounds__(256) k_profile_diagnostics(Scalars s, const T*
   const double thbar = olbar[2 * st + k];
   const double umean = (k < nz && has_mean) ? 0.5 * (olbar[k] + olbar[k + 1]) : 0.0;
   const double vmean = (k < nz && has_mean) ? 0.5 * (olbar[st + k] + olbar[st + k + 1]) : 0.0;
-  for (long long t = threadIdx.x; t < s.plane; t += blockDim.x) {
-    const int j = (int)(t / s.nx), i = (int)(t % s.nx);
+  const long long count = (long long)s.nx * (s.ny - 2 * halo);
+  for (long long t = threadIdx.x; t < count; t += blockDim.x) {
+    const int j = halo + (int)(t / s.nx), i = (int)(t % s.nx);
     const long long o = g.at(k, j, i);
     const double w0 = (double)w[o], th0 = (double)th[o];
     acc[MGPU_PD_U_WIND] += (double)u[o] + ugal;
@@ -159,15 +167,17 @@ __global__ void __launch_bounds__(256) k_profile_diagnostics(Scalars s, const T*
 
 template <typename T>
 int launch_profile_diagnostics(const Scalars& s, const T* u, const T* v, const T* w, const T* th, const T* qv,
-                               const T* ql, const double* olbar, bool has_mean, double* out, cudaStream_t st) {
-  k_profile_diagnostics<T><<<s.nz, 256, 0, st>>>(s, u, v, w, th, qv, ql, olbar, has_mean ? 1 : 0, out);
+                               const T* ql, const double* olbar, bool has_mean, double* out, cudaStream_t st,
+                               int halo) {
+  k_profile_diagnostics<T><<<s.nz, 256, 0, st>>>(s, u, v, w, th, qv, ql, olbar, has_mean ? 1 : 0, halo, out);
   return 1;
 }
 template int launch_profile_diagnostics<float>(const Scalars&, const float*, const float*, const float*, const float*,
-                                               const float*, const float*, const double*, bool, double*, cudaStream_t);
+                                               const float*, const float*, const double*, bool, double*, cudaStream_t,
+                                               int);
 template int launch_profile_diagnostics<double>(const Scalars&, const double*, const double*, const double*,
                                                 const double*, const double*, const double*, const double*, bool,
-                                                double*, cudaStream_t);
+                                                double*, cudaStream_t, int);
 
 // subsidence tendencies of the mean profiles (forcing.F90:1052-1166 with the profiles olzubar,
 // olzvbar, olzthbar + thref and olzqbar), levels 2..nz: rows usub, vsub, thsub, qsub(n)

@@ -143,6 +143,10 @@ class LoopbackComm:
     def gather_rows(self, parts):
         return parts
 
+    def allreduce_sum(self, t: torch.Tensor) -> torch.Tensor:
+        """Every slab is local: the local sum is the total."""
+        return t
+
 
 class TorchComm:
     """One slab per process over torch.distributed; collectives run on `stream` (the model's)."""
@@ -199,6 +203,15 @@ class TorchComm:
             dist.all_reduce(bufs[0], group=self.group)
             bufs[0].div_(self.size)
 
+    def allreduce_sum(self, t: torch.Tensor) -> torch.Tensor:
+        """Sum of a host tensor over the ranks (on the device for NCCL)."""
+        dev = t.device
+        if dist.get_backend(self.group) == "nccl":
+            t = t.to(torch.device("cuda", torch.cuda.current_device()))
+        with self._ctx():
+            dist.all_reduce(t, group=self.group)
+        return t.to(dev)
+
     def gather_rows(self, parts):
         with self._ctx():
             out = [torch.empty_like(parts[0]) for _ in range(self.size)]
@@ -220,6 +233,8 @@ class _Slab:
         self.state_bufs = [torch.zeros(nf * g.nz * g.halo * g.nx, dtype=dtype, device=device) for _ in range(4)]
         self.p_bufs = [torch.zeros(g.nz * g.nx, dtype=dtype, device=device) for _ in range(4)]
         self.means = torch.zeros((1 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
+        # the mean profiles damping, subsidence and profile_diagnostics read (mgpu_slab_mean_profiles)
+        self.profiles = torch.zeros((6 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
 
         def cview(buf, off, n):
             return buf[2 * off:2 * (off + n)]
@@ -237,12 +252,14 @@ class SlabDomain:
         if cfg.cfl_enabled:
             raise ValueError("cfltest on a decomposed domain needs its extrema reduced across the slabs; "
                              "run the slabs at a fixed dtm (cfl_enabled = 0)")
-        if cfg.damping_enabled or cfg.l_subs_pl_theta or cfg.l_subs_pl_q:
-            raise ValueError("damping and subsidence on a decomposed domain need the mean profiles reduced "
-                             "across the slabs; not supported")
         self.cfg = cfg
         self.comm = comm
         self.geo = SlabGeometry(cfg.nx, cfg.ny, cfg.nz, comm.size, halo)
+        # the library keeps the mean profiles when damping, mean-profile subsidence or
+        # profile_diagnostics reads them
+        self.mean_profiles = bool(cfg.damping_enabled or cfg.profile_diagnostics_enabled
+                                  or (cfg.l_subs_pl_theta and not cfg.subsidence_local_theta)
+                                  or (cfg.l_subs_pl_q and not cfg.subsidence_local_q and cfg.number_q_fields > 0))
         g = self.geo
         self.fp32 = cfg.precision == cf.FP32_MIXED
         dtype = torch.float32 if self.fp32 else torch.float64
@@ -314,6 +331,13 @@ class SlabDomain:
             for s in self.slabs:
                 s.m.step_phase(cf.PHASE_DYNAMICS)
                 s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, False)
+            if self.mean_profiles:
+                # each slab's means of this step, averaged over the slabs for the next step
+                for s in self.slabs:
+                    s.m.slab_mean_profiles(s.profiles.data_ptr(), False)
+                self.comm.allreduce_mean([s.profiles for s in self.slabs])
+                for s in self.slabs:
+                    s.m.slab_mean_profiles(s.profiles.data_ptr(), True)
             self.comm.all_to_all([s.x_blocks for s in self.slabs], [s.t_blocks for s in self.slabs])
             for s in self.slabs:
                 k0, w = g.blocks[s.rank]
@@ -324,6 +348,17 @@ class SlabDomain:
             self._exchange(cf.HALO_PRESSURE, 1)
             for s in self.slabs:
                 s.m.step_phase(cf.PHASE_PSTEP)
+
+    def profile_diagnostics(self) -> dict:
+        """profile_diagnostics sums over the whole domain: each slab's totals over its interior rows
+        (MONC's <name>_total_local of one rank), summed over the slabs.  The sums read the row
+        below each interior row, so the state halos are exchanged first."""
+        self._exchange(cf.HALO_STATE, self.geo.halo)
+        parts = [s.m.profile_diagnostics() for s in self.slabs]
+        names = list(parts[0])
+        local = torch.tensor(np.stack([sum(p[n] for p in parts) for n in names]), dtype=torch.float64)
+        total = self.comm.allreduce_sum(local)
+        return dict(zip(names, total.numpy()))
 
     def synchronize(self):
         for s in self.slabs:

@@ -6,6 +6,8 @@ after all queued work has finished; no kernel waits on another slab).
   bit, dry and moist, on the forward and centred steps; and both agree with the CPU oracle.
 * Default (contracted) FP64 arithmetic and FP32-mixed: the decomposed run tracks the
   single-domain run (FP32-mixed differs by the order in which the level means are summed).
+* Damping, mean-profile subsidence and profile_diagnostics on the slabs: the mean profiles
+  averaged over the slabs and the diagnostics sums added over them match the single domain.
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
 import os
@@ -118,6 +120,77 @@ def test_fp32_mixed_slabs_track_single_domain(gpu_lib):
         assert np.abs(got[f].mean(axis=(1, 2)) - ref[f].mean(axis=(1, 2))).max() <= 1e-6 * scale, f
 
 
+def forced_setup(precision=cf.FP64, moist=False):
+    """Damping above 300 m, subsidence from the mean profiles and profile_diagnostics on."""
+    if moist:
+        c, st = moist_setup(precision)
+        cf.enable_subsidence(c, [0.0, 1000.0], [0.0, -0.005], theta=True, q=True)
+    else:
+        c, st = dry_config(precision), dry_state()
+        cf.enable_subsidence(c, [0.0, 200.0, 450.0, 700.0], [0.0, -0.003, -0.005, -0.004], theta=True)
+        zn = api.reference_profile(c, "zn")
+        for f in ("th", "zth"):
+            st[f] = st[f] + 0.004 * zn[:, None, None]
+    cf.enable_damping(c, 0.02, 300.0, 150.0)
+    c.profile_diagnostics_enabled = 1
+    return c, st
+
+
+@pytest.mark.parametrize("nranks", [2, 4])
+@pytest.mark.parametrize("moist", [False, True], ids=["dry", "moist"])
+def test_damping_subsidence_and_diagnostics_on_slabs(gpu_lib, nranks, moist):
+    """Damping and mean-profile subsidence read the domain mean profiles (the slabs' means
+    averaged by the driver), and the profile_diagnostics sums add up over the slabs: five steps
+    (damping and forcing act from the third) match the single domain to rounding, the order of
+    the level sums being the only difference."""
+    c, st = forced_setup(moist=moist)
+    fields = STATE + (["q0", "q1", "zq0", "zq1"] if moist else [])
+    m = api.Model(c)
+    m.set_state(st)
+    m.step(5)
+    ref = {f: m.download(f) for f in fields}
+    ref_pd, ref_mp = m.profile_diagnostics(), m.mean_profiles()
+    m.close()
+    d = dc.SlabDomain(c, dc.LoopbackComm(nranks))
+    d.set_state(st)
+    d.step(5)
+    for f in fields:
+        assert np.abs(d.download(f) - ref[f]).max() <= 1e-11 * np.abs(ref[f]).max(), f
+    got_mp = d.slabs[0].m.mean_profiles()
+    for n in ref_mp:
+        assert np.abs(got_mp[n] - ref_mp[n]).max() <= 1e-12 * max(np.abs(ref_mp[n]).max(), 1e-30), n
+    got_pd = d.profile_diagnostics()
+    assert set(got_pd) == set(ref_pd)
+    for n in ref_pd:
+        scale = np.abs(ref_pd[n]).max()
+        if n == "w_wind_total_local":  # sums to zero by continuity: scale by the sum of |w|
+            scale = NX * NY * np.abs(ref["w"]).max()
+        assert np.abs(got_pd[n] - ref_pd[n]).max() <= 1e-11 * max(scale, 1e-30), n
+    d.close()
+
+
+def test_slab_forcing_is_live(gpu_lib):
+    """The slab run with damping and subsidence ends elsewhere than the one without."""
+    c, st = forced_setup()
+    out = []
+    for cfg in (c, dry_config()):
+        d = dc.SlabDomain(cfg, dc.LoopbackComm(2))
+        d.set_state(st)
+        d.step(5)
+        out.append(d.download("th"))
+        d.close()
+    assert np.abs(out[0] - out[1]).max() > 1e-8 * np.abs(out[1]).max()
+
+
+def test_fp32_mixed_forced_slabs_track_single_domain(gpu_lib):
+    c, st = forced_setup(cf.FP32_MIXED, moist=True)
+    fields = ["th", "w", "q0", "q1"]
+    ref = run_single(c, st, 5, fields)
+    got = run_slabs(c, st, 5, 4, fields)
+    for f in fields:
+        assert np.abs(got[f] - ref[f]).max() <= 1e-5 * np.abs(ref[f]).max(), f
+
+
 def test_halo_rows_pack_and_unpack(gpu_lib):
     """Pack takes the first and last `depth` interior rows, unpack writes the rows just outside."""
     halo, nyl = 4, 16
@@ -223,6 +296,14 @@ def test_slab_entry_points_check_arguments(gpu_lib):
     m.step_phase(cf.PHASE_SUBGRID)
     with pytest.raises(api.MgpuError):
         m.step_phase(cf.PHASE_DYNAMICS)  # FP32-mixed needs the domain level means first
+    m.close()
+    c = dry_config()
+    c.ny = 24
+    c.solver = cf.SOLVER_EXTERNAL
+    m = api.Model(c)
+    m.slab_init(64, 4, 9)
+    with pytest.raises(api.MgpuError):
+        m.slab_mean_profiles(buf.data_ptr(), False)  # no damping, subsidence or diagnostics: no profiles
     m.close()
     plain = api.Model(dry_config())
     with pytest.raises(api.MgpuError):
