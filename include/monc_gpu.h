@@ -438,6 +438,16 @@ int mgpu_slab_level_means(mgpu_handle* h, double* d_means);
  * before the next dynamics phase. */
 int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put);
 
+/* cfltest on slabs (cfltest.F90:62-128; MONC reduces the same extrema across its ranks with
+ * MPI_MIN/MPI_MAX in get_global_values, cfltest.F90:184-264).  On an evaluation step the
+ * subgrid phase gathers this slab's extrema over its interior rows; put = 0 then writes them to
+ * d_buf (6 doubles on the device: -min zu, max zu, -min zv, max zv, max |zw| rdzn, max of the
+ * viscous term -- every entry combined by a maximum), the driver all-reduces d_buf with a
+ * maximum over the slabs, and put = 1 hands the result back before the pressure-step phase,
+ * which runs cfltest and sets the next step's dtm.  *gathered (may be NULL) says whether this
+ * step gathered; on other steps the call does nothing, and every slab takes the same steps. */
+int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* gathered);
+
 /* x-FFT (fftsolver.F90:50-309 transforms, x pass) between the interior rows of p and d_spec,
  * which is split into nblocks (<= nx/2+1) blocks of consecutive wavenumbers dealt out as evenly
  * as possible: with b = (nx/2+1) / nblocks and r = (nx/2+1) % nblocks, block q has width

@@ -200,6 +200,8 @@ def lib():
     L.mgpu_slab_level_means.restype = C.c_int
     L.mgpu_slab_mean_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
     L.mgpu_slab_mean_profiles.restype = C.c_int
+    L.mgpu_slab_cfl_extrema.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+    L.mgpu_slab_cfl_extrema.restype = C.c_int
     L.mgpu_slab_fft_x.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
     L.mgpu_slab_fft_x.restype = C.c_int
     L.mgpu_slab_solve_columns.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
@@ -401,6 +403,13 @@ class Model:
 
     def slab_mean_profiles(self, buf: int, put: bool):
         self._check(lib().mgpu_slab_mean_profiles(self.h, buf, 1 if put else 0), "slab_mean_profiles")
+
+    def slab_cfl_extrema(self, buf: int, put: bool) -> bool:
+        """Fetch (put=False) or hand back (put=True) this slab's cfltest extrema in max form;
+        returns whether this step gathered them."""
+        g = C.c_int32(0)
+        self._check(lib().mgpu_slab_cfl_extrema(self.h, buf, 1 if put else 0, C.byref(g)), "slab_cfl_extrema")
+        return bool(g.value)
 
     def slab_fft_x(self, spec: int, nblocks: int, inverse: bool):
         self._check(lib().mgpu_slab_fft_x(self.h, spec, nblocks, 1 if inverse else 0), "slab_fft_x")

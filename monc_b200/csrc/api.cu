@@ -74,6 +74,7 @@ struct mgpu_handle {
   struct {
     int last_cfl_timestep = 0, evaluations = 0;
     bool update_dtm = false;
+    bool gathered = false;  // y-slab: this step's subgrid phase gathered the slab's extrema
     double dtm_new = 0.0, absolute_new_dtm = 0.0, dtm_last = 0.0;
     double cvel = 0.0, cvis = 0.0, cfl_number = 0.0, cvel_x = 0.0, cvel_y = 0.0, cvel_z = 0.0;
     double* part_d = nullptr;  // CFL_BLOCKS*6 block partials
@@ -250,7 +251,7 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
       (cfg->solver == MGPU_SOLVER_FFT && (!pow2(cfg->nx) || !pow2(cfg->ny))) || !(cfg->dtm > 0.0))
     return MGPU_ERR_ARGUMENT;
   if (cfg->cfl_enabled && (cfg->cfl_frequency < 1 || !(cfg->cfl_cvismax > 0.0) || !(cfg->cfl_cvelmax > 0.0) ||
-                           !(cfg->cfl_dtmmax > 0.0) || cfg->cfl_rincmax < 0.0 || cfg->solver == MGPU_SOLVER_EXTERNAL))
+                           !(cfg->cfl_dtmmax > 0.0) || cfg->cfl_rincmax < 0.0))
     return MGPU_ERR_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MGPU_ERR_NO_DEVICE;
@@ -1206,10 +1207,18 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
   h->sc.forward = (h->timestep == 1) ? 1 : 0;  // steppingdirection.F90:44-48
   const bool exact_k = h->cfg.reproducible != 0;
   switch (phase) {
-    case MGPU_PHASE_SUBGRID:
+    case MGPU_PHASE_SUBGRID: {
+      const bool cfl = h->cfg.cfl_enabled != 0;
+      if (cfl && h->cfl.update_dtm) h->sc.dtm = h->cfl.dtm_new;  // monc.F90:313
+      h->cfl.gathered = cfl && cfl_evaluation_step(h, h->timestep);
       h->launches += exact_k ? exact::launch_fused_subgrid<T>(h->sc, d, h->stream)
                              : fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
+      // this slab's extrema; the driver combines them across the slabs (mgpu_slab_cfl_extrema)
+      if (h->cfl.gathered)
+        h->launches += launch_cfl_gather<T>(h->sc, d, h->cfg.use_viscosity_and_diffusion != 0, h->cfl.part_d,
+                                            h->cfl.out_d, h->stream, h->slab_halo);
       return MGPU_OK;
+    }
     case MGPU_PHASE_DYNAMICS:
       forcing_flags(h);
       h->launches += subsidence_tendencies(h);
@@ -1239,6 +1248,15 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
       if (exact_k) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
       else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
       h->launches += 1;
+      if (h->cfg.cfl_enabled) {
+        const bool gathered = h->cfl.gathered;
+        h->cfl.gathered = false;
+        if (gathered) {
+          CK(cudaMemcpyAsync(h->cfl.out_h, h->cfl.out_d, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+          CK(cudaEventRecord(h->cfl.ev, h->stream));
+        }
+        if (int rc = cfltest_callback(h, gathered)) return rc;
+      }
       h->time += h->sc.dtm;
       h->timestep += 1;
       return MGPU_OK;
@@ -1368,6 +1386,17 @@ int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put) {
   return MGPU_OK;
 }
 
+int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* gathered) {
+  if (!h || !d_buf) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (!h->cfg.cfl_enabled) return fail(h, MGPU_ERR_ARGUMENT, "cfltest is off");
+  if (gathered) *gathered = h->cfl.gathered ? 1 : 0;
+  if (!h->cfl.gathered) return MGPU_OK;  // not an evaluation step: nothing to combine
+  h->launches += put ? launch_cfl_max_form(d_buf, h->cfl.out_d, h->stream)
+                     : launch_cfl_max_form(h->cfl.out_d, d_buf, h->stream);
+  return check_launch(h);
+}
+
 int mgpu_slab_fft_x(mgpu_handle* h, void* d_spec, int32_t nblocks, int32_t inverse) {
   if (!h || !d_spec) return MGPU_ERR_ARGUMENT;
   if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
@@ -1394,8 +1423,10 @@ int mgpu_slab_solve_columns(mgpu_handle* h, void* d_spec, int32_t kx0, int32_t n
 int mgpu_cfl_gather(mgpu_handle* h, double* out) {
   if (!h || !out) return MGPU_ERR_ARGUMENT;
   const bool vd = h->cfg.use_viscosity_and_diffusion != 0;
-  if (h->fp32) h->launches += launch_cfl_gather<float>(h->sc, h->d32, vd, h->cfl.part_d, h->cfl.out_d, h->stream);
-  else h->launches += launch_cfl_gather<double>(h->sc, h->d64, vd, h->cfl.part_d, h->cfl.out_d, h->stream);
+  if (h->fp32)
+    h->launches += launch_cfl_gather<float>(h->sc, h->d32, vd, h->cfl.part_d, h->cfl.out_d, h->stream, h->slab_halo);
+  else
+    h->launches += launch_cfl_gather<double>(h->sc, h->d64, vd, h->cfl.part_d, h->cfl.out_d, h->stream, h->slab_halo);
   if (cudaMemcpyAsync(out, h->cfl.out_d, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
       cudaStreamSynchronize(h->stream) != cudaSuccess)
     return fail(h, MGPU_ERR_CUDA, "cfl gather");

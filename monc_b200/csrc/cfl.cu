@@ -23,14 +23,17 @@ template <typename T>
 __global__ void __launch_bounds__(CFL_THREADS) k_cfl_partial(Scalars s, const T* __restrict__ zu,
                                                              const T* __restrict__ zv, const T* __restrict__ zw,
                                                              const T* __restrict__ vis, const T* __restrict__ diff,
-                                                             int with_vis, double* __restrict__ part) {
+                                                             int with_vis, int halo, double* __restrict__ part) {
   const double* rdzn = s.prof + P_RDZN * (s.nz + 2);
   double r0 = DBL_MAX, r1 = -DBL_MAX, r2 = DBL_MAX, r3 = -DBL_MAX, r4 = 0.0, r5 = 0.0;
-  const long long n = (long long)(s.nz - 1) * s.plane;  // levels 2..nz
+  // levels 2..nz of the rows halo..ny-halo-1 (a y-slab leaves its halo rows to its neighbours)
+  const long long rows = (long long)(s.ny - 2 * halo) * s.nx;
+  const long long n = (long long)(s.nz - 1) * rows;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-    const long long o = s.plane + t;
-    const int k = (int)(o / s.plane) + 1;
+    const long long lev = t / rows;
+    const long long o = (lev + 1) * s.plane + (long long)halo * s.nx + (t - lev * rows);
+    const int k = (int)lev + 2;
     const double u = (double)zu[o], v = (double)zv[o];
     r0 = u < r0 ? u : r0;
     r1 = u > r1 ? u : r1;
@@ -91,15 +94,30 @@ __global__ void __launch_bounds__(CFL_THREADS) k_cfl_final(const double* __restr
   if (t < 6) out[t] = sh[t][0];
 }
 
+// The six values in the form a maximum reduces: the minima negated (negation is exact, so
+// -max(-a, -b) = min(a, b)).  Its own inverse.
+__global__ void k_cfl_max_form(const double* __restrict__ src, double* __restrict__ dst) {
+  const int q = threadIdx.x;
+  if (q < 6) dst[q] = (q == 0 || q == 2) ? -src[q] : src[q];
+}
+
 template <typename T>
 int launch_cfl_gather(const Scalars& s, const DevState<T>& d, bool with_vis, double* part, double* out,
-                      cudaStream_t st) {
-  k_cfl_partial<T><<<CFL_BLOCKS, CFL_THREADS, 0, st>>>(s, d.zu, d.zv, d.zw, d.vis, d.diff, with_vis ? 1 : 0, part);
+                      cudaStream_t st, int halo) {
+  k_cfl_partial<T><<<CFL_BLOCKS, CFL_THREADS, 0, st>>>(s, d.zu, d.zv, d.zw, d.vis, d.diff, with_vis ? 1 : 0, halo,
+                                                       part);
   k_cfl_final<<<1, CFL_THREADS, 0, st>>>(part, CFL_BLOCKS, out);
   return 2;
 }
 
-template int launch_cfl_gather<double>(const Scalars&, const DevState<double>&, bool, double*, double*, cudaStream_t);
-template int launch_cfl_gather<float>(const Scalars&, const DevState<float>&, bool, double*, double*, cudaStream_t);
+int launch_cfl_max_form(const double* src, double* dst, cudaStream_t st) {
+  k_cfl_max_form<<<1, 32, 0, st>>>(src, dst);
+  return 1;
+}
+
+template int launch_cfl_gather<double>(const Scalars&, const DevState<double>&, bool, double*, double*, cudaStream_t,
+                                       int);
+template int launch_cfl_gather<float>(const Scalars&, const DevState<float>&, bool, double*, double*, cudaStream_t,
+                                      int);
 
 }  // namespace mgpu

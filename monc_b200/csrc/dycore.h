@@ -91,7 +91,9 @@ void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_t
 constexpr int CFL_BLOCKS = 296;
 template <typename T>
 int launch_cfl_gather(const Scalars& s, const DevState<T>& d, bool with_vis, double* part, double* out,
-                      cudaStream_t st);
+                      cudaStream_t st, int halo = 0);
+// src -> dst with the two minima negated (the form a maximum all-reduce combines); its own inverse
+int launch_cfl_max_form(const double* src, double* dst, cudaStream_t st);
 
 // mean profiles (olzubar, olzvbar, olzthbar, olzqbar) of zu, zv, th and q into olz (rows of nz+2),
 // and the mean-profile subsidence tendencies (forcing.cu)

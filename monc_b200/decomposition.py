@@ -140,6 +140,15 @@ class LoopbackComm:
             b.copy_(total)
         self._sync(bufs[0])
 
+    def allreduce_max(self, bufs):
+        self._sync(bufs[0])
+        top = bufs[0].clone()
+        for b in bufs[1:]:
+            torch.maximum(top, b, out=top)
+        for b in bufs:
+            b.copy_(top)
+        self._sync(bufs[0])
+
     def gather_rows(self, parts):
         return parts
 
@@ -203,6 +212,10 @@ class TorchComm:
             dist.all_reduce(bufs[0], group=self.group)
             bufs[0].div_(self.size)
 
+    def allreduce_max(self, bufs):
+        with self._ctx():
+            dist.all_reduce(bufs[0], op=dist.ReduceOp.MAX, group=self.group)
+
     def allreduce_sum(self, t: torch.Tensor) -> torch.Tensor:
         """Sum of a host tensor over the ranks (on the device for NCCL)."""
         dev = t.device
@@ -235,6 +248,8 @@ class _Slab:
         self.means = torch.zeros((1 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
         # the mean profiles damping, subsidence and profile_diagnostics read (mgpu_slab_mean_profiles)
         self.profiles = torch.zeros((6 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
+        # cfltest's six extrema, every one combined by a maximum (mgpu_slab_cfl_extrema)
+        self.cfl = torch.zeros(6, dtype=torch.float64, device=device)
 
         def cview(buf, off, n):
             return buf[2 * off:2 * (off + n)]
@@ -249,9 +264,6 @@ class SlabDomain:
     solver SOLVER_EXTERNAL on `device`.  Fields move in and out as global [nz][ny][nx] arrays."""
 
     def __init__(self, cfg: cf.MgpuConfig, comm, halo: int = 4, device=None):
-        if cfg.cfl_enabled:
-            raise ValueError("cfltest on a decomposed domain needs its extrema reduced across the slabs; "
-                             "run the slabs at a fixed dtm (cfl_enabled = 0)")
         self.cfg = cfg
         self.comm = comm
         self.geo = SlabGeometry(cfg.nx, cfg.ny, cfg.nz, comm.size, halo)
@@ -324,6 +336,13 @@ class SlabDomain:
             self._exchange(cf.HALO_STATE, g.halo)
             for s in self.slabs:
                 s.m.step_phase(cf.PHASE_SUBGRID)
+            if self.cfg.cfl_enabled:
+                # on cfltest's evaluation steps (the same on every slab) the domain extrema
+                gathered = [s.m.slab_cfl_extrema(s.cfl.data_ptr(), False) for s in self.slabs]
+                if gathered[0]:
+                    self.comm.allreduce_max([s.cfl for s in self.slabs])
+                    for s in self.slabs:
+                        s.m.slab_cfl_extrema(s.cfl.data_ptr(), True)
             if self.fp32:
                 for s in self.slabs:
                     s.m.slab_level_means(s.means.data_ptr())

@@ -8,6 +8,8 @@ after all queued work has finished; no kernel waits on another slab).
   single-domain run (FP32-mixed differs by the order in which the level means are summed).
 * Damping, mean-profile subsidence and profile_diagnostics on the slabs: the mean profiles
   averaged over the slabs and the diagnostics sums added over them match the single domain.
+* cfltest on the slabs: the extrema combined by a maximum give the single domain's dtm sequence,
+  and the fields of the adaptive-dtm run bit for bit.
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
 import os
@@ -191,6 +193,69 @@ def test_fp32_mixed_forced_slabs_track_single_domain(gpu_lib):
         assert np.abs(got[f] - ref[f]).max() <= 1e-5 * np.abs(ref[f]).max(), f
 
 
+CFL_KEYS = ["dtm", "dtm_new", "absolute_new_dtm", "cvel", "cvis", "cfl_number", "cvel_x", "cvel_y", "cvel_z",
+            "cfl_evaluations", "last_cfl_timestep", "timestep"]
+
+
+def cfl_setup(precision=cf.FP64, **kw):
+    c = dry_config(precision)
+    c.dtm = 1.0
+    cf.enable_cfl(c, **kw)
+    st = ini.random_flow_state(NX, NY, NZ, seed=3, amp_uv=2.0, amp_w=0.5, ug=5.0)
+    return c, st
+
+
+@pytest.mark.parametrize("nranks", [2, 4])
+def test_cfl_on_slabs_bit_identical(gpu_lib, nranks):
+    """cfltest on slabs: each slab's extrema over its interior rows, combined by a maximum across
+    the slabs (exact in any order), give the single domain's Courant numbers and dtm sequence, and
+    the steps of varying dtm end bit for bit where the single domain's do."""
+    c, st = cfl_setup(frequency=3, dtmmax=2.0)
+    m = api.Model(c)
+    m.set_state(st)
+    d = dc.SlabDomain(c, dc.LoopbackComm(nranks))
+    d.set_state(st)
+    changed = 0
+    for n in range(10):
+        m.step(1)
+        d.step(1)
+        ref = m.reductions()
+        for s in d.slabs:
+            got = s.m.reductions()
+            for k in CFL_KEYS:
+                assert getattr(got, k) == getattr(ref, k), (n, k)
+        changed += ref.dtm != c.dtm
+    assert changed > 0  # the timestep did change
+    for f in STATE + ["p"]:
+        np.testing.assert_array_equal(d.download(f), m.download(f), err_msg=f)
+    d.close()
+    m.close()
+
+
+def test_cfl_on_slabs_stops_below_dtmmin(gpu_lib):
+    c, st = cfl_setup(frequency=2, dtmmin=0.9)
+    d = dc.SlabDomain(c, dc.LoopbackComm(2))
+    d.set_state(st)
+    with pytest.raises(api.MgpuError) as e:
+        d.step(1)
+    assert e.value.code == api.ERR_CFL
+    d.close()
+
+
+def test_fp32_mixed_cfl_on_slabs_follows_single_domain(gpu_lib):
+    c, st = cfl_setup(cf.FP32_MIXED, frequency=3, dtmmax=2.0)
+    m = api.Model(c)
+    m.set_state(st)
+    d = dc.SlabDomain(c, dc.LoopbackComm(4))
+    d.set_state(st)
+    for n in range(8):
+        m.step(1)
+        d.step(1)
+        assert abs(d.slabs[0].m.reductions().dtm - m.reductions().dtm) <= 1e-5 * c.dtm, n
+    d.close()
+    m.close()
+
+
 def test_halo_rows_pack_and_unpack(gpu_lib):
     """Pack takes the first and last `depth` interior rows, unpack writes the rows just outside."""
     halo, nyl = 4, 16
@@ -304,6 +369,8 @@ def test_slab_entry_points_check_arguments(gpu_lib):
     m.slab_init(64, 4, 9)
     with pytest.raises(api.MgpuError):
         m.slab_mean_profiles(buf.data_ptr(), False)  # no damping, subsidence or diagnostics: no profiles
+    with pytest.raises(api.MgpuError):
+        m.slab_cfl_extrema(buf.data_ptr(), False)  # cfltest off
     m.close()
     plain = api.Model(dry_config())
     with pytest.raises(api.MgpuError):
