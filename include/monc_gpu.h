@@ -172,6 +172,13 @@ typedef struct mgpu_config {
   /* profile_diagnostics (profile_diagnostics.F90:311-636): keeps the mean profiles it reads up to
    * date every step, so that mgpu_profile_diagnostics can be called between steps */
   int32_t profile_diagnostics_enabled;
+  /* Galilean transformation (simplesetup.F90:239-245, cfltest.F90:184-230, pstep.F90:345-346,
+   * 453-469): the flow is stepped in a frame moving at (ugal, vgal), set on each cfltest evaluation
+   * to the middle of the domain's zu (zv) range unless fixed at ugal (vgal).  Off in MONC's
+   * global_config; most of MONC's test cases switch it on. */
+  int32_t galilean_transformation;
+  int32_t fix_ugal, fix_vgal;
+  double  ugal, vgal;                 /* the fixed frame velocities (fix_ugal, fix_vgal) */
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */
@@ -188,6 +195,7 @@ typedef struct mgpu_reductions {
   double  cvel_x, cvel_y, cvel_z;     /* their advective parts before the dtm scaling */
   int32_t cfl_evaluations;            /* CFL evaluations so far */
   int32_t last_cfl_timestep;          /* timestep of the last evaluation */
+  double  ugal, vgal;                 /* the Galilean frame velocities of the next step */
 } mgpu_reductions;
 
 typedef struct mgpu_handle mgpu_handle;
@@ -241,6 +249,13 @@ int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out);
  * min zv, max zv (levels 2..nz), max over k = 2..nz-1 of |zw| rdzn(k+1), max over k = 2..nz-1 of
  * max(vis, diff) (rdzn(k+1)^2 + cx2 + cy2).  Synchronous; reads back 48 bytes. */
 int mgpu_cfl_gather(mgpu_handle* h, double* out);
+
+/* The Galilean frame velocities (current_state%ugal, vgal) the component kernels read:
+ * stepfields adds them to u, v; pstep subtracts them from u, zu, v, zv when
+ * galilean_transformation is on (pstep.F90:345-346, 453-469); lower_bc, coriolis, damping,
+ * swap_smooth and the mean profiles read them.  For a CPU cfltest driving GPU-resident fields:
+ * it sets the frame after each evaluation, before pstep.  mgpu_step moves the frame itself. */
+int mgpu_set_galilean_velocity(mgpu_handle* h, double ugal, double vgal);
 
 /* Horizontal-mean profile of a field (meanprofiles.F90:155-293 style sum / (nx*ny)). */
 int mgpu_mean_profile(mgpu_handle* h, int32_t field_id, double* out);

@@ -111,7 +111,8 @@ class Reductions(C.Structure):
                 ("dtm", C.c_double), ("dtm_new", C.c_double), ("absolute_new_dtm", C.c_double),
                 ("cvel", C.c_double), ("cvis", C.c_double), ("cfl_number", C.c_double),
                 ("cvel_x", C.c_double), ("cvel_y", C.c_double), ("cvel_z", C.c_double),
-                ("cfl_evaluations", C.c_int32), ("last_cfl_timestep", C.c_int32)]
+                ("cfl_evaluations", C.c_int32), ("last_cfl_timestep", C.c_int32),
+                ("ugal", C.c_double), ("vgal", C.c_double)]
 
 
 _lib = None
@@ -198,6 +199,8 @@ def lib():
         f.restype = C.c_int
     L.mgpu_slab_level_means.argtypes = [C.c_void_p, C.c_void_p]
     L.mgpu_slab_level_means.restype = C.c_int
+    L.mgpu_set_galilean_velocity.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.mgpu_set_galilean_velocity.restype = C.c_int
     L.mgpu_slab_mean_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
     L.mgpu_slab_mean_profiles.restype = C.c_int
     L.mgpu_slab_cfl_extrema.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
@@ -324,6 +327,9 @@ class Model:
         r = Reductions()
         self._check(lib().mgpu_get_reductions(self.h, C.byref(r)), "reductions")
         return r
+
+    def set_galilean_velocity(self, ugal: float, vgal: float):
+        self._check(lib().mgpu_set_galilean_velocity(self.h, ugal, vgal), "set_galilean_velocity")
 
     def cfl_gather(self) -> np.ndarray:
         """cfltest's extrema from the current fields: min zu, max zu, min zv, max zv,

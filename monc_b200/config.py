@@ -81,6 +81,8 @@ class MgpuConfig(C.Structure):
         ("n_subs_pl", C.c_int32),
         ("z_subs_pl", C.c_double * MAX_SUBS_NODES), ("f_subs_pl", C.c_double * MAX_SUBS_NODES),
         ("profile_diagnostics_enabled", C.c_int32),
+        ("galilean_transformation", C.c_int32), ("fix_ugal", C.c_int32), ("fix_vgal", C.c_int32),
+        ("ugal", C.c_double), ("vgal", C.c_double),
     ]
 
 
@@ -156,6 +158,8 @@ def default_config() -> MgpuConfig:
     c.subsidence_local_theta = c.subsidence_local_q = 1
     c.n_subs_pl = 0
     c.profile_diagnostics_enabled = 0
+    c.galilean_transformation = c.fix_ugal = c.fix_vgal = 0
+    c.ugal = c.vgal = 0.0
     return c
 
 
@@ -208,6 +212,16 @@ def enable_cfl(c: MgpuConfig, frequency: int = 10, dtmmax: float = 100.0, dtmmin
     c.cfl_dtmmax, c.cfl_dtmmin, c.cfl_rincmax = dtmmax, dtmmin, rincmax
     c.cfl_tollerance, c.cfl_cvismax, c.cfl_cvelmax = tollerance, cvismax, cvelmax
     c.l_constant_dtm = 1 if constant_dtm else 0
+    return c
+
+
+def enable_galilean(c: MgpuConfig, ugal: float | None = None, vgal: float | None = None) -> MgpuConfig:
+    """Switch on the Galilean transformation (simplesetup.F90:239-245): the frame velocity follows
+    the middle of the zu (zv) range at each cfltest evaluation, or stays at a given ugal (vgal),
+    MONC's fix_ugal (fix_vgal)."""
+    c.galilean_transformation = 1
+    c.fix_ugal, c.ugal = (0, 0.0) if ugal is None else (1, ugal)
+    c.fix_vgal, c.vgal = (0, 0.0) if vgal is None else (1, vgal)
     return c
 
 

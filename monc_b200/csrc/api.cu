@@ -154,7 +154,12 @@ static void fill_scalars(mgpu_handle* h) {
   s.nx = c.nx; s.ny = c.ny; s.nz = c.nz;
   s.plane = (long long)c.nx * c.ny;
   s.cx = r.cx; s.cy = r.cy; s.cx2 = r.cx2; s.cy2 = r.cy2; s.tcx = r.tcx; s.tcy = r.tcy;
-  s.dtm = c.dtm; s.tsmth = 1e-2; s.ugal = 0.0; s.vgal = 0.0;
+  s.dtm = c.dtm; s.tsmth = 1e-2;
+  // simplesetup.F90:239-245: the frame starts at rest unless fixed
+  s.galilean = c.galilean_transformation ? 1 : 0;
+  s.ugal = (c.galilean_transformation && c.fix_ugal) ? c.ugal : 0.0;
+  s.vgal = (c.galilean_transformation && c.fix_vgal) ? c.vgal : 0.0;
+  s.ugal_p = s.ugal; s.vgal_p = s.vgal;
   s.fcoriol = c.fcoriol; s.smallp = r.smallp;
   s.czn = r.czn; s.zn2 = r.zn[2]; s.zlogm = r.zlogm; s.zlogth = r.zlogth; s.vk_on_zlogm = r.vk_on_zlogm;
   s.vk = c.von_karman_constant; s.z0 = c.z0; s.z0th = c.z0th; s.alphah = c.alphah; s.betam = c.betam;
@@ -382,6 +387,8 @@ static int ad_supported(mgpu_handle* h) {
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the PW advection of the flow");
   if (h->cfg.cfl_enabled)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs hold dtm fixed: disable cfltest");
+  if (h->cfg.galilean_transformation || h->sc.ugal != 0.0 || h->sc.vgal != 0.0)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the step in a frame at rest");
   if (h->cfg.damping_enabled || h->cfg.l_subs_pl_theta || h->cfg.l_subs_pl_q)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the step without damping and forcing");
   if (h->fp32 || h->cfg.number_q_fields > 0 || h->cfg.solver != MGPU_SOLVER_FFT)
@@ -628,9 +635,10 @@ static bool cfl_evaluation_step(const mgpu_handle* h, int n) {
 
 // cfltest's timestep callback (cfltest.F90:62-128) and update_dtm_based_on_absolute (:135-191), on
 // the host: `evaluate` when this step gathered the extrema into cfl.out_h.  The new dtm takes
-// effect at the start of the next step (monc.F90:313).  Galilean transformation is off
-// (global_config:268): ugal = vgal = 0.  The output-time alignment of time_basis runs is not on
-// this path.
+// effect at the start of the next step (monc.F90:313).  An evaluation also sets the frame of the
+// Galilean transformation (perform_cfl_and_galilean_transformation_calculation, :184-230) into
+// sc.ugal_p, vgal_p: the pressure-terms group of this step and the stepping of the next read it.
+// The output-time alignment of time_basis runs is not on this path.
 static int cfltest_callback(mgpu_handle* h, bool evaluate) {
   auto& c = h->cfl;
   const mgpu_config& g = h->cfg;
@@ -642,8 +650,16 @@ static int cfltest_callback(mgpu_handle* h, bool evaluate) {
     const double* r = c.out_h;
     c.last_cfl_timestep = h->timestep;
     c.evaluations += 1;
-    const double ugal = 0.0, vgal = 0.0;
-    const double zumin = r[0] + ugal, zumax = r[1] + ugal, zvmin = r[2] + vgal, zvmax = r[3] + vgal;
+    // the extrema are of the stepping frame's zu, zv: undo its transformation
+    const double zumin = r[0] + h->sc.ugal, zumax = r[1] + h->sc.ugal;
+    const double zvmin = r[2] + h->sc.vgal, zvmax = r[3] + h->sc.vgal;
+    double ugal = 0.0, vgal = 0.0;
+    if (g.galilean_transformation) {
+      ugal = g.fix_ugal ? h->sc.ugal : 0.5 * (zumin + zumax);
+      vgal = g.fix_vgal ? h->sc.vgal : 0.5 * (zvmin + zvmax);
+    }
+    h->sc.ugal_p = ugal;
+    h->sc.vgal_p = vgal;
     c.cvel_z = r[4];
     c.cvel_x = std::max(std::fabs(zumax - ugal), std::fabs(zumin - ugal));
     c.cvel_y = std::max(std::fabs(zvmax - vgal), std::fabs(zvmin - vgal));
@@ -720,15 +736,24 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   int rc = pressure_solve<T>(h, d.p);
   if (rc) return rc;
   if (h->cfg.solver != MGPU_SOLVER_FFT) mark(8);
+  // cfltest ends the solver group.  Where its evaluation can move the frame the pressure step
+  // works in (the Galilean transformation, or a frame to bring to rest), it runs before the
+  // pressure step is queued, waiting for the extrema; otherwise it only sets the next step's dtm
+  // and runs after, while the GPU works.
+  const bool frame = h->cfg.galilean_transformation || h->sc.ugal != 0.0 || h->sc.vgal != 0.0;
+  bool cfl_done = false;
+  if (cfl && frame) {
+    if (int rc = cfltest_callback(h, cfl_gather)) return rc;
+    cfl_done = true;
+  }
   if (h->cfg.reproducible) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
   else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
   mark(9);
   h->launches += 1;
-  if (cfl) {
-    // cfltest runs in the solver group; it only sets the next step's dtm
-    int rc = cfltest_callback(h, cfl_gather);
-    if (rc) return rc;
-  }
+  if (cfl && !cfl_done)
+    if (int rc = cfltest_callback(h, cfl_gather)) return rc;
+  h->sc.ugal = h->sc.ugal_p;  // the next step steps in the frame the pressure step left
+  h->sc.vgal = h->sc.vgal_p;
   h->time += h->sc.dtm;
   h->timestep += 1;
   if (h->profiling) collect_stage_times(h);
@@ -1017,6 +1042,15 @@ int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out) {
   out->cvel_z = h->cfl.cvel_z;
   out->cfl_evaluations = h->cfl.evaluations;
   out->last_cfl_timestep = h->cfl.last_cfl_timestep;
+  out->ugal = h->sc.ugal;
+  out->vgal = h->sc.vgal;
+  return MGPU_OK;
+}
+
+int mgpu_set_galilean_velocity(mgpu_handle* h, double ugal, double vgal) {
+  if (!h || !std::isfinite(ugal) || !std::isfinite(vgal)) return MGPU_ERR_ARGUMENT;
+  h->sc.ugal = h->sc.ugal_p = ugal;
+  h->sc.vgal = h->sc.vgal_p = vgal;
   return MGPU_OK;
 }
 
@@ -1095,6 +1129,8 @@ int mgpu_checkpoint_read(mgpu_handle* h, const char* path) {
   h->timestep = meta.timestep + 1;
   h->time = meta.time;
   h->sc.dtm = meta.dtm;
+  h->sc.ugal = h->sc.ugal_p = meta.ugal;  // readcheckpoint.F90:184
+  h->sc.vgal = h->sc.vgal_p = meta.vgal;
   h->cfl.dtm_last = meta.dtm;
   h->cfl.dtm_new = meta.dtm_new;
   h->cfl.update_dtm = h->cfg.cfl_enabled && meta.dtm_new != meta.dtm;
@@ -1245,9 +1281,7 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
       h->launches += 1;
       return MGPU_OK;
     case MGPU_PHASE_PSTEP:
-      if (exact_k) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
-      else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
-      h->launches += 1;
+      // cfltest (the end of the solver group) on the domain extrema, then the pressure terms
       if (h->cfg.cfl_enabled) {
         const bool gathered = h->cfl.gathered;
         h->cfl.gathered = false;
@@ -1257,6 +1291,11 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
         }
         if (int rc = cfltest_callback(h, gathered)) return rc;
       }
+      if (exact_k) exact::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+      else fast::launch_fused_pstep_swap<T>(h->sc, d, h->stream);
+      h->launches += 1;
+      h->sc.ugal = h->sc.ugal_p;
+      h->sc.vgal = h->sc.vgal_p;
       h->time += h->sc.dtm;
       h->timestep += 1;
       return MGPU_OK;

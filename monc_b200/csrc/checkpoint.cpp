@@ -305,7 +305,9 @@ std::vector<std::pair<std::string, std::string>> options_of(const mgpu_config& c
       {"l_subs_pl_q", fmt_bool(c.l_subs_pl_q)}, {"subsidence_input_type", std::to_string(c.subsidence_input_type)},
       {"subsidence_local_theta", fmt_bool(c.subsidence_local_theta)},
       {"subsidence_local_q", fmt_bool(c.subsidence_local_q)},
-      {"mean_profiles_enabled", fmt_bool(c.damping_enabled || c.l_subs_pl_theta || c.l_subs_pl_q)}};
+      {"mean_profiles_enabled", fmt_bool(c.damping_enabled || c.l_subs_pl_theta || c.l_subs_pl_q)},
+      {"galilean_transformation", fmt_bool(c.galilean_transformation)}, {"fix_ugal", fmt_bool(c.fix_ugal)},
+      {"fix_vgal", fmt_bool(c.fix_vgal)}, {"ugal", fmt(c.ugal)}, {"vgal", fmt(c.vgal)}};
   if (c.rmlmax > 0.0) o.push_back({"rmlmax", fmt(c.rmlmax)});
   return o;
 }

@@ -368,6 +368,14 @@ __global__ void k_c_pstep(Scalars s, DevState<T> d) {
   Prof<T> P = prof<T>(s);
   View<T> Pv = view<T>(d.p, s);
   T dtmtmp = s.forward ? (T)(0.5 * s.dtm) : (T)s.dtm;
+  if (s.galilean)  // perform_galilean_transformation, every level, before the pressure step
+    for (int k = 1; k <= s.nz; ++k) {
+      long long o = lin(s, k, j, i);
+      d.u[o] = d.u[o] - (T)s.ugal;
+      d.zu[o] = d.zu[o] - (T)s.ugal;
+      d.v[o] = d.v[o] - (T)s.vgal;
+      d.zv[o] = d.zv[o] - (T)s.vgal;
+    }
   for (int k = 2; k <= s.nz; ++k) {
     long long o = lin(s, k, j, i);
     T p0 = Pv(k, j, i);
@@ -1065,33 +1073,44 @@ __global__ void __launch_bounds__(256) k_f_pstep_swap(Scalars s, DevState<T> d) 
   const T pz1 = (k >= 2 && k < s.nz) ? __ldg(p + o + s.plane) : (T)0;
   const T zun = __ldg(d.zu_n + op), zvn = __ldg(d.zv_n + op), zwn = __ldg(d.zw_n + o);
   const T u0 = d.u[o], v0 = d.v[o], w0 = d.w[o], zu0 = d.zu[o], zv0 = d.zv[o], zw0 = d.zw[o];
-  T zu_p = zun + (T)2.0 * (T)s.cx * dtmtmp * (p0 - pe);
-  T zv_p = zvn + (T)2.0 * (T)s.cy * dtmtmp * (p0 - pn);
+  // u, v as stepfields leaves them (the frame velocity of the stepping added), then moved into the
+  // frame of the pressure-terms group by the Galilean transformation
+  const T ugp = (T)s.ugal_p, vgp = (T)s.vgal_p;
+  T ua = (T)s.ugal + u0, va = (T)s.vgal + v0, zua = zun, zva = zvn;
+  if (s.galilean) {
+    ua = ua - ugp;
+    va = va - vgp;
+    zua = zua - ugp;
+    zva = zva - vgp;
+  }
+  T zu_p = zua + (T)2.0 * (T)s.cx * dtmtmp * (p0 - pe);
+  T zv_p = zva + (T)2.0 * (T)s.cy * dtmtmp * (p0 - pn);
   if (k == 1) {
     if (bc) {
-      zu_p = -zu_p - (T)2.0 * (T)s.ugal;
-      zv_p = -zv_p - (T)2.0 * (T)s.vgal;
+      zu_p = -zu_p - (T)2.0 * ugp;
+      zv_p = -zv_p - (T)2.0 * vgp;
     }
   }
   T zw_p = zwn;
   if (k >= 2 && k < s.nz) zw_p = zw_p + (T)2.0 * P(P_RDZN, k + 1) * dtmtmp * (pz0 - pz1);
   T nu, nzu, nv, nzv, nw, nzw;
   if (fwd) {
-    T ev = ((T)s.ugal + u0) + zu_p;
-    nu = ev * (T)1.0 + ((T)s.ugal + u0) * (T)-1.0;
+    T ev = ua + zu_p;
+    nu = ev * (T)1.0 + ua * (T)-1.0;
     nzu = ev - nu;
-    ev = ((T)s.vgal + v0) + zv_p;
-    nv = ev * (T)1.0 + ((T)s.vgal + v0) * (T)-1.0;
+    ev = va + zv_p;
+    nv = ev * (T)1.0 + va * (T)-1.0;
     nzv = ev - nv;
     ev = w0 + zw_p;
     nw = ev * (T)1.0 + w0 * (T)-1.0;
     nzw = ev - nw;
   } else {
+    // savu = zu + ugal of the stepping (stepfields.F90:609-610)
     const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
     nu = zu_p;
-    nzu = c1 * ((T)s.ugal + u0) + c2 * (zu_p + (zu0 + (T)s.ugal) - (T)s.ugal);
+    nzu = c1 * ua + c2 * (zu_p + (zu0 + (T)s.ugal) - ugp);
     nv = zv_p;
-    nzv = c1 * ((T)s.vgal + v0) + c2 * (zv_p + (zv0 + (T)s.vgal) - (T)s.vgal);
+    nzv = c1 * va + c2 * (zv_p + (zv0 + (T)s.vgal) - vgp);
     nw = zw_p;
     nzw = c1 * w0 + c2 * (zw_p + (zw0 + (T)0.0));
   }

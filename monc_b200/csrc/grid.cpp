@@ -79,6 +79,9 @@ extern "C" void mgpu_config_defaults(mgpu_config* c) {
   c->n_subs_pl = 0;
   for (int q = 0; q < MGPU_MAX_SUBS_NODES; ++q) c->z_subs_pl[q] = c->f_subs_pl[q] = 0.0;
   c->profile_diagnostics_enabled = 0;
+  c->galilean_transformation = 0;  // global_config:268-270
+  c->fix_ugal = c->fix_vgal = 0;
+  c->ugal = c->vgal = 0.0;
 }
 
 // w-level heights: piecewise-linear kgd/hgd grid smoothed nsmth times

@@ -86,6 +86,12 @@ struct Scalars {
   int subs_local_th, subs_local_q; // 1: gradients of the column; 0: the tendencies in subs_tend
   const double* olz;       // device: olzubar, olzvbar, olzthbar, olzqbar(n) rows, (nz+2) each
   const double* subs_tend; // device: mean-profile subsidence tendencies usub, vsub, thsub, qsub(n) rows
+  // Galilean transformation (pstep.F90:345-346, 453-469): ugal, vgal above are the frame of this
+  // step's stepping; ugal_p, vgal_p the frame after this step's cfltest, which the pressure step
+  // moves u, zu (v, zv) into when galilean is set and which the surface condition and the Robert
+  // filter of the pressure-terms group read.  Equal to ugal, vgal outside cfltest evaluations.
+  int galilean;
+  double ugal_p, vgal_p;
 };
 
 }  // namespace mgpu

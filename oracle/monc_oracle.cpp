@@ -1470,8 +1470,16 @@ static void fftsolver(Model& m) {
 // pstep (pstep.F90:359-447) and swap_smooth (swapsmooth.F90:45-187)
 // ---------------------------------------------------------------------------------------------
 static void pstep_column(Model& m) {
-  if (m.halo_column) return;
   int y = m.col_y, x = m.col_x;
+  // perform_galilean_transformation (pstep.F90:345-346, 453-469), on every column
+  if (m.cfg.galilean_transformation)
+    for (int k = 1; k <= m.nz; ++k) {
+      m.u(k, y, x) = m.u(k, y, x) - m.ugal;
+      m.zu(k, y, x) = m.zu(k, y, x) - m.ugal;
+      m.v(k, y, x) = m.v(k, y, x) - m.vgal;
+      m.zv(k, y, x) = m.zv(k, y, x) - m.vgal;
+    }
+  if (m.halo_column) return;
   double dtmtmp = (m.field_stepping == CENTRED_STEPPING) ? m.dtm : 0.5 * m.dtm;
   for (int k = 2; k <= m.nz; ++k) {
     m.zu(k, y, x) = m.zu(k, y, x) + 2.0 * m.cx * dtmtmp * (m.p(k, y, x) - m.p(k, y, x + 1));
@@ -1740,8 +1748,8 @@ void iterative_solver(Model& m);  // defined below
 void iterative_solver_solve(Model& m);
 
 // cfltest timestep callback (cfltest.F90:62-128) with update_dtm_based_on_absolute (:135-191) on
-// normal steps, single rank (the global reductions of :193-222 are the local values), Galilean
-// transformation off (global_config:268)
+// normal steps, single rank (the global reductions of get_global_values, :246-264, are the local
+// values)
 static void cfltest(Model& m) {
   const mgpu_config& g = m.cfg;
   m.update_dtm = false;
@@ -1760,8 +1768,13 @@ static void cfltest(Model& m) {
     m.local_zvmax = m.local_zvmax + m.vgal;
     m.local_cvel_z = m.cvel_z;
     for (int k = 2; k <= m.nz - 1; ++k) m.local_cvel_z = std::max(m.local_cvel_z, m.abswmax[k] * m.rdzn(k + 1));
-    m.ugal = 0.0;
-    m.vgal = 0.0;
+    if (g.galilean_transformation) {
+      if (!g.fix_ugal) m.ugal = 0.5 * (m.local_zumin + m.local_zumax);
+      if (!g.fix_vgal) m.vgal = 0.5 * (m.local_zvmin + m.local_zvmax);
+    } else {
+      m.ugal = 0.0;
+      m.vgal = 0.0;
+    }
     m.cvel_z = m.local_cvel_z;
     m.cvel_x = std::max(std::fabs(m.local_zumax - m.ugal), std::fabs(m.local_zumin - m.ugal));
     m.cvel_y = std::max(std::fabs(m.local_zvmax - m.vgal), std::fabs(m.local_zvmin - m.vgal));
@@ -1866,6 +1879,9 @@ static Model* create(const mgpu_config* cfg) {
   m.r_over_cp = m.r / m.cp;
   m.dtm = cfg->dtm;
   m.tsmth = 1e-2;
+  // simplesetup.F90:239-245
+  if (cfg->galilean_transformation && cfg->fix_ugal) m.ugal = cfg->ugal;
+  if (cfg->galilean_transformation && cfg->fix_vgal) m.vgal = cfg->vgal;
   m.dtm_last = m.dtm;
   m.absolute_new_dtm = m.dtm;
   m.dtm_new = m.dtm;
@@ -2208,9 +2224,9 @@ int orc_step(void* h, int nsteps) {
 int orc_cfl_state(void* h, double* out, int* iout) {
   Model& m = *(Model*)h;
   const double next = m.update_dtm ? m.dtm_new : m.dtm;
-  const double v[9] = {m.dtm_last, next, m.absolute_new_dtm, m.cvel, m.cvis_last, m.cfl_number,
-                       m.cvel_x, m.cvel_y, m.cvel_z};
-  for (int q = 0; q < 9; ++q) out[q] = v[q];
+  const double v[11] = {m.dtm_last, next, m.absolute_new_dtm, m.cvel, m.cvis_last, m.cfl_number,
+                        m.cvel_x, m.cvel_y, m.cvel_z, m.ugal, m.vgal};
+  for (int q = 0; q < 11; ++q) out[q] = v[q];
   iout[0] = m.cfl_evaluations;
   iout[1] = m.last_cfl_timestep;
   return 0;

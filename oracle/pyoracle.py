@@ -139,10 +139,11 @@ class Oracle:
 
     def cfl_state(self) -> dict:
         """cfltest's state after the last step (the mgpu_reductions fields of the same names)."""
-        v = np.zeros(9)
+        v = np.zeros(11)
         i = np.zeros(2, dtype=np.int32)
         lib().orc_cfl_state(self.h, v.ctypes.data, i.ctypes.data)
-        keys = ["dtm", "dtm_new", "absolute_new_dtm", "cvel", "cvis", "cfl_number", "cvel_x", "cvel_y", "cvel_z"]
+        keys = ["dtm", "dtm_new", "absolute_new_dtm", "cvel", "cvis", "cfl_number", "cvel_x", "cvel_y", "cvel_z",
+                "ugal", "vgal"]
         out = dict(zip(keys, (float(x) for x in v)))
         out["cfl_evaluations"], out["last_cfl_timestep"] = int(i[0]), int(i[1])
         return out

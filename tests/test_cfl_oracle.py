@@ -1,7 +1,8 @@
 """cfltest in the CPU oracle (cfltest.F90:62-191 with the gathers of stepfields.F90:372-393 and
 smagorinsky.F90:143-173): the evaluation schedule, the Courant numbers recomputed in numpy from
 the fields the gathers read, the ratchet towards the target dtm, the immediate cut when the CFL
-number is too high, l_constant_dtm, and the stop below cfl_dtmmin."""
+number is too high, l_constant_dtm, the stop below cfl_dtmmin, and the Galilean transformation
+(the frame at the middle of the zu, zv range; a frame at rest changes nothing)."""
 import numpy as np
 import pytest
 
@@ -99,3 +100,48 @@ def test_disabled_cfl_keeps_dtm():
     o.step(3)
     s = o.cfl_state()
     assert s["cfl_evaluations"] == 0 and s["dtm"] == 1.0
+
+
+def galilean_setup(ugal=None, vgal=None, **cfl):
+    c = cf.dry_cbl_config(NX, NY, NZ, 50.0, 25.0, 1.0, ug=5.0, fcoriol=1e-4)
+    cf.enable_cfl(c, **cfl)
+    cf.enable_galilean(c, ugal, vgal)
+    o = po.Oracle(c)
+    st = ini.random_flow_state(NX, NY, NZ, seed=3, amp_uv=2.0, amp_w=0.5, ug=5.0)
+    for k, v in st.items():
+        o.set(F[k], v)
+    return c, o, st
+
+
+def test_galilean_frame_is_the_middle_of_the_range():
+    """cfltest.F90:184-230: an evaluation puts the frame at the middle of the (undone) zu, zv range,
+    and the advective Courant numbers are the half ranges; the forward step's pressure terms then
+    move u, zu into that frame (pstep.F90:453-469), so the old-time field zu holds u - ugal."""
+    c, o, st = galilean_setup(frequency=3, dtmmax=2.0)
+    o.step(1)
+    s = o.cfl_state()
+    zu, zv = st["zu"][1:], st["zv"][1:]
+    ugal, vgal = 0.5 * (zu.min() + zu.max()), 0.5 * (zv.min() + zv.max())
+    assert s["ugal"] == ugal and s["vgal"] == vgal
+    assert ugal > 3.0  # the flow has a mean wind of 5 m/s to follow
+    assert s["cvel_x"] == max(abs(zu.max() - ugal), abs(zu.min() - ugal))
+    assert s["cvel_y"] == max(abs(zv.max() - vgal), abs(zv.min() - vgal))
+    np.testing.assert_allclose(o.get(F["zu"]), st["u"] - ugal, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(o.get(F["zv"]), st["v"] - vgal, rtol=0, atol=1e-13)
+
+
+def test_galilean_frame_at_rest_changes_nothing():
+    """A frame fixed at zero velocity is the untransformed model, bit for bit."""
+    out = []
+    for gal in (False, True):
+        c, o, st = setup(frequency=3, dtmmax=2.0)
+        if gal:
+            cf.enable_galilean(c, 0.0, 0.0)
+            o = po.Oracle(c)
+            for k, v in st.items():
+                o.set(F[k], v)
+        o.step(6)
+        out.append({f: o.get(F[f]) for f in ("u", "v", "w", "th", "zu", "zv")})
+    for f in out[0]:
+        np.testing.assert_array_equal(out[1][f], out[0][f], err_msg=f)
+

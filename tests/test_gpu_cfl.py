@@ -95,3 +95,97 @@ def test_adjoint_refuses_adaptive_dtm(gpu_lib):
     with pytest.raises(api.MgpuError):
         m.tl_step(1)
     m.close()
+
+
+def galilean_pair(precision=cf.FP64, ugal=None, vgal=None, cfl=True):
+    c, st = setup(precision=precision, frequency=3, dtmmax=2.0)
+    if not cfl:
+        c.cfl_enabled = 0
+    cf.enable_galilean(c, ugal, vgal)
+    return c, st
+
+
+def test_galilean_sequence_matches_oracle(gpu_lib):
+    """The frame follows the middle of the zu, zv range at each evaluation; the pressure terms move
+    the flow into it; the dtm and frame sequences and the fields after 12 steps match the oracle."""
+    c, st = galilean_pair()
+    o = po.Oracle(c)
+    m = api.Model(c)
+    for k, v in st.items():
+        o.set(api.FIELDS[k], v)
+        m.upload(k, v)
+    for n in range(1, 13):
+        o.step(1)
+        m.step(1)
+        so, r = o.cfl_state(), m.reductions()
+        for k in KEYS + ["ugal", "vgal"]:
+            a, b = getattr(r, k), so[k]
+            assert abs(a - b) <= 1e-12 * max(abs(b), 1e-30), (n, k, a, b)
+    assert abs(m.reductions().ugal) > 3.0  # the frame took up the mean wind
+    for f in ("u", "v", "w", "th", "zu", "zv", "zw", "zth", "p"):
+        a, b = m.download(f), o.get(api.FIELDS[f])
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max(), f
+    m.close()
+
+
+def test_fixed_galilean_frame_matches_oracle(gpu_lib):
+    """fix_ugal, fix_vgal without cfltest: a constant moving frame."""
+    c, st = galilean_pair(ugal=3.0, vgal=-1.5, cfl=False)
+    o = po.Oracle(c)
+    m = api.Model(c)
+    for k, v in st.items():
+        o.set(api.FIELDS[k], v)
+        m.upload(k, v)
+    o.step(6)
+    m.step(6)
+    assert (m.reductions().ugal, m.reductions().vgal) == (3.0, -1.5)
+    for f in ("u", "v", "w", "th", "zu", "zv", "zw", "zth", "p"):
+        a, b = m.download(f), o.get(api.FIELDS[f])
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max(), f
+    m.close()
+
+
+def test_galilean_component_groups_match_fused_step(gpu_lib):
+    """The per-component entry points, with the frame set through mgpu_set_galilean_velocity, step
+    as mgpu_step does."""
+    c, st = galilean_pair(ugal=3.0, vgal=-1.5, cfl=False)
+    res = []
+    for fused in (True, False):
+        m = api.Model(c)
+        m.set_state(st)
+        m.step(2)
+        if fused:
+            m.step(1)
+        else:
+            m.set_galilean_velocity(3.0, -1.5)
+            api.run_groups(m)
+        res.append({f: m.download(f) for f in ("u", "v", "w", "th", "zu", "zv", "zw", "zth")})
+        m.close()
+    for f in res[0]:
+        b = res[0][f]
+        assert np.abs(res[1][f] - b).max() <= 1e-10 * np.abs(b).max(), f
+
+
+def test_fp32_mixed_galilean_follows_fp64(gpu_lib):
+    out = []
+    for prec in (cf.FP64, cf.FP32_MIXED):
+        c, st = galilean_pair(precision=prec)
+        m = api.Model(c)
+        m.set_state(st)
+        seq = []
+        for _ in range(8):
+            m.step(1)
+            r = m.reductions()
+            seq.append((r.dtm, r.ugal, r.vgal))
+        out.append(np.array(seq))
+        m.close()
+    np.testing.assert_allclose(out[1], out[0], rtol=1e-5, atol=1e-5)
+
+
+def test_adjoint_refuses_moving_frame(gpu_lib):
+    c, st = galilean_pair(ugal=3.0, cfl=False)
+    m = api.Model(c)
+    m.set_state(st)
+    with pytest.raises(api.MgpuError):
+        m.tl_step(1)
+    m.close()

@@ -1,7 +1,8 @@
 """Restart from a checkpoint on the GPU: a run interrupted by a checkpoint write, and continued by a
 new model that reads it, ends bit for bit where the uninterrupted run does -- with damping (its
 mean profiles are in the file), cfltest's adaptive dtm (its state is in the file), moist fields,
-and the FP32-mixed path (whose FP32 fields survive the FP64 file exactly)."""
+the FP32-mixed path (whose FP32 fields survive the FP64 file exactly), and the Galilean frame
+(ugal, vgal in the file)."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,7 @@ def restart_matches(c, st, n1, n2, path, extra=()):
     a.step(n1 + n2)
     ref = {f: a.download(f) for f in names}
     ref_ts, ref_dtm = a.reductions().timestep, a.reductions().dtm
+    ref_gal = (a.reductions().ugal, a.reductions().vgal)
     a.close()
     b = api.Model(c)
     b.set_state(st)
@@ -52,6 +54,7 @@ def restart_matches(c, st, n1, n2, path, extra=()):
     for f in names:
         np.testing.assert_array_equal(d.download(f), ref[f], err_msg=f)
     assert d.reductions().timestep == ref_ts and d.reductions().dtm == ref_dtm
+    assert (d.reductions().ugal, d.reductions().vgal) == ref_gal
     d.close()
 
 
@@ -68,3 +71,10 @@ def test_moist_restart_with_subsidence(gpu_lib, tmp_path):
 def test_fp32_mixed_restart(gpu_lib, tmp_path):
     c, st = dry(cf.FP32_MIXED)
     restart_matches(c, st, 4, 3, str(tmp_path / "fp32.nc"))
+
+
+def test_galilean_restart(gpu_lib, tmp_path):
+    """The frame velocity travels in the file (ugal, vgal), so a restarted run stays in it."""
+    c, st = dry()
+    cf.enable_galilean(c)
+    restart_matches(c, st, 4, 5, str(tmp_path / "gal.nc"))

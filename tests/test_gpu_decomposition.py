@@ -194,7 +194,7 @@ def test_fp32_mixed_forced_slabs_track_single_domain(gpu_lib):
 
 
 CFL_KEYS = ["dtm", "dtm_new", "absolute_new_dtm", "cvel", "cvis", "cfl_number", "cvel_x", "cvel_y", "cvel_z",
-            "cfl_evaluations", "last_cfl_timestep", "timestep"]
+            "cfl_evaluations", "last_cfl_timestep", "timestep", "ugal", "vgal"]
 
 
 def cfl_setup(precision=cf.FP64, **kw):
@@ -205,12 +205,15 @@ def cfl_setup(precision=cf.FP64, **kw):
     return c, st
 
 
+@pytest.mark.parametrize("galilean", [False, True], ids=["rest", "galilean"])
 @pytest.mark.parametrize("nranks", [2, 4])
-def test_cfl_on_slabs_bit_identical(gpu_lib, nranks):
+def test_cfl_on_slabs_bit_identical(gpu_lib, nranks, galilean):
     """cfltest on slabs: each slab's extrema over its interior rows, combined by a maximum across
-    the slabs (exact in any order), give the single domain's Courant numbers and dtm sequence, and
-    the steps of varying dtm end bit for bit where the single domain's do."""
+    the slabs (exact in any order), give the single domain's Courant numbers, dtm sequence and
+    Galilean frame, and the steps of varying dtm end bit for bit where the single domain's do."""
     c, st = cfl_setup(frequency=3, dtmmax=2.0)
+    if galilean:
+        cf.enable_galilean(c)
     m = api.Model(c)
     m.set_state(st)
     d = dc.SlabDomain(c, dc.LoopbackComm(nranks))
