@@ -435,6 +435,9 @@ int mgpu_step_phase(mgpu_handle* h, int32_t phase);
  * over it.  One kernel launch each. */
 #define MGPU_HALO_STATE     0
 #define MGPU_HALO_PRESSURE  1
+#define MGPU_HALO_ITER_X    2   /* BiCGStab on slabs: the iterate x (before MGPU_SLAB_ITER_INIT) */
+#define MGPU_HALO_ITER_PP   3   /* the search direction pp (before MGPU_SLAB_ITER_APPLY) */
+#define MGPU_HALO_ITER_CS   4   /* the preconditioned half step cs (before MGPU_SLAB_ITER_APPLY2) */
 int mgpu_halo_fields(mgpu_handle* h, int32_t set);
 int mgpu_halo_pack(mgpu_handle* h, int32_t set, int32_t depth, void* d_lo, void* d_hi);
 int mgpu_halo_unpack(mgpu_handle* h, int32_t set, int32_t depth, const void* d_lo, const void* d_hi);
@@ -462,6 +465,39 @@ int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put);
  * which runs cfltest and sets the next step's dtm.  *gathered (may be NULL) says whether this
  * step gathered; on other steps the call does nothing, and every slab takes the same steps. */
 int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* gathered);
+
+/* iterativesolver's BiCGStab on slabs (iterativesolver.F90:140-248; MONC sums the inner products
+ * over its ranks with MPI_Allreduce in inner_prod, :500-553), FP64 models with solver_type
+ * MGPU_ITER_BICGSTAB, in place of the FFT steps between the dynamics and pressure-step phases:
+ *
+ *   BEGIN                                     psource = p; the iterate x keeps the last solution
+ *   halo exchange of MGPU_HALO_ITER_X (depth 1)
+ *   INIT, sum d_sums over the slabs, FINISH   r = b - A x; <r, r>, <b, b>
+ *   until FINISH reports done:
+ *     DIRECTION                               pp = M^-1 (r - bet omg v) + bet pp
+ *     halo exchange of MGPU_HALO_ITER_PP (depth 1)
+ *     APPLY, sum, FINISH                      v = A pp; <cr, v>
+ *     HALF_STEP                               s = r - alf v; cs = M^-1 s
+ *     halo exchange of MGPU_HALO_ITER_CS (depth 1)
+ *     APPLY2, sum, FINISH                     t = A cs; <t, t>, <t, s>, <s, s>
+ *     UPDATE, sum, FINISH                     x, r; <r, cr>; convergence
+ *   END                                       p = x (then the MGPU_HALO_PRESSURE exchange)
+ *
+ * The reducing steps write this slab's sums over its interior rows to d_sums (3 doubles on the
+ * device); the driver replaces them by their sum over the slabs and passes them to FINISH,
+ * which updates the solver scalars and sets *done (every slab reaches the same verdict from
+ * the same sums).  As in mgpu_step, a solve that stops at max_iterations above the tolerance is
+ * not an error (MONC only warns); mgpu_get_reductions reports its iterations and residual. */
+#define MGPU_SLAB_ITER_BEGIN      0
+#define MGPU_SLAB_ITER_INIT       1
+#define MGPU_SLAB_ITER_DIRECTION  2
+#define MGPU_SLAB_ITER_APPLY      3
+#define MGPU_SLAB_ITER_HALF_STEP  4
+#define MGPU_SLAB_ITER_APPLY2     5
+#define MGPU_SLAB_ITER_UPDATE     6
+#define MGPU_SLAB_ITER_FINISH     7
+#define MGPU_SLAB_ITER_END        8
+int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done);
 
 /* x-FFT (fftsolver.F90:50-309 transforms, x pass) between the interior rows of p and d_spec,
  * which is split into nblocks (<= nx/2+1) blocks of consecutive wavenumbers dealt out as evenly

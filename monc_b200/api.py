@@ -199,6 +199,8 @@ def lib():
         f.restype = C.c_int
     L.mgpu_slab_level_means.argtypes = [C.c_void_p, C.c_void_p]
     L.mgpu_slab_level_means.restype = C.c_int
+    L.mgpu_slab_iter.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]
+    L.mgpu_slab_iter.restype = C.c_int
     L.mgpu_set_galilean_velocity.argtypes = [C.c_void_p, C.c_double, C.c_double]
     L.mgpu_set_galilean_velocity.restype = C.c_int
     L.mgpu_slab_mean_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
@@ -409,6 +411,12 @@ class Model:
 
     def slab_mean_profiles(self, buf: int, put: bool):
         self._check(lib().mgpu_slab_mean_profiles(self.h, buf, 1 if put else 0), "slab_mean_profiles")
+
+    def slab_iter(self, step: int, sums: int = 0) -> bool:
+        """One step of the slab BiCGStab (mgpu_slab_iter); returns the done flag of a FINISH."""
+        done = C.c_int32(0)
+        self._check(lib().mgpu_slab_iter(self.h, step, sums or None, C.byref(done)), f"slab_iter {step}")
+        return bool(done.value)
 
     def slab_cfl_extrema(self, buf: int, put: bool) -> bool:
         """Fetch (put=False) or hand back (put=True) this slab's cfltest extrema in max form;

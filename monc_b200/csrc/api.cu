@@ -1319,6 +1319,10 @@ static int halo_set(mgpu_handle* h, DevState<T>& d, int set, T** f) {
     f[n++] = d.p;
     return n;
   }
+  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CS && sizeof(T) == 8 && h->iter) {
+    f[n++] = reinterpret_cast<T*>(iter_slab_vector(h->iter, set));
+    return f[0] ? n : -1;
+  }
   return -1;
 }
 
@@ -1378,6 +1382,10 @@ int mgpu_halo_fields(mgpu_handle* h, int32_t set) {
   if (!h) return MGPU_ERR_ARGUMENT;
   if (set == MGPU_HALO_STATE) return 8 + 2 * h->cfg.number_q_fields;
   if (set == MGPU_HALO_PRESSURE) return 1;
+  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CS) {
+    if (!h->iter || h->fp32) return fail(h, MGPU_ERR_ARGUMENT, "the solver vectors exist after MGPU_SLAB_ITER_BEGIN");
+    return 1;
+  }
   return fail(h, MGPU_ERR_ARGUMENT, "unknown halo set");
 }
 
@@ -1434,6 +1442,41 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
   h->launches += put ? launch_cfl_max_form(d_buf, h->cfl.out_d, h->stream)
                      : launch_cfl_max_form(h->cfl.out_d, d_buf, h->stream);
   return check_launch(h);
+}
+
+int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done) {
+  if (!h) return MGPU_ERR_ARGUMENT;
+  if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
+  if (h->fp32 || h->cfg.solver_type != MGPU_ITER_BICGSTAB)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "the slab iterative solve is FP64 BiCGStab");
+  const size_t bytes = field_elems(h) * sizeof(double);
+  if (step == MGPU_SLAB_ITER_BEGIN) {
+    if (!h->iter) {
+      int st = MGPU_OK;
+      h->iter = iter_create(h->sc, h->rs, h->cfg, false, &st, h->slab_halo, h->cfg.ny - h->slab_halo);
+      if (st) return fail(h, st, "iterative solver setup");
+    }
+    if (int rc = iter_slab_begin(h->iter, h->d64.p, bytes, h->stream)) return fail(h, rc, "slab iterative begin");
+    return MGPU_OK;
+  }
+  if (!h->iter) return fail(h, MGPU_ERR_ARGUMENT, "MGPU_SLAB_ITER_BEGIN first");
+  if (step == MGPU_SLAB_ITER_END) {
+    int rc = iter_slab_end(h->iter, h->d64.p, bytes, h->stream, &h->solver_iterations, &h->solver_residual);
+    if (rc == MGPU_ERR_CUDA) return fail(h, rc, "slab iterative end");
+    return MGPU_OK;  // not converged: MONC only warns (iterativesolver.F90:240-242); see mgpu_get_reductions
+  }
+  const bool reduces = step == MGPU_SLAB_ITER_INIT || step == MGPU_SLAB_ITER_APPLY || step == MGPU_SLAB_ITER_APPLY2 ||
+                       step == MGPU_SLAB_ITER_UPDATE || step == MGPU_SLAB_ITER_FINISH;
+  if (reduces && !d_sums) return fail(h, MGPU_ERR_ARGUMENT, "this step needs d_sums");
+  if (step == MGPU_SLAB_ITER_FINISH) {
+    int dn = 0;
+    int rc = iter_slab_finish(h->iter, d_sums, h->stream, &h->launches, &dn);
+    if (rc) return fail(h, rc, "slab iterative finish (no reduction pending?)");
+    if (done) *done = dn;
+    return MGPU_OK;
+  }
+  if (int rc = iter_slab_step(h->iter, step, d_sums, h->stream, &h->launches)) return fail(h, rc, "slab iterative step");
+  return MGPU_OK;
 }
 
 int mgpu_slab_fft_x(mgpu_handle* h, void* d_spec, int32_t nblocks, int32_t inverse) {

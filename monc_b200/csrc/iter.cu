@@ -23,6 +23,7 @@
 // The FP32-mixed model solves in FP64 by iterative refinement: r = b - A x in FP64, an FP32
 // BiCGStab solve of A e = r, x += e, until the FP64 residual meets the tolerance.
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <vector>
 
@@ -32,8 +33,10 @@ namespace mgpu {
 
 struct IterScalars {
   double rho, rho_prev, nrm, alf, omg, err, sc_err, tol, shift, bet;
-  int it, done, it_done, pad;
-  unsigned int counter;
+  int it, done, it_done;
+  int ext;  // 1: the dot products are summed outside (over y-slabs): the last block leaves them in loc
+  unsigned int counter, pad;
+  double loc[3];
 };
 
 namespace {
@@ -48,6 +51,7 @@ struct Geom {
   long long plane;
   double A_n, A_e;
   const double* coef;  // [NCOEF][nz+2]
+  int j0, j1;          // rows solved: all (0, ny), or a y-slab's interior rows between its halo rows
   __device__ __forceinline__ double au(int k) const { return coef[k]; }
   __device__ __forceinline__ double ad(int k) const { return coef[(nz + 2) + k]; }
   __device__ __forceinline__ double ap(int k) const { return coef[2 * (nz + 2) + k]; }
@@ -112,7 +116,44 @@ __device__ bool last_block_sums(IterScalars* st, const double* partials, int nbl
     out[q] = a;
   }
   st->counter = 0u;
+  if (st->ext) {
+    // this slab's sums; the scalars are updated once the sums over all slabs are back
+#pragma unroll
+    for (int q = 0; q < NV; ++q) st->loc[q] = out[q];
+    return false;
+  }
   return true;
+}
+
+// The scalar updates that close each reduction (the same code for one domain, where the last
+// block runs them, and for y-slabs, where k_bicg_finish runs them on the sums over the slabs).
+__device__ void finish_init(IterScalars* st, const double* s, double sc_floor) {
+  st->sc_err = fmax(sqrt(s[1]), sc_floor);
+  st->rho = s[0];
+  st->rho_prev = 1.0;
+  st->nrm = 1.0;
+  st->alf = 1.0;
+  st->omg = 1.0;
+  st->err = sqrt(s[0]) / st->sc_err;
+  st->it = 1;
+  st->it_done = 0;
+  st->done = st->err < st->tol ? 1 : 0;
+}
+__device__ void finish_apply_dot(IterScalars* st, const double* s) {
+  st->nrm = s[0];
+  st->alf = st->rho / s[0];
+}
+__device__ void finish_apply_dots(IterScalars* st, const double* s) {
+  const double omg = s[1] / s[0];
+  st->omg = omg;
+  st->err = sqrt(s[2] - 2 * omg * s[1] + omg * omg * s[0]) / st->sc_err;
+}
+__device__ void finish_update(IterScalars* st, const double* s, int max_it) {
+  st->rho_prev = st->rho;
+  st->rho = s[0];
+  st->it_done = st->it;
+  st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
+  st->it += 1;
 }
 
 // (A x)(k, j, i) for 2 <= k <= nz (calc_Ax); x(o) gives the value at offset o.  The symmetric
@@ -140,9 +181,9 @@ __device__ __forceinline__ int block_id() { return blockIdx.x + gridDim.x * (blo
 template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_init(Geom g, const W* __restrict__ x, const W* __restrict__ b, W* r, W* cr,
                                                     double* partials, int nblocks, IterScalars* st, double sc_floor) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W rv = b[o] - apply_A<W>(g, x, k, j, i);
     r[o] = rv;
@@ -152,18 +193,7 @@ __global__ void __launch_bounds__(NTH) k_bicg_init(Geom g, const W* __restrict__
   }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
-  if (last_block_sums<2>(st, partials, nblocks, s)) {
-    st->sc_err = fmax(sqrt(s[1]), sc_floor);
-    st->rho = s[0];
-    st->rho_prev = 1.0;
-    st->nrm = 1.0;
-    st->alf = 1.0;
-    st->omg = 1.0;
-    st->err = sqrt(s[0]) / st->sc_err;
-    st->it = 1;
-    st->it_done = 0;
-    st->done = st->err < st->tol ? 1 : 0;
-  }
+  if (last_block_sums<2>(st, partials, nblocks, s)) finish_init(st, s, sc_floor);
 }
 
 // column LU solve of the vertical operator: out = M^-1 in (precond); `tmp` holds the forward sweep
@@ -184,8 +214,8 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_direction(Geom g, const W* __restrict__ r, const W* __restrict__ v, W* pp,
                                                          W* tmp, const IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-  if (i >= g.nx || j >= g.ny) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
+  if (i >= g.nx || j >= g.j1) return;
   const bool first = st->it == 1;
   const double bet_d = (st->rho / st->rho_prev) * (st->alf / st->omg);
   const W bet = (W)bet_d, bo = (W)(bet_d * st->omg);
@@ -207,9 +237,9 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_apply_dot(Geom g, const W* __restrict__ pp, const W* __restrict__ cr, W* v,
                                                          double* partials, int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double a[1] = {0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W vv = apply_A<W>(g, pp, k, j, i);
     v[o] = vv;
@@ -217,10 +247,7 @@ __global__ void __launch_bounds__(NTH) k_bicg_apply_dot(Geom g, const W* __restr
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
-  if (last_block_sums<1>(st, partials, nblocks, s)) {
-    st->nrm = s[0];
-    st->alf = st->rho / s[0];
-  }
+  if (last_block_sums<1>(st, partials, nblocks, s)) finish_apply_dot(st, s);
 }
 
 // iteration step 3: s = r - alf*v, cs = M^-1 s
@@ -228,8 +255,8 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_half_step(Geom g, const W* __restrict__ r, const W* __restrict__ v, W* s_,
                                                          W* cs, W* tmp, const IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-  if (i >= g.nx || j >= g.ny) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
+  if (i >= g.nx || j >= g.j1) return;
   const W alf = (W)st->alf;
   column_precond<W>(g, [&](long long o) {
     const W sv = r[o] - alf * v[o];
@@ -251,9 +278,9 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_apply_dots(Geom g, const W* __restrict__ cs, const W* __restrict__ s_, W* t,
                                                           double* partials, int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double a[3] = {0.0, 0.0, 0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W tv = apply_A<W>(g, cs, k, j, i);
     t[o] = tv;
@@ -264,11 +291,7 @@ __global__ void __launch_bounds__(NTH) k_bicg_apply_dots(Geom g, const W* __rest
   }
   block_partials<3>(a, partials, nblocks, block_id());
   double s[3];
-  if (last_block_sums<3>(st, partials, nblocks, s)) {
-    const double omg = s[1] / s[0];
-    st->omg = omg;
-    st->err = sqrt(s[2] - 2 * omg * s[1] + omg * omg * s[0]) / st->sc_err;
-  }
+  if (last_block_sums<3>(st, partials, nblocks, s)) finish_apply_dots(st, s);
 }
 
 // iteration step 5: x += alf*pp + omg*cs, r = s - omg*t, rho = <r, cr>, convergence test
@@ -278,9 +301,9 @@ __global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __re
                                                       const W* __restrict__ cr, double* partials, int nblocks,
                                                       IterScalars* st, int max_it) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double a[1] = {0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W alf = (W)st->alf, omg = (W)st->omg;
     x[o] = x[o] + alf * pp[o] + omg * cs[o];
@@ -290,12 +313,20 @@ __global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __re
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
-  if (last_block_sums<1>(st, partials, nblocks, s)) {
-    st->rho_prev = st->rho;
-    st->rho = s[0];
-    st->it_done = st->it;
-    st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
-    st->it += 1;
+  if (last_block_sums<1>(st, partials, nblocks, s)) finish_update(st, s, max_it);
+}
+
+// y-slabs: close reduction `which` (0 init, 1 apply_dot, 2 apply_dots, 3 update) with the sums
+// over all slabs
+__global__ void k_bicg_finish(IterScalars* st, const double* __restrict__ sums, int which, double sc_floor,
+                              int max_it) {
+  if (threadIdx.x != 0) return;
+  const double s[3] = {sums[0], sums[1], sums[2]};
+  switch (which) {
+    case 0: finish_init(st, s, sc_floor); break;
+    case 1: if (!st->done) finish_apply_dot(st, s); break;
+    case 2: if (!st->done) finish_apply_dots(st, s); break;
+    default: if (!st->done) finish_update(st, s, max_it); break;
   }
 }
 
@@ -307,9 +338,9 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_init(Geom g, const W* __restrict__ x, const W* __restrict__ b, W* r,
                                                   double* partials, int nblocks, IterScalars* st, double sc_floor,
                                                   int scale_rhs) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W bv = scale_rhs ? b[o] * (W)g.avol(k) : b[o];
     const W rv = bv - apply_A<W>(g, x, k, j, i);
@@ -336,9 +367,9 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_precond(Geom g, const W* __restrict__ r, W* z, W* tmp, double* partials,
                                                      int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double a[1] = {0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     column_precond<W>(g, [&](long long o) { return r[o]; }, tmp, j, i);
     long long o = g.at(g.nz, j, i);
     W zk = tmp[o];
@@ -376,12 +407,12 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_apply(Geom g, const W* __restrict__ z, const W* __restrict__ p_old,
                                                    W* p_new, W* Ax, double* partials, int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   const bool first = st->it == 1;
   const W bet = (W)st->bet;
   auto pn = [&](long long o) { return first ? z[o] : axpy_rn<W>(bet, p_old[o], z[o]); };
   double a[1] = {0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W pc = pn(o);
     p_new[o] = pc;
@@ -399,9 +430,9 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_update(Geom g, W* x, const W* __restrict__ p, const W* __restrict__ Ax, W* r,
                                                     double* partials, int nblocks, IterScalars* st, int max_it) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double a[1] = {0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const W alf = (W)st->alf;
     x[o] = x[o] + alf * p[o];
@@ -423,9 +454,9 @@ __global__ void __launch_bounds__(NTH) k_cg_update(Geom g, W* x, const W* __rest
 __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* __restrict__ x, const double* __restrict__ b,
                                                           double* r, float* r32, double* partials, int nblocks,
                                                           IterScalars* st) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.j1) {
     const long long o = g.at(k, j, i);
     const double bv = g.symm ? b[o] * g.avol(k) : b[o];
     const double rv = bv - apply_A<double>(g, x, k, j, i);
@@ -449,9 +480,9 @@ __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* _
 // solve cannot remove; the refinement takes it out of b first (a constant shift of levels 2..nz).
 __global__ void __launch_bounds__(NTH) k_compat_sum(Geom g, const double* __restrict__ b, double* partials, int nblocks,
                                                      IterScalars* st) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
   double v[1] = {0.0};
-  if (i < g.nx && j < g.ny) v[0] = g.vol(k) * b[g.at(k, j, i)];
+  if (i < g.nx && j < g.j1) v[0] = g.vol(k) * b[g.at(k, j, i)];
   block_partials<1>(v, partials, nblocks, block_id());
   double s[1];
   if (last_block_sums<1>(st, partials, nblocks, s)) {
@@ -498,6 +529,7 @@ struct IterSolverDev {
   Work<double> w64{};
   Work<float> w32{};
   double* r64 = nullptr;  // refinement residual (FP32-mixed model)
+  int pending = -1;       // y-slab steps: the reduction iter_slab_finish closes next
   std::vector<void*> allocs;
   dim3 grid_pt, grid_col, block;
 };
@@ -509,8 +541,10 @@ static int dev_alloc(IterSolverDev* it, void** p, size_t bytes) {
   return MGPU_OK;
 }
 
-IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status) {
+IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status, int j0,
+                           int j1) {
   *status = MGPU_OK;
+  if (j1 < 0) j1 = s.ny;
   if (cfg.solver_type != MGPU_ITER_BICGSTAB && cfg.solver_type != MGPU_ITER_CG) {
     std::fprintf(stderr, "iterative solver: unknown solver_type %d\n", cfg.solver_type);
     *status = MGPU_ERR_UNSUPPORTED;
@@ -557,9 +591,9 @@ IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_conf
   };
   if (dev_alloc(it, (void**)&it->coef, c.size() * sizeof(double))) return fail(MGPU_ERR_CUDA);
   cudaMemcpy(it->coef, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice);
-  it->g = Geom{s.nx, s.ny, nz, it->symm ? 1 : 0, s.plane, A_n, A_e, it->coef};
+  it->g = Geom{s.nx, s.ny, nz, it->symm ? 1 : 0, s.plane, A_n, A_e, it->coef, j0, j1};
   it->block = dim3(BX, BY, 1);
-  it->grid_col = dim3((s.nx + BX - 1) / BX, (s.ny + BY - 1) / BY, 1);
+  it->grid_col = dim3((s.nx + BX - 1) / BX, (j1 - j0 + BY - 1) / BY, 1);
   it->grid_pt = dim3(it->grid_col.x, it->grid_col.y, nz - 1);
   it->nblocks = (int)(it->grid_pt.x * it->grid_pt.y * it->grid_pt.z);
   if (dev_alloc(it, (void**)&it->partials, sizeof(double) * 3 * (size_t)it->nblocks)) return fail(MGPU_ERR_CUDA);
@@ -740,6 +774,100 @@ static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream
   *iterations = total;
   *residual = err;
   return rc;
+}
+
+// ---- BiCGStab over y-slabs, one step at a time -----------------------------------------------
+// The driver runs the iteration of run_bicgstab step by step, exchanging the halo rows of x, pp
+// and cs before the steps that apply A to them and summing each step's dot products over the
+// slabs before iter_slab_finish closes the reduction.
+int iter_slab_begin(IterSolverDev* it, const double* p, size_t bytes, cudaStream_t st) {
+  if (!it || it->fp32 || it->symm) return MGPU_ERR_UNSUPPORTED;
+  // psource = p; the initial guess is the previous solution (iterativesolver.F90:95-106)
+  if (cudaMemcpyAsync(it->w64.b, p, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
+  IterScalars init{};
+  init.tol = it->tol;
+  init.ext = 1;
+  it->st_host[0] = init;
+  if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return MGPU_ERR_CUDA;
+  it->pending = -1;
+  return MGPU_OK;
+}
+
+int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st, int64_t* launches) {
+  Work<double>& w = it->w64;
+  const Geom& g = it->g;
+  int nsum = 0;
+  switch (step) {
+    case MGPU_SLAB_ITER_INIT:
+      k_bicg_init<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, w.cr, it->partials, it->nblocks, it->st,
+                                                             0.0001);
+      it->pending = 0;
+      nsum = 2;
+      break;
+    case MGPU_SLAB_ITER_DIRECTION:
+      k_bicg_direction<double><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.pp, w.tmp, it->st);
+      break;
+    case MGPU_SLAB_ITER_APPLY:
+      k_bicg_apply_dot<double><<<it->grid_pt, it->block, 0, st>>>(g, w.pp, w.cr, w.v, it->partials, it->nblocks, it->st);
+      it->pending = 1;
+      nsum = 1;
+      break;
+    case MGPU_SLAB_ITER_HALF_STEP:
+      k_bicg_half_step<double><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.s, w.cs, w.tmp, it->st);
+      break;
+    case MGPU_SLAB_ITER_APPLY2:
+      k_bicg_apply_dots<double><<<it->grid_pt, it->block, 0, st>>>(g, w.cs, w.s, w.t, it->partials, it->nblocks, it->st);
+      it->pending = 2;
+      nsum = 3;
+      break;
+    case MGPU_SLAB_ITER_UPDATE:
+      k_bicg_update<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.pp, w.cs, w.s, w.t, w.r, w.cr, it->partials,
+                                                               it->nblocks, it->st, it->max_it);
+      it->pending = 3;
+      nsum = 1;
+      break;
+    default:
+      return MGPU_ERR_ARGUMENT;
+  }
+  *launches += 1;
+  if (nsum) {
+    // this slab's sums (zeros past nsum), for the driver to add over the slabs
+    if (cudaMemsetAsync(d_sums, 0, 3 * sizeof(double), st) != cudaSuccess ||
+        cudaMemcpyAsync(d_sums, reinterpret_cast<const char*>(it->st) + offsetof(IterScalars, loc),
+                        nsum * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
+}
+
+int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done) {
+  if (it->pending < 0) return MGPU_ERR_ARGUMENT;
+  k_bicg_finish<<<1, 32, 0, st>>>(it->st, d_sums, it->pending, 0.0001, it->max_it);
+  *launches += 1;
+  it->pending = -1;
+  if (cudaMemcpyAsync(it->st_host, it->st, sizeof(IterScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return MGPU_ERR_CUDA;
+  *done = it->st_host->done;
+  return MGPU_OK;
+}
+
+int iter_slab_end(IterSolverDev* it, double* p, size_t bytes, cudaStream_t st, int* iterations, double* residual) {
+  if (cudaMemcpyAsync(p, it->w64.x, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
+  *iterations = it->st_host->it_done;
+  *residual = it->st_host->err;
+  return it->st_host->err < it->tol ? MGPU_OK : MGPU_ERR_NOT_CONVERGED;
+}
+
+double* iter_slab_vector(IterSolverDev* it, int set) {
+  if (!it || it->fp32) return nullptr;
+  switch (set) {
+    case MGPU_HALO_ITER_X: return it->w64.x;
+    case MGPU_HALO_ITER_PP: return it->w64.pp;
+    case MGPU_HALO_ITER_CS: return it->w64.cs;
+  }
+  return nullptr;
 }
 
 template <typename T>

@@ -140,6 +140,15 @@ class LoopbackComm:
             b.copy_(total)
         self._sync(bufs[0])
 
+    def allreduce_sum_inplace(self, bufs):
+        self._sync(bufs[0])
+        total = bufs[0].clone()
+        for b in bufs[1:]:
+            total += b
+        for b in bufs:
+            b.copy_(total)
+        self._sync(bufs[0])
+
     def allreduce_max(self, bufs):
         self._sync(bufs[0])
         top = bufs[0].clone()
@@ -212,6 +221,10 @@ class TorchComm:
             dist.all_reduce(bufs[0], group=self.group)
             bufs[0].div_(self.size)
 
+    def allreduce_sum_inplace(self, bufs):
+        with self._ctx():
+            dist.all_reduce(bufs[0], group=self.group)
+
     def allreduce_max(self, bufs):
         with self._ctx():
             dist.all_reduce(bufs[0], op=dist.ReduceOp.MAX, group=self.group)
@@ -250,6 +263,8 @@ class _Slab:
         self.profiles = torch.zeros((6 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
         # cfltest's six extrema, every one combined by a maximum (mgpu_slab_cfl_extrema)
         self.cfl = torch.zeros(6, dtype=torch.float64, device=device)
+        # the iterative solve's dot products of one step (mgpu_slab_iter)
+        self.sums = torch.zeros(3, dtype=torch.float64, device=device)
 
         def cview(buf, off, n):
             return buf[2 * off:2 * (off + n)]
@@ -269,6 +284,10 @@ class SlabDomain:
         self.geo = SlabGeometry(cfg.nx, cfg.ny, cfg.nz, comm.size, halo)
         # the library keeps the mean profiles when damping, mean-profile subsidence or
         # profile_diagnostics reads them
+        # the pressure solve: the distributed FFT, or iterativesolver's BiCGStab (FP64)
+        self.iterative = cfg.solver == cf.SOLVER_ITERATIVE
+        if self.iterative and (cfg.precision != cf.FP64 or cfg.solver_type != cf.ITER_BICGSTAB):
+            raise ValueError("the decomposed iterative solve is FP64 BiCGStab")
         self.mean_profiles = bool(cfg.damping_enabled or cfg.profile_diagnostics_enabled
                                   or (cfg.l_subs_pl_theta and not cfg.subsidence_local_theta)
                                   or (cfg.l_subs_pl_q and not cfg.subsidence_local_q and cfg.number_q_fields > 0))
@@ -322,6 +341,7 @@ class SlabDomain:
 
     # -- stepping
     def _exchange(self, halo_set: int, depth: int):
+        # one-field sets (p and the solver vectors, depth 1) share the pressure buffers
         bufs = [s.state_bufs if halo_set == cf.HALO_STATE else s.p_bufs for s in self.slabs]
         for s, b in zip(self.slabs, bufs):
             s.m.halo_pack(halo_set, depth, b[0].data_ptr(), b[1].data_ptr())
@@ -349,7 +369,8 @@ class SlabDomain:
                 self.comm.allreduce_mean([s.means for s in self.slabs])
             for s in self.slabs:
                 s.m.step_phase(cf.PHASE_DYNAMICS)
-                s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, False)
+                if not self.iterative:
+                    s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, False)
             if self.mean_profiles:
                 # each slab's means of this step, averaged over the slabs for the next step
                 for s in self.slabs:
@@ -357,16 +378,47 @@ class SlabDomain:
                 self.comm.allreduce_mean([s.profiles for s in self.slabs])
                 for s in self.slabs:
                     s.m.slab_mean_profiles(s.profiles.data_ptr(), True)
-            self.comm.all_to_all([s.x_blocks for s in self.slabs], [s.t_blocks for s in self.slabs])
-            for s in self.slabs:
-                k0, w = g.blocks[s.rank]
-                s.m.slab_solve_columns(s.spec_t.data_ptr(), k0, w, g.nyl)
-            self.comm.all_to_all([s.t_blocks for s in self.slabs], [s.x_blocks for s in self.slabs])
-            for s in self.slabs:
-                s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, True)
+            if self.iterative:
+                self._iterative_solve()
+            else:
+                self.comm.all_to_all([s.x_blocks for s in self.slabs], [s.t_blocks for s in self.slabs])
+                for s in self.slabs:
+                    k0, w = g.blocks[s.rank]
+                    s.m.slab_solve_columns(s.spec_t.data_ptr(), k0, w, g.nyl)
+                self.comm.all_to_all([s.t_blocks for s in self.slabs], [s.x_blocks for s in self.slabs])
+                for s in self.slabs:
+                    s.m.slab_fft_x(s.spec_x.data_ptr(), g.nranks, True)
             self._exchange(cf.HALO_PRESSURE, 1)
             for s in self.slabs:
                 s.m.step_phase(cf.PHASE_PSTEP)
+
+    def _reduce_step(self, step: int) -> bool:
+        """A reducing BiCGStab step on every slab, its sums added over the slabs, then FINISH."""
+        for s in self.slabs:
+            s.m.slab_iter(step, s.sums.data_ptr())
+        self.comm.allreduce_sum_inplace([s.sums for s in self.slabs])
+        done = [s.m.slab_iter(cf.SLAB_ITER_FINISH, s.sums.data_ptr()) for s in self.slabs]
+        return done[0]
+
+    def _iterative_solve(self):
+        """iterativesolver's BiCGStab over the slabs (mgpu_slab_iter): halo rows of the vectors A
+        is applied to, and every inner product summed over the slabs (inner_prod's allreduce)."""
+        for s in self.slabs:
+            s.m.slab_iter(cf.SLAB_ITER_BEGIN)
+        self._exchange(cf.HALO_ITER_X, 1)
+        done = self._reduce_step(cf.SLAB_ITER_INIT)
+        while not done:
+            for s in self.slabs:
+                s.m.slab_iter(cf.SLAB_ITER_DIRECTION)
+            self._exchange(cf.HALO_ITER_PP, 1)
+            self._reduce_step(cf.SLAB_ITER_APPLY)
+            for s in self.slabs:
+                s.m.slab_iter(cf.SLAB_ITER_HALF_STEP)
+            self._exchange(cf.HALO_ITER_CS, 1)
+            self._reduce_step(cf.SLAB_ITER_APPLY2)
+            done = self._reduce_step(cf.SLAB_ITER_UPDATE)
+        for s in self.slabs:
+            s.m.slab_iter(cf.SLAB_ITER_END)
 
     def profile_diagnostics(self) -> dict:
         """profile_diagnostics sums over the whole domain: each slab's totals over its interior rows

@@ -10,6 +10,8 @@ after all queued work has finished; no kernel waits on another slab).
   averaged over the slabs and the diagnostics sums added over them match the single domain.
 * cfltest on the slabs: the extrema combined by a maximum give the single domain's dtm sequence,
   and the fields of the adaptive-dtm run bit for bit.
+* iterativesolver's BiCGStab on the slabs: the inner products summed over the slabs, the
+  iterates match the single domain's to rounding.
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
 import os
@@ -257,6 +259,59 @@ def test_fp32_mixed_cfl_on_slabs_follows_single_domain(gpu_lib):
         assert abs(d.slabs[0].m.reductions().dtm - m.reductions().dtm) <= 1e-5 * c.dtm, n
     d.close()
     m.close()
+
+
+def iterative_config(tol, max_it):
+    c = dry_config()
+    c.solver = cf.SOLVER_ITERATIVE
+    c.solver_type = cf.ITER_BICGSTAB
+    c.tolerance = tol
+    c.max_iterations = max_it
+    return c
+
+
+@pytest.mark.parametrize("nranks", [2, 4])
+def test_bicgstab_on_slabs_fixed_iterations(gpu_lib, nranks):
+    """BiCGStab over the slabs (halo rows of x, pp, cs; every inner product summed over the slabs)
+    with the tolerance out of reach: the same 8 iterations per step as the single domain, whose
+    iterates differ only by the order of the dot-product sums (1e-10 after 3 steps)."""
+    c = iterative_config(1e-30, 8)
+    st = dry_state()
+    m = api.Model(c)
+    m.set_state(st)
+    m.step(3)
+    ref = {f: m.download(f) for f in STATE + ["p"]}
+    assert m.reductions().solver_iterations == 8
+    m.close()
+    d = dc.SlabDomain(c, dc.LoopbackComm(nranks))
+    d.set_state(st)
+    d.step(3)
+    for s in d.slabs:
+        assert s.m.reductions().solver_iterations == 8
+    for f in STATE + ["p"]:
+        assert np.abs(d.download(f) - ref[f]).max() <= 1e-10 * np.abs(ref[f]).max(), f
+    d.close()
+
+
+def test_bicgstab_on_slabs_to_tolerance(gpu_lib):
+    """Solved to a tolerance: every slab stops at the same iteration, within one of the single
+    domain's, with the residual met."""
+    c = iterative_config(1e-10, 500)
+    st = dry_state()
+    m = api.Model(c)
+    m.set_state(st)
+    m.step(3)
+    ref = {f: m.download(f) for f in STATE}
+    its = m.reductions().solver_iterations
+    m.close()
+    d = dc.SlabDomain(c, dc.LoopbackComm(4))
+    d.set_state(st)
+    d.step(3)
+    got = [(s.m.reductions().solver_iterations, s.m.reductions().solver_residual) for s in d.slabs]
+    assert len(set(got)) == 1 and abs(got[0][0] - its) <= 1 and got[0][1] < 1e-10
+    for f in STATE:
+        assert np.abs(d.download(f) - ref[f]).max() <= 1e-8 * np.abs(ref[f]).max(), f
+    d.close()
 
 
 def test_halo_rows_pack_and_unpack(gpu_lib):
