@@ -135,6 +135,18 @@ def run_slab_checks(comm, ranks):
     comm.allreduce_mean([means[r] for r in ranks])
     for r in ranks:
         np.testing.assert_allclose(means[r].numpy(), full.mean(axis=(1, 2)), rtol=1e-14, atol=1e-15)
+    # cfltest's extrema in max form (minima negated): one maximum gives the domain's min and max
+    ext = {r: torch.tensor([-full[:, g.y0(r):g.y0(r) + g.nyl].min(), full[:, g.y0(r):g.y0(r) + g.nyl].max()])
+           for r in ranks}
+    comm.allreduce_max([ext[r] for r in ranks])
+    for r in ranks:
+        assert (-ext[r][0].item(), ext[r][1].item()) == (full.min(), full.max())
+    # inner products of the iterative solve: the slabs' partial sums add up to the domain's
+    dots = {r: torch.tensor([(full[:, g.y0(r):g.y0(r) + g.nyl] ** 2).sum(), float(g.nyl), 0.0]) for r in ranks}
+    comm.allreduce_sum_inplace([dots[r] for r in ranks])
+    for r in ranks:
+        np.testing.assert_allclose(dots[r][0].item(), (full ** 2).sum(), rtol=1e-13)
+        assert dots[r][1].item() == NY and dots[r][2].item() == 0.0
 
 
 @pytest.mark.parametrize("nranks", [1, 2, 4])
