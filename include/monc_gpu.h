@@ -438,6 +438,7 @@ int mgpu_step_phase(mgpu_handle* h, int32_t phase);
 #define MGPU_HALO_ITER_X    2   /* BiCGStab on slabs: the iterate x (before MGPU_SLAB_ITER_INIT) */
 #define MGPU_HALO_ITER_PP   3   /* the search direction pp (before MGPU_SLAB_ITER_APPLY) */
 #define MGPU_HALO_ITER_CS   4   /* the preconditioned half step cs (before MGPU_SLAB_ITER_APPLY2) */
+#define MGPU_HALO_ITER_CG   5   /* conjugate gradients: z and the old direction p (before APPLY) */
 int mgpu_halo_fields(mgpu_handle* h, int32_t set);
 int mgpu_halo_pack(mgpu_handle* h, int32_t set, int32_t depth, void* d_lo, void* d_hi);
 int mgpu_halo_unpack(mgpu_handle* h, int32_t set, int32_t depth, const void* d_lo, const void* d_hi);
@@ -466,9 +467,10 @@ int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put);
  * step gathered; on other steps the call does nothing, and every slab takes the same steps. */
 int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* gathered);
 
-/* iterativesolver's BiCGStab on slabs (iterativesolver.F90:140-248; MONC sums the inner products
- * over its ranks with MPI_Allreduce in inner_prod, :500-553), FP64 models with solver_type
- * MGPU_ITER_BICGSTAB, in place of the FFT steps between the dynamics and pressure-step phases:
+/* iterativesolver on slabs (bicgstab, iterativesolver.F90:140-248, and cg_solver, :255-321; MONC
+ * sums the inner products over its ranks with MPI_Allreduce in inner_prod, :500-553), FP64 models,
+ * in place of the FFT steps between the dynamics and pressure-step phases.  solver_type
+ * MGPU_ITER_BICGSTAB:
  *
  *   BEGIN                                     psource = p; the iterate x keeps the last solution
  *   halo exchange of MGPU_HALO_ITER_X (depth 1)
@@ -497,6 +499,16 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
 #define MGPU_SLAB_ITER_UPDATE     6
 #define MGPU_SLAB_ITER_FINISH     7
 #define MGPU_SLAB_ITER_END        8
+#define MGPU_SLAB_ITER_PRECOND    9
+/* solver_type MGPU_ITER_CG (MONC's default; the symmetric form of the operator):
+ *
+ *   BEGIN; halo exchange of MGPU_HALO_ITER_X; INIT, sum, FINISH     r = b A_vol - A x
+ *   until FINISH after UPDATE reports done:
+ *     PRECOND, sum, FINISH                    z = M^-1 r; <z, r>
+ *     halo exchange of MGPU_HALO_ITER_CG (depth 1)
+ *     APPLY, sum, FINISH                      p' = z + bet p; A p'; <p', A p'>
+ *     UPDATE, sum, FINISH                     x, r; |r|^2; convergence
+ *   END */
 int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done);
 
 /* x-FFT (fftsolver.F90:50-309 transforms, x pass) between the interior rows of p and d_spec,

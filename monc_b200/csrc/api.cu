@@ -1319,9 +1319,11 @@ static int halo_set(mgpu_handle* h, DevState<T>& d, int set, T** f) {
     f[n++] = d.p;
     return n;
   }
-  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CS && sizeof(T) == 8 && h->iter) {
-    f[n++] = reinterpret_cast<T*>(iter_slab_vector(h->iter, set));
-    return f[0] ? n : -1;
+  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CG && sizeof(T) == 8 && h->iter) {
+    double* v[2] = {nullptr, nullptr};
+    const int nv = iter_slab_vectors(h->iter, set, v);
+    for (int q = 0; q < nv; ++q) f[q] = reinterpret_cast<T*>(v[q]);
+    return nv;
   }
   return -1;
 }
@@ -1382,9 +1384,9 @@ int mgpu_halo_fields(mgpu_handle* h, int32_t set) {
   if (!h) return MGPU_ERR_ARGUMENT;
   if (set == MGPU_HALO_STATE) return 8 + 2 * h->cfg.number_q_fields;
   if (set == MGPU_HALO_PRESSURE) return 1;
-  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CS) {
+  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CG) {
     if (!h->iter || h->fp32) return fail(h, MGPU_ERR_ARGUMENT, "the solver vectors exist after MGPU_SLAB_ITER_BEGIN");
-    return 1;
+    return set == MGPU_HALO_ITER_CG ? 2 : 1;
   }
   return fail(h, MGPU_ERR_ARGUMENT, "unknown halo set");
 }
@@ -1447,8 +1449,7 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
 int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done) {
   if (!h) return MGPU_ERR_ARGUMENT;
   if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
-  if (h->fp32 || h->cfg.solver_type != MGPU_ITER_BICGSTAB)
-    return fail(h, MGPU_ERR_UNSUPPORTED, "the slab iterative solve is FP64 BiCGStab");
+  if (h->fp32) return fail(h, MGPU_ERR_UNSUPPORTED, "the slab iterative solve runs in FP64 models");
   const size_t bytes = field_elems(h) * sizeof(double);
   if (step == MGPU_SLAB_ITER_BEGIN) {
     if (!h->iter) {
@@ -1466,7 +1467,8 @@ int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done) 
     return MGPU_OK;  // not converged: MONC only warns (iterativesolver.F90:240-242); see mgpu_get_reductions
   }
   const bool reduces = step == MGPU_SLAB_ITER_INIT || step == MGPU_SLAB_ITER_APPLY || step == MGPU_SLAB_ITER_APPLY2 ||
-                       step == MGPU_SLAB_ITER_UPDATE || step == MGPU_SLAB_ITER_FINISH;
+                       step == MGPU_SLAB_ITER_UPDATE || step == MGPU_SLAB_ITER_FINISH ||
+                       step == MGPU_SLAB_ITER_PRECOND;
   if (reduces && !d_sums) return fail(h, MGPU_ERR_ARGUMENT, "this step needs d_sums");
   if (step == MGPU_SLAB_ITER_FINISH) {
     int dn = 0;

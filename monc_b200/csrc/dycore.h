@@ -117,12 +117,13 @@ int launch_profile_diagnostics(const Scalars& s, const T* u, const T* v, const T
 struct IterSolverDev;
 IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status,
                            int j0 = 0, int j1 = -1);
-// BiCGStab over y-slabs (FP64), one step at a time (iter.cu)
+// BiCGStab and conjugate gradients over y-slabs (FP64), one step at a time (iter.cu)
 int iter_slab_begin(IterSolverDev* it, const double* p, size_t bytes, cudaStream_t st);
 int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st, int64_t* launches);
 int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done);
 int iter_slab_end(IterSolverDev* it, double* p, size_t bytes, cudaStream_t st, int* iterations, double* residual);
-double* iter_slab_vector(IterSolverDev* it, int set);
+// the halo set's solver vectors into f (at most 2); returns their number, or -1
+int iter_slab_vectors(IterSolverDev* it, int set, double** f);
 void iter_destroy(IterSolverDev* it);
 template <typename T>
 int iter_solve(IterSolverDev* it, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, int* iterations,

@@ -126,7 +126,7 @@ __device__ bool last_block_sums(IterScalars* st, const double* partials, int nbl
 }
 
 // The scalar updates that close each reduction (the same code for one domain, where the last
-// block runs them, and for y-slabs, where k_bicg_finish runs them on the sums over the slabs).
+// block runs them, and for y-slabs, where k_iter_finish runs them on the sums over the slabs).
 __device__ void finish_init(IterScalars* st, const double* s, double sc_floor) {
   st->sc_err = fmax(sqrt(s[1]), sc_floor);
   st->rho = s[0];
@@ -151,6 +151,33 @@ __device__ void finish_apply_dots(IterScalars* st, const double* s) {
 __device__ void finish_update(IterScalars* st, const double* s, int max_it) {
   st->rho_prev = st->rho;
   st->rho = s[0];
+  st->it_done = st->it;
+  st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
+  st->it += 1;
+}
+// conjugate gradients: sums <b, b>, <r, r> (MONC's loop runs at least one iteration, so init
+// never marks the solve done)
+__device__ void finish_cg_init(IterScalars* st, const double* s, double sc_floor) {
+  st->sc_err = fmax(sqrt(s[0]), sc_floor);
+  st->err = sqrt(s[1]) / st->sc_err;
+  st->rho = 0.0;
+  st->alf = 0.0;
+  st->bet = 0.0;
+  st->it = 1;
+  st->it_done = 0;
+  st->done = 0;
+}
+// <z, r>: bet = <z, r> / rho and rho = <z, r> (iteration 1: rho = <z, r>)
+__device__ void finish_cg_precond(IterScalars* st, const double* s) {
+  st->bet = st->it == 1 ? 0.0 : s[0] / st->rho;
+  st->rho = s[0];
+  st->alf = s[0];
+}
+// <p', Ap'>: alf = rho / <p', Ap'>
+__device__ void finish_cg_apply(IterScalars* st, const double* s) { st->alf = st->alf / s[0]; }
+// |r|^2: err, convergence
+__device__ void finish_cg_update(IterScalars* st, const double* s, int max_it) {
+  st->err = sqrt(s[0]) / st->sc_err;
   st->it_done = st->it;
   st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
   st->it += 1;
@@ -316,17 +343,22 @@ __global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __re
   if (last_block_sums<1>(st, partials, nblocks, s)) finish_update(st, s, max_it);
 }
 
-// y-slabs: close reduction `which` (0 init, 1 apply_dot, 2 apply_dots, 3 update) with the sums
-// over all slabs
-__global__ void k_bicg_finish(IterScalars* st, const double* __restrict__ sums, int which, double sc_floor,
+// y-slabs: close reduction `which` with the sums over all slabs: BiCGStab 0 init, 1 apply_dot,
+// 2 apply_dots, 3 update; conjugate gradients 4 init, 5 precond, 6 apply, 7 update
+__global__ void k_iter_finish(IterScalars* st, const double* __restrict__ sums, int which, double sc_floor,
                               int max_it) {
   if (threadIdx.x != 0) return;
   const double s[3] = {sums[0], sums[1], sums[2]};
+  if (which == 0) { finish_init(st, s, sc_floor); return; }
+  if (which == 4) { finish_cg_init(st, s, sc_floor); return; }
+  if (st->done) return;
   switch (which) {
-    case 0: finish_init(st, s, sc_floor); break;
-    case 1: if (!st->done) finish_apply_dot(st, s); break;
-    case 2: if (!st->done) finish_apply_dots(st, s); break;
-    default: if (!st->done) finish_update(st, s, max_it); break;
+    case 1: finish_apply_dot(st, s); break;
+    case 2: finish_apply_dots(st, s); break;
+    case 3: finish_update(st, s, max_it); break;
+    case 5: finish_cg_precond(st, s); break;
+    case 6: finish_cg_apply(st, s); break;
+    default: finish_cg_update(st, s, max_it); break;
   }
 }
 
@@ -350,16 +382,7 @@ __global__ void __launch_bounds__(NTH) k_cg_init(Geom g, const W* __restrict__ x
   }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
-  if (last_block_sums<2>(st, partials, nblocks, s)) {
-    st->sc_err = fmax(sqrt(s[0]), sc_floor);
-    st->err = sqrt(s[1]) / st->sc_err;
-    st->rho = 0.0;
-    st->alf = 0.0;
-    st->bet = 0.0;
-    st->it = 1;
-    st->it_done = 0;
-    st->done = 0;
-  }
+  if (last_block_sums<2>(st, partials, nblocks, s)) finish_cg_init(st, s, sc_floor);
 }
 
 // z = M^-1 r per column, <z, r>; bet = <z, r> / rho and rho = <z, r> (iteration 1: rho = <z, r>)
@@ -384,15 +407,7 @@ __global__ void __launch_bounds__(NTH) k_cg_precond(Geom g, const W* __restrict_
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
-  if (last_block_sums<1>(st, partials, nblocks, s)) {
-    if (st->it == 1) {
-      st->bet = 0.0;
-    } else {
-      st->bet = s[0] / st->rho;
-    }
-    st->rho = s[0];
-    st->alf = s[0];
-  }
+  if (last_block_sums<1>(st, partials, nblocks, s)) finish_cg_precond(st, s);
 }
 
 // p' = z + bet*p (p' = z on iteration 1) into p_new, Ap' into Ax, alf = rho / <p', Ap'>.  Every
@@ -422,7 +437,7 @@ __global__ void __launch_bounds__(NTH) k_cg_apply(Geom g, const W* __restrict__ 
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
-  if (last_block_sums<1>(st, partials, nblocks, s)) st->alf = st->alf / s[0];
+  if (last_block_sums<1>(st, partials, nblocks, s)) finish_cg_apply(st, s);
 }
 
 // x += alf*p', r -= alf*Ap', err = |r| / sc_err, convergence
@@ -442,12 +457,7 @@ __global__ void __launch_bounds__(NTH) k_cg_update(Geom g, W* x, const W* __rest
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
-  if (last_block_sums<1>(st, partials, nblocks, s)) {
-    st->err = sqrt(s[0]) / st->sc_err;
-    st->it_done = st->it;
-    st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
-    st->it += 1;
-  }
+  if (last_block_sums<1>(st, partials, nblocks, s)) finish_cg_update(st, s, max_it);
 }
 
 // FP64 residual of the refinement: r = b - A x (levels 2..nz) with <r, r>, <b, b>
@@ -530,6 +540,7 @@ struct IterSolverDev {
   Work<float> w32{};
   double* r64 = nullptr;  // refinement residual (FP32-mixed model)
   int pending = -1;       // y-slab steps: the reduction iter_slab_finish closes next
+  int cg_n = 0;           // y-slab conjugate gradients: iterations done (which direction buffer is old)
   std::vector<void*> allocs;
   dim3 grid_pt, grid_col, block;
 };
@@ -781,7 +792,7 @@ static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream
 // and cs before the steps that apply A to them and summing each step's dot products over the
 // slabs before iter_slab_finish closes the reduction.
 int iter_slab_begin(IterSolverDev* it, const double* p, size_t bytes, cudaStream_t st) {
-  if (!it || it->fp32 || it->symm) return MGPU_ERR_UNSUPPORTED;
+  if (!it || it->fp32) return MGPU_ERR_UNSUPPORTED;
   // psource = p; the initial guess is the previous solution (iterativesolver.F90:95-106)
   if (cudaMemcpyAsync(it->w64.b, p, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
   IterScalars init{};
@@ -791,14 +802,53 @@ int iter_slab_begin(IterSolverDev* it, const double* p, size_t bytes, cudaStream
   if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return MGPU_ERR_CUDA;
   it->pending = -1;
+  it->cg_n = 0;
   return MGPU_OK;
+}
+
+// the two search-direction buffers of conjugate gradients alternate: p_old = pbuf[n & 1]
+static double* cg_p(IterSolverDev* it, int n) { return (n & 1) ? it->w64.cs : it->w64.pp; }
+
+static int cg_slab_step(IterSolverDev* it, int step, int* nsum, cudaStream_t st) {
+  Work<double>& w = it->w64;
+  const Geom& g = it->g;
+  const int ncol = (int)(it->grid_col.x * it->grid_col.y);
+  switch (step) {
+    case MGPU_SLAB_ITER_INIT:
+      // MONC's symmetric form: the right-hand side scaled by A_vol (run_cg with scale_rhs)
+      k_cg_init<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, it->partials, it->nblocks, it->st, 0.0001, 1);
+      it->pending = 4;
+      *nsum = 2;
+      return MGPU_OK;
+    case MGPU_SLAB_ITER_PRECOND:
+      k_cg_precond<double><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.s, w.tmp, it->partials, ncol, it->st);
+      it->pending = 5;
+      *nsum = 1;
+      return MGPU_OK;
+    case MGPU_SLAB_ITER_APPLY:
+      k_cg_apply<double><<<it->grid_pt, it->block, 0, st>>>(g, w.s, cg_p(it, it->cg_n), cg_p(it, it->cg_n + 1), w.v,
+                                                            it->partials, it->nblocks, it->st);
+      it->pending = 6;
+      *nsum = 1;
+      return MGPU_OK;
+    case MGPU_SLAB_ITER_UPDATE:
+      k_cg_update<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, cg_p(it, it->cg_n + 1), w.v, w.r, it->partials,
+                                                             it->nblocks, it->st, it->max_it);
+      it->cg_n += 1;
+      it->pending = 7;
+      *nsum = 1;
+      return MGPU_OK;
+  }
+  return MGPU_ERR_ARGUMENT;
 }
 
 int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st, int64_t* launches) {
   Work<double>& w = it->w64;
   const Geom& g = it->g;
   int nsum = 0;
-  switch (step) {
+  if (it->symm) {
+    if (int rc = cg_slab_step(it, step, &nsum, st)) return rc;
+  } else switch (step) {
     case MGPU_SLAB_ITER_INIT:
       k_bicg_init<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, w.cr, it->partials, it->nblocks, it->st,
                                                              0.0001);
@@ -843,7 +893,7 @@ int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st,
 
 int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done) {
   if (it->pending < 0) return MGPU_ERR_ARGUMENT;
-  k_bicg_finish<<<1, 32, 0, st>>>(it->st, d_sums, it->pending, 0.0001, it->max_it);
+  k_iter_finish<<<1, 32, 0, st>>>(it->st, d_sums, it->pending, 0.0001, it->max_it);
   *launches += 1;
   it->pending = -1;
   if (cudaMemcpyAsync(it->st_host, it->st, sizeof(IterScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -860,14 +910,20 @@ int iter_slab_end(IterSolverDev* it, double* p, size_t bytes, cudaStream_t st, i
   return it->st_host->err < it->tol ? MGPU_OK : MGPU_ERR_NOT_CONVERGED;
 }
 
-double* iter_slab_vector(IterSolverDev* it, int set) {
-  if (!it || it->fp32) return nullptr;
+int iter_slab_vectors(IterSolverDev* it, int set, double** f) {
+  if (!it || it->fp32) return -1;
   switch (set) {
-    case MGPU_HALO_ITER_X: return it->w64.x;
-    case MGPU_HALO_ITER_PP: return it->w64.pp;
-    case MGPU_HALO_ITER_CS: return it->w64.cs;
+    case MGPU_HALO_ITER_X: f[0] = it->w64.x; return 1;
+    case MGPU_HALO_ITER_PP: f[0] = it->w64.pp; return 1;
+    case MGPU_HALO_ITER_CS: f[0] = it->w64.cs; return 1;
+    case MGPU_HALO_ITER_CG:
+      // conjugate gradients: z and the old direction, from which k_cg_apply forms p' at the
+      // neighbours of each interior point
+      f[0] = it->w64.s;
+      f[1] = cg_p(it, it->cg_n);
+      return 2;
   }
-  return nullptr;
+  return -1;
 }
 
 template <typename T>

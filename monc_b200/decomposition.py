@@ -257,7 +257,8 @@ class _Slab:
         nf = model.halo_fields(cf.HALO_STATE)
         # send below, send above, received from below, received from above
         self.state_bufs = [torch.zeros(nf * g.nz * g.halo * g.nx, dtype=dtype, device=device) for _ in range(4)]
-        self.p_bufs = [torch.zeros(g.nz * g.nx, dtype=dtype, device=device) for _ in range(4)]
+        # depth-1 sets of one or two fields: p, the iterative solve's vectors
+        self.p_bufs = [torch.zeros(2 * g.nz * g.nx, dtype=dtype, device=device) for _ in range(4)]
         self.means = torch.zeros((1 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
         # the mean profiles damping, subsidence and profile_diagnostics read (mgpu_slab_mean_profiles)
         self.profiles = torch.zeros((6 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
@@ -286,8 +287,8 @@ class SlabDomain:
         # profile_diagnostics reads them
         # the pressure solve: the distributed FFT, or iterativesolver's BiCGStab (FP64)
         self.iterative = cfg.solver == cf.SOLVER_ITERATIVE
-        if self.iterative and (cfg.precision != cf.FP64 or cfg.solver_type != cf.ITER_BICGSTAB):
-            raise ValueError("the decomposed iterative solve is FP64 BiCGStab")
+        if self.iterative and cfg.precision != cf.FP64:
+            raise ValueError("the decomposed iterative solve runs in FP64")
         self.mean_profiles = bool(cfg.damping_enabled or cfg.profile_diagnostics_enabled
                                   or (cfg.l_subs_pl_theta and not cfg.subsidence_local_theta)
                                   or (cfg.l_subs_pl_q and not cfg.subsidence_local_q and cfg.number_q_fields > 0))
@@ -341,7 +342,7 @@ class SlabDomain:
 
     # -- stepping
     def _exchange(self, halo_set: int, depth: int):
-        # one-field sets (p and the solver vectors, depth 1) share the pressure buffers
+        # the depth-1 sets (p and the solver vectors) share the pressure buffers
         bufs = [s.state_bufs if halo_set == cf.HALO_STATE else s.p_bufs for s in self.slabs]
         for s, b in zip(self.slabs, bufs):
             s.m.halo_pack(halo_set, depth, b[0].data_ptr(), b[1].data_ptr())
@@ -401,12 +402,23 @@ class SlabDomain:
         return done[0]
 
     def _iterative_solve(self):
-        """iterativesolver's BiCGStab over the slabs (mgpu_slab_iter): halo rows of the vectors A
-        is applied to, and every inner product summed over the slabs (inner_prod's allreduce)."""
+        """iterativesolver over the slabs (mgpu_slab_iter), BiCGStab or conjugate gradients: halo
+        rows of the vectors A is applied to, and every inner product summed over the slabs
+        (inner_prod's allreduce)."""
         for s in self.slabs:
             s.m.slab_iter(cf.SLAB_ITER_BEGIN)
         self._exchange(cf.HALO_ITER_X, 1)
         done = self._reduce_step(cf.SLAB_ITER_INIT)
+        if self.cfg.solver_type == cf.ITER_CG:
+            done = False  # cg_solver runs at least one iteration
+            while not done:
+                self._reduce_step(cf.SLAB_ITER_PRECOND)
+                self._exchange(cf.HALO_ITER_CG, 1)
+                self._reduce_step(cf.SLAB_ITER_APPLY)
+                done = self._reduce_step(cf.SLAB_ITER_UPDATE)
+            for s in self.slabs:
+                s.m.slab_iter(cf.SLAB_ITER_END)
+            return
         while not done:
             for s in self.slabs:
                 s.m.slab_iter(cf.SLAB_ITER_DIRECTION)

@@ -10,8 +10,8 @@ after all queued work has finished; no kernel waits on another slab).
   averaged over the slabs and the diagnostics sums added over them match the single domain.
 * cfltest on the slabs: the extrema combined by a maximum give the single domain's dtm sequence,
   and the fields of the adaptive-dtm run bit for bit.
-* iterativesolver's BiCGStab on the slabs: the inner products summed over the slabs, the
-  iterates match the single domain's to rounding.
+* iterativesolver on the slabs, BiCGStab and conjugate gradients: the inner products summed over
+  the slabs, the iterates match the single domain's to rounding.
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
 import os
@@ -261,21 +261,26 @@ def test_fp32_mixed_cfl_on_slabs_follows_single_domain(gpu_lib):
     m.close()
 
 
-def iterative_config(tol, max_it):
+def iterative_config(tol, max_it, stype=cf.ITER_BICGSTAB):
     c = dry_config()
     c.solver = cf.SOLVER_ITERATIVE
-    c.solver_type = cf.ITER_BICGSTAB
+    c.solver_type = stype
     c.tolerance = tol
     c.max_iterations = max_it
     return c
 
 
+ITER_TYPES = pytest.mark.parametrize("stype", [cf.ITER_BICGSTAB, cf.ITER_CG], ids=["bicgstab", "cg"])
+
+
+@ITER_TYPES
 @pytest.mark.parametrize("nranks", [2, 4])
-def test_bicgstab_on_slabs_fixed_iterations(gpu_lib, nranks):
-    """BiCGStab over the slabs (halo rows of x, pp, cs; every inner product summed over the slabs)
-    with the tolerance out of reach: the same 8 iterations per step as the single domain, whose
-    iterates differ only by the order of the dot-product sums (1e-10 after 3 steps)."""
-    c = iterative_config(1e-30, 8)
+def test_iterative_solve_on_slabs_fixed_iterations(gpu_lib, nranks, stype):
+    """BiCGStab (halo rows of x, pp, cs) and conjugate gradients (x, then z and the old direction)
+    over the slabs, every inner product summed over the slabs, with the tolerance out of reach:
+    the same 8 iterations per step as the single domain, whose iterates differ only by the order
+    of the dot-product sums (1e-10 after 3 steps)."""
+    c = iterative_config(1e-30, 8, stype)
     st = dry_state()
     m = api.Model(c)
     m.set_state(st)
@@ -293,10 +298,11 @@ def test_bicgstab_on_slabs_fixed_iterations(gpu_lib, nranks):
     d.close()
 
 
-def test_bicgstab_on_slabs_to_tolerance(gpu_lib):
+@ITER_TYPES
+def test_iterative_solve_on_slabs_to_tolerance(gpu_lib, stype):
     """Solved to a tolerance: every slab stops at the same iteration, within one of the single
     domain's, with the residual met."""
-    c = iterative_config(1e-10, 500)
+    c = iterative_config(1e-10, 500, stype)
     st = dry_state()
     m = api.Model(c)
     m.set_state(st)
