@@ -91,7 +91,9 @@ class ClockSampler:
         except Exception:
             self.gpu = str(device)
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+        # the raw samples; BENCH_OUT_DIR names a folder to keep them in
+        out_dir = os.environ.get("BENCH_OUT_DIR") or os.path.join(ROOT, "_bench_out")
+        self.path = os.path.join(out_dir, f"clocks_rank{rank}.csv")
 
     def start(self, wait_s: float = 10.0):
         """Start sampling every 100 ms and return once the first sample has been written."""

@@ -267,7 +267,7 @@ void* mgpu_stream(mgpu_handle* h);
 int64_t mgpu_launch_count(mgpu_handle* h);
 
 /* Horizontal-mean profiles computed on the device in FP64: mean theta (th + thref) and the
- * mean of w squared per level (the domain-mean theta and w'^2 profiles used to judge runs);
+ * mean of w squared per level (the domain-mean theta and w'^2 profiles used to compare runs);
  * either pointer may be NULL.  Reads back 8*nz bytes per non-NULL pointer. */
 int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2);
 
