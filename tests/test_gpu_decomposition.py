@@ -452,19 +452,42 @@ NCCL_ONE_RANK = textwrap.dedent("""
     torch.cuda.set_device(0)
     dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
                             device_id=torch.device("cuda", 0))
+    mode = sys.argv[2]
     c = cf.dry_cbl_config(64, 64, 24, 50.0, 25.0, 0.5, ug=5.0, fcoriol=1e-4, precision=int(sys.argv[1]))
     c.reproducible = 1
+    tol = 0.0 if c.precision == cf.FP64 else 1e-5
+    if mode == "forced":
+        # damping and subsidence (mean-profile all-reduce), profile diagnostics (sum), cfltest
+        # with the Galilean frame (max all-reduce)
+        cf.enable_damping(c, 0.02, 300.0, 150.0)
+        cf.enable_subsidence(c, [0.0, 700.0], [0.0, -0.004], theta=True)
+        c.profile_diagnostics_enabled = 1
+        cf.enable_cfl(c, frequency=2, dtmmax=1.0)
+        cf.enable_galilean(c)
+        tol = max(tol, 1e-11)
+    elif mode == "iterative":
+        # conjugate gradients: halo sets of the solver vectors and the sum all-reduce
+        c.solver, c.solver_type, c.tolerance, c.max_iterations = cf.SOLVER_ITERATIVE, cf.ITER_CG, 1e-30, 6
+        tol = 1e-10
     st = ini.random_flow_state(64, 64, 24, seed=4, amp_uv=1.0, amp_w=0.3, amp_th=0.5, ug=5.0)
     m = api.Model(c)
     m.set_state(st)
-    m.step(3)
+    m.step(5)
     d = dc.SlabDomain(c, dc.TorchComm(), halo=4)
     d.set_state(st)
-    d.step(3)
+    d.step(5)
     for f in ("u", "v", "w", "th", "zu", "zv", "zw", "zth"):
         a, b = d.download(f), m.download(f)
         err = np.abs(a - b).max() / np.abs(b).max()
-        assert err <= (0.0 if c.precision == cf.FP64 else 1e-5), (f, err)
+        assert err <= tol, (f, err)
+    if mode == "forced":
+        rd, rm = d.slabs[0].m.reductions(), m.reductions()
+        assert abs(rd.dtm - rm.dtm) <= 1e-12 * rm.dtm and abs(rd.ugal - rm.ugal) <= 1e-12 * abs(rm.ugal)
+        assert rm.ugal != 0.0 and rd.cfl_evaluations == rm.cfl_evaluations
+        pd, ref = d.profile_diagnostics(), m.profile_diagnostics()
+        for n in ref:
+            scale = max(np.abs(ref[n]).max(), 64 * 64 * np.abs(m.download("w")).max())
+            assert np.abs(pd[n] - ref[n]).max() <= 1e-11 * scale, n
     d.close()
     m.close()
     dist.destroy_process_group()
@@ -472,14 +495,17 @@ NCCL_ONE_RANK = textwrap.dedent("""
 """)
 
 
-@pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32_mixed"])
-def test_torch_comm_over_nccl_single_rank(gpu_lib, precision):
+@pytest.mark.parametrize("precision,mode", [(cf.FP64, "plain"), (cf.FP32_MIXED, "plain"), (cf.FP64, "forced"),
+                                            (cf.FP64, "iterative")],
+                         ids=["fp64", "fp32_mixed", "forced", "iterative"])
+def test_torch_comm_over_nccl_single_rank(gpu_lib, precision, mode):
     """The torch.distributed communicator on NCCL with one rank (the model's stream as the
-    collectives' stream, all-to-all and halo exchange as local copies, the FP32 level-mean
-    all-reduce through NCCL) reproduces the single-domain model; run in a child process so the
-    process group does not outlive the test."""
-    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(29600 + precision))
+    collectives' stream, all-to-all and halo exchange as local copies, the FP32 level-mean,
+    mean-profile, extrema and inner-product all-reduces through NCCL) reproduces the
+    single-domain model; run in a child process so the process group does not outlive the test."""
+    port = 29600 + 10 * precision + ["plain", "forced", "iterative"].index(mode)
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    r = subprocess.run([sys.executable, "-c", NCCL_ONE_RANK, str(precision)], cwd=root, env=env,
+    r = subprocess.run([sys.executable, "-c", NCCL_ONE_RANK, str(precision), mode], cwd=root, env=env,
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "SLAB-NCCL-OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
