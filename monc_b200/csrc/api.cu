@@ -1184,8 +1184,9 @@ int mgpu_profile_diagnostics(mgpu_handle* h, double* out, int32_t* nrows) {
 int mgpu_diagnostics(mgpu_handle* h, double* mean_theta, double* mean_w2) {
   if (!h) return MGPU_ERR_ARGUMENT;
   const int nz = h->cfg.nz;
-  if (h->fp32) launch_diagnostics<float>(h->sc, h->d32.th, h->d32.w, h->diag_d, h->diag_d + nz, h->stream);
-  else launch_diagnostics<double>(h->sc, h->d64.th, h->d64.w, h->diag_d, h->diag_d + nz, h->stream);
+  // a y-slab's means are over its interior rows
+  if (h->fp32) launch_diagnostics<float>(h->sc, h->d32.th, h->d32.w, h->diag_d, h->diag_d + nz, h->stream, h->slab_halo);
+  else launch_diagnostics<double>(h->sc, h->d64.th, h->d64.w, h->diag_d, h->diag_d + nz, h->stream, h->slab_halo);
   h->launches += 1;
   if (mean_theta) CK(cudaMemcpyAsync(mean_theta, h->diag_d, nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (mean_w2) CK(cudaMemcpyAsync(mean_w2, h->diag_d + nz, nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -83,7 +83,8 @@ void launch_halo_rows(const Scalars& s, T* const* f, int n, int depth, int r_lo,
                       cudaStream_t st);
 
 template <typename T>
-void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st);
+void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st,
+                        int halo = 0);
 
 // cfltest's reductions of the current zu, zv, zw (and vis, diff when with_vis) into out[0..5]:
 // min zu, max zu, min zv, max zv (levels 2..nz), max |zw| rdzn(k+1), max max(vis, diff) (rdzn(k+1)^2

@@ -789,12 +789,14 @@ template void slab_solve_columns<float>(const FftPlanDev&, const Scalars&, void*
 // ---- horizontal-mean diagnostics: one block per level, FP64 accumulation in a fixed order ----
 template <typename T>
 __global__ void k_diagnostics(const T* __restrict__ th, const T* __restrict__ w, const double* __restrict__ prof,
-                              int prof_stride, long long plane, double* out_th, double* out_w2) {
+                              int prof_stride, long long plane, long long first, long long count, double* out_th,
+                              double* out_w2) {
+  // the `count` points from `first` of each level: the whole plane, or a y-slab's interior rows
   const int k = blockIdx.x + 1;
-  const T* thk = th + (long long)(k - 1) * plane;
-  const T* wk = w + (long long)(k - 1) * plane;
+  const T* thk = th + (long long)(k - 1) * plane + first;
+  const T* wk = w + (long long)(k - 1) * plane + first;
   double a = 0.0, b = 0.0;
-  for (long long t = threadIdx.x; t < plane; t += blockDim.x) {
+  for (long long t = threadIdx.x; t < count; t += blockDim.x) {
     a += (double)thk[t];
     double wv = (double)wk[t];
     b += wv * wv;
@@ -811,16 +813,19 @@ __global__ void k_diagnostics(const T* __restrict__ th, const T* __restrict__ w,
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    if (out_th) out_th[k - 1] = sa[0] / (double)plane + prof[P_THREF * prof_stride + k];
-    if (out_w2) out_w2[k - 1] = sb[0] / (double)plane;
+    if (out_th) out_th[k - 1] = sa[0] / (double)count + prof[P_THREF * prof_stride + k];
+    if (out_w2) out_w2[k - 1] = sb[0] / (double)count;
   }
 }
 
 template <typename T>
-void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st) {
-  k_diagnostics<T><<<s.nz, 256, 0, st>>>(th, w, s.prof, s.nz + 2, s.plane, out_th, out_w2);
+void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st,
+                        int halo) {
+  const long long first = (long long)halo * s.nx, count = (long long)(s.ny - 2 * halo) * s.nx;
+  k_diagnostics<T><<<s.nz, 256, 0, st>>>(th, w, s.prof, s.nz + 2, s.plane, first, count, out_th, out_w2);
 }
-template void launch_diagnostics<double>(const Scalars&, const double*, const double*, double*, double*, cudaStream_t);
+template void launch_diagnostics<double>(const Scalars&, const double*, const double*, double*, double*, cudaStream_t,
+                                         int);
 
 // ---- horizontal means of th and the q fields per level (FP64 sums in a fixed order) ----------
 template <typename T>
@@ -854,7 +859,8 @@ void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, doub
 }
 template void launch_level_means<double>(const Scalars&, const double*, double* const*, int, double*, cudaStream_t, int);
 template void launch_level_means<float>(const Scalars&, const float*, float* const*, int, double*, cudaStream_t, int);
-template void launch_diagnostics<float>(const Scalars&, const float*, const float*, double*, double*, cudaStream_t);
+template void launch_diagnostics<float>(const Scalars&, const float*, const float*, double*, double*, cudaStream_t,
+                                        int);
 
 }  // namespace mgpu
 

@@ -432,6 +432,18 @@ class SlabDomain:
         for s in self.slabs:
             s.m.slab_iter(cf.SLAB_ITER_END)
 
+    def diagnostics(self):
+        """Domain-mean theta and w'^2 per level (mgpu_diagnostics): each slab's means over its
+        interior rows, averaged over the slabs."""
+        nz = self.geo.nz
+        local = torch.zeros(2 * nz, dtype=torch.float64)
+        for s in self.slabs:
+            th, w2 = s.m.diagnostics()
+            local[:nz] += torch.from_numpy(th)
+            local[nz:] += torch.from_numpy(w2)
+        total = self.comm.allreduce_sum(local) / self.comm.size
+        return total[:nz].numpy(), total[nz:].numpy()
+
     def profile_diagnostics(self) -> dict:
         """profile_diagnostics sums over the whole domain: each slab's totals over its interior rows
         (MONC's <name>_total_local of one rank), summed over the slabs.  The sums read the row

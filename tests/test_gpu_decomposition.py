@@ -70,6 +70,25 @@ def test_dry_fp64_slabs_bit_identical(gpu_lib, nranks, nsteps):
         np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
 
 
+@pytest.mark.parametrize("nranks", [2, 4])
+def test_slab_mean_diagnostics(gpu_lib, nranks):
+    """mgpu_diagnostics on a slab averages its interior rows only; the slabs' means averaged over
+    the slabs are the domain's mean theta and w'^2 profiles (to the order of the sums)."""
+    cfg, st = dry_config(), dry_state()
+    m = api.Model(cfg)
+    m.set_state(st)
+    m.step(3)
+    th_ref, w2_ref = m.diagnostics()
+    m.close()
+    d = dc.SlabDomain(cfg, dc.LoopbackComm(nranks))
+    d.set_state(st)
+    d.step(3)
+    th, w2 = d.diagnostics()
+    d.close()
+    np.testing.assert_allclose(th, th_ref, rtol=1e-14)
+    np.testing.assert_allclose(w2, w2_ref, rtol=1e-12, atol=1e-14 * np.abs(w2_ref).max())
+
+
 def test_dry_fp64_slabs_match_oracle(gpu_lib):
     cfg, st = dry_config(), dry_state(seed=7)
     o = po.Oracle(cfg)
