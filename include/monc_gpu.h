@@ -289,6 +289,13 @@ typedef struct mgpu_checkpoint_meta {
 int mgpu_checkpoint_write(mgpu_handle* h, const char* path);
 int mgpu_checkpoint_read(mgpu_handle* h, const char* path);
 
+/* The step state a checkpoint carries, without a file: for a decomposed run, whose driver
+ * gathers the slabs' fields into one global file with mgpu_checkpoint_write_host (MONC's ranks
+ * write their parts of one file, writecheckpoint.F90) and restores every slab after reading it.
+ * mean (may be NULL): (3 + number_q_fields) rows of nz, olzubar, olzvbar, olzthbar, olzqbar(n). */
+int mgpu_checkpoint_state(mgpu_handle* h, mgpu_checkpoint_meta* meta);
+int mgpu_restore_state(mgpu_handle* h, const mgpu_checkpoint_meta* meta, const double* mean);
+
 /* The same without a GPU, on host arrays: fields[0..8] = u v w th zu zv zw zth p, then q(n) and
  * zq(n) for n < number_q_fields, each [nz][ny][nx] x fastest; mean = (3 + number_q_fields) rows of
  * nz (olzubar, olzvbar, olzthbar, olzqbar(n)) or null.  read sets *has_mean when the file holds

@@ -201,6 +201,10 @@ def lib():
     L.mgpu_slab_level_means.restype = C.c_int
     L.mgpu_slab_iter.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]
     L.mgpu_slab_iter.restype = C.c_int
+    L.mgpu_checkpoint_state.argtypes = [C.c_void_p, C.c_void_p]
+    L.mgpu_checkpoint_state.restype = C.c_int
+    L.mgpu_restore_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mgpu_restore_state.restype = C.c_int
     L.mgpu_set_galilean_velocity.argtypes = [C.c_void_p, C.c_double, C.c_double]
     L.mgpu_set_galilean_velocity.restype = C.c_int
     L.mgpu_slab_mean_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
@@ -366,6 +370,18 @@ class Model:
     def checkpoint_write(self, path: str):
         """Write a MONC-layout checkpoint (NetCDF classic) of the model's state."""
         self._check(lib().mgpu_checkpoint_write(self.h, os.fsencode(path)), "checkpoint_write")
+
+    def checkpoint_state(self) -> "CheckpointMeta":
+        """The step count, time, dtm state and Galilean frame a checkpoint of the model carries."""
+        meta = CheckpointMeta()
+        self._check(lib().mgpu_checkpoint_state(self.h, C.byref(meta)), "checkpoint_state")
+        return meta
+
+    def restore_state(self, meta: "CheckpointMeta", mean: np.ndarray | None = None):
+        """Continue after the step `meta` describes; mean: (3 + number_q_fields, nz) olz*bar rows."""
+        m = None if mean is None else np.ascontiguousarray(mean, dtype=np.float64)
+        self._check(lib().mgpu_restore_state(self.h, C.byref(meta), None if m is None else m.ctypes.data),
+                    "restore_state")
 
     def checkpoint_read(self, path: str):
         """Restart from a MONC-layout checkpoint: state, mean profiles, step count, time, dtm."""

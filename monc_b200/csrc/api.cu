@@ -1085,14 +1085,7 @@ int mgpu_checkpoint_write(mgpu_handle* h, const char* path) {
     if (int rc = mgpu_mean_profiles(h, mean.data())) return rc;
   }
   mgpu_checkpoint_meta meta{};
-  meta.timestep = h->timestep - 1;
-  meta.last_cfl_timestep = h->cfl.last_cfl_timestep;
-  meta.time = h->time;
-  meta.dtm = h->sc.dtm;
-  meta.dtm_new = h->cfl.update_dtm ? h->cfl.dtm_new : h->sc.dtm;
-  meta.absolute_new_dtm = h->cfl.absolute_new_dtm;
-  meta.ugal = h->sc.ugal;
-  meta.vgal = h->sc.vgal;
+  mgpu_checkpoint_state(h, &meta);
   std::string err;
   int rc = checkpoint_write_host(h->cfg, h->rs, path, ptr.data(), with_mean ? mean.data() : nullptr, meta, err);
   if (rc) return fail(h, rc, "checkpoint write: " + err);
@@ -1117,7 +1110,26 @@ int mgpu_checkpoint_read(mgpu_handle* h, const char* path) {
                  : upload<double>(h, h->d64, ids[q], buf[q].data(), MGPU_LAYOUT_XFAST);
     if (rc) return rc;
   }
-  if (has_mean) {
+  return mgpu_restore_state(h, &meta, has_mean ? mean.data() : nullptr);
+}
+
+int mgpu_checkpoint_state(mgpu_handle* h, mgpu_checkpoint_meta* meta) {
+  if (!h || !meta) return MGPU_ERR_ARGUMENT;
+  *meta = mgpu_checkpoint_meta{};
+  meta->timestep = h->timestep - 1;  // the last completed step
+  meta->last_cfl_timestep = h->cfl.last_cfl_timestep;
+  meta->time = h->time;
+  meta->dtm = h->sc.dtm;
+  meta->dtm_new = h->cfl.update_dtm ? h->cfl.dtm_new : h->sc.dtm;
+  meta->absolute_new_dtm = h->cfl.absolute_new_dtm;
+  meta->ugal = h->sc.ugal;
+  meta->vgal = h->sc.vgal;
+  return MGPU_OK;
+}
+
+int mgpu_restore_state(mgpu_handle* h, const mgpu_checkpoint_meta* meta, const double* mean) {
+  if (!h || !meta) return MGPU_ERR_ARGUMENT;
+  if (mean && h->olz_d) {
     const int nz = h->cfg.nz;
     std::vector<double> rows((size_t)(3 + MGPU_MAX_Q) * (nz + 2), 0.0);
     for (int r = 0; r < 3 + h->cfg.number_q_fields; ++r)
@@ -1126,16 +1138,16 @@ int mgpu_checkpoint_read(mgpu_handle* h, const char* path) {
     CK(cudaStreamSynchronize(h->stream));
   }
   // readcheckpoint.F90 load_misc: the run continues at the step after the checkpointed one
-  h->timestep = meta.timestep + 1;
-  h->time = meta.time;
-  h->sc.dtm = meta.dtm;
-  h->sc.ugal = h->sc.ugal_p = meta.ugal;  // readcheckpoint.F90:184
-  h->sc.vgal = h->sc.vgal_p = meta.vgal;
-  h->cfl.dtm_last = meta.dtm;
-  h->cfl.dtm_new = meta.dtm_new;
-  h->cfl.update_dtm = h->cfg.cfl_enabled && meta.dtm_new != meta.dtm;
-  h->cfl.absolute_new_dtm = meta.absolute_new_dtm;
-  h->cfl.last_cfl_timestep = meta.last_cfl_timestep;
+  h->timestep = meta->timestep + 1;
+  h->time = meta->time;
+  h->sc.dtm = meta->dtm;
+  h->sc.ugal = h->sc.ugal_p = meta->ugal;  // readcheckpoint.F90:184
+  h->sc.vgal = h->sc.vgal_p = meta->vgal;
+  h->cfl.dtm_last = meta->dtm;
+  h->cfl.dtm_new = meta->dtm_new;
+  h->cfl.update_dtm = h->cfg.cfl_enabled && meta->dtm_new != meta->dtm;
+  h->cfl.absolute_new_dtm = meta->absolute_new_dtm;
+  h->cfl.last_cfl_timestep = meta->last_cfl_timestep;
   return MGPU_OK;
 }
 

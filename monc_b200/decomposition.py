@@ -140,6 +140,9 @@ class LoopbackComm:
             b.copy_(total)
         self._sync(bufs[0])
 
+    def barrier(self):
+        pass
+
     def allreduce_sum_inplace(self, bufs):
         self._sync(bufs[0])
         total = bufs[0].clone()
@@ -220,6 +223,9 @@ class TorchComm:
         with self._ctx():
             dist.all_reduce(bufs[0], group=self.group)
             bufs[0].div_(self.size)
+
+    def barrier(self):
+        dist.barrier(group=self.group)
 
     def allreduce_sum_inplace(self, bufs):
         with self._ctx():
@@ -431,6 +437,30 @@ class SlabDomain:
             done = self._reduce_step(cf.SLAB_ITER_UPDATE)
         for s in self.slabs:
             s.m.slab_iter(cf.SLAB_ITER_END)
+
+    def checkpoint_write(self, path: str):
+        """One MONC-layout checkpoint of the whole domain: the slabs' interior rows gathered, the
+        mean profiles and step state of the first slab (the same on every slab), written by rank 0
+        through the host codec."""
+        names = api._checkpoint_names(self.cfg)
+        fields = {n: self.download(n) for n in names}
+        m = self.slabs[0].m
+        mean = None
+        if self.mean_profiles:
+            mp = m.mean_profiles()
+            nq = self.cfg.number_q_fields
+            mean = np.stack([mp["olzubar"], mp["olzvbar"], mp["olzthbar"]] + [mp[f"olzqbar{n}"] for n in range(nq)])
+        meta = m.checkpoint_state()
+        if 0 in self.comm.local_ranks:
+            api.checkpoint_write_host(self.cfg, path, fields, meta, mean)
+        self.comm.barrier()
+
+    def checkpoint_read(self, path: str):
+        """Restart every slab from a whole-domain checkpoint (its fields scattered by rows)."""
+        fields, mean, meta = api.checkpoint_read_host(self.cfg, path)
+        self.set_state(fields)
+        for s in self.slabs:
+            s.m.restore_state(meta, mean)
 
     def diagnostics(self):
         """Domain-mean theta and w'^2 per level (mgpu_diagnostics): each slab's means over its

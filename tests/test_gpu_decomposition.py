@@ -12,6 +12,7 @@ after all queued work has finished; no kernel waits on another slab).
   and the fields of the adaptive-dtm run bit for bit.
 * iterativesolver on the slabs, BiCGStab and conjugate gradients: the inner products summed over
   the slabs, the iterates match the single domain's to rounding.
+* Checkpoints of a decomposed run: one whole-domain file, restarts bit for bit.
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
 import os
@@ -337,6 +338,43 @@ def test_iterative_solve_on_slabs_to_tolerance(gpu_lib, stype):
     for f in STATE:
         assert np.abs(d.download(f) - ref[f]).max() <= 1e-8 * np.abs(ref[f]).max(), f
     d.close()
+
+
+@pytest.mark.parametrize("nranks", [2, 4])
+def test_slab_checkpoint_restart(gpu_lib, tmp_path, nranks):
+    """A decomposed run checkpointed into one whole-domain file (damping, cfltest and the Galilean
+    frame on, so the mean profiles and step state travel too) and continued by a new decomposed
+    domain that reads it ends bit for bit where the uninterrupted run does; the single-domain
+    model reads the same file and agrees with both to rounding."""
+    c, st = forced_setup()
+    cf.enable_cfl(c, frequency=2, dtmmax=1.0)
+    cf.enable_galilean(c)
+    path = str(tmp_path / "slabs.nc")
+    a = dc.SlabDomain(c, dc.LoopbackComm(nranks))
+    a.set_state(st)
+    a.step(7)
+    ref = {f: a.download(f) for f in STATE}
+    ref_state = a.slabs[0].m.reductions()
+    a.close()
+    b = dc.SlabDomain(c, dc.LoopbackComm(nranks))
+    b.set_state(st)
+    b.step(4)
+    b.checkpoint_write(path)
+    b.close()
+    d = dc.SlabDomain(c, dc.LoopbackComm(nranks))
+    d.checkpoint_read(path)
+    d.step(3)
+    for f in STATE:
+        np.testing.assert_array_equal(d.download(f), ref[f], err_msg=f)
+    r = d.slabs[0].m.reductions()
+    assert (r.timestep, r.dtm, r.ugal) == (ref_state.timestep, ref_state.dtm, ref_state.ugal)
+    d.close()
+    m = api.Model(c)
+    m.checkpoint_read(path)
+    m.step(3)
+    for f in STATE:
+        assert np.abs(m.download(f) - ref[f]).max() <= 1e-10 * np.abs(ref[f]).max(), f
+    m.close()
 
 
 def test_halo_rows_pack_and_unpack(gpu_lib):
