@@ -446,6 +446,7 @@ int mgpu_step_phase(mgpu_handle* h, int32_t phase);
 #define MGPU_HALO_ITER_PP   3   /* the search direction pp (before MGPU_SLAB_ITER_APPLY) */
 #define MGPU_HALO_ITER_CS   4   /* the preconditioned half step cs (before MGPU_SLAB_ITER_APPLY2) */
 #define MGPU_HALO_ITER_CG   5   /* conjugate gradients: z and the old direction p (before APPLY) */
+#define MGPU_HALO_ITER_X64  6   /* FP32-mixed: the refinement's FP64 iterate (double buffers) */
 int mgpu_halo_fields(mgpu_handle* h, int32_t set);
 int mgpu_halo_pack(mgpu_handle* h, int32_t set, int32_t depth, void* d_lo, void* d_hi);
 int mgpu_halo_unpack(mgpu_handle* h, int32_t set, int32_t depth, const void* d_lo, const void* d_hi);
@@ -507,6 +508,12 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
 #define MGPU_SLAB_ITER_FINISH     7
 #define MGPU_SLAB_ITER_END        8
 #define MGPU_SLAB_ITER_PRECOND    9
+#define MGPU_SLAB_ITER_COMPAT    10
+#define MGPU_SLAB_ITER_SHIFT     11
+#define MGPU_SLAB_ITER_REFINE    12
+#define MGPU_SLAB_ITER_INNER     13
+#define MGPU_SLAB_ITER_CORRECT   14
+#define MGPU_SLAB_ITER_UNCORRECT 15
 /* solver_type MGPU_ITER_CG (MONC's default; the symmetric form of the operator):
  *
  *   BEGIN; halo exchange of MGPU_HALO_ITER_X; INIT, sum, FINISH     r = b A_vol - A x
@@ -515,7 +522,23 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
  *     halo exchange of MGPU_HALO_ITER_CG (depth 1)
  *     APPLY, sum, FINISH                      p' = z + bet p; A p'; <p', A p'>
  *     UPDATE, sum, FINISH                     x, r; |r|^2; convergence
- *   END */
+ *   END
+ *
+ * FP32-mixed models (iterative refinement: the FP64 residual, an FP32 correction solve, the FP64
+ * iterate corrected; the single-domain solve's loop):
+ *
+ *   BEGIN                                     b (FP64) = p
+ *   COMPAT, sum, FINISH; SHIFT                b minus its incompatible horizontal-mean part
+ *   up to 8 times:
+ *     halo exchange of MGPU_HALO_ITER_X64 (depth 1, double buffers)
+ *     REFINE, sum, FINISH                     r = b - A x in FP64; stop when FINISH reports done
+ *     if the residual did not fall below the last one: UNCORRECT (x -= e) and stop
+ *     INNER                                   e = 0; then the BiCGStab or conjugate-gradient
+ *                                             steps above on the FP32 vectors, to 1e-5
+ *     CORRECT                                 x += e
+ *   END                                       p = x
+ *
+ * FINISH reports the solver's relative residual through mgpu_get_reductions as it goes. */
 int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done);
 
 /* x-FFT (fftsolver.F90:50-309 transforms, x pass) between the interior rows of p and d_spec,

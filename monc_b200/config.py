@@ -22,9 +22,10 @@ SOLVER_ITERATIVE = 1
 SOLVER_EXTERNAL = 2  # one y-slab of a decomposed domain; the slab driver runs the pressure solve
 PHASE_SUBGRID, PHASE_DYNAMICS, PHASE_PSTEP = 0, 1, 2
 HALO_STATE, HALO_PRESSURE = 0, 1
-HALO_ITER_X, HALO_ITER_PP, HALO_ITER_CS, HALO_ITER_CG = 2, 3, 4, 5
+HALO_ITER_X, HALO_ITER_PP, HALO_ITER_CS, HALO_ITER_CG, HALO_ITER_X64 = 2, 3, 4, 5, 6
 (SLAB_ITER_BEGIN, SLAB_ITER_INIT, SLAB_ITER_DIRECTION, SLAB_ITER_APPLY, SLAB_ITER_HALF_STEP, SLAB_ITER_APPLY2,
- SLAB_ITER_UPDATE, SLAB_ITER_FINISH, SLAB_ITER_END, SLAB_ITER_PRECOND) = range(10)
+ SLAB_ITER_UPDATE, SLAB_ITER_FINISH, SLAB_ITER_END, SLAB_ITER_PRECOND, SLAB_ITER_COMPAT, SLAB_ITER_SHIFT,
+ SLAB_ITER_REFINE, SLAB_ITER_INNER, SLAB_ITER_CORRECT, SLAB_ITER_UNCORRECT) = range(16)
 ITER_BICGSTAB = 0
 ITER_CG = 1
 SUBS_DIVERGENCE, SUBS_VELOCITY = 0, 1  # subsidence_input_type (forcing.F90:40-41)

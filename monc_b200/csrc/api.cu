@@ -1332,10 +1332,11 @@ static int halo_set(mgpu_handle* h, DevState<T>& d, int set, T** f) {
     f[n++] = d.p;
     return n;
   }
-  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CG && sizeof(T) == 8 && h->iter) {
-    double* v[2] = {nullptr, nullptr};
+  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CG && h->iter) {
+    // the solver vectors in the model's type (FP32-mixed: the FP32 correction solve's)
+    void* v[2] = {nullptr, nullptr};
     const int nv = iter_slab_vectors(h->iter, set, v);
-    for (int q = 0; q < nv; ++q) f[q] = reinterpret_cast<T*>(v[q]);
+    for (int q = 0; q < nv; ++q) f[q] = static_cast<T*>(v[q]);
     return nv;
   }
   return -1;
@@ -1397,8 +1398,9 @@ int mgpu_halo_fields(mgpu_handle* h, int32_t set) {
   if (!h) return MGPU_ERR_ARGUMENT;
   if (set == MGPU_HALO_STATE) return 8 + 2 * h->cfg.number_q_fields;
   if (set == MGPU_HALO_PRESSURE) return 1;
-  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_CG) {
-    if (!h->iter || h->fp32) return fail(h, MGPU_ERR_ARGUMENT, "the solver vectors exist after MGPU_SLAB_ITER_BEGIN");
+  if (set >= MGPU_HALO_ITER_X && set <= MGPU_HALO_ITER_X64) {
+    if (!h->iter) return fail(h, MGPU_ERR_ARGUMENT, "the solver vectors exist after MGPU_SLAB_ITER_BEGIN");
+    if (set == MGPU_HALO_ITER_X64 && !h->fp32) return fail(h, MGPU_ERR_ARGUMENT, "MGPU_HALO_ITER_X64 is FP32-mixed only");
     return set == MGPU_HALO_ITER_CG ? 2 : 1;
   }
   return fail(h, MGPU_ERR_ARGUMENT, "unknown halo set");
@@ -1408,6 +1410,18 @@ static int halo_entry(mgpu_handle* h, int32_t set, int32_t depth, void* lo, void
   if (!h || !lo || !hi) return MGPU_ERR_ARGUMENT;
   if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
   if (depth < 1 || depth > h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "halo depth out of range");
+  if (set == MGPU_HALO_ITER_X64) {
+    // an FP64 vector of an FP32-mixed model
+    void* v[2] = {nullptr, nullptr};
+    if (!h->iter || !h->fp32 || iter_slab_vectors(h->iter, set, v) != 1)
+      return fail(h, MGPU_ERR_ARGUMENT, "MGPU_HALO_ITER_X64 is the FP32-mixed refinement's iterate");
+    double* f[1] = {static_cast<double*>(v[0])};
+    const int H = h->slab_halo, ny = h->cfg.ny;
+    launch_halo_rows<double>(h->sc, f, 1, depth, unpack ? H - depth : H, unpack ? ny - H : ny - H - depth,
+                             static_cast<double*>(lo), static_cast<double*>(hi), unpack, h->stream);
+    h->launches += 1;
+    return check_launch(h);
+  }
   int rc = h->fp32 ? halo_rows<float>(h, h->d32, set, depth, lo, hi, unpack)
                    : halo_rows<double>(h, h->d64, set, depth, lo, hi, unpack);
   return rc ? rc : check_launch(h);
@@ -1462,31 +1476,34 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
 int mgpu_slab_iter(mgpu_handle* h, int32_t step, double* d_sums, int32_t* done) {
   if (!h) return MGPU_ERR_ARGUMENT;
   if (!h->slab_halo) return fail(h, MGPU_ERR_ARGUMENT, "mgpu_slab_init first");
-  if (h->fp32) return fail(h, MGPU_ERR_UNSUPPORTED, "the slab iterative solve runs in FP64 models");
-  const size_t bytes = field_elems(h) * sizeof(double);
+  const size_t n = field_elems(h);
+  void* p = h->fp32 ? static_cast<void*>(h->d32.p) : static_cast<void*>(h->d64.p);
   if (step == MGPU_SLAB_ITER_BEGIN) {
     if (!h->iter) {
       int st = MGPU_OK;
-      h->iter = iter_create(h->sc, h->rs, h->cfg, false, &st, h->slab_halo, h->cfg.ny - h->slab_halo);
+      h->iter = iter_create(h->sc, h->rs, h->cfg, h->fp32, &st, h->slab_halo, h->cfg.ny - h->slab_halo,
+                            h->slab_ny_global);
       if (st) return fail(h, st, "iterative solver setup");
     }
-    if (int rc = iter_slab_begin(h->iter, h->d64.p, bytes, h->stream)) return fail(h, rc, "slab iterative begin");
+    if (int rc = iter_slab_begin(h->iter, p, n, h->stream)) return fail(h, rc, "slab iterative begin");
     return MGPU_OK;
   }
   if (!h->iter) return fail(h, MGPU_ERR_ARGUMENT, "MGPU_SLAB_ITER_BEGIN first");
   if (step == MGPU_SLAB_ITER_END) {
-    int rc = iter_slab_end(h->iter, h->d64.p, bytes, h->stream, &h->solver_iterations, &h->solver_residual);
+    int rc = iter_slab_end(h->iter, p, n, h->stream, &h->solver_iterations, &h->solver_residual);
     if (rc == MGPU_ERR_CUDA) return fail(h, rc, "slab iterative end");
     return MGPU_OK;  // not converged: MONC only warns (iterativesolver.F90:240-242); see mgpu_get_reductions
   }
   const bool reduces = step == MGPU_SLAB_ITER_INIT || step == MGPU_SLAB_ITER_APPLY || step == MGPU_SLAB_ITER_APPLY2 ||
                        step == MGPU_SLAB_ITER_UPDATE || step == MGPU_SLAB_ITER_FINISH ||
-                       step == MGPU_SLAB_ITER_PRECOND;
+                       step == MGPU_SLAB_ITER_PRECOND || step == MGPU_SLAB_ITER_COMPAT || step == MGPU_SLAB_ITER_REFINE;
   if (reduces && !d_sums) return fail(h, MGPU_ERR_ARGUMENT, "this step needs d_sums");
   if (step == MGPU_SLAB_ITER_FINISH) {
     int dn = 0;
-    int rc = iter_slab_finish(h->iter, d_sums, h->stream, &h->launches, &dn);
+    double err = 0.0;
+    int rc = iter_slab_finish(h->iter, d_sums, h->stream, &h->launches, &dn, &err);
     if (rc) return fail(h, rc, "slab iterative finish (no reduction pending?)");
+    h->solver_residual = err;
     if (done) *done = dn;
     return MGPU_OK;
   }

@@ -117,14 +117,17 @@ int launch_profile_diagnostics(const Scalars& s, const T* u, const T* v, const T
 // BiCGStab pressure solve (iterativesolver)
 struct IterSolverDev;
 IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status,
-                           int j0 = 0, int j1 = -1);
-// BiCGStab and conjugate gradients over y-slabs (FP64), one step at a time (iter.cu)
-int iter_slab_begin(IterSolverDev* it, const double* p, size_t bytes, cudaStream_t st);
+                           int j0 = 0, int j1 = -1, int ny_total = -1);
+// BiCGStab and conjugate gradients over y-slabs, with the FP32-mixed refinement around them, one
+// step at a time (iter.cu); p holds n elements of the model's type
+int iter_slab_begin(IterSolverDev* it, const void* p, size_t n, cudaStream_t st);
 int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st, int64_t* launches);
-int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done);
-int iter_slab_end(IterSolverDev* it, double* p, size_t bytes, cudaStream_t st, int* iterations, double* residual);
-// the halo set's solver vectors into f (at most 2); returns their number, or -1
-int iter_slab_vectors(IterSolverDev* it, int set, double** f);
+int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done,
+                     double* err);
+int iter_slab_end(IterSolverDev* it, void* p, size_t n, cudaStream_t st, int* iterations, double* residual);
+// the halo set's solver vectors into f (at most 2; float for the FP32 inner solve, double for
+// MGPU_HALO_ITER_X64 and FP64 models); returns their number, or -1
+int iter_slab_vectors(IterSolverDev* it, int set, void** f);
 void iter_destroy(IterSolverDev* it);
 template <typename T>
 int iter_solve(IterSolverDev* it, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, int* iterations,

@@ -52,6 +52,7 @@ struct Geom {
   double A_n, A_e;
   const double* coef;  // [NCOEF][nz+2]
   int j0, j1;          // rows solved: all (0, ny), or a y-slab's interior rows between its halo rows
+  int ny_total;        // rows of the whole domain (the compatibility shift's point count)
   __device__ __forceinline__ double au(int k) const { return coef[k]; }
   __device__ __forceinline__ double ad(int k) const { return coef[(nz + 2) + k]; }
   __device__ __forceinline__ double ap(int k) const { return coef[2 * (nz + 2) + k]; }
@@ -181,6 +182,19 @@ __device__ void finish_cg_update(IterScalars* st, const double* s, int max_it) {
   st->it_done = st->it;
   st->done = (st->err < st->tol || st->it >= max_it) ? 1 : 0;
   st->it += 1;
+}
+// the refinement's compatibility shift: sum_k vol(k) sum_ij b over the volume of the domain
+__device__ void finish_compat(IterScalars* st, const double* s, const Geom& g) {
+  double w = 0.0;
+  for (int kk = 2; kk <= g.nz; ++kk) w += g.vol(kk);
+  st->shift = s[0] / (w * (double)g.nx * (double)g.ny_total);
+}
+// the refinement's FP64 residual: <r, r>, <b, b>
+__device__ void finish_refine(IterScalars* st, const double* s) {
+  st->sc_err = fmax(sqrt(s[1]), 0.0001);
+  st->rho = s[0];
+  st->err = sqrt(s[0]) / st->sc_err;
+  st->done = st->err < st->tol ? 1 : 0;
 }
 
 // (A x)(k, j, i) for 2 <= k <= nz (calc_Ax); x(o) gives the value at offset o.  The symmetric
@@ -344,13 +358,16 @@ __global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __re
 }
 
 // y-slabs: close reduction `which` with the sums over all slabs: BiCGStab 0 init, 1 apply_dot,
-// 2 apply_dots, 3 update; conjugate gradients 4 init, 5 precond, 6 apply, 7 update
+// 2 apply_dots, 3 update; conjugate gradients 4 init, 5 precond, 6 apply, 7 update; the FP32-mixed
+// refinement 8 compatibility sum, 9 FP64 residual
 __global__ void k_iter_finish(IterScalars* st, const double* __restrict__ sums, int which, double sc_floor,
-                              int max_it) {
+                              int max_it, Geom g) {
   if (threadIdx.x != 0) return;
   const double s[3] = {sums[0], sums[1], sums[2]};
   if (which == 0) { finish_init(st, s, sc_floor); return; }
   if (which == 4) { finish_cg_init(st, s, sc_floor); return; }
+  if (which == 8) { finish_compat(st, s, g); return; }
+  if (which == 9) { finish_refine(st, s); return; }
   if (st->done) return;
   switch (which) {
     case 1: finish_apply_dot(st, s); break;
@@ -477,12 +494,7 @@ __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* _
   }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
-  if (last_block_sums<2>(st, partials, nblocks, s)) {
-    st->sc_err = fmax(sqrt(s[1]), 0.0001);
-    st->rho = s[0];
-    st->err = sqrt(s[0]) / st->sc_err;
-    st->done = st->err < st->tol ? 1 : 0;
-  }
+  if (last_block_sums<2>(st, partials, nblocks, s)) finish_refine(st, s);
 }
 
 // The horizontal-mean problem is singular: sum_k rhon(k) dz(k) sum_ij (A x)(k, j, i) = 0 for any x.
@@ -495,11 +507,7 @@ __global__ void __launch_bounds__(NTH) k_compat_sum(Geom g, const double* __rest
   if (i < g.nx && j < g.j1) v[0] = g.vol(k) * b[g.at(k, j, i)];
   block_partials<1>(v, partials, nblocks, block_id());
   double s[1];
-  if (last_block_sums<1>(st, partials, nblocks, s)) {
-    double w = 0.0;
-    for (int kk = 2; kk <= g.nz; ++kk) w += g.vol(kk);
-    st->shift = s[0] / (w * (double)g.nx * (double)g.ny);
-  }
+  if (last_block_sums<1>(st, partials, nblocks, s)) finish_compat(st, s, g);
 }
 __global__ void k_compat_shift(Geom g, double* b, const IterScalars* st) {
   const double c = st->shift;
@@ -541,6 +549,11 @@ struct IterSolverDev {
   double* r64 = nullptr;  // refinement residual (FP32-mixed model)
   int pending = -1;       // y-slab steps: the reduction iter_slab_finish closes next
   int cg_n = 0;           // y-slab conjugate gradients: iterations done (which direction buffer is old)
+  bool inner32 = false;   // y-slab FP32-mixed: the FP32 correction solve is running
+  double sc_floor = 0.0001;
+  bool scale_rhs = true;
+  int inner_its = 0;      // y-slab FP32-mixed: FP32 iterations of this solve
+  double slab_err = 0.0, slab_prev_err = 0.0;  // y-slab FP32-mixed: the last two FP64 residuals
   std::vector<void*> allocs;
   dim3 grid_pt, grid_col, block;
 };
@@ -553,9 +566,10 @@ static int dev_alloc(IterSolverDev* it, void** p, size_t bytes) {
 }
 
 IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_config& cfg, bool fp32, int* status, int j0,
-                           int j1) {
+                           int j1, int ny_total) {
   *status = MGPU_OK;
   if (j1 < 0) j1 = s.ny;
+  if (ny_total < 0) ny_total = s.ny;
   if (cfg.solver_type != MGPU_ITER_BICGSTAB && cfg.solver_type != MGPU_ITER_CG) {
     std::fprintf(stderr, "iterative solver: unknown solver_type %d\n", cfg.solver_type);
     *status = MGPU_ERR_UNSUPPORTED;
@@ -602,7 +616,7 @@ IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_conf
   };
   if (dev_alloc(it, (void**)&it->coef, c.size() * sizeof(double))) return fail(MGPU_ERR_CUDA);
   cudaMemcpy(it->coef, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice);
-  it->g = Geom{s.nx, s.ny, nz, it->symm ? 1 : 0, s.plane, A_n, A_e, it->coef, j0, j1};
+  it->g = Geom{s.nx, s.ny, nz, it->symm ? 1 : 0, s.plane, A_n, A_e, it->coef, j0, j1, ny_total};
   it->block = dim3(BX, BY, 1);
   it->grid_col = dim3((s.nx + BX - 1) / BX, (j1 - j0 + BY - 1) / BY, 1);
   it->grid_pt = dim3(it->grid_col.x, it->grid_col.y, nz - 1);
@@ -787,98 +801,144 @@ static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream
   return rc;
 }
 
-// ---- BiCGStab over y-slabs, one step at a time -----------------------------------------------
-// The driver runs the iteration of run_bicgstab step by step, exchanging the halo rows of x, pp
-// and cs before the steps that apply A to them and summing each step's dot products over the
-// slabs before iter_slab_finish closes the reduction.
-int iter_slab_begin(IterSolverDev* it, const double* p, size_t bytes, cudaStream_t st) {
-  if (!it || it->fp32) return MGPU_ERR_UNSUPPORTED;
-  // psource = p; the initial guess is the previous solution (iterativesolver.F90:95-106)
-  if (cudaMemcpyAsync(it->w64.b, p, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
+// ---- the iterative solve over y-slabs, one step at a time --------------------------------------
+// The driver runs the iterations of run_bicgstab / run_cg (and, for FP32-mixed models, the
+// refinement of solve_mixed around them) step by step: it exchanges the halo rows of the vectors A
+// is applied to before the steps that apply it, and sums each reducing step's dot products over
+// the slabs before iter_slab_finish closes the reduction with the update the single-domain
+// kernel's last block makes.
+static void slab_scalars(IterSolverDev* it, double tol, cudaStream_t st) {
   IterScalars init{};
-  init.tol = it->tol;
+  init.tol = tol;
   init.ext = 1;
   it->st_host[0] = init;
-  if (cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return MGPU_ERR_CUDA;
+  cudaMemcpyAsync(it->st, it->st_host, sizeof(IterScalars), cudaMemcpyHostToDevice, st);
+}
+
+int iter_slab_begin(IterSolverDev* it, const void* p, size_t n, cudaStream_t st) {
+  if (!it) return MGPU_ERR_ARGUMENT;
+  if (it->fp32) {
+    // the refinement's FP64 right-hand side; x (FP64) keeps the last solution
+    k_convert_levels<float, double><<<592, 256, 0, st>>>(static_cast<const float*>(p), it->w64.b, (long long)n);
+  } else {
+    // psource = p; the initial guess is the previous solution (iterativesolver.F90:95-106)
+    if (cudaMemcpyAsync(it->w64.b, p, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return MGPU_ERR_CUDA;
+  }
+  slab_scalars(it, it->tol, st);
   it->pending = -1;
   it->cg_n = 0;
-  return MGPU_OK;
+  it->inner32 = false;
+  it->sc_floor = 0.0001;
+  it->scale_rhs = true;
+  return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
 }
 
 // the two search-direction buffers of conjugate gradients alternate: p_old = pbuf[n & 1]
-static double* cg_p(IterSolverDev* it, int n) { return (n & 1) ? it->w64.cs : it->w64.pp; }
+template <typename W>
+static W* cg_p(Work<W>& w, int n) { return (n & 1) ? w.cs : w.pp; }
 
-static int cg_slab_step(IterSolverDev* it, int step, int* nsum, cudaStream_t st) {
-  Work<double>& w = it->w64;
+template <typename W>
+static int solver_step(IterSolverDev* it, Work<W>& w, int step, int* nsum, cudaStream_t st) {
   const Geom& g = it->g;
-  const int ncol = (int)(it->grid_col.x * it->grid_col.y);
+  if (it->symm) {
+    const int ncol = (int)(it->grid_col.x * it->grid_col.y);
+    switch (step) {
+      case MGPU_SLAB_ITER_INIT:
+        // MONC's symmetric form: the FP64 solve scales the right-hand side by A_vol (run_cg)
+        k_cg_init<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, it->partials, it->nblocks, it->st,
+                                                         it->sc_floor, it->scale_rhs ? 1 : 0);
+        it->pending = 4; *nsum = 2; return MGPU_OK;
+      case MGPU_SLAB_ITER_PRECOND:
+        k_cg_precond<W><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.s, w.tmp, it->partials, ncol, it->st);
+        it->pending = 5; *nsum = 1; return MGPU_OK;
+      case MGPU_SLAB_ITER_APPLY:
+        k_cg_apply<W><<<it->grid_pt, it->block, 0, st>>>(g, w.s, cg_p(w, it->cg_n), cg_p(w, it->cg_n + 1), w.v,
+                                                          it->partials, it->nblocks, it->st);
+        it->pending = 6; *nsum = 1; return MGPU_OK;
+      case MGPU_SLAB_ITER_UPDATE:
+        k_cg_update<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, cg_p(w, it->cg_n + 1), w.v, w.r, it->partials,
+                                                           it->nblocks, it->st, it->max_it);
+        it->cg_n += 1;
+        it->pending = 7; *nsum = 1; return MGPU_OK;
+    }
+    return MGPU_ERR_ARGUMENT;
+  }
   switch (step) {
     case MGPU_SLAB_ITER_INIT:
-      // MONC's symmetric form: the right-hand side scaled by A_vol (run_cg with scale_rhs)
-      k_cg_init<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, it->partials, it->nblocks, it->st, 0.0001, 1);
-      it->pending = 4;
-      *nsum = 2;
-      return MGPU_OK;
-    case MGPU_SLAB_ITER_PRECOND:
-      k_cg_precond<double><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.s, w.tmp, it->partials, ncol, it->st);
-      it->pending = 5;
-      *nsum = 1;
+      k_bicg_init<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, w.cr, it->partials, it->nblocks, it->st,
+                                                        it->sc_floor);
+      it->pending = 0; *nsum = 2; return MGPU_OK;
+    case MGPU_SLAB_ITER_DIRECTION:
+      k_bicg_direction<W><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.pp, w.tmp, it->st);
       return MGPU_OK;
     case MGPU_SLAB_ITER_APPLY:
-      k_cg_apply<double><<<it->grid_pt, it->block, 0, st>>>(g, w.s, cg_p(it, it->cg_n), cg_p(it, it->cg_n + 1), w.v,
-                                                            it->partials, it->nblocks, it->st);
-      it->pending = 6;
-      *nsum = 1;
+      k_bicg_apply_dot<W><<<it->grid_pt, it->block, 0, st>>>(g, w.pp, w.cr, w.v, it->partials, it->nblocks, it->st);
+      it->pending = 1; *nsum = 1; return MGPU_OK;
+    case MGPU_SLAB_ITER_HALF_STEP:
+      k_bicg_half_step<W><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.s, w.cs, w.tmp, it->st);
       return MGPU_OK;
+    case MGPU_SLAB_ITER_APPLY2:
+      k_bicg_apply_dots<W><<<it->grid_pt, it->block, 0, st>>>(g, w.cs, w.s, w.t, it->partials, it->nblocks, it->st);
+      it->pending = 2; *nsum = 3; return MGPU_OK;
     case MGPU_SLAB_ITER_UPDATE:
-      k_cg_update<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, cg_p(it, it->cg_n + 1), w.v, w.r, it->partials,
-                                                             it->nblocks, it->st, it->max_it);
-      it->cg_n += 1;
-      it->pending = 7;
-      *nsum = 1;
-      return MGPU_OK;
+      k_bicg_update<W><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.pp, w.cs, w.s, w.t, w.r, w.cr, it->partials,
+                                                          it->nblocks, it->st, it->max_it);
+      it->pending = 3; *nsum = 1; return MGPU_OK;
   }
   return MGPU_ERR_ARGUMENT;
 }
 
 int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st, int64_t* launches) {
-  Work<double>& w = it->w64;
   const Geom& g = it->g;
+  const long long n = (long long)g.nz * g.plane;
   int nsum = 0;
-  if (it->symm) {
-    if (int rc = cg_slab_step(it, step, &nsum, st)) return rc;
-  } else switch (step) {
-    case MGPU_SLAB_ITER_INIT:
-      k_bicg_init<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.b, w.r, w.cr, it->partials, it->nblocks, it->st,
-                                                             0.0001);
-      it->pending = 0;
+  switch (step) {
+    // the FP32-mixed refinement (solve_mixed)
+    case MGPU_SLAB_ITER_COMPAT:
+      if (!it->fp32) return MGPU_ERR_ARGUMENT;
+      k_compat_sum<<<it->grid_pt, it->block, 0, st>>>(g, it->w64.b, it->partials, it->nblocks, it->st);
+      it->pending = 8;
+      nsum = 1;
+      break;
+    case MGPU_SLAB_ITER_SHIFT:
+      if (!it->fp32) return MGPU_ERR_ARGUMENT;
+      k_compat_shift<<<592, 256, 0, st>>>(g, it->w64.b, it->st);
+      break;
+    case MGPU_SLAB_ITER_REFINE:
+      if (!it->fp32) return MGPU_ERR_ARGUMENT;
+      slab_scalars(it, it->tol, st);
+      k_refine_residual<<<it->grid_pt, it->block, 0, st>>>(g, it->w64.x, it->w64.b, it->r64, it->w32.b, it->partials,
+                                                          it->nblocks, it->st);
+      it->inner32 = false;
+      it->pending = 9;
       nsum = 2;
       break;
-    case MGPU_SLAB_ITER_DIRECTION:
-      k_bicg_direction<double><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.pp, w.tmp, it->st);
+    case MGPU_SLAB_ITER_INNER:
+      // the FP32 correction solve A e = r, from e = 0, to a relative residual of 1e-5
+      if (!it->fp32) return MGPU_ERR_ARGUMENT;
+      if (cudaMemsetAsync(it->w32.x, 0, (size_t)n * sizeof(float), st) != cudaSuccess) return MGPU_ERR_CUDA;
+      slab_scalars(it, 1e-5, st);
+      it->inner32 = true;
+      it->sc_floor = 1e-300;
+      it->scale_rhs = false;
+      it->cg_n = 0;
       break;
-    case MGPU_SLAB_ITER_APPLY:
-      k_bicg_apply_dot<double><<<it->grid_pt, it->block, 0, st>>>(g, w.pp, w.cr, w.v, it->partials, it->nblocks, it->st);
-      it->pending = 1;
-      nsum = 1;
+    case MGPU_SLAB_ITER_CORRECT:
+    case MGPU_SLAB_ITER_UNCORRECT:
+      if (!it->fp32) return MGPU_ERR_ARGUMENT;
+      k_add_correction<<<592, 256, 0, st>>>(it->w64.x, it->w32.x, g.plane, n,
+                                            step == MGPU_SLAB_ITER_CORRECT ? 1.0 : -1.0);
+      // taking back a correction that did not reduce the residual: the previous one stands
+      if (step == MGPU_SLAB_ITER_UNCORRECT) it->slab_err = it->slab_prev_err;
+      it->inner32 = false;
       break;
-    case MGPU_SLAB_ITER_HALF_STEP:
-      k_bicg_half_step<double><<<it->grid_col, it->block, 0, st>>>(g, w.r, w.v, w.s, w.cs, w.tmp, it->st);
-      break;
-    case MGPU_SLAB_ITER_APPLY2:
-      k_bicg_apply_dots<double><<<it->grid_pt, it->block, 0, st>>>(g, w.cs, w.s, w.t, it->partials, it->nblocks, it->st);
-      it->pending = 2;
-      nsum = 3;
-      break;
-    case MGPU_SLAB_ITER_UPDATE:
-      k_bicg_update<double><<<it->grid_pt, it->block, 0, st>>>(g, w.x, w.pp, w.cs, w.s, w.t, w.r, w.cr, it->partials,
-                                                               it->nblocks, it->st, it->max_it);
-      it->pending = 3;
-      nsum = 1;
-      break;
-    default:
-      return MGPU_ERR_ARGUMENT;
+    default: {
+      if (it->fp32 && !it->inner32) return MGPU_ERR_ARGUMENT;
+      const int rc = it->fp32 ? solver_step<float>(it, it->w32, step, &nsum, st)
+                              : solver_step<double>(it, it->w64, step, &nsum, st);
+      if (rc) return rc;
+    }
   }
   *launches += 1;
   if (nsum) {
@@ -891,39 +951,64 @@ int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st,
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
 }
 
-int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done) {
-  if (it->pending < 0) return MGPU_ERR_ARGUMENT;
-  k_iter_finish<<<1, 32, 0, st>>>(it->st, d_sums, it->pending, 0.0001, it->max_it);
+int iter_slab_finish(IterSolverDev* it, const double* d_sums, cudaStream_t st, int64_t* launches, int* done,
+                     double* err) {
+  const int which = it->pending;
+  if (which < 0) return MGPU_ERR_ARGUMENT;
+  k_iter_finish<<<1, 32, 0, st>>>(it->st, d_sums, which, it->sc_floor, it->max_it, it->g);
   *launches += 1;
   it->pending = -1;
   if (cudaMemcpyAsync(it->st_host, it->st, sizeof(IterScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return MGPU_ERR_CUDA;
   *done = it->st_host->done;
+  *err = it->st_host->err;
+  if (it->inner32 && it->st_host->done) it->inner_its += it->st_host->it_done;
+  if (which == 9) {
+    it->slab_prev_err = it->slab_err;
+    it->slab_err = it->st_host->err;
+  }
   return MGPU_OK;
 }
 
-int iter_slab_end(IterSolverDev* it, double* p, size_t bytes, cudaStream_t st, int* iterations, double* residual) {
-  if (cudaMemcpyAsync(p, it->w64.x, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MGPU_ERR_CUDA;
+int iter_slab_end(IterSolverDev* it, void* p, size_t n, cudaStream_t st, int* iterations, double* residual) {
+  if (it->fp32) {
+    k_convert_levels<double, float><<<592, 256, 0, st>>>(it->w64.x, static_cast<float*>(p), (long long)n);
+    *iterations = it->inner_its;
+    it->inner_its = 0;
+    *residual = it->slab_err;
+    return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
+  }
+  if (cudaMemcpyAsync(p, it->w64.x, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MGPU_ERR_CUDA;
   *iterations = it->st_host->it_done;
   *residual = it->st_host->err;
   return it->st_host->err < it->tol ? MGPU_OK : MGPU_ERR_NOT_CONVERGED;
 }
 
-int iter_slab_vectors(IterSolverDev* it, int set, double** f) {
-  if (!it || it->fp32) return -1;
-  switch (set) {
-    case MGPU_HALO_ITER_X: f[0] = it->w64.x; return 1;
-    case MGPU_HALO_ITER_PP: f[0] = it->w64.pp; return 1;
-    case MGPU_HALO_ITER_CS: f[0] = it->w64.cs; return 1;
-    case MGPU_HALO_ITER_CG:
-      // conjugate gradients: z and the old direction, from which k_cg_apply forms p' at the
-      // neighbours of each interior point
-      f[0] = it->w64.s;
-      f[1] = cg_p(it, it->cg_n);
-      return 2;
+int iter_slab_vectors(IterSolverDev* it, int set, void** f) {
+  if (!it) return -1;
+  if (set == MGPU_HALO_ITER_X64) {
+    // the refinement's FP64 iterate of an FP32-mixed model
+    if (!it->fp32) return -1;
+    f[0] = it->w64.x;
+    return 1;
   }
-  return -1;
+  auto pick = [&](auto& w) -> int {
+    switch (set) {
+      case MGPU_HALO_ITER_X: f[0] = w.x; return 1;
+      case MGPU_HALO_ITER_PP: f[0] = w.pp; return 1;
+      case MGPU_HALO_ITER_CS: f[0] = w.cs; return 1;
+      case MGPU_HALO_ITER_CG:
+        // conjugate gradients: z and the old direction, from which k_cg_apply forms p' at the
+        // neighbours of each interior point
+        f[0] = w.s;
+        f[1] = cg_p(w, it->cg_n);
+        return 2;
+    }
+    return -1;
+  };
+  return it->fp32 ? pick(it->w32) : pick(it->w64);
 }
 
 template <typename T>

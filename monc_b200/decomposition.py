@@ -265,6 +265,8 @@ class _Slab:
         self.state_bufs = [torch.zeros(nf * g.nz * g.halo * g.nx, dtype=dtype, device=device) for _ in range(4)]
         # depth-1 sets of one or two fields: p, the iterative solve's vectors
         self.p_bufs = [torch.zeros(2 * g.nz * g.nx, dtype=dtype, device=device) for _ in range(4)]
+        # the FP32-mixed refinement's FP64 iterate
+        self.x64_bufs = [torch.zeros(g.nz * g.nx, dtype=torch.float64, device=device) for _ in range(4)]
         self.means = torch.zeros((1 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
         # the mean profiles damping, subsidence and profile_diagnostics read (mgpu_slab_mean_profiles)
         self.profiles = torch.zeros((6 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
@@ -293,8 +295,6 @@ class SlabDomain:
         # profile_diagnostics reads them
         # the pressure solve: the distributed FFT, or iterativesolver's BiCGStab (FP64)
         self.iterative = cfg.solver == cf.SOLVER_ITERATIVE
-        if self.iterative and cfg.precision != cf.FP64:
-            raise ValueError("the decomposed iterative solve runs in FP64")
         self.mean_profiles = bool(cfg.damping_enabled or cfg.profile_diagnostics_enabled
                                   or (cfg.l_subs_pl_theta and not cfg.subsidence_local_theta)
                                   or (cfg.l_subs_pl_q and not cfg.subsidence_local_q and cfg.number_q_fields > 0))
@@ -349,7 +349,8 @@ class SlabDomain:
     # -- stepping
     def _exchange(self, halo_set: int, depth: int):
         # the depth-1 sets (p and the solver vectors) share the pressure buffers
-        bufs = [s.state_bufs if halo_set == cf.HALO_STATE else s.p_bufs for s in self.slabs]
+        bufs = [s.state_bufs if halo_set == cf.HALO_STATE else
+                (s.x64_bufs if halo_set == cf.HALO_ITER_X64 else s.p_bufs) for s in self.slabs]
         for s, b in zip(self.slabs, bufs):
             s.m.halo_pack(halo_set, depth, b[0].data_ptr(), b[1].data_ptr())
         self.comm.halo_exchange([b[0] for b in bufs], [b[1] for b in bufs], [b[2] for b in bufs],
@@ -407,12 +408,42 @@ class SlabDomain:
         done = [s.m.slab_iter(cf.SLAB_ITER_FINISH, s.sums.data_ptr()) for s in self.slabs]
         return done[0]
 
-    def _iterative_solve(self):
-        """iterativesolver over the slabs (mgpu_slab_iter), BiCGStab or conjugate gradients: halo
-        rows of the vectors A is applied to, and every inner product summed over the slabs
-        (inner_prod's allreduce)."""
+    def _all(self, step: int):
         for s in self.slabs:
-            s.m.slab_iter(cf.SLAB_ITER_BEGIN)
+            s.m.slab_iter(step)
+
+    def _iterative_solve(self):
+        """iterativesolver over the slabs (mgpu_slab_iter), BiCGStab or conjugate gradients, with
+        the FP32-mixed models' iterative refinement around an FP32 solve: halo rows of the vectors
+        A is applied to, and every inner product summed over the slabs (inner_prod's allreduce)."""
+        self._all(cf.SLAB_ITER_BEGIN)
+        if self.fp32:
+            self._refinement()
+        else:
+            self._krylov()
+        self._all(cf.SLAB_ITER_END)
+
+    def _refinement(self):
+        """The FP32-mixed solve: the compatible right-hand side, then FP64 residuals and FP32
+        corrections until the residual meets the tolerance or stops falling (8 at most)."""
+        self._reduce_step(cf.SLAB_ITER_COMPAT)
+        self._all(cf.SLAB_ITER_SHIFT)
+        prev_err = 0.0
+        for outer in range(8):
+            self._exchange(cf.HALO_ITER_X64, 1)
+            if self._reduce_step(cf.SLAB_ITER_REFINE):
+                break
+            err = self.slabs[0].m.reductions().solver_residual
+            if outer > 0 and not err < prev_err:
+                self._all(cf.SLAB_ITER_UNCORRECT)
+                break
+            prev_err = err
+            self._all(cf.SLAB_ITER_INNER)
+            self._krylov()
+            self._all(cf.SLAB_ITER_CORRECT)
+
+    def _krylov(self):
+        """BiCGStab or conjugate gradients on the current work vectors."""
         self._exchange(cf.HALO_ITER_X, 1)
         done = self._reduce_step(cf.SLAB_ITER_INIT)
         if self.cfg.solver_type == cf.ITER_CG:
@@ -422,21 +453,15 @@ class SlabDomain:
                 self._exchange(cf.HALO_ITER_CG, 1)
                 self._reduce_step(cf.SLAB_ITER_APPLY)
                 done = self._reduce_step(cf.SLAB_ITER_UPDATE)
-            for s in self.slabs:
-                s.m.slab_iter(cf.SLAB_ITER_END)
             return
         while not done:
-            for s in self.slabs:
-                s.m.slab_iter(cf.SLAB_ITER_DIRECTION)
+            self._all(cf.SLAB_ITER_DIRECTION)
             self._exchange(cf.HALO_ITER_PP, 1)
             self._reduce_step(cf.SLAB_ITER_APPLY)
-            for s in self.slabs:
-                s.m.slab_iter(cf.SLAB_ITER_HALF_STEP)
+            self._all(cf.SLAB_ITER_HALF_STEP)
             self._exchange(cf.HALO_ITER_CS, 1)
             self._reduce_step(cf.SLAB_ITER_APPLY2)
             done = self._reduce_step(cf.SLAB_ITER_UPDATE)
-        for s in self.slabs:
-            s.m.slab_iter(cf.SLAB_ITER_END)
 
     def checkpoint_write(self, path: str):
         """One MONC-layout checkpoint of the whole domain: the slabs' interior rows gathered, the

@@ -11,7 +11,8 @@ after all queued work has finished; no kernel waits on another slab).
 * cfltest on the slabs: the extrema combined by a maximum give the single domain's dtm sequence,
   and the fields of the adaptive-dtm run bit for bit.
 * iterativesolver on the slabs, BiCGStab and conjugate gradients: the inner products summed over
-  the slabs, the iterates match the single domain's to rounding.
+  the slabs, the iterates match the single domain's to rounding; the FP32-mixed refinement
+  reaches the same residual.
 * Checkpoints of a decomposed run: one whole-domain file, restarts bit for bit.
 * The slab entry points themselves: halo rows, the transposed column solve, argument checks.
 """
@@ -375,6 +376,30 @@ def test_slab_checkpoint_restart(gpu_lib, tmp_path, nranks):
     for f in STATE:
         assert np.abs(m.download(f) - ref[f]).max() <= 1e-10 * np.abs(ref[f]).max(), f
     m.close()
+
+
+@ITER_TYPES
+def test_fp32_mixed_iterative_solve_on_slabs(gpu_lib, stype):
+    """The FP32-mixed solve on slabs (the compatible right-hand side, FP64 residuals over the
+    slabs' interior rows, FP32 corrections, each with its sums over the slabs) reaches the
+    single domain's residual and tracks its fields."""
+    c = iterative_config(1e-8, 500, stype)
+    c.precision = cf.FP32_MIXED
+    st = dry_state()
+    m = api.Model(c)
+    m.set_state(st)
+    m.step(3)
+    ref = {f: m.download(f) for f in STATE}
+    res_ref = m.reductions().solver_residual
+    m.close()
+    d = dc.SlabDomain(c, dc.LoopbackComm(2))
+    d.set_state(st)
+    d.step(3)
+    res = [s.m.reductions().solver_residual for s in d.slabs]
+    assert len(set(res)) == 1 and res[0] < 1e-8 and res_ref < 1e-8
+    for f in STATE:
+        assert np.abs(d.download(f) - ref[f]).max() <= 1e-5 * np.abs(ref[f]).max(), f
+    d.close()
 
 
 def test_halo_rows_pack_and_unpack(gpu_lib):
