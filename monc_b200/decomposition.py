@@ -9,14 +9,19 @@ whole x rows (x stays periodic inside each model) and the FFT solve needs one tr
     per step, on every slab
       halo exchange of the state (u v w th zu zv zw zth q zq), `halo` rows each side
       subgrid phase
+      cfltest evaluation steps: the six extrema, max-reduced over all slabs
       FP32-mixed: level means of th and q over the slab, averaged over all slabs
       dynamics phase (dynamics, scalar swap, pressure source)
-      x-FFT of the interior rows, written straight into per-destination kx blocks
-      all-to-all: rank q receives kx block q of every slab (all rows of its wavenumbers)
-      y-FFT, tridiagonal solve, inverse y-FFT on those columns
-      all-to-all back, inverse x-FFT into the interior rows of p
+      damping, mean-profile subsidence or profile diagnostics: the mean profiles, averaged
+      FFT solve:
+        x-FFT of the interior rows, written straight into per-destination kx blocks
+        all-to-all: rank q receives kx block q of every slab (all rows of its wavenumbers)
+        y-FFT, tridiagonal solve, inverse y-FFT on those columns
+        all-to-all back, inverse x-FFT into the interior rows of p
+      or iterative solve (BiCGStab or conjugate gradients, FP32-mixed refinement around them):
+        depth-1 halo rows of each vector before A is applied to it, every inner product summed
       halo exchange of p (1 row each side: the pressure gradient reaches row j+1)
-      pstep phase (pressure step, swap_smooth)
+      pstep phase (cfltest and the Galilean frame, pressure step, swap_smooth)
 
 `halo` = 4 rows covers the step's stencil reach: 2 rows for TVD advection and the viscous and
 diffusive fluxes, 1 more for the pressure source, which reads the stepped velocities at j-1.
