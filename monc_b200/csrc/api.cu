@@ -51,6 +51,7 @@ struct mgpu_handle {
   IterSolverDev* iter = nullptr;
   unsigned long long* divmax_d = nullptr;
   double global_divmax = 0.0;
+  bool divmax_step = false;  // the last mgpu_step left diverr's max in divmax_d (iterative solver)
   int solver_iterations = 0;
   double solver_residual = 0.0;
   int64_t launches = 0;
@@ -698,6 +699,13 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   h->launches += subsidence_tendencies(h);
   if (h->cfg.reproducible) h->launches += exact::launch_fused_subgrid<T>(h->sc, d, h->stream);
   else h->launches += fast::launch_fused_subgrid<T>(h->sc, d, h->stream);
+  if (h->cfg.solver == MGPU_SOLVER_ITERATIVE) {
+    // diverr's divergence error, which the iterative solver reduces to global_divmax
+    // (iterativesolver.F90:102, 606-613)
+    cudaMemsetAsync(h->divmax_d, 0, sizeof(unsigned long long), h->stream);
+    h->launches += launch_divmax<T>(h->sc, d, h->divmax_d, h->stream);
+    h->divmax_step = true;
+  }
   if (cfl_gather) {
     // the extrema of the pre-step zu, zv, zw and of this step's vis, diff (zu..zw change only in
     // the pressure step at the end of the step)
@@ -1027,6 +1035,13 @@ int mgpu_set_timestep(mgpu_handle* h, int32_t ts) {
 
 int mgpu_get_reductions(mgpu_handle* h, mgpu_reductions* out) {
   if (!h || !out) return MGPU_ERR_ARGUMENT;
+  if (h->divmax_step) {
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, h->divmax_d, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::memcpy(&h->global_divmax, &bits, sizeof(bits));
+    h->divmax_step = false;
+  }
   out->global_divmax = h->global_divmax;
   out->solver_iterations = h->solver_iterations;
   out->solver_residual = h->solver_residual;

@@ -115,6 +115,55 @@ int launch_cfl_max_form(const double* src, double* dst, cudaStream_t st) {
   return 1;
 }
 
+// diverr's divergence error (diverr.F90:69-82, 120-175): max |p| over levels 2..nz of the rows
+// halo .. ny-halo-1, p = (cx du + cy dv + 4 (tzc2 w_k - tzc1 w_{k-1})) timec from the velocities the
+// step starts from (u, v, w forward; zu, zv, zw centred).  A block maximum, then one atomicMax on
+// the bit pattern (non-negative doubles order as their bits do).
+template <typename T>
+__global__ void __launch_bounds__(CFL_THREADS) k_divmax(Scalars s, const T* __restrict__ u, const T* __restrict__ v,
+                                                        const T* __restrict__ w, int halo,
+                                                        unsigned long long* __restrict__ out) {
+  const double* tzc1 = s.prof + P_TZC1 * (s.nz + 2);
+  const double* tzc2 = s.prof + P_TZC2 * (s.nz + 2);
+  const T timec = s.forward ? (T)(1.0 / s.dtm) : (T)(1.0 / (2.0 * s.dtm));
+  const long long rows = (long long)(s.ny - 2 * halo) * s.nx;
+  const long long n = (long long)(s.nz - 1) * rows;
+  double m = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long lev = t / rows, r = t - lev * rows;
+    const int k = (int)lev + 2, j = halo + (int)(r / s.nx), i = (int)(r % s.nx);
+    const int iw = i == 0 ? s.nx - 1 : i - 1, js = j == 0 ? s.ny - 1 : j - 1;
+    const long long o = (long long)(k - 1) * s.plane + (long long)j * s.nx + i;
+    T pp = (T)0.0;
+    pp = pp + (T)s.cx * (u[o] - u[o - i + iw]);
+    pp = pp + (T)s.cy * (v[o] - v[o + (long long)(js - j) * s.nx]);
+    pp = pp + (T)4.0 * ((T)tzc2[k] * w[o] - (T)tzc1[k] * w[o - s.plane]);
+    pp = pp * timec;
+    const double a = fabs((double)pp);
+    m = a > m ? a : m;
+  }
+  for (int off = 16; off; off >>= 1) {
+    const double o2 = __shfl_down_sync(0xffffffffu, m, off);
+    m = o2 > m ? o2 : m;
+  }
+  __shared__ double sh[CFL_THREADS / 32];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < CFL_THREADS / 32; ++q) m = sh[q] > m ? sh[q] : m;
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+template <typename T>
+int launch_divmax(const Scalars& s, const DevState<T>& d, unsigned long long* out, cudaStream_t st, int halo) {
+  const bool fwd = s.forward != 0;
+  k_divmax<T><<<CFL_BLOCKS, CFL_THREADS, 0, st>>>(s, fwd ? d.u : d.zu, fwd ? d.v : d.zv, fwd ? d.w : d.zw, halo, out);
+  return 1;
+}
+template int launch_divmax<double>(const Scalars&, const DevState<double>&, unsigned long long*, cudaStream_t, int);
+template int launch_divmax<float>(const Scalars&, const DevState<float>&, unsigned long long*, cudaStream_t, int);
+
 template int launch_cfl_gather<double>(const Scalars&, const DevState<double>&, bool, double*, double*, cudaStream_t,
                                        int);
 template int launch_cfl_gather<float>(const Scalars&, const DevState<float>&, bool, double*, double*, cudaStream_t,

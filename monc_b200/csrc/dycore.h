@@ -95,6 +95,9 @@ int launch_cfl_gather(const Scalars& s, const DevState<T>& d, bool with_vis, dou
                       cudaStream_t st, int halo = 0);
 // src -> dst with the two minima negated (the form a maximum all-reduce combines); its own inverse
 int launch_cfl_max_form(const double* src, double* dst, cudaStream_t st);
+// diverr's max |p| of the velocities the step starts from, atomically maxed into *out (double bits)
+template <typename T>
+int launch_divmax(const Scalars& s, const DevState<T>& d, unsigned long long* out, cudaStream_t st, int halo = 0);
 
 // mean profiles (olzubar, olzvbar, olzthbar, olzqbar) of zu, zv, th and q into olz (rows of nz+2),
 // and the mean-profile subsidence tendencies (forcing.cu)
