@@ -540,6 +540,33 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def launch_plan(gpus: int, env) -> str:
+    """How `--gpus N` is honoured: "run" when this process is one of N ranks (or N = 1 without a
+    launcher), "spawn" when N > 1 was asked for without a launcher (bench.py then starts N ranks
+    under torch.distributed.run itself).  A launcher whose world size differs from N is an error,
+    so that a run never reports a GPU count other than the one requested."""
+    if gpus < 1:
+        raise SystemExit(f"bench.py: --gpus must be >= 1 (got {gpus})")
+    world = env.get("WORLD_SIZE")
+    if world is None:
+        return "spawn" if gpus > 1 else "run"
+    if int(world) != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but the launcher started WORLD_SIZE={world} ranks")
+    return "run"
+
+
+def spawn_ranks(gpus: int, argv: list) -> int:
+    """Re-run this command as `gpus` ranks under torch.distributed.run on 127.0.0.1."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *argv]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -557,6 +584,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if launch_plan(args.gpus, os.environ) == "spawn":
+        raise SystemExit(spawn_ranks(args.gpus, sys.argv[1:]))
     if args.impl == "reference":
         run_reference(args)
     else:
