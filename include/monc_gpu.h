@@ -351,23 +351,28 @@ int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches);
 
 /* Pressure solve that allocates nothing on the device (no counterpart in the reference).
  *
- * For callers that may not call cudaMalloc -- code that runs while a CUDA graph is being
- * captured, or a host model whose device memory belongs to another allocator and must not grow
- * during a run.  The caller passes p (device pointer, FP64 [nz][ny][nx], x fastest): the
- * right-hand side on entry, the pressure on return, solved exactly as the fftsolver component
- * solves it.  czb, cza, czg, czh are host arrays of nz values, element k-1 holding MONC level k
- * (as mgpu_get_profile / mgpu_reference_profile return them); dx, dy the horizontal spacings;
- * stream a cudaStream_t or NULL.  nx and ny must be powers of two.
+ * For host models that cannot call cudaMalloc: their device memory belongs to another allocator
+ * (a caching allocator, or a pool sized at start-up to most of HBM) and may not grow during a
+ * run, or their step loop must not meet the device-wide synchronisation that cudaFree implies.
+ * The caller passes p (device pointer, FP64 [nz][ny][nx], x fastest): the right-hand side on
+ * entry, the pressure on return, solved exactly as the fftsolver component solves it.  czb, cza,
+ * czg, czh are DEVICE arrays of nz doubles owned by the caller, element k-1 holding MONC level k
+ * (the values mgpu_get_profile / mgpu_reference_profile return), read during the call; dx, dy
+ * the horizontal spacings; stream a cudaStream_t or NULL.  nx and ny must be powers of two.
  *
- * All working storage (spectra, elimination scratch, pivots, twiddles) is one file-scope device
- * array of MGPU_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit;
- * grids needing more (about 128 x 128 x 64 is the largest cube-like grid that fits) are
- * rejected with MGPU_ERR_ARGUMENT and a message on stderr.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Nothing in the array has to start at zero -- each call writes every value it later
- * reads -- but all calls share the array and keep the last call's contents, so calls whose work
- * overlaps on the GPU (different streams or devices sharing a context) race and must be
- * serialised by the caller. */
+ * All working storage (spectra, elimination scratch, pivots, twiddles, a copy of the
+ * coefficients) is one file-scope device array of MGPU_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit; grids needing more (about 128 x 128 x 64 is the largest
+ * cube-like grid that fits) are rejected with MGPU_ERR_ARGUMENT and a message on stderr.  The
+ * first call on a device looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  Nothing in the array has to start at zero -- each call
+ * writes every value it later reads -- but all calls share the array and keep the last call's
+ * contents, so calls whose work overlaps on the GPU (different streams or devices sharing a
+ * context) race and must be serialised by the caller.
+ *
+ * There is no handle, so mgpu_last_error does not apply: the call returns a status code and
+ * writes its message to stderr.  A CUDA error left pending by earlier work is reported on stderr
+ * as such and cleared; MGPU_ERR_CUDA means a launch of this call failed. */
 #define MGPU_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
 int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32_t nz, double dx, double dy,
                              const double* czb, const double* cza, const double* czg, const double* czh,

@@ -867,13 +867,14 @@ template void launch_diagnostics<float>(const Scalars&, const float*, const floa
 // =============================================================================================
 // Poisson solve without device allocation.
 //
-// Callers that cannot allocate device memory -- code running while a CUDA graph is being
-// captured, or a host model whose device memory is owned by another allocator and which may not
-// grow the device footprint during a run -- can still solve for the pressure: the caller passes
-// the right-hand side (overwritten with the solution) and the vertical coefficients, and every
-// piece of working storage (spectra, Thomas scratch, pivots, twiddles) lives in the fixed
-// file-scope array below.  That array is part of the library image: every GPU that loads the
-// library holds MGPU_NOALLOC_SCRATCH_BYTES until the process exits.
+// Some host models cannot call cudaMalloc: their device memory is owned by another allocator (a
+// caching allocator or a pool sized at start-up to most of HBM) and may not grow during a run, or
+// their step loop must not meet the device-wide synchronisation that cudaFree implies.  They can
+// still solve for the pressure: the caller passes the right-hand side (overwritten with the
+// solution) and the vertical coefficients, all in device memory it owns, and every piece of
+// working storage (spectra, Thomas scratch, pivots, twiddles, the coefficient block) lives in the
+// fixed file-scope array below.  That array is part of the library image: every GPU that loads
+// the library holds MGPU_NOALLOC_SCRATCH_BYTES until the process exits.
 // =============================================================================================
 
 #include "../../include/monc_gpu.h"
@@ -908,6 +909,19 @@ __global__ void k_noalloc_twiddles(double2* tw, int n) {
   double sv, cv;
   sincospi(2.0 * (double)q / (double)n, &sv, &cv);
   tw[q] = make_double2(cv, -sv);
+}
+
+// the caller's vertical coefficients (device arrays, element k-1 = level k) into the scratch
+// profile block, level k at index k as the tridiagonal kernels read it
+__global__ void k_noalloc_coeffs(double* prof, int stride, int nz, const double* __restrict__ czb,
+                                 const double* __restrict__ cza, const double* __restrict__ czg,
+                                 const double* __restrict__ czh) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (k > nz) return;
+  prof[(size_t)P_CZB * stride + k] = czb[k - 1];
+  prof[(size_t)P_CZA * stride + k] = cza[k - 1];
+  prof[(size_t)P_CZG * stride + k] = czg[k - 1];
+  prof[(size_t)P_CZH * stride + k] = czh[k - 1];
 }
 
 // Thomas pivots per (|ky|, kx), formed as fftsolver.F90:72-90 and :259-280 form them
@@ -960,9 +974,17 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
                  nx, ny, nz, need, (size_t)MGPU_NOALLOC_SCRATCH_BYTES);
     return MGPU_ERR_ARGUMENT;
   }
+  // an error left pending by earlier, unrelated work is reported as such and not as this call's
+  const cudaError_t earlier = cudaGetLastError();
+  if (earlier != cudaSuccess)
+    std::fprintf(stderr, "mgpu_poisson_fft_noalloc: a CUDA error was pending before this call: %s\n",
+                 cudaGetErrorString(earlier));
   int status = MGPU_OK;
   unsigned char* base = reinterpret_cast<unsigned char*>(noalloc_scratch_address(&status));
-  if (status != MGPU_OK) return status;
+  if (status != MGPU_OK) {
+    std::fprintf(stderr, "mgpu_poisson_fft_noalloc: cudaGetSymbolAddress of the scratch array failed\n");
+    return status;
+  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   double2* spec = reinterpret_cast<double2*>(base);
   double2* s1 = reinterpret_cast<double2*>(base + b_spec);
@@ -970,13 +992,7 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   double2* twx = reinterpret_cast<double2*>(base + b_spec + b_s1 + b_b1);
   double2* twy = reinterpret_cast<double2*>(base + b_spec + b_s1 + b_b1 + b_twx);
   double* prof = reinterpret_cast<double*>(base + b_spec + b_s1 + b_b1 + b_twx + b_twy);
-  // vertical coefficients: caller arrays hold level k at element k-1; the kernels index level k
-  const double* src[4] = {czb, cza, czg, czh};
-  const int ids[4] = {P_CZB, P_CZA, P_CZG, P_CZH};
-  for (int q = 0; q < 4; ++q)
-    if (cudaMemcpyAsync(prof + (size_t)ids[q] * stride + 1, src[q], sizeof(double) * nz, cudaMemcpyHostToDevice, st) !=
-        cudaSuccess)
-      return MGPU_ERR_CUDA;
+  k_noalloc_coeffs<<<(nz + 127) / 128, 128, 0, st>>>(prof, stride, nz, czb, cza, czg, czh);
   k_noalloc_twiddles<<<(nx + 127) / 128, 128, 0, st>>>(twx, nx);
   k_noalloc_twiddles<<<(ny + 127) / 128, 128, 0, st>>>(twy, ny);
   k_noalloc_pivots<<<(nyh * nxh + 127) / 128, 128, 0, st>>>(b1, prof, stride, nx, ny, nz, dx, dy);
@@ -988,5 +1004,10 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
       spec, s1, b1, prof, stride, nx, ny, nz, 0, nxh, 0, ny);
   launch_fft_y<double>(true, ilog2(ny), spec, twy, nxh, nz, ny, st);
   launch_fft_x<double>(true, ilog2(nx), p, spec, twx, ny, nz, ny, 0, 1, st);
-  return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "mgpu_poisson_fft_noalloc: kernel launch failed: %s\n", cudaGetErrorString(e));
+    return MGPU_ERR_CUDA;
+  }
+  return MGPU_OK;
 }
