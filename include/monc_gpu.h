@@ -103,6 +103,7 @@ enum mgpu_component_id {
   MGPU_C_MEAN_PROFILES,         /* meanprofiles.F90:95-216: olzubar, olzvbar, olzthbar, olzqbar */
   MGPU_C_DAMPING,               /* damping.F90:301-409 */
   MGPU_C_FORCING,               /* forcing.F90:918-1166: subsidence of u, v, theta and q */
+  MGPU_C_TH_ADVECTION,          /* thadvection.F90:129-219: advection of the mean baroclinicity */
   MGPU_C_COUNT
 };
 
@@ -179,6 +180,19 @@ typedef struct mgpu_config {
   int32_t galilean_transformation;
   int32_t fix_ugal, fix_vgal;
   double  ugal, vgal;                 /* the fixed frame velocities (fix_ugal, fix_vgal) */
+  /* th_advection (thadvection.F90:129-219) and the geostrophic shear of coriolis
+   * (coriolis.F90:140-163, global_config:52,147-154).  With baroclinicity_use_geostrophic_shear
+   * the geostrophic wind grows with height, ug(k) = surface_geostrophic_wind_x +
+   * geostrophic_wind_rate_of_change_in_x zn(k) (v likewise), and th_advection adds the advection
+   * of the mean baroclinicity, ((v + vgal) mfx - (u + ugal) mfy) with mfx =
+   * rate_change_geostrophic_wind_x thref0 fcoriol / G (mfy likewise), to the theta source at
+   * levels 2..nz; MONC does the latter only with passive q.  The library is Boussinesq (rho =
+   * rhobous), where thref is constant and th_advection's vertical advection of the reference
+   * state is zero. */
+  int32_t th_advection_enabled;       /* th_advection_enabled */
+  int32_t baroclinicity_use_geostrophic_shear;
+  double  rate_change_geostrophic_wind_x, rate_change_geostrophic_wind_y;          /* th_advection's keys */
+  double  geostrophic_wind_rate_of_change_in_x, geostrophic_wind_rate_of_change_in_y; /* coriolis's keys */
 } mgpu_config;
 
 /* Diagnostic reductions computed on the device after a step. */
@@ -207,8 +221,9 @@ void mgpu_config_defaults(mgpu_config* cfg);
  * (replaces gridmanager.F90:2008-2075 + simplesetup.F90:60-126 initialisation callbacks)
  * and allocates every field on the current CUDA device.
  * MGPU_ERR_ARGUMENT (checked on the host before any device call): nx, ny even and >= 4; with the
- * FFT solver nx and ny powers of two <= 4096; 3 <= nz <= MGPU_MAX_NZ; dtm > 0; known precision and
- * solver.  MGPU_ERR_NO_DEVICE when no CUDA device is visible.  A model with solver
+ * FFT solver nx and ny <= 4096 with no prime factor other than 2, 3 and 5 (FFTPACK's radix-2, 3, 4
+ * and 5 passes, cffti1.f90:8; powers of two take the radix-16 kernels, the rest mixed-radix
+ * ones); 3 <= nz <= MGPU_MAX_NZ; dtm > 0; known precision and solver.  MGPU_ERR_NO_DEVICE when no CUDA device is visible.  A model with solver
  * MGPU_SOLVER_EXTERNAL is one slab of a decomposed domain (see mgpu_slab_init below); mgpu_step
  * refuses it. */
 int mgpu_create(const mgpu_config* cfg, mgpu_handle** out);
@@ -401,6 +416,14 @@ int mgpu_tl_step(mgpu_handle* h, int32_t nsteps, double d_rmlmax);
  * checkpoint_interval steps; the reverse sweep recomputes each segment from its checkpoint. */
 int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval, double* rmlmax_bar);
 
+/* Gradient-check diagnostic (no counterpart in the reference): the number of branch decisions in
+ * which the next steps of two dry FP64 models of one grid differ -- for every point, the theta TVD
+ * faces' upwind sides, smooth-region early returns, limiter choices and gradient-term stencil
+ * signs, and the Smagorinsky regime of the Richardson number.  Stepping two models started at
+ * x + eps d and x - eps d side by side and adding the counts shows whether a central difference
+ * along d straddles a kink of the discrete step.  Sets *count. */
+int mgpu_branch_flips(mgpu_handle* a, mgpu_handle* b, int64_t* count);
+
 /* ---- y-slab domain decomposition ---------------------------------------------------------
  *
  * The horizontal domain split into y-slabs, one per GPU (MONC splits it into 2-D blocks,
@@ -429,7 +452,7 @@ int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval
  * step computes each interior point with the operations of the single-domain step; with
  * reproducible = 1 an FP64 decomposed run equals the single-domain run bit for bit. */
 
-/* Set the slab geometry: ny_global (power of two) rows in all, `halo` rows each side, at most
+/* Set the slab geometry: ny_global rows in all (nx and ny_global as mgpu_create's FFT sizes), `halo` rows each side, at most
  * max_cols kx columns per mgpu_slab_solve_columns call.  Builds the pivots and twiddles of the
  * (nx, ny_global) solve.  Needs ny - 2*halo even, >= max(halo, 2). */
 int mgpu_slab_init(mgpu_handle* h, int32_t ny_global, int32_t halo, int32_t max_cols);

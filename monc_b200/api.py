@@ -72,6 +72,7 @@ COMPONENTS = {
     "mean_profiles": 20,
     "damping": 21,
     "forcing": 22,
+    "th_advection": 23,
 }
 
 # the profile_diagnostics sums mgpu_profile_diagnostics returns, under the names MONC's component
@@ -85,8 +86,8 @@ PROFILE_DIAGNOSTICS = ["u_wind_total_local", "v_wind_total_local", "w_wind_total
 GROUPS = {
     "start": ["clearsourceterms", "stepping_direction", "halo_swapper"],
     "subgrid": ["lower_bc", "smagorinsky"],
-    "dynamics": ["pw_advection", "tvd_advection", "diffusion", "viscosity", "coriolis", "buoyancy", "damping",
-                 "forcing", "set_consistent_lowbc", "simplecloud", "diverr", "psrce", "stepfields"],
+    "dynamics": ["pw_advection", "tvd_advection", "th_advection", "diffusion", "viscosity", "coriolis", "buoyancy",
+                 "damping", "forcing", "set_consistent_lowbc", "simplecloud", "diverr", "psrce", "stepfields"],
     "solver": ["mean_profiles", "fftsolver", "iterativesolver"],
     "pressure-terms": ["pstep", "swap_smooth"],
 }
@@ -179,6 +180,8 @@ def lib():
     L.mgpu_poisson_fft_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.mgpu_poisson_fft_noalloc.restype = C.c_int
+    L.mgpu_branch_flips.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
+    L.mgpu_branch_flips.restype = C.c_int
     L.mgpu_fftsolver_adjoint.argtypes = [C.c_void_p]
     L.mgpu_fftsolver_adjoint.restype = C.c_int
     L.mgpu_tl_step.argtypes = [C.c_void_p, C.c_int32, C.c_double]
@@ -312,6 +315,13 @@ class Model:
 
     def set_timestep(self, ts: int):
         self._check(lib().mgpu_set_timestep(self.h, ts), "set_timestep")
+
+    def branch_flips(self, other: "Model") -> int:
+        """Branch decisions (theta TVD faces, Smagorinsky regime) in which this model's next step
+        and `other`'s differ (dry FP64 models of one grid)."""
+        n = C.c_int64(0)
+        self._check(lib().mgpu_branch_flips(self.h, other.h, C.byref(n)), "branch_flips")
+        return int(n.value)
 
     def fftsolver_adjoint(self):
         """Apply the transpose of the FFT pressure solve to p in place."""
@@ -505,6 +515,8 @@ def run_groups(model: Model, groups=("start", "subgrid", "dynamics", "solver", "
             if name == "simplecloud" and not model.cfg.simplecloud_enabled:
                 continue
             if name == "coriolis" and not model.cfg.coriolis_enabled:
+                continue
+            if name == "th_advection" and not model.cfg.th_advection_enabled:
                 continue
             if name == "damping" and not model.cfg.damping_enabled:
                 continue

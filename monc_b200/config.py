@@ -87,6 +87,9 @@ class MgpuConfig(C.Structure):
         ("profile_diagnostics_enabled", C.c_int32),
         ("galilean_transformation", C.c_int32), ("fix_ugal", C.c_int32), ("fix_vgal", C.c_int32),
         ("ugal", C.c_double), ("vgal", C.c_double),
+        ("th_advection_enabled", C.c_int32), ("baroclinicity_use_geostrophic_shear", C.c_int32),
+        ("rate_change_geostrophic_wind_x", C.c_double), ("rate_change_geostrophic_wind_y", C.c_double),
+        ("geostrophic_wind_rate_of_change_in_x", C.c_double), ("geostrophic_wind_rate_of_change_in_y", C.c_double),
     ]
 
 
@@ -226,6 +229,21 @@ def enable_galilean(c: MgpuConfig, ugal: float | None = None, vgal: float | None
     c.galilean_transformation = 1
     c.fix_ugal, c.ugal = (0, 0.0) if ugal is None else (1, ugal)
     c.fix_vgal, c.vgal = (0, 0.0) if vgal is None else (1, vgal)
+    return c
+
+
+def enable_baroclinicity(c: MgpuConfig, rate_x: float, rate_y: float, shear_x: float | None = None,
+                         shear_y: float | None = None) -> MgpuConfig:
+    """Geostrophic shear and th_advection's advection of the mean baroclinicity, with MONC's keys
+    (global_config:52,147-154): baroclinicity_use_geostrophic_shear, th_advection_enabled,
+    rate_change_geostrophic_wind_x/_y (th_advection, thadvection.F90:73-78) and
+    geostrophic_wind_rate_of_change_in_x/_y (coriolis, coriolis.F90:142-163), which default to the
+    same rates.  MONC advects the mean baroclinicity only with passive q."""
+    c.th_advection_enabled = 1
+    c.baroclinicity_use_geostrophic_shear = 1
+    c.rate_change_geostrophic_wind_x, c.rate_change_geostrophic_wind_y = rate_x, rate_y
+    c.geostrophic_wind_rate_of_change_in_x = rate_x if shear_x is None else shear_x
+    c.geostrophic_wind_rate_of_change_in_y = rate_y if shear_y is None else shear_y
     return c
 
 

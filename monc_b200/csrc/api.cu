@@ -50,6 +50,7 @@ struct mgpu_handle {
   FftPlanDev fft;
   IterSolverDev* iter = nullptr;
   unsigned long long* divmax_d = nullptr;
+  unsigned long long* flips_d = nullptr;  // mgpu_branch_flips' counter, allocated on first use
   double global_divmax = 0.0;
   bool divmax_step = false;  // the last mgpu_step left diverr's max in divmax_d (iterative solver)
   int solver_iterations = 0;
@@ -205,6 +206,11 @@ static void fill_scalars(mgpu_handle* h) {
   s.subs_local_q = c.subsidence_local_q;
   s.olz = h->olz_d;
   s.subs_tend = h->subs_tend_d;
+  // thadvection.F90:63-78: the mean baroclinicity is advected with passive q only
+  s.th_baroclinic = (c.th_advection_enabled && c.baroclinicity_use_geostrophic_shear && c.passive_q && !c.passive_th) ? 1 : 0;
+  const double fcoriol_over_G = c.fcoriol / c.G;
+  s.mfx = c.rate_change_geostrophic_wind_x * c.thref0 * fcoriol_over_G;
+  s.mfy = c.rate_change_geostrophic_wind_y * c.thref0 * fcoriol_over_G;
 }
 
 // damping and forcing act from timestep 3 (damping.F90:329-330, forcing.F90:974-975)
@@ -249,12 +255,11 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
   if (!cfg || !out) return MGPU_ERR_ARGUMENT;
   *out = nullptr;
   // host-side checks first, so a bad configuration is reported the same with or without a device
-  auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
   if (cfg->nx < 4 || cfg->ny < 4 || (cfg->nx % 2) || (cfg->ny % 2) || cfg->nz < 3 || cfg->nz > MGPU_MAX_NZ ||
       cfg->number_q_fields < 0 || cfg->number_q_fields > MGPU_MAX_Q ||
       (cfg->precision != MGPU_FP64 && cfg->precision != MGPU_FP32_MIXED) ||
       (cfg->solver != MGPU_SOLVER_FFT && cfg->solver != MGPU_SOLVER_ITERATIVE && cfg->solver != MGPU_SOLVER_EXTERNAL) ||
-      (cfg->solver == MGPU_SOLVER_FFT && (!pow2(cfg->nx) || !pow2(cfg->ny))) || !(cfg->dtm > 0.0))
+      (cfg->solver == MGPU_SOLVER_FFT && (!fft_length_ok(cfg->nx) || !fft_length_ok(cfg->ny))) || !(cfg->dtm > 0.0))
     return MGPU_ERR_ARGUMENT;
   if (cfg->cfl_enabled && (cfg->cfl_frequency < 1 || !(cfg->cfl_cvismax > 0.0) || !(cfg->cfl_cvelmax > 0.0) ||
                            !(cfg->cfl_dtmmax > 0.0) || cfg->cfl_rincmax < 0.0))
@@ -346,6 +351,7 @@ int mgpu_destroy(mgpu_handle* h) {
   cudaFree(h->prof_d);
   cudaFree(h->lookup_d);
   cudaFree(h->divmax_d);
+  cudaFree(h->flips_d);
   cudaFree(h->xfer);
   cudaFree(h->diag_d);
   cudaFree(h->bmean_d);
@@ -392,6 +398,8 @@ static int ad_supported(mgpu_handle* h) {
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the step in a frame at rest");
   if (h->cfg.damping_enabled || h->cfg.l_subs_pl_theta || h->cfg.l_subs_pl_q)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the step without damping and forcing");
+  if (h->sc.th_baroclinic)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs differentiate the step without th_advection");
   if (h->fp32 || h->cfg.number_q_fields > 0 || h->cfg.solver != MGPU_SOLVER_FFT)
     return fail(h, MGPU_ERR_UNSUPPORTED, "tangent-linear and adjoint runs need a dry FP64 model with the FFT solver");
   return MGPU_OK;
@@ -1263,6 +1271,26 @@ int mgpu_adjoint_run(mgpu_handle* h, int32_t nsteps, int32_t checkpoint_interval
   return adjoint_run(h, nsteps, checkpoint_interval, rmlmax_bar);
 }
 
+int mgpu_branch_flips(mgpu_handle* a, mgpu_handle* b, int64_t* count) {
+  if (!a || !b || !count) return MGPU_ERR_ARGUMENT;
+  mgpu_handle* h = a;  // the model whose stream runs the comparison and which reports errors
+  if (a->fp32 || b->fp32 || a->cfg.nx != b->cfg.nx || a->cfg.ny != b->cfg.ny || a->cfg.nz != b->cfg.nz ||
+      a->cfg.number_q_fields > 0 || b->cfg.number_q_fields > 0)
+    return fail(h, MGPU_ERR_ARGUMENT, "branch_flips compares two dry FP64 models of one grid");
+  a->sc.forward = (a->timestep == 1) ? 1 : 0;
+  if (!a->flips_d) CK(cudaMalloc(&a->flips_d, sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(a->flips_d, 0, sizeof(unsigned long long), a->stream));
+  // b's queued steps must be complete before a's stream reads its fields
+  CK(cudaStreamSynchronize(b->stream));
+  branch_flips(a->sc, a->d64, b->d64, a->flips_d, a->stream);
+  a->launches += 1;
+  unsigned long long host = 0;
+  CK(cudaMemcpyAsync(&host, a->flips_d, sizeof(host), cudaMemcpyDeviceToHost, a->stream));
+  CK(cudaStreamSynchronize(a->stream));
+  *count = (int64_t)host;
+  return MGPU_OK;
+}
+
 }  // extern "C"
 
 // ---- y-slab decomposition ----------------------------------------------------------------
@@ -1384,12 +1412,11 @@ int mgpu_slab_init(mgpu_handle* h, int32_t ny_global, int32_t halo, int32_t max_
     return fail(h, MGPU_ERR_UNSUPPORTED, "a slab model is created with solver MGPU_SOLVER_EXTERNAL");
   if (h->slab.b1) return fail(h, MGPU_ERR_ARGUMENT, "slab already initialised");
   const int nyl = h->cfg.ny - 2 * halo, nxh = h->cfg.nx / 2 + 1;
-  auto pow2 = [](int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; };
-  if (halo < 1 || nyl < 2 || nyl < halo || (nyl % 2) || !pow2(h->cfg.nx) || !pow2(ny_global) || nyl > ny_global ||
+  if (halo < 1 || nyl < 2 || nyl < halo || (nyl % 2) || !fft_length_ok(h->cfg.nx) || !fft_length_ok(ny_global) || nyl > ny_global ||
       max_cols < 1 || max_cols > nxh)
     return fail(h, MGPU_ERR_ARGUMENT,
                 "slab needs halo >= 1, an even number of interior rows (ny - 2*halo) >= max(halo, 2) and <= ny_global, "
-                "power-of-two nx and ny_global, and 1 <= max_cols <= nx/2+1");
+                "nx and ny_global of 4..4096 points with prime factors 2, 3 and 5, and 1 <= max_cols <= nx/2+1");
   int rc = fft_slab_plan_create(h->slab, h->sc, h->rs, ny_global, max_cols);
   if (rc) {
     fft_plan_destroy(h->slab);

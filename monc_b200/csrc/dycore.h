@@ -48,6 +48,8 @@ struct FftPlanDev {
   float* twx_f = nullptr;          // the same twiddles rounded to FP32
   float* twy_f = nullptr;
 };
+// horizontal transform lengths of the spectral solve: 4 .. 4096 points with prime factors 2, 3, 5
+bool fft_length_ok(int n);
 int fft_plan_create(FftPlanDev& plan, const Scalars& s, const RefState& rs, bool fp32);
 void fft_plan_destroy(FftPlanDev& plan);
 // evs: NULL, or 6 events recorded before, between and after the five kernels.  transpose: apply
@@ -141,6 +143,10 @@ int iter_solve(IterSolverDev* it, const Scalars& s, T* p, cudaStream_t st, int64
 enum AdField { F_U, F_V, F_W, F_TH, F_ZU, F_ZV, F_ZW, F_ZTH, F_VIS, F_DIFF, F_ZUN, F_ZVN, F_ZWN, F_P, F_PROF, F_COUNT,
                F_FACE0 = 64 };
 // pass 0 subgrid, 1 dynamics, 2 pressure source, 3 pstep + swap_smooth; t holds the tangents
+// the number of branch decisions (TVD faces of theta, Smagorinsky regime) in which two models'
+// next steps differ, added to *count (device)
+void branch_flips(const Scalars& s, const DevState<double>& a, const DevState<double>& b, unsigned long long* count,
+                  cudaStream_t st);
 void tl_pass(int pass, const Scalars& s, const DevState<double>& d, const DevState<double>& t, const double* drsq,
              double dpar, cudaStream_t st);
 // pass 0 subgrid, 1 momentum, 2 scalars, 3 pressure source, 4 pstep + swap_smooth; seed[0..7] are

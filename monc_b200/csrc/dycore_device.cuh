@@ -145,29 +145,54 @@ __device__ void lower_bc_column(const Scalars& s, const PA& P, const A& zu_state
 // ------------------------------------------------------------------------------------------
 // smagorinsky (smagorinsky.F90:180-304 setfri + dry Ri, :316-402 moist Ri, :487-696 strain)
 // ------------------------------------------------------------------------------------------
+// The parts of the strain rate that belong to one level kk (smagorinsky.F90:487-696): the squared
+// x and y differences of u and v at kk, the squared vertical difference of w below kk, and the
+// four squared horizontal-shear terms at kk.  half_squared_strain at level k combines the parts
+// of levels k and k+1, so a kernel marching up the levels carries the k+1 parts to the next level.
+template <typename T>
+struct StrainLevel {
+  T a11, a22, a33, g12;
+};
+
 template <typename T, class A, class PA>
-__device__ T half_squared_strain(const Scalars& s, const PA& P, const A& U, const A& V,
-                                 const A& W, int k, int j, int i) {
+__device__ __forceinline__ StrainLevel<T> strain_level(const Scalars& s, const PA& P, const A& U, const A& V,
+                                                       const A& W, int kk, int j, int i) {
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  StrainLevel<T> r;
+  r.a11 = sqr(U(kk, j, i) - U(kk, j, i - 1));
+  r.a22 = sqr(V(kk, j, i) - V(kk, j - 1, i));
+  r.a33 = sqr((W(kk, j, i) - W(kk - 1, j, i)) * P(P_RDZ, kk));
+  r.g12 = (sqr((U(kk, j, i - 1) - U(kk, j - 1, i - 1)) * cy + (V(kk, j - 1, i) - V(kk, j - 1, i - 1)) * cx) +
+           sqr((U(kk, j + 1, i - 1) - U(kk, j, i - 1)) * cy + (V(kk, j, i) - V(kk, j, i - 1)) * cx)) +
+          (sqr((U(kk, j, i) - U(kk, j - 1, i)) * cy + (V(kk, j - 1, i + 1) - V(kk, j - 1, i)) * cx) +
+           sqr((U(kk, j + 1, i) - U(kk, j, i)) * cy + (V(kk, j, i + 1) - V(kk, j, i)) * cx));
+  return r;
+}
+
+// half the squared strain rate at level k from the level parts lo (level k) and hi (level k+1)
+template <typename T, class A, class PA>
+__device__ __forceinline__ T half_squared_strain_parts(const Scalars& s, const PA& P, const A& U, const A& V,
+                                                       const A& W, int k, int j, int i, const StrainLevel<T>& lo,
+                                                       const StrainLevel<T>& hi) {
   const T cx = (T)s.cx, cy = (T)s.cy, cx2 = (T)s.cx2, cy2 = (T)s.cy2;
   const T rdzn1 = P(P_RDZN, k + 1);
-  T ssq11 = cx2 * (sqr(U(k + 1, j, i) - U(k + 1, j, i - 1)) + sqr(U(k, j, i) - U(k, j, i - 1)));
-  T ssq22 = cy2 * (sqr(V(k + 1, j, i) - V(k + 1, j - 1, i)) + sqr(V(k, j, i) - V(k, j - 1, i)));
-  T ssq33 = sqr((W(k, j, i) - W(k - 1, j, i)) * P(P_RDZ, k)) + sqr((W(k + 1, j, i) - W(k, j, i)) * P(P_RDZ, k + 1));
+  T ssq11 = cx2 * (hi.a11 + lo.a11);
+  T ssq22 = cy2 * (hi.a22 + lo.a22);
+  T ssq33 = lo.a33 + hi.a33;
   T ssq13 = (sqr((U(k + 1, j, i) - U(k, j, i)) * rdzn1 + (W(k, j, i + 1) - W(k, j, i)) * cx) +
              sqr((U(k + 1, j, i - 1) - U(k, j, i - 1)) * rdzn1 + (W(k, j, i) - W(k, j, i - 1)) * cx)) * (T)0.5;
   T ssq23 = (sqr((W(k, j, i) - W(k, j - 1, i)) * cy + (V(k + 1, j - 1, i) - V(k, j - 1, i)) * rdzn1) +
              sqr((W(k, j + 1, i) - W(k, j, i)) * cy + (V(k + 1, j, i) - V(k, j, i)) * rdzn1)) * (T)0.5;
-  T ssq12 =
-      (((sqr((U(k, j, i - 1) - U(k, j - 1, i - 1)) * cy + (V(k, j - 1, i) - V(k, j - 1, i - 1)) * cx) +
-         sqr((U(k, j + 1, i - 1) - U(k, j, i - 1)) * cy + (V(k, j, i) - V(k, j, i - 1)) * cx)) +
-        (sqr((U(k, j, i) - U(k, j - 1, i)) * cy + (V(k, j - 1, i + 1) - V(k, j - 1, i)) * cx) +
-         sqr((U(k, j + 1, i) - U(k, j, i)) * cy + (V(k, j, i + 1) - V(k, j, i)) * cx))) +
-       ((sqr((U(k + 1, j, i - 1) - U(k + 1, j - 1, i - 1)) * cy + (V(k + 1, j - 1, i) - V(k + 1, j - 1, i - 1)) * cx) +
-         sqr((U(k + 1, j + 1, i - 1) - U(k + 1, j, i - 1)) * cy + (V(k + 1, j, i) - V(k + 1, j, i - 1)) * cx)) +
-        (sqr((U(k + 1, j, i) - U(k + 1, j - 1, i)) * cy + (V(k + 1, j - 1, i + 1) - V(k + 1, j - 1, i)) * cx) +
-         sqr((U(k + 1, j + 1, i) - U(k + 1, j, i)) * cy + (V(k + 1, j, i + 1) - V(k + 1, j, i)) * cx)))) *
-      (T)0.125;
+  T ssq12 = (lo.g12 + hi.g12) * (T)0.125;
   return ssq11 + ssq22 + ssq33 + ssq13 + ssq23 + ssq12 + (T)s.smallp;
+}
+
+template <typename T, class A, class PA>
+__device__ T half_squared_strain(const Scalars& s, const PA& P, const A& U, const A& V,
+                                 const A& W, int k, int j, int i) {
+  const StrainLevel<T> lo = strain_level<T, A, PA>(s, P, U, V, W, k, j, i);
+  const StrainLevel<T> hi = strain_level<T, A, PA>(s, P, U, V, W, k + 1, j, i);
+  return half_squared_strain_parts<T, A, PA>(s, P, U, V, W, k, j, i, lo, hi);
 }
 
 // moist_ri_2 for one level (RICHARDSON_NUMBER_CALCULATION = 2)
@@ -218,10 +243,9 @@ __device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A
 }
 
 // vis/diff at level 2 <= k <= nz-1 from the strain rate and Richardson number
-template <typename T, class A, class PA, class AT>
-__device__ void smagorinsky_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const AT& THcur,
-                                  const AT& THarg, const AT* QV, const AT* QL, int k, int j, int i, T& vis, T& diff) {
-  T ssq = half_squared_strain<T, A>(s, P, U, V, W, k, j, i);
+template <typename T, class PA, class AT>
+__device__ void smagorinsky_from_strain(const Scalars& s, const PA& P, T ssq, const AT& THcur, const AT& THarg,
+                                        const AT* QV, const AT* QL, int k, int j, int i, T& vis, T& diff) {
   T ri = (T)0.0;
   if (!s.passive_th) {
     if (!s.passive_q) ri = moist_ri<T, AT>(s, P, ssq, THarg, *QV, *QL, k, j, i);
@@ -245,6 +269,13 @@ __device__ void smagorinsky_point(const Scalars& s, const PA& P, const A& U, con
   T sctmp = P(P_RNEUTML_SQ, k) * sqrt(ssq);
   vis = vs * sctmp;
   diff = df * sctmp;
+}
+
+template <typename T, class A, class PA, class AT>
+__device__ void smagorinsky_point(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, const AT& THcur,
+                                  const AT& THarg, const AT* QV, const AT* QL, int k, int j, int i, T& vis, T& diff) {
+  T ssq = half_squared_strain<T, A>(s, P, U, V, W, k, j, i);
+  smagorinsky_from_strain<T, PA, AT>(s, P, ssq, THcur, THarg, QV, QL, k, j, i, vis, diff);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -324,10 +355,14 @@ __device__ T tau33_at(const Scalars& s, const PA& P, const A& ZW, const A& VIS, 
   return visonp2 * (ZW(k, j, i) - ZW(k - 1, j, i)) * P(P_RDZ, k);
 }
 
+// Viscous increments at level k from this level's stresses and the level-below values tm13, tm23
+// (tau_13_23(k-1).t13, .t23) and t33 (tau33_at(k)); t13, t23 and t33p return this level's
+// tau_13_23(k).t13, .t23 and tau33_at(k+1), which a kernel marching up the levels carries to the
+// level above instead of recomputing them.
 template <typename T, class A, class PA>
-__device__ void viscosity_point(const Scalars& s, const PA& P, const A& ZU, const A& ZV,
-                                const A& ZW, const A& ZU_state, const A& VIS, int k, int j, int i,
-                                T& du, T& dv, T& dw) {
+__device__ void viscosity_core(const Scalars& s, const PA& P, const A& ZU, const A& ZV, const A& ZW,
+                               const A& ZU_state, const A& VIS, int k, int j, int i, T tm13, T tm23, T t33, T& du,
+                               T& dv, T& dw, T& t13, T& t23, T& t33p) {
   const T cx = (T)s.cx, cy = (T)s.cy, rhon = P(P_RHON, k);
   // horizontal stresses at level k (k >= 2)
   T vistmp = VIS(k, j, i) + VIS(k, j + 1, i) + VIS(k - 1, j, i) + VIS(k - 1, j + 1, i);
@@ -352,16 +387,27 @@ __device__ void viscosity_point(const Scalars& s, const PA& P, const A& ZU, cons
   T visonp2a = rhon * (VIS(k, j, i + 1) + VIS(k - 1, j, i + 1));
   T tau11p1 = visonp2a * (ZU_state(k, j, i + 1) - ZU(k, j, i)) * cx;  // reads current_state%zu at x+1
   Tau13<T> t0 = tau_13_23<T, A>(s, P, ZU, ZV, ZW, VIS, k, j, i);
-  Tau13<T> tm = tau_13_23<T, A>(s, P, ZU, ZV, ZW, VIS, k - 1, j, i);
-  du = div_rho<T>(s, (tau11p1 - tau11) * cx + (tau12 - tau12_ym1) * cy + (t0.t13 - tm.t13) * P(P_RDZ, k), rhon);
-  dv = div_rho<T>(s, (tau12 - tau12m1) * cx + (tau22_yp1 - tau22) * cy + (t0.t23 - tm.t23) * P(P_RDZ, k), rhon);
+  du = div_rho<T>(s, (tau11p1 - tau11) * cx + (tau12 - tau12_ym1) * cy + (t0.t13 - tm13) * P(P_RDZ, k), rhon);
+  dv = div_rho<T>(s, (tau12 - tau12m1) * cx + (tau22_yp1 - tau22) * cy + (t0.t23 - tm23) * P(P_RDZ, k), rhon);
   if (k < s.nz) {
-    T t33p = tau33_at<T, A>(s, P, ZW, VIS, k + 1, j, i);
-    T t33 = tau33_at<T, A>(s, P, ZW, VIS, k, j, i);
+    t33p = tau33_at<T, A>(s, P, ZW, VIS, k + 1, j, i);
     dw = div_rho<T>(s, (t0.t13 - t0.t13m1) * cx + (t0.t23 - t0.t23m1) * cy + (t33p - t33) * P(P_RDZN, k + 1), P(P_RHO, k));
   } else {
+    t33p = (T)0.0;
     dw = (T)0.0;
   }
+  t13 = t0.t13;
+  t23 = t0.t23;
+}
+
+template <typename T, class A, class PA>
+__device__ void viscosity_point(const Scalars& s, const PA& P, const A& ZU, const A& ZV,
+                                const A& ZW, const A& ZU_state, const A& VIS, int k, int j, int i,
+                                T& du, T& dv, T& dw) {
+  const Tau13<T> tm = tau_13_23<T, A>(s, P, ZU, ZV, ZW, VIS, k - 1, j, i);
+  const T t33 = k < s.nz ? tau33_at<T, A>(s, P, ZW, VIS, k, j, i) : (T)0.0;
+  T t13, t23, t33p;
+  viscosity_core<T, A, PA>(s, P, ZU, ZV, ZW, ZU_state, VIS, k, j, i, tm.t13, tm.t23, t33, du, dv, dw, t13, t23, t33p);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -544,9 +590,27 @@ struct TvdMetricScalar {
 struct TvdMetricW {
   static constexpr int RDZ = P_RDZN, RDZN = P_RDZ, DZN = P_DZ, KDOF = 1, TZ1 = P_TZD1, TZ2 = P_TZD2;
 };
+// Branch recorders of the face functions: NoRec (the kernels) records nothing and compiles away;
+// BitRec appends each decision's bits to a code, so that a gradient check can count where two
+// nearby trajectories take different branches (the kinks that finite differences straddle).
+struct NoRec {
+  __device__ __forceinline__ void operator()(unsigned, int) const {}
+};
+struct BitRec {
+  unsigned* code;
+  __device__ __forceinline__ void operator()(unsigned v, int nbits) const { *code = (*code << nbits) | v; }
+};
+
+// which of fncs, fnfs, fnrefs and 1 the limiter max(fncs, min(min(fnfs, fnrefs), 1)) takes
 template <typename T>
+__device__ __forceinline__ unsigned limiter_choice(T fncs, T fnfs, T fnrefs) {
+  const T m = tmin<T>(fnfs, fnrefs);
+  return fncs > tmin<T>(m, (T)1.0) ? 0u : (m < (T)1.0 ? (fnfs < fnrefs ? 1u : 2u) : 3u);
+}
+
+template <typename T, class Rec = NoRec>
 __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, T fdels, T fd, T fc, T fu, T fgt1, T fgt2,
-                                        T curv_term) {
+                                        T curv_term, const Rec& rec = Rec()) {
   const T r6 = (T)(1.0 / 6.0);
   T cflmod = fabs(data_value * c * dt);
   T hrcfl = rcp(sum_cfl_out + (T)1.e-30);
@@ -558,13 +622,43 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
   T fncs = (fc - fu) * rfdels;
   T fnrefs = fncs * hrcfl;
   T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+  rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
   return ftemp * fdels + fu;
 }
 
-// face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx
-template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
-__device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
-                        const AF& ZF, T dt, int k, int j, int i) {
+// Sum of the outgoing Courant numbers of cell (k, j, i) without the factor dt: the sum_cfl_out
+// that ultimateflux.F90's face routines form for the upwind cell of a face (calculate_flux_in_x,
+// _y, _w and their callers), one term per face of the cell through which the flow leaves it.
+// Written once for every face direction: the x routine's u0 + |min(0, u(i-1))| (u0 > 0) and
+// max(0, u(i+1)) - u0 (u0 <= 0) are the same values as this cell formula for cells i and i+1.
+template <typename T, class A, class PA, class M = TvdMetricScalar>
+__device__ __forceinline__ T cell_cfl_out(const Scalars& s, const PA& P, const A& U, const A& V, const A& W, int k,
+                                          int j, int i) {
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  T sum = (T)0.0;
+  sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
+  sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
+  sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i)) + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
+  return sum;
+}
+
+// The cell sums evaluated from the advecting flow where a face needs them
+template <typename T, class A, class PA, class M>
+struct CflInline {
+  const Scalars& s;
+  const PA& P;
+  const A& U;
+  const A& V;
+  const A& W;
+  __device__ __forceinline__ T operator()(int k, int j, int i) const {
+    return cell_cfl_out<T, A, PA, M>(s, P, U, V, W, k, j, i);
+  }
+};
+
+// face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx; cfl(k, j, i) gives cell_cfl_out
+template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec>
+__device__ T tvd_face_x_g(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                          const AF& ZF, T dt, int k, int j, int i, const CS& cfl, const Rec& rec = Rec()) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const int kp1 = k + 1 < nz ? k + 1 : nz;
@@ -577,26 +671,18 @@ __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fd = ZF(k, j, i + 1) * advpos + ZF(k, j, i) * advneg;
   T fdels = fd - fu;
   T fcurvs = fd - (T)2.0 * fc + fu;
+  rec(signbit(u0) ? 1u : 0u, 1);
+  rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
   if (fabs(fcurvs) >= fabs(fdels)) return fc;
-  T sum;
-  if (u0 > (T)0.0) {
-    sum = (T)0.0;
-    sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
-    sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i))));
-    sum = sum + cx * (u0 + fabs(tmin<T>((T)0.0, U(k, j, i - 1))));
-    sum = sum * dt;
-  } else {
-    sum = (T)0.0;
-    sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j, i + 1)) + fabs(tmin<T>((T)0.0, W(k - 1, j, i + 1))));
-    sum = sum + cy * (tmax<T>((T)0.0, V(k, j, i + 1)) + fabs(tmin<T>((T)0.0, V(k, j - 1, i + 1))));
-    sum = sum + cx * (tmax<T>((T)0.0, U(k, j, i + 1)) - u0);
-    sum = sum * dt;
-  }
+  // the upwind cell: i when u0 > 0, otherwise i + 1 (u0 = 0 included, as ultflx tests u > 0)
+  rec(u0 > (T)0.0 ? 1u : 0u, 1);
+  T sum = cfl(k, j, u0 > (T)0.0 ? i : i + 1) * dt;
   // gradient term in z (calculate_gradient_term_in_z with two source columns)
   T fgt1;
   {
     T sf = (T)0.125 * (W(k, j, i) + W(k - 1, j, i) + W(k, j, i + 1) + W(k - 1, j, i + 1));
     bool pos = !signbit(sf);
+    rec(pos ? 1u : 0u, 1);
     int ksu = pos ? k - 1 : kp1;
     int ksl = pos ? k : kp0;
     T ts = ZF(ksl, j, i) - ZF(ksu, j, i);
@@ -607,19 +693,26 @@ __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fgt2;
   {
     T sf = (T)0.125 * (V(k, j, i + 1) + V(k, j, i) + V(k, j - 1, i + 1) + V(k, j - 1, i));
+    rec(signbit(sf) ? 1u : 0u, 1);
     int jsu = signbit(sf) ? j + 1 : j - 1;
     T t1 = ZF(k, jsu, i) * advpos;
     T t2 = ZF(k, jsu, i + 1) * advneg;
     t1 = t1 + t2;
     fgt2 = fabs(sf) * cy * dt * (fc - t1);
   }
-  return limit_face<T>(u0, cx, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs);
+  return limit_face<T, Rec>(u0, cx, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs, rec);
+}
+
+template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
+__device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                        const AF& ZF, T dt, int k, int j, int i) {
+  return tvd_face_x_g<T, A, AF, PA, M>(s, P, U, V, W, ZF, dt, k, j, i, CflInline<T, A, PA, M>{s, P, U, V, W});
 }
 
 // face y+1/2 of cell (k, j, i): flux_y(k) of ultflx
-template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
-__device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
-                        const AF& ZF, T dt, int k, int j, int i) {
+template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec>
+__device__ T tvd_face_y_g(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                          const AF& ZF, T dt, int k, int j, int i, const CS& cfl, const Rec& rec = Rec()) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const int kp1 = k + 1 < nz ? k + 1 : nz;
@@ -633,16 +726,15 @@ __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fd = ZF(k, j + 1, i) * advpos + ZF(k, j, i) * advneg;
   T fdels = fd - fu;
   T fcurvs = fd - (T)2.0 * fc + fu;
+  rec((unsigned)jo, 1);
+  rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
   if (fabs(fcurvs) >= fabs(fdels)) return fc;
-  T sum = (T)0.0;
-  sum = sum + P(M::RDZ, k) * (tmax<T>((T)0.0, W(k, j + jo, i)) + fabs(tmin<T>((T)0.0, W(k - 1, j + jo, i))));
-  sum = sum + cy * (tmax<T>((T)0.0, V(k, j + jo, i)) + fabs(tmin<T>((T)0.0, V(k, j - 1 + jo, i))));
-  sum = sum + cx * (tmax<T>((T)0.0, U(k, j + jo, i)) + fabs(tmin<T>((T)0.0, U(k, j + jo, i - 1))));
-  sum = sum * dt;
+  T sum = cfl(k, j + jo, i) * dt;
   T fgt1;
   {
     T sf = (T)0.125 * (W(k, j, i) + W(k - 1, j, i) + W(k, j + 1, i) + W(k - 1, j + 1, i));
     bool pos = !signbit(sf);
+    rec(pos ? 1u : 0u, 1);
     int ksu = pos ? k - 1 : kp1;
     int ksl = pos ? k : kp0;
     T ts = ZF(ksl, j + jo, i) - ZF(ksu, j + jo, i);
@@ -651,16 +743,23 @@ __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fgt2;
   {
     T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k, j + 1, i - 1) + U(k, j + 1, i));
+    rec(signbit(sf) ? 1u : 0u, 1);
     T posuf = (T)0.5 + tsign<T>((T).5, sf);
     fgt2 = fabs(sf) * cx * dt * (fc - (ZF(k, j + jo, i + 1) * ((T)1. - posuf) + ZF(k, j + jo, i - 1) * posuf));
   }
-  return limit_face<T>(v0, cy, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs);
+  return limit_face<T, Rec>(v0, cy, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs, rec);
+}
+
+template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
+__device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                        const AF& ZF, T dt, int k, int j, int i) {
+  return tvd_face_y_g<T, A, AF, PA, M>(s, P, U, V, W, ZF, dt, k, j, i, CflInline<T, A, PA, M>{s, P, U, V, W});
 }
 
 // flux_z(k+1): face above level k (2 <= k <= nz-1); the top routine handles k = nz-1
-template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
-__device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
-                        const AF& ZF, T dt, int k, int j, int i) {
+template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec>
+__device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                          const AF& ZF, T dt, int k, int j, int i, const CS& cfl, const Rec& rec = Rec()) {
   const int nz = s.nz;
   const T cx = (T)s.cx, cy = (T)s.cy;
   const T w0 = W(k, j, i);
@@ -672,6 +771,8 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
     else { fu = (T)2.0 * ZF(k + 1, j, i) - ZF(k, j, i); fc = ZF(k + 1, j, i); fd = ZF(k, j, i); }
     T fcurvs = fd - (T)2.0 * fc + fu;
     T fdels = fd - fu;
+    rec(up ? 1u : 0u, 1);
+    rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
     if (fabs(fcurvs) >= fabs(fdels)) return fc;
     if (up) {
       sum = (T)0.0;
@@ -694,11 +795,13 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
     }
     {
       T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
+      rec(signbit(sf) ? 1u : 0u, 1);
       int jsu = signbit(sf) ? j + 1 : j - 1;
       fgt1 = fabs(sf) * cy * dt * (fc - ZF(kf, jsu, i));
     }
     {
       T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k + 1, j, i - 1) + U(k + 1, j, i));
+      rec(signbit(sf) ? 1u : 0u, 1);
       T posuf = (T)0.5 + tsign<T>((T).5, sf);
       fgt2 = fabs(sf) * cx * dt * (fc - (ZF(kf, j, i + 1) * ((T)1. - posuf) + ZF(kf, j, i - 1) * posuf));
     }
@@ -714,6 +817,7 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
     T fncs = (fc - fu) * rfdels;
     T fnrefs = fncs * hrcfl;
     T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+    rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
     return ftemp * fdels + fu;
   }
   // middle of the column
@@ -725,19 +829,19 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
   fd = ZF(k + 1, j, i) * advpos + ZF(k, j, i) * advneg;
   T fcurvs = fd - (T)2.0 * fc + fu;
   T fdels = fd - fu;
+  rec((unsigned)ko, 1);
+  rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
   if (fabs(fcurvs) >= fabs(fdels)) return fc;
-  sum = (T)0.0;
-  sum = sum + P(M::RDZ, k + ko) * (tmax<T>((T)0.0, W(k + ko, j, i)) + fabs(tmin<T>((T)0.0, W(k - 1 + ko, j, i))));
-  sum = sum + cy * (tmax<T>((T)0.0, V(k + ko, j, i)) + fabs(tmin<T>((T)0.0, V(k + ko, j - 1, i))));
-  sum = sum + cx * (tmax<T>((T)0.0, U(k + ko, j, i)) + fabs(tmin<T>((T)0.0, U(k + ko, j, i - 1))));
-  sum = sum * dt;
+  sum = cfl(k + ko, j, i) * dt;
   {
     T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
+    rec(signbit(sf) ? 1u : 0u, 1);
     int jsu = signbit(sf) ? j + 1 : j - 1;
     fgt1 = fabs(sf) * cy * dt * (fc - ZF(k + ko, jsu, i));
   }
   {
     T sf = (T)0.125 * (U(k, j, i - 1) + U(k, j, i) + U(k + 1, j, i - 1) + U(k + 1, j, i));
+    rec(signbit(sf) ? 1u : 0u, 1);
     T posuf = (T)0.5 + tsign<T>((T).5, sf);
     fgt2 = fabs(sf) * cx * dt * (fc - (ZF(k + ko, j, i + 1) * ((T)1. - posuf) + ZF(k + ko, j, i - 1) * posuf));
   }
@@ -754,8 +858,16 @@ __device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, c
   T fncs = (fc - fu) * rfdels;
   T fnrefs = fncs * hrcfl;
   T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+  rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
   return ftemp * fdels + fu;
 }
+
+template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
+__device__ T tvd_face_z(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
+                        const AF& ZF, T dt, int k, int j, int i) {
+  return tvd_face_z_g<T, A, AF, PA, M>(s, P, U, V, W, ZF, dt, k, j, i, CflInline<T, A, PA, M>{s, P, U, V, W});
+}
+
 
 // TVD source of cell (k, j, i), 2 <= k <= nz, from the six face values
 // acc0 is the source value before the callback (MONC accumulates into it below the top level
@@ -912,6 +1024,15 @@ __device__ void tvd_flow_point(const Scalars& s, const PA& P, const A& U, const 
     T fzp = tvd_face_z<T, F, A, PA, TvdMetricW>(s, P, IU, IV, IW, ZW, dt, k, j, i);
     sw = tvd_source<T, F, PA, TvdMetricW>(s, P, IU, IV, IW, fxm, fxp, fym, fyp, fzm, fzp, k, j, i, sw_in);
   }
+}
+
+// ------------------------------------------------------------------------------------------
+// th_advection (thadvection.F90:196-216): the advection of the mean baroclinicity, Boussinesq
+// form, added to the theta source at 2 <= k <= nz; u, v are the current flow fields
+// ------------------------------------------------------------------------------------------
+template <typename T, class A>
+__device__ __forceinline__ T th_baroclinic_point(const Scalars& s, const A& U, const A& V, int k, int j, int i) {
+  return (V(k, j, i) + (T)s.vgal) * (T)s.mfx - (U(k, j, i) + (T)s.ugal) * (T)s.mfy;
 }
 
 // ------------------------------------------------------------------------------------------

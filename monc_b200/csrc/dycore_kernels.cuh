@@ -159,6 +159,17 @@ __global__ void k_c_tvd(Scalars s, DevState<T> d, const T* zf_th, T* sth, int n_
   (void)zf_th; (void)sth; (void)n_extra;
 }
 
+// th_advection: the mean-baroclinicity term added to sth, levels 2..nz
+template <typename T>
+__global__ void k_c_th_advection(Scalars s, DevState<T> d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z + 2;
+  if (i >= s.nx || j >= s.ny || k > s.nz) return;
+  long long o = lin(s, k, j, i);
+  d.sth[o] = d.sth[o] + th_baroclinic_point<T>(s, view<T>(d.u, s), view<T>(d.v, s), k, j, i);
+}
+
 template <typename T>
 __global__ void k_c_diffusion(Scalars s, DevState<T> d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -524,6 +535,7 @@ __global__ void __launch_bounds__(256) k_f_dynamics(Scalars s, DevState<T> d) {
     if (s.subs_th) subsidence_flow_point<T>(s, P, view<T>(d.zu, s), view<T>(d.zv, s), k, j, i, su, sv);
     // tvd_advection then diffusion of theta and q, then their damping and subsidence
     sth = tvd_point<T, View<T>>(s, P, U, V, W, view<T>(fwd ? d.th : d.zth, s), k, j, i, (T)0.0);
+    if (s.th_baroclinic) sth = sth + th_baroclinic_point<T>(s, U, V, k, j, i);
     if (s.use_vd) sth = sth + diffusion_point<T, View<T>>(s, P, view<T>(d.zth, s), view<T>(d.diff, s), k, j, i);
     if (s.damping && !s.passive_th) sth = damping_scalar_point<T>(s, P, k, d.zth[o], 2, sth);
     if (s.subs_th) sth = subsidence_theta_point<T>(s, P, view<T>(d.zth, s), k, j, i, sth);
@@ -608,10 +620,12 @@ template <typename T>
 constexpr size_t smag_smem() { return sizeof(T) * ((size_t)3 * RM * G<T>::PLANE + (size_t)RP * P_COUNT); }
 template <typename T>
 constexpr size_t momentum_smem() { return sizeof(T) * ((size_t)M_PLANES * G<T>::PLANE + (size_t)RP * P_COUNT); }
+// the scalar kernel's table of cell outflow Courant sums: rows j0-1 .. j0+TY, columns i0-1 .. i0+TX
+constexpr int CW = TX + 2, CN = (TY + 2) * CW;
 template <typename T>
 constexpr size_t scalar_smem() {
   return sizeof(T) * ((size_t)S_PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
-                      (size_t)(TY + 1) * TX);
+                      (size_t)(TY + 1) * TX + (size_t)2 * CN);
 }
 }  // namespace tiled
 
@@ -748,6 +762,18 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
   T th_hi = th[lin(s, kb, j, i)];
   cp_async_wait_all();
   __syncthreads();
+  // the viscous stresses of the level below (tau13, tau23 at kb-1 and tau33 at kb), carried up
+  // the column from then on
+  T tm13 = (T)0.0, tm23 = (T)0.0, t33 = (T)0.0;
+  if (s.use_vd) {
+    const CProf<T> P = cprof<T>(rP, kb);
+    const CRing<T> ZU = cring<T, RM>(rZU, kb, co, j, i), ZV = cring<T, RM>(rZV, kb, co, j, i),
+                   ZW = cring<T, RM>(rZW, kb, co, j, i), VIS = cring<T, RM>(rVIS, kb, co, j, i);
+    const Tau13<T> tm = tau_13_23<T>(s, P, ZU, ZV, ZW, VIS, kb - 1, j, i);
+    tm13 = tm.t13;
+    tm23 = tm.t23;
+    if (kb < nz) t33 = tau33_at<T>(s, P, ZW, VIS, kb, j, i);
+  }
   for (int k = kb; k <= ke; ++k) {
     if (k + 2 <= min(nz, ke + 1)) stage_level(k + 2);
     const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
@@ -764,7 +790,7 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
     pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
     if (s.use_vd) {
       T du, dv, dw;
-      viscosity_point<T>(s, P, ZU, ZV, ZW, ZU, VIS, k, j, i, du, dv, dw);
+      viscosity_core<T>(s, P, ZU, ZV, ZW, ZU, VIS, k, j, i, tm13, tm23, t33, du, dv, dw, tm13, tm23, t33);
       su = su + du;
       sv = sv + dv;
       if (k < nz) sw = sw + dw;
@@ -834,7 +860,17 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
   T* rP = rF + RZF * Gt::PLANE;  // profile ring
   T* FX = rP + RP * P_COUNT;     // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
   T* FY = FX + TY * (TX + 1);    // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
+  T* CT = FY + (TY + 1) * TX;    // [2][TY+2][TX+2]: cell_cfl_out of levels of parity 0 and 1
   const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  // Each face's limiter needs the outflow Courant sum of its upwind cell.  The sums of one level
+  // go into a table once (each thread its own cell, the first 2*CW + 2*TY threads one border cell
+  // each), one level ahead of the faces that read them.
+  const int own_cell = (ty + 1) * CW + tx + 1;
+  int hr = -1, hc = -1;
+  if (tid < CW) { hr = 0; hc = tid; }
+  else if (tid < 2 * CW) { hr = TY + 1; hc = tid - CW; }
+  else if (tid < 2 * CW + TY) { hr = tid - 2 * CW + 1; hc = 0; }
+  else if (tid < 2 * CW + 2 * TY) { hr = tid - 2 * CW - TY + 1; hc = TX + 1; }
   Stager<T> sg;
   sg.init(s, j0, i0, tid);
   // level k reads the scalar at k-1 .. k+2, u v w at k-1 .. k+1, diff at k-1 .. k and profiles
@@ -877,8 +913,18 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
                    W = cring<T, RF>(rW, kz, co, j, i);
     const CRing<T> ZF = cring<T, RZF>(rF, kz, co, j, i);
     fz_lo = tvd_face_z<T>(s, P, U, V, W, ZF, dt, kz, j, i);
-    __syncthreads();  // level kb-2 of the u, v, w rings is overwritten by the first prefetch
   }
+  {
+    // the cell sums of level kb
+    const CProf<T> P = cprof<T>(rP, kb);
+    const CRing<T> U = cring<T, RF>(rU, kb, co, j, i), V = cring<T, RF>(rV, kb, co, j, i),
+                   W = cring<T, RF>(rW, kb, co, j, i);
+    T* C = CT + (kb & 1) * CN;
+    C[own_cell] = cell_cfl_out<T>(s, P, U, V, W, kb, j, i);
+    if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T>(s, P, U, V, W, kb, j0 - 1 + hr, i0 - 1 + hc);
+  }
+  // the table is complete; level kb-2 of the u, v, w rings is overwritten by the first prefetch
+  __syncthreads();
   for (int k = kb; k <= ke; ++k) {
     if (k + 3 <= min(nz, ke + 2)) sg.template stage<RZF>(rF, job.zf, plane, k + 3);
     if (k + 2 <= min(nz, ke + 1)) {
@@ -895,15 +941,35 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     const CRing<T> U = cring<T, RF>(rU, k, co, j, i), V = cring<T, RF>(rV, k, co, j, i),
                    W = cring<T, RF>(rW, k, co, j, i), DIFF = cring<T, RF>(rD, k, co, j, i);
     const CRing<T> ZF = cring<T, RZF>(rF, k, co, j, i);
+    // the cell sums of level k+1: the own cell's for the z face above, the table for the next level
+    T c_hi = (T)0.0;
+    if (k < nz) {
+      c_hi = cell_cfl_out<T>(s, P, U, V, W, k + 1, j, i);
+      if (k + 1 <= ke) {
+        T* C = CT + ((k + 1) & 1) * CN;
+        C[own_cell] = c_hi;
+        if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T>(s, P, U, V, W, k + 1, j0 - 1 + hr, i0 - 1 + hc);
+      }
+    }
+    const T* Ck = CT + (k & 1) * CN;
+    auto cfl = [&](int kk, int jj, int ii) -> T { return kk == k ? Ck[(jj - j0 + 1) * CW + (ii - i0 + 1)] : c_hi; };
     // TVD faces of this level: own x+1/2 and y+1/2 faces, then the tile's low-side faces
-    FX[ty * (TX + 1) + tx + 1] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j, i);
-    FY[(ty + 1) * TX + tx] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j, i);
-    if (tid < TX) FY[tid] = tvd_face_y<T>(s, P, U, V, W, ZF, dt, k, j0 - 1, i0 + tid);
-    else if (tid < TX + TY) FX[(tid - TX) * (TX + 1)] = tvd_face_x<T>(s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1);
-    T fz_hi = (k < nz) ? tvd_face_z<T>(s, P, U, V, W, ZF, dt, k, j, i) : (T)0.0;
+    FX[ty * (TX + 1) + tx + 1] =
+        tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    FY[(ty + 1) * TX + tx] =
+        tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    if (tid < TX)
+      FY[tid] = tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j0 - 1,
+                                                                               i0 + tid, cfl);
+    else if (tid < TX + TY)
+      FX[(tid - TX) * (TX + 1)] = tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(
+          s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1, cfl);
+    T fz_hi = (k < nz) ? tvd_face_z_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl)
+                       : (T)0.0;
     __syncthreads();
     T sth = tvd_source<T>(s, P, U, V, W, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1], FY[ty * TX + tx],
                           FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
+    if (s.th_baroclinic && job.row == 2) sth = sth + th_baroclinic_point<T>(s, U, V, k, j, i);
     if (s.use_vd) sth = sth + diffusion_point<T>(s, P, ZF, DIFF, k, j, i);
     // damping, then forcing's subsidence (the dynamics group's order)
     if (s.damping && (job.row > 2 || !s.passive_th)) sth = damping_scalar_point<T>(s, P, k, ZF(k, j, i), job.row, sth);
@@ -1011,6 +1077,14 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_smag_tile
   }
   cp_async_wait_all();
   __syncthreads();
+  // the strain-rate parts of level k come from the level below, where they were level k+1's
+  StrainLevel<T> lo;
+  {
+    const CProf<T> P = cprof<T>(rP, kb);
+    const CRing<T> U = cring<T, RM>(rU, kb, co, j, i), V = cring<T, RM>(rV, kb, co, j, i),
+                   W = cring<T, RM>(rW, kb, co, j, i);
+    lo = strain_level<T>(s, P, U, V, W, kb, j, i);
+  }
   for (int k = kb; k <= ke; ++k) {
     if (k + 2 <= min(nz, ke + 1)) stage_level(k + 2);
     const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
@@ -1018,9 +1092,12 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_smag_tile
     const CProf<T> P = cprof<T>(rP, k);
     const CRing<T> U = cring<T, RM>(rU, k, co, j, i), V = cring<T, RM>(rV, k, co, j, i),
                    W = cring<T, RM>(rW, k, co, j, i);
+    const StrainLevel<T> hi = strain_level<T>(s, P, U, V, W, k + 1, j, i);
+    const T ssq = half_squared_strain_parts<T>(s, P, U, V, W, k, j, i, lo, hi);
+    lo = hi;
     T vis, diff;
-    smagorinsky_point<T>(s, P, U, V, W, THc, THa, moist ? &QV : (const View<T>*)nullptr,
-                         moist ? &QL : (const View<T>*)nullptr, k, j, i, vis, diff);
+    smagorinsky_from_strain<T>(s, P, ssq, THc, THa, moist ? &QV : (const View<T>*)nullptr,
+                               moist ? &QL : (const View<T>*)nullptr, k, j, i, vis, diff);
     const long long o = lin(s, k, j, i);
     d.vis[o] = vis;
     d.diff[o] = diff;
@@ -1137,6 +1214,10 @@ int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st,
     case MGPU_C_PW_ADVECTION: k_c_pw<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
     case MGPU_C_TVD_ADVECTION: k_c_tvd<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d, nullptr, nullptr, 0); break;
     case MGPU_C_DIFFUSION: k_c_diffusion<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
+    case MGPU_C_TH_ADVECTION:
+      if (s.th_baroclinic) k_c_th_advection<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d);
+      else nl = 0;
+      break;
     case MGPU_C_VISCOSITY: k_c_viscosity<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
     case MGPU_C_CORIOLIS: k_c_coriolis<T><<<pt_grid(s, s.nz - 1), b, 0, st>>>(s, d); break;
     case MGPU_C_BUOYANCY: k_c_buoyancy<T><<<pt_grid(s, s.nz - 2), b, 0, st>>>(s, d); break;
@@ -1184,9 +1265,7 @@ static inline int choose_level_chunks(int tiles, int slots, int levels) {
 // returns the number of kernels launched
 template <typename T>
 int launch_fused_subgrid(const Scalars& s, DevState<T>& d, cudaStream_t st) {
-  // measured on B200: the tiled Smagorinsky pays in FP32 (0.18 -> 0.13 ms at 256x256x128) but
-  // not in FP64, where the point kernel is as fast (0.20 ms), so FP64 keeps the point kernel
-  const bool tiled_ok = sizeof(T) == 4 && !s.point_dynamics && (s.nx % tiled::TX) == 0 &&
+  const bool tiled_ok = !s.point_dynamics && (s.nx % tiled::TX) == 0 &&
                         (s.ny % tiled::TY) == 0 && s.nz >= 4;
   if (!tiled_ok) {
     k_f_subgrid<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);

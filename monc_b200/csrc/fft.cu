@@ -15,6 +15,7 @@
 // Level 1 is transformed too: its non-mean modes pass through unchanged, its mean is zeroed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -351,6 +352,252 @@ __global__ void __launch_bounds__(line_block(LOGN)) k_fft_y(typename Cx<T>::t* _
   line_fft<C, LOGN, INV, false, false>(j, buf, tw, in, out);
 }
 
+// ---- lengths that are not powers of two: mixed-radix Stockham passes in shared memory ---------
+// MONC's FFTPACK factorises any length (cffti1.f90 tries 4, 2, 3, 5, then odd factors); the
+// lengths with prime factors 2, 3 and 5 only (96, 384, 100, 360, ...) take these kernels.  A line
+// of n points sits in shared memory (two buffers, ping-pong) and is transformed by the threads of
+// its block: pass p of radix R (4, 2, 3 or 5) and span NS forms, for j < n/R, the R points
+// x[j + r n/R], multiplies point r by W_{NS R}^{(j mod NS) r} = tw[(j mod NS) r n/(NS R)] (the
+// same table of W_n^q the power-of-two kernels use), applies the R-point DFT and stores point r
+// to y[(j/NS) NS R + j mod NS + r NS] -- the self-sorting form of the radix-16 passes above with
+// the radix varying from pass to pass, so the last pass leaves the result in natural order.
+struct GenFactors {
+  int n, npass;
+  int radix[16];
+};
+
+// factors of n in the order the passes use them (4s, then 2, 3s, 5s); false if n has another
+// prime factor or is out of range
+static bool gen_factor(int n, GenFactors& g) {
+  g.n = n;
+  g.npass = 0;
+  if (n < 2 || n > 4096) return false;
+  int m = n;
+  while (m % 4 == 0) { g.radix[g.npass++] = 4; m /= 4; }
+  while (m % 2 == 0) { g.radix[g.npass++] = 2; m /= 2; }
+  while (m % 3 == 0) { g.radix[g.npass++] = 3; m /= 3; }
+  while (m % 5 == 0) { g.radix[g.npass++] = 5; m /= 5; }
+  return m == 1 && g.npass <= 16;
+}
+
+// the R-point DFTs; forward uses W_R = e^{-2 pi i / R}, inverse its conjugate.  The constants are
+// cos and sin of 2 pi/3, 2 pi/5 and 4 pi/5 to 30 digits.
+template <typename C>
+__device__ __forceinline__ C cmul_i(C a, bool inv) {  // a * (-i) forward, a * (+i) inverse
+  C r;
+  if (inv) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+template <typename C, typename T>
+__device__ __forceinline__ C cscale(C a, T s) { C r; r.x = a.x * s; r.y = a.y * s; return r; }
+
+template <typename T, typename C>
+__device__ __forceinline__ void gen_dft(C* v, int R, bool inv) {
+  if (R == 2) {
+    const C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if (R == 4) {
+    const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]);
+    const C t3 = cmul_i(csub(v[1], v[3]), inv);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  } else if (R == 3) {
+    const T c = (T)-0.5;
+    const T sn = inv ? (T)0.866025403784438646763723170753 : (T)-0.866025403784438646763723170753;
+    const C t1 = cadd(v[1], v[2]);
+    const C t2 = cadd(v[0], cscale(t1, c));
+    const C d = cscale(csub(v[1], v[2]), sn);  // i * d is added to y1
+    C y1, y2;
+    y1.x = t2.x - d.y; y1.y = t2.y + d.x;
+    y2.x = t2.x + d.y; y2.y = t2.y - d.x;
+    v[0] = cadd(v[0], t1);
+    v[1] = y1;
+    v[2] = y2;
+  } else {  // R == 5
+    const T c1 = (T)0.309016994374947424102293417183, c2 = (T)-0.809016994374947424102293417183;
+    const T s1 = inv ? (T)0.951056516295153572116439333379 : (T)-0.951056516295153572116439333379;
+    const T s2 = inv ? (T)0.587785252292473129180916317273 : (T)-0.587785252292473129180916317273;
+    const C a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
+    const C b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
+    const C x0 = v[0];
+    const C r1 = cadd(x0, cadd(cscale(a1, c1), cscale(a2, c2)));
+    const C r2 = cadd(x0, cadd(cscale(a1, c2), cscale(a2, c1)));
+    const C q1 = cadd(cscale(b1, s1), cscale(b2, s2));   // y1 = r1 + i q1, y4 = r1 - i q1
+    const C q2 = csub(cscale(b1, s2), cscale(b2, s1));   // y2 = r2 + i q2, y3 = r2 - i q2
+    v[0] = cadd(x0, cadd(a1, a2));
+    v[1].x = r1.x - q1.y; v[1].y = r1.y + q1.x;
+    v[4].x = r1.x + q1.y; v[4].y = r1.y - q1.x;
+    v[2].x = r2.x - q2.y; v[2].y = r2.y + q2.x;
+    v[3].x = r2.x + q2.y; v[3].y = r2.y - q2.x;
+  }
+}
+
+// Transform `nl` lines of n points held at a + l*n (l < nl) in shared memory; b is scratch of the
+// same size.  Returns the buffer holding the result.  All threads of the block take part.
+template <typename T, bool INV>
+__device__ typename Cx<T>::t* gen_lines_fft(typename Cx<T>::t* a, typename Cx<T>::t* b, int nl, const GenFactors& g,
+                                            const typename Cx<T>::t* __restrict__ tw) {
+  typedef typename Cx<T>::t C;
+  const int n = g.n;
+  int ns = 1;
+  for (int p = 0; p < g.npass; ++p) {
+    const int R = g.radix[p], nb = n / R, step = n / (ns * R);
+    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
+      const int l = t / nb, j = t - l * nb;
+      const C* x = a + l * n;
+      C* y = b + l * n;
+      const int jm = j % ns;
+      C v[5];
+      for (int r = 0; r < R; ++r) {
+        C z = x[j + r * nb];
+        if (r > 0 && jm > 0) {
+          C w = tw[jm * r * step];
+          if (INV) w.y = -w.y;
+          z = cmul(z, w);
+        }
+        v[r] = z;
+      }
+      gen_dft<T, C>(v, R, INV);
+      const int o = (j / ns) * ns * R + jm;
+      for (int r = 0; r < R; ++r) y[o + r * ns] = v[r];
+    }
+    __syncthreads();
+    C* tmp = a; a = b; b = tmp;
+    ns *= R;
+  }
+  return a;
+}
+
+constexpr int GEN_BLOCK = 128;
+
+// forward x of generic length: one block per row pair, packed, transformed and split as
+// k_fft_x_fwd does it
+template <typename T>
+__global__ void __launch_bounds__(GEN_BLOCK) k_fftg_x_fwd(const T* __restrict__ p, typename Cx<T>::t* __restrict__ spec,
+                                                          const typename Cx<T>::t* __restrict__ tw, GenFactors g, int ny,
+                                                          int nz, int p_rows, int p_row0, int nblk) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = g.n, nxh = n / 2 + 1, pairs = ny / 2;
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + n;
+  const int pr = blockIdx.x;
+  const int k = pr / pairs + 1, jr = 2 * (pr % pairs);
+  const T* row = p + ((long long)(k - 1) * p_rows + p_row0 + jr) * n;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    C z;
+    z.x = row[e];
+    z.y = row[n + e];
+    a[e] = z;
+  }
+  __syncthreads();
+  const C* zt = gen_lines_fft<T, false>(a, b, 1, g, tw);
+  for (int m = threadIdx.x; m < nxh; m += blockDim.x) {
+    const C zm = zt[m];
+    const C zn = zt[(n - m) % n];
+    C ra, rb;
+    ra.x = (T)0.5 * (zm.x + zn.x);
+    ra.y = (T)0.5 * (zm.y - zn.y);
+    rb.x = (T)0.5 * (zm.y + zn.y);
+    rb.y = (T)0.5 * (zn.x - zm.x);
+    int w;
+    C* o = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, jr, &w);
+    o[0] = ra;
+    o[w] = rb;
+  }
+}
+
+// inverse x of generic length, the inverse of k_fftg_x_fwd (imaginary parts of kx = 0 and, for
+// even n, kx = n/2 dropped)
+template <typename T>
+__global__ void __launch_bounds__(GEN_BLOCK) k_fftg_x_inv(T* __restrict__ p, const typename Cx<T>::t* __restrict__ spec,
+                                                          const typename Cx<T>::t* __restrict__ tw, GenFactors g, int ny,
+                                                          int nz, int p_rows, int p_row0, int nblk) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = g.n, nxh = n / 2 + 1, pairs = ny / 2;
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + n;
+  const int pr = blockIdx.x;
+  const int k = pr / pairs + 1, jr = 2 * (pr % pairs);
+  for (int m = threadIdx.x; m < nxh; m += blockDim.x) {
+    int w;
+    const C* in = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, jr, &w);
+    C ra = in[0], rb = in[w];
+    const bool nyquist = 2 * m == n;
+    if (m == 0 || nyquist) { ra.y = (T)0; rb.y = (T)0; }
+    C z;
+    z.x = ra.x - rb.y;
+    z.y = ra.y + rb.x;
+    a[m] = z;
+    if (m > 0 && !nyquist) {
+      C zc;
+      zc.x = ra.x + rb.y;
+      zc.y = rb.x - ra.y;
+      a[n - m] = zc;
+    }
+  }
+  __syncthreads();
+  const C* zt = gen_lines_fft<T, true>(a, b, 1, g, tw);
+  T* row = p + ((long long)(k - 1) * p_rows + p_row0 + jr) * n;
+  const T sc = (T)(1.0 / (double)n);
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    row[e] = zt[e].x * sc;
+    row[n + e] = zt[e].y * sc;
+  }
+}
+
+// columns per block of the generic y kernel: as many as keep the two buffers within 64 KB of
+// FP64 lines (at least one)
+static int gen_y_cols(int n) { return std::max(1, std::min(8, 2048 / n)); }
+
+// y of generic length on a tile of kx columns of one level, the layout of k_fft_y; the inverse
+// is scaled by 1/n
+template <typename T, bool INV>
+__global__ void __launch_bounds__(GEN_BLOCK) k_fftg_y(typename Cx<T>::t* __restrict__ spec,
+                                                      const typename Cx<T>::t* __restrict__ tw, GenFactors g, int ncols,
+                                                      int nz, int rpb, int tc) {
+  typedef typename Cx<T>::t C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = g.n;
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + (size_t)tc * n;
+  const int kx0 = blockIdx.x * tc, k = blockIdx.y + 1;
+  const int nc = min(tc, ncols - kx0);
+  for (int t = threadIdx.x; t < nc * n; t += blockDim.x) {
+    const int e = t / nc, c = t - e * nc;  // consecutive threads take consecutive columns
+    a[c * n + e] = spec[spec_row(e, k, rpb, ncols, nz) + kx0 + c];
+  }
+  __syncthreads();
+  const C* zt = gen_lines_fft<T, INV>(a, b, nc, g, tw);
+  const T sc = INV ? (T)(1.0 / (double)n) : (T)1.0;
+  for (int t = threadIdx.x; t < nc * n; t += blockDim.x) {
+    const int e = t / nc, c = t - e * nc;
+    C z = zt[c * n + e];
+    if (INV) { z.x = z.x * sc; z.y = z.y * sc; }
+    spec[spec_row(e, k, rpb, ncols, nz) + kx0 + c] = z;
+  }
+}
+
+template <typename T>
+static void ensure_gen_attr() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  const int mx = (int)(2 * 4096 * sizeof(typename Cx<T>::t));
+  cudaFuncSetAttribute(k_fftg_x_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_fftg_x_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_fftg_y<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_fftg_y<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  done[dev] = true;
+}
+
 // ---- launches: one kernel instantiation per transform length (4 .. 4096 points) ----------------
 template <typename T>
 static size_t line_smem(int logn) {
@@ -379,10 +626,23 @@ static void ensure_line_attr() {
   done[dev] = true;
 }
 
-// x-FFT of `pairs_total` row pairs (nz levels of ny rows), forward or inverse
+static bool is_pow2(int n) { return n >= 4 && n <= 4096 && (n & (n - 1)) == 0; }
+
+// x-FFT of the nz * ny/2 row pairs of length n, forward or inverse
 template <typename T>
-static void launch_fft_x(bool inverse, int logn, T* p, typename Cx<T>::t* spec, const typename Cx<T>::t* tw, int ny,
+static void launch_fft_x(bool inverse, int n, T* p, typename Cx<T>::t* spec, const typename Cx<T>::t* tw, int ny,
                          int nz, int p_rows, int p_row0, int nblk, cudaStream_t st) {
+  if (!is_pow2(n)) {
+    GenFactors g;
+    if (!gen_factor(n, g)) return;
+    ensure_gen_attr<T>();
+    const unsigned grid = (unsigned)((long long)nz * (ny / 2));
+    const size_t smem = 2 * (size_t)n * sizeof(typename Cx<T>::t);
+    if (inverse) k_fftg_x_inv<T><<<grid, GEN_BLOCK, smem, st>>>(p, spec, tw, g, ny, nz, p_rows, p_row0, nblk);
+    else k_fftg_x_fwd<T><<<grid, GEN_BLOCK, smem, st>>>(p, spec, tw, g, ny, nz, p_rows, p_row0, nblk);
+    return;
+  }
+  const int logn = ilog2(n);
   ensure_line_attr<T>();
   const long long pairs = (long long)nz * (ny / 2);
   const int L = line_lines(logn);
@@ -401,10 +661,22 @@ static void launch_fft_x(bool inverse, int logn, T* p, typename Cx<T>::t* spec, 
   }
 }
 
-// y-FFT of ncols columns of 2^logn rows on each of nz levels (rows in blocks of rpb)
+// y-FFT of ncols columns of n rows on each of nz levels (rows in blocks of rpb)
 template <typename T>
-static void launch_fft_y(bool inverse, int logn, typename Cx<T>::t* spec, const typename Cx<T>::t* tw, int ncols, int nz,
+static void launch_fft_y(bool inverse, int n, typename Cx<T>::t* spec, const typename Cx<T>::t* tw, int ncols, int nz,
                          int rpb, cudaStream_t st) {
+  if (!is_pow2(n)) {
+    GenFactors g;
+    if (!gen_factor(n, g)) return;
+    ensure_gen_attr<T>();
+    const int tc = gen_y_cols(n);
+    dim3 grid((unsigned)((ncols + tc - 1) / tc), (unsigned)nz);
+    const size_t smem = 2 * (size_t)tc * n * sizeof(typename Cx<T>::t);
+    if (inverse) k_fftg_y<T, true><<<grid, GEN_BLOCK, smem, st>>>(spec, tw, g, ncols, nz, rpb, tc);
+    else k_fftg_y<T, false><<<grid, GEN_BLOCK, smem, st>>>(spec, tw, g, ncols, nz, rpb, tc);
+    return;
+  }
+  const int logn = ilog2(n);
   ensure_line_attr<T>();
   const int cols = line_lines(logn);
   dim3 grid((unsigned)((ncols + cols - 1) / cols), (unsigned)nz);
@@ -680,13 +952,18 @@ static int plan_tables(FftPlanDev& pl, const RefState& rs) {
   return cudaGetLastError() == cudaSuccess ? MGPU_OK : MGPU_ERR_CUDA;
 }
 
+// Horizontal transform lengths the solve supports: 4 .. 4096 points with prime factors 2, 3, 5
+bool fft_length_ok(int n) {
+  GenFactors g;
+  return n >= 4 && gen_factor(n, g);
+}
+
 int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool fp32) {
   pl.nx = s.nx;
   pl.ny = s.ny;
   pl.nz = s.nz;
   pl.nxh = s.nx / 2 + 1;
-  auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
-  if (!pow2(s.nx) || !pow2(s.ny) || s.nx > 4096 || s.ny > 4096) return MGPU_ERR_UNSUPPORTED;
+  if (!fft_length_ok(s.nx) || !fft_length_ok(s.ny) || (s.ny % 2)) return MGPU_ERR_UNSUPPORTED;
   const size_t plane = (size_t)s.ny * pl.nxh;
   const size_t cs = fp32 ? sizeof(float2) : sizeof(double2);
   if (cudaMalloc(&pl.spec, cs * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
@@ -699,8 +976,7 @@ int fft_slab_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, i
   pl.ny = ny_global;
   pl.nz = s.nz;
   pl.nxh = s.nx / 2 + 1;
-  auto pow2 = [](int n) { return n >= 4 && (n & (n - 1)) == 0; };
-  if (!pow2(s.nx) || !pow2(ny_global) || s.nx > 4096 || ny_global > 4096 || max_cols < 1 || max_cols > pl.nxh)
+  if (!fft_length_ok(s.nx) || !fft_length_ok(ny_global) || max_cols < 1 || max_cols > pl.nxh)
     return MGPU_ERR_UNSUPPORTED;
   if (cudaMalloc(&pl.s1, sizeof(double2) * (size_t)ny_global * max_cols * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
   return plan_tables(pl, rs);
@@ -725,7 +1001,7 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   C* spec = reinterpret_cast<C*>(pl.spec);
   const C* twx = reinterpret_cast<const C*>(f32 ? (void*)pl.twx_f : (void*)pl.twx);
   const C* twy = reinterpret_cast<const C*>(f32 ? (void*)pl.twy_f : (void*)pl.twy);
-  const int logx = ilog2(s.nx), logy = ilog2(s.ny);
+  const int logx = s.nx, logy = s.ny;  // transform lengths
   const size_t plane = (size_t)s.ny * pl.nxh;
   double2* s1 = pl.s1;
   auto mark = [&](int q) { if (evs) cudaEventRecord(evs[q], st); };
@@ -758,7 +1034,7 @@ void slab_fft_x(const FftPlanDev& pl, const Scalars& s, T* p, int halo, int nblk
   const C* twx = reinterpret_cast<const C*>(f32 ? (void*)pl.twx_f : (void*)pl.twx);
   C* sp = reinterpret_cast<C*>(spec);
   const int nyl = s.ny - 2 * halo;
-  launch_fft_x<T>(inverse, ilog2(s.nx), p, sp, twx, nyl, s.nz, s.ny, halo, nblk, st);
+  launch_fft_x<T>(inverse, s.nx, p, sp, twx, nyl, s.nz, s.ny, halo, nblk, st);
   *launches += 1;
 }
 
@@ -769,7 +1045,7 @@ void slab_solve_columns(const FftPlanDev& pl, const Scalars& s, void* spec, int 
   const bool f32 = sizeof(T) == 4;
   const C* twy = reinterpret_cast<const C*>(f32 ? (void*)pl.twy_f : (void*)pl.twy);
   C* sp = reinterpret_cast<C*>(spec);
-  const int logy = ilog2(pl.ny);
+  const int logy = pl.ny;  // transform length
   const long long ncol = (long long)pl.ny * nkx;
   launch_fft_y<T>(false, logy, sp, twy, nkx, s.nz, rpb, st);
   ensure_tri_attr();
@@ -997,13 +1273,13 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   k_noalloc_twiddles<<<(ny + 127) / 128, 128, 0, st>>>(twy, ny);
   k_noalloc_pivots<<<(nyh * nxh + 127) / 128, 128, 0, st>>>(b1, prof, stride, nx, ny, nz, dx, dy);
   // the five solve kernels of fft_solve, on the scratch buffers
-  launch_fft_x<double>(false, ilog2(nx), p, spec, twx, ny, nz, ny, 0, 1, st);
-  launch_fft_y<double>(false, ilog2(ny), spec, twy, nxh, nz, ny, st);
+  launch_fft_x<double>(false, nx, p, spec, twx, ny, nz, ny, 0, 1, st);
+  launch_fft_y<double>(false, ny, spec, twy, nxh, nz, ny, st);
   ensure_tri_attr();
   k_tridiag<double><<<(unsigned)((plane + TRI_TB - 1) / TRI_TB + 1), TRI_TB, tri_smem_bytes<double2>(nz), st>>>(
       spec, s1, b1, prof, stride, nx, ny, nz, 0, nxh, 0, ny);
-  launch_fft_y<double>(true, ilog2(ny), spec, twy, nxh, nz, ny, st);
-  launch_fft_x<double>(true, ilog2(nx), p, spec, twx, ny, nz, ny, 0, 1, st);
+  launch_fft_y<double>(true, ny, spec, twy, nxh, nz, ny, st);
+  launch_fft_x<double>(true, nx, p, spec, twx, ny, nz, ny, 0, 1, st);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     std::fprintf(stderr, "mgpu_poisson_fft_noalloc: kernel launch failed: %s\n", cudaGetErrorString(e));

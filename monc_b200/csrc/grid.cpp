@@ -242,9 +242,14 @@ void build_reference_state(const mgpu_config& c, RefState& rs) {
   rs.cy2 = rs.cy * rs.cy;
   rs.tcx = 0.25 / rs.dx;
   rs.tcy = 0.25 / rs.dy;
+  // geostrophic wind profile (coriolis.F90:155-163), growing with height under the shear
   for (int k = 1; k <= n; ++k) {
     rs.gwx[k] = c.surface_geostrophic_wind_x;
     rs.gwy[k] = c.surface_geostrophic_wind_y;
+    if (c.baroclinicity_use_geostrophic_shear) {
+      rs.gwx[k] = rs.gwx[k] + c.geostrophic_wind_rate_of_change_in_x * rs.zn[k];
+      rs.gwy[k] = rs.gwy[k] + c.geostrophic_wind_rate_of_change_in_y * rs.zn[k];
+    }
   }
   // water loading coefficient of the vapour field (setfluxlook.F90:70-76)
   rs.cq.assign(std::max(c.number_q_fields, 1), 0.0);
@@ -350,7 +355,8 @@ const std::vector<double>* profile_by_name(const RefState& rs, const std::string
                        {"buoy_co", &rs.buoy_co}, {"prefn", &rs.prefn}, {"prefrcp", &rs.prefrcp},
                        {"rprefrcp", &rs.rprefrcp}, {"tref", &rs.tref}, {"qsat", &rs.qsat},
                        {"dqsatdt", &rs.dqsatdt}, {"qsatfac", &rs.qsatfac}, {"dmpco", &rs.dmpco},
-                       {"dmpcoz", &rs.dmpcoz}, {"w_subs", &rs.w_subs}};
+                       {"dmpcoz", &rs.dmpcoz}, {"w_subs", &rs.w_subs}, {"geostrophic_wind_x", &rs.gwx},
+                       {"geostrophic_wind_y", &rs.gwy}};
   for (const Entry& e : tab)
     if (nm == e.name) return e.v;
   return nullptr;

@@ -92,6 +92,10 @@ struct Scalars {
   // filter of the pressure-terms group read.  Equal to ugal, vgal outside cfltest evaluations.
   int galilean;
   double ugal_p, vgal_p;
+  // th_advection's advection of the mean baroclinicity (thadvection.F90:196-216, Boussinesq form):
+  // sth += (v + vgal) mfx - (u + ugal) mfy at levels 2..nz
+  int th_baroclinic;
+  double mfx, mfy;
 };
 
 }  // namespace mgpu

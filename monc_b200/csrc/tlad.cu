@@ -479,6 +479,62 @@ void adj_lower_bc(const Scalars& s, const DevState<double>& d, double* const* tg
   tlad::k_adj_subgrid<<<grid, ad_block(), 0, st>>>(s, a);
 }
 
+// ---- branch decisions of two states (a gradient-check diagnostic) -------------------------
+// For every point: the branch codes of the theta TVD faces x+1/2, y+1/2 and z+1/2 (upwind side,
+// the smooth-region early return, the limiter's choice among fncs, fnfs, fnrefs and 1, the signs
+// that pick the gradient-term stencils) and the Smagorinsky regime of the dry Richardson number
+// (ri <= 0, 0 < ri < ric, ri >= ric), evaluated on the state each model would step next.  The
+// kernel counts the decisions that differ between the two models.
+__device__ __forceinline__ unsigned smag_regime(const Scalars& s, const Prof<double>& P, const View<double>& U,
+                                                const View<double>& V, const View<double>& W, const View<double>& TH,
+                                                int k, int j, int i) {
+  const double ssq = half_squared_strain<double>(s, P, U, V, W, k, j, i);
+  const double ri = (P(P_DTHREF, k) + TH(k + 1, j, i) - TH(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k) / ssq;
+  return ri <= 0.0 ? 0u : (ri < s.ric ? 1u : 2u);
+}
+
+__global__ void k_branch_flips(Scalars s, DevState<double> a, DevState<double> b, unsigned long long* count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z + 2;
+  unsigned n = 0;
+  if (i < s.nx && j < s.ny && k <= s.nz) {
+    const Geo g{s.nx, s.ny, s.nz, s.plane};
+    Prof<double> P;
+    P.base = s.prof;
+    P.stride = s.nz + 2;
+    const double dt = s.dtm * 2.0;
+    unsigned code[2][4];
+    const DevState<double>* st[2] = {&a, &b};
+    for (int q = 0; q < 2; ++q) {
+      const DevState<double>& d = *st[q];
+      const View<double> U{d.u, g}, V{d.v, g}, W{d.w, g}, ZF{s.forward ? d.th : d.zth, g};
+      const CflInline<double, View<double>, Prof<double>, TvdMetricScalar> cfl{s, P, U, V, W};
+      for (int c = 0; c < 4; ++c) code[q][c] = 0;
+      tvd_face_x_g<double, View<double>, View<double>, Prof<double>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i,
+                                                                                     cfl, BitRec{&code[q][0]});
+      tvd_face_y_g<double, View<double>, View<double>, Prof<double>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i,
+                                                                                     cfl, BitRec{&code[q][1]});
+      if (k < s.nz) {
+        tvd_face_z_g<double, View<double>, View<double>, Prof<double>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i,
+                                                                                       cfl, BitRec{&code[q][2]});
+        const View<double> SU{s.forward ? d.u : d.zu, g}, SV{s.forward ? d.v : d.zv, g}, SW{s.forward ? d.w : d.zw, g};
+        code[q][3] = smag_regime(s, P, SU, SV, SW, View<double>{d.th, g}, k, j, i);
+      }
+    }
+    for (int c = 0; c < 4; ++c) n += code[0][c] != code[1][c] ? 1u : 0u;
+  }
+  // one atomic per warp
+  for (int off = 16; off > 0; off >>= 1) n += __shfl_down_sync(0xffffffffu, n, off);
+  if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, (unsigned long long)n);
+}
+
+void branch_flips(const Scalars& s, const DevState<double>& a, const DevState<double>& b, unsigned long long* count,
+                  cudaStream_t st) {
+  dim3 block(32, 4, 1), grid((s.nx + 31) / 32, (s.ny + 3) / 4, s.nz - 1);
+  k_branch_flips<<<grid, block, 0, st>>>(s, a, b, count);
+}
+
 void tl_pass(int pass, const Scalars& s, const DevState<double>& d, const DevState<double>& t, const double* drsq,
              double dpar, cudaStream_t st) {
   tlad::TlArgs a{d, t, drsq, dpar};

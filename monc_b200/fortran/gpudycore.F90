@@ -90,6 +90,10 @@ module gpudycore_mod
     integer(c_int32_t) :: galilean_transformation
     integer(c_int32_t) :: fix_ugal, fix_vgal
     real(c_double)     :: ugal, vgal
+    integer(c_int32_t) :: th_advection_enabled
+    integer(c_int32_t) :: baroclinicity_use_geostrophic_shear
+    real(c_double)     :: rate_change_geostrophic_wind_x, rate_change_geostrophic_wind_y
+    real(c_double)     :: geostrophic_wind_rate_of_change_in_x, geostrophic_wind_rate_of_change_in_y
   end type mgpu_config
 
   !> mgpu_reductions of include/monc_gpu.h
@@ -263,6 +267,15 @@ contains
     cfg%fix_vgal = logical_flag(options_get_logical(current_state%options_database, "fix_vgal"))
     cfg%ugal = options_get_real(current_state%options_database, "ugal")
     cfg%vgal = options_get_real(current_state%options_database, "vgal")
+    cfg%th_advection_enabled = logical_flag(options_get_logical(current_state%options_database, "th_advection_enabled"))
+    cfg%baroclinicity_use_geostrophic_shear = logical_flag(options_get_logical(current_state%options_database, &
+         "baroclinicity_use_geostrophic_shear"))
+    cfg%rate_change_geostrophic_wind_x = options_get_real(current_state%options_database, "rate_change_geostrophic_wind_x")
+    cfg%rate_change_geostrophic_wind_y = options_get_real(current_state%options_database, "rate_change_geostrophic_wind_y")
+    cfg%geostrophic_wind_rate_of_change_in_x = options_get_real(current_state%options_database, &
+         "geostrophic_wind_rate_of_change_in_x")
+    cfg%geostrophic_wind_rate_of_change_in_y = options_get_real(current_state%options_database, &
+         "geostrophic_wind_rate_of_change_in_y")
 
     call check(mgpu_create(cfg, handle), "mgpu_create")
     call upload_state(current_state)

@@ -3,10 +3,11 @@
 //   components/fftsolver/src/fftpack/cffti1.f90  (factorisation into 4,2 and twiddle table)
 //   components/fftsolver/src/fftpack/cfftf1.f90  (forward driver, ping-pong between c and ch)
 //   components/fftsolver/src/fftpack/cfftb1.f90  (backward driver)
-//   components/fftsolver/src/fftpack/passf2.f90, passf4.f90, passb2.f90, passb4.f90
+//   components/fftsolver/src/fftpack/passf2.f90, passf3.f90, passf4.f90, passf5.f90 and the
+//   passb counterparts
 // and the wrappers components/fftsolver/src/fftnorth.F90:17-80 (fftn_r2c / fftn_c2r).
-// Only radix 2 and 4 passes are restated: every horizontal size this oracle runs is a power
-// of two; other factors are rejected by fft_plan_init.
+// The radix 2, 3, 4 and 5 passes are restated; lengths with another prime factor (FFTPACK's
+// general passf.f90) are rejected by fft_plan_init.
 #include "oracle_internal.h"
 
 #include <cmath>
@@ -49,8 +50,8 @@ void fft_plan_init(FftPlan& plan, int n) {
   ifac[2] = nf;
   for (int k1 = 1; k1 <= nf; ++k1) {
     int ip = ifac[k1 + 2];
-    if (ip != 2 && ip != 4)
-      throw std::runtime_error("oracle FFT supports power-of-two lengths only");
+    if (ip != 2 && ip != 3 && ip != 4 && ip != 5)
+      throw std::runtime_error("oracle FFT supports lengths with prime factors 2, 3 and 5 only");
   }
   const double tpi = 2.0 * std::acos(-1.0);
   const double argh = tpi / (double)n;
@@ -186,6 +187,151 @@ static void pass4(int ido, int l1, const double* cc_, double* ch_, const double*
 #undef WA3
 }
 
+// passf3.f90 / passb3.f90
+static void pass3(int ido, int l1, const double* cc_, double* ch_, const double* wa1_, const double* wa2_, int sign) {
+#define CC(i, j, k) cc_[((i) - 1) + ido * (((j) - 1) + 3 * ((k) - 1))]
+#define CH(i, k, j) ch_[((i) - 1) + ido * (((k) - 1) + l1 * ((j) - 1))]
+#define WA1(i) wa1_[(i) - 1]
+#define WA2(i) wa2_[(i) - 1]
+  const double taur = -0.5;
+  const double taui = (sign < 0) ? -std::sqrt(3.0) / 2.0 : std::sqrt(3.0) / 2.0;
+  if (ido != 2) {
+    for (int k = 1; k <= l1; ++k)
+      for (int i = 2; i <= ido; i += 2) {
+        double tr2 = CC(i - 1, 2, k) + CC(i - 1, 3, k);
+        double cr2 = CC(i - 1, 1, k) + taur * tr2;
+        CH(i - 1, k, 1) = CC(i - 1, 1, k) + tr2;
+        double ti2 = CC(i, 2, k) + CC(i, 3, k);
+        double ci2 = CC(i, 1, k) + taur * ti2;
+        CH(i, k, 1) = CC(i, 1, k) + ti2;
+        double cr3 = taui * (CC(i - 1, 2, k) - CC(i - 1, 3, k));
+        double ci3 = taui * (CC(i, 2, k) - CC(i, 3, k));
+        double dr2 = cr2 - ci3;
+        double dr3 = cr2 + ci3;
+        double di2 = ci2 + cr3;
+        double di3 = ci2 - cr3;
+        if (sign < 0) {
+          CH(i, k, 2) = WA1(i - 1) * di2 - WA1(i) * dr2;
+          CH(i - 1, k, 2) = WA1(i - 1) * dr2 + WA1(i) * di2;
+          CH(i, k, 3) = WA2(i - 1) * di3 - WA2(i) * dr3;
+          CH(i - 1, k, 3) = WA2(i - 1) * dr3 + WA2(i) * di3;
+        } else {
+          CH(i, k, 2) = WA1(i - 1) * di2 + WA1(i) * dr2;
+          CH(i - 1, k, 2) = WA1(i - 1) * dr2 - WA1(i) * di2;
+          CH(i, k, 3) = WA2(i - 1) * di3 + WA2(i) * dr3;
+          CH(i - 1, k, 3) = WA2(i - 1) * dr3 - WA2(i) * di3;
+        }
+      }
+  } else {
+    for (int k = 1; k <= l1; ++k) {
+      double tr2 = CC(1, 2, k) + CC(1, 3, k);
+      double cr2 = CC(1, 1, k) + taur * tr2;
+      CH(1, k, 1) = CC(1, 1, k) + tr2;
+      double ti2 = CC(2, 2, k) + CC(2, 3, k);
+      double ci2 = CC(2, 1, k) + taur * ti2;
+      CH(2, k, 1) = CC(2, 1, k) + ti2;
+      double cr3 = taui * (CC(1, 2, k) - CC(1, 3, k));
+      double ci3 = taui * (CC(2, 2, k) - CC(2, 3, k));
+      CH(1, k, 2) = cr2 - ci3;
+      CH(1, k, 3) = cr2 + ci3;
+      CH(2, k, 2) = ci2 + cr3;
+      CH(2, k, 3) = ci2 - cr3;
+    }
+  }
+#undef CC
+#undef CH
+#undef WA1
+#undef WA2
+}
+
+// passf5.f90 / passb5.f90
+static void pass5(int ido, int l1, const double* cc_, double* ch_, const double* wa1_, const double* wa2_,
+                  const double* wa3_, const double* wa4_, int sign) {
+#define CC(i, j, k) cc_[((i) - 1) + ido * (((j) - 1) + 5 * ((k) - 1))]
+#define CH(i, k, j) ch_[((i) - 1) + ido * (((k) - 1) + l1 * ((j) - 1))]
+  const double pi = std::acos(-1.0);
+  const double tr11 = std::cos(2.0 * pi / 5.0);
+  const double ti11 = (sign < 0 ? -1.0 : 1.0) * std::sin(2.0 * pi / 5.0);
+  const double tr12 = std::cos(4.0 * pi / 5.0);
+  const double ti12 = (sign < 0 ? -1.0 : 1.0) * std::sin(4.0 * pi / 5.0);
+  // the twiddle products of one output pair: passf5's w*d forward, passb5's conj(w)*d backward
+  auto put = [&](int i, int k, int j, const double* wa, double dr, double di) {
+    if (sign < 0) {
+      CH(i - 1, k, j) = wa[(i - 1) - 1] * dr + wa[i - 1] * di;
+      CH(i, k, j) = wa[(i - 1) - 1] * di - wa[i - 1] * dr;
+    } else {
+      CH(i - 1, k, j) = wa[(i - 1) - 1] * dr - wa[i - 1] * di;
+      CH(i, k, j) = wa[(i - 1) - 1] * di + wa[i - 1] * dr;
+    }
+  };
+  if (ido != 2) {
+    for (int k = 1; k <= l1; ++k)
+      for (int i = 2; i <= ido; i += 2) {
+        double ti5 = CC(i, 2, k) - CC(i, 5, k);
+        double ti2 = CC(i, 2, k) + CC(i, 5, k);
+        double ti4 = CC(i, 3, k) - CC(i, 4, k);
+        double ti3 = CC(i, 3, k) + CC(i, 4, k);
+        double tr5 = CC(i - 1, 2, k) - CC(i - 1, 5, k);
+        double tr2 = CC(i - 1, 2, k) + CC(i - 1, 5, k);
+        double tr4 = CC(i - 1, 3, k) - CC(i - 1, 4, k);
+        double tr3 = CC(i - 1, 3, k) + CC(i - 1, 4, k);
+        CH(i - 1, k, 1) = CC(i - 1, 1, k) + tr2 + tr3;
+        CH(i, k, 1) = CC(i, 1, k) + ti2 + ti3;
+        double cr2 = CC(i - 1, 1, k) + tr11 * tr2 + tr12 * tr3;
+        double ci2 = CC(i, 1, k) + tr11 * ti2 + tr12 * ti3;
+        double cr3 = CC(i - 1, 1, k) + tr12 * tr2 + tr11 * tr3;
+        double ci3 = CC(i, 1, k) + tr12 * ti2 + tr11 * ti3;
+        double cr5 = ti11 * tr5 + ti12 * tr4;
+        double ci5 = ti11 * ti5 + ti12 * ti4;
+        double cr4 = ti12 * tr5 - ti11 * tr4;
+        double ci4 = ti12 * ti5 - ti11 * ti4;
+        double dr3 = cr3 - ci4;
+        double dr4 = cr3 + ci4;
+        double di3 = ci3 + cr4;
+        double di4 = ci3 - cr4;
+        double dr5 = cr2 + ci5;
+        double dr2 = cr2 - ci5;
+        double di5 = ci2 - cr5;
+        double di2 = ci2 + cr5;
+        put(i, k, 2, wa1_, dr2, di2);
+        put(i, k, 3, wa2_, dr3, di3);
+        put(i, k, 4, wa3_, dr4, di4);
+        put(i, k, 5, wa4_, dr5, di5);
+      }
+  } else {
+    for (int k = 1; k <= l1; ++k) {
+      double ti5 = CC(2, 2, k) - CC(2, 5, k);
+      double ti2 = CC(2, 2, k) + CC(2, 5, k);
+      double ti4 = CC(2, 3, k) - CC(2, 4, k);
+      double ti3 = CC(2, 3, k) + CC(2, 4, k);
+      double tr5 = CC(1, 2, k) - CC(1, 5, k);
+      double tr2 = CC(1, 2, k) + CC(1, 5, k);
+      double tr4 = CC(1, 3, k) - CC(1, 4, k);
+      double tr3 = CC(1, 3, k) + CC(1, 4, k);
+      CH(1, k, 1) = CC(1, 1, k) + tr2 + tr3;
+      CH(2, k, 1) = CC(2, 1, k) + ti2 + ti3;
+      double cr2 = CC(1, 1, k) + tr11 * tr2 + tr12 * tr3;
+      double ci2 = CC(2, 1, k) + tr11 * ti2 + tr12 * ti3;
+      double cr3 = CC(1, 1, k) + tr12 * tr2 + tr11 * tr3;
+      double ci3 = CC(2, 1, k) + tr12 * ti2 + tr11 * ti3;
+      double cr5 = ti11 * tr5 + ti12 * tr4;
+      double ci5 = ti11 * ti5 + ti12 * ti4;
+      double cr4 = ti12 * tr5 - ti11 * tr4;
+      double ci4 = ti12 * ti5 - ti11 * ti4;
+      CH(1, k, 2) = cr2 - ci5;
+      CH(1, k, 5) = cr2 + ci5;
+      CH(2, k, 2) = ci2 + cr5;
+      CH(2, k, 3) = ci3 + cr4;
+      CH(1, k, 3) = cr3 - ci4;
+      CH(1, k, 4) = cr3 + ci4;
+      CH(2, k, 4) = ci3 - cr4;
+      CH(2, k, 5) = ci2 - cr5;
+    }
+  }
+#undef CC
+#undef CH
+}
+
 // cfftf1.f90 / cfftb1.f90: apply the passes, ping-ponging between c and ch.
 static void cfft1(const FftPlan& plan, double* c, double* ch, int sign) {
   const int n = plan.n;
@@ -203,9 +349,19 @@ static void cfft1(const FftPlan& plan, double* c, double* ch, int sign) {
       if (na != 0) pass4(idot, l1, ch, c, &wa[iw], &wa[ix2], &wa[ix3], sign);
       else pass4(idot, l1, c, ch, &wa[iw], &wa[ix2], &wa[ix3], sign);
       na = 1 - na;
-    } else {  // ip == 2
+    } else if (ip == 2) {
       if (na != 0) pass2(idot, l1, ch, c, &wa[iw], sign);
       else pass2(idot, l1, c, ch, &wa[iw], sign);
+      na = 1 - na;
+    } else if (ip == 3) {
+      int ix2 = iw + idot;
+      if (na != 0) pass3(idot, l1, ch, c, &wa[iw], &wa[ix2], sign);
+      else pass3(idot, l1, c, ch, &wa[iw], &wa[ix2], sign);
+      na = 1 - na;
+    } else {  // ip == 5 (fft_plan_init rejects other factors)
+      int ix2 = iw + idot, ix3 = ix2 + idot, ix4 = ix3 + idot;
+      if (na != 0) pass5(idot, l1, ch, c, &wa[iw], &wa[ix2], &wa[ix3], &wa[ix4], sign);
+      else pass5(idot, l1, c, ch, &wa[iw], &wa[ix2], &wa[ix3], &wa[ix4], sign);
       na = 1 - na;
     }
     l1 = l2;

@@ -274,10 +274,14 @@ static void build_grid(Model& m) {
   m.cy2 = m.cy * m.cy;
   m.tcx = 0.25 / m.dx;
   m.tcy = 0.25 / m.dy;
-  // coriolis.F90:146-160 geostrophic profile (no shear)
+  // coriolis.F90:155-163 geostrophic profile, with the shear of baroclinicity_use_geostrophic_shear
   for (int k = 1; k <= kkp; ++k) {
     m.geostrophic_wind_x(k) = c.surface_geostrophic_wind_x;
     m.geostrophic_wind_y(k) = c.surface_geostrophic_wind_y;
+    if (c.baroclinicity_use_geostrophic_shear) {
+      m.geostrophic_wind_x(k) = m.geostrophic_wind_x(k) + c.geostrophic_wind_rate_of_change_in_x * m.zn(k);
+      m.geostrophic_wind_y(k) = m.geostrophic_wind_y(k) + c.geostrophic_wind_rate_of_change_in_y * m.zn(k);
+    }
   }
 }
 
@@ -996,6 +1000,27 @@ static void tvd_advection_column(Model& m) {
   double dt = m.dtm * 2.0;  // scalar_stepping is always CENTRED_STEPPING (steppingdirection.F90:29-33)
   if (m.th.active) advect_scalar_field(m, dt, m.zth, m.th, m.sth, m.tvd_th);
   for (int n = 0; n < m.cfg.number_q_fields; ++n) advect_scalar_field(m, dt, m.zq[n], m.q[n], m.sq[n], m.tvd_q[n]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// th_advection (thadvection.F90:53-78 initialisation, :129-219 timestep).  The oracle is Boussinesq
+// (use_anelastic_equations = .false.): vertical_advection_of_reference_state does nothing there,
+// and advection_of_mean_baroclinicity takes its Boussinesq branch (:205-212).  The callback
+// touches every column it is given, halo columns included.
+// ---------------------------------------------------------------------------------------------
+static void th_advection_column(Model& m) {
+  const mgpu_config& c = m.cfg;
+  if (!c.th_advection_enabled) return;
+  // l_advect_mean_baroclinicity (:62-71): only with passive q
+  if (!(c.baroclinicity_use_geostrophic_shear && c.passive_q)) return;
+  if (!m.th.active) return;
+  const double fcoriol_over_G = c.fcoriol / c.G;
+  const double multiplicative_factor_x = c.rate_change_geostrophic_wind_x * c.thref0 * fcoriol_over_G;
+  const double multiplicative_factor_y = c.rate_change_geostrophic_wind_y * c.thref0 * fcoriol_over_G;
+  int y = m.col_y, x = m.col_x;
+  for (int k = 2; k <= m.nz; ++k)
+    m.sth(k, y, x) = m.sth(k, y, x) + ((m.v(k, y, x) + m.vgal) * multiplicative_factor_x -
+                                       (m.u(k, y, x) + m.ugal) * multiplicative_factor_y);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1811,14 +1836,15 @@ static void timestep(Model& m) {
   // dynamics
   if (m.cfg.advection_flow_fields == MGPU_ADVECT_TVD)
     for (int c = 0; c < 3; ++c) interpolate_flow(m, c);
+  // global_config:88: pw_advection, tvd_advection, th_advection, diffusion, viscosity, coriolis, ...
   if (m.cfg.simplecloud_enabled)
-    column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
-                     buoyancy_column, damping_column, forcing_column, set_consistent_lowbc_column,
-                     simplecloud_column, diverr_column, psrce_column, stepfields_column});
+    column_group(m, {pw_advection_column, tvd_advection_column, th_advection_column, diffusion_column,
+                     viscosity_column, coriolis_column, buoyancy_column, damping_column, forcing_column,
+                     set_consistent_lowbc_column, simplecloud_column, diverr_column, psrce_column, stepfields_column});
   else
-    column_group(m, {pw_advection_column, tvd_advection_column, diffusion_column, viscosity_column, coriolis_column,
-                     buoyancy_column, damping_column, forcing_column, set_consistent_lowbc_column, diverr_column,
-                     psrce_column, stepfields_column});
+    column_group(m, {pw_advection_column, tvd_advection_column, th_advection_column, diffusion_column,
+                     viscosity_column, coriolis_column, buoyancy_column, damping_column, forcing_column,
+                     set_consistent_lowbc_column, diverr_column, psrce_column, stepfields_column});
   // solver: mean_profiles, then the pressure solve
   if (mean_profiles_enabled(m)) mean_profiles(m);
   if (m.cfg.solver == MGPU_SOLVER_FFT) fftsolver(m);
@@ -1854,7 +1880,8 @@ Prof* profile_by_name(Model& m, const std::string& n) {
       {"prefn", &m.prefn}, {"prefrcp", &m.prefrcp}, {"rprefrcp", &m.rprefrcp}, {"tref", &m.tref},
       {"qsat", &m.qsat}, {"dqsatdt", &m.dqsatdt}, {"qsatfac", &m.qsatfac}, {"dmpco", &m.dmpco},
       {"dmpcoz", &m.dmpcoz}, {"w_subs", &m.w_subs}, {"olzubar", &m.olzubar}, {"olzvbar", &m.olzvbar},
-      {"olzthbar", &m.olzthbar}, {"olubar", &m.olubar}, {"olvbar", &m.olvbar}, {"olthbar", &m.olthbar}};
+      {"olzthbar", &m.olzthbar}, {"olubar", &m.olubar}, {"olvbar", &m.olvbar}, {"olthbar", &m.olthbar},
+      {"geostrophic_wind_x", &m.geostrophic_wind_x}, {"geostrophic_wind_y", &m.geostrophic_wind_y}};
   for (auto& t : tab)
     if (n == t.name) return t.p;
   return nullptr;
@@ -2274,6 +2301,7 @@ int orc_component(void* h, int cid) {
       case MGPU_C_MEAN_PROFILES: mean_profiles(m); break;
       case MGPU_C_DAMPING: column_group(m, {damping_column}); break;
       case MGPU_C_FORCING: column_group(m, {forcing_column}); break;
+      case MGPU_C_TH_ADVECTION: column_group(m, {th_advection_column}); break;
       default: return -5;
     }
   } catch (std::exception& e) {

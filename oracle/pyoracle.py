@@ -173,5 +173,5 @@ def fft_c2c(x: np.ndarray, sign: int) -> np.ndarray:
     buf[0::2] = x.real
     buf[1::2] = x.imag
     if lib().orc_fft_c2c(n, buf.ctypes.data, sign) != 0:
-        raise ValueError("length must be a power of two")
+        raise ValueError("length must have no prime factor above 5")
     return buf[0::2] + 1j * buf[1::2]

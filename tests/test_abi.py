@@ -94,10 +94,11 @@ def test_create_without_device_fails_loudly():
         api.Model(cfg)
 
 
-@pytest.mark.parametrize("nx,ny,nz", [(30, 32, 10), (32, 24, 10), (32, 32, 2), (2, 32, 10)])
+@pytest.mark.parametrize("nx,ny,nz", [(28, 32, 10), (32, 22, 10), (32, 27, 10), (32, 32, 2), (2, 32, 10),
+                                      (8192, 32, 10)])
 def test_create_rejects_unsupported_grids(nx, ny, nz):
-    """Non-power-of-two horizontal sizes (FFT) and fewer than 3 levels are argument errors, checked
-    on the host before any device work."""
+    """Horizontal sizes with a prime factor above 5 or beyond 4096 points (FFT), odd sizes and
+    fewer than 3 levels are argument errors, checked on the host before any device work."""
     cfg = cf.dry_cbl_config(nx, ny, nz, 50.0, 25.0, 1.0)
     h = C.c_void_p()
     rc = api.lib().mgpu_create(C.byref(cfg), C.byref(h))

@@ -220,3 +220,29 @@ def test_autograd_function_gradient(gpu_lib):
     ad = float((th0.grad * dth).sum())
     assert abs(ad - float(fd)) <= 1e-4 * abs(float(fd)), (ad, float(fd))
     assert abs(float(r0.grad) - float(fd_r)) <= 1e-4 * abs(float(fd_r)), (float(r0.grad), float(fd_r))
+
+
+def test_branch_flips_counts_differing_decisions(gpu_lib):
+    """Two models on one state take the same branches; a perturbation of order one changes some
+    limiter, upwind or Richardson-regime decisions; the count is symmetric."""
+    c = config()
+    st = base_state()
+    a, b = api.Model(c), api.Model(config())
+    a.set_state(st)
+    b.set_state(st)
+    for m in (a, b):
+        m.set_timestep(2)
+    assert a.branch_flips(b) == 0
+    pert = dict(st)
+    pert["u"] = st["u"] + ini.uniform_noise((NZ, NY, NX), 77, 1, 1.0)
+    pert["zth"] = st["zth"] + ini.uniform_noise((NZ, NY, NX), 78, 1, 0.5)
+    b.set_state(pert)
+    b.set_timestep(2)
+    n_ab = a.branch_flips(b)
+    assert n_ab > 0
+    assert b.branch_flips(a) == n_ab
+    a.step(1)
+    b.step(1)
+    assert a.branch_flips(b) > 0
+    a.close()
+    b.close()

@@ -21,7 +21,8 @@ def direct_dft(x, sign):
     return np.exp(sign * 2j * np.pi * np.outer(k, k) / n) @ x
 
 
-@pytest.mark.parametrize("n", [4, 8, 16, 32, 64, 128, 256, 512, 1024])
+@pytest.mark.parametrize("n", [4, 8, 16, 32, 64, 128, 256, 512, 1024, 3, 5, 6, 10, 12, 15, 24, 30, 45, 60, 96, 100,
+                               360, 384, 750])
 def test_fftpack_matches_direct_dft(n):
     rng = np.random.RandomState(n)
     x = rng.randn(n) + 1j * rng.randn(n)
@@ -34,9 +35,11 @@ def test_fftpack_matches_direct_dft(n):
     assert np.abs(rt - x).max() <= 1e-14 * np.abs(x).max() * np.log2(n)
 
 
-def test_fftpack_rejects_non_power_of_two():
+@pytest.mark.parametrize("n", [7, 14, 22, 26, 49])
+def test_fftpack_rejects_factors_beyond_five(n):
+    """FFTPACK's general passf.f90 (prime factors above 5) is not restated."""
     with pytest.raises(ValueError):
-        po.fft_c2c(np.ones(12, dtype=complex), -1)
+        po.fft_c2c(np.ones(n, dtype=complex), -1)
 
 
 def test_uniform_grid_coefficients():
