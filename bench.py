@@ -403,12 +403,36 @@ def precision_moist():
 
     a = _ap.Namespace(nx=512, ny=512, nz=160, dx=35.0, dz_bottom=5.0, dz_top=20.0, dt=0.3, steps=500, seed=1,
                       noise_levels=10, solver="fft", tolerance=1e-12)
-    ms64, th64, w64, qv64, _ = pr.run(a, cf.FP64)
-    ms32, th32, w32, qv32, _ = pr.run(a, cf.FP32_MIXED)
-    return {"case": "moist layer 512x512x160, dx=35 m, dz 5->20 m, dt=0.3 s, simplecloud, 500 steps",
-            "fp64_ms_per_step": round(ms64, 4), "fp32_mixed_ms_per_step": round(ms32, 4),
-            "speedup": round(ms64 / ms32, 3), "rel_err_mean_theta": pr.rel(th32, th64),
-            "rel_err_mean_w2": pr.rel(w32, w64), "rel_err_mean_qv": pr.rel(qv32, qv64)}
+    f64, f32 = {}, {}
+    ms64, th64, w64, qv64, _ = pr.run(a, cf.FP64, fields=f64)
+    ms32, th32, w32, qv32, _ = pr.run(a, cf.FP32_MIXED, fields=f32)
+    per_field = pr.field_errors(f32, f64)
+    del f64, f32
+    out = {"case": "moist layer 512x512x160, dx=35 m, dz 5->20 m, dt=0.3 s, simplecloud, 500 steps",
+           "fp64_ms_per_step": round(ms64, 4), "fp32_mixed_ms_per_step": round(ms32, 4),
+           "speedup": round(ms64 / ms32, 3), "rel_err_mean_theta": pr.rel(th32, th64),
+           "rel_err_mean_w2": pr.rel(w32, w64), "rel_err_mean_qv": pr.rel(qv32, qv64),
+           "fields_fp32_vs_fp64": per_field}
+    # the same layer with the iterative solver (BiCGStab to 1e-12, FP64 refinement in the FP32-mixed
+    # run) over its first ITER_STEPS steps
+    ai = _ap.Namespace(**{**vars(a), "solver": "iterative", "steps": ITER_STEPS})
+    g64, g32 = {}, {}
+    mi64, ti64, wi64, _, _ = pr.run(ai, cf.FP64, fields=g64)
+    it64 = ai.iterations_per_step
+    mi32, ti32, wi32, _, _ = pr.run(ai, cf.FP32_MIXED, fields=g32)
+    it32 = ai.iterations_per_step
+    out["iterative"] = {"steps": ITER_STEPS, "tolerance": 1e-12, "solver": "BiCGStab",
+                        "fp64_ms_per_step": round(mi64, 4), "fp32_mixed_ms_per_step": round(mi32, 4),
+                        "speedup": round(mi64 / mi32, 3),
+                        "iterations_per_step": {"fp64": round(it64, 2), "fp32_mixed": round(it32, 2)},
+                        "rel_err_mean_theta": pr.rel(ti32, ti64), "rel_err_mean_w2": pr.rel(wi32, wi64),
+                        "fields_fp32_vs_fp64": pr.field_errors(g32, g64)}
+    return out
+
+
+# steps of the iterative-solver run on the moist layer (each BiCGStab solve to 1e-12 takes several
+# iterations; the full 500 steps would hold the bench for minutes)
+ITER_STEPS = 100
 
 
 def large_fp32_mixed():

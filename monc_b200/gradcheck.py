@@ -10,6 +10,15 @@ against central finite differences along random directions in the theta-noise sp
 the tangent-linear model along the same directions.  The forward window and its adjoint are timed
 with CUDA events on the model's stream; one JSON line reports the agreement and the
 adjoint/forward time ratio.
+
+    python -m monc_b200.gradcheck ... --directions 8 --sweep 1e-4 1e-5 1e-6 1e-7 1e-8 1e-9
+
+runs the finite differences at each eps instead, the two runs of each difference stepped side by
+side: for every step it counts the branch decisions (TVD limiter and upwind choices of theta, the
+Smagorinsky regime) in which the two runs differ (mgpu_branch_flips).  A difference whose runs
+differ in no decision measures a smooth function and must converge to the adjoint as eps shrinks,
+until the rounding of J dominates; one that straddles kinks measures a secant.  The derivative
+with respect to rmlmax (= Cs dx) is checked the same way with relative steps.
 """
 from __future__ import annotations
 
@@ -77,6 +86,80 @@ def timed_window(cfg, state, nsteps, adjoint_seed=None, interval=25, warm=True):
     return final, fwd_ms, adj_ms
 
 
+def state_objective(m, zn, dz, ztop):
+    return objective_np({f: m.download(f) for f in ("u", "v", "w")}, zn, dz, ztop)
+
+
+def central_difference(plus, minus, nsteps, zn, dz, ztop):
+    """(J(plus) - J(minus)) / 2 after nsteps steps of two models, each given as (config, state),
+    stepped side by side, and the branch decisions in which their steps differed, summed over the
+    steps."""
+    mp, mm = api.Model(plus[0]), api.Model(minus[0])
+    mp.set_state(plus[1])
+    mm.set_state(minus[1])
+    mp.set_timestep(1)
+    mm.set_timestep(1)
+    flips = 0
+    for _ in range(nsteps):
+        flips += mp.branch_flips(mm)
+        mp.step(1)
+        mm.step(1)
+    half = 0.5 * (state_objective(mp, zn, dz, ztop) - state_objective(mm, zn, dz, ztop))
+    mp.close()
+    mm.close()
+    return half, flips
+
+
+def sweep(a, cfg, zn, dz, base):
+    """Finite differences against the adjoint over a range of eps on one set of directions, with
+    the branch decisions each pair of runs straddles; and the Cs derivative the same way."""
+    dev = torch.device("cuda")
+    mask = torch.from_numpy(((zn <= a.ztop) & (np.arange(a.nz) >= 1)).astype(np.float64)).to(dev)
+    window = autodiff.Window(cfg, base, a.steps, a.interval)
+    th0 = torch.from_numpy(base["th"]).to(dev).requires_grad_(True)
+    rml = torch.tensor(cfg.rmlmax, dtype=torch.float64, device=dev, requires_grad=True)
+    u, v, w, _ = autodiff.MoncWindow.apply(th0, rml, window)
+    J = autodiff.resolved_tke(u, v, w, torch.from_numpy(dz).to(dev), mask)
+    J.backward()
+    g_th = th0.grad.cpu().numpy()
+    g_rml = float(rml.grad)
+    rng = np.random.default_rng(a.seed)
+    dirs = []
+    for _ in range(a.directions):
+        dth = np.zeros_like(base["th"])
+        dth[1:11] = rng.uniform(-1.0, 1.0, size=dth[1:11].shape)
+        dirs.append(dth)
+    table = []
+    for eps in a.eps_list:
+        rows = []
+        for dth in dirs:
+            sp, sm = dict(base), dict(base)
+            sp["th"] = base["th"] + eps * dth
+            sm["th"] = base["th"] - eps * dth
+            half, flips = central_difference((cfg, sp), (cfg, sm), a.steps, zn, dz, a.ztop)
+            fd = half / eps
+            ad = float(np.vdot(g_th, dth))
+            rows.append((abs(ad - fd) / max(abs(fd), 1e-300), flips))
+        err = np.array([r[0] for r in rows])
+        fl = np.array([r[1] for r in rows])
+        smooth = err[fl == 0]
+        table.append({"eps": eps, "median_rel_err": float(np.median(err)), "max_rel_err": float(err.max()),
+                      "directions_with_flips": int((fl > 0).sum()), "median_flips": float(np.median(fl)),
+                      "max_rel_err_without_flips": float(smooth.max()) if smooth.size else None,
+                      "per_direction": [{"rel_err": float(e), "flips": int(f)} for e, f in rows]})
+    cs_rows = []
+    for eps in a.eps_list:
+        cp, cm = setup(a)[0], setup(a)[0]
+        cp.rmlmax = cfg.rmlmax * (1.0 + eps)
+        cm.rmlmax = cfg.rmlmax * (1.0 - eps)
+        half, flips = central_difference((cp, base), (cm, base), a.steps, zn, dz, a.ztop)
+        fd = half / (eps * cfg.rmlmax)
+        cs_rows.append({"eps_relative": eps, "fd_dJ_drmlmax": fd, "flips": flips,
+                        "rel_err": abs(g_rml - fd) / max(abs(fd), 1e-300)})
+    return {"grid": [a.nx, a.ny, a.nz], "steps": a.steps, "J": float(J.detach()), "directions": a.directions,
+            "adjoint_dJ_drmlmax": g_rml, "adjoint_dJ_dCs": g_rml * cfg.dxx, "theta": table, "cs": cs_rows}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--nx", type=int, default=128)
@@ -93,8 +176,14 @@ def main(argv=None):
     ap.add_argument("--directions", type=int, default=64)
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--ztop", type=float, default=1000.0)
+    ap.add_argument("--sweep", type=float, nargs="*", dest="eps_list",
+                    help="finite differences at each of these eps on --directions directions, with the branch "
+                         "decisions each pair of runs straddles, and the Cs derivative (one JSON line)")
     a = ap.parse_args(argv)
     cfg, zn, dz, base = setup(a)
+    if a.eps_list:
+        print(json.dumps(sweep(a, cfg, zn, dz, base)))
+        return
     dev = torch.device("cuda")
     mask = torch.from_numpy(((zn <= a.ztop) & (np.arange(a.nz) >= 1)).astype(np.float64)).to(dev)
     dzt = torch.from_numpy(dz).to(dev)

@@ -8,7 +8,12 @@ and 1.5 g/kg above (as vapour; simplecloud forms the cloud), seeded +-0.1 K nois
 Both precisions start from the same state.  Reported: ms per step of each (CUDA events on the
 model's stream, after the first step), the speed-up, and after the last step the maximum
 relative difference of the domain-mean theta and w'^2 profiles (max |a-b| / max |b| over
-levels), plus the same for the mean vapour.
+levels), plus the same for the mean vapour, and for every prognostic field (u, v, w, theta,
+vapour, liquid) its maximum and RMS relative difference from the FP64 run: max |a-b| / max |b|
+and rms(a-b) / rms(b) over the grid, theta as its departure from the reference state thref0.
+With --solver iterative both runs solve for the pressure with BiCGStab to --tolerance (FP64, and
+FP32 corrections inside FP64 iterative refinement for FP32-mixed); the iterations per step are
+reported (each step is then queued on its own, to read its solve's iteration count).
 """
 from __future__ import annotations
 
@@ -32,7 +37,13 @@ def build(a, precision):
     return c, st
 
 
-def run(a, precision, reproducible=0, round_state=False):
+FIELDS = ("u", "v", "w", "th", "q0", "q1")
+
+
+def run(a, precision, reproducible=0, round_state=False, fields=None):
+    """ms per step, the mean theta, w'^2, vapour and liquid profiles after a.steps steps, and
+    (when `fields` is a dict) the final prognostic fields in it; iterations per step of an
+    iterative solve in a.iterations_per_step."""
     c, st = build(a, precision)
     c.reproducible = reproducible
     if round_state:  # the initial state as the FP32-mixed model holds it
@@ -44,15 +55,37 @@ def run(a, precision, reproducible=0, round_state=False):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    m.step(a.steps - 1)
+    if a.solver == "iterative":
+        its = 0
+        for _ in range(a.steps - 1):
+            m.step(1)
+            its += m.reductions().solver_iterations
+        a.iterations_per_step = its / max(a.steps - 1, 1)
+    else:
+        m.step(a.steps - 1)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / max(a.steps - 1, 1)
     th, w2 = m.diagnostics()
     qv = m.mean_profile("q0")
     ql = m.mean_profile("q1")
+    if fields is not None:
+        for f in FIELDS:
+            fields[f] = m.download(f)
     m.close()
     return ms, th, w2, qv, ql
+
+
+def field_errors(test: dict, ref: dict) -> dict:
+    """Per field: max |a-b| / max |b| and rms(a-b) / rms(b) over the grid (theta as the departure
+    from the reference state, which is what the model holds)."""
+    out = {}
+    for f in FIELDS:
+        a, b = test[f], ref[f]
+        d = a - b
+        out[f] = {"max_rel": float(np.abs(d).max() / max(np.abs(b).max(), 1e-300)),
+                  "rms_rel": float(np.sqrt(np.mean(d * d)) / max(np.sqrt(np.mean(b * b)), 1e-300))}
+    return out
 
 
 def rel(a, b):
@@ -76,8 +109,13 @@ def main(argv=None):
     ap.add_argument("--no-control", dest="control", action="store_false",
                     help="skip the FP64 run with separately rounded multiply-adds")
     a = ap.parse_args(argv)
-    ms64, th64, w64, qv64, ql64 = run(a, cf.FP64)
-    ms32, th32, w32, qv32, ql32 = run(a, cf.FP32_MIXED)
+    f64, f32 = {}, {}
+    ms64, th64, w64, qv64, ql64 = run(a, cf.FP64, fields=f64)
+    its64 = getattr(a, "iterations_per_step", None)
+    ms32, th32, w32, qv32, ql32 = run(a, cf.FP32_MIXED, fields=f32)
+    its32 = getattr(a, "iterations_per_step", None)
+    per_field = field_errors(f32, f64)
+    del f64, f32
     # control: the same FP64 model with separately rounded multiply-adds; the difference shows how
     # far rounding-level changes alone grow in this developing convection
     _, thr, wr, qvr, _ = run(a, cf.FP64, reproducible=1) if a.control else (None, th64, w64, qv64, None)
@@ -99,6 +137,8 @@ def main(argv=None):
         "rel_err_mean_qv": rel(qv32, qv64),
         "max_mean_ql_fp64": float(ql64.max()),
         "rel_err_mean_ql": rel(ql32, ql64),
+        "fields_fp32_vs_fp64": per_field,
+        "iterations_per_step": {"fp64": its64, "fp32_mixed": its32} if a.solver == "iterative" else None,
         "fp64_fma_vs_separate_rounding": {"rel_err_mean_theta": rel(thr, th64), "rel_err_mean_w2": rel(wr, w64),
                                            "rel_err_mean_qv": rel(qvr, qv64)},
         "fp64_from_fp32_rounded_initial_state": {"rel_err_mean_theta": rel(thi, th64), "rel_err_mean_w2": rel(wi, w64),

@@ -39,7 +39,12 @@ def test_gpus_2_under_a_one_rank_launcher_is_refused():
 
 def test_gpus_2_without_a_launcher_starts_two_ranks():
     r = _run({}, "--gpus", "2", "--steps", "1")
-    # two ranks were started; each stops for want of a CUDA device, and nothing is reported
+    # torch.distributed.run started two ranks (it reports the per-process thread setting only for
+    # more than one process, and names local rank 1 when it ends them); a rank stops for want of a
+    # CUDA device, the launcher ends the other, and nothing is reported
+    out = r.stdout + r.stderr
     assert r.returncode != 0
-    assert (r.stdout + r.stderr).count("no CUDA device") >= 2, r.stderr[-2000:]
+    assert "for each process" in out, out[-2000:]
+    assert "no CUDA device" in out, out[-2000:]
+    assert "local_rank: 1" in out, out[-2000:]
     assert '"n_gpus"' not in r.stdout
