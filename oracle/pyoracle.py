@@ -14,19 +14,22 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libmonc_oracle.so")
+# MONC_ORACLE_LIB=native loads the -O3 -march=native build that bench.py times as the CPU
+# baseline; the checker (tests, smoke) always uses the default build
+_NATIVE_PATH = os.path.join(_HERE, "_build", "libmonc_oracle_native.so")
 _lib = None
 
 
-def build() -> str:
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    return _LIB_PATH
+def build(native: bool = False) -> str:
+    subprocess.run(["make", "-s", "-C", _HERE] + (["native"] if native else []), check=True)
+    return _NATIVE_PATH if native else _LIB_PATH
 
 
 def lib():
     global _lib
     if _lib is None:
-        build()  # make is a no-op when the library is newer than its sources
-        L = C.CDLL(_LIB_PATH)
+        native = os.environ.get("MONC_ORACLE_LIB") == "native"
+        L = C.CDLL(build(native))  # make is a no-op when the library is newer than its sources
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_void_p]
         L.orc_destroy.argtypes = [C.c_void_p]
