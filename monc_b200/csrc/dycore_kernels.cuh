@@ -629,6 +629,14 @@ constexpr size_t scalar_smem() {
 }
 }  // namespace tiled
 
+// A column's values at levels k0 and k0+1 held in registers, read through the accessor interface
+template <typename T>
+struct ColPair {
+  T v0, v1;
+  int k0;
+  __device__ __forceinline__ T operator()(int k, int, int) const { return k == k0 ? v0 : v1; }
+};
+
 // Centred ring view: the thread's own point at levels kc-1 .. kc+2 through four slot pointers.
 // Every access the device functions make at k +- const, j +- const, i +- const folds to one
 // shared-memory load with an immediate offset; data-dependent levels select among the four.
@@ -954,18 +962,22 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     const T* Ck = CT + (k & 1) * CN;
     auto cfl = [&](int kk, int jj, int ii) -> T { return kk == k ? Ck[(jj - j0 + 1) * CW + (ii - i0 + 1)] : c_hi; };
     // TVD faces of this level: own x+1/2 and y+1/2 faces, then the tile's low-side faces
-    FX[ty * (TX + 1) + tx + 1] =
-        tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
-    FY[(ty + 1) * TX + tx] =
-        tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    // the own faces are evaluated without early returns (SELECT), so that the compiler can
+    // interleave the three independent face computations
+    typedef decltype(cfl) CS;
+    FX[ty * (TX + 1) + tx + 1] = tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS, NoRec, true>(
+        s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    FY[(ty + 1) * TX + tx] = tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS, NoRec, true>(
+        s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    T fz_hi = (k < nz) ? tvd_face_z_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS, NoRec, true>(
+                             s, P, U, V, W, ZF, dt, k, j, i, cfl)
+                       : (T)0.0;
     if (tid < TX)
       FY[tid] = tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j0 - 1,
                                                                                i0 + tid, cfl);
     else if (tid < TX + TY)
       FX[(tid - TX) * (TX + 1)] = tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(
           s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1, cfl);
-    T fz_hi = (k < nz) ? tvd_face_z_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl)
-                       : (T)0.0;
     __syncthreads();
     T sth = tvd_source<T>(s, P, U, V, W, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1], FY[ty * TX + tx],
                           FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
@@ -1077,6 +1089,14 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_smag_tile
   }
   cp_async_wait_all();
   __syncthreads();
+  // the dry Richardson number reads th at k and k+1 of the column: kept in registers, the level
+  // k+2 value loaded one level ahead so that its latency overlaps the strain rate
+  const T* __restrict__ thg = d.th;
+  T th0 = (T)0.0, th1 = (T)0.0;
+  if (!moist) {
+    th0 = __ldg(thg + lin(s, kb, j, i));
+    th1 = __ldg(thg + lin(s, kb + 1, j, i));
+  }
   // the strain-rate parts of level k come from the level below, where they were level k+1's
   StrainLevel<T> lo;
   {
@@ -1092,12 +1112,19 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_smag_tile
     const CProf<T> P = cprof<T>(rP, k);
     const CRing<T> U = cring<T, RM>(rU, k, co, j, i), V = cring<T, RM>(rV, k, co, j, i),
                    W = cring<T, RM>(rW, k, co, j, i);
+    const T th2 = (!moist && k + 2 <= nz) ? __ldg(thg + lin(s, k + 2, j, i)) : (T)0.0;
     const StrainLevel<T> hi = strain_level<T>(s, P, U, V, W, k + 1, j, i);
     const T ssq = half_squared_strain_parts<T>(s, P, U, V, W, k, j, i, lo, hi);
     lo = hi;
     T vis, diff;
-    smagorinsky_from_strain<T>(s, P, ssq, THc, THa, moist ? &QV : (const View<T>*)nullptr,
-                               moist ? &QL : (const View<T>*)nullptr, k, j, i, vis, diff);
+    if (moist)
+      smagorinsky_from_strain<T, CProf<T>, View<T>, View<T>>(s, P, ssq, THc, THa, &QV, &QL, k, j, i, vis, diff);
+    else
+      smagorinsky_from_strain<T, CProf<T>, ColPair<T>, View<T>>(s, P, ssq, ColPair<T>{th0, th1, k}, THa,
+                                                                (const View<T>*)nullptr, (const View<T>*)nullptr, k, j,
+                                                                i, vis, diff);
+    th0 = th1;
+    th1 = th2;
     const long long o = lin(s, k, j, i);
     d.vis[o] = vis;
     d.diff[o] = diff;

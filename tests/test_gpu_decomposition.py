@@ -485,7 +485,7 @@ def test_slab_entry_points_check_arguments(gpu_lib):
     with pytest.raises(api.MgpuError):
         m.slab_init(64, 12, 8)  # no interior rows left
     with pytest.raises(api.MgpuError):
-        m.slab_init(48, 4, 8)  # ny_global not a power of two
+        m.slab_init(56, 4, 8)  # ny_global with a prime factor above 5
     m.slab_init(64, 4, 9)
     buf = torch.zeros(8 * NZ * 4 * NX, dtype=torch.float64, device="cuda")
     with pytest.raises(api.MgpuError):
