@@ -12,7 +12,9 @@
   dt = 0.5 s, noise on the lowest 10 levels): every field <= 1e-10 after 1 and 2 steps.
 * Moist layer 512x512x160 (dx = 35 m, stretched dz 5 -> 20 m, dt = 0.3 s, simplecloud), FP64:
   every field, vapour and liquid included, <= 1e-10 after 1 step.
-* Dry CBL 128x128x96 (dx = 50 m, dz = 20 m, dt = 1 s): every field <= 1e-10 after 1 and 2 steps.
+* Dry CBL 128x128x96 (dx = 50 m, dz = 20 m, dt = 1 s, windless): every field <= 1e-10 after 1
+  and 2 steps above level 1; at level 1 the windless surface scheme's conditioning sets the bound
+  (see LEVEL1_WINDLESS_TOL).
 
 The oracle runs MONC's column order in FP64 on one host core; these sizes take it from about a
 second (128x128x96) to about 15 s per step (512x512x160, with ~12 GB of host memory).
@@ -94,6 +96,17 @@ def test_dry_cbl_256x256x128_benchmark_grid(gpu_lib):
     o.close()
 
 
+# In a windless start the surface scheme is ill-conditioned at level 1: with u = v = 0 the
+# convective branch of lowerbc.F90:601-633 takes u* from the free-convection limit (~1e-8 m/s),
+# and its denominator zlogth - 2 log((1 + sqrt(1 + X1)) / (1 + sqrt(1 + X2))) (X ~ 1e23) cancels to
+# ~6e-11 out of ~4.6, a condition number of ~8e10.  One unit in the last place of log moves the
+# level-1 diffusivity by ~1e-5 relative, and the ghost value theta(1) with it, so the GPU's log and
+# the host's differ there by that much although both are correctly computed.  The surface flux
+# diff(1) (theta(1) - theta(2)) that the interior sees is well-conditioned, so every field above
+# level 1 is still held to STEP_TOL.
+LEVEL1_WINDLESS_TOL = 1e-4
+
+
 def test_dry_cbl_128x128x96_differentiation_grid(gpu_lib):
     cfg = cf.dry_cbl_config(128, 128, 96, 50.0, 20.0, 1.0)
     zn = api.reference_profile(cfg, "zn")
@@ -102,7 +115,17 @@ def test_dry_cbl_128x128x96_differentiation_grid(gpu_lib):
     for n in (1, 2):
         o.step(1)
         m.step(1)
-        check_fields(o, m, FIELDS, STEP_TOL, f"step {n}")
+        bad = {}
+        for f in FIELDS:
+            a, b = m.download(f), o.get(api.field_id(f))
+            e = rel_err(a[1:], b[1:])
+            if not e <= STEP_TOL:
+                bad[f] = e
+            tol1 = LEVEL1_WINDLESS_TOL if f in ("diff", "th", "zth") else STEP_TOL
+            e1 = rel_err(a[0], b[0]) if np.abs(b[0]).max() > 0 else float(np.abs(a[0]).max())
+            if not e1 <= tol1:
+                bad[f + "(level 1)"] = e1
+        assert not bad, f"step {n}: {bad}"
     m.close()
     o.close()
 
