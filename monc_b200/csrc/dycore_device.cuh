@@ -656,7 +656,7 @@ struct CflInline {
 };
 
 // face x+1/2 of cell (k, j, i): flux_previous_x(k) of ultflx; cfl(k, j, i) gives cell_cfl_out
-template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec, bool SELECT = false>
+template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec>
 __device__ T tvd_face_x_g(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                           const AF& ZF, T dt, int k, int j, int i, const CS& cfl, const Rec& rec = Rec()) {
   const int nz = s.nz;
@@ -673,10 +673,7 @@ __device__ T tvd_face_x_g(const Scalars& s, const PA& P, const A& U, const A& V,
   T fcurvs = fd - (T)2.0 * fc + fu;
   rec(signbit(u0) ? 1u : 0u, 1);
   rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
-  // smooth: ultflx returns fc; with SELECT the rest is evaluated anyway and fc chosen at the end,
-  // so that a kernel can interleave several faces without branches between them
-  const bool smooth = fabs(fcurvs) >= fabs(fdels);
-  if (!SELECT && smooth) return fc;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
   // the upwind cell: i when u0 > 0, otherwise i + 1 (u0 = 0 included, as ultflx tests u > 0)
   rec(u0 > (T)0.0 ? 1u : 0u, 1);
   T sum = cfl(k, j, u0 > (T)0.0 ? i : i + 1) * dt;
@@ -703,8 +700,7 @@ __device__ T tvd_face_x_g(const Scalars& s, const PA& P, const A& U, const A& V,
     t1 = t1 + t2;
     fgt2 = fabs(sf) * cy * dt * (fc - t1);
   }
-  const T lim = limit_face<T, Rec>(u0, cx, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs, rec);
-  return (SELECT && smooth) ? fc : lim;
+  return limit_face<T, Rec>(u0, cx, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs, rec);
 }
 
 template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
@@ -714,7 +710,7 @@ __device__ T tvd_face_x(const Scalars& s, const PA& P, const A& U, const A& V, c
 }
 
 // face y+1/2 of cell (k, j, i): flux_y(k) of ultflx
-template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec, bool SELECT = false>
+template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec>
 __device__ T tvd_face_y_g(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                           const AF& ZF, T dt, int k, int j, int i, const CS& cfl, const Rec& rec = Rec()) {
   const int nz = s.nz;
@@ -732,8 +728,7 @@ __device__ T tvd_face_y_g(const Scalars& s, const PA& P, const A& U, const A& V,
   T fcurvs = fd - (T)2.0 * fc + fu;
   rec((unsigned)jo, 1);
   rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
-  const bool smooth = fabs(fcurvs) >= fabs(fdels);
-  if (!SELECT && smooth) return fc;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
   T sum = cfl(k, j + jo, i) * dt;
   T fgt1;
   {
@@ -752,8 +747,7 @@ __device__ T tvd_face_y_g(const Scalars& s, const PA& P, const A& U, const A& V,
     T posuf = (T)0.5 + tsign<T>((T).5, sf);
     fgt2 = fabs(sf) * cx * dt * (fc - (ZF(k, j + jo, i + 1) * ((T)1. - posuf) + ZF(k, j + jo, i - 1) * posuf));
   }
-  const T lim = limit_face<T, Rec>(v0, cy, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs, rec);
-  return (SELECT && smooth) ? fc : lim;
+  return limit_face<T, Rec>(v0, cy, dt, sum, fdels, fd, fc, fu, fgt1, fgt2, fcurvs, rec);
 }
 
 template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
@@ -763,7 +757,7 @@ __device__ T tvd_face_y(const Scalars& s, const PA& P, const A& U, const A& V, c
 }
 
 // flux_z(k+1): face above level k (2 <= k <= nz-1); the top routine handles k = nz-1
-template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec, bool SELECT = false>
+template <typename T, class A, class AF, class PA, class M, class CS, class Rec = NoRec>
 __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V, const A& W,
                           const AF& ZF, T dt, int k, int j, int i, const CS& cfl, const Rec& rec = Rec()) {
   const int nz = s.nz;
@@ -779,8 +773,7 @@ __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V,
     T fdels = fd - fu;
     rec(up ? 1u : 0u, 1);
     rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
-    const bool smooth = fabs(fcurvs) >= fabs(fdels);
-    if (!SELECT && smooth) return fc;
+    if (fabs(fcurvs) >= fabs(fdels)) return fc;
     if (up) {
       sum = (T)0.0;
       sum = sum + P(M::RDZ, k + M::KDOF) * (w0 + fabs(tmin<T>((T)0.0, W(k - 1, j, i))));
@@ -825,8 +818,7 @@ __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V,
     T fnrefs = fncs * hrcfl;
     T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
     rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
-    const T lim = ftemp * fdels + fu;
-    return (SELECT && smooth) ? fc : lim;
+    return ftemp * fdels + fu;
   }
   // middle of the column
   T sm = tsign<T>((T).5, w0);
@@ -839,8 +831,7 @@ __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V,
   T fdels = fd - fu;
   rec((unsigned)ko, 1);
   rec(fabs(fcurvs) >= fabs(fdels) ? 1u : 0u, 1);
-  const bool smooth = fabs(fcurvs) >= fabs(fdels);
-  if (!SELECT && smooth) return fc;
+  if (fabs(fcurvs) >= fabs(fdels)) return fc;
   sum = cfl(k + ko, j, i) * dt;
   {
     T sf = (T)0.125 * (V(k, j - 1, i) + V(k, j, i) + V(k + 1, j - 1, i) + V(k + 1, j, i));
@@ -868,8 +859,7 @@ __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V,
   T fnrefs = fncs * hrcfl;
   T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
   rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
-  const T lim = ftemp * fdels + fu;
-  return (SELECT && smooth) ? fc : lim;
+  return ftemp * fdels + fu;
 }
 
 template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>

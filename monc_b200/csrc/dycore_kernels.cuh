@@ -962,15 +962,11 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
     const T* Ck = CT + (k & 1) * CN;
     auto cfl = [&](int kk, int jj, int ii) -> T { return kk == k ? Ck[(jj - j0 + 1) * CW + (ii - i0 + 1)] : c_hi; };
     // TVD faces of this level: own x+1/2 and y+1/2 faces, then the tile's low-side faces
-    // the own faces are evaluated without early returns (SELECT), so that the compiler can
-    // interleave the three independent face computations
-    typedef decltype(cfl) CS;
-    FX[ty * (TX + 1) + tx + 1] = tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS, NoRec, true>(
-        s, P, U, V, W, ZF, dt, k, j, i, cfl);
-    FY[(ty + 1) * TX + tx] = tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS, NoRec, true>(
-        s, P, U, V, W, ZF, dt, k, j, i, cfl);
-    T fz_hi = (k < nz) ? tvd_face_z_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS, NoRec, true>(
-                             s, P, U, V, W, ZF, dt, k, j, i, cfl)
+    FX[ty * (TX + 1) + tx + 1] =
+        tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    FY[(ty + 1) * TX + tx] =
+        tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+    T fz_hi = (k < nz) ? tvd_face_z_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j, i, cfl)
                        : (T)0.0;
     if (tid < TX)
       FY[tid] = tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar>(s, P, U, V, W, ZF, dt, k, j0 - 1,

@@ -908,177 +908,15 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   cp_async_wait_0();
 }
 
-// ---- vertical tridiagonal with the levels split across the warps of a block ------------------
-// 32 consecutive columns per block (lane = column), the levels 2..nz split into TRS_NSEG
-// segments of at most L levels, one per warp; every value a thread needs stays in its registers,
-// so the spectrum is read and written once and nothing else goes to memory (k_tridiag keeps the
-// forward sweep's s1 in global memory).  The forward elimination s(k) = r(k) - lo(k) s(k-1) b1(k-1)
-// and the back substitution p(k) = (s(k) - up(k) p(k+1)) b1(k) are first-order affine
-// recurrences: each warp composes the map of its segment, the maps of the segments below (above)
-// give its carry-in, and the segment then runs from that carry with k_tridiag's expressions.  The
-// carries are rounded differently from a sequential sweep, so results agree with k_tridiag to
-// rounding, not bit for bit.  The horizontal-mean mode runs in an extra block, as in k_tridiag.
-constexpr int TRS_NSEG = 16;
-
-template <typename T, int L>
-__global__ void __launch_bounds__(32 * TRS_NSEG) k_tridiag_seg(typename Cx<T>::t* __restrict__ spec,
-                                                              const double* __restrict__ b1,
-                                                              const double* __restrict__ prof, int prof_stride, int nx,
-                                                              int ny, int nz, int transpose, int ncols, int kx0,
-                                                              int rpb) {
-  typedef typename Cx<T>::t C;
-  __shared__ double sA[TRS_NSEG][32];
-  __shared__ double2 sB[TRS_NSEG][32];
-  __shared__ double sC[TRS_NSEG][32];
-  __shared__ double2 sD[TRS_NSEG][32];
-  __shared__ C colv[MGPU_MAX_NZ];
-  const int nxh = nx / 2 + 1;
-  const long long lstride = (long long)rpb * ncols;
-  const double* czb = prof + P_CZB * prof_stride;
-  const double* cza = prof + P_CZA * prof_stride;
-  const double* czg = prof + P_CZG * prof_stride;
-  if (kx0 == 0 && blockIdx.x == gridDim.x - 1) {
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) colv[k] = spec[(long long)k * lstride];
-    __syncthreads();
-    if (threadIdx.x == 0) mean_mode_column<T>(colv, nz, czb, cza, czg, transpose);
-    __syncthreads();
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) spec[(long long)k * lstride] = colv[k];
-    return;
-  }
-  const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
-  const long long col = (long long)blockIdx.x * 32 + lane;
-  int ky = 0, c = 0;
-  bool ok = col < (long long)ny * ncols;
-  if (ok) {
-    ky = (int)(col / ncols);
-    c = (int)(col - (long long)ky * ncols);
-    if (kx0 + c == 0 && ky == 0) ok = false;  // the mean mode's column
-  }
-  const int kx = kx0 + c;
-  C* sp = spec + spec_row(ky, 1, rpb, ncols, nz) + c;
-  const double* lo = transpose ? cza - 1 : czb;
-  const double* up = transpose ? czb + 1 : cza;
-  const int kyi = ky <= ny / 2 ? ky : ny - ky;
-  const long long bstride = (long long)(ny / 2 + 1) * nxh;
-  const double* bcol = b1 + (long long)kyi * nxh + kx;
-  const int segl = (nz - 1 + TRS_NSEG - 1) / TRS_NSEG;
-  const int k0 = 2 + seg * segl, k1 = min(nz, k0 + segl - 1);
-  double rr[L], ri[L], bm[L];  // r(k) (then s(k)) and b1(k-1) of the segment's levels
-  double btop = 0.0;           // b1(k1)
-#pragma unroll
-  for (int q = 0; q < L; ++q) {
-    const int k = k0 + q;
-    rr[q] = ri[q] = bm[q] = 0.0;
-    if (ok && q < segl && k <= k1) {
-      const C v = sp[(long long)(k - 1) * lstride];
-      rr[q] = (double)v.x;
-      ri[q] = (double)v.y;
-      bm[q] = __ldg(bcol + (long long)(k - 1) * bstride);
-    }
-  }
-  if (ok && k0 <= k1) btop = __ldg(bcol + (long long)k1 * bstride);
-  // forward: the segment's map s(k1) = A s(k0-1) + B
-  double A = 1.0, Br = 0.0, Bi = 0.0;
-#pragma unroll
-  for (int q = 0; q < L; ++q) {
-    const int k = k0 + q;
-    if (q < segl && k <= k1) {
-      const double a = k == 2 ? 0.0 : -(lo[k] * bm[q]);
-      A = a * A;
-      Br = a * Br + rr[q];
-      Bi = a * Bi + ri[q];
-    }
-  }
-  sA[seg][lane] = A;
-  sB[seg][lane] = make_double2(Br, Bi);
-  __syncthreads();
-  double sr = 0.0, si = 0.0;  // s(k0-1)
-  for (int q = 0; q < seg; ++q) {
-    const double2 b = sB[q][lane];
-    const double aq = sA[q][lane];
-    sr = aq * sr + b.x;
-    si = aq * si + b.y;
-  }
-#pragma unroll
-  for (int q = 0; q < L; ++q) {
-    const int k = k0 + q;
-    if (q < segl && k <= k1) {
-      if (k == 2) {
-        sr = rr[q];
-        si = ri[q];
-      } else {
-        sr = rr[q] - lo[k] * sr * bm[q];
-        si = ri[q] - lo[k] * si * bm[q];
-      }
-      rr[q] = sr;
-      ri[q] = si;
-    }
-  }
-  // backward: the segment's map p(k0) = Cm p(k1+1) + D, from the top level of the segment down;
-  // b1(k) of level k0+q is bm[q+1], of the top level btop
-  double Cm = 1.0, Dr = 0.0, Di = 0.0;
-#pragma unroll
-  for (int q = L - 1; q >= 0; --q) {
-    const int k = k0 + q;
-    if (q < segl && k <= k1) {
-      const double bk = (k == k1) ? btop : bm[q + 1 < L ? q + 1 : q];
-      const double cq = k == nz ? 0.0 : -(up[k] * bk);
-      Cm = cq * Cm;
-      Dr = cq * Dr + rr[q] * bk;
-      Di = cq * Di + ri[q] * bk;
-    }
-  }
-  sC[seg][lane] = Cm;
-  sD[seg][lane] = make_double2(Dr, Di);
-  __syncthreads();
-  double pr = 0.0, pi = 0.0;  // p(k1+1)
-  for (int q = TRS_NSEG - 1; q > seg; --q) {
-    const double2 d = sD[q][lane];
-    const double cq = sC[q][lane];
-    pr = cq * pr + d.x;
-    pi = cq * pi + d.y;
-  }
-#pragma unroll
-  for (int q = L - 1; q >= 0; --q) {
-    const int k = k0 + q;
-    if (q < segl && k <= k1) {
-      const double bk = (k == k1) ? btop : bm[q + 1 < L ? q + 1 : q];
-      if (k == nz) {
-        pr = rr[q] * bk;
-        pi = ri[q] * bk;
-      } else {
-        pr = (rr[q] - up[k] * pr) * bk;
-        pi = (ri[q] - up[k] * pi) * bk;
-      }
-      if (ok) {
-        C o;
-        o.x = (T)pr;
-        o.y = (T)pi;
-        sp[(long long)(k - 1) * lstride] = o;
-      }
-    }
-  }
-}
-
-// The column solve of ncols kx columns (global kx0 ..) on ny rows: the segmented kernel when
-// its segments fit its registers (segments of up to 12 levels: nz <= 193), k_tridiag otherwise.
+// The column solve of ncols kx columns (global kx0 ..) on ny rows
 template <typename T>
 static void launch_tridiag(typename Cx<T>::t* spec, double2* s1, const double* b1, const double* prof, int prof_stride,
                            int nx, int ny, int nz, bool transpose, int ncols, int kx0, int rpb, cudaStream_t st) {
   typedef typename Cx<T>::t C;
   const long long ncol = (long long)ny * ncols;
-  const int segl = (nz - 1 + TRS_NSEG - 1) / TRS_NSEG;
-  const unsigned grid = (unsigned)((ncol + 31) / 32 + (kx0 == 0 ? 1 : 0));
-  const int tr = transpose ? 1 : 0;
-  if (segl <= 8)
-    k_tridiag_seg<T, 8><<<grid, 32 * TRS_NSEG, 0, st>>>(spec, b1, prof, prof_stride, nx, ny, nz, tr, ncols, kx0, rpb);
-  else if (segl <= 12)
-    k_tridiag_seg<T, 12><<<grid, 32 * TRS_NSEG, 0, st>>>(spec, b1, prof, prof_stride, nx, ny, nz, tr, ncols, kx0, rpb);
-  else {
-    ensure_tri_attr();
-    k_tridiag<T><<<(unsigned)((ncol + TRI_TB - 1) / TRI_TB + (kx0 == 0 ? 1 : 0)), TRI_TB, tri_smem_bytes<C>(nz), st>>>(
-        spec, s1, b1, prof, prof_stride, nx, ny, nz, tr, ncols, kx0, rpb);
-  }
+  ensure_tri_attr();
+  k_tridiag<T><<<(unsigned)((ncol + TRI_TB - 1) / TRI_TB + (kx0 == 0 ? 1 : 0)), TRI_TB, tri_smem_bytes<C>(nz), st>>>(
+      spec, s1, b1, prof, prof_stride, nx, ny, nz, transpose ? 1 : 0, ncols, kx0, rpb);
 }
 
 // Pivots and twiddles of the (pl.nx, pl.ny, pl.nz) grid; pl.spec and pl.s1 are left to the caller.
