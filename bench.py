@@ -430,9 +430,9 @@ def precision_moist():
     return out
 
 
-# steps of the iterative-solver run on the moist layer (each BiCGStab solve to 1e-12 takes several
-# iterations; the full 500 steps would hold the bench for minutes)
-ITER_STEPS = 100
+# steps of the iterative-solver run on the moist layer (each BiCGStab solve to 1e-12 takes over a
+# hundred iterations, 0.35 s a step in FP64; the full 500 steps would hold the bench for minutes)
+ITER_STEPS = 20
 
 
 def large_fp32_mixed():
