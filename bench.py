@@ -435,10 +435,10 @@ def precision_moist():
 ITER_STEPS = 20
 
 
-def large_fp32_mixed():
-    """The largest configuration: 1024x1024x200 FP32-mixed, dz 10->50 m to 6 km, vapour, liquid and
-    three passive tracers with log-normal surface sources, 150 / 200 W m-2 surface fluxes, +-0.2 K
-    noise, dt = 0.5 s, 200 steps; CUDA events on the model's stream over steps 2..200."""
+def _large_run(precision, fields=None):
+    """One run of the largest configuration in the given precision: ms per step over steps 2..200
+    (CUDA events on the model's stream), the mean theta and w'^2 profiles, and (when `fields` is a
+    dict) the final u, v, w, theta, vapour and liquid fields."""
     import torch
 
     from monc_b200 import api, config as cf, init as ini
@@ -447,7 +447,7 @@ def large_fp32_mixed():
     nz, steps = 200, 200
     z = cf.stretched_levels(nz, 10.0, 50.0, ztop=6000.0)
     c = cf.moist_config(nx, ny, z, 25.0, 0.5, shf_wm2=150.0, lhf_wm2=200.0, max_height_cloud=5000.0, n_tracers=3,
-                        precision=cf.FP32_MIXED)
+                        precision=precision)
     m = api.Model(c)
     # the state of init.moist_layer_state, built and uploaded one field at a time (each 1.7 GB on
     # the host): theta with +-0.2 K noise on the lowest levels, vapour, no liquid, three tracers
@@ -462,7 +462,10 @@ def large_fp32_mixed():
     f[:] = np.where(zn > 840.0, 1.5e-3, 9e-3)[:, None, None]
     m.upload("q0", f)
     m.upload("zq0", f)
-    f[:] = 2.0  # a uniform 2 m/s wind: MONC's surface scheme has no windless limit (u* -> 0)
+    # a uniform 2 m/s wind: with u = v = 0 the convective surface formula of lowerbc.F90:601-633
+    # takes u* from its free-convection limit and cancels to a condition number of ~1e10, which
+    # FP32 cannot carry
+    f[:] = 2.0
     m.upload("u", f)
     m.upload("zu", f)
     f[:] = 0.0
@@ -484,12 +487,34 @@ def large_fp32_mixed():
     e1.synchronize()
     ms = e0.elapsed_time(e1) / (steps - 1)
     th, w2 = m.diagnostics()
-    finite = bool(np.isfinite(th).all() and np.isfinite(w2).all())
+    if fields is not None:
+        for name in ("u", "v", "w", "th", "q0", "q1"):
+            fields[name] = m.download(name)
     m.close()
+    return ms, th, w2, nx * ny * nz
+
+
+def large_fp32_mixed():
+    """The largest configuration: 1024x1024x200 FP32-mixed, dz 10->50 m to 6 km, vapour, liquid and
+    three passive tracers with log-normal surface sources, 150 / 200 W m-2 surface fluxes, +-0.2 K
+    noise, dt = 0.5 s, 200 steps; CUDA events on the model's stream over steps 2..200.  The same
+    run in FP64 (about 80 GB of fields, inside the 180 GB of one B200) gives the reference for the
+    FP32-mixed run's per-field and mean-profile differences."""
+    from monc_b200 import config as cf, precision as pr
+
+    f32, f64 = {}, {}
+    ms32, th32, w32, npts = _large_run(cf.FP32_MIXED, f32)
+    ms64, th64, w64, _ = _large_run(cf.FP64, f64)
+    finite = bool(np.isfinite(th32).all() and np.isfinite(w32).all())
+    per_field = pr.field_errors(f32, f64)
+    del f32, f64
     return {"case": "1024x1024x200 FP32-mixed, dx=25 m, dz 10->50 m to 6 km, u = 2 m/s, vapour + liquid + "
                     "3 tracers, shf 150 / lhf 200 W m-2, dt=0.5 s, 200 steps",
-            "ms_per_step": round(ms, 3), "mpoint_steps_per_s": round(nx * ny * nz / (ms * 1e-3) / 1e6, 1),
-            "finite": finite, "max_mean_w2": float(np.max(w2)) if finite else None}
+            "ms_per_step": round(ms32, 3), "mpoint_steps_per_s": round(npts / (ms32 * 1e-3) / 1e6, 1),
+            "fp64_ms_per_step": round(ms64, 3), "fp64_mpoint_steps_per_s": round(npts / (ms64 * 1e-3) / 1e6, 1),
+            "speedup_vs_fp64": round(ms64 / ms32, 3), "finite": finite,
+            "rel_err_mean_theta": pr.rel(th32, th64), "rel_err_mean_w2": pr.rel(w32, w64),
+            "fields_fp32_vs_fp64": per_field}
 
 
 def _oracle_run(steps, warmup=1):
