@@ -27,7 +27,7 @@ from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
-STEP_TOL = 1e-10          # per field, after 1-2 steps (the north-star criterion)
+STEP_TOL = 1e-10          # per field, after 1-2 steps
 MEAN_TOL = 1e-9           # domain-mean theta' and w'^2 profiles after 200 steps
 FIELD_TOL_200 = 1e-8      # every field after 200 steps
 FIELDS = ["u", "v", "w", "th", "zu", "zv", "zw", "zth", "p", "vis", "diff"]
