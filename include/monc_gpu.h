@@ -61,9 +61,11 @@ extern "C" {
 #define MGPU_ITER_BICGSTAB 0
 #define MGPU_ITER_CG       1
 
-/* host array layouts accepted by upload/download */
+/* array layouts accepted by upload/download */
 #define MGPU_LAYOUT_XFAST    0  /* C order [nz][ny][nx], interior only (the device layout) */
 #define MGPU_LAYOUT_MONC     1  /* Fortran data(nz, ny+4, nx+4): z fastest, 2-deep x/y halo */
+#define MGPU_LAYOUT_DEVICE   2  /* as MGPU_LAYOUT_XFAST, but a pointer to FP64 device memory of the
+                                   handle's GPU: the copy stays on the device */
 
 /* field identifiers (state.F90:86-92 names) */
 enum mgpu_field_id {
@@ -231,8 +233,10 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out);
 /* Release every device allocation (the finalisation callbacks). */
 int mgpu_destroy(mgpu_handle* h);
 
-/* Copy a field between host and device (host pointer to FP64 data).  In MONC layout the
- * halo is ignored on upload and filled periodically on download. */
+/* Copy a field between host and device (host pointer to FP64 data), or, with
+ * MGPU_LAYOUT_DEVICE, between the model and another FP64 device array.  In MONC layout the halo
+ * is ignored on upload and filled periodically on download.  The call returns when the copy is
+ * complete; a device source must be ready before the call (work on other streams finished). */
 int mgpu_upload_field(mgpu_handle* h, int32_t field_id, const double* host, int32_t layout);
 int mgpu_download_field(mgpu_handle* h, int32_t field_id, double* host, int32_t layout);
 
@@ -375,10 +379,10 @@ int mgpu_stage_times(mgpu_handle* h, double* ms_total, int64_t* launches);
  * (the values mgpu_get_profile / mgpu_reference_profile return), read during the call; dx, dy
  * the horizontal spacings; stream a cudaStream_t or NULL.  nx and ny must be powers of two.
  *
- * All working storage (spectra, elimination scratch, pivots, twiddles, a copy of the
- * coefficients) is one file-scope device array of MGPU_NOALLOC_SCRATCH_BYTES that every GPU
- * loading the library holds until exit; grids needing more (about 128 x 128 x 64 is the largest
- * cube-like grid that fits) are rejected with MGPU_ERR_ARGUMENT and a message on stderr.  The
+ * All working storage (the spectrum, pivots, twiddles, a copy of the coefficients) is one
+ * file-scope device array of MGPU_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit; grids needing more (about 128 x 128 x 128 is the largest cube-like grid that fits)
+ * are rejected with MGPU_ERR_ARGUMENT and a message on stderr.  The
  * first call on a device looks up the array's device address (cudaGetSymbolAddress); make that
  * first call before any stream capture.  Nothing in the array has to start at zero -- each call
  * writes every value it later reads -- but all calls share the array and keep the last call's

@@ -34,6 +34,7 @@ ERR_CFL = -7
 
 LAYOUT_XFAST = 0
 LAYOUT_MONC = 1
+LAYOUT_DEVICE = 2
 
 FIELDS = {
     "u": 0, "v": 1, "w": 2, "th": 3, "zu": 4, "zv": 5, "zw": 6, "zth": 7, "p": 8,
@@ -295,6 +296,27 @@ class Model:
             a = np.empty((self.nx + 4, self.ny + 4, self.nz), dtype=np.float64)
         self._check(lib().mgpu_download_field(self.h, field_id(name), a.ctypes.data, layout), f"download {name}")
         return a
+
+    def upload_tensor(self, name, t):
+        """Copy a contiguous FP64 CUDA tensor [nz][ny][nx] into the model; it stays in HBM."""
+        import torch
+
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+                and tuple(t.shape) == (self.nz, self.ny, self.nx)):
+            raise ValueError(f"upload {name}: needs a contiguous float64 CUDA tensor of shape "
+                             f"{(self.nz, self.ny, self.nx)}")
+        torch.cuda.current_stream(t.device).synchronize()  # the tensor's producers have finished
+        self._check(lib().mgpu_upload_field(self.h, field_id(name), t.data_ptr(), LAYOUT_DEVICE), f"upload {name}")
+
+    def download_tensor(self, name, device):
+        """A new FP64 CUDA tensor [nz][ny][nx] on `device` holding the field, copied in HBM."""
+        import torch
+
+        out = torch.empty((self.nz, self.ny, self.nx), dtype=torch.float64, device=device)
+        torch.cuda.current_stream(out.device).synchronize()  # the memory's earlier users are done with it
+        self._check(lib().mgpu_download_field(self.h, field_id(name), out.data_ptr(), LAYOUT_DEVICE),
+                    f"download {name}")
+        return out
 
     def set_state(self, state: dict):
         for k, v in state.items():

@@ -4,14 +4,14 @@
 `window.base` with theta replaced by `th0` and the Smagorinsky mixing length `rmlmax` (= Cs*dx),
 and returns the final (u, v, w, th).  Its backward pass is the library's adjoint
 (`mgpu_adjoint_run`): a checkpointed reverse sweep of hand-differentiated step kernels, which
-returns the gradients with respect to th0 and rmlmax.  Tensors cross the boundary as float64
-host arrays; the model state itself stays on the GPU throughout.
+returns the gradients with respect to th0 and rmlmax.  CUDA tensors stay in HBM: they are copied
+device to device into and out of the model (MGPU_LAYOUT_DEVICE); CPU tensors go through float64
+host arrays.  The model state itself stays on the GPU throughout.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass
 
-import numpy as np
 import torch
 
 from . import api, config as cf
@@ -26,13 +26,28 @@ class Window:
     timestep: int = 1
 
 
-def _model(window: Window, th0: np.ndarray, rmlmax: float) -> api.Model:
+def _put(m: api.Model, name: str, a):
+    """A CUDA tensor device to device, anything else through a host array."""
+    if isinstance(a, torch.Tensor) and a.is_cuda:
+        m.upload_tensor(name, a.detach().to(torch.float64).contiguous())
+    elif isinstance(a, torch.Tensor):
+        m.upload(name, a.detach().to(torch.float64).numpy())
+    else:
+        m.upload(name, a)
+
+
+def _get(m: api.Model, name: str, device: torch.device) -> torch.Tensor:
+    if device.type == "cuda":
+        return m.download_tensor(name, device)
+    return torch.from_numpy(m.download(name))
+
+
+def _model(window: Window, th0, rmlmax: float) -> api.Model:
     c = cf.MgpuConfig.from_buffer_copy(window.cfg)
     c.rmlmax = float(rmlmax)
     m = api.Model(c)
-    st = dict(window.base)
-    st["th"] = th0
-    m.set_state(st)
+    m.set_state({k: v for k, v in window.base.items() if k != "th"})
+    _put(m, "th", th0)
     m.set_timestep(window.timestep)
     return m
 
@@ -40,30 +55,28 @@ def _model(window: Window, th0: np.ndarray, rmlmax: float) -> api.Model:
 class MoncWindow(torch.autograd.Function):
     @staticmethod
     def forward(ctx, th0: torch.Tensor, rmlmax: torch.Tensor, window: Window):
-        th0_np = th0.detach().to("cpu", torch.float64).numpy()
+        th_in = th0.detach().to(torch.float64)
         r = float(rmlmax.detach().cpu())
-        m = _model(window, th0_np, r)
+        m = _model(window, th_in, r)
         m.step(window.nsteps)
-        outs = [torch.from_numpy(m.download(f)) for f in ("u", "v", "w", "th")]
+        outs = [_get(m, f, th0.device) for f in ("u", "v", "w", "th")]
         m.close()
         ctx.window = window
-        ctx.th0 = th0_np
+        ctx.th0 = th_in
         ctx.r = r
         ctx.device = th0.device
-        return tuple(o.to(th0.device) for o in outs)
+        return tuple(outs)
 
     @staticmethod
     def backward(ctx, gu, gv, gw, gth):
         window = ctx.window
         m = _model(window, ctx.th0, ctx.r)
-        shape = ctx.th0.shape
         seeds = {"u": gu, "v": gv, "w": gw, "th": gth}
         for f in api.STATE_FIELDS:
             g = seeds.get(f)
-            arr = np.zeros(shape) if g is None else g.detach().to("cpu", torch.float64).numpy()
-            m.upload("adj:" + f, arr)
+            _put(m, "adj:" + f, torch.zeros_like(ctx.th0) if g is None else g)
         rbar = m.adjoint_run(window.nsteps, window.checkpoint_interval)
-        th_bar = torch.from_numpy(m.download("adj:th")).to(ctx.device)
+        th_bar = _get(m, "adj:th", ctx.device)
         m.close()
         return th_bar, torch.tensor(rbar, dtype=torch.float64, device=ctx.device), None
 

@@ -541,11 +541,15 @@ static int upload(mgpu_handle* h, DevState<T>& d, int id, const double* host, in
   if (!dst) return fail(h, MGPU_ERR_ARGUMENT, "unknown field id");
   const int nx = h->cfg.nx, ny = h->cfg.ny, nz = h->cfg.nz;
   const long long n = (long long)nx * ny * nz;
-  if (layout == MGPU_LAYOUT_XFAST) {
+  if (layout == MGPU_LAYOUT_XFAST || layout == MGPU_LAYOUT_DEVICE) {
+    const cudaMemcpyKind kind = layout == MGPU_LAYOUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (sizeof(T) == sizeof(double)) {
-      CK(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(dst, host, n * sizeof(double), kind, h->stream));
+    } else if (layout == MGPU_LAYOUT_DEVICE) {
+      k_convert<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(host, dst, n);
+      h->launches++;
     } else {
-      CK(cudaMemcpyAsync(h->xfer, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->xfer, host, n * sizeof(double), kind, h->stream));
       k_convert<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->xfer, dst, n);
       h->launches++;
     }
@@ -570,13 +574,17 @@ static int download(mgpu_handle* h, DevState<T>& d, int id, double* host, int la
   if (!src) return fail(h, MGPU_ERR_ARGUMENT, "unknown field id");
   const int nx = h->cfg.nx, ny = h->cfg.ny, nz = h->cfg.nz;
   const long long n = (long long)nx * ny * nz;
-  if (layout == MGPU_LAYOUT_XFAST) {
+  if (layout == MGPU_LAYOUT_XFAST || layout == MGPU_LAYOUT_DEVICE) {
+    const cudaMemcpyKind kind = layout == MGPU_LAYOUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (sizeof(T) == sizeof(double)) {
-      CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(host, src, n * sizeof(double), kind, h->stream));
+    } else if (layout == MGPU_LAYOUT_DEVICE) {
+      k_convert_back<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(src, host, n);
+      h->launches++;
     } else {
       k_convert_back<T><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(src, h->xfer, n);
       h->launches++;
-      CK(cudaMemcpyAsync(host, h->xfer, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(host, h->xfer, n * sizeof(double), kind, h->stream));
     }
   } else if (layout == MGPU_LAYOUT_MONC) {
     long long nm = (long long)(nx + 4) * (ny + 4) * nz;

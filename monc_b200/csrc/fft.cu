@@ -13,6 +13,7 @@
 // pencilfft.F90:276-332); the solve is linear with real coefficients that depend only on
 // |kx|, |ky|, so this complex half-spectrum form gives the same field up to rounding.
 // Level 1 is transformed too: its non-mean modes pass through unchanged, its mean is zeroed.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -279,17 +280,27 @@ __global__ void __launch_bounds__(line_block(LOGN)) k_fft_x_inv(T* __restrict__ 
   const long long pr = (long long)blockIdx.x * L + line;
   const bool ok = pr < (long long)nz * pairs;
   const int k = ok ? (int)(pr / pairs) + 1 : 1, jr = ok ? 2 * (int)(pr % pairs) : 0;
-  constexpr int nxh = N / 2 + 1;
-  for (int m = j; m < nxh; m += G) {
-    C a, b;
-    if (ok) {
+  constexpr int nxh = N / 2 + 1, NM = (nxh + G - 1) / G;
+  // every bin this thread needs is loaded before the first is used, so that the loads are in
+  // flight together rather than one DRAM round trip per bin
+  C av[NM], bv[NM];
+#pragma unroll
+  for (int q = 0; q < NM; ++q) {
+    const int m = j + q * G;
+    if (ok && m < nxh) {
       int w;
       const C* in = spec + spec_x_offset(m, nxh, nblk, ny, nz, k, jr, &w);
-      a = in[0];
-      b = in[w];
+      av[q] = in[0];
+      bv[q] = in[w];
     } else {
-      a.x = a.y = b.x = b.y = (T)0;
+      av[q].x = av[q].y = bv[q].x = bv[q].y = (T)0;
     }
+  }
+#pragma unroll
+  for (int q = 0; q < NM; ++q) {
+    const int m = j + q * G;
+    if (m >= nxh) break;
+    C a = av[q], b = bv[q];
     if (m == 0 || m == N / 2) { a.y = (T)0; b.y = (T)0; }
     C z;
     z.x = a.x - b.y;
@@ -707,12 +718,22 @@ __device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src) { 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// tridiagonal launch shape: TRI_TB columns (threads) per block, TRI_KC levels per staged chunk
-constexpr int TRI_TB = 128, TRI_KC = 16;
-constexpr size_t TRI_SMEM = (size_t)2 * TRI_KC * TRI_TB * (sizeof(double2) + sizeof(double));
+// tridiagonal launch shape: TRI_TB columns (threads) per block, TRI_KC levels per staged chunk,
+// TRI_NS chunks in the ring (TRI_NS - 1 of them in flight while one is used).  Two blocks of 112
+// fit an SM, so the 33,024 columns of a 256 x 256 grid are one wave on 148 SMs.
+constexpr int TRI_TB = 112, TRI_KC = 8, TRI_NS = 4;
+constexpr size_t TRI_SMEM = (size_t)TRI_NS * TRI_KC * TRI_TB * (sizeof(double2) + sizeof(double));
+// the staging ring (or the mean mode's column), then czb, cza, czg of levels 0 .. nz+1
 template <typename C>
-static size_t tri_smem_bytes(int nz) { return std::max(TRI_SMEM, (size_t)nz * sizeof(C)); }
+__host__ __device__ constexpr size_t tri_coef_off(int nz) {
+  return ((TRI_SMEM > (size_t)nz * sizeof(C) ? TRI_SMEM : (size_t)nz * sizeof(C)) + 15) & ~(size_t)15;
+}
+template <typename C>
+static size_t tri_smem_bytes(int nz) { return tri_coef_off<C>(nz) + 3 * (size_t)(nz + 2) * sizeof(double); }
+constexpr size_t TRI_SMEM_MAX = TRI_SMEM + 3 * (size_t)(MGPU_MAX_NZ + 2) * sizeof(double);
 template <typename T>
 __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restrict__ s1buf, const double* __restrict__ b1,
                           const double* __restrict__ prof, int prof_stride, int nx, int ny, int nz, int transpose,
@@ -726,8 +747,8 @@ static void ensure_tri_attr() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
   std::lock_guard<std::mutex> lock(mu);
   if (done[dev]) return;
-  cudaFuncSetAttribute(k_tridiag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM);
-  cudaFuncSetAttribute(k_tridiag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM);
+  cudaFuncSetAttribute(k_tridiag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM_MAX);
+  cudaFuncSetAttribute(k_tridiag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM_MAX);
   done[dev] = true;
 }
 __device__ __forceinline__ unsigned char* tri_smem() {
@@ -798,9 +819,17 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   typedef typename Cx<T>::t C;
   const int nxh = nx / 2 + 1;
   const long long lstride = (long long)rpb * ncols;   // level stride of the spectrum
-  const double* czb = prof + P_CZB * prof_stride;
-  const double* cza = prof + P_CZA * prof_stride;
-  const double* czg = prof + P_CZG * prof_stride;
+  // the three coefficient profiles, read at every level of every column, from shared memory
+  const int cs = nz + 2;
+  double* cf = reinterpret_cast<double*>(tri_smem() + tri_coef_off<C>(nz));
+  for (int q = threadIdx.x; q < 3 * cs; q += blockDim.x) {
+    const int r = q / cs, kk = q - r * cs;
+    cf[q] = prof[(r == 0 ? P_CZB : (r == 1 ? P_CZA : P_CZG)) * prof_stride + kk];
+  }
+  __syncthreads();
+  const double* czb = cf;
+  const double* cza = cf + cs;
+  const double* czg = cf + 2 * cs;
   if (kx0 == 0 && blockIdx.x == gridDim.x - 1) {
     // the mean mode is one sequential recurrence over the levels: stage its column (row 0,
     // column 0 of every level) in shared memory so that no step of it waits on a global load
@@ -826,20 +855,27 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
   const long long bstride = (long long)(ny / 2 + 1) * nxh;
   const double* bcol = b1 + (long long)kyi * nxh + kx;
   // Every level a thread needs (spectrum or s1, and the pivot) is staged in shared memory by
-  // cp.async, TRI_KC levels per chunk, the next chunk in flight while this one is used.  Each
+  // cp.async, TRI_KC levels per chunk, TRI_NS - 1 chunks in flight while one is used.  Each
   // thread copies and reads only its own slots, so no block barrier is involved.
   // Slots are 16 bytes whatever the spectrum type, so that a thread's forward slots (spectrum)
   // and backward slots (s1) are the same bytes and no thread's slot overlaps another's.
   unsigned char* raw = tri_smem();
-  double2* sbuf = reinterpret_cast<double2*>(raw);    // [2][TRI_KC][TRI_TB] 16-byte slots
-  double* bbuf = reinterpret_cast<double*>(raw + (size_t)2 * TRI_KC * TRI_TB * sizeof(double2));
+  double2* sbuf = reinterpret_cast<double2*>(raw);    // [TRI_NS][TRI_KC][TRI_TB] 16-byte slots
+  double* bbuf = reinterpret_cast<double*>(raw + (size_t)TRI_NS * TRI_KC * TRI_TB * sizeof(double2));
   const int t = threadIdx.x;
-  auto slot = [&](int ch, int q) { return ((ch & 1) * TRI_KC + q) * TRI_TB + t; };
+  auto slot = [&](int ch, int q) { return ((ch % TRI_NS) * TRI_KC + q) * TRI_TB + t; };
   auto fslot = [&](int ch, int q) { return reinterpret_cast<C*>(sbuf + slot(ch, q)); };
-  // forward elimination s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1) for k = 3..nz
+  // forward elimination s1(k) = pt(k) - czb(k)*s1(k-1)*b1(k-1) for k = 3..nz.  An FP64 spectrum
+  // takes s1(k) in place of pt(k), which the sweep has read by then: the column's one array then
+  // stays in L2 between the two sweeps, where a separate s1 array would double the footprint.  An
+  // FP32 spectrum keeps s1 in FP64 in s1buf.
+  constexpr bool in_place = sizeof(C) == sizeof(double2);
+  auto s1_at = [&](int k) -> double2* {
+    return in_place ? reinterpret_cast<double2*>(sp + (long long)(k - 1) * lstride) : s1buf + col + (long long)(k - 1) * plane;
+  };
   C v = sp[lstride];
   double sr = (double)v.x, si = (double)v.y;
-  s1buf[col + plane] = make_double2(sr, si);
+  if (!in_place) *s1_at(2) = make_double2(sr, si);
   const int nch = (nz - 2 + TRI_KC - 1) / TRI_KC;
   auto issue_fwd = [&](int ch) {
     for (int q = 0; q < TRI_KC; ++q) {
@@ -851,11 +887,14 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
     }
     cp_async_commit();
   };
-  issue_fwd(0);
-  for (int ch = 0; ch < nch; ++ch) {
-    if (ch + 1 < nch) issue_fwd(ch + 1);
+  for (int c = 0; c < TRI_NS - 1; ++c) {
+    if (c < nch) issue_fwd(c);
     else cp_async_commit();
-    cp_async_wait_1();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + TRI_NS - 1 < nch) issue_fwd(ch + TRI_NS - 1);
+    else cp_async_commit();
+    cp_async_wait<TRI_NS - 1>();
 #pragma unroll 4
     for (int q = 0; q < TRI_KC; ++q) {
       const int k = 3 + ch * TRI_KC + q;
@@ -864,7 +903,7 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
         const double bq = bbuf[slot(ch, q)];
         sr = (double)vq.x - lo[k] * sr * bq;
         si = (double)vq.y - lo[k] * si * bq;
-        s1buf[col + (long long)(k - 1) * plane] = make_double2(sr, si);
+        *s1_at(k) = make_double2(sr, si);
       }
     }
   }
@@ -880,17 +919,20 @@ __global__ void k_tridiag(typename Cx<T>::t* __restrict__ spec, double2* __restr
     for (int q = 0; q < TRI_KC; ++q) {
       const int k = nz - 1 - ch * TRI_KC - q;
       if (k >= 2) {
-        cp_async_16(sbuf + slot(ch, q), s1buf + col + (long long)(k - 1) * plane);
+        cp_async_16(sbuf + slot(ch, q), s1_at(k));
         cp_async_8(bbuf + slot(ch, q), bcol + (long long)k * bstride);
       }
     }
     cp_async_commit();
   };
-  issue_bwd(0);
-  for (int ch = 0; ch < nch; ++ch) {
-    if (ch + 1 < nch) issue_bwd(ch + 1);
+  for (int c = 0; c < TRI_NS - 1; ++c) {
+    if (c < nch) issue_bwd(c);
     else cp_async_commit();
-    cp_async_wait_1();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + TRI_NS - 1 < nch) issue_bwd(ch + TRI_NS - 1);
+    else cp_async_commit();
+    cp_async_wait<TRI_NS - 1>();
 #pragma unroll 4
     for (int q = 0; q < TRI_KC; ++q) {
       const int k = nz - 1 - ch * TRI_KC - q;
@@ -978,7 +1020,8 @@ int fft_plan_create(FftPlanDev& pl, const Scalars& s, const RefState& rs, bool f
   const size_t plane = (size_t)s.ny * pl.nxh;
   const size_t cs = fp32 ? sizeof(float2) : sizeof(double2);
   if (cudaMalloc(&pl.spec, cs * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
-  if (cudaMalloc(&pl.s1, sizeof(double2) * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
+  // an FP64 spectrum holds the Thomas forward-elimination values in place (k_tridiag)
+  if (fp32 && cudaMalloc(&pl.s1, sizeof(double2) * plane * s.nz) != cudaSuccess) return MGPU_ERR_CUDA;
   return plan_tables(pl, rs);
 }
 
@@ -1067,34 +1110,68 @@ template void slab_solve_columns<float>(const FftPlanDev&, const Scalars&, void*
                                         int64_t*);
 
 // ---- horizontal-mean diagnostics: one block per level, FP64 accumulation in a fixed order ----
+// Level sums split over a cluster of PSPLIT blocks (one cluster per level): block r sums its
+// contiguous share of the level's points, each thread in a fixed stride order and the block by a
+// tree; block 0 then adds the PSPLIT partial sums in rank order through distributed shared memory.
+// Deterministic, and a level keeps PSPLIT blocks busy where one block per level left most of the
+// GPU idle.
+constexpr int PSPLIT = 8, PRED_T = 256;
+
+template <int NV>
+__device__ __forceinline__ void block_tree(double (*sh)[PRED_T]) {
+  __syncthreads();
+  for (int h = PRED_T / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+#pragma unroll
+      for (int q = 0; q < NV; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + h];
+    __syncthreads();
+  }
+}
+
+// the cluster's total of sh[q][0] over its blocks, valid in block 0 (thread 0)
+template <int NV>
+__device__ __forceinline__ void cluster_total(double (*sh)[PRED_T], double* tot) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  cluster.sync();
+  if (cluster.block_rank() == 0 && threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) tot[q] = 0.0;
+    for (int r = 0; r < PSPLIT; ++r) {
+      double(*rs)[PRED_T] = cluster.map_shared_rank(sh, r);
+#pragma unroll
+      for (int q = 0; q < NV; ++q) tot[q] += rs[q][0];
+    }
+  }
+  cluster.sync();  // no block leaves while block 0 reads its partial sums
+}
+
 template <typename T>
-__global__ void k_diagnostics(const T* __restrict__ th, const T* __restrict__ w, const double* __restrict__ prof,
-                              int prof_stride, long long plane, long long first, long long count, double* out_th,
-                              double* out_w2) {
+__global__ void __cluster_dims__(PSPLIT, 1, 1) __launch_bounds__(PRED_T)
+    k_diagnostics(const T* __restrict__ th, const T* __restrict__ w, const double* __restrict__ prof, int prof_stride,
+                  long long plane, long long first, long long count, double* out_th, double* out_w2) {
   // the `count` points from `first` of each level: the whole plane, or a y-slab's interior rows
-  const int k = blockIdx.x + 1;
+  const int k = blockIdx.y + 1, r = blockIdx.x;
+  const long long chunk = (count + PSPLIT - 1) / PSPLIT;
+  const long long t0 = r * chunk, t1 = min(count, t0 + chunk);
   const T* thk = th + (long long)(k - 1) * plane + first;
   const T* wk = w + (long long)(k - 1) * plane + first;
   double a = 0.0, b = 0.0;
-  for (long long t = threadIdx.x; t < count; t += blockDim.x) {
+#pragma unroll 4
+  for (long long t = t0 + threadIdx.x; t < t1; t += PRED_T) {
     a += (double)thk[t];
     double wv = (double)wk[t];
     b += wv * wv;
   }
-  __shared__ double sa[256], sb[256];
-  sa[threadIdx.x] = a;
-  sb[threadIdx.x] = b;
-  __syncthreads();
-  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-    if ((int)threadIdx.x < h) {
-      sa[threadIdx.x] += sa[threadIdx.x + h];
-      sb[threadIdx.x] += sb[threadIdx.x + h];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    if (out_th) out_th[k - 1] = sa[0] / (double)count + prof[P_THREF * prof_stride + k];
-    if (out_w2) out_w2[k - 1] = sb[0] / (double)count;
+  __shared__ double sh[2][PRED_T];
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  block_tree<2>(sh);
+  double tot[2];
+  cluster_total<2>(sh, tot);
+  if (r == 0 && threadIdx.x == 0) {
+    if (out_th) out_th[k - 1] = tot[0] / (double)count + prof[P_THREF * prof_stride + k];
+    if (out_w2) out_w2[k - 1] = tot[1] / (double)count;
   }
 }
 
@@ -1102,7 +1179,8 @@ template <typename T>
 void launch_diagnostics(const Scalars& s, const T* th, const T* w, double* out_th, double* out_w2, cudaStream_t st,
                         int halo) {
   const long long first = (long long)halo * s.nx, count = (long long)(s.ny - 2 * halo) * s.nx;
-  k_diagnostics<T><<<s.nz, 256, 0, st>>>(th, w, s.prof, s.nz + 2, s.plane, first, count, out_th, out_w2);
+  k_diagnostics<T><<<dim3(PSPLIT, s.nz), PRED_T, 0, st>>>(th, w, s.prof, s.nz + 2, s.plane, first, count, out_th,
+                                                          out_w2);
 }
 template void launch_diagnostics<double>(const Scalars&, const double*, const double*, double*, double*, cudaStream_t,
                                          int);
@@ -1112,30 +1190,31 @@ template <typename T>
 struct MeanFields {
   const T* f[1 + MGPU_MAX_Q];
 };
-template <typename T>
 // the mean over `count` points of each level starting `off` points into the level
-__global__ void k_level_means(MeanFields<T> mf, long long plane, long long off, long long count, int stride,
-                              double* out) {
-  const int k = blockIdx.x + 1, row = blockIdx.y;
+template <typename T>
+__global__ void __cluster_dims__(PSPLIT, 1, 1) __launch_bounds__(PRED_T)
+    k_level_means(MeanFields<T> mf, long long plane, long long off, long long count, int stride, double* out) {
+  const int k = blockIdx.y + 1, row = blockIdx.z, r = blockIdx.x;
+  const long long chunk = (count + PSPLIT - 1) / PSPLIT;
+  const long long t0 = r * chunk, t1 = min(count, t0 + chunk);
   const T* fk = mf.f[row] + (long long)(k - 1) * plane + off;
   double a = 0.0;
-  for (long long t = threadIdx.x; t < count; t += blockDim.x) a += (double)fk[t];
-  __shared__ double sa[256];
-  sa[threadIdx.x] = a;
-  __syncthreads();
-  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-    if ((int)threadIdx.x < h) sa[threadIdx.x] += sa[threadIdx.x + h];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[(long long)row * stride + k] = sa[0] / (double)count;
+#pragma unroll 4
+  for (long long t = t0 + threadIdx.x; t < t1; t += PRED_T) a += (double)fk[t];
+  __shared__ double sh[1][PRED_T];
+  sh[0][threadIdx.x] = a;
+  block_tree<1>(sh);
+  double tot[1];
+  cluster_total<1>(sh, tot);
+  if (r == 0 && threadIdx.x == 0) out[(long long)row * stride + k] = tot[0] / (double)count;
 }
 template <typename T>
 void launch_level_means(const Scalars& s, const T* th, T* const* q, int nq, double* out, cudaStream_t st, int halo) {
   MeanFields<T> mf{};
   mf.f[0] = th;
   for (int n = 0; n < nq; ++n) mf.f[1 + n] = q[n];
-  k_level_means<T><<<dim3(s.nz, 1 + nq), 256, 0, st>>>(mf, s.plane, (long long)halo * s.nx,
-                                                       (long long)(s.ny - 2 * halo) * s.nx, s.nz + 2, out);
+  k_level_means<T><<<dim3(PSPLIT, s.nz, 1 + nq), PRED_T, 0, st>>>(mf, s.plane, (long long)halo * s.nx,
+                                                                  (long long)(s.ny - 2 * halo) * s.nx, s.nz + 2, out);
 }
 template void launch_level_means<double>(const Scalars&, const double*, double* const*, int, double*, cudaStream_t, int);
 template void launch_level_means<float>(const Scalars&, const float*, float* const*, int, double*, cudaStream_t, int);
@@ -1152,7 +1231,7 @@ template void launch_diagnostics<float>(const Scalars&, const float*, const floa
 // their step loop must not meet the device-wide synchronisation that cudaFree implies.  They can
 // still solve for the pressure: the caller passes the right-hand side (overwritten with the
 // solution) and the vertical coefficients, all in device memory it owns, and every piece of
-// working storage (spectra, Thomas scratch, pivots, twiddles, the coefficient block) lives in the
+// working storage (the spectrum, pivots, twiddles, the coefficient block) lives in the
 // fixed file-scope array below.  That array is part of the library image: every GPU that loads
 // the library holds MGPU_NOALLOC_SCRATCH_BYTES until the process exits.
 // =============================================================================================
@@ -1241,7 +1320,7 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   const size_t plane = (size_t)ny * nxh;
   const int stride = nz + 2;
   const size_t b_spec = align256(sizeof(double2) * plane * nz);
-  const size_t b_s1 = align256(sizeof(double2) * plane * nz);
+  const size_t b_s1 = 0;  // the FP64 column solve keeps its elimination values in the spectrum
   const size_t b_b1 = align256(sizeof(double) * (size_t)(nz + 1) * nyh * nxh);
   const size_t b_twx = align256(sizeof(double2) * nx);
   const size_t b_twy = align256(sizeof(double2) * ny);
@@ -1267,7 +1346,7 @@ extern "C" int mgpu_poisson_fft_noalloc(double* p, int32_t nx, int32_t ny, int32
   }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   double2* spec = reinterpret_cast<double2*>(base);
-  double2* s1 = reinterpret_cast<double2*>(base + b_spec);
+  double2* s1 = nullptr;
   double* b1 = reinterpret_cast<double*>(base + b_spec + b_s1);
   double2* twx = reinterpret_cast<double2*>(base + b_spec + b_s1 + b_b1);
   double2* twy = reinterpret_cast<double2*>(base + b_spec + b_s1 + b_b1 + b_twx);

@@ -98,7 +98,10 @@ __device__ bool last_block_sums(IterScalars* st, const double* partials, int nbl
   double v[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
+    // the loads are independent of the running sum: unrolled, eight of them are in flight at once
+    // instead of one L2 round trip per step of the ~60-step loop
     double a = 0.0;
+#pragma unroll 8
     for (int b = tid; b < nblocks; b += NTH) a += __ldcg(partials + (long long)q * nblocks + b);
     v[q] = a;
   }

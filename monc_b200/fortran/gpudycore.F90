@@ -31,7 +31,7 @@ module gpudycore_mod
   integer(c_int32_t), parameter :: MGPU_SOLVER_FFT = 0, MGPU_SOLVER_ITERATIVE = 1
   integer(c_int32_t), parameter :: MGPU_ITER_BICGSTAB = 0, MGPU_ITER_CG = 1
   integer(c_int32_t), parameter :: MGPU_ADVECT_PW = 0, MGPU_ADVECT_TVD = 1
-  integer(c_int32_t), parameter :: MGPU_LAYOUT_MONC = 1
+  integer(c_int32_t), parameter :: MGPU_LAYOUT_XFAST = 0, MGPU_LAYOUT_MONC = 1, MGPU_LAYOUT_DEVICE = 2
   integer(c_int32_t), parameter :: MGPU_U = 0, MGPU_V = 1, MGPU_W = 2, MGPU_TH = 3, MGPU_ZU = 4, &
        MGPU_ZV = 5, MGPU_ZW = 6, MGPU_ZTH = 7, MGPU_P = 8, MGPU_Q0 = 32, MGPU_ZQ0 = 48
 
