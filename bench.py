@@ -42,8 +42,10 @@ METRIC = "Mpoint-steps/s (MONC dynamical-core timestep, 1 B200)"
 # kernel, for the dry centred step.  The horizontal transforms are counted as what they must move:
 # the field in and the half spectrum out (forward), and back (inverse), whether one fused kernel per
 # level or an x and a y kernel does it.
+# When the forward x transform forms the pressure source itself ("source_fft_fwd"), it reads zu,
+# zv, zw and writes the half spectrum.
 KERNEL_PASSES = {"subgrid": 6, "dynamics_scalars": 8, "dynamics_momentum": 11, "pressure_source": 4,
-                 "fft_fwd": 2, "tridiag": 2, "fft_inv": 2, "pstep_swap": 16}
+                 "fft_fwd": 2, "source_fft_fwd": 4, "tridiag": 2, "fft_inv": 2, "pstep_swap": 16}
 
 
 def kernel_times(stages: dict) -> dict:
@@ -57,6 +59,9 @@ def kernel_times(stages: dict) -> dict:
         out["fft_fwd"] = stages["fft_x_fwd"] + stages.get("fft_y_fwd", 0.0)
     if "fft_x_inv" in stages:
         out["fft_inv"] = stages["fft_x_inv"] + stages.get("fft_y_inv", 0.0)
+    if "fft_fwd" in out and stages.get("pressure_source", 1.0) < 0.01:
+        # no source kernel (the stage's events enclose nothing): the forward transform formed it
+        out["source_fft_fwd"] = out.pop("fft_fwd") + out.pop("pressure_source", 0.0)
     return out
 
 
@@ -322,6 +327,7 @@ def run_ours(args):
     r64 = results["fp64"]
     peak, peak_kind = measured_peaks()
     kt = kernel_times(r64["stages"])
+    step_passes = sum(KERNEL_PASSES[k] for k in kt)
     dom = max(kt, key=lambda k: kt[k])
     dom_ms = kt[dom]
     dom_bytes = KERNEL_PASSES[dom] * 8 * npts
@@ -366,8 +372,8 @@ def run_ours(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic,
                      "algorithmic_bytes_per_launch": dom_bytes},
-        "step_roofline": {"algorithmic_bytes_per_point": sum(KERNEL_PASSES.values()) * 8,
-                          "frac": round(sum(KERNEL_PASSES.values()) * 8 * npts / (r64["ms_per_step"] * 1e-3) / 1e9 / peak, 4)},
+        "step_roofline": {"algorithmic_bytes_per_point": step_passes * 8,
+                          "frac": round(step_passes * 8 * npts / (r64["ms_per_step"] * 1e-3) / 1e9 / peak, 4)},
         "kernels": per_kernel,
         "stages_ms": {k: round(v, 4) for k, v in r64["stages"].items()},
         "cpu_baseline": cpu,

@@ -613,9 +613,9 @@ static void swap_scalar_buffers(DevState<T>& d, int nq) {
 }
 
 template <typename T>
-static int pressure_solve(mgpu_handle* h, T* p) {
+static int pressure_solve(mgpu_handle* h, T* p, const SourceFields<T>* src = nullptr) {
   if (h->cfg.solver == MGPU_SOLVER_FFT) {
-    fft_solve<T>(h->fft, h->sc, p, h->stream, &h->launches, h->profiling ? &h->ev[3] : nullptr);
+    fft_solve<T>(h->fft, h->sc, p, h->stream, &h->launches, h->profiling ? &h->ev[3] : nullptr, false, src);
     return MGPU_OK;
   }
   int rc = iter_solve<T>(h->iter, h->sc, p, h->stream, &h->launches, &h->solver_iterations, &h->solver_residual);
@@ -753,11 +753,17 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
                                                  h->sc.vgal, 1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d,
                                                  h->stream);
   }
-  if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
-  else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
-  h->launches += 1;
+  // The FFT solve of a power-of-two nx forms the source inside its first transform (fast
+  // build); the reproducible build keeps the source kernel, whose rounding the oracle matches.
+  const bool src_in_fft = !h->cfg.reproducible && h->cfg.solver == MGPU_SOLVER_FFT && (h->cfg.nx & (h->cfg.nx - 1)) == 0;
+  const SourceFields<T> src{d.zu_n, d.zv_n, d.zw_n};
+  if (!src_in_fft) {
+    if (h->cfg.reproducible) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
+    else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
+    h->launches += 1;
+  }
   if (h->cfg.solver != MGPU_SOLVER_FFT) mark(3);
-  int rc = pressure_solve<T>(h, d.p);
+  int rc = pressure_solve<T>(h, d.p, src_in_fft ? &src : nullptr);
   if (rc) return rc;
   if (h->cfg.solver != MGPU_SOLVER_FFT) mark(8);
   // cfltest ends the solver group.  Where its evaluation can move the frame the pressure step

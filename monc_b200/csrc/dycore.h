@@ -52,11 +52,20 @@ struct FftPlanDev {
 bool fft_length_ok(int n);
 int fft_plan_create(FftPlanDev& plan, const Scalars& s, const RefState& rs, bool fp32);
 void fft_plan_destroy(FftPlanDev& plan);
+// The stepped z-velocities from which the fused step forms the pressure source.
+template <typename T>
+struct SourceFields {
+  const T* zu;
+  const T* zv;
+  const T* zw;
+};
 // evs: NULL, or 6 events recorded before, between and after the five kernels.  transpose: apply
-// the transpose of the solve (the adjoint of the pressure solve) instead.
+// the transpose of the solve (the adjoint of the pressure solve) instead.  src: when given (and
+// nx is a power of two), the forward x transform forms the pressure source from these fields
+// itself and p's input is not read; the solution is written to p as always.
 template <typename T>
 void fft_solve(const FftPlanDev& plan, const Scalars& s, T* p, cudaStream_t st, int64_t* launches,
-               cudaEvent_t* evs = nullptr, bool transpose = false);
+               cudaEvent_t* evs = nullptr, bool transpose = false, const SourceFields<T>* src = nullptr);
 
 // horizontal means of th (row 0) and q[0..nq-1] (rows 1..nq) per level into out[row*(nz+2) + k],
 // over the rows halo .. ny-halo-1 (all rows for halo 0)

@@ -263,6 +263,81 @@ __global__ void __launch_bounds__(line_block(LOGN)) k_fft_x_fwd(const T* __restr
   }
 }
 
+// ---- forward x of the pressure source, formed on the fly ------------------------------------
+// The fused step's source p = (cx (zu(i) - zu(i-1)) + cy (zv(j) - zv(j-1)) + 4 (tzc2 zw(k) -
+// tzc1 zw(k-1))) * timec (k_f_pressure_source, the same expression in the same order) is
+// computed for a row pair straight into its shared-memory line, which the x transform then
+// reads: the source never goes through global memory.  One domain (all ny rows), plain
+// [nz][ny][nx/2+1] spectrum.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(line_block(LOGN)) k_fft_x_fwd_src(Scalars s, SourceFields<T> f,
+                                                                  typename Cx<T>::t* __restrict__ spec,
+                                                                  const typename Cx<T>::t* __restrict__ tw) {
+  typedef typename Cx<T>::t C;
+  typedef LineShape<LOGN> S;
+  constexpr int N = S::N, G = S::G, L = line_lines(LOGN);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int line = threadIdx.x / G, j = threadIdx.x - line * G;
+  C* buf = reinterpret_cast<C*>(smem_raw) + line * S::LPL;
+  const int ny = s.ny, nz = s.nz, pairs = ny / 2;
+  const long long pr = (long long)blockIdx.x * L + line;
+  const bool ok = pr < (long long)nz * pairs;
+  const int k = ok ? (int)(pr / pairs) + 1 : 1, jr = ok ? 2 * (int)(pr % pairs) : 0;
+  const long long plane = s.plane;
+  const T timec = s.forward ? (T)(1.0 / s.dtm) : (T)(1.0 / (2.0 * s.dtm));
+  const T cx = (T)s.cx, cy = (T)s.cy;
+  const T tzc1 = (T)__ldg(s.prof + P_TZC1 * (nz + 2) + k), tzc2 = (T)__ldg(s.prof + P_TZC2 * (nz + 2) + k);
+  const long long lv = (long long)(k - 1) * plane;
+  const int jm = jr == 0 ? ny - 1 : jr - 1;
+  const T* __restrict__ u0 = f.zu + lv + (long long)jr * N;
+  const T* __restrict__ u1 = u0 + N;
+  const T* __restrict__ vm = f.zv + lv + (long long)jm * N;
+  const T* __restrict__ v0 = f.zv + lv + (long long)jr * N;
+  const T* __restrict__ v1 = v0 + N;
+  const T* __restrict__ w0 = f.zw + lv + (long long)jr * N;
+  const T* __restrict__ w1 = w0 + N;
+  auto src = [&](const T* u, const T* vlo, const T* v, const T* w, int e) {
+    const int em = e == 0 ? N - 1 : e - 1;
+    T pp = (T)0.0;
+    pp = pp + cx * (__ldg(u + e) - __ldg(u + em));
+    pp = pp + cy * (__ldg(v + e) - __ldg(vlo + e));
+    pp = pp + (T)4.0 * (tzc2 * __ldg(w + e) - tzc1 * __ldg(w - plane + e));
+    return pp * timec;
+  };
+#pragma unroll 4
+  for (int q = 0; q < N / G; ++q) {
+    const int e = j + q * G;
+    C z;
+    if (ok && k > 1) {
+      z.x = src(u0, vm, v0, w0, e);
+      z.y = src(u1, v0, v1, w1, e);
+    } else {
+      z.x = (T)0;
+      z.y = (T)0;
+    }
+    buf[lpad(e)] = z;
+  }
+  __syncthreads();  // the line's points come from all G threads of the line
+  auto in = [&](int i) { return buf[lpad(i)]; };
+  auto out = [&](int i, C z) { buf[lpad(i)] = z; };
+  line_fft<C, LOGN, false, true, true>(j, buf, tw, in, out);
+  __syncthreads();
+  if (!ok) return;
+  constexpr int nxh = N / 2 + 1;
+  for (int m = j; m < nxh; m += G) {
+    const C zm = buf[lpad(m)];
+    const C zn = buf[lpad((N - m) & (N - 1))];
+    C a, b;
+    a.x = (T)0.5 * (zm.x + zn.x);
+    a.y = (T)0.5 * (zm.y - zn.y);
+    b.x = (T)0.5 * (zm.y + zn.y);
+    b.y = (T)0.5 * (zn.x - zm.x);
+    C* o = spec + ((long long)(k - 1) * ny + jr) * nxh + m;
+    o[0] = a;
+    o[nxh] = b;
+  }
+}
+
 // ---- inverse x: half spectra -> real rows (k, j), (k, j+1) -----------------------------
 // the inverse of k_fft_x_fwd, with the same row window and spectrum blocks; the imaginary parts
 // of the kx = 0 and kx = nx/2 bins are dropped (the Hermitian completion of fftnorth.F90:54-73)
@@ -630,6 +705,7 @@ static void ensure_line_attr() {
 #define MGPU_SET_ATTR(L)                                                                                  \
   cudaFuncSetAttribute(k_fft_x_fwd<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
   cudaFuncSetAttribute(k_fft_x_inv<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
+  cudaFuncSetAttribute(k_fft_x_fwd_src<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
   cudaFuncSetAttribute(k_fft_y<T, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L)); \
   cudaFuncSetAttribute(k_fft_y<T, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_smem<T>(L));
   MGPU_LOGN_CASES(MGPU_SET_ATTR)
@@ -668,6 +744,28 @@ static void launch_fft_x(bool inverse, int n, T* p, typename Cx<T>::t* spec, con
     break;
     MGPU_LOGN_CASES(MGPU_X_CASE)
 #undef MGPU_X_CASE
+    default: break;
+  }
+}
+
+// forward x-FFT of the pressure source formed from zu, zv, zw (power-of-two nx, one domain)
+template <typename T>
+static void launch_fft_x_src(const Scalars& s, const SourceFields<T>& f, typename Cx<T>::t* spec,
+                             const typename Cx<T>::t* tw, cudaStream_t st) {
+  const int logn = ilog2(s.nx);
+  ensure_line_attr<T>();
+  const long long pairs = (long long)s.nz * (s.ny / 2);
+  const int L = line_lines(logn);
+  const unsigned grid = (unsigned)((pairs + L - 1) / L);
+  const int block = line_block(logn);
+  const size_t smem = line_smem<T>(logn);
+  switch (logn) {
+#define MGPU_XS_CASE(LG)                                                        \
+  case LG:                                                                      \
+    k_fft_x_fwd_src<T, LG><<<grid, block, smem, st>>>(s, f, spec, tw);          \
+    break;
+    MGPU_LOGN_CASES(MGPU_XS_CASE)
+#undef MGPU_XS_CASE
     default: break;
   }
 }
@@ -1049,7 +1147,7 @@ void fft_plan_destroy(FftPlanDev& pl) {
 
 template <typename T>
 void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, int64_t* launches, cudaEvent_t* evs,
-               bool transpose) {
+               bool transpose, const SourceFields<T>* src) {
   typedef typename Cx<T>::t C;
   const bool f32 = sizeof(T) == 4;
   C* spec = reinterpret_cast<C*>(pl.spec);
@@ -1059,7 +1157,8 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   double2* s1 = pl.s1;
   auto mark = [&](int q) { if (evs) cudaEventRecord(evs[q], st); };
   mark(0);
-  launch_fft_x<T>(false, logx, p, spec, twx, s.ny, s.nz, s.ny, 0, 1, st);
+  if (src && is_pow2(s.nx)) launch_fft_x_src<T>(s, *src, spec, twx, st);
+  else launch_fft_x<T>(false, logx, p, spec, twx, s.ny, s.nz, s.ny, 0, 1, st);
   mark(1);
   launch_fft_y<T>(false, logy, spec, twy, pl.nxh, s.nz, s.ny, st);
   mark(2);
@@ -1072,8 +1171,10 @@ void fft_solve(const FftPlanDev& pl, const Scalars& s, T* p, cudaStream_t st, in
   *launches += 5;
 }
 
-template void fft_solve<double>(const FftPlanDev&, const Scalars&, double*, cudaStream_t, int64_t*, cudaEvent_t*, bool);
-template void fft_solve<float>(const FftPlanDev&, const Scalars&, float*, cudaStream_t, int64_t*, cudaEvent_t*, bool);
+template void fft_solve<double>(const FftPlanDev&, const Scalars&, double*, cudaStream_t, int64_t*, cudaEvent_t*, bool,
+                                const SourceFields<double>*);
+template void fft_solve<float>(const FftPlanDev&, const Scalars&, float*, cudaStream_t, int64_t*, cudaEvent_t*, bool,
+                               const SourceFields<float>*);
 
 // ---- y-slab decomposition: the solve split at the two transposes -------------------------
 template <typename T>
