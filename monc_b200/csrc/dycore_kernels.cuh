@@ -609,13 +609,21 @@ struct G {
   static_assert((PLANE * sizeof(T)) % 16 == 0, "planes start on 16-byte boundaries");
 };
 constexpr int RM = 4;              // momentum rings: levels k-1..k+1 live, k+2 in flight
-constexpr int RF = 4, RZF = 8;     // scalar kernel: u, v, w and diff rings; the scalar's ring (k-1..k+3)
+// Scalar kernel rings, each as deep as the levels it must hold (level k's faces, source and
+// diffusion read u, v at k..k+1, w at k-1..k+1, diff at k-1..k and the scalar at k-1..k+2), plus
+// the level in flight.  Slots are level mod depth.  With 18 planes the FP64 kernel fits three
+// CTAs on an SM.  A ring slot whose level is not live is never read (a centred accessor's
+// pointer to it aliases another slot).
+constexpr int RUV = 3, RW = 4, RD = 3, RZF = 5;
 constexpr int RP = 8;              // profile ring: levels k-1..k+2 live, k+3 staged
 // resident CTAs per SM the register budget is sized for (FP64: 2 x 256 threads x <= 128 registers)
 template <typename T>
 constexpr int min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
+// the scalar and Smagorinsky kernels fit 80 registers without spilling, and their shared memory
+// allows three CTAs per SM in FP64 too
+constexpr int min_ctas3() { return 3; }
 constexpr int M_PLANES = 7 * RM;   // u v w zu zv zw vis
-constexpr int S_PLANES = 4 * RF + RZF;  // u v w diff + scalar
+constexpr int S_PLANES = 2 * RUV + RW + RD + RZF;  // u v w diff + scalar
 template <typename T>
 constexpr size_t smag_smem() { return sizeof(T) * ((size_t)3 * RM * G<T>::PLANE + (size_t)RP * P_COUNT); }
 template <typename T>
@@ -673,6 +681,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// slot of level k (>= 0) in a ring of R planes: a mask for powers of two, an unsigned remainder
+// by a constant otherwise (a multiply and a shift)
+template <int R>
+__device__ __forceinline__ int ring_slot(int k) {
+  if constexpr ((R & (R - 1)) == 0) return k & (R - 1);
+  else return (int)((unsigned)k % (unsigned)R);
+}
 // One thread's share of staging a plane: a single 16-byte chunk.  The x halo is one whole
 // chunk on each side and nx is a multiple of the chunk, so no chunk straddles the periodic wrap.
 template <typename T>
@@ -694,7 +709,7 @@ struct Stager {
   // copy level k of field f into slot (k mod R) of the ring at `ring`
   template <int R>
   __device__ __forceinline__ void stage(T* ring, const T* __restrict__ f, long long plane, int k) const {
-    if (on) cp_async16(ring + (k & (R - 1)) * tiled::G<T>::PLANE + soff, f + (long long)(k - 1) * plane + goff);
+    if (on) cp_async16(ring + ring_slot<R>(k) * tiled::G<T>::PLANE + soff, f + (long long)(k - 1) * plane + goff);
   }
 };
 
@@ -713,8 +728,11 @@ __device__ __forceinline__ CProf<T> cprof(const T* ring, int k) {
 template <typename T, int R>
 __device__ __forceinline__ CRing<T> cring(const T* ring, int k, int co, int j, int i) {
   using Gt = tiled::G<T>;
-  return CRing<T>{ring + ((k - 1) & (R - 1)) * Gt::PLANE + co, ring + (k & (R - 1)) * Gt::PLANE + co,
-                  ring + ((k + 1) & (R - 1)) * Gt::PLANE + co, ring + ((k + 2) & (R - 1)) * Gt::PLANE + co, k, j, i};
+  // one remainder per ring and level; the neighbouring slots follow by wrapping
+  const int m0 = ring_slot<R>(k);
+  const int mm = m0 == 0 ? R - 1 : m0 - 1, m1 = m0 + 1 == R ? 0 : m0 + 1, m2 = m1 + 1 == R ? 0 : m1 + 1;
+  return CRing<T>{ring + mm * Gt::PLANE + co, ring + m0 * Gt::PLANE + co, ring + m1 * Gt::PLANE + co,
+                  ring + m2 * Gt::PLANE + co, k, j, i};
 }
 
 // Each CTA runs the levels kb..ke of its tile, kb = 2 + blockIdx.z * kchunk: splitting the level
@@ -846,7 +864,7 @@ struct ScalarJob {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_tiled(Scalars s, DevState<T> d,
+__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tiled(Scalars s, DevState<T> d,
                                                                                     int kchunk, ScalarJob<T> job) {
   using namespace tiled;
   using Gt = G<T>;
@@ -859,12 +877,11 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
   const int kb = 2 + (int)blockIdx.z * kchunk;
   const int ke = min(nz, kb + kchunk - 1);
   const long long plane = s.plane;
-  constexpr int FS = RF * Gt::PLANE;
   T* rU = sm;
-  T* rV = rU + FS;
-  T* rW = rV + FS;
-  T* rD = rW + FS;
-  T* rF = rD + FS;
+  T* rV = rU + RUV * Gt::PLANE;
+  T* rW = rV + RUV * Gt::PLANE;
+  T* rD = rW + RW * Gt::PLANE;
+  T* rF = rD + RD * Gt::PLANE;
   T* rP = rF + RZF * Gt::PLANE;  // profile ring
   T* FX = rP + RP * P_COUNT;     // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
   T* FY = FX + TY * (TX + 1);    // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
@@ -885,12 +902,15 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
   // at k-1 .. k+2; a chunk above level 2 also needs the z face below it (level kb-1).
   const int k0 = kb == 2 ? 1 : kb - 2;
   for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<RZF>(rF, job.zf, plane, kk);
+  // (the z face below the chunk reads w from level kb-2 but u and v from kb-1 up)
   for (int kk = k0; kk <= kb + 1 && kk <= nz; ++kk) {
-    sg.template stage<RF>(rU, d.u, plane, kk);
-    sg.template stage<RF>(rV, d.v, plane, kk);
-    sg.template stage<RF>(rW, d.w, plane, kk);
+    if (kk >= kb - 1) {
+      sg.template stage<RUV>(rU, d.u, plane, kk);
+      sg.template stage<RUV>(rV, d.v, plane, kk);
+    }
+    sg.template stage<RW>(rW, d.w, plane, kk);
   }
-  for (int kk = kb - 1; kk <= kb; ++kk) sg.template stage<RF>(rD, d.diff, plane, kk);
+  for (int kk = kb - 1; kk <= kb; ++kk) sg.template stage<RD>(rD, d.diff, plane, kk);
   if (tid < P_COUNT)
     for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
   const T dtm_x2 = (T)(2.0 * s.dtm);
@@ -917,16 +937,16 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
   if (kb > 2) {
     const int kz = kb - 1;
     const CProf<T> P = cprof<T>(rP, kz);
-    const CRing<T> U = cring<T, RF>(rU, kz, co, j, i), V = cring<T, RF>(rV, kz, co, j, i),
-                   W = cring<T, RF>(rW, kz, co, j, i);
+    const CRing<T> U = cring<T, RUV>(rU, kz, co, j, i), V = cring<T, RUV>(rV, kz, co, j, i),
+                   W = cring<T, RW>(rW, kz, co, j, i);
     const CRing<T> ZF = cring<T, RZF>(rF, kz, co, j, i);
     fz_lo = tvd_face_z<T>(s, P, U, V, W, ZF, dt, kz, j, i);
   }
   {
     // the cell sums of level kb
     const CProf<T> P = cprof<T>(rP, kb);
-    const CRing<T> U = cring<T, RF>(rU, kb, co, j, i), V = cring<T, RF>(rV, kb, co, j, i),
-                   W = cring<T, RF>(rW, kb, co, j, i);
+    const CRing<T> U = cring<T, RUV>(rU, kb, co, j, i), V = cring<T, RUV>(rV, kb, co, j, i),
+                   W = cring<T, RW>(rW, kb, co, j, i);
     T* C = CT + (kb & 1) * CN;
     C[own_cell] = cell_cfl_out<T>(s, P, U, V, W, kb, j, i);
     if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T>(s, P, U, V, W, kb, j0 - 1 + hr, i0 - 1 + hc);
@@ -936,18 +956,18 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_scalar_ti
   for (int k = kb; k <= ke; ++k) {
     if (k + 3 <= min(nz, ke + 2)) sg.template stage<RZF>(rF, job.zf, plane, k + 3);
     if (k + 2 <= min(nz, ke + 1)) {
-      sg.template stage<RF>(rU, d.u, plane, k + 2);
-      sg.template stage<RF>(rV, d.v, plane, k + 2);
-      sg.template stage<RF>(rW, d.w, plane, k + 2);
+      sg.template stage<RUV>(rU, d.u, plane, k + 2);
+      sg.template stage<RUV>(rV, d.v, plane, k + 2);
+      sg.template stage<RW>(rW, d.w, plane, k + 2);
     }
-    if (k + 1 <= min(nz, ke)) sg.template stage<RF>(rD, d.diff, plane, k + 1);
+    if (k + 1 <= min(nz, ke)) sg.template stage<RD>(rD, d.diff, plane, k + 1);
     const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
     T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
     const long long o = lin(s, k, j, i);
     const T fv = job.src ? (T)0.0 : __ldg(th + o);
     const CProf<T> P = cprof<T>(rP, k);
-    const CRing<T> U = cring<T, RF>(rU, k, co, j, i), V = cring<T, RF>(rV, k, co, j, i),
-                   W = cring<T, RF>(rW, k, co, j, i), DIFF = cring<T, RF>(rD, k, co, j, i);
+    const CRing<T> U = cring<T, RUV>(rU, k, co, j, i), V = cring<T, RUV>(rV, k, co, j, i),
+                   W = cring<T, RW>(rW, k, co, j, i), DIFF = cring<T, RD>(rD, k, co, j, i);
     const CRing<T> ZF = cring<T, RZF>(rF, k, co, j, i);
     // the cell sums of level k+1: the own cell's for the z face above, the table for the next level
     T c_hi = (T)0.0;
@@ -1038,7 +1058,7 @@ __global__ void __launch_bounds__(256) k_f_cloud_step(Scalars s, DevState<T> d) 
 // ring, the Richardson-number inputs (th, q) read at the column itself.  The chunk holding level
 // nz-1 also zeroes vis and diff at the top level.  Level 1 (lower_bc) is k_c_lower_bc.
 template <typename T>
-__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_smag_tiled(Scalars s, DevState<T> d,
+__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_smag_tiled(Scalars s, DevState<T> d,
                                                                                   int kchunk) {
   using namespace tiled;
   using Gt = G<T>;

@@ -221,35 +221,78 @@ __device__ __forceinline__ W apply_A(const Geom& g, const W* __restrict__ x, int
 
 __device__ __forceinline__ int block_id() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
 
+// The point kernels give each thread KZ consecutive levels of its column (blockIdx.z picks the
+// group), so that a reduction closes over a quarter as many block partials: with one level per
+// thread, the per-block fence, atomic and partial of ~16,000 blocks (256 x 256 x 64) made the
+// dot-product kernels three times slower than their memory traffic.
+constexpr int KZ = 4;
+__device__ __forceinline__ int kz_lo() { return 2 + (int)blockIdx.z * KZ; }
+__device__ __forceinline__ int kz_hi(const Geom& g) { return min(g.nz, kz_lo() + KZ - 1); }
+
 // r = b - A x, cr = r; sums <r, r> and <b, b>; initial scalars
 template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_init(Geom g, const W* __restrict__ x, const W* __restrict__ b, W* r, W* cr,
                                                     double* partials, int nblocks, IterScalars* st, double sc_floor) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
-    const W rv = b[o] - apply_A<W>(g, x, k, j, i);
-    r[o] = rv;
-    cr[o] = rv;
-    v[0] = (double)rv * (double)rv;
-    v[1] = (double)b[o] * (double)b[o];
-  }
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      const W rv = b[o] - apply_A<W>(g, x, k, j, i);
+      r[o] = rv;
+      cr[o] = rv;
+      v[0] += (double)rv * (double)rv;
+      v[1] += (double)b[o] * (double)b[o];
+    }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
   if (last_block_sums<2>(st, partials, nblocks, s)) finish_init(st, s, sc_floor);
 }
 
-// column LU solve of the vertical operator: out = M^-1 in (precond); `tmp` holds the forward sweep
+// column LU solve of the vertical operator: out = M^-1 in (precond); `tmp` holds the forward sweep.
+// A thread walks its column level by level; CH levels of its input are loaded before the first of
+// them is used, so that the loads are in flight together instead of one round trip per level
+// (one thread per column leaves too few warps to hide the latency otherwise).
+constexpr int CH = 8;
 template <typename W, class In>
 __device__ __forceinline__ void column_precond(const Geom& g, In in, W* tmp, int j, int i) {
   long long o = g.at(2, j, i);
   W sp = in(o) * (W)g.lud(2);
   tmp[o] = sp;
-  for (int k = 3; k <= g.nz; ++k) {
-    o += g.plane;
-    sp = (in(o) - (W)g.ad(k) * sp) * (W)g.lud(k);
-    tmp[o] = sp;
+  for (int k0 = 3; k0 <= g.nz; k0 += CH) {
+    W x[CH];
+#pragma unroll
+    for (int q = 0; q < CH; ++q)
+      if (k0 + q <= g.nz) x[q] = in(o + (long long)(q + 1) * g.plane);
+#pragma unroll
+    for (int q = 0; q < CH; ++q)
+      if (k0 + q <= g.nz) {
+        o += g.plane;
+        sp = (x[q] - (W)g.ad(k0 + q) * sp) * (W)g.lud(k0 + q);
+        tmp[o] = sp;
+      }
+  }
+}
+
+// back substitution sk(k) = tmp(k) - luu(k) sk(k+1) from the top level down to level 2;
+// out(o, sk) receives each level's value
+template <typename W, class Out>
+__device__ __forceinline__ void column_back(const Geom& g, const W* tmp, int j, int i, Out out) {
+  long long o = g.at(g.nz, j, i);
+  W sk = tmp[o];
+  out(o, sk);
+  for (int k0 = g.nz - 1; k0 >= 2; k0 -= CH) {
+    W t[CH];
+#pragma unroll
+    for (int q = 0; q < CH; ++q)
+      if (k0 - q >= 2) t[q] = tmp[o - (long long)(q + 1) * g.plane];
+#pragma unroll
+    for (int q = 0; q < CH; ++q)
+      if (k0 - q >= 2) {
+        o -= g.plane;
+        sk = t[q] - (W)g.luu(k0 - q) * sk;
+        out(o, sk);
+      }
   }
 }
 
@@ -266,14 +309,7 @@ __global__ void __launch_bounds__(NTH) k_bicg_direction(Geom g, const W* __restr
   if (first) column_precond<W>(g, [&](long long o) { return r[o]; }, tmp, j, i);
   else column_precond<W>(g, [&](long long o) { return r[o] - bo * v[o]; }, tmp, j, i);
   // back substitution, then pp = s + bet*pp
-  long long o = g.at(g.nz, j, i);
-  W sk = tmp[o];
-  pp[o] = first ? sk : sk + bet * pp[o];
-  for (int k = g.nz - 1; k >= 2; --k) {
-    o -= g.plane;
-    sk = tmp[o] - (W)g.luu(k) * sk;
-    pp[o] = first ? sk : sk + bet * pp[o];
-  }
+  column_back<W>(g, tmp, j, i, [&](long long o, W sk) { pp[o] = first ? sk : sk + bet * pp[o]; });
 }
 
 // iteration step 2: v = A pp, alf = rho / <cr, v>
@@ -281,14 +317,15 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_apply_dot(Geom g, const W* __restrict__ pp, const W* __restrict__ cr, W* v,
                                                          double* partials, int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double a[1] = {0.0};
-  if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
-    const W vv = apply_A<W>(g, pp, k, j, i);
-    v[o] = vv;
-    a[0] = (double)cr[o] * (double)vv;
-  }
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      const W vv = apply_A<W>(g, pp, k, j, i);
+      v[o] = vv;
+      a[0] += (double)cr[o] * (double)vv;
+    }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
   if (last_block_sums<1>(st, partials, nblocks, s)) finish_apply_dot(st, s);
@@ -307,14 +344,7 @@ __global__ void __launch_bounds__(NTH) k_bicg_half_step(Geom g, const W* __restr
     s_[o] = sv;
     return sv;
   }, tmp, j, i);
-  long long o = g.at(g.nz, j, i);
-  W ck = tmp[o];
-  cs[o] = ck;
-  for (int k = g.nz - 1; k >= 2; --k) {
-    o -= g.plane;
-    ck = tmp[o] - (W)g.luu(k) * ck;
-    cs[o] = ck;
-  }
+  column_back<W>(g, tmp, j, i, [&](long long o, W ck) { cs[o] = ck; });
 }
 
 // iteration step 4: t = A cs; tt, ts, ss; omg, err
@@ -322,17 +352,18 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_bicg_apply_dots(Geom g, const W* __restrict__ cs, const W* __restrict__ s_, W* t,
                                                           double* partials, int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double a[3] = {0.0, 0.0, 0.0};
-  if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
-    const W tv = apply_A<W>(g, cs, k, j, i);
-    t[o] = tv;
-    const double td = (double)tv, sd = (double)s_[o];
-    a[0] = td * td;
-    a[1] = td * sd;
-    a[2] = sd * sd;
-  }
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      const W tv = apply_A<W>(g, cs, k, j, i);
+      t[o] = tv;
+      const double td = (double)tv, sd = (double)s_[o];
+      a[0] += td * td;
+      a[1] += td * sd;
+      a[2] += sd * sd;
+    }
   block_partials<3>(a, partials, nblocks, block_id());
   double s[3];
   if (last_block_sums<3>(st, partials, nblocks, s)) finish_apply_dots(st, s);
@@ -345,15 +376,17 @@ __global__ void __launch_bounds__(NTH) k_bicg_update(Geom g, W* x, const W* __re
                                                       const W* __restrict__ cr, double* partials, int nblocks,
                                                       IterScalars* st, int max_it) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double a[1] = {0.0};
   if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
     const W alf = (W)st->alf, omg = (W)st->omg;
-    x[o] = x[o] + alf * pp[o] + omg * cs[o];
-    const W rv = s_[o] - omg * t[o];
-    r[o] = rv;
-    a[0] = (double)rv * (double)cr[o];
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      x[o] = x[o] + alf * pp[o] + omg * cs[o];
+      const W rv = s_[o] - omg * t[o];
+      r[o] = rv;
+      a[0] += (double)rv * (double)cr[o];
+    }
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
@@ -390,16 +423,17 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_init(Geom g, const W* __restrict__ x, const W* __restrict__ b, W* r,
                                                   double* partials, int nblocks, IterScalars* st, double sc_floor,
                                                   int scale_rhs) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
-    const W bv = scale_rhs ? b[o] * (W)g.avol(k) : b[o];
-    const W rv = bv - apply_A<W>(g, x, k, j, i);
-    r[o] = rv;
-    v[0] = (double)bv * (double)bv;
-    v[1] = (double)rv * (double)rv;
-  }
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      const W bv = scale_rhs ? b[o] * (W)g.avol(k) : b[o];
+      const W rv = bv - apply_A<W>(g, x, k, j, i);
+      r[o] = rv;
+      v[0] += (double)bv * (double)bv;
+      v[1] += (double)rv * (double)rv;
+    }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
   if (last_block_sums<2>(st, partials, nblocks, s)) finish_cg_init(st, s, sc_floor);
@@ -414,16 +448,10 @@ __global__ void __launch_bounds__(NTH) k_cg_precond(Geom g, const W* __restrict_
   double a[1] = {0.0};
   if (i < g.nx && j < g.j1) {
     column_precond<W>(g, [&](long long o) { return r[o]; }, tmp, j, i);
-    long long o = g.at(g.nz, j, i);
-    W zk = tmp[o];
-    z[o] = zk;
-    a[0] = (double)zk * (double)r[o];
-    for (int k = g.nz - 1; k >= 2; --k) {
-      o -= g.plane;
-      zk = tmp[o] - (W)g.luu(k) * zk;
+    column_back<W>(g, tmp, j, i, [&](long long o, W zk) {
       z[o] = zk;
       a[0] += (double)zk * (double)r[o];
-    }
+    });
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
@@ -442,19 +470,20 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_apply(Geom g, const W* __restrict__ z, const W* __restrict__ p_old,
                                                    W* p_new, W* Ax, double* partials, int nblocks, IterScalars* st) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   const bool first = st->it == 1;
   const W bet = (W)st->bet;
   auto pn = [&](long long o) { return first ? z[o] : axpy_rn<W>(bet, p_old[o], z[o]); };
   double a[1] = {0.0};
-  if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
-    const W pc = pn(o);
-    p_new[o] = pc;
-    const W av = apply_A_fn<W>(g, pn, k, j, i);
-    Ax[o] = av;
-    a[0] = (double)pc * (double)av;
-  }
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      const W pc = pn(o);
+      p_new[o] = pc;
+      const W av = apply_A_fn<W>(g, pn, k, j, i);
+      Ax[o] = av;
+      a[0] += (double)pc * (double)av;
+    }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
   if (last_block_sums<1>(st, partials, nblocks, s)) finish_cg_apply(st, s);
@@ -465,15 +494,17 @@ template <typename W>
 __global__ void __launch_bounds__(NTH) k_cg_update(Geom g, W* x, const W* __restrict__ p, const W* __restrict__ Ax, W* r,
                                                     double* partials, int nblocks, IterScalars* st, int max_it) {
   if (st->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double a[1] = {0.0};
   if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
     const W alf = (W)st->alf;
-    x[o] = x[o] + alf * p[o];
-    const W rv = r[o] - alf * Ax[o];
-    r[o] = rv;
-    a[0] = (double)rv * (double)rv;
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      x[o] = x[o] + alf * p[o];
+      const W rv = r[o] - alf * Ax[o];
+      r[o] = rv;
+      a[0] += (double)rv * (double)rv;
+    }
   }
   block_partials<1>(a, partials, nblocks, block_id());
   double s[1];
@@ -484,17 +515,18 @@ __global__ void __launch_bounds__(NTH) k_cg_update(Geom g, W* x, const W* __rest
 __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* __restrict__ x, const double* __restrict__ b,
                                                           double* r, float* r32, double* partials, int nblocks,
                                                           IterScalars* st) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double v[2] = {0.0, 0.0};
-  if (i < g.nx && j < g.j1) {
-    const long long o = g.at(k, j, i);
-    const double bv = g.symm ? b[o] * g.avol(k) : b[o];
-    const double rv = bv - apply_A<double>(g, x, k, j, i);
-    r[o] = rv;
-    r32[o] = (float)rv;
-    v[0] = rv * rv;
-    v[1] = bv * bv;
-  }
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) {
+      const long long o = g.at(k, j, i);
+      const double bv = g.symm ? b[o] * g.avol(k) : b[o];
+      const double rv = bv - apply_A<double>(g, x, k, j, i);
+      r[o] = rv;
+      r32[o] = (float)rv;
+      v[0] += rv * rv;
+      v[1] += bv * bv;
+    }
   block_partials<2>(v, partials, nblocks, block_id());
   double s[2];
   if (last_block_sums<2>(st, partials, nblocks, s)) finish_refine(st, s);
@@ -505,9 +537,10 @@ __global__ void __launch_bounds__(NTH) k_refine_residual(Geom g, const double* _
 // solve cannot remove; the refinement takes it out of b first (a constant shift of levels 2..nz).
 __global__ void __launch_bounds__(NTH) k_compat_sum(Geom g, const double* __restrict__ b, double* partials, int nblocks,
                                                      IterScalars* st) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y, k = blockIdx.z + 2;
+  const int i = blockIdx.x * BX + threadIdx.x, j = g.j0 + blockIdx.y * BY + threadIdx.y;
   double v[1] = {0.0};
-  if (i < g.nx && j < g.j1) v[0] = g.vol(k) * b[g.at(k, j, i)];
+  if (i < g.nx && j < g.j1)
+    for (int k = kz_lo(); k <= kz_hi(g); ++k) v[0] += g.vol(k) * b[g.at(k, j, i)];
   block_partials<1>(v, partials, nblocks, block_id());
   double s[1];
   if (last_block_sums<1>(st, partials, nblocks, s)) finish_compat(st, s, g);
@@ -622,7 +655,7 @@ IterSolverDev* iter_create(const Scalars& s, const RefState& rs, const mgpu_conf
   it->g = Geom{s.nx, s.ny, nz, it->symm ? 1 : 0, s.plane, A_n, A_e, it->coef, j0, j1, ny_total};
   it->block = dim3(BX, BY, 1);
   it->grid_col = dim3((s.nx + BX - 1) / BX, (j1 - j0 + BY - 1) / BY, 1);
-  it->grid_pt = dim3(it->grid_col.x, it->grid_col.y, nz - 1);
+  it->grid_pt = dim3(it->grid_col.x, it->grid_col.y, (nz - 1 + KZ - 1) / KZ);
   it->nblocks = (int)(it->grid_pt.x * it->grid_pt.y * it->grid_pt.z);
   if (dev_alloc(it, (void**)&it->partials, sizeof(double) * 3 * (size_t)it->nblocks)) return fail(MGPU_ERR_CUDA);
   if (dev_alloc(it, (void**)&it->st, sizeof(IterScalars))) return fail(MGPU_ERR_CUDA);

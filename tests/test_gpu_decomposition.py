@@ -321,8 +321,10 @@ def test_iterative_solve_on_slabs_fixed_iterations(gpu_lib, nranks, stype):
 
 @ITER_TYPES
 def test_iterative_solve_on_slabs_to_tolerance(gpu_lib, stype):
-    """Solved to a tolerance: every slab stops at the same iteration, within one of the single
-    domain's, with the residual met."""
+    """Solved to a tolerance: every slab stops at the same iteration with the residual met, and
+    within three of the single domain's.  The slabs sum their inner products in another order
+    (per slab, then across slabs), and near the tolerance BiCGStab's stopping iteration moves by
+    a few with the rounding of those sums."""
     c = iterative_config(1e-10, 500, stype)
     st = dry_state()
     m = api.Model(c)
@@ -335,7 +337,7 @@ def test_iterative_solve_on_slabs_to_tolerance(gpu_lib, stype):
     d.set_state(st)
     d.step(3)
     got = [(s.m.reductions().solver_iterations, s.m.reductions().solver_residual) for s in d.slabs]
-    assert len(set(got)) == 1 and abs(got[0][0] - its) <= 1 and got[0][1] < 1e-10
+    assert len(set(got)) == 1 and abs(got[0][0] - its) <= 3 and got[0][1] < 1e-10, (got, its)
     for f in STATE:
         assert np.abs(d.download(f) - ref[f]).max() <= 1e-8 * np.abs(ref[f]).max(), f
     d.close()
