@@ -132,6 +132,15 @@ static int alloc_state(mgpu_handle* h, DevState<T>& d) {
     int rc = alloc_field<T>(h, &d.sth);
     if (rc) return rc;
   }
+  // TVD advection of the flow: the tiled centred step passes its advective sources through su,
+  // sv, sw to the momentum kernel
+  if (h->cfg.advection_flow_fields == MGPU_ADVECT_TVD) {
+    T** flow[] = {&d.su, &d.sv, &d.sw};
+    for (T** pp : flow) {
+      int rc = alloc_field<T>(h, pp);
+      if (rc) return rc;
+    }
+  }
   return MGPU_OK;
 }
 

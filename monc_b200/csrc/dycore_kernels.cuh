@@ -17,6 +17,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "dycore.h"
 #include "dycore_device.cuh"
 
@@ -614,7 +616,14 @@ constexpr int RM = 4;              // momentum rings: levels k-1..k+1 live, k+2 
 // the level in flight.  Slots are level mod depth.  With 18 planes the FP64 kernel fits three
 // CTAs on an SM.  A ring slot whose level is not live is never read (a centred accessor's
 // pointer to it aliases another slot).
-constexpr int RUV = 3, RW = 4, RD = 3, RZF = 5;
+// FP64 keeps the minimum depths; FP32, whose occupancy registers limit, keeps powers of two
+// (slots by mask).
+template <typename T>
+struct ScalarRings {
+  static constexpr bool F64 = sizeof(T) == 8;
+  static constexpr int RUV = F64 ? 3 : 4, RW = 4, RD = F64 ? 3 : 4, RZF = F64 ? 5 : 8;
+  static constexpr int PLANES = 2 * RUV + RW + RD + RZF;  // u v w diff + scalar
+};
 constexpr int RP = 8;              // profile ring: levels k-1..k+2 live, k+3 staged
 // resident CTAs per SM the register budget is sized for (FP64: 2 x 256 threads x <= 128 registers)
 template <typename T>
@@ -623,7 +632,6 @@ constexpr int min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
 // allows three CTAs per SM in FP64 too
 constexpr int min_ctas3() { return 3; }
 constexpr int M_PLANES = 7 * RM;   // u v w zu zv zw vis
-constexpr int S_PLANES = 2 * RUV + RW + RD + RZF;  // u v w diff + scalar
 template <typename T>
 constexpr size_t smag_smem() { return sizeof(T) * ((size_t)3 * RM * G<T>::PLANE + (size_t)RP * P_COUNT); }
 template <typename T>
@@ -632,8 +640,23 @@ constexpr size_t momentum_smem() { return sizeof(T) * ((size_t)M_PLANES * G<T>::
 constexpr int CW = TX + 2, CN = (TY + 2) * CW;
 template <typename T>
 constexpr size_t scalar_smem() {
-  return sizeof(T) * ((size_t)S_PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
+  return sizeof(T) * ((size_t)ScalarRings<T>::PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
                       (size_t)(TY + 1) * TX + (size_t)2 * CN);
+}
+// TVD advection of a flow component (DIM 0: u, 1: v, 2: w).  The advecting velocities are
+// interpolated to the component's dual grid, which for w averages levels k and k+1: its faces at
+// level k read u, v up to k+2 and w up to k+2 (UPF = 2), the others up to k+1 (UPF = 1).  The
+// rings hold those levels and the one in flight; the advected component's ring holds k-1..k+2.
+template <int DIM>
+struct FlowRings {
+  static constexpr int UPF = DIM == 2 ? 2 : 1;
+  static constexpr int RUV = UPF + 2, RW = UPF + 3, RZ = 5;
+  static constexpr int PLANES = 2 * RUV + RW + RZ;
+};
+template <typename T, int DIM>
+constexpr size_t flow_smem() {
+  return sizeof(T) * ((size_t)FlowRings<DIM>::PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
+                      (size_t)(TY + 1) * TX);
 }
 }  // namespace tiled
 
@@ -737,7 +760,7 @@ __device__ __forceinline__ CRing<T> cring(const T* ring, int k, int co, int j, i
 
 // Each CTA runs the levels kb..ke of its tile, kb = 2 + blockIdx.z * kchunk: splitting the level
 // range gives enough CTAs to fill every SM on grids with few tiles.
-template <typename T>
+template <typename T, bool TVD>
 __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_tiled(Scalars s, DevState<T> d,
                                                                                       int kchunk) {
   using namespace tiled;
@@ -813,7 +836,14 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_
     const CRing<T> ZU = cring<T, RM>(rZU, k, co, j, i), ZV = cring<T, RM>(rZV, k, co, j, i),
                    ZW = cring<T, RM>(rZW, k, co, j, i), VIS = cring<T, RM>(rVIS, k, co, j, i);
     T su, sv, sw;
-    pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
+    if constexpr (TVD) {
+      // the TVD advective sources k_f_flow_tvd_tiled wrote (they start the sums, as PW's do)
+      su = d.su[o];
+      sv = d.sv[o];
+      sw = d.sw[o];
+    } else {
+      pw_point<T>(s, P, U, V, W, k, j, i, su, sv, sw);
+    }
     if (s.use_vd) {
       T du, dv, dw;
       viscosity_core<T>(s, P, ZU, ZV, ZW, ZU, VIS, k, j, i, tm13, tm23, t33, du, dv, dw, tm13, tm23, t33);
@@ -868,6 +898,7 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tile
                                                                                     int kchunk, ScalarJob<T> job) {
   using namespace tiled;
   using Gt = G<T>;
+  typedef ScalarRings<T> SR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -878,11 +909,11 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tile
   const int ke = min(nz, kb + kchunk - 1);
   const long long plane = s.plane;
   T* rU = sm;
-  T* rV = rU + RUV * Gt::PLANE;
-  T* rW = rV + RUV * Gt::PLANE;
-  T* rD = rW + RW * Gt::PLANE;
-  T* rF = rD + RD * Gt::PLANE;
-  T* rP = rF + RZF * Gt::PLANE;  // profile ring
+  T* rV = rU + SR::RUV * Gt::PLANE;
+  T* rW = rV + SR::RUV * Gt::PLANE;
+  T* rD = rW + SR::RW * Gt::PLANE;
+  T* rF = rD + SR::RD * Gt::PLANE;
+  T* rP = rF + SR::RZF * Gt::PLANE;  // profile ring
   T* FX = rP + RP * P_COUNT;     // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
   T* FY = FX + TY * (TX + 1);    // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
   T* CT = FY + (TY + 1) * TX;    // [2][TY+2][TX+2]: cell_cfl_out of levels of parity 0 and 1
@@ -901,16 +932,16 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tile
   // level k reads the scalar at k-1 .. k+2, u v w at k-1 .. k+1, diff at k-1 .. k and profiles
   // at k-1 .. k+2; a chunk above level 2 also needs the z face below it (level kb-1).
   const int k0 = kb == 2 ? 1 : kb - 2;
-  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<RZF>(rF, job.zf, plane, kk);
+  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<SR::RZF>(rF, job.zf, plane, kk);
   // (the z face below the chunk reads w from level kb-2 but u and v from kb-1 up)
   for (int kk = k0; kk <= kb + 1 && kk <= nz; ++kk) {
     if (kk >= kb - 1) {
-      sg.template stage<RUV>(rU, d.u, plane, kk);
-      sg.template stage<RUV>(rV, d.v, plane, kk);
+      sg.template stage<SR::RUV>(rU, d.u, plane, kk);
+      sg.template stage<SR::RUV>(rV, d.v, plane, kk);
     }
-    sg.template stage<RW>(rW, d.w, plane, kk);
+    sg.template stage<SR::RW>(rW, d.w, plane, kk);
   }
-  for (int kk = kb - 1; kk <= kb; ++kk) sg.template stage<RD>(rD, d.diff, plane, kk);
+  for (int kk = kb - 1; kk <= kb; ++kk) sg.template stage<SR::RD>(rD, d.diff, plane, kk);
   if (tid < P_COUNT)
     for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
   const T dtm_x2 = (T)(2.0 * s.dtm);
@@ -937,38 +968,38 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tile
   if (kb > 2) {
     const int kz = kb - 1;
     const CProf<T> P = cprof<T>(rP, kz);
-    const CRing<T> U = cring<T, RUV>(rU, kz, co, j, i), V = cring<T, RUV>(rV, kz, co, j, i),
-                   W = cring<T, RW>(rW, kz, co, j, i);
-    const CRing<T> ZF = cring<T, RZF>(rF, kz, co, j, i);
+    const CRing<T> U = cring<T, SR::RUV>(rU, kz, co, j, i), V = cring<T, SR::RUV>(rV, kz, co, j, i),
+                   W = cring<T, SR::RW>(rW, kz, co, j, i);
+    const CRing<T> ZF = cring<T, SR::RZF>(rF, kz, co, j, i);
     fz_lo = tvd_face_z<T>(s, P, U, V, W, ZF, dt, kz, j, i);
   }
   {
     // the cell sums of level kb
     const CProf<T> P = cprof<T>(rP, kb);
-    const CRing<T> U = cring<T, RUV>(rU, kb, co, j, i), V = cring<T, RUV>(rV, kb, co, j, i),
-                   W = cring<T, RW>(rW, kb, co, j, i);
+    const CRing<T> U = cring<T, SR::RUV>(rU, kb, co, j, i), V = cring<T, SR::RUV>(rV, kb, co, j, i),
+                   W = cring<T, SR::RW>(rW, kb, co, j, i);
     T* C = CT + (kb & 1) * CN;
     C[own_cell] = cell_cfl_out<T>(s, P, U, V, W, kb, j, i);
     if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T>(s, P, U, V, W, kb, j0 - 1 + hr, i0 - 1 + hc);
   }
-  // the table is complete; level kb-2 of the u, v, w rings is overwritten by the first prefetch
+  // the table is complete; the first prefetch overwrites the slots of levels kb-1 (u, v) and kb-2 (w)
   __syncthreads();
   for (int k = kb; k <= ke; ++k) {
-    if (k + 3 <= min(nz, ke + 2)) sg.template stage<RZF>(rF, job.zf, plane, k + 3);
+    if (k + 3 <= min(nz, ke + 2)) sg.template stage<SR::RZF>(rF, job.zf, plane, k + 3);
     if (k + 2 <= min(nz, ke + 1)) {
-      sg.template stage<RUV>(rU, d.u, plane, k + 2);
-      sg.template stage<RUV>(rV, d.v, plane, k + 2);
-      sg.template stage<RW>(rW, d.w, plane, k + 2);
+      sg.template stage<SR::RUV>(rU, d.u, plane, k + 2);
+      sg.template stage<SR::RUV>(rV, d.v, plane, k + 2);
+      sg.template stage<SR::RW>(rW, d.w, plane, k + 2);
     }
-    if (k + 1 <= min(nz, ke)) sg.template stage<RD>(rD, d.diff, plane, k + 1);
+    if (k + 1 <= min(nz, ke)) sg.template stage<SR::RD>(rD, d.diff, plane, k + 1);
     const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
     T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
     const long long o = lin(s, k, j, i);
     const T fv = job.src ? (T)0.0 : __ldg(th + o);
     const CProf<T> P = cprof<T>(rP, k);
-    const CRing<T> U = cring<T, RUV>(rU, k, co, j, i), V = cring<T, RUV>(rV, k, co, j, i),
-                   W = cring<T, RW>(rW, k, co, j, i), DIFF = cring<T, RD>(rD, k, co, j, i);
-    const CRing<T> ZF = cring<T, RZF>(rF, k, co, j, i);
+    const CRing<T> U = cring<T, SR::RUV>(rU, k, co, j, i), V = cring<T, SR::RUV>(rV, k, co, j, i),
+                   W = cring<T, SR::RW>(rW, k, co, j, i), DIFF = cring<T, SR::RD>(rD, k, co, j, i);
+    const CRing<T> ZF = cring<T, SR::RZF>(rF, k, co, j, i);
     // the cell sums of level k+1: the own cell's for the z face above, the table for the next level
     T c_hi = (T)0.0;
     if (k < nz) {
@@ -1014,6 +1045,109 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tile
       if (job.clip && zn < (T)0.0) zn = (T)0.0;
       job.out_zf[o] = smo + (T)s.tsmth * zn;
       job.out_f[o] = zn;
+    }
+    if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
+// TVD advection of one flow component on a centred step (advection_flow_fields = tvd): the
+// advective source of u (DIM 0), v (1) or w (2) into `src`, levels 2..nz (w: 2..nz-1, 0 at nz),
+// which the momentum kernel then takes in place of pw_advection's.  Tiled like the scalar
+// kernel: the same face functions on the component's dual-grid velocities (`DualFlow`), each
+// x and y face computed once and shared through shared memory, the z face carried up the column;
+// the faces and the source are tvd_flow_point's, so the result is bit-identical to it.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_flow_tvd_tiled(Scalars s, DevState<T> d,
+                                                                                   int kchunk, T* __restrict__ src) {
+  using namespace tiled;
+  using Gt = G<T>;
+  typedef FlowRings<DIM> R;
+  typedef typename std::conditional<DIM == 2, TvdMetricW, TvdMetricScalar>::type M;
+  typedef DualFlow<T, CRing<T>, DIM> F;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int nz = s.nz;
+  const int ktop = DIM == 2 ? nz - 1 : nz;  // the last level with a source
+  const int kb = 2 + (int)blockIdx.z * kchunk;
+  const int ke = min(nz, kb + kchunk - 1);
+  const long long plane = s.plane;
+  T* rU = sm;
+  T* rV = rU + R::RUV * Gt::PLANE;
+  T* rW = rV + R::RUV * Gt::PLANE;
+  T* rZ = rW + R::RW * Gt::PLANE;
+  T* rP = rZ + R::RZ * Gt::PLANE;
+  T* FX = rP + RP * P_COUNT;   // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
+  T* FY = FX + TY * (TX + 1);  // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
+  const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  const T* zf = DIM == 0 ? d.zu : (DIM == 1 ? d.zv : d.zw);
+  Stager<T> sg;
+  sg.init(s, j0, i0, tid);
+  // the chunk starts with the z face below level kb (at kb-1): w from kb-2, u and v from kb-1
+  const int k0 = kb == 2 ? 1 : kb - 2;
+  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) sg.template stage<R::RZ>(rZ, zf, plane, kk);
+  for (int kk = k0; kk <= kb + R::UPF && kk <= nz; ++kk) {
+    if (kk >= kb - 1) {
+      sg.template stage<R::RUV>(rU, d.u, plane, kk);
+      sg.template stage<R::RUV>(rV, d.v, plane, kk);
+    }
+    sg.template stage<R::RW>(rW, d.w, plane, kk);
+  }
+  if (tid < P_COUNT)
+    for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
+  cp_async_wait_all();
+  __syncthreads();
+  const T dt = (T)(s.dtm * 2.0);  // momentum_stepping is always centred
+  T fz_lo = (T)0.0;               // u, v: no flux through the face above level 1
+  {
+    const int kz = kb - 1;
+    const CProf<T> P = cprof<T>(rP, kz);
+    const CRing<T> U = cring<T, R::RUV>(rU, kz, co, j, i), V = cring<T, R::RUV>(rV, kz, co, j, i),
+                   W = cring<T, R::RW>(rW, kz, co, j, i), ZF = cring<T, R::RZ>(rZ, kz, co, j, i);
+    const F IU{U, nz}, IV{V, nz}, IW{W, nz};
+    if (kb > 2) fz_lo = tvd_face_z<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, kz, j, i);
+    else if (DIM == 2) fz_lo = tvd_face_z_bottom<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, j, i);
+  }
+  // The first prefetch below overwrites the slot of level kb-1 that this face read.  The copy is
+  // an asm statement without a memory clobber, so without the barrier the compiler may sink the
+  // face's shared-memory loads past it (a race that showed as run-to-run differences in w's
+  // lowest source).
+  __syncthreads();
+  for (int k = kb; k <= ke; ++k) {
+    if (k + 3 <= min(nz, ke + 2)) sg.template stage<R::RZ>(rZ, zf, plane, k + 3);
+    if (k + R::UPF + 1 <= min(nz, ke + R::UPF)) {
+      sg.template stage<R::RUV>(rU, d.u, plane, k + R::UPF + 1);
+      sg.template stage<R::RUV>(rV, d.v, plane, k + R::UPF + 1);
+      sg.template stage<R::RW>(rW, d.w, plane, k + R::UPF + 1);
+    }
+    const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
+    T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
+    const long long o = lin(s, k, j, i);
+    if (k <= ktop) {
+      const CProf<T> P = cprof<T>(rP, k);
+      const CRing<T> U = cring<T, R::RUV>(rU, k, co, j, i), V = cring<T, R::RUV>(rV, k, co, j, i),
+                     W = cring<T, R::RW>(rW, k, co, j, i), ZF = cring<T, R::RZ>(rZ, k, co, j, i);
+      const F IU{U, nz}, IV{V, nz}, IW{W, nz};
+      FX[ty * (TX + 1) + tx + 1] = tvd_face_x<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j, i);
+      FY[(ty + 1) * TX + tx] = tvd_face_y<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j, i);
+      // u, v have no z face above the top level; w's top level (nz-1) has one
+      const T fz_hi = (DIM == 2 || k < nz) ? tvd_face_z<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j, i)
+                                           : (T)0.0;
+      if (tid < TX)
+        FY[tid] = tvd_face_y<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j0 - 1, i0 + tid);
+      else if (tid < TX + TY)
+        FX[(tid - TX) * (TX + 1)] =
+            tvd_face_x<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j0 + tid - TX, i0 - 1);
+      __syncthreads();
+      src[o] = tvd_source<T, F, CProf<T>, M>(s, P, IU, IV, IW, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1],
+                                            FY[ty * TX + tx], FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
+      fz_lo = fz_hi;
+    } else {
+      src[o] = (T)0.0;  // w at the top level
     }
     if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
     cp_async_wait_all();
@@ -1304,6 +1438,25 @@ static inline int choose_level_chunks(int tiles, int slots, int levels) {
   return best;
 }
 
+// the TVD advection of flow component DIM on the centred step, into src (one launch)
+template <typename T, int DIM>
+static int launch_flow_tvd(const Scalars& s, DevState<T>& d, T* src, int tiles, int nsm, int levels,
+                           cudaStream_t st) {
+  const size_t smem = tiled::flow_smem<T, DIM>();
+  static int occ = 0;
+  if (!occ) {
+    cudaFuncSetAttribute(k_f_flow_tvd_tiled<T, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_f_flow_tvd_tiled<T, DIM>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_f_flow_tvd_tiled<T, DIM>, tiled::NT, smem);
+    if (occ < 1) occ = 1;
+  }
+  const int nc = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ * nsm, levels);
+  const int kc = (levels + nc - 1) / nc;
+  dim3 grid(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc - 1) / kc);
+  k_f_flow_tvd_tiled<T, DIM><<<grid, dim3(tiled::TX, tiled::TY, 1), smem, st>>>(s, d, kc, src);
+  return 1;
+}
+
 // returns the number of kernels launched; `mid` (may be null) is recorded before the momentum kernel
 // returns the number of kernels launched
 template <typename T>
@@ -1339,8 +1492,8 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
   // the tiled kernels cover centred dry steps; the first (forward) step and moist runs use the
   // point kernel
   const bool moist = s.nq > 0;
-  const bool tiled_ok = !s.forward && !s.point_dynamics && !s.tvd_flow && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 &&
-                        s.nz >= 4 && (!moist || (d.sth && d.sq[s.nq - 1]));
+  const bool tiled_ok = !s.forward && !s.point_dynamics && (s.nx % tiled::TX) == 0 && (s.ny % tiled::TY) == 0 &&
+                        s.nz >= 4 && (!moist || (d.sth && d.sq[s.nq - 1])) && (!s.tvd_flow || (d.su && d.sv && d.sw));
   if (!tiled_ok) {
     k_f_dynamics<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
     if (mid) cudaEventRecord(mid, st);
@@ -1349,11 +1502,13 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
   const size_t sm_m = tiled::momentum_smem<T>(), sm_s = tiled::scalar_smem<T>();
   static int occ_m = 0, occ_s = 0, nsm = 0;
   if (!nsm) {
-    cudaFuncSetAttribute(k_f_momentum_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_m);
+    cudaFuncSetAttribute(k_f_momentum_tiled<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_m);
+    cudaFuncSetAttribute(k_f_momentum_tiled<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_m);
     cudaFuncSetAttribute(k_f_scalar_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_s);
-    cudaFuncSetAttribute(k_f_momentum_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_f_momentum_tiled<T, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_f_momentum_tiled<T, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_f_scalar_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_f_momentum_tiled<T>, tiled::NT, sm_m);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_f_momentum_tiled<T, false>, tiled::NT, sm_m);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_f_scalar_tiled<T>, tiled::NT, sm_s);
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1379,8 +1534,15 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
     k_f_cloud_step<T><<<pt_grid(s, s.nz), pt_block(), 0, st>>>(s, d);
   }
   if (mid) cudaEventRecord(mid, st);
-  k_f_momentum_tiled<T><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
-  return moist ? s.nq + 3 : 2;
+  int flow = 0;
+  if (s.tvd_flow) {
+    flow += launch_flow_tvd<T, 0>(s, d, d.su, tiles, nsm, levels, st);
+    flow += launch_flow_tvd<T, 1>(s, d, d.sv, tiles, nsm, levels, st);
+    flow += launch_flow_tvd<T, 2>(s, d, d.sw, tiles, nsm, levels, st);
+  }
+  if (s.tvd_flow) k_f_momentum_tiled<T, true><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
+  else k_f_momentum_tiled<T, false><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
+  return (moist ? s.nq + 3 : 2) + flow;
 }
 template <typename T>
 void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st) {
