@@ -656,7 +656,7 @@ struct FlowRings {
 template <typename T, int DIM>
 constexpr size_t flow_smem() {
   return sizeof(T) * ((size_t)FlowRings<DIM>::PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
-                      (size_t)(TY + 1) * TX);
+                      (size_t)(TY + 1) * TX + (size_t)2 * CN);
 }
 }  // namespace tiled
 
@@ -1083,7 +1083,16 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_flow_tvd_ti
   T* rP = rZ + R::RZ * Gt::PLANE;
   T* FX = rP + RP * P_COUNT;   // [TY][TX+1]: x-faces of columns i0-1 .. i0+TX-1
   T* FY = FX + TY * (TX + 1);  // [TY+1][TX]: y-faces of rows j0-1 .. j0+TY-1
+  T* CT = FY + (TY + 1) * TX;  // [2][TY+2][TX+2]: cell Courant sums of levels of parity 0 and 1
   const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  // the cell sums each face's limiter needs, once per cell and level, as the scalar kernel forms
+  // them (own cell per thread, the tile's border cells by the first 2*CW + 2*TY threads)
+  const int own_cell = (ty + 1) * CW + tx + 1;
+  int hr = -1, hc = -1;
+  if (tid < CW) { hr = 0; hc = tid; }
+  else if (tid < 2 * CW) { hr = TY + 1; hc = tid - CW; }
+  else if (tid < 2 * CW + TY) { hr = tid - 2 * CW + 1; hc = 0; }
+  else if (tid < 2 * CW + 2 * TY) { hr = tid - 2 * CW - TY + 1; hc = TX + 1; }
   const T* zf = DIM == 0 ? d.zu : (DIM == 1 ? d.zv : d.zw);
   Stager<T> sg;
   sg.init(s, j0, i0, tid);
@@ -1112,6 +1121,16 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_flow_tvd_ti
     if (kb > 2) fz_lo = tvd_face_z<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, kz, j, i);
     else if (DIM == 2) fz_lo = tvd_face_z_bottom<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, j, i);
   }
+  if (kb <= ktop) {
+    // the cell sums of level kb
+    const CProf<T> P = cprof<T>(rP, kb);
+    const CRing<T> U = cring<T, R::RUV>(rU, kb, co, j, i), V = cring<T, R::RUV>(rV, kb, co, j, i),
+                   W = cring<T, R::RW>(rW, kb, co, j, i);
+    const F IU{U, nz}, IV{V, nz}, IW{W, nz};
+    T* C = CT + (kb & 1) * CN;
+    C[own_cell] = cell_cfl_out<T, F, CProf<T>, M>(s, P, IU, IV, IW, kb, j, i);
+    if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T, F, CProf<T>, M>(s, P, IU, IV, IW, kb, j0 - 1 + hr, i0 - 1 + hc);
+  }
   // The first prefetch below overwrites the slot of level kb-1 that this face read.  The copy is
   // an asm statement without a memory clobber, so without the barrier the compiler may sink the
   // face's shared-memory loads past it (a race that showed as run-to-run differences in w's
@@ -1132,16 +1151,30 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_flow_tvd_ti
       const CRing<T> U = cring<T, R::RUV>(rU, k, co, j, i), V = cring<T, R::RUV>(rV, k, co, j, i),
                      W = cring<T, R::RW>(rW, k, co, j, i), ZF = cring<T, R::RZ>(rZ, k, co, j, i);
       const F IU{U, nz}, IV{V, nz}, IW{W, nz};
-      FX[ty * (TX + 1) + tx + 1] = tvd_face_x<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j, i);
-      FY[(ty + 1) * TX + tx] = tvd_face_y<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j, i);
+      // the cell sums of level k+1: the own cell's for the z face above, the table for the next level
+      T c_hi = (T)0.0;
+      if (k < nz) {
+        c_hi = cell_cfl_out<T, F, CProf<T>, M>(s, P, IU, IV, IW, k + 1, j, i);
+        if (k + 1 <= min(ke, ktop)) {
+          T* C = CT + ((k + 1) & 1) * CN;
+          C[own_cell] = c_hi;
+          if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T, F, CProf<T>, M>(s, P, IU, IV, IW, k + 1, j0 - 1 + hr, i0 - 1 + hc);
+        }
+      }
+      const T* Ck = CT + (k & 1) * CN;
+      auto cfl = [&](int kk, int jj, int ii) -> T { return kk == k ? Ck[(jj - j0 + 1) * CW + (ii - i0 + 1)] : c_hi; };
+      typedef decltype(cfl) CS;
+      FX[ty * (TX + 1) + tx + 1] = tvd_face_x_g<T, F, CRing<T>, CProf<T>, M, CS>(s, P, IU, IV, IW, ZF, dt, k, j, i, cfl);
+      FY[(ty + 1) * TX + tx] = tvd_face_y_g<T, F, CRing<T>, CProf<T>, M, CS>(s, P, IU, IV, IW, ZF, dt, k, j, i, cfl);
       // u, v have no z face above the top level; w's top level (nz-1) has one
-      const T fz_hi = (DIM == 2 || k < nz) ? tvd_face_z<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j, i)
-                                           : (T)0.0;
+      const T fz_hi = (DIM == 2 || k < nz)
+                          ? tvd_face_z_g<T, F, CRing<T>, CProf<T>, M, CS>(s, P, IU, IV, IW, ZF, dt, k, j, i, cfl)
+                          : (T)0.0;
       if (tid < TX)
-        FY[tid] = tvd_face_y<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j0 - 1, i0 + tid);
+        FY[tid] = tvd_face_y_g<T, F, CRing<T>, CProf<T>, M, CS>(s, P, IU, IV, IW, ZF, dt, k, j0 - 1, i0 + tid, cfl);
       else if (tid < TX + TY)
-        FX[(tid - TX) * (TX + 1)] =
-            tvd_face_x<T, F, CRing<T>, CProf<T>, M>(s, P, IU, IV, IW, ZF, dt, k, j0 + tid - TX, i0 - 1);
+        FX[(tid - TX) * (TX + 1)] = tvd_face_x_g<T, F, CRing<T>, CProf<T>, M, CS>(s, P, IU, IV, IW, ZF, dt, k,
+                                                                                 j0 + tid - TX, i0 - 1, cfl);
       __syncthreads();
       src[o] = tvd_source<T, F, CProf<T>, M>(s, P, IU, IV, IW, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1],
                                             FY[ty * TX + tx], FY[(ty + 1) * TX + tx], fz_lo, fz_hi, k, j, i, (T)0.0);
