@@ -658,6 +658,19 @@ constexpr size_t flow_smem() {
   return sizeof(T) * ((size_t)FlowRings<DIM>::PLANES * G<T>::PLANE + (size_t)RP * P_COUNT + (size_t)TY * (TX + 1) +
                       (size_t)(TY + 1) * TX + (size_t)2 * CN);
 }
+// The moist centred step with vapour and liquid (theta and two q fields) in one kernel: the flow,
+// diff and the cell Courant sums are staged and formed once for the three scalars; each scalar
+// has its own ring (k-1..k+2 and the level in flight).  Two x/y face buffers alternate between
+// the scalars.
+struct MoistRings {
+  static constexpr int NS = 3, RUV = 3, RW = 4, RD = 3, RZF = 5;
+  static constexpr int PLANES = 2 * RUV + RW + RD + NS * RZF;
+};
+template <typename T>
+constexpr size_t moist_smem() {
+  return sizeof(T) * ((size_t)MoistRings::PLANES * G<T>::PLANE + (size_t)RP * P_COUNT +
+                      (size_t)2 * (TY * (TX + 1) + (TY + 1) * TX) + (size_t)2 * CN);
+}
 }  // namespace tiled
 
 // A column's values at levels k0 and k0+1 held in registers, read through the accessor interface
@@ -1188,6 +1201,197 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_flow_tvd_ti
   }
 }
 
+// The whole moist centred step of theta, vapour and liquid in one pass (number_q_fields = 2):
+// for each scalar the TVD faces, source, diffusion, damping and subsidence of k_f_scalar_tiled,
+// then simplecloud and stepfields (with swap_smooth's pre-smoothing and the negative-q clip) of
+// k_f_cloud_step, at each point as soon as its three sources are known.  The sources never go
+// to memory, the flow, diff and the Courant sums are staged once for the three scalars, and the
+// results are those of the point kernel, to the bit.
+template <typename T>
+__global__ void __launch_bounds__(tiled::NT, 2) k_f_moist_tiled(Scalars s, DevState<T> d, int kchunk) {
+  using namespace tiled;
+  using Gt = G<T>;
+  typedef MoistRings R;
+  constexpr int NS = R::NS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int nz = s.nz;
+  const int kb = 2 + (int)blockIdx.z * kchunk;
+  const int ke = min(nz, kb + kchunk - 1);
+  const long long plane = s.plane;
+  T* rU = sm;
+  T* rV = rU + R::RUV * Gt::PLANE;
+  T* rW = rV + R::RUV * Gt::PLANE;
+  T* rD = rW + R::RW * Gt::PLANE;
+  T* rF[NS];
+  rF[0] = rD + R::RD * Gt::PLANE;
+  for (int n = 1; n < NS; ++n) rF[n] = rF[n - 1] + R::RZF * Gt::PLANE;
+  T* rP = rF[NS - 1] + R::RZF * Gt::PLANE;
+  T* FXs[2];
+  T* FYs[2];
+  FXs[0] = rP + RP * P_COUNT;
+  FYs[0] = FXs[0] + TY * (TX + 1);
+  FXs[1] = FYs[0] + (TY + 1) * TX;
+  FYs[1] = FXs[1] + TY * (TX + 1);
+  T* CT = FYs[1] + (TY + 1) * TX;
+  const int co = (ty + HY) * Gt::PW + (tx + Gt::V);
+  const int own_cell = (ty + 1) * CW + tx + 1;
+  int hr = -1, hc = -1;
+  if (tid < CW) { hr = 0; hc = tid; }
+  else if (tid < 2 * CW) { hr = TY + 1; hc = tid - CW; }
+  else if (tid < 2 * CW + TY) { hr = tid - 2 * CW + 1; hc = 0; }
+  else if (tid < 2 * CW + 2 * TY) { hr = tid - 2 * CW - TY + 1; hc = TX + 1; }
+  // scalar n: 0 theta, 1 + m the q field m; its state, z-field, outputs and mean-profile row
+  const T* fs[NS] = {d.th, d.q[0], d.q[1]};
+  const T* zfs[NS] = {d.zth, d.zq[0], d.zq[1]};
+  T* fo[NS] = {d.th_n, d.q_n[0], d.q_n[1]};
+  T* zfo[NS] = {d.zth_n, d.zq_n[0], d.zq_n[1]};
+  Stager<T> sg;
+  sg.init(s, j0, i0, tid);
+  const int k0 = kb == 2 ? 1 : kb - 2;
+  for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk)
+#pragma unroll
+    for (int n = 0; n < NS; ++n) sg.template stage<R::RZF>(rF[n], zfs[n], plane, kk);
+  for (int kk = k0; kk <= kb + 1 && kk <= nz; ++kk) {
+    if (kk >= kb - 1) {
+      sg.template stage<R::RUV>(rU, d.u, plane, kk);
+      sg.template stage<R::RUV>(rV, d.v, plane, kk);
+    }
+    sg.template stage<R::RW>(rW, d.w, plane, kk);
+  }
+  for (int kk = kb - 1; kk <= kb; ++kk) sg.template stage<R::RD>(rD, d.diff, plane, kk);
+  if (tid < P_COUNT)
+    for (int kk = k0; kk <= kb + 2 && kk <= nz; ++kk) rP[(kk & (RP - 1)) * P_COUNT + tid] = load_profile<T>(s, tid, kk);
+  const T dtm_x2 = (T)(2.0 * s.dtm);
+  const T c1 = (T)(1.0 - 2.0 * s.tsmth), c2 = (T)s.tsmth;
+  // stepfields with the pre-smoothing of swap_smooth (k_f_cloud_step's `step`)
+  auto step = [&](int n, long long o, T zv, T src) {
+    const T fv = fs[n][o];
+    const T smo = c1 * fv + c2 * zv;
+    T zn = (T)0.0 + zv + dtm_x2 * src;
+    if (n > 0 && zn < (T)0.0) zn = (T)0.0;
+    zfo[n][o] = smo + (T)s.tsmth * zn;
+    fo[n][o] = zn;
+  };
+  if (kb == 2) {
+    // level 1: zero sources
+    const long long o = lin(s, 1, j, i);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) step(n, o, zfs[n][o], (T)0.0);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const T dt = (T)(s.dtm * 2.0);
+  T fz_lo[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) fz_lo[n] = (T)0.0;  // flux_z(2) = 0
+  if (kb > 2) {
+    const int kz = kb - 1;
+    const CProf<T> P = cprof<T>(rP, kz);
+    const CRing<T> U = cring<T, R::RUV>(rU, kz, co, j, i), V = cring<T, R::RUV>(rV, kz, co, j, i),
+                   W = cring<T, R::RW>(rW, kz, co, j, i);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const CRing<T> ZF = cring<T, R::RZF>(rF[n], kz, co, j, i);
+      fz_lo[n] = tvd_face_z<T>(s, P, U, V, W, ZF, dt, kz, j, i);
+    }
+  }
+  {
+    const CProf<T> P = cprof<T>(rP, kb);
+    const CRing<T> U = cring<T, R::RUV>(rU, kb, co, j, i), V = cring<T, R::RUV>(rV, kb, co, j, i),
+                   W = cring<T, R::RW>(rW, kb, co, j, i);
+    T* C = CT + (kb & 1) * CN;
+    C[own_cell] = cell_cfl_out<T>(s, P, U, V, W, kb, j, i);
+    if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T>(s, P, U, V, W, kb, j0 - 1 + hr, i0 - 1 + hc);
+  }
+  // the first prefetch overwrites the slots of levels kb-1 (u, v) and kb-2 (w, the scalars)
+  __syncthreads();
+  for (int k = kb; k <= ke; ++k) {
+    if (k + 3 <= min(nz, ke + 2))
+#pragma unroll
+      for (int n = 0; n < NS; ++n) sg.template stage<R::RZF>(rF[n], zfs[n], plane, k + 3);
+    if (k + 2 <= min(nz, ke + 1)) {
+      sg.template stage<R::RUV>(rU, d.u, plane, k + 2);
+      sg.template stage<R::RUV>(rV, d.v, plane, k + 2);
+      sg.template stage<R::RW>(rW, d.w, plane, k + 2);
+    }
+    if (k + 1 <= min(nz, ke)) sg.template stage<R::RD>(rD, d.diff, plane, k + 1);
+    const bool pstage = tid < P_COUNT && k + 3 <= min(nz, ke + 2);
+    T pnext = pstage ? load_profile<T>(s, tid, k + 3) : (T)0;
+    const long long o = lin(s, k, j, i);
+    const CProf<T> P = cprof<T>(rP, k);
+    const CRing<T> U = cring<T, R::RUV>(rU, k, co, j, i), V = cring<T, R::RUV>(rV, k, co, j, i),
+                   W = cring<T, R::RW>(rW, k, co, j, i), DIFF = cring<T, R::RD>(rD, k, co, j, i);
+    // the cell sums of level k+1: the own cell's for the z faces above, the table for the next level
+    T c_hi = (T)0.0;
+    if (k < nz) {
+      c_hi = cell_cfl_out<T>(s, P, U, V, W, k + 1, j, i);
+      if (k + 1 <= ke) {
+        T* C = CT + ((k + 1) & 1) * CN;
+        C[own_cell] = c_hi;
+        if (hr >= 0) C[hr * CW + hc] = cell_cfl_out<T>(s, P, U, V, W, k + 1, j0 - 1 + hr, i0 - 1 + hc);
+      }
+    }
+    const T* Ck = CT + (k & 1) * CN;
+    auto cfl = [&](int kk, int jj, int ii) -> T { return kk == k ? Ck[(jj - j0 + 1) * CW + (ii - i0 + 1)] : c_hi; };
+    typedef decltype(cfl) CS;
+    T src[NS], zv[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      // faces of scalar n into buffer n & 1; the barrier also ends the reads of that buffer by
+      // scalar n - 2's source
+      T* FX = FXs[n & 1];
+      T* FY = FYs[n & 1];
+      const CRing<T> ZF = cring<T, R::RZF>(rF[n], k, co, j, i);
+      FX[ty * (TX + 1) + tx + 1] =
+          tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+      FY[(ty + 1) * TX + tx] =
+          tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS>(s, P, U, V, W, ZF, dt, k, j, i, cfl);
+      const T fz_hi = (k < nz) ? tvd_face_z_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS>(
+                                     s, P, U, V, W, ZF, dt, k, j, i, cfl)
+                               : (T)0.0;
+      if (tid < TX)
+        FY[tid] = tvd_face_y_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS>(s, P, U, V, W, ZF, dt, k, j0 - 1,
+                                                                                    i0 + tid, cfl);
+      else if (tid < TX + TY)
+        FX[(tid - TX) * (TX + 1)] = tvd_face_x_g<T, CRing<T>, CRing<T>, CProf<T>, TvdMetricScalar, CS>(
+            s, P, U, V, W, ZF, dt, k, j0 + tid - TX, i0 - 1, cfl);
+      __syncthreads();
+      const int row = n == 0 ? 2 : 2 + n;
+      T sf = tvd_source<T>(s, P, U, V, W, FX[ty * (TX + 1) + tx], FX[ty * (TX + 1) + tx + 1], FY[ty * TX + tx],
+                           FY[(ty + 1) * TX + tx], fz_lo[n], fz_hi, k, j, i, (T)0.0);
+      if (n == 0 && s.th_baroclinic) sf = sf + th_baroclinic_point<T>(s, U, V, k, j, i);
+      if (s.use_vd) sf = sf + diffusion_point<T>(s, P, ZF, DIFF, k, j, i);
+      if (s.damping && (row > 2 || !s.passive_th)) sf = damping_scalar_point<T>(s, P, k, ZF(k, j, i), row, sf);
+      if (n == 0 ? s.subs_th : s.subs_q)
+        sf = n == 0 ? subsidence_theta_point<T>(s, P, ZF, k, j, i, sf)
+                    : subsidence_q_point<T>(s, P, ZF, n - 1, k, j, i, sf);
+      fz_lo[n] = fz_hi;
+      src[n] = sf;
+      zv[n] = ZF(k, j, i);
+    }
+    // simplecloud and stepfields (k_f_cloud_step)
+    if (s.simplecloud) {
+      // vapour and liquid are q fields iqv and iql, scalars 1 + iqv and 1 + iql (selected, so
+      // that the arrays stay in registers)
+      const bool v0 = s.iqv == 0;
+      const T zqv = v0 ? zv[1] : zv[2], zql = v0 ? zv[2] : zv[1];
+      T sqv = v0 ? src[1] : src[2], sql = v0 ? src[2] : src[1];
+      simplecloud_point<T>(s, P, k, zqv, zql, zv[0], zql, src[0], sqv, sql);
+      src[1] = v0 ? sqv : sql;
+      src[2] = v0 ? sql : sqv;
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) step(n, o, zv[n], src[n]);
+    if (pstage) rP[((k + 3) & (RP - 1)) * P_COUNT + tid] = pnext;
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
 // Moist centred step after the tiled scalar kernels have written the advective + diffusive
 // sources: simplecloud (when enabled), then stepfields with the Robert pre-smoothing of
 // swap_smooth for theta and every q field (negative q clipped), as the point kernel does.
@@ -1490,6 +1694,24 @@ static int launch_flow_tvd(const Scalars& s, DevState<T>& d, T* src, int tiles, 
   return 1;
 }
 
+// the moist scalar step of theta and two q fields (one launch)
+template <typename T>
+static int launch_moist(const Scalars& s, DevState<T>& d, int tiles, int nsm, int levels, cudaStream_t st) {
+  const size_t smem = tiled::moist_smem<T>();
+  static int occ = 0;
+  if (!occ) {
+    cudaFuncSetAttribute(k_f_moist_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_f_moist_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_f_moist_tiled<T>, tiled::NT, smem);
+    if (occ < 1) occ = 1;
+  }
+  const int nc = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ * nsm, levels);
+  const int kc = (levels + nc - 1) / nc;
+  dim3 grid(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc - 1) / kc);
+  k_f_moist_tiled<T><<<grid, dim3(tiled::TX, tiled::TY, 1), smem, st>>>(s, d, kc);
+  return 1;
+}
+
 // returns the number of kernels launched; `mid` (may be null) is recorded before the momentum kernel
 // returns the number of kernels launched
 template <typename T>
@@ -1557,8 +1779,12 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
   dim3 block(tiled::TX, tiled::TY, 1);
   dim3 grid_s(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_s - 1) / kc_s);
   dim3 grid_m(s.nx / tiled::TX, s.ny / tiled::TY, (levels + kc_m - 1) / kc_m);
+  int nscal = moist ? s.nq + 2 : 1;  // launches of the scalar part
   if (!moist) {
     k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, d.th_n, d.zth_n, nullptr, 0, 2});
+  } else if (s.nq == 2) {
+    // theta, vapour and liquid in one pass, sources, cloud and stepping included
+    nscal = launch_moist<T>(s, d, tiles, nsm, levels, st);
   } else {
     // one launch per scalar writing its source, then saturation adjustment and stepping
     k_f_scalar_tiled<T><<<grid_s, block, sm_s, st>>>(s, d, kc_s, ScalarJob<T>{d.th, d.zth, nullptr, nullptr, d.sth, 0, 2});
@@ -1575,7 +1801,7 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
   }
   if (s.tvd_flow) k_f_momentum_tiled<T, true><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
   else k_f_momentum_tiled<T, false><<<grid_m, block, sm_m, st>>>(s, d, kc_m);
-  return (moist ? s.nq + 3 : 2) + flow;
+  return nscal + 1 + flow;
 }
 template <typename T>
 void launch_fused_pressure_source(const Scalars& s, DevState<T>& d, cudaStream_t st) {

@@ -101,16 +101,20 @@ def test_fp32_surface_ghost_theta_keeps_the_perturbation(gpu_lib, timestep):
     assert np.abs(out[1] - out[0]).max() <= 2e-6
 
 
+@pytest.mark.parametrize("n_tracers", [0, 1], ids=["vapour-liquid", "with-tracer"])
 @pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
-def test_moist_tiled_bit_identical_to_point_kernel(gpu_lib, monkeypatch, precision):
-    """The per-scalar tiled kernels plus the cloud step reproduce the point kernel bit for bit."""
+def test_moist_tiled_bit_identical_to_point_kernel(gpu_lib, monkeypatch, precision, n_tracers):
+    """The tiled moist step reproduces the point kernel bit for bit, for any split of the levels:
+    with vapour and liquid only, one kernel for theta and both q fields (sources, cloud and
+    stepping included); with a tracer as well, one kernel per scalar and the cloud step."""
     outs = []
-    for point, chunks in (("1", "0"), ("0", "0"), ("0", "3")):
+    extra = ["q2", "zq2"] if n_tracers else []
+    for point, chunks in (("1", "0"), ("0", "0"), ("0", "1"), ("0", "3"), ("0", "7")):
         monkeypatch.setenv("MGPU_POINT_DYNAMICS", point)
         monkeypatch.setenv("MGPU_LEVEL_CHUNKS", chunks)
-        o, m = moist_pair(precision=precision, n_tracers=1, reproducible=1)
+        o, m = moist_pair(precision=precision, n_tracers=n_tracers, reproducible=1)
         m.step(4)
-        outs.append({f: m.download(f) for f in FIELDS + ["q2", "zq2"]})
+        outs.append({f: m.download(f) for f in FIELDS + extra})
         m.close()
     for res in outs[1:]:
         for f in outs[0]:
