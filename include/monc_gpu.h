@@ -311,24 +311,26 @@ int mgpu_checkpoint_read(mgpu_handle* h, const char* path);
 /* The step state a checkpoint carries, without a file: for a decomposed run, whose driver
  * gathers the slabs' fields into one global file with mgpu_checkpoint_write_host (MONC's ranks
  * write their parts of one file, writecheckpoint.F90) and restores every slab after reading it.
- * mean (may be NULL): (3 + number_q_fields) rows of nz, olzubar, olzvbar, olzthbar, olzqbar(n). */
+ * mean (may be NULL): the rows of mgpu_mean_profiles, 2 (3 + number_q_fields) rows of nz. */
 int mgpu_checkpoint_state(mgpu_handle* h, mgpu_checkpoint_meta* meta);
 int mgpu_restore_state(mgpu_handle* h, const mgpu_checkpoint_meta* meta, const double* mean);
 
 /* The same without a GPU, on host arrays: fields[0..8] = u v w th zu zv zw zth p, then q(n) and
- * zq(n) for n < number_q_fields, each [nz][ny][nx] x fastest; mean = (3 + number_q_fields) rows of
- * nz (olzubar, olzvbar, olzthbar, olzqbar(n)) or null.  read sets *has_mean when the file holds
- * the mean profiles. */
+ * zq(n) for n < number_q_fields, each [nz][ny][nx] x fastest; mean = the rows of
+ * mgpu_mean_profiles (2 (3 + number_q_fields) rows of nz) or null.  read sets *has_mean to 1 when
+ * the file holds the olz*bar profiles, 2 when it also holds olubar, olvbar, olthbar and olqbar
+ * (otherwise those rows are zero), 0 when it holds none. */
 int mgpu_checkpoint_write_host(const mgpu_config* cfg, const char* path, const double* const* fields,
                                const double* mean, const mgpu_checkpoint_meta* meta);
 int mgpu_checkpoint_read_host(const mgpu_config* cfg, const char* path, double* const* fields, double* mean,
                               int32_t* has_mean, mgpu_checkpoint_meta* meta);
 
 /* The mean profiles (meanprofiles.F90:95-216, global_grid vertical olzubar, olzvbar, olzthbar,
- * olzqbar, olubar, olvbar, olthbar): out receives (6 + number_q_fields) rows of nz values,
- * k = 1..nz: olzubar, olzvbar, olzthbar, olzqbar(n), then olubar, olvbar, olthbar.  They are the
- * means of the fields as MONC's solver group sees them: the stepped zu, zv, zth, zq before the
- * pressure step, u + ugal, v + vgal, and theta after stepfields' time smoothing.  mgpu_step
+ * olzqbar, olubar, olvbar, olthbar, olqbar): out receives 2 (3 + number_q_fields) rows of nz
+ * values, k = 1..nz: olzubar, olzvbar, olzthbar, olzqbar(n), then olubar, olvbar, olthbar,
+ * olqbar(n).  They are the means of the fields as MONC's solver group sees them: the stepped zu,
+ * zv, zth, zq before the pressure step, u + ugal, v + vgal, and theta and q after stepfields'
+ * time smoothing.  mgpu_step
  * refreshes them every step when damping, subsidence or profile_diagnostics reads them;
  * MGPU_C_MEAN_PROFILES refreshes them from the component fields. */
 int mgpu_mean_profiles(mgpu_handle* h, double* out);
@@ -491,10 +493,10 @@ int mgpu_slab_level_means(mgpu_handle* h, double* d_means);
 
 /* The mean profiles of a slab (mgpu_mean_profiles' rows; damping, subsidence and
  * profile_diagnostics read them).  The dynamics phase leaves this slab's means; the driver
- * fetches them into d_buf (put = 0: (6 + number_q_fields) rows of nz + 2 doubles on the device,
- * olz*bar rows then olubar, olvbar, olthbar), averages them over the slabs (all slabs hold the
- * same number of rows: the average is the domain mean) and puts the result back (put = 1)
- * before the next dynamics phase. */
+ * fetches them into d_buf (put = 0: 2 (3 + number_q_fields) rows of nz + 2 doubles on the
+ * device, olz*bar rows then olubar, olvbar, olthbar, olqbar(n)), averages them over the slabs
+ * (all slabs hold the same number of rows: the average is the domain mean) and puts the result
+ * back (put = 1) before the next dynamics phase. */
 int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put);
 
 /* cfltest on slabs (cfltest.F90:62-128; MONC reduces the same extrema across its ranks with

@@ -383,13 +383,15 @@ class Model:
 
     def mean_profiles(self) -> dict:
         """The mean profiles (meanprofiles.F90): olzubar, olzvbar, olzthbar, olzqbar(n), olubar,
-        olvbar, olthbar, as refreshed by the last step or mean_profiles component."""
-        rows = 6 + self.cfg.number_q_fields
-        out = np.empty((rows, self.nz), dtype=np.float64)
+        olvbar, olthbar, olqbar(n), as refreshed by the last step or mean_profiles component."""
+        out = self.mean_profile_rows()
+        return dict(zip(mean_profile_names(self.cfg.number_q_fields), out))
+
+    def mean_profile_rows(self) -> np.ndarray:
+        """mgpu_mean_profiles' rows, (2 (3 + number_q_fields), nz): the checkpoints' `mean`."""
+        out = np.empty((2 * (3 + self.cfg.number_q_fields), self.nz), dtype=np.float64)
         self._check(lib().mgpu_mean_profiles(self.h, out.ctypes.data), "mean_profiles")
-        names = (["olzubar", "olzvbar", "olzthbar"] + [f"olzqbar{n}" for n in range(self.cfg.number_q_fields)]
-                 + ["olubar", "olvbar", "olthbar"])
-        return dict(zip(names, out))
+        return out
 
     def profile_diagnostics(self) -> dict:
         """MONC's profile_diagnostics sums (<name>_total_local, per level) from the current state,
@@ -410,7 +412,8 @@ class Model:
         return meta
 
     def restore_state(self, meta: "CheckpointMeta", mean: np.ndarray | None = None):
-        """Continue after the step `meta` describes; mean: (3 + number_q_fields, nz) olz*bar rows."""
+        """Continue after the step `meta` describes; mean: mgpu_mean_profiles' rows,
+        (2 (3 + number_q_fields), nz)."""
         m = None if mean is None else np.ascontiguousarray(mean, dtype=np.float64)
         self._check(lib().mgpu_restore_state(self.h, C.byref(meta), None if m is None else m.ctypes.data),
                     "restore_state")
@@ -560,9 +563,16 @@ def _checkpoint_names(cfg) -> list:
     return CHECKPOINT_FIELDS + [f"q{n}" for n in range(nq)] + [f"zq{n}" for n in range(nq)]
 
 
+def mean_profile_names(nq: int) -> list:
+    """Names of mgpu_mean_profiles' rows."""
+    return (["olzubar", "olzvbar", "olzthbar"] + [f"olzqbar{n}" for n in range(nq)]
+            + ["olubar", "olvbar", "olthbar"] + [f"olqbar{n}" for n in range(nq)])
+
+
 def checkpoint_write_host(cfg, path: str, fields: dict, meta: CheckpointMeta, mean: np.ndarray | None = None):
     """Write a MONC-layout checkpoint from host arrays (no GPU): fields by name, each (nz, ny, nx);
-    mean, when given, (3 + number_q_fields, nz) rows olzubar, olzvbar, olzthbar, olzqbar(n)."""
+    mean, when given, mgpu_mean_profiles' rows (2 (3 + number_q_fields), nz): olz*bar, then
+    olubar, olvbar, olthbar, olqbar(n)."""
     names = _checkpoint_names(cfg)
     arrs = [np.ascontiguousarray(fields[n], dtype=np.float64) for n in names]
     ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
@@ -574,12 +584,13 @@ def checkpoint_write_host(cfg, path: str, fields: dict, meta: CheckpointMeta, me
 
 
 def checkpoint_read_host(cfg, path: str):
-    """Read a MONC-layout checkpoint into host arrays: (fields, mean or None, meta)."""
+    """Read a MONC-layout checkpoint into host arrays: (fields, mean or None, meta).  mean has
+    mgpu_mean_profiles' rows; those of olubar .. olqbar are zero when the file lacks them."""
     names = _checkpoint_names(cfg)
     shape = (cfg.nz, cfg.ny, cfg.nx)
     arrs = [np.empty(shape, dtype=np.float64) for _ in names]
     ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
-    mean = np.empty((3 + cfg.number_q_fields, cfg.nz), dtype=np.float64)
+    mean = np.empty((2 * (3 + cfg.number_q_fields), cfg.nz), dtype=np.float64)
     has_mean = C.c_int32(0)
     meta = CheckpointMeta()
     rc = lib().mgpu_checkpoint_read_host(C.byref(cfg), os.fsencode(path), ptrs, mean.ctypes.data,

@@ -61,7 +61,7 @@ struct mgpu_handle {
   double* bmean_d = nullptr; // FP32-mixed: horizontal means of th and q per level (1+nq rows of nz+2)
   double* olz_d = nullptr;       // mean profiles olzubar, olzvbar, olzthbar, olzqbar (3+MGPU_MAX_Q rows of nz+2)
   double* subs_tend_d = nullptr; // mean-profile subsidence tendencies, the same rows
-  double* olbar_d = nullptr;     // olubar, olvbar, olthbar (3 rows of nz+2)
+  double* olbar_d = nullptr;     // olubar, olvbar, olthbar, olqbar (3+MGPU_MAX_Q rows of nz+2)
   double* pd_d = nullptr;        // profile_diagnostics sums (MGPU_PD_COUNT rows of nz)
   bool profiling = false;
   cudaEvent_t ev[16] = {};
@@ -313,7 +313,8 @@ int mgpu_create(const mgpu_config* cfg, mgpu_handle** out) {
       return cleanup(MGPU_ERR_CUDA);
     cudaMemset(h->olz_d, 0, nb);
     cudaMemset(h->subs_tend_d, 0, nb);
-    const size_t nbar = (size_t)3 * (cfg->nz + 2) * sizeof(double), npd = (size_t)MGPU_PD_COUNT * cfg->nz * sizeof(double);
+    const size_t nbar = (size_t)(3 + MGPU_MAX_Q) * (cfg->nz + 2) * sizeof(double),
+                 npd = (size_t)MGPU_PD_COUNT * cfg->nz * sizeof(double);
     if (cudaMalloc(&h->olbar_d, nbar) != cudaSuccess || cudaMalloc(&h->pd_d, npd) != cudaSuccess)
       return cleanup(MGPU_ERR_CUDA);
     cudaMemset(h->olbar_d, 0, nbar);
@@ -756,11 +757,12 @@ static int step_once(mgpu_handle* h, DevState<T>& d) {
   if (needs_mean_profiles(h->cfg)) {
     h->launches += launch_mean_profiles<T>(h->sc, d.zu_n, d.zv_n, d.th, d.q, h->olz_d, h->stream);
     // u + ugal, v + vgal (stepfields.F90 adds the Galilean velocity before the solver group) and
-    // the old theta, time-smoothed on a centred step; the swap left the old th, zth in th_n, zth_n
+    // the old theta and q, time-smoothed on a centred step; the swap left the old th, zth, q, zq
+    // in th_n, zth_n, q_n, zq_n
     const bool fwd = h->sc.forward != 0;
-    h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th_n, fwd ? nullptr : d.zth_n, h->sc.ugal,
-                                                 h->sc.vgal, 1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d,
-                                                 h->stream);
+    h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th_n, fwd ? nullptr : d.zth_n, d.q_n,
+                                                 fwd ? nullptr : d.zq_n, h->sc.ugal, h->sc.vgal,
+                                                 1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d, h->stream);
   }
   // The FFT solve of a power-of-two nx forms the source inside its first transform (fast
   // build); the reproducible build keeps the source kernel, whose rounding the oracle matches.
@@ -977,8 +979,8 @@ static int component(mgpu_handle* h, DevState<T>& d, int cid) {
     case MGPU_C_MEAN_PROFILES:
       // the component fields already hold u + ugal and the time-smoothed theta, as MONC's do
       h->launches += launch_mean_profiles<T>(h->sc, d.zu, d.zv, d.zth, d.zq, h->olz_d, h->stream);
-      h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th, nullptr, 0.0, 0.0, 1.0, 0.0, h->olbar_d,
-                                                   h->stream);
+      h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th, nullptr, d.q, nullptr, 0.0, 0.0, 1.0, 0.0,
+                                                   h->olbar_d, h->stream);
       break;
     case MGPU_C_FORCING:
       h->launches += subsidence_tendencies(h);
@@ -1126,8 +1128,8 @@ int mgpu_checkpoint_write(mgpu_handle* h, const char* path) {
   std::vector<double> mean;
   const bool with_mean = needs_mean_profiles(h->cfg);
   if (with_mean) {
-    // the olz*bar rows come first; olubar, olvbar, olthbar follow and are not checkpointed
-    mean.resize((size_t)(6 + h->cfg.number_q_fields) * h->cfg.nz);
+    // (3 + nq) rows of olz*bar, then olubar, olvbar, olthbar, olqbar(n)
+    mean.resize((size_t)(6 + 2 * h->cfg.number_q_fields) * h->cfg.nz);
     if (int rc = mgpu_mean_profiles(h, mean.data())) return rc;
   }
   mgpu_checkpoint_meta meta{};
@@ -1145,7 +1147,7 @@ int mgpu_checkpoint_read(mgpu_handle* h, const char* path) {
   checkpoint_fields(h, buf, ids);
   std::vector<double*> ptr;
   for (auto& b : buf) ptr.push_back(b.data());
-  std::vector<double> mean((size_t)(3 + h->cfg.number_q_fields) * h->cfg.nz);
+  std::vector<double> mean((size_t)(6 + 2 * h->cfg.number_q_fields) * h->cfg.nz);
   int has_mean = 0;
   mgpu_checkpoint_meta meta{};
   std::string err;
@@ -1176,11 +1178,16 @@ int mgpu_checkpoint_state(mgpu_handle* h, mgpu_checkpoint_meta* meta) {
 int mgpu_restore_state(mgpu_handle* h, const mgpu_checkpoint_meta* meta, const double* mean) {
   if (!h || !meta) return MGPU_ERR_ARGUMENT;
   if (mean && h->olz_d) {
-    const int nz = h->cfg.nz;
-    std::vector<double> rows((size_t)(3 + MGPU_MAX_Q) * (nz + 2), 0.0);
-    for (int r = 0; r < 3 + h->cfg.number_q_fields; ++r)
-      for (int k = 1; k <= nz; ++k) rows[(size_t)r * (nz + 2) + k] = mean[(size_t)r * nz + k - 1];
+    // (3 + nq) rows of olz*bar, then (3 + nq) rows of olubar, olvbar, olthbar, olqbar(n)
+    const int nz = h->cfg.nz, nr = 3 + h->cfg.number_q_fields;
+    std::vector<double> rows((size_t)(3 + MGPU_MAX_Q) * (nz + 2), 0.0), bars(rows.size(), 0.0);
+    for (int r = 0; r < nr; ++r)
+      for (int k = 1; k <= nz; ++k) {
+        rows[(size_t)r * (nz + 2) + k] = mean[(size_t)r * nz + k - 1];
+        bars[(size_t)r * (nz + 2) + k] = mean[(size_t)(nr + r) * nz + k - 1];
+      }
     CK(cudaMemcpyAsync(h->olz_d, rows.data(), rows.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->olbar_d, bars.data(), bars.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
   }
   // readcheckpoint.F90 load_misc: the run continues at the step after the checkpointed one
@@ -1199,15 +1206,17 @@ int mgpu_restore_state(mgpu_handle* h, const mgpu_checkpoint_meta* meta, const d
 
 int mgpu_mean_profiles(mgpu_handle* h, double* out) {
   if (!h || !out) return MGPU_ERR_ARGUMENT;
+  // (3 + nq) rows of olz*bar, then (3 + nq) rows of olubar, olvbar, olthbar, olqbar(n)
   const int nz = h->cfg.nz, rows = 3 + h->cfg.number_q_fields;
-  std::vector<double> buf((size_t)rows * (nz + 2)), bar((size_t)3 * (nz + 2));
+  std::vector<double> buf((size_t)rows * (nz + 2)), bar((size_t)rows * (nz + 2));
   CK(cudaMemcpyAsync(buf.data(), h->olz_d, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(bar.data(), h->olbar_d, bar.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   for (int r = 0; r < rows; ++r)
-    for (int k = 1; k <= nz; ++k) out[(size_t)r * nz + k - 1] = buf[(size_t)r * (nz + 2) + k];
-  for (int r = 0; r < 3; ++r)
-    for (int k = 1; k <= nz; ++k) out[(size_t)(rows + r) * nz + k - 1] = bar[(size_t)r * (nz + 2) + k];
+    for (int k = 1; k <= nz; ++k) {
+      out[(size_t)r * nz + k - 1] = buf[(size_t)r * (nz + 2) + k];
+      out[(size_t)(rows + r) * nz + k - 1] = bar[(size_t)r * (nz + 2) + k];
+    }
   return MGPU_OK;
 }
 
@@ -1351,9 +1360,10 @@ static int step_phase(mgpu_handle* h, DevState<T>& d, int phase) {
         // this slab's means; the driver averages them across the slabs (mgpu_slab_mean_profiles)
         const bool fwd = h->sc.forward != 0;
         h->launches += launch_mean_profiles<T>(h->sc, d.zu_n, d.zv_n, d.th, d.q, h->olz_d, h->stream, h->slab_halo);
-        h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th_n, fwd ? nullptr : d.zth_n, h->sc.ugal,
-                                                     h->sc.vgal, 1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d,
-                                                     h->stream, h->slab_halo);
+        h->launches += launch_mean_profiles_state<T>(h->sc, d.u, d.v, d.th_n, fwd ? nullptr : d.zth_n, d.q_n,
+                                                     fwd ? nullptr : d.zq_n, h->sc.ugal, h->sc.vgal,
+                                                     1.0 - 2.0 * h->sc.tsmth, h->sc.tsmth, h->olbar_d, h->stream,
+                                                     h->slab_halo);
       }
       if (exact_k) exact::launch_fused_pressure_source<T>(h->sc, d, h->stream);
       else fast::launch_fused_pressure_source<T>(h->sc, d, h->stream);
@@ -1516,7 +1526,7 @@ int mgpu_slab_mean_profiles(mgpu_handle* h, double* d_buf, int32_t put) {
   if (!needs_mean_profiles(h->cfg))
     return fail(h, MGPU_ERR_ARGUMENT, "no mean profiles are kept (no damping, mean-profile subsidence or profile diagnostics)");
   const size_t row = (size_t)(h->cfg.nz + 2) * sizeof(double);
-  const size_t nz_rows = (size_t)(3 + h->cfg.number_q_fields) * row, bar = 3 * row;
+  const size_t nz_rows = (size_t)(3 + h->cfg.number_q_fields) * row, bar = nz_rows;
   if (put) {
     CK(cudaMemcpyAsync(h->olz_d, d_buf, nz_rows, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(h->olbar_d, (const char*)d_buf + nz_rows, bar, cudaMemcpyDeviceToDevice, h->stream));

@@ -9,6 +9,7 @@
 // dimension ids, attributes, type, size and 8-byte data offset) followed by each variable's data,
 // padded to 4 bytes.  Variables are laid out as MONC defines them: the Fortran dimension order
 // (z, y, x) is (x, y, zn) in the file, z varying fastest.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -402,10 +403,19 @@ int checkpoint_write_host(const mgpu_config& c, const RefState& rs, const std::s
     var("zn", NC_DOUBLE, {dzn}, doubles(&rs.zn[1], nz), metres);
     var("thref", NC_DOUBLE, {dz}, doubles(&rs.thref[1], nz));
     if (mean) {
+      // mean: (3 + nq) rows of olz*bar, then (3 + nq) rows of olubar, olvbar, olthbar, olqbar(n);
+      // writecheckpoint.F90:508-535 defines each one mean_profiles allocated
+      const double* bar = mean + (size_t)(3 + nq) * nz;
+      var("olubar", NC_DOUBLE, {dz}, doubles(bar, nz));
       var("olzubar", NC_DOUBLE, {dz}, doubles(mean, nz));
+      var("olvbar", NC_DOUBLE, {dz}, doubles(bar + nz, nz));
       var("olzvbar", NC_DOUBLE, {dz}, doubles(mean + nz, nz));
+      var("olthbar", NC_DOUBLE, {dz}, doubles(bar + 2 * nz, nz));
       var("olzthbar", NC_DOUBLE, {dz}, doubles(mean + 2 * nz, nz));
-      if (nq > 0) var("olzqbar", NC_DOUBLE, {dq, dz}, doubles(mean + 3 * nz, (size_t)nq * nz));
+      if (nq > 0) {
+        var("olqbar", NC_DOUBLE, {dq, dz}, doubles(bar + 3 * nz, (size_t)nq * nz));
+        var("olzqbar", NC_DOUBLE, {dq, dz}, doubles(mean + 3 * nz, (size_t)nq * nz));
+      }
     }
     std::vector<double> buf(npt);
     if (nq > 0) {
@@ -497,14 +507,28 @@ int checkpoint_read_host(const mgpu_config& c, const std::string& path, double* 
     meta.dtm_new = scalar_d("dtm_new", meta.dtm);
     meta.absolute_new_dtm = scalar_d("absolute_new_dtm", meta.dtm);
     meta.last_cfl_timestep = scalar_i("last_cfl_timestep", 0);
+    // readcheckpoint.F90:540-600 reads each mean profile that is present: here the olz*bar set
+    // (has_mean 1) and, when it is complete too, the olubar, olvbar, olthbar, olqbar set (has_mean
+    // 2; otherwise those rows are zero)
     *has_mean = 0;
     if (mean && f.var("olzubar") && f.var("olzvbar") && f.var("olzthbar") && (nq == 0 || f.var("olzqbar"))) {
-      const char* names[3] = {"olzubar", "olzvbar", "olzthbar"};
-      for (int r = 0; r < 3; ++r)
-        for (int k = 0; k < nz; ++k) mean[r * nz + k] = get_double(need(names[r]), k);
-      for (int n = 0; n < nq; ++n)
-        for (int k = 0; k < nz; ++k) mean[(3 + n) * nz + k] = get_double(need("olzqbar"), (size_t)n * nz + k);
+      const size_t rows = (size_t)(3 + nq);
+      auto read_set = [&](const char* const* names, const char* qname, double* out) {
+        for (int r = 0; r < 3; ++r)
+          for (int k = 0; k < nz; ++k) out[r * nz + k] = get_double(need(names[r]), k);
+        for (int n = 0; n < nq; ++n)
+          for (int k = 0; k < nz; ++k) out[(3 + n) * nz + k] = get_double(need(qname), (size_t)n * nz + k);
+      };
+      const char* zn[3] = {"olzubar", "olzvbar", "olzthbar"};
+      read_set(zn, "olzqbar", mean);
       *has_mean = 1;
+      double* bar = mean + rows * nz;
+      std::fill(bar, bar + rows * nz, 0.0);
+      if (f.var("olubar") && f.var("olvbar") && f.var("olthbar") && (nq == 0 || f.var("olqbar"))) {
+        const char* bn[3] = {"olubar", "olvbar", "olthbar"};
+        read_set(bn, "olqbar", bar);
+        *has_mean = 2;
+      }
     }
   } catch (std::exception& e) {
     err = e.what();

@@ -117,10 +117,12 @@ int launch_mean_profiles(const Scalars& s, const T* zu, const T* zv, const T* th
                          cudaStream_t st, int halo = 0);
 int launch_subsidence_tendencies(const Scalars& s, const double* olz, double* tend, bool flow_theta, bool q,
                                  cudaStream_t st);
-// olubar, olvbar, olthbar from u, v and theta (zth given: theta after time smoothing c1 th + c2 zth)
+// olubar, olvbar, olthbar, olqbar(n) from u, v, theta and the q fields (q may be null: no olqbar);
+// zth, zq given: the scalars after time smoothing c1 f + c2 zf
 template <typename T>
-int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth, double ugal,
-                               double vgal, double c1, double c2, double* olbar, cudaStream_t st, int halo = 0);
+int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth,
+                               const T* const* q, const T* const* zq, double ugal, double vgal, double c1, double c2,
+                               double* olbar, cudaStream_t st, int halo = 0);
 // profile_diagnostics sums into out (MGPU_PD_* rows of nz); qv, ql null for a dry model.  With halo
 // > 0 (a y-slab) the means and sums run over the interior rows halo .. ny-1-halo
 template <typename T>

@@ -68,11 +68,12 @@ template int launch_mean_profiles<float>(const Scalars&, const float*, const flo
 template int launch_mean_profiles<double>(const Scalars&, const double*, const double*, const double*,
                                           const double* const*, double*, cudaStream_t, int);
 
-// olubar, olvbar, olthbar: the means of ugal + u, vgal + v and of theta, with zth (time
-// smoothing c1 th + c2 zth) when given
+// olubar, olvbar, olthbar and olqbar(n): the means of ugal + u, vgal + v, theta and each q field,
+// the scalars time-smoothed (c1 f + c2 zf) where their z-fields are given
 template <typename T>
-int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth, double ugal,
-                               double vgal, double c1, double c2, double* olbar, cudaStream_t st, int halo) {
+int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T* th, const T* zth,
+                               const T* const* q, const T* const* zq, double ugal, double vgal, double c1, double c2,
+                               double* olbar, cudaStream_t st, int halo) {
   MeanFields<T> f{};
   f.p[0] = u;
   f.c[0] = ugal;
@@ -82,15 +83,23 @@ int launch_mean_profiles_state(const Scalars& s, const T* u, const T* v, const T
   f.p2[2] = zth;
   f.a[2] = c1;
   f.b[2] = c2;
-  k_plane_means<T><<<dim3(s.nz, 3), 256, 0, st>>>(f, s.plane, (long long)halo * s.nx, interior(s, halo),
-                                                  rnhpts(s, halo), olbar, s.nz + 2);
+  const int nq = q ? s.nq : 0;
+  for (int n = 0; n < nq; ++n) {
+    f.p[3 + n] = q[n];
+    f.p2[3 + n] = zq ? zq[n] : nullptr;
+    f.a[3 + n] = c1;
+    f.b[3 + n] = c2;
+  }
+  k_plane_means<T><<<dim3(s.nz, 3 + nq), 256, 0, st>>>(f, s.plane, (long long)halo * s.nx, interior(s, halo),
+                                                       rnhpts(s, halo), olbar, s.nz + 2);
   return 1;
 }
 template int launch_mean_profiles_state<float>(const Scalars&, const float*, const float*, const float*, const float*,
-                                               double, double, double, double, double*, cudaStream_t, int);
+                                               const float* const*, const float* const*, double, double, double,
+                                               double, double*, cudaStream_t, int);
 template int launch_mean_profiles_state<double>(const Scalars&, const double*, const double*, const double*,
-                                                const double*, double, double, double, double, double*, cudaStream_t,
-                                                int);
+                                                const double*, const double* const*, const double* const*, double,
+                                                double, double, double, double*, cudaStream_t, int);
 
 // profile_diagnostics (profile_diagnostics.F90:311-636, PW flow and TVD scalars): one block per
 // level sums the MGPU_PD_* quantities over the plane in FP64, in a fixed order

@@ -274,7 +274,8 @@ class _Slab:
         self.x64_bufs = [torch.zeros(g.nz * g.nx, dtype=torch.float64, device=device) for _ in range(4)]
         self.means = torch.zeros((1 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
         # the mean profiles damping, subsidence and profile_diagnostics read (mgpu_slab_mean_profiles)
-        self.profiles = torch.zeros((6 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64, device=device)
+        self.profiles = torch.zeros(2 * (3 + model.cfg.number_q_fields) * (g.nz + 2), dtype=torch.float64,
+                                    device=device)
         # cfltest's six extrema, every one combined by a maximum (mgpu_slab_cfl_extrema)
         self.cfl = torch.zeros(6, dtype=torch.float64, device=device)
         # the iterative solve's dot products of one step (mgpu_slab_iter)
@@ -477,9 +478,7 @@ class SlabDomain:
         m = self.slabs[0].m
         mean = None
         if self.mean_profiles:
-            mp = m.mean_profiles()
-            nq = self.cfg.number_q_fields
-            mean = np.stack([mp["olzubar"], mp["olzvbar"], mp["olzthbar"]] + [mp[f"olzqbar{n}"] for n in range(nq)])
+            mean = m.mean_profile_rows()
         meta = m.checkpoint_state()
         if 0 in self.comm.local_ranks:
             api.checkpoint_write_host(self.cfg, path, fields, meta, mean)

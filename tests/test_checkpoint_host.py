@@ -25,7 +25,8 @@ def dry_case():
     cf.enable_damping(c, 0.01, 150.0, 80.0)
     st = ini.random_flow_state(NX, NY, NZ, seed=3, amp_uv=1.0, amp_w=0.3, amp_th=0.5, ug=3.0)
     st["p"] = np.random.default_rng(1).normal(size=(NZ, NY, NX))
-    mean = np.random.default_rng(2).normal(size=(3, NZ))
+    # mgpu_mean_profiles' rows: olzubar, olzvbar, olzthbar, then olubar, olvbar, olthbar
+    mean = np.random.default_rng(2).normal(size=(6, NZ))
     return c, st, mean
 
 
@@ -72,7 +73,9 @@ def test_layout_read_by_scipy(tmp_path):
                           ("zv", "zv"), ("zw", "zw"), ("zth", "zth"), ("p", "p")):
             assert v[name].dimensions == ("x", "y", "zn"), name
             np.testing.assert_array_equal(v[name].data, st[src].transpose(2, 1, 0), err_msg=name)
-        for name, row in (("olzubar", 0), ("olzvbar", 1), ("olzthbar", 2)):
+        for name, row in (("olzubar", 0), ("olzvbar", 1), ("olzthbar", 2), ("olubar", 3), ("olvbar", 4),
+                          ("olthbar", 5)):
+            assert v[name].dimensions == ("z",), name
             np.testing.assert_array_equal(v[name].data, mean[row])
         np.testing.assert_array_equal(v["z"].data, api.reference_profile(c, "z"))
         np.testing.assert_array_equal(v["zn"].data, api.reference_profile(c, "zn"))
@@ -95,7 +98,8 @@ def test_layout_read_by_scipy(tmp_path):
 def test_moist_q_fields_and_indices(tmp_path):
     c, st = moist_case()
     path = str(tmp_path / "ck.nc")
-    api.checkpoint_write_host(c, path, st, meta())
+    mean = np.random.default_rng(4).normal(size=(10, NZ))  # olz*bar (3 + 2 q), ol*bar (3 + 2 q)
+    api.checkpoint_write_host(c, path, st, meta(), mean)
     nc = netcdf_file(path, "r", mmap=False)
     try:
         v = nc.variables
@@ -106,11 +110,15 @@ def test_moist_q_fields_and_indices(tmp_path):
         names = [b"".join(qi[q, 0]).rstrip(b"\0").decode() for q in range(qi.shape[0])]
         assert names == ["vapour", "cloud_liquid_mass"]
         assert int(v["nqfields"].data) == 2
+        for name, rows in (("olzqbar", mean[3:5]), ("olqbar", mean[8:10])):
+            assert v[name].dimensions == ("q", "z"), name
+            np.testing.assert_array_equal(v[name].data, rows, err_msg=name)
     finally:
         nc.close()
-    f, _, _ = api.checkpoint_read_host(c, path)
+    f, m, _ = api.checkpoint_read_host(c, path)
     for k in ("q0", "q1", "zq0", "zq1"):
         np.testing.assert_array_equal(f[k], st[k], err_msg=k)
+    np.testing.assert_array_equal(m, mean)
 
 
 def test_reads_a_classic_file_in_monc_layout(tmp_path):
@@ -134,6 +142,31 @@ def test_reads_a_classic_file_in_monc_layout(tmp_path):
     for k in api.CHECKPOINT_FIELDS:
         np.testing.assert_array_equal(f[k], st[k], err_msg=k)
     assert mean is None and md.timestep == 11 and md.time == 11.5 and md.last_cfl_timestep == 10
+
+
+def test_reads_the_olz_profiles_alone(tmp_path):
+    """MONC reads each mean profile only if the file has it: a file with olzubar, olzvbar and
+    olzthbar but no olubar, olvbar, olthbar gives those rows, the others zero."""
+    c, st, mean = dry_case()
+    path = str(tmp_path / "ck.nc")
+    api.checkpoint_write_host(c, path, st, meta(), mean)
+    src = netcdf_file(path, "r", mmap=False)
+    dst_path = str(tmp_path / "olz_only.nc")
+    dst = netcdf_file(dst_path, "w", version=2)
+    try:
+        for name, n in src.dimensions.items():
+            dst.createDimension(name, n)
+        for name, var in src.variables.items():
+            if name in ("olubar", "olvbar", "olthbar"):
+                continue
+            out = dst.createVariable(name, var.data.dtype, var.dimensions)
+            out[...] = var.data
+    finally:
+        src.close()
+        dst.close()
+    _, m, _ = api.checkpoint_read_host(c, dst_path)
+    np.testing.assert_array_equal(m[:3], mean[:3])
+    assert not m[3:].any()
 
 
 def test_refuses_a_different_grid(tmp_path):

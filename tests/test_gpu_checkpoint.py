@@ -46,10 +46,15 @@ def restart_matches(c, st, n1, n2, path, extra=()):
     b.set_state(st)
     b.step(n1)
     b.checkpoint_write(path)
+    keep = bool(c.damping_enabled or c.l_subs_pl_theta or c.l_subs_pl_q)
+    mp = b.mean_profiles() if keep else {}
     b.close()
     d = api.Model(c)
     d.checkpoint_read(path)
     assert d.reductions().timestep == n1 + 1
+    # every mean profile comes back: olz*bar and olubar, olvbar, olthbar, olqbar(n)
+    for n, prof in (d.mean_profiles() if keep else {}).items():
+        np.testing.assert_array_equal(prof, mp[n], err_msg=n)
     d.step(n2)
     for f in names:
         np.testing.assert_array_equal(d.download(f), ref[f], err_msg=f)
