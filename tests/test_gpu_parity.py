@@ -194,3 +194,18 @@ def test_fma_variant_close_to_exact(gpu_lib, precision):
     tol = 1e-12 if precision == cf.FP64 else 1e-4
     for f in STATE_FIELDS:
         assert rel_err(res[1][f], res[0][f]) <= tol, f
+
+
+@pytest.mark.parametrize("precision", [cf.FP64, cf.FP32_MIXED], ids=["fp64", "fp32"])
+def test_device_level_means_match_numpy(gpu_lib, precision):
+    """mgpu_diagnostics' per-level sums (a cluster of blocks per level, partial sums added in rank
+    order) give the horizontal mean theta (with thref) and mean w**2 of the downloaded fields."""
+    o, m = cbl_pair(n=64, nz=40, precision=precision)
+    m.step(3)
+    th, w = m.download("th"), m.download("w")
+    th_mean, w2_mean = m.diagnostics()
+    thref = api.reference_profile(m.cfg, "thref")
+    np.testing.assert_allclose(th_mean, th.mean(axis=(1, 2)) + thref, rtol=1e-12, atol=0.0)
+    np.testing.assert_allclose(w2_mean, (w * w).mean(axis=(1, 2)), rtol=1e-12, atol=1e-300)
+    m.close()
+    o.close()
