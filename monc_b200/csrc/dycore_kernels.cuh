@@ -631,6 +631,12 @@ constexpr int min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
 // the scalar and Smagorinsky kernels fit 80 registers without spilling, and their shared memory
 // allows three CTAs per SM in FP64 too
 constexpr int min_ctas3() { return 3; }
+// resident CTAs per SM of the centred-step kernels: FP32 fits all three in 64 registers (no
+// spills) and four CTAs' shared memory; FP64 runs three scalar and Smagorinsky CTAs, two momentum
+template <typename T>
+constexpr int ctas_scalar() { return sizeof(T) == 4 ? 4 : 3; }
+template <typename T>
+constexpr int ctas_momentum() { return sizeof(T) == 4 ? 4 : 2; }
 constexpr int M_PLANES = 7 * RM;   // u v w zu zv zw vis
 template <typename T>
 constexpr size_t smag_smem() { return sizeof(T) * ((size_t)3 * RM * G<T>::PLANE + (size_t)RP * P_COUNT); }
@@ -774,7 +780,7 @@ __device__ __forceinline__ CRing<T> cring(const T* ring, int k, int co, int j, i
 // Each CTA runs the levels kb..ke of its tile, kb = 2 + blockIdx.z * kchunk: splitting the level
 // range gives enough CTAs to fill every SM on grids with few tiles.
 template <typename T, bool TVD>
-__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas<T>()) k_f_momentum_tiled(Scalars s, DevState<T> d,
+__global__ void __launch_bounds__(tiled::NT, tiled::ctas_momentum<T>()) k_f_momentum_tiled(Scalars s, DevState<T> d,
                                                                                       int kchunk) {
   using namespace tiled;
   using Gt = G<T>;
@@ -907,7 +913,7 @@ struct ScalarJob {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_scalar_tiled(Scalars s, DevState<T> d,
+__global__ void __launch_bounds__(tiled::NT, tiled::ctas_scalar<T>()) k_f_scalar_tiled(Scalars s, DevState<T> d,
                                                                                     int kchunk, ScalarJob<T> job) {
   using namespace tiled;
   using Gt = G<T>;
@@ -1429,7 +1435,7 @@ __global__ void __launch_bounds__(256) k_f_cloud_step(Scalars s, DevState<T> d) 
 // ring, the Richardson-number inputs (th, q) read at the column itself.  The chunk holding level
 // nz-1 also zeroes vis and diff at the top level.  Level 1 (lower_bc) is k_c_lower_bc.
 template <typename T>
-__global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_smag_tiled(Scalars s, DevState<T> d,
+__global__ void __launch_bounds__(tiled::NT, tiled::ctas_scalar<T>()) k_f_smag_tiled(Scalars s, DevState<T> d,
                                                                                   int kchunk) {
   using namespace tiled;
   using Gt = G<T>;
