@@ -438,7 +438,7 @@ def precision_moist():
     from monc_b200 import config as cf, precision as pr
 
     a = _ap.Namespace(nx=512, ny=512, nz=160, dx=35.0, dz_bottom=5.0, dz_top=20.0, dt=0.3, steps=500, seed=1,
-                      noise_levels=10, solver="fft", tolerance=1e-12)
+                      noise_levels=10, solver="fft", tolerance=1e-4)
     f64, f32 = {}, {}
     ms64, th64, w64, qv64, _ = pr.run(a, cf.FP64, fields=f64)
     ms32, th32, w32, qv32, _ = pr.run(a, cf.FP32_MIXED, fields=f32)
@@ -449,26 +449,32 @@ def precision_moist():
            "speedup": round(ms64 / ms32, 3), "rel_err_mean_theta": pr.rel(th32, th64),
            "rel_err_mean_w2": pr.rel(w32, w64), "rel_err_mean_qv": pr.rel(qv32, qv64),
            "fields_fp32_vs_fp64": per_field}
-    # the same layer with the iterative solver (BiCGStab to 1e-12, FP64 refinement in the FP32-mixed
-    # run) over its first ITER_STEPS steps
-    ai = _ap.Namespace(**{**vars(a), "solver": "iterative", "steps": ITER_STEPS})
-    g64, g32 = {}, {}
-    mi64, ti64, wi64, _, _ = pr.run(ai, cf.FP64, fields=g64)
-    it64 = ai.iterations_per_step
-    mi32, ti32, wi32, _, _ = pr.run(ai, cf.FP32_MIXED, fields=g32)
-    it32 = ai.iterations_per_step
-    out["iterative"] = {"steps": ITER_STEPS, "tolerance": 1e-12, "solver": "BiCGStab",
-                        "fp64_ms_per_step": round(mi64, 4), "fp32_mixed_ms_per_step": round(mi32, 4),
-                        "speedup": round(mi64 / mi32, 3),
-                        "iterations_per_step": {"fp64": round(it64, 2), "fp32_mixed": round(it32, 2)},
-                        "rel_err_mean_theta": pr.rel(ti32, ti64), "rel_err_mean_w2": pr.rel(wi32, wi64),
-                        "fields_fp32_vs_fp64": pr.field_errors(g32, g64)}
+    # the same layer with the iterative solver over its first ITER_STEPS steps (BiCGStab, FP64
+    # refinement around FP32 corrections in the FP32-mixed run): at MONC's default tolerance and at
+    # a strict one
+    runs = []
+    for tol in ITER_TOLERANCES:
+        ai = _ap.Namespace(**{**vars(a), "solver": "iterative", "steps": ITER_STEPS, "tolerance": tol})
+        g64, g32 = {}, {}
+        mi64, ti64, wi64, _, _ = pr.run(ai, cf.FP64, fields=g64)
+        it64 = ai.iterations_per_step
+        mi32, ti32, wi32, _, _ = pr.run(ai, cf.FP32_MIXED, fields=g32)
+        it32 = ai.iterations_per_step
+        runs.append({"tolerance": tol, "fp64_ms_per_step": round(mi64, 4), "fp32_mixed_ms_per_step": round(mi32, 4),
+                     "speedup": round(mi64 / mi32, 3),
+                     "iterations_per_step": {"fp64": round(it64, 2), "fp32_mixed": round(it32, 2)},
+                     "rel_err_mean_theta": pr.rel(ti32, ti64), "rel_err_mean_w2": pr.rel(wi32, wi64),
+                     "fields_fp32_vs_fp64": pr.field_errors(g32, g64)})
+    out["iterative"] = {"steps": ITER_STEPS, "solver": "BiCGStab", "max_iterations": 500, "by_tolerance": runs}
     return out
 
 
-# steps of the iterative-solver run on the moist layer (each BiCGStab solve to 1e-12 takes over a
-# hundred iterations, 0.35 s a step in FP64; the full 500 steps would hold the bench for minutes)
+# steps of the iterative-solver runs on the moist layer, and their tolerances: 1e-4 is MONC's
+# default (global_config), 1e-8 a strict one.  Much below 1e-8 the FP64 solve, which like MONC's
+# has no compatibility shift, stalls near a relative residual of 5e-8 on this layer and ends most
+# solves at the iteration cap.
 ITER_STEPS = 20
+ITER_TOLERANCES = (1e-4, 1e-8)
 
 
 def _large_run(precision, fields=None):

@@ -1214,7 +1214,7 @@ __global__ void __launch_bounds__(tiled::NT, tiled::min_ctas3()) k_f_flow_tvd_ti
 // to memory, the flow, diff and the Courant sums are staged once for the three scalars, and the
 // results are those of the point kernel, to the bit.
 template <typename T>
-__global__ void __launch_bounds__(tiled::NT, 2) k_f_moist_tiled(Scalars s, DevState<T> d, int kchunk) {
+__global__ void __launch_bounds__(tiled::NT, sizeof(T) == 4 ? 3 : 2) k_f_moist_tiled(Scalars s, DevState<T> d, int kchunk) {
   using namespace tiled;
   using Gt = G<T>;
   typedef MoistRings R;

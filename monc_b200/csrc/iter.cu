@@ -21,7 +21,8 @@
 // converged, so the host launches iterations in batches and reads the state back once a batch.
 //
 // The FP32-mixed model solves in FP64 by iterative refinement: r = b - A x in FP64, an FP32
-// BiCGStab solve of A e = r, x += e, until the FP64 residual meets the tolerance.
+// BiCGStab solve of A e = r to a relative residual set by the FP64 one (inner_tolerance), x += e,
+// until the FP64 residual meets the tolerance.
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -775,6 +776,15 @@ static int solve_fp64(IterSolverDev* it, const Scalars& s, double* p, cudaStream
   return rc;
 }
 
+// The relative residual reduction asked of an FP32 correction solve: enough to bring the FP64
+// residual err to half the tolerance, but no more than a factor 1e-3, which the FP32 iteration
+// reaches in a few tens of iterations.  A fixed 1e-5 over-solved at loose tolerances and, on large
+// grids (512 x 512 x 160), ran into the FP32 iteration's attainable accuracy and the iteration cap.
+static double inner_tolerance(double err, double tol) {
+  const double t = 0.5 * tol / err;
+  return t < 1e-3 ? 1e-3 : (t > 0.5 ? 0.5 : t);
+}
+
 static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream_t st, int64_t* launches,
                        int* iterations, double* residual) {
   if (!it || !it->fp32) return MGPU_ERR_ARGUMENT;
@@ -818,12 +828,13 @@ static int solve_mixed(IterSolverDev* it, const Scalars& s, float* p, cudaStream
       break;
     }
     prev_err = err;
-    // FP32 correction solve A e = r, from e = 0, to a relative residual of 1e-5
+    // FP32 correction solve A e = r, from e = 0, to the relative residual inner_tolerance asks
     if (cudaMemsetAsync(it->w32.x, 0, (size_t)n * sizeof(float), st) != cudaSuccess) return MGPU_ERR_CUDA;
     int its = 0;
     double inner = 0.0;
-    int irc = it->symm ? run_cg<float>(it, it->w32, 1e-5, 1e-300, false, st, launches, &its, &inner)
-                       : run_bicgstab<float>(it, it->w32, 1e-5, 1e-300, st, launches, &its, &inner);
+    const double itol = inner_tolerance(err, it->tol);
+    int irc = it->symm ? run_cg<float>(it, it->w32, itol, 1e-300, false, st, launches, &its, &inner)
+                       : run_bicgstab<float>(it, it->w32, itol, 1e-300, st, launches, &its, &inner);
     if (irc != MGPU_OK && irc != MGPU_ERR_NOT_CONVERGED) return irc;
     total += its;
     k_add_correction<<<592, 256, 0, st>>>(x64, it->w32.x, s.plane, n, 1.0);
@@ -951,10 +962,10 @@ int iter_slab_step(IterSolverDev* it, int step, double* d_sums, cudaStream_t st,
       nsum = 2;
       break;
     case MGPU_SLAB_ITER_INNER:
-      // the FP32 correction solve A e = r, from e = 0, to a relative residual of 1e-5
+      // the FP32 correction solve A e = r, from e = 0, to the relative residual inner_tolerance asks
       if (!it->fp32) return MGPU_ERR_ARGUMENT;
       if (cudaMemsetAsync(it->w32.x, 0, (size_t)n * sizeof(float), st) != cudaSuccess) return MGPU_ERR_CUDA;
-      slab_scalars(it, 1e-5, st);
+      slab_scalars(it, inner_tolerance(it->slab_err, it->tol), st);
       it->inner32 = true;
       it->sc_floor = 1e-300;
       it->scale_rhs = false;

@@ -105,7 +105,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--noise-levels", type=int, default=10)
     ap.add_argument("--solver", choices=["fft", "iterative"], default="fft")
-    ap.add_argument("--tolerance", type=float, default=1e-12)
+    ap.add_argument("--tolerance", type=float, default=1e-4)
     ap.add_argument("--no-control", dest="control", action="store_false",
                     help="skip the FP64 run with separately rounded multiply-adds")
     a = ap.parse_args(argv)
