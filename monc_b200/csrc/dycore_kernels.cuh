@@ -1668,14 +1668,17 @@ int launch_component(int cid, const Scalars& s, DevState<T>& d, cudaStream_t st,
 }
 
 // Number of level chunks for a grid of `tiles` tiles: the count (chunks of at least 8 levels) whose
-// CTAs fill the resident slots most evenly; each extra chunk costs a few staged levels.
-static inline int choose_level_chunks(int tiles, int slots, int levels) {
+// CTAs fill the resident slots most evenly; each extra chunk costs a few staged levels, weighed
+// by `per_chunk` against the fill.  The scalar kernel takes a smaller weight: its CTAs vary in
+// duration with the limiter's path, so more and shorter chunks balance the SMs better, and
+// staging is a small part of its level.
+static inline int choose_level_chunks(int tiles, int slots, int levels, double per_chunk = 0.01) {
   int best = 1;
   double best_score = -1.0;
   for (int n = 1; n <= 16 && levels / n >= 8; ++n) {
     const long long ctas = (long long)tiles * n;
     const long long waves = (ctas + slots - 1) / slots;
-    const double score = (double)ctas / (double)(waves * slots) - 0.01 * n;
+    const double score = (double)ctas / (double)(waves * slots) - per_chunk * n;
     if (score > best_score + 1e-9) { best_score = score; best = n; }
   }
   return best;
@@ -1779,7 +1782,7 @@ int launch_fused_dynamics(const Scalars& s, DevState<T>& d, cudaStream_t st, cud
     if (nsm < 1) nsm = 1;
   }
   const int tiles = (s.nx / tiled::TX) * (s.ny / tiled::TY), levels = s.nz - 1;
-  const int nc_s = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ_s * nsm, levels);
+  const int nc_s = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ_s * nsm, levels, 0.002);
   const int nc_m = s.level_chunks > 0 ? s.level_chunks : choose_level_chunks(tiles, occ_m * nsm, levels);
   const int kc_s = (levels + nc_s - 1) / nc_s, kc_m = (levels + nc_m - 1) / nc_m;
   dim3 block(tiled::TX, tiled::TY, 1);
