@@ -568,7 +568,9 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
  *     REFINE, sum, FINISH                     r = b - A x in FP64; stop when FINISH reports done
  *     if the residual did not fall below the last one: UNCORRECT (x -= e) and stop
  *     INNER                                   e = 0; then the BiCGStab or conjugate-gradient
- *                                             steps above on the FP32 vectors, to 1e-5
+ *                                             steps above on the FP32 vectors, to a relative
+ *                                             residual of 0.5 tolerance / (the FP64 residual),
+ *                                             kept within 1e-3 .. 0.5
  *     CORRECT                                 x += e
  *   END                                       p = x
  *
