@@ -529,7 +529,7 @@ int mgpu_slab_cfl_extrema(mgpu_handle* h, double* d_buf, int32_t put, int32_t* g
  *
  * The reducing steps write this slab's sums over its interior rows to d_sums (3 doubles on the
  * device); the driver replaces them by their sum over the slabs and passes them to FINISH,
- * which updates the solver scalars and sets *done (every slab reaches the same verdict from
+ * which updates the solver scalars and sets *done (every slab reaches the same decision from
  * the same sums).  As in mgpu_step, a solve that stops at max_iterations above the tolerance is
  * not an error (MONC only warns); mgpu_get_reductions reports its iterations and residual. */
 #define MGPU_SLAB_ITER_BEGIN      0
