@@ -195,10 +195,11 @@ __device__ T half_squared_strain(const Scalars& s, const PA& P, const A& U, cons
   return half_squared_strain_parts<T, A, PA>(s, P, U, V, W, k, j, i, lo, hi);
 }
 
-// moist_ri_2 for one level (RICHARDSON_NUMBER_CALCULATION = 2)
-template <typename T, class A, class PA>
+// moist_ri_2 for one level (RICHARDSON_NUMBER_CALCULATION = 2); with NUM, ri * ssq (the number
+// without its 1/ssq factor)
+template <typename T, class A, class PA, bool NUM = false>
 __device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A& QV, const A& QL, int k, int j, int i) {
-  T tmpinv = rcp(ssq);
+  T tmpinv = NUM ? (T)1.0 : rcp(ssq);
   T scltmp = P(P_RDZN, k + 1) * P(P_BUOY_CO, k);
   const T rl = (T)s.rlvap_over_cp, eps = (T)s.eps;
   const T qsat = P(P_QSAT, k), dq = P(P_DQSATDT, k), rpr = P(P_RPREFRCP, k), tst = P(P_TSTARPR, k), fac = P(P_QSATFAC, k);
@@ -224,7 +225,8 @@ __device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A
     (void)thr;
     (void)thr1;
     (void)tref;
-    return scltmp * tmpinv * ((T)s.thconb * (qt_kp1 - qt_k) + (dl - du) * (T)s.repsh);
+    if constexpr (NUM) return scltmp * ((T)s.thconb * (qt_kp1 - qt_k) + (dl - du) * (T)s.repsh);
+    else return scltmp * tmpinv * ((T)s.thconb * (qt_kp1 - qt_k) + (dl - du) * (T)s.repsh);
   }
   T qlli = tmax<T>((T)0.0, (qt_k - (qsat + dq * (rpr * thlpr_k - tst))) * fac);
   T qlui = tmax<T>((T)0.0, (qt_kp1 - (qsat + dq * (rpr * (thlpr_kp1 + thr1) - tst - tref))) * fac);
@@ -239,13 +241,44 @@ __device__ T moist_ri(const Scalars& s, const PA& P, T ssq, const A& TH, const A
   T qlun = tmax<T>((T)0.0, (qtun - (qsat + dq * (rpr * (thlpr_un + thr1) - tst - tref))) * fac);
   T thvln = thlpr_ln + thr + (rl * pr - (T)s.thcona) * qlln;
   T thvun = thlpr_un + thr1 + (rl * pr - (T)s.thconap1) * qlun;
-  return scltmp * tmpinv * ((T)s.thconb * (qt_kp1 - qt_k) + ((thvln - thvli) - (thvun - thvui)) * (T)s.repsh);
+  if constexpr (NUM) return scltmp * ((T)s.thconb * (qt_kp1 - qt_k) + ((thvln - thvli) - (thvun - thvui)) * (T)s.repsh);
+  else return scltmp * tmpinv * ((T)s.thconb * (qt_kp1 - qt_k) + ((thvln - thvli) - (thvun - thvui)) * (T)s.repsh);
 }
 
 // vis/diff at level 2 <= k <= nz-1 from the strain rate and Richardson number
 template <typename T, class PA, class ATC, class AT>
 __device__ void smagorinsky_from_strain(const Scalars& s, const PA& P, T ssq, const ATC& THcur, const AT& THarg,
                                         const AT* QV, const AT* QL, int k, int j, int i, T& vis, T& diff) {
+#ifdef MGPU_CONTRACTED
+  // The contracted build folds the neutral factor sqrt(ssq) into the unstable branch's stability
+  // functions: with X = ri ssq (the Richardson number's numerator), sqrt(1 - c ri) sqrt(ssq) =
+  // sqrt(ssq - c X), so that branch, the common one in a convective layer, takes two square roots
+  // and no division where MONC's order takes three and one.  The branches are the same (ri and X
+  // have one sign); the values agree to rounding.
+  T X = (T)0.0;
+  if (!s.passive_th) {
+    if (!s.passive_q) X = moist_ri<T, AT, PA, true>(s, P, ssq, THarg, *QV, *QL, k, j, i);
+    else X = (P(P_DTHREF, k) + THcur(k + 1, j, i) - THcur(k, j, i)) * P(P_RDZN, k + 1) * P(P_BUOY_CO, k);
+  }
+  const T rn = P(P_RNEUTML_SQ, k);
+  if (X <= (T)0.0) {
+    vis = rn * sqrt(ssq - (T)s.subc * X);
+    diff = rn * ((T)s.suba * sqrt(ssq - (T)s.subb * X));
+  } else {
+    const T ri = X / ssq;
+    if (ri < (T)s.ric) {
+      T t = (T)1. - ri * (T)s.ricinv;
+      t = t * t;
+      const T rifac = t * t;
+      const T sctmp = rn * sqrt(ssq);
+      vis = (rifac * ((T)1. - (T)s.subh * ri)) * sctmp;
+      diff = (rifac * (T)s.suba * ((T)1. - (T)s.subg * ri)) * sctmp;
+    } else {
+      vis = (T)0.0;
+      diff = (T)0.0;
+    }
+  }
+#else
   T ri = (T)0.0;
   if (!s.passive_th) {
     if (!s.passive_q) ri = moist_ri<T, AT>(s, P, ssq, THarg, *QV, *QL, k, j, i);
@@ -269,6 +302,7 @@ __device__ void smagorinsky_from_strain(const Scalars& s, const PA& P, T ssq, co
   T sctmp = P(P_RNEUTML_SQ, k) * sqrt(ssq);
   vis = vs * sctmp;
   diff = df * sctmp;
+#endif
 }
 
 template <typename T, class A, class PA, class AT>

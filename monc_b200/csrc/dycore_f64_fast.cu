@@ -1,6 +1,8 @@
 // Instantiation of the dynamical-core kernels for FP64 fields, `fast` variant.
 // Built with the default --fmad=true: multiply-adds are contracted into FMAs.
 #define KVARIANT fast
+// contracted-build forms of some expressions (see smagorinsky_from_strain)
+#define MGPU_CONTRACTED 1
 #include "dycore_kernels.cuh"
 
 namespace mgpu {
