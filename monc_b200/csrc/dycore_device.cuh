@@ -8,6 +8,8 @@
 // up to 2 points outside [0, n) (wrapped periodically).
 #pragma once
 
+#include <type_traits>
+
 #include "mgpu_internal.h"
 
 namespace mgpu {
@@ -642,6 +644,33 @@ __device__ __forceinline__ unsigned limiter_choice(T fncs, T fnfs, T fnrefs) {
   return fncs > tmin<T>(m, (T)1.0) ? 0u : (m < (T)1.0 ? (fnfs < fnrefs ? 1u : 2u) : 3u);
 }
 
+// The limited face value fu + fdels max(fncs, min(fnfs, fnrefs, 1)), fncs = (fc - fu) / fdels',
+// fnfs = (ffs - fu) / fdels', fnrefs = fncs hrcfl, fdels' = fdels + 1e-30 (calculate_flux_in_x /
+// _y / _w), with the branch recorded.  Where |fdels| is far above the 1e-30 offset, the
+// contracted build multiplies the limiter through by fdels: max(fc - fu, min(ffs - fu,
+// (fc - fu) hrcfl, fdels)) for fdels > 0, min and max exchanged for fdels < 0.  That needs no
+// reciprocal of fdels; the values agree to rounding.
+template <typename T, class Rec = NoRec>
+__device__ __forceinline__ T limited_face(T ffs, T fc, T fu, T fdels, T hrcfl, const Rec& rec = Rec()) {
+#ifdef MGPU_CONTRACTED
+  if constexpr (std::is_same<Rec, NoRec>::value) {
+    if (fabs(fdels) > (T)1.e-20) {
+      const T a = fc - fu, b = ffs - fu, ah = a * hrcfl;
+      const T x = fdels > (T)0.0 ? tmax<T>(a, tmin<T>(tmin<T>(b, ah), fdels))
+                                 : tmin<T>(a, tmax<T>(tmax<T>(b, ah), fdels));
+      return x + fu;
+    }
+  }
+#endif
+  T rfdels = rcp_limiter(fdels + (T)1.e-30);
+  T fnfs = (ffs - fu) * rfdels;
+  T fncs = (fc - fu) * rfdels;
+  T fnrefs = fncs * hrcfl;
+  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
+  rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
+  return ftemp * fdels + fu;
+}
+
 template <typename T, class Rec = NoRec>
 __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, T fdels, T fd, T fc, T fu, T fgt1, T fgt2,
                                         T curv_term, const Rec& rec = Rec()) {
@@ -650,14 +679,8 @@ __device__ __forceinline__ T limit_face(T data_value, T c, T dt, T sum_cfl_out, 
   T hrcfl = rcp(sum_cfl_out + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = r6 * ((T)1.0 - cflmod * cflmod);
-  T rfdels = rcp_limiter(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * curv_term - fgt1 - fgt2;
-  T fnfs = (ffs - fu) * rfdels;
-  T fncs = (fc - fu) * rfdels;
-  T fnrefs = fncs * hrcfl;
-  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
-  rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
-  return ftemp * fdels + fu;
+  return limited_face<T, Rec>(ffs, fc, fu, fdels, hrcfl, rec);
 }
 
 // Sum of the outgoing Courant numbers of cell (k, j, i) without the factor dt: the sum_cfl_out
@@ -845,14 +868,8 @@ __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V,
     T hrcfl = rcp(sum + (T)1.e-30);
     T hcfl = (T)0.5 * cflmod;
     T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-    T rfdels = rcp_limiter(fdels + (T)1.e-30);
     T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
-    T fnfs = (ffs - fu) * rfdels;
-    T fncs = (fc - fu) * rfdels;
-    T fnrefs = fncs * hrcfl;
-    T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
-    rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
-    return ftemp * fdels + fu;
+    return limited_face<T, Rec>(ffs, fc, fu, fdels, hrcfl, rec);
   }
   // middle of the column
   T sm = tsign<T>((T).5, w0);
@@ -886,14 +903,8 @@ __device__ T tvd_face_z_g(const Scalars& s, const PA& P, const A& U, const A& V,
   T hrcfl = rcp(sum + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-  T rfdels = rcp_limiter(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
-  T fnfs = (ffs - fu) * rfdels;
-  T fncs = (fc - fu) * rfdels;
-  T fnrefs = fncs * hrcfl;
-  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
-  rec(limiter_choice<T>(fncs, fnfs, fnrefs), 2);
-  return ftemp * fdels + fu;
+  return limited_face<T, Rec>(ffs, fc, fu, fdels, hrcfl, rec);
 }
 
 template <typename T, class A, class AF, class PA, class M = TvdMetricScalar>
@@ -1005,13 +1016,8 @@ __device__ T tvd_face_z_bottom(const Scalars& s, const PA& P, const A& U, const 
   T hrcfl = rcp(sum + (T)1.e-30);
   T hcfl = (T)0.5 * cflmod;
   T cflcoef = (T)(1.0 / 6.0) * ((T)1.0 - cflmod * cflmod) * (dd * dd * rdc);
-  T rfdels = rcp_limiter(fdels + (T)1.e-30);
   T ffs = (T)0.5 * (fd + fc) - hcfl * (fd - fc) - cflcoef * ((fd - fc) * rdd - (fc - fu) * rdu) - fgt1 - fgt2;
-  T fnfs = (ffs - fu) * rfdels;
-  T fncs = (fc - fu) * rfdels;
-  T fnrefs = fncs * hrcfl;
-  T ftemp = tmax<T>(fncs, tmin<T>(tmin<T>(fnfs, fnrefs), (T)1.0));
-  return ftemp * fdels + fu;
+  return limited_face<T>(ffs, fc, fu, fdels, hrcfl);
 }
 
 // TVD sources of u, v (2 <= k <= nz) and w (2 <= k <= nz-1) at (k, j, i), added to su_in, sv_in,
